@@ -1,0 +1,82 @@
+/*
+ * lmieb.h -- internal interface between the C host layer (host_*.c) and the
+ * CUDA driver (driver.cu) of liblmie_b200.so.  Not installed; the public
+ * interface is include/lmie_interface.h and include/lmie_b200.h.
+ *
+ * The host layer does what the reference does on the host before its Mie
+ * core: size-distribution quadrature, moments, derivative split, and the
+ * per-radius size parameters and truncation integers (computed with the host
+ * libm so that n1(r), n2(r) and the global n1 are the reference's integers).
+ * Everything from the Mie recurrences to the phase matrix at user angles runs
+ * on the GPU.
+ */
+#ifndef LMIEB_H
+#define LMIEB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* One polydisperse problem, ready for the device.  Derivative slots are in
+ * the caller's order kk = 0..nd-1; idx1/idx2 split them like the reference's
+ * create_derivs_indexes (src/lmie_interface.c:304-353). */
+typedef struct {
+     int n;                     /* radii */
+     int nd, nd1, nd2;
+     const int *idx1;           /* [nd1] */
+     const int *idx2;           /* [nd2] */
+
+     double lambda;
+     double mr, mi;             /* m = mr - i mi */
+     const double *lambda_l;    /* [nd] */
+     const double *mr_l;        /* [nd] */
+     const double *mi_l;        /* [nd] */
+
+     /* per radius (host-computed, reference src/lmie_core.c:263-292) */
+     const double *x;           /* [n]        size parameter 2 pi r / lambda */
+     const double *xl;          /* [nd1 * n]  d x / d p for index1 slot k (row k) */
+     const double *w;           /* [(1+nd)*n] row 0: f = nr qw; row 1+kk: f_l (index1) or f_l2 (index2) */
+     const int *n1r;            /* [n] */
+     const int *n2r;            /* [n] */
+
+     int n1;                    /* global truncation at r2 */
+     int n_qang;                /* 2 n1 when gc or lc is wanted, else 0 */
+     int n_coef;                /* 2 n1 */
+
+     int want_gc, want_lc;      /* expansions requested (reference: gc/lc pointers non-NULL) */
+     int pf_from;               /* 0: no phase matrix, 1: from gc, 2: from lc */
+     int n_angles;
+     const double *mu_user;     /* [n_angles] cos(theta_i) */
+     double accuracy;
+
+     int save_control;          /* 0, 1 or 2 */
+     const double *save1_in;    /* [4*n]            save_control 2 */
+     const double *save2_in;    /* [4*n*n_qang]     save_control 2 */
+     const double *w2;          /* [nd*n] save_control 2: nr_l qw + nr qw_l per slot */
+} lmieb_problem;
+
+/* Results, in device column order: column 0 = value, column 1+kk = slot kk. */
+typedef struct {
+     double *scal;              /* [(1+nd)*4] cext, csca, cbak, g (normalised) */
+     double *gc;                /* [(1+nd)*6*n_coef] or NULL */
+     double *lc;                /* [(1+nd)*6*n_coef] or NULL */
+     double *pf;                /* [(1+nd)*6*n_angles] or NULL */
+     int n_coef_out;            /* truncated count (the reference's return value) */
+     double *save1;             /* [4*n] (save_control 1) or NULL */
+     double *save2;             /* [4*n*n_qang] (save_control 1) or NULL */
+} lmieb_result;
+
+/* Runs the device solve.  Returns 0 or -1 (after printing "ERROR: ..."). */
+int lmieb_device_solve(const lmieb_problem *p, lmieb_result *r);
+
+/* Device timing of the last lmieb_device_solve (ms per stage), for bench.py. */
+int lmieb_last_timing(double *ms, int n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
