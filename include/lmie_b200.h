@@ -53,6 +53,31 @@ int lmieb_last_work(double *flops, long long *launches, size_t *h2d, size_t *d2h
  * register-resident microbenchmark on the library's stream. */
 int lmieb_fp64_peak(double *tflops);
 
+/* Cross sections of single spheres with no device allocation.  This entry
+ * point has no counterpart in the reference.  It is for callers that cannot
+ * call cudaMalloc -- for example a model embedded in a host application whose
+ * memory pool already owns the whole GPU, or a retrieval loop that cannot
+ * afford cudaMalloc's implicit device-wide synchronisation -- and that bring
+ * their own device buffers.
+ *
+ * For each radius[i] (device memory, n_radii of them, same length unit as
+ * lambda) and m = mr - i*mi it writes to `out` (device memory, [4][n_radii])
+ * the values lmie_solution returns for a SIZE_DIST_MONO distribution of that
+ * radius: out[0][i] cext, out[1][i] csca, out[2][i] cbak, out[3][i] g.
+ *
+ * Limits: 1 <= n_radii <= 1024 and size parameters 0 < 2 pi r / lambda <= 900;
+ * larger requests return -1 with an ERROR line (out-of-range radii get NaN).
+ * The work uses a fixed 24 MiB scratch array compiled into the library, which
+ * every GPU that loads the library keeps until the process exits; no call
+ * allocates or frees device memory.  All calls on a device share that array:
+ * calls that overlap on the GPU (other threads, other streams) race on it.
+ * The first call on a device looks up the array's device address, so make it
+ * before any stream capture.  Runs on the calling thread's current device on
+ * `stream` (a cudaStream_t; NULL for the default stream) and returns after
+ * the results are in `out`.  Returns 0 or -1. */
+int lmie_cross_sections_noalloc(int n_radii, const double *radius, double lambda,
+                                double mr, double mi, double *out, void *stream);
+
 /* Name, SM count and compute capability of the device the library uses. */
 int lmieb_device_info(char *name, int len, int *sms, int *cc_major, int *cc_minor);
 
