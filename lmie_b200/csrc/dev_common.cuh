@@ -43,6 +43,12 @@ __host__ __device__ __forceinline__ cplx operator/(cplx a, cplx b) {
     }
 }
 __host__ __device__ __forceinline__ cplx operator/(double s, cplx b) { return mk(s, 0.) / b; }
+// 1/c = conj(c) / |c|^2 with one real division; for operands whose squared
+// modulus stays inside the double range (all Mie recurrence denominators do).
+__host__ __device__ __forceinline__ cplx cinv(cplx c) {
+    const double d = 1. / (c.re * c.re + c.im * c.im);
+    return mk(c.re * d, -c.im * d);
+}
 __host__ __device__ __forceinline__ cplx operator/(cplx a, double s) { return mk(a.re / s, a.im / s); }
 
 #define LMIEB_CUDA_TRY(expr)                                                              \

@@ -18,7 +18,6 @@
 namespace {
 
 constexpr int NSTAGE = LMIEB_N_STAGES;
-constexpr size_t SCRATCH_LIMIT = (size_t) 1 << 30;     // K1 recurrence scratch per radius batch
 constexpr size_t TABLE_LIMIT = (size_t) 256 << 20;     // expansion basis table per order chunk
 constexpr size_t FLUSH_BYTES = (size_t) 256 << 20;     // > 126 MB L2
 
@@ -45,7 +44,13 @@ struct Ctx {
     // state of the last solve, for re-running the device part in place
     bool have_plan = false;
     struct Plan *plan = nullptr;
+    // Gauss-Legendre angles depend only on their number: computed once per n
+    // and kept on the device (oldest entry evicted beyond GL_CACHE entries)
+    struct GlEntry { int n; double *mu; double *wq; };
+    std::vector<GlEntry> gl_cache;
 };
+
+constexpr size_t GL_CACHE = 32;
 
 Ctx g_ctx;
 std::mutex g_mu;
@@ -69,13 +74,15 @@ struct Plan {
     int nd1c = 0;               // number of index1 chunks for K1
     int n_ang_launch = 0;       // launches of K3
     int G = 0;                  // radius groups of K3
-    int nb = 0, jmax = 0;       // K1 radius batch and scratch depth
+    int2 *tiles = nullptr;      // K1b (radius, first order) per block
+    int *tstart = nullptr;      // [n+1] first tile of each radius
     int lchunk = 0;
     int want_gc = 0, want_lc = 0, pf_from = 0;
     double accuracy = 0.;
     int save_control = 0;
     int *gstart = nullptr;
-    double *scr_r = nullptr, *scr_d = nullptr, *coef = nullptr, *rs = nullptr;
+    double4 *rec = nullptr;
+    double *rsp = nullptr, *coef = nullptr, *rs = nullptr;
     double *sums = nullptr, *part = nullptr, *pfacc = nullptr, *pfn = nullptr;
     double *state = nullptr, *tab = nullptr, *raw = nullptr;
     double *mu_user = nullptr;
@@ -161,18 +168,14 @@ int run_kernels(Plan &L) {
     c.launches = L.launches;
     stage(1);
     if (L.save_control != 2) {
-        if (P.n_qang > 0 && launch_gauss(s, P.n_qang, P.gl_guess, (double *) P.mu, (double *) P.wq)) return -1;
-        // K1: recurrences + coefficients, per index1 chunk and radius batch
+        // K1: recurrences + coefficients, per chunk of up to 4 index1 columns
         for (int ch = 0; ch < (L.nd1c > 0 ? L.nd1c : 1); ++ch) {
             int c0 = ch * 4;
             int nc = P.nd1 - c0 < 4 ? P.nd1 - c0 : 4;
             if (nc < 0) nc = 0;
-            for (int r0 = 0; r0 < P.n; r0 += L.nb) {
-                int nb = P.n - r0 < L.nb ? P.n - r0 : L.nb;
-                if (launch_coef(s, P, nc, c0, ch == 0, r0, nb, L.jmax, L.scr_r, L.scr_d, L.coef, L.rs))
-                    return -1;
-            }
+            if (launch_coef(s, P, nc, c0, ch == 0, L.tiles, L.rec, L.coef, L.rsp)) return -1;
         }
+        if (launch_tile_reduce(s, P, L.tstart, L.rsp, L.rs)) return -1;
         stage(2);
         if (launch_reduce_scalars(s, P, L.rs, L.sums, L.save_control == 1 ? L.o_save1 : nullptr)) return -1;
         stage(3);
@@ -190,7 +193,6 @@ int run_kernels(Plan &L) {
             if (launch_reduce_pf(s, P, L.G, L.part, L.pfacc)) return -1;
         }
     } else {
-        if (P.n_qang > 0 && launch_gauss(s, P.n_qang, P.gl_guess, (double *) P.mu, (double *) P.wq)) return -1;
         stage(2);
         if (launch_save_reweight(s, P, L.save1_in, L.save2_in, L.w2, L.sums, L.pfacc)) return -1;
         stage(3);
@@ -247,6 +249,18 @@ extern "C" int lmieb_device_solve(const lmieb_problem *p, lmieb_result *res) {
     }
     const long long tot = off[n];
     const int n1 = p->n1;
+    std::vector<long long> offp(n + 1);
+    std::vector<int> tstart(n + 1);
+    std::vector<int2> tiles;
+    offp[0] = 0;
+    for (int r = 0; r < n; ++r) {
+        offp[r + 1] = offp[r] + p->n1r[r] + 1;
+        tstart[r] = (int) tiles.size();
+        for (int j0 = 1; j0 <= p->n1r[r]; j0 += 127) tiles.push_back(make_int2(r, j0));
+    }
+    tstart[n] = (int) tiles.size();
+    const long long totp = offp[n];
+    const int ntiles = (int) tiles.size();
     std::vector<double> fv((size_t) 4 * (n1 + 2), 0.);
     for (int i = 1; i <= n1 + 1; ++i) {
         double f1 = 2. * i + 1., f2 = (i + 1.) / i;
@@ -260,7 +274,9 @@ extern "C" int lmieb_device_solve(const lmieb_problem *p, lmieb_result *res) {
     int G = 1;
     std::vector<int> gstart;
     if (n_qang > 0) {
-        int tiles = (nh + 63) / 64;
+        const int per = angular_angles_per_block(nd1 < 4 ? nd1 : 4);
+        int tiles = (nh + per - 1) / per;
+        // one full wave at the kernel's occupancy (4 blocks per SM)
         int target = 4 * c.sms;
         G = (target + tiles - 1) / tiles;
         if (G > n) G = n;
@@ -290,6 +306,25 @@ extern "C" int lmieb_device_solve(const lmieb_problem *p, lmieb_result *res) {
             guess[i] = cos(th + da / tan(th));
         }
     }
+    std::vector<double> gl_jr(n_qang > 0 ? n_qang : 1, 0.);
+    for (int j = 0; j < n_qang; ++j) gl_jr[j] = j / (j + 1.);
+    // GSF / Legendre recurrence coefficients per order l (j = l - 1)
+    std::vector<double> rc((size_t) 8 * (n_coef > 0 ? n_coef : 1), 0.);
+    for (int l = 3; l < n_coef; ++l) {
+        const int j = l - 1;
+        const double jj = (double) j * j, jp1 = j + 1., jjp1 = j * jp1, jp1s = jp1 * jp1, tj1 = 2 * j + 1;
+        const double a02 = sqrt(jj - 4), b02 = sqrt(jp1s - 4);
+        const double a22 = tj1 * 4, b22 = jp1 * (jj - 4), c22 = j * (jp1s - 4);
+        double *q = &rc[(size_t) 8 * l];
+        q[0] = tj1 / jp1;
+        q[1] = j / jp1;
+        q[2] = tj1 / b02;
+        q[3] = a02 / b02;
+        q[4] = tj1 * jjp1 / c22;
+        q[5] = a22 / c22;
+        q[6] = b22 / c22;
+    }
+    for (int l = 2; l < 3 && l < n_coef; ++l) rc[(size_t) 8 * l + 1] = 1. / 2.;   // Legendre at l = 2
     std::vector<cplx> ml(nd > 0 ? nd : 1);
     for (int k = 0; k < nd; ++k) ml[k] = mk(p->mr_l[k], -p->mi_l[k]);
 
@@ -297,14 +332,7 @@ extern "C" int lmieb_device_solve(const lmieb_problem *p, lmieb_result *res) {
     L.n_ang_launch = (nd1 > nd2 ? (nd1 + 3) / 4 : (nd2 + 3) / 4);
     if (L.n_ang_launch < 1) L.n_ang_launch = 1;
     L.G = G;
-    L.jmax = n1max + 1;
-    {
-        int widest = nd1 < 4 ? nd1 : 4;
-        size_t per = (size_t) (1 + widest) * L.jmax * 24;
-        size_t nb = SCRATCH_LIMIT / (per ? per : 1);
-        if (nb < 1) nb = 1;
-        L.nb = (int) (nb < (size_t) n ? nb : (size_t) n);
-    }
+    (void) n1max;
     if (nh > 0) {
         size_t lc = TABLE_LIMIT / ((size_t) 4 * nh * 8);
         if (lc < 32) lc = 32;
@@ -319,11 +347,9 @@ extern "C" int lmieb_device_solve(const lmieb_problem *p, lmieb_result *res) {
     // ---- launches per run and algorithmic work (flops) of this solve ----
     {
         long long nl = 0;
-        const int nbatch = (n + L.nb - 1) / L.nb;
         const long long lchunks = nh > 0 ? (n_coef + L.lchunk - 1) / L.lchunk : 0;
-        if (n_qang > 0) nl += 1;                                      // Gauss angles
         if (p->save_control != 2) {
-            nl += (long long) (L.nd1c > 0 ? L.nd1c : 1) * nbatch;     // K1
+            nl += (long long) (L.nd1c > 0 ? L.nd1c : 1) * 2 + 1;      // K1a + K1b per chunk, tile sums
             nl += 1;                                                  // K2
             if (n_qang > 0) nl += L.n_ang_launch + 1;                 // K3 + group reduction
         } else {
@@ -360,10 +386,13 @@ extern "C" int lmieb_device_solve(const lmieb_problem *p, lmieb_result *res) {
     {
         auto add = [&](size_t b) { in_bytes += pad(b); };
         add(n * 8); add((size_t) nd1 * n * 8); add((size_t) ncol * n * 8); add(n * 4); add(n * 4);
-        add((size_t) (n + 1) * 8); add(fv.size() * 8); add(ml.size() * 16); add((nd > 0 ? nd : 1) * 8);
+        add((size_t) (n + 1) * 8); add((size_t) (n + 1) * 8); add((size_t) (n + 1) * 4);
+        add(tiles.size() * 8); add(fv.size() * 8); add(ml.size() * 16); add((nd > 0 ? nd : 1) * 8);
         add((nd1 > 0 ? nd1 : 1) * 4); add((nd2 > 0 ? nd2 : 1) * 4); add((na > 0 ? na : 1) * 8);
         add(gstart.size() * 4);
         add(guess.size() * 8);
+        add(gl_jr.size() * 8);
+        add(rc.size() * 8);
         if (p->save_control == 2) { add((size_t) 4 * n * 8); add(n_save2 * 8); add((size_t) (nd > 0 ? nd : 1) * n * 8); }
     }
     size_t out_bytes = 0;
@@ -385,6 +414,9 @@ extern "C" int lmieb_device_solve(const lmieb_problem *p, lmieb_result *res) {
     int *h_n1r = put(hp, ho, p->n1r, n);
     int *h_n2r = put(hp, ho, p->n2r, n);
     long long *h_off = put(hp, ho, off.data(), n + 1);
+    long long *h_offp = put(hp, ho, offp.data(), n + 1);
+    int *h_tstart = put(hp, ho, tstart.data(), n + 1);
+    int2 *h_tiles = put(hp, ho, tiles.data(), tiles.size());
     double *h_fv = put(hp, ho, fv.data(), fv.size());
     cplx *h_ml = put(hp, ho, ml.data(), ml.size());
     double *h_laml = put(hp, ho, p->lambda_l, nd);
@@ -393,6 +425,8 @@ extern "C" int lmieb_device_solve(const lmieb_problem *p, lmieb_result *res) {
     double *h_mu = put(hp, ho, p->mu_user, na);
     int *h_gs = put(hp, ho, gstart.data(), gstart.size());
     double *h_guess = put(hp, ho, guess.data(), guess.size());
+    double *h_jr = put(hp, ho, gl_jr.data(), gl_jr.size());
+    double *h_rc = put(hp, ho, rc.data(), rc.size());
     double *h_s1 = nullptr, *h_s2 = nullptr, *h_w2 = nullptr;
     if (p->save_control == 2) {
         h_s1 = put(hp, ho, p->save1_in, (size_t) 4 * n);
@@ -407,11 +441,9 @@ extern "C" int lmieb_device_solve(const lmieb_problem *p, lmieb_result *res) {
     size_t dev_bytes = in_bytes + out_bytes + 64 * 256;
     {
         auto add = [&](size_t b) { dev_bytes += pad(b); };
-        add((size_t) (n_qang > 0 ? n_qang : 1) * 8 * 2);
         if (p->save_control != 2) {
-            int widest = nd1 < 4 ? nd1 : 4;
-            add((size_t) (1 + widest) * L.jmax * L.nb * 8);
-            add((size_t) (1 + widest) * L.jmax * L.nb * 16);
+            add((size_t) (1 + nd1) * (size_t) totp * 32);
+            add((size_t) (1 + nd1) * 5 * (size_t) ntiles * 8);
             add((size_t) (1 + nd1) * (size_t) tot * 32);
             add((size_t) (1 + nd1) * 5 * n * 8);
             add((size_t) G * Q * (n_qang > 0 ? n_qang : 1) * 8);
@@ -455,23 +487,44 @@ extern "C" int lmieb_device_solve(const lmieb_problem *p, lmieb_result *res) {
     P.n2r = (const int *) dptr(h_n2r);
     P.off = (const long long *) dptr(h_off);
     P.tot = tot;
+    P.offp = (const long long *) dptr(h_offp);
+    P.totp = totp;
+    P.ntiles = ntiles;
+    L.tiles = (int2 *) dptr(h_tiles);
+    L.tstart = (int *) dptr(h_tstart);
     P.fv = (const double *) dptr(h_fv);
     L.gstart = (int *) dptr(h_gs);
     P.gl_guess = (const double *) dptr(h_guess);
+    P.gl_jr = (const double *) dptr(h_jr);
+    P.rc = (const double *) dptr(h_rc);
     L.mu_user = (double *) dptr(h_mu);
     if (p->save_control == 2) {
         L.save1_in = (double *) dptr(h_s1);
         L.save2_in = (double *) dptr(h_s2);
         L.w2 = (double *) dptr(h_w2);
     }
-    double *mu = A.take<double>(n_qang > 0 ? n_qang : 1);
-    double *wq = A.take<double>(n_qang > 0 ? n_qang : 1);
-    P.mu = mu;
-    P.wq = wq;
+    bool gl_new = false;
+    P.mu = P.wq = nullptr;
+    if (n_qang > 0) {
+        for (auto &e : c.gl_cache)
+            if (e.n == n_qang) { P.mu = e.mu; P.wq = e.wq; }
+        if (!P.mu) {
+            if (c.gl_cache.size() >= GL_CACHE) {
+                LMIEB_CUDA_TRY(cudaFree(c.gl_cache.front().mu));
+                c.gl_cache.erase(c.gl_cache.begin());
+            }
+            Ctx::GlEntry e{n_qang, nullptr, nullptr};
+            LMIEB_CUDA_TRY(cudaMalloc((void **) &e.mu, sizeof(double) * 2 * (size_t) n_qang));
+            e.wq = e.mu + n_qang;
+            c.gl_cache.push_back(e);
+            P.mu = e.mu;
+            P.wq = e.wq;
+            gl_new = true;
+        }
+    }
     if (p->save_control != 2) {
-        int widest = nd1 < 4 ? nd1 : 4;
-        L.scr_r = A.take<double>((size_t) (1 + widest) * L.jmax * L.nb);
-        L.scr_d = A.take<double>((size_t) (1 + widest) * L.jmax * L.nb * 2);
+        L.rec = A.take<double4>((size_t) (1 + nd1) * (size_t) totp);
+        L.rsp = A.take<double>((size_t) (1 + nd1) * 5 * (size_t) ntiles);
         L.coef = A.take<double>((size_t) (1 + nd1) * (size_t) tot * 4);
         L.rs = A.take<double>((size_t) (1 + nd1) * 5 * n);
         L.part = A.take<double>((size_t) G * Q * (n_qang > 0 ? n_qang : 1));
@@ -513,6 +566,7 @@ extern "C" int lmieb_device_solve(const lmieb_problem *p, lmieb_result *res) {
     stage(0);
     LMIEB_CUDA_TRY(cudaMemcpyAsync(d_in, hp, h_in_end, cudaMemcpyHostToDevice, s));
     LMIEB_CUDA_TRY(cudaMemsetAsync(d_out, 0, out_bytes, s));
+    if (gl_new && launch_gauss(s, n_qang, P.gl_guess, P.gl_jr, (double *) P.mu, (double *) P.wq)) return -1;
     if (run_kernels(L)) return -1;
     LMIEB_CUDA_TRY(cudaMemcpyAsync(h_out, d_out, out_bytes, cudaMemcpyDeviceToHost, s));
     stage(9 < NSTAGE ? 9 : NSTAGE);
