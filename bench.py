@@ -2,23 +2,30 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
-Workload (one step = one polydisperse solve with its Jacobian): the
-forward-linearized FP64 cloud droplet -- gamma distribution r_eff = 10 um,
-v_eff = 0.1, r in [0.01, 60] um, 4 intervals x 500 Gauss radii, lambda =
-0.865 um, m = 1.335 + 1e-6 i, x_max ~ 436, 4 derivatives (mr, mi, r_eff,
-v_eff), GSF expansion and 181-angle phase matrix.  Inputs are synthetic (the
-reference's published case parameters), nothing is read from disk.
+Workload (one step = one batch): 4096 independent polydisperse cases of
+uneven size, generated from a fixed seed (lmie_b200.workloads.batched_uneven:
+r_eff log-uniform 0.05-20 um, v_eff 0.02-0.3, wavelength 0.34-2.1 um,
+m = 1.33-1.60 + i 1e-8..0.1, gamma or log-normal distributions, 100-2000
+radii scaled to the size parameter, size parameters 0.2-1063, n_max 9-1112),
+each with its Jacobian w.r.t. mr, mi and the two distribution parameters, GSF
+expansion and 181-angle phase matrix.  Inputs are synthetic; nothing is read
+from disk.
 
-  value  device time of the solve on inputs resident in HBM (L2 flushed
-         between steps), whole job over all ranks;
-  e2e    the same solve through the public C call lmie_solution() with host
-         buffers: host preparation, host->device and device->host copies inside
-         the timed region.
+  value  device time of the batch on inputs resident in HBM (the L2 is
+         flushed before every step), solves/s over all ranks;
+  e2e    the same batch through the public C call lmie_solution_batch() on
+         host buffers: host preparation, the host->device and device->host
+         copies and the scatter into the caller's lmie_out_data are inside the
+         timed region.
 
-With N > 1 (torchrun, one process per GPU) every rank solves its own case per
-step (independent cases, no data-path collective): weak scaling.
+A second measurement, `single_case`, is the reference's cloud-droplet case
+(2000 radii, x_max ~436, 4 derivatives) through lmie_solution().
+
+With N > 1 (torchrun, one process per GPU) every rank solves its own batch
+(independent cases, no data-path collective): weak scaling.
 `--impl reference` times the reference's own CPU lmie_solution (compiled from
-its sources into oracle/_ref) on all host cores, on rank 0 only.
+its sources into oracle/_ref) on all host cores over a bounded sample of the
+same cases, on rank 0 only.
 """
 from __future__ import annotations
 
@@ -36,16 +43,17 @@ from pathlib import Path
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-from lmie_b200 import abi  # noqa: E402
+from lmie_b200 import abi, workloads  # noqa: E402
 
 METRIC = "polydisperse solves/s (+Jacobian)"
 UNIT = "solves/s"
-WORKLOAD = ("cloud droplet, forward-linearized FP64: gamma r_eff=10um v_eff=0.1, "
-            "r in [0.01,60]um, 4x500 Gauss radii, lambda=0.865um, m=1.335+1e-6i, x_max~436, "
-            "4 derivatives (mr, mi, r_eff, v_eff), GSF + 181-angle phase matrix")
+N_CASES = 4096
+WORKLOAD = ("batched uneven: 4096 seeded cases (r_eff 0.05-20 um, v_eff 0.02-0.3, lambda 0.34-2.1 um, "
+            "mr 1.33-1.60, mi 1e-8-0.1, gamma/log-normal, 100-2000 radii, x_max 0.2-1063), "
+            "4 derivatives each (mr, mi, a1, a2), GSF + 181-angle phase matrix, FP64")
 
 
-def workload_case() -> abi.Case:
+def single_case() -> abi.Case:
     return abi.Case(dist="gamma", lam=0.865, mr=1.335, mi=1e-6, a1=10.0, a2=0.1, r1=0.01,
                     r2=60.0, n_int2=4, n_quad=500, n_angles=181, accuracy=1e-7,
                     derivs=abi.deriv_unit("mr", "mi", "a1", "a2"))
@@ -110,8 +118,39 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-# CPU baseline: the reference library (oracle/_ref) or the CPU oracle port
+# C-level batch: in/out structs built once, outputs preallocated
 # ---------------------------------------------------------------------------
+class CBatch:
+    """lmie_in_data / lmie_out_data arrays for a list of cases, with outputs
+    allocated once by the library (the caller-owned arrays of alloc_out = 0)."""
+
+    def __init__(self, lib, cases):
+        self.lib = lib
+        self.cases = cases
+        self.blocks = [abi.InputBlock(c) for c in cases]
+        n = len(cases)
+        self.ins = (abi.lmie_in_data * n)(*[b.s for b in self.blocks])
+        self.outs = (abi.lmie_out_data * n)()
+        lib.lmie_out_alloc.argtypes = [C.POINTER(abi.lmie_in_data), C.POINTER(abi.lmie_out_data), C.c_int]
+        for i, c in enumerate(cases):
+            mc = lib.lmie_calc_max_coef(c.lam, self.ins[i].dist_type, c.a1, c.a2, c.a3, c.r1, c.r2)
+            lib.lmie_out_alloc(C.byref(self.ins[i]), C.byref(self.outs[i]), mc)
+
+    def solve_batch(self, n_threads: int) -> int:
+        f = self.lib.lmie_solution_batch
+        f.restype = C.c_int
+        f.argtypes = [C.c_int, C.POINTER(abi.lmie_in_data), C.POINTER(abi.lmie_out_data), C.c_int,
+                      C.c_int, C.c_int]
+        return f(len(self.cases), self.ins, self.outs, 0, 0, n_threads)
+
+    def solve_each(self, n_threads: int) -> int:
+        for i in range(len(self.cases)):
+            rc = self.lib.lmie_solution(C.byref(self.ins[i]), C.byref(self.outs[i]), 0, 0, n_threads, 0)
+            if rc != 0:
+                return rc
+        return 0
+
+
 def _cpu_library():
     ref = ROOT / "oracle" / "_ref" / "liblmie_ref.so"
     if ref.exists():
@@ -126,70 +165,50 @@ def _cpu_library():
     return lib, "port"
 
 
-def cpu_solve_seconds(lib, kind: str, case: abi.Case, threads: int) -> float:
-    t0 = time.perf_counter()
-    if kind == "reference":
-        r = abi.solve(lib, case, n_threads=threads)
-    else:
-        r = abi.solve(lib, case, kind="oracle")
-    dt = time.perf_counter() - t0
-    if r.rc != 0:
-        raise RuntimeError("CPU baseline solve failed")
-    return dt
-
-
-def cpu_baseline(case: abi.Case, budget_s: float = 20.0) -> dict:
+def cpu_sample_rate(cases, budget_s: float) -> dict:
+    """Solves/s of the CPU implementation over a bounded sample of `cases`
+    (taken in a seeded order from the whole batch, so sizes are represented)."""
     lib, kind = _cpu_library()
     threads = os.cpu_count() if kind == "reference" else 1
-    cpu_solve_seconds(lib, kind, case, threads)          # warm caches
-    times = []
+    import random
+    order = list(range(len(cases)))
+    random.Random(workloads.SEED).shuffle(order)
     t_start = time.perf_counter()
-    while len(times) < 20 and (time.perf_counter() - t_start) < budget_s:
-        times.append(cpu_solve_seconds(lib, kind, case, threads))
-    per = statistics.median(times)
-    return {"value": 1.0 / per, "unit": UNIT, "cores": threads, "kind": kind,
-            "sample": f"{len(times)} full solves of the benchmark case "
-                      f"(median {per * 1e3:.1f} ms each, lmie_solution with n_threads={threads})"}
+    done, busy = 0, 0.0
+    for i in order:
+        c = cases[i]
+        t0 = time.perf_counter()
+        r = abi.solve(lib, c, n_threads=threads) if kind == "reference" else abi.solve(lib, c, kind="oracle")
+        busy += time.perf_counter() - t0
+        if r.rc != 0:
+            raise RuntimeError("CPU solve failed")
+        done += 1
+        if time.perf_counter() - t_start > budget_s:
+            break
+    return {"value": done / busy, "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": f"{done} of the {len(cases)} batch cases in seeded random order "
+                      f"({busy:.1f} s), lmie_solution with n_threads={threads}, one case after another"}
 
 
 def run_reference_arm(args) -> int:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    case = workload_case()
-    lib, kind = _cpu_library()
-    threads = os.cpu_count() if kind == "reference" else 1
-    for _ in range(args.warmup):
-        cpu_solve_seconds(lib, kind, case, threads)
-    total = 0.0
-    for _ in range(args.steps):
-        total += cpu_solve_seconds(lib, kind, case, threads)
-    value = args.steps / total
+    cases = workloads.batched_uneven(N_CASES)
+    budget = max(10.0, 3.0 * args.steps)
+    cpu = cpu_sample_rate(cases, budget)
+    value = cpu["value"]
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": N_CASES / value * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (reference case parameters)",
-        "config": {"workload": WORKLOAD, "n_radii": 2000, "n_derivs": 4},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
-                         "sample": f"{args.steps} full solves, lmie_solution(n_threads={threads})"},
+        "data": "synthetic (seeded generator)",
+        "config": {"workload": WORKLOAD, "n_cases": N_CASES, "n_derivs": 4},
+        "cpu_baseline": cpu,
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
-
-
-# ---------------------------------------------------------------------------
-# the B200 arm
-# ---------------------------------------------------------------------------
-def measured_peaks() -> dict:
-    p = ROOT / "MEASURED_PEAKS.json"
-    if p.exists():
-        try:
-            return json.loads(p.read_text())
-        except ValueError:
-            pass
-    return {}
 
 
 def run_b200(args) -> int:
@@ -202,7 +221,7 @@ def run_b200(args) -> int:
 
     torch.cuda.set_device(local)
     if world > 1:
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
 
     def barrier():
@@ -222,13 +241,14 @@ def run_b200(args) -> int:
     lib = lmie_b200.library()
     if lib.lmieb_set_device(local) != 0:
         raise RuntimeError("lmieb_set_device failed")
-    case = workload_case()
+    threads = max(1, (os.cpu_count() or 1) // max(1, world))
+    # every rank solves its own seeded batch (independent cases)
+    cases = workloads.batched_uneven(N_CASES, seed=workloads.SEED + rank)
+    batch = CBatch(lib, cases)
 
-    # warm-up through the public call (allocates and plans)
-    for _ in range(max(args.warmup, 1)):
-        r = abi.solve(lib, case)
-        if r.rc != 0:
-            raise RuntimeError("lmie_solution failed")
+    for _ in range(args.warmup):
+        if batch.solve_batch(threads) != 0:
+            raise RuntimeError("lmie_solution_batch failed")
     flops = (C.c_double * 4)()
     launches = C.c_longlong()
     h2d, d2h = C.c_size_t(), C.c_size_t()
@@ -237,20 +257,20 @@ def run_b200(args) -> int:
     clocks = ClockSampler(local)
     clocks.start()
 
-    # e2e: K public calls with host buffers
+    # e2e: K public batch calls on host buffers
     barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        r = abi.solve(lib, case)
-        if r.rc != 0:
-            raise RuntimeError("lmie_solution failed")
+        if batch.solve_batch(threads) != 0:
+            raise RuntimeError("lmie_solution_batch failed")
     barrier()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
 
-    # device: K re-runs on resident inputs, L2 flushed before each (untimed)
+    # device: K re-runs of the resident batch, L2 flushed before each (untimed)
     ms_total = C.c_double()
     ms_stage = (C.c_double * lmie_b200.N_STAGES)()
-    lib.lmieb_rerun_device(args.warmup, 1, C.byref(ms_total), ms_stage)   # warm
+    if lib.lmieb_rerun_device(1, 1, C.byref(ms_total), ms_stage) != 0:
+        raise RuntimeError("device re-run failed (batch did not fit one sub-batch)")
     barrier()
     if lib.lmieb_rerun_device(args.steps, 1, C.byref(ms_total), ms_stage) != 0:
         raise RuntimeError("device re-run failed")
@@ -258,25 +278,43 @@ def run_b200(args) -> int:
     dev_ms = max_over_ranks(ms_total.value)
     clk = clocks.stop()
 
-    value = world * args.steps / (dev_ms * 1e-3)
-    e2e = world * args.steps / e2e_s
+    value = world * N_CASES * args.steps / (dev_ms * 1e-3)
+    e2e = world * N_CASES * args.steps / e2e_s
+    batch_stage_ms = {n: ms_stage[i] / args.steps for i, n in enumerate(lmie_b200.STAGES)}
     ang_ms = ms_stage[3] / args.steps
     peak = C.c_double()
     lib.lmieb_fp64_peak(C.byref(peak))
     achieved = flops[0] / (ang_ms * 1e-3) / 1e12 if ang_ms > 0 else None
 
+    # secondary: the single cloud-droplet case through lmie_solution()
+    single = None
     if rank == 0:
-        cpu = cpu_baseline(case) if world == 1 else None
+        one = CBatch(lib, [single_case()])
+        for _ in range(3):
+            one.solve_each(1)
+        t1 = time.perf_counter()
+        for _ in range(10):
+            one.solve_each(1)
+        single_e2e = 10 / (time.perf_counter() - t1)
+        lib.lmieb_rerun_device(2, 1, C.byref(ms_total), ms_stage)
+        lib.lmieb_rerun_device(10, 1, C.byref(ms_total), ms_stage)
+        single = {"workload": "cloud droplet: gamma r_eff=10um v_eff=0.1, 4x500 radii, x_max~436, 4 derivatives",
+                  "value": 10 / (ms_total.value * 1e-3), "e2e": single_e2e, "unit": UNIT,
+                  "stage_ms": {n: ms_stage[i] / 10 for i, n in enumerate(lmie_b200.STAGES)}}
+
+    if rank == 0:
+        cpu = cpu_sample_rate(cases, 20.0) if world == 1 else None
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (reference case parameters, generated in-process)",
-            "config": {"workload": WORKLOAD, "n_radii": 2000, "n_derivs": 4,
-                       "n_gauss_angles": 948, "parallelism": f"independent cases x{world}",
-                       "l2": "flushed (256 MiB write) before every timed step"},
+            "data": "synthetic (seeded generator, rank r uses seed + r)",
+            "config": {"workload": WORKLOAD, "n_cases": N_CASES, "n_derivs": 4,
+                       "parallelism": f"independent batches x{world}",
+                       "l2": "flushed (256 MiB write) before every timed device step; "
+                             "the batch's working set (~8 GB) exceeds L2 in any case"},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d.value),
-                    "d2h_bytes_per_step": int(d2h.value)},
+                    "d2h_bytes_per_step": int(d2h.value), "host_threads": threads},
             "gpu_launches": int(launches.value) * args.steps,
             "roofline": {
                 "kernel": "k_angular (S1/S2 accumulation + phase-matrix forms, FP64)",
@@ -285,7 +323,8 @@ def run_b200(args) -> int:
                 "peak_source": "live FP64 FMA microbenchmark (lmieb_fp64_peak); "
                                "MEASURED_PEAKS.json holds HBM and BF16 only",
                 "flops_per_launch": flops[0], "ms_per_launch": ang_ms},
-            "stage_ms": {n: ms_stage[i] / args.steps for i, n in enumerate(lmie_b200.STAGES)},
+            "stage_ms": batch_stage_ms,
+            "single_case": single,
             "clocks": clk,
         }
         if cpu is not None:
@@ -300,12 +339,10 @@ def run_b200(args) -> int:
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
     args = ap.parse_args(argv)
-    if args.warmup < 3:
-        args.warmup = 3
     if args.impl == "reference":
         return run_reference_arm(args)
     return run_b200(args)

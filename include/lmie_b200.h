@@ -15,6 +15,18 @@
 extern "C" {
 #endif
 
+/* Solves n_cases independent polydisperse problems, in[i] -> out[i], with
+ * the same meaning, outputs and errors as calling
+ * lmie_solution(&in[i], &out[i], alloc_out, verbose, n_threads, 0) for each
+ * i.  The host preparation of the cases runs on n_threads threads; cases
+ * that share their derivative layout and requested outputs are solved
+ * together in batched device launches (size-parameter-balanced work lists),
+ * so thousands of small and large cases keep the whole GPU busy.  This entry
+ * point has no counterpart in the reference, whose callers loop over
+ * lmie_solution.  Returns 0, or -1 if any case fails. */
+int lmie_solution_batch(int n_cases, lmie_in_data *in, lmie_out_data *out, int alloc_out,
+                        int verbose, int n_threads);
+
 /* Stages of one solve, timed with CUDA events when timing is on:
  * 0 upload, 1 Mie recurrences and coefficients (K1), 2 radius reduction of
  * the cross sections (K2), 3 angular accumulation (K3), 4 normalisation,

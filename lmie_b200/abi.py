@@ -273,3 +273,24 @@ def bind_product_like(lib: C.CDLL) -> None:
 def deriv_unit(*names: str) -> List[Dict[str, float]]:
     """One derivative per name, each with unit perturbation of that input."""
     return [{n: 1.0} for n in names]
+
+
+def solve_batch(lib: C.CDLL, cases: Sequence[Case], n_threads: int = 8) -> List[Result]:
+    """Solve many cases with one lmie_solution_batch() call."""
+    n = len(cases)
+    blocks = [InputBlock(c) for c in cases]
+    ins = (lmie_in_data * n)(*[b.s for b in blocks])
+    outs = (lmie_out_data * n)()
+    f = lib.lmie_solution_batch
+    f.restype = C.c_int
+    f.argtypes = [C.c_int, C.POINTER(lmie_in_data), C.POINTER(lmie_out_data), C.c_int, C.c_int, C.c_int]
+    rc = f(n, ins, outs, 1, 0, n_threads)
+    if rc != 0:
+        return [Result(rc=rc) for _ in cases]
+    res = []
+    for i, c in enumerate(cases):
+        mc = lib.lmie_calc_max_coef(c.lam, ins[i].dist_type, c.a1, c.a2, c.a3, c.r1, c.r2)
+        nqang = mc if (c.save_control == 1 and (c.calc_gc or c.calc_lc)) else 0
+        res.append(read_output(c, outs[i], mc, n_qsize(c), nqang))
+        lib.lmie_out_free(C.byref(outs[i]), 1 if c.n_derivs > 0 else 0)
+    return res

@@ -1,9 +1,12 @@
-// driver.cu -- device side of one drop-in solve: owns the CUDA context state
-// (stream, device arena, pinned staging), uploads a prepared problem, runs
-// the kernel sequence and returns the results.  Replaces the reference's
+// driver.cu -- device side of the polydisperse solve: owns the CUDA context
+// state (stream, device arena, pinned staging, Gauss-angle pool), lays out a
+// batch of prepared cases, uploads it in one copy, runs the kernel sequence
+// and returns the results in one copy.  Replaces the reference's
 // lmie_core_shared / lmie_core_sequential / lmie_core_xthreads fan-out
 // (src/lmie_schedule.c:154-452) and the driver half of lmie_core_solution
-// (src/lmie_schedule.c:942-1268).
+// (src/lmie_schedule.c:942-1268); a batch of cases is the unit of work, and a
+// single lmie_solution() is a batch of one.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -18,12 +21,14 @@
 namespace {
 
 constexpr int NSTAGE = LMIEB_N_STAGES;
-constexpr size_t TABLE_LIMIT = (size_t) 256 << 20;     // expansion basis table per order chunk
 constexpr size_t FLUSH_BYTES = (size_t) 256 << 20;     // > 126 MB L2
+constexpr size_t BATCH_BYTES = (size_t) 24 << 30;      // device working set of one sub-batch
 
 // Every staged array starts on a 256-byte boundary and takes at least one
 // 256-byte block, so empty arrays never alias their neighbours.
 inline size_t pad(size_t bytes) { return ((bytes ? bytes : 1) + 255) & ~(size_t) 255; }
+
+struct Plan;
 
 struct Ctx {
     bool ready = false;
@@ -38,22 +43,21 @@ struct Ctx {
     cudaEvent_t ev[NSTAGE + 1] = {};
     bool timing = false;
     double stage_ms[NSTAGE] = {};
-    long long launches = 0;         // kernel launches of the last run_kernels
     double work[4] = {};            // algorithmic flops of the last solve (see lmieb_last_work)
+    long long launches = 0;         // kernel launches of one device run of the last solve
     size_t h2d = 0, d2h = 0;        // bytes copied by the last solve
-    // state of the last solve, for re-running the device part in place
     bool have_plan = false;
-    struct Plan *plan = nullptr;
+    Plan *plan = nullptr;
     // Gauss-Legendre angles depend only on their number: computed once per n
-    // and kept on the device (oldest entry evicted beyond GL_CACHE entries)
-    struct GlEntry { int n; double *mu; double *wq; };
-    std::vector<GlEntry> gl_cache;
+    // into a device pool ([n nodes][n weights] per entry) and kept
+    double *gl_pool = nullptr;
+    size_t gl_cap = 0, gl_used = 0;
+    std::vector<std::pair<int, long long>> gl_map;
 };
-
-constexpr size_t GL_CACHE = 32;
 
 Ctx g_ctx;
 std::mutex g_mu;
+int g_want_device = -1;
 
 struct Arena {
     char *base;
@@ -68,35 +72,29 @@ struct Arena {
     }
 };
 
-// Everything the kernel sequence needs, in device memory.
+// Everything the kernel sequence of one sub-batch needs, in device memory.
 struct Plan {
-    DevProblem P;
-    int nd1c = 0;               // number of index1 chunks for K1
-    int n_ang_launch = 0;       // launches of K3
-    int G = 0;                  // radius groups of K3
-    int2 *tiles = nullptr;      // K1b (radius, first order) per block
-    int *tstart = nullptr;      // [n+1] first tile of each radius
-    int lchunk = 0;
-    int want_gc = 0, want_lc = 0, pf_from = 0;
-    double accuracy = 0.;
-    int save_control = 0;
-    int *gstart = nullptr;
+    DevBatch B;
+    int ncase = 0;
+    int nd1c = 0, n_ang_launch = 0;
+    int want_gc = 0, want_lc = 0, pf_from = 0, save_control = 0, n_qang0 = 0;
+    int2 *tiles = nullptr;
+    int *tstart = nullptr;
     double4 *rec = nullptr;
-    double *rsp = nullptr, *coef = nullptr, *rs = nullptr;
-    double *sums = nullptr, *part = nullptr, *pfacc = nullptr, *pfn = nullptr;
-    double *state = nullptr, *tab = nullptr, *raw = nullptr;
-    double *mu_user = nullptr;
+    double *rsp = nullptr, *coef = nullptr, *rs = nullptr, *sums = nullptr, *part = nullptr;
+    double *pfacc = nullptr, *pfn = nullptr, *ckpt = nullptr, *exq = nullptr;
+    AngItem *ang = nullptr;
+    int n_ang = 0;
+    ExpItem *ex = nullptr;
+    int n_ex = 0;
+    long long *pf_start = nullptr, *ck_gc = nullptr, *ck_lc = nullptr, *fin_start = nullptr, *pu_start = nullptr;
+    long long pf_total = 0, nck_gc = 0, nck_lc = 0, nfin = 0, pu_total = 0;
     double *save1_in = nullptr, *save2_in = nullptr, *w2 = nullptr;
-    // output region (one D2H copy)
     double *o_scal = nullptr, *o_gc = nullptr, *o_lc = nullptr, *o_pf = nullptr;
-    int *o_trunc = nullptr;     // [2]: gc, lc
+    int *o_trunc = nullptr;     // [2][ncase]: gc, lc
     double *o_save1 = nullptr, *o_save2 = nullptr;
-    char *out_begin = nullptr;
-    size_t out_bytes = 0;
-    long long launches = 0;     // kernel launches one run_kernels issues
+    long long launches = 0;
 };
-
-int g_want_device = -1;
 
 int ensure_ready() {
     Ctx &c = g_ctx;
@@ -156,161 +154,188 @@ int ensure_host(size_t bytes) {
     return 0;
 }
 
+// grow the Gauss pool, keeping its contents
+int ensure_gl_pool(size_t doubles) {
+    Ctx &c = g_ctx;
+    if (doubles <= c.gl_cap) return 0;
+    size_t want = std::max(doubles + doubles / 2, (size_t) 1 << 16);
+    double *np = nullptr;
+    LMIEB_CUDA_TRY(cudaMalloc((void **) &np, want * sizeof(double)));
+    if (c.gl_pool) {
+        LMIEB_CUDA_TRY(cudaMemcpyAsync(np, c.gl_pool, c.gl_used * sizeof(double), cudaMemcpyDeviceToDevice,
+                                       c.stream));
+        LMIEB_CUDA_TRY(cudaStreamSynchronize(c.stream));
+        LMIEB_CUDA_TRY(cudaFree(c.gl_pool));
+    }
+    c.gl_pool = np;
+    c.gl_cap = want;
+    c.have_plan = false;
+    return 0;
+}
+
 inline void stage(int i) {
     if (g_ctx.timing) cudaEventRecord(g_ctx.ev[i], g_ctx.stream);
 }
 
-// The kernel sequence of one solve on resident inputs (stages 1..8).
+// The kernel sequence of one sub-batch on resident inputs (stages 1..7).
 int run_kernels(Plan &L) {
     Ctx &c = g_ctx;
     cudaStream_t s = c.stream;
-    const DevProblem &P = L.P;
-    c.launches = L.launches;
+    const DevBatch &B = L.B;
     stage(1);
     if (L.save_control != 2) {
-        // K1: recurrences + coefficients, per chunk of up to 4 index1 columns
         for (int ch = 0; ch < (L.nd1c > 0 ? L.nd1c : 1); ++ch) {
-            int c0 = ch * 4;
-            int nc = P.nd1 - c0 < 4 ? P.nd1 - c0 : 4;
-            if (nc < 0) nc = 0;
-            if (launch_coef(s, P, nc, c0, ch == 0, L.tiles, L.rec, L.coef, L.rsp)) return -1;
+            const int c0 = ch * 4;
+            const int nc = std::max(0, std::min(4, B.nd1 - c0));
+            if (launch_coef(s, B, nc, c0, ch == 0, L.tiles, L.rec, L.coef, L.rsp)) return -1;
         }
-        if (launch_tile_reduce(s, P, L.tstart, L.rsp, L.rs)) return -1;
+        if (launch_tile_reduce(s, B, L.tstart, L.rsp, L.rs)) return -1;
         stage(2);
-        if (launch_reduce_scalars(s, P, L.rs, L.sums, L.save_control == 1 ? L.o_save1 : nullptr)) return -1;
+        if (launch_reduce_scalars(s, B, L.rs, L.sums, L.save_control == 1 ? L.o_save1 : nullptr)) return -1;
         stage(3);
-        if (P.n_qang > 0) {
+        if (L.n_ang > 0) {
             for (int t = 0; t < L.n_ang_launch; ++t) {
-                int c1 = t * 4, c2 = t * 4;
-                int nc1 = P.nd1 - c1 < 4 ? P.nd1 - c1 : 4;
-                int nc2 = P.nd2 - c2 < 4 ? P.nd2 - c2 : 4;
-                if (nc1 < 0) nc1 = 0;
-                if (nc2 < 0) nc2 = 0;
-                if (launch_angular(s, P, nc1, c1, nc2, c2, t == 0, L.G, L.gstart, L.coef, L.part,
+                const int c1 = t * 4, c2 = t * 4;
+                const int nc1 = std::max(0, std::min(4, B.nd1 - c1));
+                const int nc2 = std::max(0, std::min(4, B.nd2 - c2));
+                if (launch_angular(s, B, nc1, c1, nc2, c2, t == 0, L.n_ang, L.ang, L.coef, L.part,
                                    L.save_control == 1 ? L.o_save2 : nullptr))
                     return -1;
             }
-            if (launch_reduce_pf(s, P, L.G, L.part, L.pfacc)) return -1;
+            if (launch_reduce_pf(s, B, L.pf_total, L.pf_start, L.part, L.pfacc)) return -1;
         }
     } else {
         stage(2);
-        if (launch_save_reweight(s, P, L.save1_in, L.save2_in, L.w2, L.sums, L.pfacc)) return -1;
+        if (launch_save_reweight(s, B, L.n_qang0, L.save1_in, L.save2_in, L.w2, L.sums, L.pfacc)) return -1;
         stage(3);
     }
     stage(4);
-    if (launch_normalize(s, P, L.sums, L.pfacc, L.o_scal, L.pfn)) return -1;
+    if (launch_normalize(s, B, L.pf_total, L.pf_start, L.sums, L.pfacc, L.o_scal, L.pfn)) return -1;
+    LMIEB_CUDA_TRY(cudaMemsetAsync(L.o_trunc, 0, sizeof(int) * 2 * L.ncase, s));
     stage(5);
-    if (L.want_gc && launch_expand(s, P, 0, L.lchunk, L.accuracy, L.pfn, L.state, L.tab, L.raw, L.o_gc,
-                                   L.o_trunc))
+    if (L.want_gc && launch_expand(s, B, 0, L.nck_gc, L.ck_gc, L.n_ex, L.ex, L.nfin, L.fin_start, L.pfn,
+                                   L.ckpt, L.exq, L.o_gc, L.o_trunc))
         return -1;
     stage(6);
-    if (L.want_lc && launch_expand(s, P, 1, L.lchunk, L.accuracy, L.pfn, L.state, L.tab, L.raw, L.o_lc,
-                                   L.o_trunc + 1))
+    if (L.want_lc && launch_expand(s, B, 1, L.nck_lc, L.ck_lc, L.n_ex, L.ex, L.nfin, L.fin_start, L.pfn,
+                                   L.ckpt, L.exq, L.o_lc, L.o_trunc + L.ncase))
         return -1;
     stage(7);
     if (L.pf_from) {
-        const int *tr = L.want_lc ? L.o_trunc + 1 : L.o_trunc;
+        const int *tr = L.want_lc ? L.o_trunc + L.ncase : L.o_trunc;
         const double *cf = L.pf_from == 1 ? L.o_gc : L.o_lc;
-        if (launch_phase_user(s, P, L.pf_from == 1 ? 0 : 1, cf, tr, L.mu_user, L.o_pf)) return -1;
+        if (launch_phase_user(s, B, L.pf_from == 1 ? 0 : 1, L.pu_total, L.pu_start, cf, tr, L.o_pf)) return -1;
     }
     stage(8);
     return 0;
 }
 
 template <class T>
-T *put(char *&hp, size_t &off, const T *src, size_t count) {
+T *put(char *hp, size_t &off, const T *src, size_t count) {
     T *at = (T *) (hp + off);
     if (src && count) memcpy(at, src, count * sizeof(T));
     off += pad(count * sizeof(T));
     return at;
 }
 
-}  // namespace
+// Device bytes one case needs beyond its inputs (for cutting sub-batches).
+size_t case_bytes(const lmieb_problem &p) {
+    long long tot = 0;
+    for (int r = 0; r < p.n; ++r) tot += p.n1r[r] + 1;
+    const size_t ncol = 1 + p.nd;
+    size_t b = (size_t) tot * 32 * 2 * (1 + p.nd1);                    // rec + coef
+    b += (size_t) p.n * (64 + 8 * ncol + 40 * (1 + p.nd1));           // per-radius arrays, sums
+    b += (size_t) 4 * ncol * p.n_qang * 8 * 8;                        // partials (groups), pf, pfn
+    b += (size_t) ncol * 6 * p.n_coef * 8 * (3 + (p.n_qang / 2 + 31) / 32);   // expansion partials + outputs
+    b += (size_t) 4 * (p.n_qang / 2) * (p.n_coef / EX_LT + 1) * 16;   // checkpoints
+    return b;
+}
 
-extern "C" int lmieb_device_solve(const lmieb_problem *p, lmieb_result *res) {
-    std::lock_guard<std::mutex> lock(g_mu);
-    if (ensure_ready()) return -1;
+// One sub-batch: ps[0..n).
+int solve_sub(int ncase, const lmieb_problem *ps, lmieb_result *rs_out) {
     Ctx &c = g_ctx;
     Plan &L = *c.plan;
     L = Plan();
+    const lmieb_problem &p0 = ps[0];
+    const int nd = p0.nd, nd1 = p0.nd1, nd2 = p0.nd2, ncol = 1 + nd;
+    const size_t Q = (size_t) 4 * ncol;
+    L.ncase = ncase;
+    L.want_gc = p0.want_gc && p0.n_qang > 0;
+    L.want_lc = p0.want_lc && p0.n_qang > 0;
+    L.pf_from = p0.n_angles > 0 ? p0.pf_from : 0;
+    L.save_control = p0.save_control;
+    L.n_qang0 = p0.n_qang;
+    L.nd1c = (nd1 + 3) / 4;
+    L.n_ang_launch = std::max(1, std::max((nd1 + 3) / 4, (nd2 + 3) / 4));
 
-    const int n = p->n, nd = p->nd, nd1 = p->nd1, nd2 = p->nd2;
-    const int ncol = 1 + nd;
-    const int n_qang = p->n_qang, nh = n_qang / 2, n_coef = p->n_coef;
-    const int na = p->n_angles;
-
-    // ---- host-side plan: offsets, order tables, radius groups ----
-    std::vector<long long> off(n + 1);
-    off[0] = 0;
-    int n1max = 0;
-    for (int r = 0; r < n; ++r) {
-        off[r + 1] = off[r] + p->n1r[r];
-        if (p->n1r[r] > n1max) n1max = p->n1r[r];
+    // ---- case table and batch-wide per-radius arrays ----
+    std::vector<DevCase> cs(ncase);
+    int R = 0, n1max = 1, ncmax = 1, nqmax = 0;
+    for (int k = 0; k < ncase; ++k) {
+        R += ps[k].n;
+        ncmax = std::max(ncmax, ps[k].n_coef);
+        nqmax = std::max(nqmax, ps[k].n_qang);
+        for (int r = 0; r < ps[k].n; ++r) n1max = std::max(n1max, ps[k].n1r[r]);
     }
-    const long long tot = off[n];
-    const int n1 = p->n1;
-    std::vector<long long> offp(n + 1);
-    std::vector<int> tstart(n + 1);
+    std::vector<double> x(R), xl((size_t) std::max(nd1, 1) * R), w((size_t) ncol * R);
+    std::vector<int> n1r(R), n2r(R), rcase(R), tstart(R + 1);
+    std::vector<long long> off(R + 1), offp(R + 1);
     std::vector<int2> tiles;
-    offp[0] = 0;
-    for (int r = 0; r < n; ++r) {
-        offp[r + 1] = offp[r] + p->n1r[r] + 1;
-        tstart[r] = (int) tiles.size();
-        for (int j0 = 1; j0 <= p->n1r[r]; j0 += 127) tiles.push_back(make_int2(r, j0));
+    std::vector<cplx> ml((size_t) std::max(1, ncase * nd));
+    std::vector<double> laml((size_t) std::max(1, ncase * nd));
+    off[0] = offp[0] = 0;
+    {
+        int r = 0;
+        for (int k = 0; k < ncase; ++k) {
+            const lmieb_problem &p = ps[k];
+            DevCase &C = cs[k];
+            memset(&C, 0, sizeof(C));
+            C.lambda = p.lambda;
+            C.m = mk(p.mr, -p.mi);
+            C.minv = 1. / C.m;
+            C.accuracy = p.accuracy;
+            C.r0 = r;
+            C.nr = p.n;
+            C.n1 = p.n1;
+            C.n_qang = p.n_qang;
+            C.nh = p.n_qang / 2;
+            C.n_coef = p.n_coef;
+            C.n_angles = L.pf_from ? p.n_angles : 0;
+            C.ml_off = k * nd;
+            for (int kk = 0; kk < nd; ++kk) {
+                ml[(size_t) k * nd + kk] = mk(p.mr_l[kk], -p.mi_l[kk]);
+                laml[(size_t) k * nd + kk] = p.lambda_l[kk];
+            }
+            for (int i = 0; i < p.n; ++i, ++r) {
+                x[r] = p.x[i];
+                for (int q = 0; q < nd1; ++q) xl[(size_t) q * R + r] = p.xl[(size_t) q * p.n + i];
+                for (int q = 0; q < ncol; ++q) w[(size_t) q * R + r] = p.w[(size_t) q * p.n + i];
+                n1r[r] = p.n1r[i];
+                n2r[r] = p.n2r[i];
+                rcase[r] = k;
+                off[r + 1] = off[r] + n1r[r];
+                offp[r + 1] = offp[r] + n1r[r] + 1;
+                tstart[r] = (int) tiles.size();
+                for (int j0 = 1; j0 <= n1r[r]; j0 += 127) tiles.push_back(make_int2(r, j0));
+            }
+        }
     }
-    tstart[n] = (int) tiles.size();
-    const long long totp = offp[n];
+    tstart[R] = (int) tiles.size();
+    const long long tot = off[R], totp = offp[R];
     const int ntiles = (int) tiles.size();
-    std::vector<double> fv((size_t) 4 * (n1 + 2), 0.);
-    for (int i = 1; i <= n1 + 1; ++i) {
-        double f1 = 2. * i + 1., f2 = (i + 1.) / i;
+
+    // ---- order tables ----
+    std::vector<double> fv((size_t) 4 * (n1max + 2), 0.);
+    for (int i = 1; i <= n1max + 1; ++i) {
+        const double f1 = 2. * i + 1., f2 = (i + 1.) / i;
         fv[i] = f1;
-        fv[(size_t) (n1 + 2) + i] = f2;
-        fv[(size_t) 2 * (n1 + 2) + i] = (i + 2.) / f2;
-        fv[(size_t) 3 * (n1 + 2) + i] = f1 / (i * (i + 1.));
+        fv[(size_t) (n1max + 2) + i] = f2;
+        fv[(size_t) 2 * (n1max + 2) + i] = (i + 2.) / f2;
+        fv[(size_t) 3 * (n1max + 2) + i] = f1 / (i * (i + 1.));
     }
     fv[0] = 1.;
-    // radius groups of roughly equal work for K3
-    int G = 1;
-    std::vector<int> gstart;
-    if (n_qang > 0) {
-        const int per = angular_angles_per_block(nd1 < 4 ? nd1 : 4);
-        int tiles = (nh + per - 1) / per;
-        // one full wave at the kernel's occupancy (4 blocks per SM)
-        int target = 4 * c.sms;
-        G = (target + tiles - 1) / tiles;
-        if (G > n) G = n;
-        if (G < 1) G = 1;
-        gstart.resize(G + 1);
-        gstart[0] = 0;
-        int gi = 1;
-        for (int r = 0; r < n && gi < G; ++r) {
-            if ((double) off[r + 1] * G >= (double) tot * gi) gstart[gi++] = r + 1;
-        }
-        while (gi < G) gstart[gi++] = n;
-        gstart[G] = n;
-        // keep the groups strictly increasing
-        for (int i = 1; i <= G; ++i)
-            if (gstart[i] < gstart[i - 1]) gstart[i] = gstart[i - 1];
-    } else {
-        gstart.assign(2, 0);
-        gstart[1] = n;
-    }
-    // Newton starting points of the Gauss angles (host libm, as the reference)
-    std::vector<double> guess(n_qang > 0 ? (n_qang + 1) / 2 : 1, 0.);
-    if (n_qang > 0) {
-        const int ia = 4 * n_qang + 2;
-        const double da = (n_qang - 1) / (8. * pow((double) n_qang, 3));
-        for (int i = 0; i < (n_qang + 1) / 2; ++i) {
-            double th = (4. * i + 3.) / ia * LMIEB_PI;
-            guess[i] = cos(th + da / tan(th));
-        }
-    }
-    std::vector<double> gl_jr(n_qang > 0 ? n_qang : 1, 0.);
-    for (int j = 0; j < n_qang; ++j) gl_jr[j] = j / (j + 1.);
-    // GSF / Legendre recurrence coefficients per order l (j = l - 1)
-    std::vector<double> rc((size_t) 8 * (n_coef > 0 ? n_coef : 1), 0.);
-    for (int l = 3; l < n_coef; ++l) {
+    std::vector<double> rc((size_t) 8 * ncmax, 0.);
+    for (int l = 3; l < ncmax; ++l) {
         const int j = l - 1;
         const double jj = (double) j * j, jp1 = j + 1., jjp1 = j * jp1, jp1s = jp1 * jp1, tj1 = 2 * j + 1;
         const double a02 = sqrt(jj - 4), b02 = sqrt(jp1s - 4);
@@ -324,279 +349,441 @@ extern "C" int lmieb_device_solve(const lmieb_problem *p, lmieb_result *res) {
         q[5] = a22 / c22;
         q[6] = b22 / c22;
     }
-    for (int l = 2; l < 3 && l < n_coef; ++l) rc[(size_t) 8 * l + 1] = 1. / 2.;   // Legendre at l = 2
-    std::vector<cplx> ml(nd > 0 ? nd : 1);
-    for (int k = 0; k < nd; ++k) ml[k] = mk(p->mr_l[k], -p->mi_l[k]);
+    if (ncmax > 2) rc[(size_t) 8 * 2 + 1] = 1. / 2.;   // Legendre at l = 2
 
-    L.nd1c = (nd1 + 3) / 4;
-    L.n_ang_launch = (nd1 > nd2 ? (nd1 + 3) / 4 : (nd2 + 3) / 4);
-    if (L.n_ang_launch < 1) L.n_ang_launch = 1;
-    L.G = G;
-    (void) n1max;
-    if (nh > 0) {
-        size_t lc = TABLE_LIMIT / ((size_t) 4 * nh * 8);
-        if (lc < 32) lc = 32;
-        L.lchunk = (int) (lc < (size_t) n_coef ? lc : (size_t) n_coef);
+    // ---- Gauss angles: pool entries, new orders computed on the device ----
+    std::vector<int> gl_ns, gl_pt, gl_pi;
+    std::vector<long long> gl_mo, gl_go;
+    std::vector<double> gl_guess, gl_jr((size_t) std::max(nqmax, 1), 0.);
+    for (int j = 0; j < nqmax; ++j) gl_jr[j] = j / (j + 1.);
+    {
+        size_t need = c.gl_used;
+        for (int k = 0; k < ncase; ++k) {
+            const int nq = cs[k].n_qang;
+            if (nq <= 0) continue;
+            long long at = -1;
+            for (auto &e : c.gl_map)
+                if (e.first == nq) at = e.second;
+            if (at < 0) {
+                for (size_t t = 0; t < gl_ns.size(); ++t)
+                    if (gl_ns[t] == nq) at = gl_mo[t];
+            }
+            if (at < 0) {
+                at = (long long) need;
+                need += 2 * (size_t) nq;
+                const int ia = 4 * nq + 2, half = (nq + 1) / 2;
+                const double da = (nq - 1) / (8. * pow((double) nq, 3));
+                gl_ns.push_back(nq);
+                gl_mo.push_back(at);
+                gl_go.push_back((long long) gl_guess.size());
+                for (int i = 0; i < half; ++i) {
+                    const double th = (4. * i + 3.) / ia * LMIEB_PI;
+                    gl_guess.push_back(cos(th + da / tan(th)));
+                    gl_pt.push_back((int) gl_ns.size() - 1);
+                    gl_pi.push_back(i);
+                }
+            }
+            cs[k].mu_off = at;
+        }
+        if (ensure_gl_pool(need)) return -1;
+        for (size_t t = 0; t < gl_ns.size(); ++t) c.gl_map.push_back({gl_ns[t], gl_mo[t]});
+        c.gl_used = need;
     }
-    L.want_gc = p->want_gc && n_qang > 0;
-    L.want_lc = p->want_lc && n_qang > 0;
-    L.pf_from = na > 0 ? p->pf_from : 0;
-    L.accuracy = p->accuracy;
-    L.save_control = p->save_control;
 
-    // ---- launches per run and algorithmic work (flops) of this solve ----
+    // ---- angular work items (largest first), partial and pf offsets ----
+    std::vector<AngItem> ang;
+    std::vector<long long> pf_start(ncase + 1, 0);
+    long long part_total = 0;
+    {
+        const int per = angular_angles_per_block(std::min(nd1, 4));
+        double W = 0.;
+        std::vector<double> wc(ncase, 0.);
+        for (int k = 0; k < ncase; ++k) {
+            if (cs[k].n_qang <= 0) continue;
+            double s = 0.;
+            for (int r = cs[k].r0; r < cs[k].r0 + cs[k].nr; ++r) s += n1r[r];
+            wc[k] = s * cs[k].nh;
+            W += wc[k];
+        }
+        const double wt = std::max(W / (4. * c.sms), 64. * 2 * 64 * 16);   // work per block
+        std::vector<std::pair<double, AngItem>> tmp;
+        for (int k = 0; k < ncase; ++k) {
+            DevCase &C = cs[k];
+            pf_start[k + 1] = pf_start[k] + (long long) Q * C.n_qang;
+            C.pf_off = pf_start[k];
+            if (C.n_qang <= 0) { C.G = 0; continue; }
+            const int xt = (C.nh + per - 1) / per;
+            int G = (int) std::lround(wc[k] / (xt * wt));
+            G = std::max(1, std::min(G, C.nr));
+            // groups of roughly equal sum of n1 over the case's radii
+            std::vector<int> gs(G + 1, C.r0 + C.nr);
+            gs[0] = C.r0;
+            const long long o0 = off[C.r0], ot = off[C.r0 + C.nr] - o0;
+            int gi = 1;
+            for (int r = C.r0; r < C.r0 + C.nr && gi < G; ++r)
+                if ((double) (off[r + 1] - o0) * G >= (double) ot * gi) gs[gi++] = r + 1;
+            for (int g = 1; g <= G; ++g) gs[g] = std::max(gs[g], gs[g - 1]);
+            C.G = G;
+            C.part_off = part_total;
+            part_total += (long long) G * Q * C.n_qang;
+            for (int g = 0; g < G; ++g)
+                for (int t = 0; t < xt; ++t) {
+                    AngItem it{k, t, g, gs[g], gs[g + 1]};
+                    const double cost = (double) (off[gs[g + 1]] - off[gs[g]]) * std::min(per, C.nh - t * per);
+                    tmp.push_back({cost, it});
+                }
+        }
+        std::stable_sort(tmp.begin(), tmp.end(), [](const std::pair<double, AngItem> &a,
+                                                    const std::pair<double, AngItem> &b) { return a.first > b.first; });
+        for (auto &e : tmp) ang.push_back(e.second);
+        L.pf_total = pf_start[ncase];
+        L.n_ang = (int) ang.size();
+    }
+
+    // ---- expansion work items and offsets ----
+    std::vector<ExpItem> ex;
+    std::vector<long long> ck_gc(ncase + 1, 0), ck_lc(ncase + 1, 0), fin_start(ncase + 1, 0);
+    long long ck_total = 0, ex_total = 0;
+    for (int k = 0; k < ncase; ++k) {
+        DevCase &C = cs[k];
+        const bool on = (L.want_gc || L.want_lc) && C.n_qang > 0;
+        const int nlt = on ? (C.n_coef + EX_LT - 1) / EX_LT : 0;
+        const int nat = on ? (C.nh + EX_AT - 1) / EX_AT : 0;
+        ck_gc[k + 1] = ck_gc[k] + (on ? 4LL * C.nh : 0);
+        ck_lc[k + 1] = ck_lc[k] + (on ? 1LL * C.nh : 0);
+        fin_start[k + 1] = fin_start[k] + (on ? (long long) ncol * C.n_coef : 0);
+        C.ck_off = ck_total;
+        ck_total += (long long) nlt * 4 * C.nh * 2;
+        C.ex_off = ex_total;
+        ex_total += (long long) nat * ncol * 6 * C.n_coef;
+        for (int lt = 0; lt < nlt; ++lt)
+            for (int at = 0; at < nat; ++at) ex.push_back(ExpItem{k, lt, at});
+    }
+    L.nck_gc = ck_gc[ncase];
+    L.nck_lc = ck_lc[ncase];
+    L.nfin = fin_start[ncase];
+    L.n_ex = (int) ex.size();
+
+    // ---- user angles and output offsets ----
+    std::vector<long long> pu_start(ncase + 1, 0);
+    std::vector<double> mu_user;
+    size_t o_scal = 0, o_gc = 0, o_lc = 0, o_pf = 0;
+    for (int k = 0; k < ncase; ++k) {
+        DevCase &C = cs[k];
+        C.mu_user_off = (long long) mu_user.size();
+        for (int a = 0; a < C.n_angles; ++a) mu_user.push_back(ps[k].mu_user[a]);
+        pu_start[k + 1] = pu_start[k] + (long long) ncol * C.n_angles;
+        C.scal_off = (int) o_scal;
+        o_scal += (size_t) ncol * 4;
+        C.gc_off = (long long) o_gc;
+        if (L.want_gc) o_gc += (size_t) ncol * 6 * C.n_coef;
+        C.lc_off = (long long) o_lc;
+        if (L.want_lc) o_lc += (size_t) ncol * 6 * C.n_coef;
+        C.pf_out_off = (long long) o_pf;
+        o_pf += (size_t) ncol * 6 * C.n_angles;
+    }
+    L.pu_total = pu_start[ncase];
+
+    // ---- launches per device run and algorithmic work ----
     {
         long long nl = 0;
-        const long long lchunks = nh > 0 ? (n_coef + L.lchunk - 1) / L.lchunk : 0;
-        if (p->save_control != 2) {
-            nl += (long long) (L.nd1c > 0 ? L.nd1c : 1) * 2 + 1;      // K1a + K1b per chunk, tile sums
-            nl += 1;                                                  // K2
-            if (n_qang > 0) nl += L.n_ang_launch + 1;                 // K3 + group reduction
+        if (L.save_control != 2) {
+            nl += (long long) std::max(L.nd1c, 1) * 2 + 1 + 1;                  // K1a+K1b per chunk, tiles, K2
+            if (L.n_ang > 0) nl += L.n_ang_launch + 1;                          // K3 + group reduction
         } else {
-            nl += 1 + (n_qang > 0);
+            nl += 1 + (L.n_qang0 > 0);
         }
-        nl += 1;                                                      // normalisation
-        if (L.want_gc) nl += 2 * lchunks + 1;
-        if (L.want_lc) nl += 2 * lchunks + 1;
-        if (L.pf_from) nl += 1;
+        nl += 1 + (L.pf_total > 0);                                              // normalisation
+        if (L.want_gc && L.n_ex > 0) nl += 3;
+        if (L.want_lc && L.n_ex > 0) nl += 3;
+        if (L.pf_from && L.pu_total > 0) nl += 1;
         L.launches = nl;
-        // Algorithmic flop counts (fixed per-order constants counted from the
-        // FP64 kernels): angular S1/S2 contraction 8 flops per (angle, order,
-        // radius, column); recurrences 14 per D_n order + 93 per a_n/b_n order
-        // for the value and 16 + 154 for each tangent-linear column;
-        // expansion 12 per (order, angle, column); user angles 12 per
-        // (order, angle, column).
-        double fang = 0., frec = 0.;
-        for (int r = 0; r < n; ++r) {
-            fang += 8. * n_qang * p->n1r[r] * (1. + nd1);
-            frec += (14. * p->n2r[r] + 93. * p->n1r[r]) + nd1 * (16. * p->n2r[r] + 154. * p->n1r[r]);
+        double fang = 0., frec = 0., fgsf = 0., fexp = 0.;
+        for (int k = 0; k < ncase; ++k) {
+            const DevCase &C = cs[k];
+            for (int r = C.r0; r < C.r0 + C.nr; ++r) {
+                fang += 8. * C.n_qang * n1r[r] * (1. + nd1);
+                frec += (14. * n2r[r] + 93. * n1r[r]) + nd1 * (16. * n2r[r] + 154. * n1r[r]);
+            }
+            fgsf += 12. * C.n_coef * C.n_qang * ncol * ((L.want_gc ? 1 : 0) + (L.want_lc ? 1 : 0));
+            fexp += 12. * C.n_angles * C.n_coef * ncol;
         }
-        if (p->save_control == 2) fang = frec = 0.;
-        double fgsf = 12. * n_coef * n_qang * ncol * ((L.want_gc ? 1 : 0) + (L.want_lc ? 1 : 0));
-        double fexp = L.pf_from ? 12. * na * n_coef * ncol : 0.;
-        c.work[0] = fang;
-        c.work[1] = frec;
-        c.work[2] = fgsf;
-        c.work[3] = fexp;
+        if (L.save_control == 2) fang = frec = 0.;
+        c.work[0] += fang;
+        c.work[1] += frec;
+        c.work[2] += fgsf;
+        c.work[3] += fexp;
+        c.launches += nl + (gl_pt.empty() ? 0 : 1);
     }
 
     // ---- host staging: inputs then outputs ----
-    const size_t n_save2 = (size_t) 4 * n * (n_qang > 0 ? n_qang : 1);
+    const size_t n_save2 = (size_t) 4 * R * std::max(L.n_qang0, 1);
     size_t in_bytes = 0;
     {
         auto add = [&](size_t b) { in_bytes += pad(b); };
-        add(n * 8); add((size_t) nd1 * n * 8); add((size_t) ncol * n * 8); add(n * 4); add(n * 4);
-        add((size_t) (n + 1) * 8); add((size_t) (n + 1) * 8); add((size_t) (n + 1) * 4);
-        add(tiles.size() * 8); add(fv.size() * 8); add(ml.size() * 16); add((nd > 0 ? nd : 1) * 8);
-        add((nd1 > 0 ? nd1 : 1) * 4); add((nd2 > 0 ? nd2 : 1) * 4); add((na > 0 ? na : 1) * 8);
-        add(gstart.size() * 4);
-        add(guess.size() * 8);
-        add(gl_jr.size() * 8);
-        add(rc.size() * 8);
-        if (p->save_control == 2) { add((size_t) 4 * n * 8); add(n_save2 * 8); add((size_t) (nd > 0 ? nd : 1) * n * 8); }
+        add(cs.size() * sizeof(DevCase)); add((size_t) R * 8); add(xl.size() * 8); add(w.size() * 8);
+        add((size_t) R * 4); add((size_t) R * 4); add((size_t) R * 4);
+        add((size_t) (R + 1) * 8); add((size_t) (R + 1) * 8); add((size_t) (R + 1) * 4);
+        add(tiles.size() * 8); add(fv.size() * 8); add(rc.size() * 8); add(ml.size() * 16); add(laml.size() * 8);
+        add((size_t) nd1 * 4); add((size_t) nd2 * 4); add(mu_user.size() * 8);
+        add(ang.size() * sizeof(AngItem)); add(ex.size() * sizeof(ExpItem));
+        for (int q = 0; q < 5; ++q) add((size_t) (ncase + 1) * 8);
+        add(gl_ns.size() * 4); add(gl_mo.size() * 8); add(gl_go.size() * 8); add(gl_pt.size() * 4);
+        add(gl_pi.size() * 4); add(gl_guess.size() * 8); add(gl_jr.size() * 8);
+        if (L.save_control == 2) { add((size_t) 4 * R * 8); add(n_save2 * 8); add((size_t) std::max(nd, 1) * R * 8); }
     }
     size_t out_bytes = 0;
     {
         auto add = [&](size_t b) { out_bytes += pad(b); };
-        add((size_t) ncol * 4 * 8);
-        if (L.want_gc) add((size_t) ncol * 6 * n_coef * 8);
-        if (L.want_lc) add((size_t) ncol * 6 * n_coef * 8);
-        if (L.pf_from) add((size_t) ncol * 6 * na * 8);
-        add(2 * 4);
-        if (p->save_control == 1) { add((size_t) 4 * n * 8); add(n_save2 * 8); }
+        add(o_scal * 8); add(o_gc * 8); add(o_lc * 8); add(o_pf * 8); add((size_t) 2 * ncase * 4);
+        if (L.save_control == 1) { add((size_t) 4 * R * 8); add(n_save2 * 8); }
     }
     if (ensure_host(in_bytes + out_bytes)) return -1;
     char *hp = c.hbuf;
     size_t ho = 0;
-    double *h_x = put(hp, ho, p->x, n);
-    double *h_xl = put(hp, ho, p->xl, (size_t) nd1 * n);
-    double *h_w = put(hp, ho, p->w, (size_t) ncol * n);
-    int *h_n1r = put(hp, ho, p->n1r, n);
-    int *h_n2r = put(hp, ho, p->n2r, n);
-    long long *h_off = put(hp, ho, off.data(), n + 1);
-    long long *h_offp = put(hp, ho, offp.data(), n + 1);
-    int *h_tstart = put(hp, ho, tstart.data(), n + 1);
+    DevCase *h_cs = put(hp, ho, cs.data(), cs.size());
+    double *h_x = put(hp, ho, x.data(), (size_t) R);
+    double *h_xl = put(hp, ho, xl.data(), xl.size());
+    double *h_w = put(hp, ho, w.data(), w.size());
+    int *h_n1r = put(hp, ho, n1r.data(), (size_t) R);
+    int *h_n2r = put(hp, ho, n2r.data(), (size_t) R);
+    int *h_rcase = put(hp, ho, rcase.data(), (size_t) R);
+    long long *h_off = put(hp, ho, off.data(), (size_t) R + 1);
+    long long *h_offp = put(hp, ho, offp.data(), (size_t) R + 1);
+    int *h_tstart = put(hp, ho, tstart.data(), (size_t) R + 1);
     int2 *h_tiles = put(hp, ho, tiles.data(), tiles.size());
     double *h_fv = put(hp, ho, fv.data(), fv.size());
-    cplx *h_ml = put(hp, ho, ml.data(), ml.size());
-    double *h_laml = put(hp, ho, p->lambda_l, nd);
-    int *h_i1 = put(hp, ho, p->idx1, nd1);
-    int *h_i2 = put(hp, ho, p->idx2, nd2);
-    double *h_mu = put(hp, ho, p->mu_user, na);
-    int *h_gs = put(hp, ho, gstart.data(), gstart.size());
-    double *h_guess = put(hp, ho, guess.data(), guess.size());
-    double *h_jr = put(hp, ho, gl_jr.data(), gl_jr.size());
     double *h_rc = put(hp, ho, rc.data(), rc.size());
+    cplx *h_ml = put(hp, ho, ml.data(), ml.size());
+    double *h_laml = put(hp, ho, laml.data(), laml.size());
+    int *h_i1 = put(hp, ho, p0.idx1, (size_t) nd1);
+    int *h_i2 = put(hp, ho, p0.idx2, (size_t) nd2);
+    double *h_mu = put(hp, ho, mu_user.data(), mu_user.size());
+    AngItem *h_ang = put(hp, ho, ang.data(), ang.size());
+    ExpItem *h_ex = put(hp, ho, ex.data(), ex.size());
+    long long *h_pfs = put(hp, ho, pf_start.data(), pf_start.size());
+    long long *h_ckg = put(hp, ho, ck_gc.data(), ck_gc.size());
+    long long *h_ckl = put(hp, ho, ck_lc.data(), ck_lc.size());
+    long long *h_fin = put(hp, ho, fin_start.data(), fin_start.size());
+    long long *h_pus = put(hp, ho, pu_start.data(), pu_start.size());
+    int *h_gns = put(hp, ho, gl_ns.data(), gl_ns.size());
+    long long *h_gmo = put(hp, ho, gl_mo.data(), gl_mo.size());
+    long long *h_ggo = put(hp, ho, gl_go.data(), gl_go.size());
+    int *h_gpt = put(hp, ho, gl_pt.data(), gl_pt.size());
+    int *h_gpi = put(hp, ho, gl_pi.data(), gl_pi.size());
+    double *h_gguess = put(hp, ho, gl_guess.data(), gl_guess.size());
+    double *h_gjr = put(hp, ho, gl_jr.data(), gl_jr.size());
     double *h_s1 = nullptr, *h_s2 = nullptr, *h_w2 = nullptr;
-    if (p->save_control == 2) {
-        h_s1 = put(hp, ho, p->save1_in, (size_t) 4 * n);
-        h_s2 = put(hp, ho, p->save2_in, n_save2);
-        h_w2 = put(hp, ho, p->w2, (size_t) (nd > 0 ? nd : 1) * n);
+    if (L.save_control == 2) {
+        h_s1 = put(hp, ho, p0.save1_in, (size_t) 4 * R);
+        h_s2 = put(hp, ho, p0.save2_in, n_save2);
+        h_w2 = put(hp, ho, p0.w2, (size_t) std::max(nd, 1) * R);
     }
     const size_t h_in_end = ho;
+    if (h_in_end > in_bytes) {
+        fprintf(stderr, "ERROR: lmie_b200: staging layout mismatch\n");
+        return -1;
+    }
     char *h_out = hp + h_in_end;
 
     // ---- device arena ----
-    const size_t Q = (size_t) 4 * ncol;
     size_t dev_bytes = in_bytes + out_bytes + 64 * 256;
     {
         auto add = [&](size_t b) { dev_bytes += pad(b); };
-        if (p->save_control != 2) {
+        if (L.save_control != 2) {
             add((size_t) (1 + nd1) * (size_t) totp * 32);
             add((size_t) (1 + nd1) * 5 * (size_t) ntiles * 8);
             add((size_t) (1 + nd1) * (size_t) tot * 32);
-            add((size_t) (1 + nd1) * 5 * n * 8);
-            add((size_t) G * Q * (n_qang > 0 ? n_qang : 1) * 8);
+            add((size_t) (1 + nd1) * 5 * (size_t) R * 8);
+            add((size_t) part_total * 8);
         }
-        add((size_t) ncol * 4 * 8);
-        add(Q * (n_qang > 0 ? n_qang : 1) * 8 * 2);
-        if (L.want_gc || L.want_lc) {
-            add((size_t) 8 * nh * 8);
-            add((size_t) 4 * L.lchunk * nh * 8);
-            add((size_t) ncol * 6 * n_coef * 8);
-        }
+        add((size_t) ncase * ncol * 4 * 8);
+        add((size_t) L.pf_total * 8);
+        add((size_t) L.pf_total * 8);
+        add((size_t) ck_total * 8);
+        add((size_t) ex_total * 8);
     }
     if (ensure_device(dev_bytes)) return -1;
     Arena A{c.dbuf, 0, c.dcap};
-    // inputs mirror the host staging layout exactly: one H2D copy
     char *d_in = A.take<char>(h_in_end);
-    auto dptr = [&](void *h) { return d_in + ((char *) h - hp); };
     char *d_out = A.take<char>(out_bytes);
     if (!d_in || !d_out) {
         fprintf(stderr, "ERROR: lmie_b200: device arena too small\n");
         return -1;
     }
+    auto dptr = [&](void *h) { return d_in + ((char *) h - hp); };
 
-    DevProblem &P = L.P;
-    P.n = n; P.nd = nd; P.nd1 = nd1; P.nd2 = nd2;
-    P.n1 = n1; P.n_qang = n_qang; P.nh = nh; P.n_coef = n_coef;
-    P.n_angles = L.pf_from ? na : 0;
-    P.save_control = p->save_control;
-    P.lambda = p->lambda;
-    P.m = mk(p->mr, -p->mi);
-    P.minv = 1. / P.m;
-    P.m2 = P.m * P.m;
-    P.m_l = (const cplx *) dptr(h_ml);
-    P.lambda_l = (const double *) dptr(h_laml);
-    P.idx1 = (const int *) dptr(h_i1);
-    P.idx2 = (const int *) dptr(h_i2);
-    P.x = (const double *) dptr(h_x);
-    P.xl = (const double *) dptr(h_xl);
-    P.w = (const double *) dptr(h_w);
-    P.n1r = (const int *) dptr(h_n1r);
-    P.n2r = (const int *) dptr(h_n2r);
-    P.off = (const long long *) dptr(h_off);
-    P.tot = tot;
-    P.offp = (const long long *) dptr(h_offp);
-    P.totp = totp;
-    P.ntiles = ntiles;
+    DevBatch &B = L.B;
+    memset(&B, 0, sizeof(B));
+    B.ncase = ncase;
+    B.R = R;
+    B.nd = nd; B.nd1 = nd1; B.nd2 = nd2;
+    B.n1max = n1max; B.ncmax = ncmax;
+    B.cs = (const DevCase *) dptr(h_cs);
+    B.idx1 = (const int *) dptr(h_i1);
+    B.idx2 = (const int *) dptr(h_i2);
+    B.m_l = (const cplx *) dptr(h_ml);
+    B.lambda_l = (const double *) dptr(h_laml);
+    B.rcase = (const int *) dptr(h_rcase);
+    B.x = (const double *) dptr(h_x);
+    B.xl = (const double *) dptr(h_xl);
+    B.w = (const double *) dptr(h_w);
+    B.n1r = (const int *) dptr(h_n1r);
+    B.n2r = (const int *) dptr(h_n2r);
+    B.off = (const long long *) dptr(h_off);
+    B.offp = (const long long *) dptr(h_offp);
+    B.tot = tot;
+    B.totp = totp;
+    B.ntiles = ntiles;
+    B.fv = (const double *) dptr(h_fv);
+    B.rc = (const double *) dptr(h_rc);
+    B.mu_pool = c.gl_pool;
+    B.mu_user = (const double *) dptr(h_mu);
     L.tiles = (int2 *) dptr(h_tiles);
     L.tstart = (int *) dptr(h_tstart);
-    P.fv = (const double *) dptr(h_fv);
-    L.gstart = (int *) dptr(h_gs);
-    P.gl_guess = (const double *) dptr(h_guess);
-    P.gl_jr = (const double *) dptr(h_jr);
-    P.rc = (const double *) dptr(h_rc);
-    L.mu_user = (double *) dptr(h_mu);
-    if (p->save_control == 2) {
+    L.ang = (AngItem *) dptr(h_ang);
+    L.ex = (ExpItem *) dptr(h_ex);
+    L.pf_start = (long long *) dptr(h_pfs);
+    L.ck_gc = (long long *) dptr(h_ckg);
+    L.ck_lc = (long long *) dptr(h_ckl);
+    L.fin_start = (long long *) dptr(h_fin);
+    L.pu_start = (long long *) dptr(h_pus);
+    if (L.save_control == 2) {
         L.save1_in = (double *) dptr(h_s1);
         L.save2_in = (double *) dptr(h_s2);
         L.w2 = (double *) dptr(h_w2);
     }
-    bool gl_new = false;
-    P.mu = P.wq = nullptr;
-    if (n_qang > 0) {
-        for (auto &e : c.gl_cache)
-            if (e.n == n_qang) { P.mu = e.mu; P.wq = e.wq; }
-        if (!P.mu) {
-            if (c.gl_cache.size() >= GL_CACHE) {
-                LMIEB_CUDA_TRY(cudaFree(c.gl_cache.front().mu));
-                c.gl_cache.erase(c.gl_cache.begin());
-            }
-            Ctx::GlEntry e{n_qang, nullptr, nullptr};
-            LMIEB_CUDA_TRY(cudaMalloc((void **) &e.mu, sizeof(double) * 2 * (size_t) n_qang));
-            e.wq = e.mu + n_qang;
-            c.gl_cache.push_back(e);
-            P.mu = e.mu;
-            P.wq = e.wq;
-            gl_new = true;
-        }
-    }
-    if (p->save_control != 2) {
+    if (L.save_control != 2) {
         L.rec = A.take<double4>((size_t) (1 + nd1) * (size_t) totp);
         L.rsp = A.take<double>((size_t) (1 + nd1) * 5 * (size_t) ntiles);
         L.coef = A.take<double>((size_t) (1 + nd1) * (size_t) tot * 4);
-        L.rs = A.take<double>((size_t) (1 + nd1) * 5 * n);
-        L.part = A.take<double>((size_t) G * Q * (n_qang > 0 ? n_qang : 1));
+        L.rs = A.take<double>((size_t) (1 + nd1) * 5 * (size_t) R);
+        L.part = A.take<double>((size_t) part_total);
     }
-    L.sums = A.take<double>((size_t) ncol * 4);
-    L.pfacc = A.take<double>(Q * (n_qang > 0 ? n_qang : 1));
-    L.pfn = A.take<double>(Q * (n_qang > 0 ? n_qang : 1));
-    if (L.want_gc || L.want_lc) {
-        L.state = A.take<double>((size_t) 8 * nh);
-        L.tab = A.take<double>((size_t) 4 * L.lchunk * nh);
-        L.raw = A.take<double>((size_t) ncol * 6 * n_coef);
-    }
-    // output region
+    L.sums = A.take<double>((size_t) ncase * ncol * 4);
+    L.pfacc = A.take<double>((size_t) L.pf_total);
+    L.pfn = A.take<double>((size_t) L.pf_total);
+    L.ckpt = A.take<double>((size_t) ck_total);
+    L.exq = A.take<double>((size_t) ex_total);
     {
         char *o = d_out;
         auto take = [&](size_t bytes) { char *r = o; o += pad(bytes); return r; };
-        L.o_scal = (double *) take((size_t) ncol * 4 * 8);
-        if (L.want_gc) L.o_gc = (double *) take((size_t) ncol * 6 * n_coef * 8);
-        if (L.want_lc) L.o_lc = (double *) take((size_t) ncol * 6 * n_coef * 8);
-        if (L.pf_from) L.o_pf = (double *) take((size_t) ncol * 6 * na * 8);
-        L.o_trunc = (int *) take(2 * 4);
-        if (p->save_control == 1) {
-            L.o_save1 = (double *) take((size_t) 4 * n * 8);
+        L.o_scal = (double *) take(o_scal * 8);
+        L.o_gc = (double *) take(o_gc * 8);
+        L.o_lc = (double *) take(o_lc * 8);
+        L.o_pf = (double *) take(o_pf * 8);
+        L.o_trunc = (int *) take((size_t) 2 * ncase * 4);
+        if (L.save_control == 1) {
+            L.o_save1 = (double *) take((size_t) 4 * R * 8);
             L.o_save2 = (double *) take(n_save2 * 8);
         }
-        L.out_begin = d_out;
-        L.out_bytes = out_bytes;
     }
-    if (!L.sums || !L.pfn || (p->save_control != 2 && !L.part) || ((L.want_gc || L.want_lc) && !L.raw)) {
+    if (!L.sums || !L.pfn || !L.exq || (L.save_control != 2 && !L.part)) {
         fprintf(stderr, "ERROR: lmie_b200: device arena too small\n");
         return -1;
     }
 
-    c.h2d = h_in_end;
-    c.d2h = out_bytes;
-
     // ---- run ----
+    c.h2d += h_in_end;
+    c.d2h += out_bytes;
     cudaStream_t s = c.stream;
     stage(0);
     LMIEB_CUDA_TRY(cudaMemcpyAsync(d_in, hp, h_in_end, cudaMemcpyHostToDevice, s));
     LMIEB_CUDA_TRY(cudaMemsetAsync(d_out, 0, out_bytes, s));
-    if (gl_new && launch_gauss(s, n_qang, P.gl_guess, P.gl_jr, (double *) P.mu, (double *) P.wq)) return -1;
+    if (!gl_pt.empty() &&
+        launch_gauss(s, (int) gl_pt.size(), (int *) dptr(h_gpt), (int *) dptr(h_gpi), (int *) dptr(h_gns),
+                     (long long *) dptr(h_gmo), (long long *) dptr(h_ggo), (double *) dptr(h_gguess),
+                     (double *) dptr(h_gjr), c.gl_pool))
+        return -1;
     if (run_kernels(L)) return -1;
     LMIEB_CUDA_TRY(cudaMemcpyAsync(h_out, d_out, out_bytes, cudaMemcpyDeviceToHost, s));
-    stage(9 < NSTAGE ? 9 : NSTAGE);
+    stage(NSTAGE);
     LMIEB_CUDA_TRY(cudaStreamSynchronize(s));
     LMIEB_CUDA_TRY(cudaGetLastError());
     if (c.timing) {
         for (int i = 0; i < NSTAGE; ++i) {
             float ms = 0.f;
             if (cudaEventElapsedTime(&ms, c.ev[i], c.ev[i + 1]) != cudaSuccess) ms = 0.f;
-            c.stage_ms[i] = ms;
+            c.stage_ms[i] += ms;
         }
     }
     c.have_plan = true;
 
     // ---- unpack ----
     auto hostp = [&](void *d) { return h_out + ((char *) d - d_out); };
-    memcpy(res->scal, hostp(L.o_scal), (size_t) ncol * 4 * 8);
-    if (L.want_gc && res->gc) memcpy(res->gc, hostp(L.o_gc), (size_t) ncol * 6 * n_coef * 8);
-    if (L.want_lc && res->lc) memcpy(res->lc, hostp(L.o_lc), (size_t) ncol * 6 * n_coef * 8);
-    if (L.pf_from && res->pf) memcpy(res->pf, hostp(L.o_pf), (size_t) ncol * 6 * na * 8);
-    {
-        const int *tr = (const int *) hostp(L.o_trunc);
-        int t = L.want_lc ? tr[1] : (L.want_gc ? tr[0] : 0);
-        res->n_coef_out = (L.want_gc || L.want_lc) ? (t > 0 ? n_coef - t + 1 : n_coef) : 0;
+    const double *hs = (const double *) hostp(L.o_scal);
+    const double *hg = (const double *) hostp(L.o_gc);
+    const double *hl = (const double *) hostp(L.o_lc);
+    const double *hpf = (const double *) hostp(L.o_pf);
+    const int *htr = (const int *) hostp(L.o_trunc);
+    for (int k = 0; k < ncase; ++k) {
+        const DevCase &C = cs[k];
+        lmieb_result &r = rs_out[k];
+        memcpy(r.scal, hs + C.scal_off, (size_t) ncol * 4 * 8);
+        if (L.want_gc && r.gc) memcpy(r.gc, hg + C.gc_off, (size_t) ncol * 6 * C.n_coef * 8);
+        if (L.want_lc && r.lc) memcpy(r.lc, hl + C.lc_off, (size_t) ncol * 6 * C.n_coef * 8);
+        if (L.pf_from && r.pf) memcpy(r.pf, hpf + C.pf_out_off, (size_t) ncol * 6 * C.n_angles * 8);
+        const int t = L.want_lc ? htr[ncase + k] : (L.want_gc ? htr[k] : 0);
+        r.n_coef_out = (L.want_gc || L.want_lc) ? (t > 0 ? C.n_coef - t + 1 : C.n_coef) : 0;
     }
-    if (p->save_control == 1) {
-        if (res->save1) memcpy(res->save1, hostp(L.o_save1), (size_t) 4 * n * 8);
-        if (res->save2 && n_qang > 0) memcpy(res->save2, hostp(L.o_save2), n_save2 * 8);
+    if (L.save_control == 1) {
+        lmieb_result &r = rs_out[0];
+        if (r.save1) memcpy(r.save1, hostp(L.o_save1), (size_t) 4 * R * 8);
+        if (r.save2 && L.n_qang0 > 0) memcpy(r.save2, hostp(L.o_save2), n_save2 * 8);
     }
     return 0;
+}
+
+int check_uniform(int n, const lmieb_problem *p) {
+    for (int k = 1; k < n; ++k) {
+        bool same = p[k].nd == p[0].nd && p[k].nd1 == p[0].nd1 && p[k].nd2 == p[0].nd2 &&
+                    p[k].want_gc == p[0].want_gc && p[k].want_lc == p[0].want_lc &&
+                    p[k].pf_from == p[0].pf_from && p[k].save_control == 0 && p[0].save_control == 0;
+        for (int q = 0; same && q < p[0].nd1; ++q) same = p[k].idx1[q] == p[0].idx1[q];
+        for (int q = 0; same && q < p[0].nd2; ++q) same = p[k].idx2[q] == p[0].idx2[q];
+        if (!same) {
+            fprintf(stderr, "ERROR: lmie_b200: case %d of a batch differs from case 0 in its derivative "
+                    "layout, requested outputs or save_control\n", k);
+            return -1;
+        }
+    }
+    return 0;
+}
+
+}  // namespace
+
+extern "C" int lmieb_device_solve_batch(int n, const lmieb_problem *p, lmieb_result *r) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    if (n < 1) return 0;
+    if (ensure_ready()) return -1;
+    if (check_uniform(n, p)) return -1;
+    Ctx &c = g_ctx;
+    for (int i = 0; i < NSTAGE; ++i) c.stage_ms[i] = 0.;
+    for (int i = 0; i < 4; ++i) c.work[i] = 0.;
+    c.launches = 0;
+    c.h2d = c.d2h = 0;
+    c.have_plan = false;
+    // cut sub-batches by device working set
+    int k0 = 0, nsub = 0;
+    while (k0 < n) {
+        size_t bytes = 0;
+        int k1 = k0;
+        while (k1 < n) {
+            const size_t b = case_bytes(p[k1]);
+            if (k1 > k0 && bytes + b > BATCH_BYTES) break;
+            bytes += b;
+            ++k1;
+        }
+        if (solve_sub(k1 - k0, p + k0, r + k0)) return -1;
+        ++nsub;
+        k0 = k1;
+    }
+    if (nsub > 1) c.have_plan = false;   // re-running is only defined for one sub-batch
+    return 0;
+}
+
+extern "C" int lmieb_device_solve(const lmieb_problem *p, lmieb_result *r) {
+    return lmieb_device_solve_batch(1, p, r);
 }
 
 // ---------------------------------------------------------------------------
@@ -628,7 +815,7 @@ extern "C" int lmieb_rerun_device(int reps, int flush_l2, double *ms_total, doub
     std::lock_guard<std::mutex> lock(g_mu);
     Ctx &c = g_ctx;
     if (!c.ready || !c.have_plan) {
-        fprintf(stderr, "ERROR: lmieb_rerun_device: no solve has been prepared on this device\n");
+        fprintf(stderr, "ERROR: lmieb_rerun_device: no single-sub-batch solve is resident on the device\n");
         return -1;
     }
     if (flush_l2 && !c.flush) LMIEB_CUDA_TRY(cudaMalloc((void **) &c.flush, FLUSH_BYTES));
@@ -664,7 +851,7 @@ extern "C" int lmieb_last_work(double *flops, long long *launches, size_t *h2d, 
     Ctx &c = g_ctx;
     if (flops)
         for (int i = 0; i < 4; ++i) flops[i] = c.work[i];
-    if (launches) *launches = c.plan ? c.plan->launches : 0;
+    if (launches) *launches = c.launches;
     if (h2d) *h2d = c.h2d;
     if (d2h) *d2h = c.d2h;
     return 0;

@@ -7,6 +7,7 @@
  * usable GPU every solve returns -1 with an ERROR line.
  */
 #include <complex.h>
+#include <pthread.h>
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -294,18 +295,285 @@ int lmie_solution_slave(void) {
 }
 
 /* Scratch owned by one lmie_solution2_l call. */
-typedef struct {
-     double *qx, *qw, *nr, *qx_l, *qw_l, *nr_l;
-     double *x, *xl, *w, *w2, *mu_user, *sv1, *sv2;
-     int *n1r, *n2r, *idx1, *idx2;
-     double *dev_out;
-} call_scratch;
+/* ---- one case: host preparation, device solve, scatter ------------------- */
 
-static void scratch_free(call_scratch *s) {
-     free(s->qx); free(s->qw); free(s->nr); free(s->qx_l); free(s->qw_l); free(s->nr_l);
-     free(s->x); free(s->xl); free(s->w); free(s->w2); free(s->mu_user);
-     free(s->n1r); free(s->n2r); free(s->idx1); free(s->idx2); free(s->dev_out);
-     free(s->sv1); free(s->sv2);
+/* Everything one lmie_solution2_l call needs: its arguments (inputs and the
+ * caller's output pointers) and the scratch of its host preparation. */
+typedef struct {
+     /* inputs */
+     int calc_gc, calc_lc, calc_pf, dist_type, n_int1, n_int2, n_quad, n_angles, n_derivs, save_control;
+     double lambda, mr, mi, a1, a2, a3, a4, a5, r1, r2, accuracy;
+     double *lambda_l, *mr_l, *mi_l, *a1_l, *a2_l, *a3_l, *a4_l, *a5_l, *r1_l, *r2_l;
+     int verbose;
+     /* outputs */
+     int *n_coef;
+     double *r21, *r22, *norm, *reff, *veff, *gavg, *vavg, *ravg, *rvw, *cext, *csca, *cbak, *g;
+     double **gc, **lc, *theta, **pf;
+     double *r21_l, *r22_l, *norm_l, *reff_l, *veff_l, *gavg_l, *vavg_l, *ravg_l, *rvw_l;
+     double *cext_l, *csca_l, *cbak_l, *g_l;
+     double ***gc_l, ***lc_l, ***pf_l;
+     double ***save1;
+     double ****save2;
+     /* state */
+     int rc;
+     int n, nd, n_coef_all;
+     double *qx, *qw, *nr, *qx_l, *qw_l, *nr_l;
+     double *x, *xl, *w, *w2, *mu_user, *sv1, *sv2, *dev_out;
+     int *n1r, *n2r, *idx1, *idx2;
+     lmieb_problem P;
+     lmieb_result R;
+} case_job;
+
+static void job_free(case_job *j) {
+     free(j->qx); free(j->qw); free(j->nr); free(j->qx_l); free(j->qw_l); free(j->nr_l);
+     free(j->x); free(j->xl); free(j->w); free(j->w2); free(j->mu_user);
+     free(j->n1r); free(j->n2r); free(j->idx1); free(j->idx2); free(j->dev_out);
+     free(j->sv1); free(j->sv2);
+     j->qx = j->qw = j->nr = j->qx_l = j->qw_l = j->nr_l = NULL;
+     j->x = j->xl = j->w = j->w2 = j->mu_user = j->dev_out = j->sv1 = j->sv2 = NULL;
+     j->n1r = j->n2r = j->idx1 = j->idx2 = NULL;
+}
+
+/* Host steps before the Mie core (reference src/lmie_interface.c:404-451,
+ * src/lmie_schedule.c:1004-1072, src/lmie_core.c:263-292): size distribution,
+ * moments, derivative split, per-radius size parameters and truncation,
+ * user angles; fills j->P and points j->R at the output staging. */
+static int job_prepare(case_job *j) {
+     int n, nd = j->n_derivs > 0 ? j->n_derivs : 0, nd1 = 0, nd2 = 0, i, k;
+     int n1, n_qang, ncol;
+     double x2;
+     double complex m;
+     lmieb_dist_in din;
+     lmieb_dist_out dout;
+     lmieb_moments_out mom;
+     size_t n_out;
+
+     j->nd = nd;
+     /* input check (reference src/lmie_interface.c:404-408) */
+     if (j->calc_pf && (!j->calc_gc && !j->calc_lc)) {
+          fprintf(stderr, "ERROR: either calc_gc or calc_lc must be set to true when "
+                  "calc_pf is true\n");
+          return -1;
+     }
+     if (j->save_control < 0 || j->save_control > 2) {
+          fprintf(stderr, "ERROR: invalid save_control: %d\n", j->save_control);
+          return -1;
+     }
+     if (j->calc_pf && j->n_angles < 1) {
+          fprintf(stderr, "ERROR: n_angles must be >= 1 when calc_pf is true\n");
+          return -1;
+     }
+     n = lmieb_dist_count(j->dist_type, j->n_int1, j->n_int2, j->n_quad);
+     if (n <= 0) {
+          if (n == 0)
+               fprintf(stderr, "ERROR: size distribution has no quadrature points\n");
+          return -1;
+     }
+     j->n = n;
+
+     /* size distribution quadrature and moments */
+     j->qx = lmieb_arr1(n);
+     j->qw = lmieb_arr1(n);
+     j->nr = lmieb_arr1(n);
+     j->qx_l = lmieb_arr1((size_t) n * nd);
+     j->qw_l = lmieb_arr1((size_t) n * nd);
+     j->nr_l = lmieb_arr1((size_t) n * nd);
+     memset(&din, 0, sizeof(din));
+     din.dist_type = j->dist_type; din.n_int1 = j->n_int1; din.n_int2 = j->n_int2;
+     din.n_quad = j->n_quad; din.nd = nd;
+     din.a1 = j->a1; din.a2 = j->a2; din.a3 = j->a3; din.a4 = j->a4; din.a5 = j->a5;
+     din.r1 = j->r1; din.r2 = j->r2;
+     din.a1_l = j->a1_l; din.a2_l = j->a2_l; din.a3_l = j->a3_l; din.a4_l = j->a4_l;
+     din.a5_l = j->a5_l; din.r1_l = j->r1_l; din.r2_l = j->r2_l;
+     dout.qx = j->qx; dout.qw = j->qw; dout.nr = j->nr;
+     dout.qx_l = j->qx_l; dout.qw_l = j->qw_l; dout.nr_l = j->nr_l;
+     dout.r1_l = j->r21_l; dout.r2_l = j->r22_l; dout.norm_l = j->norm_l;
+     if (lmieb_particle_dist(&din, &dout) < 0) {
+          fprintf(stderr, "ERROR: get_particle_dist()\n");
+          return -1;
+     }
+     *j->r21 = dout.r1;
+     *j->r22 = dout.r2;
+     *j->norm = dout.norm;
+     mom.reff_l = j->reff_l; mom.veff_l = j->veff_l; mom.gavg_l = j->gavg_l;
+     mom.vavg_l = j->vavg_l; mom.ravg_l = j->ravg_l; mom.rvw_l = j->rvw_l;
+     lmieb_moments(n, nd, j->qx, j->qw, j->nr, j->qx_l, j->qw_l, j->nr_l, &mom);
+     *j->reff = mom.reff; *j->veff = mom.veff; *j->gavg = mom.gavg;
+     *j->vavg = mom.vavg; *j->ravg = mom.ravg; *j->rvw = mom.rvw;
+
+     /* derivative split (reference src/lmie_interface.c:304-353) */
+     j->idx1 = (int *) calloc(nd > 0 ? nd : 1, sizeof(int));
+     j->idx2 = (int *) calloc(nd > 0 ? nd : 1, sizeof(int));
+     for (i = 0; i < nd; ++i) {
+          if (j->lambda_l[i] != 0. || j->mr_l[i] != 0. || j->mi_l[i] != 0. ||
+              j->r21_l[i] != 0. || j->r22_l[i] != 0.)
+               j->idx1[nd1++] = i;
+          else
+               j->idx2[nd2++] = i;
+     }
+
+     /* global truncation (reference src/lmie_schedule.c:1004-1017) */
+     m = j->mr - I * j->mi;
+     x2 = 2. * M_PI * *j->r22 / j->lambda;
+     n1 = lmieb_calc_n1(x2);
+     n_qang = (!j->gc && !j->lc) ? 0 : 2 * n1;
+     j->n_coef_all = 2 * n1;
+
+     /* per-radius size parameters, truncation and weights
+      * (reference src/lmie_core.c:263-292) */
+     j->x = lmieb_arr1(n);
+     j->xl = lmieb_arr1((size_t) n * (nd1 > 0 ? nd1 : 1));
+     j->w = lmieb_arr1((size_t) n * (1 + nd));
+     j->n1r = (int *) calloc(n, sizeof(int));
+     j->n2r = (int *) calloc(n, sizeof(int));
+     for (i = 0; i < n; ++i) {
+          double x = 2. * M_PI * j->qx[i] / j->lambda;
+          double complex z = m * x;
+          j->x[i] = x;
+          j->n1r[i] = lmieb_calc_n1(x);
+          j->n2r[i] = lmieb_calc_n2(j->n1r[i], creal(z), cimag(z));
+          j->w[i] = j->nr[i] * j->qw[i];
+          for (k = 0; k < nd1; ++k) {
+               int kk = j->idx1[k];
+               j->xl[(size_t) k * n + i] = 2. * M_PI * (j->qx_l[(size_t) i * nd + kk] -
+                                           j->qx[i] * j->lambda_l[kk] / j->lambda) / j->lambda;
+               j->w[(size_t) (1 + kk) * n + i] = j->nr_l[(size_t) i * nd + kk] * j->qw[i] +
+                                                 j->nr[i] * j->qw_l[(size_t) i * nd + kk];
+          }
+          for (k = 0; k < nd2; ++k) {
+               int kk = j->idx2[k];
+               j->w[(size_t) (1 + kk) * n + i] = j->nr_l[(size_t) i * nd + kk] * j->qw[i];
+          }
+     }
+     if (n1 < 1 || j->n1r[n - 1] < 1) {
+          fprintf(stderr, "ERROR: invalid size parameter (lambda = %g, r2 = %g)\n", j->lambda, *j->r22);
+          return -1;
+     }
+     for (i = 0; i < n; ++i) {
+          if (j->n1r[i] > n1) {
+               fprintf(stderr, "ERROR: radius %d (r = %g) lies above r2 = %g\n", i, j->qx[i], *j->r22);
+               return -1;
+          }
+     }
+
+     /* save_control: allocate / gather the per-radius kernels */
+     if (j->save_control == 1) {
+          *j->save1 = lmieb_arr2(4, n);
+          *j->save2 = lmieb_arr3(4, n, n_qang > 0 ? n_qang : 1);
+     }
+     if (j->save_control == 2) {
+          int q, r;
+          if (!j->save1 || !*j->save1 || (n_qang > 0 && (!j->save2 || !*j->save2))) {
+               fprintf(stderr, "ERROR: save_control = 2 needs save1 and save2 from a "
+                       "save_control = 1 call\n");
+               return -1;
+          }
+          j->w2 = lmieb_arr1((size_t) n * (nd > 0 ? nd : 1));
+          for (i = 0; i < n; ++i)
+               for (k = 0; k < nd2; ++k) {
+                    int kk = j->idx2[k];
+                    j->w2[(size_t) kk * n + i] = j->nr_l[(size_t) i * nd + kk] * j->qw[i] +
+                                                 j->nr[i] * j->qw_l[(size_t) i * nd + kk];
+               }
+          /* gather the caller's kernels through their row pointers */
+          j->sv1 = lmieb_arr1((size_t) 4 * n);
+          j->sv2 = lmieb_arr1((size_t) 4 * n * (n_qang > 0 ? n_qang : 1));
+          for (q = 0; q < 4; ++q) {
+               memcpy(j->sv1 + (size_t) q * n, (*j->save1)[q], sizeof(double) * n);
+               if (n_qang > 0)
+                    for (r = 0; r < n; ++r)
+                         memcpy(j->sv2 + ((size_t) q * n + r) * n_qang, (*j->save2)[q][r],
+                                sizeof(double) * n_qang);
+          }
+     }
+
+     /* user angles (reference misc/rtutil_scat_int.c:487-503,580) */
+     if (j->calc_pf) {
+          double d = 180. / (j->n_angles - 1);
+          j->mu_user = lmieb_arr1(j->n_angles);
+          for (i = 0; i < j->n_angles; ++i) {
+               j->theta[i] = i * d;
+               j->mu_user[i] = cos(j->theta[i] * (M_PI / 180.0));
+          }
+     }
+
+     /* device problem and result staging */
+     memset(&j->P, 0, sizeof(j->P));
+     j->P.n = n; j->P.nd = nd; j->P.nd1 = nd1; j->P.nd2 = nd2;
+     j->P.idx1 = j->idx1; j->P.idx2 = j->idx2;
+     j->P.lambda = j->lambda; j->P.mr = j->mr; j->P.mi = j->mi;
+     j->P.lambda_l = j->lambda_l; j->P.mr_l = j->mr_l; j->P.mi_l = j->mi_l;
+     j->P.x = j->x; j->P.xl = j->xl; j->P.w = j->w; j->P.n1r = j->n1r; j->P.n2r = j->n2r;
+     j->P.n1 = n1; j->P.n_qang = n_qang; j->P.n_coef = j->n_coef_all;
+     j->P.want_gc = j->gc != NULL; j->P.want_lc = j->lc != NULL;
+     j->P.pf_from = j->calc_pf ? (j->calc_gc ? 1 : 2) : 0;
+     j->P.n_angles = j->calc_pf ? j->n_angles : 0;
+     j->P.mu_user = j->mu_user;
+     j->P.accuracy = j->accuracy;
+     j->P.save_control = j->save_control;
+     if (j->save_control == 2) {
+          j->P.save1_in = j->sv1;
+          j->P.save2_in = j->sv2;
+          j->P.w2 = j->w2;
+     }
+     ncol = 1 + nd;
+     n_out = (size_t) ncol * 4 + (j->P.want_gc ? (size_t) ncol * 6 * j->n_coef_all : 0) +
+             (j->P.want_lc ? (size_t) ncol * 6 * j->n_coef_all : 0) + (size_t) ncol * 6 * j->P.n_angles;
+     j->dev_out = lmieb_arr1(n_out);
+     memset(&j->R, 0, sizeof(j->R));
+     j->R.scal = j->dev_out;
+     j->R.gc = j->P.want_gc ? j->R.scal + ncol * 4 : NULL;
+     j->R.lc = j->P.want_lc ? j->R.scal + ncol * 4 + (j->P.want_gc ? (size_t) ncol * 6 * j->n_coef_all : 0)
+                            : NULL;
+     j->R.pf = j->P.n_angles > 0 ? j->dev_out + n_out - (size_t) ncol * 6 * j->P.n_angles : NULL;
+     if (j->save_control == 1) {
+          j->R.save1 = (*j->save1)[0];
+          j->R.save2 = (*j->save2)[0][0];
+     }
+     if (j->verbose)
+          fprintf(stderr, "lmie_b200: n_radii = %d, n1 = %d, n_qang = %d, n_derivs = %d (%d Mie, %d shape)\n",
+                  n, n1, n_qang, nd, nd1, nd2);
+     return 0;
+}
+
+/* Copies a solved case's results into the caller's arrays. */
+static void job_finish(case_job *j) {
+     int nd = j->nd, ncol = 1 + nd, nc = j->n_coef_all, k, e;
+     const double *scal = j->R.scal;
+     *j->cext = scal[0];
+     *j->csca = scal[1];
+     *j->cbak = scal[2];
+     *j->g = scal[3];
+     for (k = 0; k < nd; ++k) {
+          j->cext_l[k] = scal[(1 + k) * 4 + 0];
+          j->csca_l[k] = scal[(1 + k) * 4 + 1];
+          j->cbak_l[k] = scal[(1 + k) * 4 + 2];
+          j->g_l[k] = scal[(1 + k) * 4 + 3];
+     }
+     if (j->gc) {
+          for (e = 0; e < 6; ++e)
+               memcpy(j->gc[e], j->R.gc + (size_t) e * nc, sizeof(double) * nc);
+          for (k = 0; k < nd; ++k)
+               for (e = 0; e < 6; ++e)
+                    memcpy(j->gc_l[k][e], j->R.gc + ((size_t) (1 + k) * 6 + e) * nc, sizeof(double) * nc);
+     }
+     if (j->lc) {
+          for (e = 0; e < 6; ++e)
+               memcpy(j->lc[e], j->R.lc + (size_t) e * nc, sizeof(double) * nc);
+          for (k = 0; k < nd; ++k)
+               for (e = 0; e < 6; ++e)
+                    memcpy(j->lc_l[k][e], j->R.lc + ((size_t) (1 + k) * 6 + e) * nc, sizeof(double) * nc);
+     }
+     if (j->calc_pf) {
+          int na = j->n_angles;
+          for (e = 0; e < 6; ++e)
+               memcpy(j->pf[e], j->R.pf + (size_t) e * na, sizeof(double) * na);
+          for (k = 0; k < nd; ++k)
+               for (e = 0; e < 6; ++e)
+                    memcpy(j->pf_l[k][e], j->R.pf + ((size_t) (1 + k) * 6 + e) * na, sizeof(double) * na);
+     }
+     *j->n_coef = j->R.n_coef_out;
+     (void) ncol;
 }
 
 int lmie_solution2_l(int calc_gc, int calc_lc, int calc_pf,
@@ -331,259 +599,190 @@ int lmie_solution2_l(int calc_gc, int calc_lc, int calc_pf,
                      double ***gc_l, double ***lc_l, double ***pf_l,
                      double ***save1, double ****save2,
                      int verbose, int n_threads, int use_mpi) {
-     int n, nd = n_derivs > 0 ? n_derivs : 0, nd1 = 0, nd2 = 0, i, k, e;
-     int n1, n_qang, n_coef_all, ncol;
-     double x2;
-     double complex m, z2;
-     call_scratch s;
-     lmieb_dist_in din;
-     lmieb_dist_out dout;
-     lmieb_moments_out mom;
-     lmieb_problem P;
-     lmieb_result R;
-     double *scal, *dgc, *dlc, *dpf;
-     size_t n_out;
+     case_job j;
+     int rc;
      (void) n_threads;
      (void) use_mpi;
-
-     memset(&s, 0, sizeof(s));
-
-     /* input check (reference src/lmie_interface.c:404-408) */
-     if (calc_pf && (!calc_gc && !calc_lc)) {
-          fprintf(stderr, "ERROR: either calc_gc or calc_lc must be set to true when "
-                  "calc_pf is true\n");
-          return -1;
+     memset(&j, 0, sizeof(j));
+     j.calc_gc = calc_gc; j.calc_lc = calc_lc; j.calc_pf = calc_pf; j.dist_type = dist_type;
+     j.n_int1 = n_int1; j.n_int2 = n_int2; j.n_quad = n_quad; j.n_angles = n_angles;
+     j.n_derivs = n_derivs; j.save_control = save_control;
+     j.lambda = lambda; j.mr = mr; j.mi = mi; j.a1 = a1; j.a2 = a2; j.a3 = a3; j.a4 = a4; j.a5 = a5;
+     j.r1 = r1; j.r2 = r2; j.accuracy = accuracy;
+     j.lambda_l = lambda_l; j.mr_l = mr_l; j.mi_l = mi_l; j.a1_l = a1_l; j.a2_l = a2_l;
+     j.a3_l = a3_l; j.a4_l = a4_l; j.a5_l = a5_l; j.r1_l = r1_l; j.r2_l = r2_l;
+     j.verbose = verbose;
+     j.n_coef = n_coef; j.r21 = r21; j.r22 = r22; j.norm = norm; j.reff = reff; j.veff = veff;
+     j.gavg = gavg; j.vavg = vavg; j.ravg = ravg; j.rvw = rvw;
+     j.cext = cext; j.csca = csca; j.cbak = cbak; j.g = g;
+     j.gc = gc; j.lc = lc; j.theta = theta; j.pf = pf;
+     j.r21_l = r21_l; j.r22_l = r22_l; j.norm_l = norm_l; j.reff_l = reff_l; j.veff_l = veff_l;
+     j.gavg_l = gavg_l; j.vavg_l = vavg_l; j.ravg_l = ravg_l; j.rvw_l = rvw_l;
+     j.cext_l = cext_l; j.csca_l = csca_l; j.cbak_l = cbak_l; j.g_l = g_l;
+     j.gc_l = gc_l; j.lc_l = lc_l; j.pf_l = pf_l;
+     j.save1 = save1; j.save2 = save2;
+     rc = job_prepare(&j);
+     if (rc == 0 && lmieb_device_solve(&j.P, &j.R)) {
+          fprintf(stderr, "ERROR: lmie_core_solution()\n");
+          rc = -1;
      }
-     if (save_control < 0 || save_control > 2) {
-          fprintf(stderr, "ERROR: invalid save_control: %d\n", save_control);
-          return -1;
-     }
-     if (calc_pf && n_angles < 1) {
-          fprintf(stderr, "ERROR: n_angles must be >= 1 when calc_pf is true\n");
-          return -1;
-     }
+     if (rc == 0)
+          job_finish(&j);
+     job_free(&j);
+     return rc;
+}
 
-     n = lmieb_dist_count(dist_type, n_int1, n_int2, n_quad);
-     if (n <= 0) {
-          if (n == 0)
-               fprintf(stderr, "ERROR: size distribution has no quadrature points\n");
-          return -1;
+/* ---- batches -------------------------------------------------------------- */
+
+static void job_from_struct(case_job *j, lmie_in_data *in, lmie_out_data *out, int verbose) {
+     memset(j, 0, sizeof(*j));
+     j->calc_gc = in->calc_gc; j->calc_lc = in->calc_lc; j->calc_pf = in->calc_pf;
+     j->dist_type = in->dist_type; j->n_int1 = in->n_int1; j->n_int2 = in->n_int2;
+     j->n_quad = in->n_quad; j->n_angles = in->n_angles; j->n_derivs = in->n_derivs;
+     j->save_control = in->save_control;
+     j->lambda = in->lambda; j->mr = in->mr; j->mi = in->mi;
+     j->a1 = in->a1; j->a2 = in->a2; j->a3 = in->a3; j->a4 = in->a4; j->a5 = in->a5;
+     j->r1 = in->r1; j->r2 = in->r2; j->accuracy = in->accuracy;
+     j->lambda_l = in->lambda_l; j->mr_l = in->mr_l; j->mi_l = in->mi_l; j->a1_l = in->a1_l;
+     j->a2_l = in->a2_l; j->a3_l = in->a3_l; j->a4_l = in->a4_l; j->a5_l = in->a5_l;
+     j->r1_l = in->r1_l; j->r2_l = in->r2_l;
+     j->verbose = verbose;
+     j->n_coef = &out->n_coef; j->r21 = &out->r1; j->r22 = &out->r2; j->norm = &out->norm;
+     j->reff = &out->reff; j->veff = &out->veff; j->gavg = &out->gavg; j->vavg = &out->vavg;
+     j->ravg = &out->ravg; j->rvw = &out->rvw; j->cext = &out->cext; j->csca = &out->csca;
+     j->cbak = &out->cbak; j->g = &out->g;
+     j->gc = out->gc; j->lc = out->lc; j->theta = out->theta; j->pf = out->pf;
+     j->r21_l = out->r1_l; j->r22_l = out->r2_l; j->norm_l = out->norm_l; j->reff_l = out->reff_l;
+     j->veff_l = out->veff_l; j->gavg_l = out->gavg_l; j->vavg_l = out->vavg_l;
+     j->ravg_l = out->ravg_l; j->rvw_l = out->rvw_l; j->cext_l = out->cext_l;
+     j->csca_l = out->csca_l; j->cbak_l = out->cbak_l; j->g_l = out->g_l;
+     j->gc_l = out->gc_l; j->lc_l = out->lc_l; j->pf_l = out->pf_l;
+     j->save1 = &out->save1; j->save2 = &out->save2;
+}
+
+typedef struct {
+     case_job *jobs;
+     int n, next, stage;
+     pthread_mutex_t mu;
+} job_pool;
+
+static void *job_worker(void *arg) {
+     job_pool *p = (job_pool *) arg;
+     for (;;) {
+          int i;
+          pthread_mutex_lock(&p->mu);
+          i = p->next++;
+          pthread_mutex_unlock(&p->mu);
+          if (i >= p->n)
+               break;
+          if (p->stage == 0)
+               p->jobs[i].rc = job_prepare(&p->jobs[i]);
+          else if (p->jobs[i].rc == 0)
+               job_finish(&p->jobs[i]);
      }
+     return NULL;
+}
 
-     /* ---- size distribution quadrature and moments ---- */
-     s.qx = lmieb_arr1(n);
-     s.qw = lmieb_arr1(n);
-     s.nr = lmieb_arr1(n);
-     s.qx_l = lmieb_arr1((size_t) n * nd);
-     s.qw_l = lmieb_arr1((size_t) n * nd);
-     s.nr_l = lmieb_arr1((size_t) n * nd);
-     memset(&din, 0, sizeof(din));
-     din.dist_type = dist_type; din.n_int1 = n_int1; din.n_int2 = n_int2; din.n_quad = n_quad;
-     din.nd = nd;
-     din.a1 = a1; din.a2 = a2; din.a3 = a3; din.a4 = a4; din.a5 = a5; din.r1 = r1; din.r2 = r2;
-     din.a1_l = a1_l; din.a2_l = a2_l; din.a3_l = a3_l; din.a4_l = a4_l; din.a5_l = a5_l;
-     din.r1_l = r1_l; din.r2_l = r2_l;
-     dout.qx = s.qx; dout.qw = s.qw; dout.nr = s.nr;
-     dout.qx_l = s.qx_l; dout.qw_l = s.qw_l; dout.nr_l = s.nr_l;
-     dout.r1_l = r21_l; dout.r2_l = r22_l; dout.norm_l = norm_l;
-     if (lmieb_particle_dist(&din, &dout) < 0) {
-          fprintf(stderr, "ERROR: get_particle_dist()\n");
-          scratch_free(&s);
-          return -1;
-     }
-     *r21 = dout.r1;
-     *r22 = dout.r2;
-     *norm = dout.norm;
-     mom.reff_l = reff_l; mom.veff_l = veff_l; mom.gavg_l = gavg_l;
-     mom.vavg_l = vavg_l; mom.ravg_l = ravg_l; mom.rvw_l = rvw_l;
-     lmieb_moments(n, nd, s.qx, s.qw, s.nr, s.qx_l, s.qw_l, s.nr_l, &mom);
-     *reff = mom.reff; *veff = mom.veff; *gavg = mom.gavg;
-     *vavg = mom.vavg; *ravg = mom.ravg; *rvw = mom.rvw;
+/* Runs stage 0 (prepare) or 1 (finish) of every job on up to n_threads host
+ * threads. */
+static void run_jobs(case_job *jobs, int n, int stage, int n_threads) {
+     job_pool p;
+     int t, nt = n_threads > 0 ? n_threads : 1;
+     pthread_t th[64];
+     if (nt > 64)
+          nt = 64;
+     if (nt > n)
+          nt = n;
+     p.jobs = jobs; p.n = n; p.next = 0; p.stage = stage;
+     pthread_mutex_init(&p.mu, NULL);
+     for (t = 1; t < nt; ++t)
+          if (pthread_create(&th[t], NULL, job_worker, &p) != 0)
+               break;
+     nt = t;
+     job_worker(&p);
+     for (t = 1; t < nt; ++t)
+          pthread_join(th[t], NULL);
+     pthread_mutex_destroy(&p.mu);
+}
 
-     /* ---- derivative split (reference src/lmie_interface.c:304-353) ---- */
-     s.idx1 = (int *) calloc(nd > 0 ? nd : 1, sizeof(int));
-     s.idx2 = (int *) calloc(nd > 0 ? nd : 1, sizeof(int));
-     for (i = 0; i < nd; ++i) {
-          if (lambda_l[i] != 0. || mr_l[i] != 0. || mi_l[i] != 0. ||
-              r21_l[i] != 0. || r22_l[i] != 0.)
-               s.idx1[nd1++] = i;
-          else
-               s.idx2[nd2++] = i;
-     }
+/* Two prepared cases can share a device batch when their derivative layout
+ * and requested outputs agree. */
+static int jobs_compatible(const case_job *a, const case_job *b) {
+     int q;
+     if (a->P.save_control != 0 || b->P.save_control != 0)
+          return 0;
+     if (a->P.nd != b->P.nd || a->P.nd1 != b->P.nd1 || a->P.nd2 != b->P.nd2 ||
+         a->P.want_gc != b->P.want_gc || a->P.want_lc != b->P.want_lc || a->P.pf_from != b->P.pf_from)
+          return 0;
+     for (q = 0; q < a->P.nd1; ++q)
+          if (a->P.idx1[q] != b->P.idx1[q])
+               return 0;
+     for (q = 0; q < a->P.nd2; ++q)
+          if (a->P.idx2[q] != b->P.idx2[q])
+               return 0;
+     return 1;
+}
 
-     /* ---- global truncation (reference src/lmie_schedule.c:1004-1017) ---- */
-     m = mr - I * mi;
-     x2 = 2. * M_PI * *r22 / lambda;
-     z2 = m * x2;
-     n1 = lmieb_calc_n1(x2);
-     (void) z2;
-     n_qang = (!gc && !lc) ? 0 : 2 * n1;
-     n_coef_all = 2 * n1;
-
-     /* ---- per-radius size parameters, truncation and weights
-      *      (reference src/lmie_core.c:263-292) ---- */
-     s.x = lmieb_arr1(n);
-     s.xl = lmieb_arr1((size_t) n * (nd1 > 0 ? nd1 : 1));
-     s.w = lmieb_arr1((size_t) n * (1 + nd));
-     s.n1r = (int *) calloc(n, sizeof(int));
-     s.n2r = (int *) calloc(n, sizeof(int));
-     for (i = 0; i < n; ++i) {
-          double x = 2. * M_PI * s.qx[i] / lambda;
-          double complex z = m * x;
-          s.x[i] = x;
-          s.n1r[i] = lmieb_calc_n1(x);
-          s.n2r[i] = lmieb_calc_n2(s.n1r[i], creal(z), cimag(z));
-          s.w[i] = s.nr[i] * s.qw[i];
-          for (k = 0; k < nd1; ++k) {
-               int kk = s.idx1[k];
-               s.xl[(size_t) k * n + i] = 2. * M_PI * (s.qx_l[(size_t) i * nd + kk] -
-                                        s.qx[i] * lambda_l[kk] / lambda) / lambda;
-               s.w[(size_t) (1 + kk) * n + i] = s.nr_l[(size_t) i * nd + kk] * s.qw[i] +
-                                                s.nr[i] * s.qw_l[(size_t) i * nd + kk];
+int lmie_solution_batch(int n_cases, lmie_in_data *in, lmie_out_data *out, int alloc_out,
+                        int verbose, int n_threads) {
+     case_job *jobs;
+     lmieb_problem *P;
+     lmieb_result *R;
+     int *done, i, k, rc = 0;
+     if (n_cases <= 0)
+          return 0;
+     if (alloc_out) {
+          for (i = 0; i < n_cases; ++i) {
+               int max_coef = lmie_calc_max_coef(in[i].lambda, in[i].dist_type, in[i].a1, in[i].a2,
+                                                 in[i].a3, in[i].r1, in[i].r2);
+               if (lmie_out_alloc(&in[i], &out[i], max_coef)) {
+                    fprintf(stderr, "ERROR: lmie_out_alloc()\n");
+                    return -1;
+               }
           }
-          for (k = 0; k < nd2; ++k) {
-               int kk = s.idx2[k];
-               s.w[(size_t) (1 + kk) * n + i] = s.nr_l[(size_t) i * nd + kk] * s.qw[i];
+     }
+     jobs = (case_job *) calloc(n_cases, sizeof(case_job));
+     P = (lmieb_problem *) calloc(n_cases, sizeof(lmieb_problem));
+     R = (lmieb_result *) calloc(n_cases, sizeof(lmieb_result));
+     done = (int *) calloc(n_cases, sizeof(int));
+     for (i = 0; i < n_cases; ++i)
+          job_from_struct(&jobs[i], &in[i], &out[i], verbose);
+     run_jobs(jobs, n_cases, 0, n_threads);
+     for (i = 0; i < n_cases; ++i)
+          if (jobs[i].rc) {
+               fprintf(stderr, "ERROR: lmie_solution_batch(): case %d\n", i);
+               rc = -1;
           }
-     }
-     if (n1 < 1 || s.n1r[n - 1] < 1) {
-          fprintf(stderr, "ERROR: invalid size parameter (lambda = %g, r2 = %g)\n", lambda, *r22);
-          scratch_free(&s);
-          return -1;
-     }
-     for (i = 0; i < n; ++i) {
-          if (s.n1r[i] > n1) {
-               fprintf(stderr, "ERROR: radius %d (r = %g) lies above r2 = %g\n", i, s.qx[i], *r22);
-               scratch_free(&s);
-               return -1;
+     /* device batches of compatible cases, in input order */
+     for (i = 0; rc == 0 && i < n_cases; ++i) {
+          int m = 0;
+          if (done[i])
+               continue;
+          for (k = i; k < n_cases; ++k) {
+               if (done[k] || (k != i && !jobs_compatible(&jobs[i], &jobs[k])))
+                    continue;
+               P[m] = jobs[k].P;
+               R[m] = jobs[k].R;
+               done[k] = m + 1;
+               ++m;
+               if (jobs[i].P.save_control != 0)
+                    break;
           }
-     }
-
-     /* ---- save_control: allocate / gather the per-radius kernels ---- */
-     if (save_control == 1) {
-          *save1 = lmieb_arr2(4, n);
-          *save2 = lmieb_arr3(4, n, n_qang > 0 ? n_qang : 1);
-     }
-     if (save_control == 2) {
-          s.w2 = lmieb_arr1((size_t) n * (nd > 0 ? nd : 1));
-          for (i = 0; i < n; ++i)
-               for (k = 0; k < nd2; ++k) {
-                    int kk = s.idx2[k];
-                    s.w2[(size_t) kk * n + i] = s.nr_l[(size_t) i * nd + kk] * s.qw[i] +
-                                                s.nr[i] * s.qw_l[(size_t) i * nd + kk];
+          if (lmieb_device_solve_batch(m, P, R)) {
+               fprintf(stderr, "ERROR: lmie_solution_batch(): device solve\n");
+               rc = -1;
+               break;
+          }
+          for (k = i; k < n_cases; ++k)
+               if (done[k] > 0) {
+                    jobs[k].R = R[done[k] - 1];
+                    done[k] = -1;
                }
      }
-
-     /* ---- user angles (reference misc/rtutil_scat_int.c:487-503,580) ---- */
-     if (calc_pf) {
-          double d = 180. / (n_angles - 1);
-          s.mu_user = lmieb_arr1(n_angles);
-          for (i = 0; i < n_angles; ++i) {
-               theta[i] = i * d;
-               s.mu_user[i] = cos(theta[i] * (M_PI / 180.0));
-          }
-     }
-
-     /* ---- device solve ---- */
-     memset(&P, 0, sizeof(P));
-     P.n = n; P.nd = nd; P.nd1 = nd1; P.nd2 = nd2; P.idx1 = s.idx1; P.idx2 = s.idx2;
-     P.lambda = lambda; P.mr = mr; P.mi = mi;
-     P.lambda_l = lambda_l; P.mr_l = mr_l; P.mi_l = mi_l;
-     P.x = s.x; P.xl = s.xl; P.w = s.w; P.n1r = s.n1r; P.n2r = s.n2r;
-     P.n1 = n1; P.n_qang = n_qang; P.n_coef = n_coef_all;
-     P.want_gc = gc != NULL; P.want_lc = lc != NULL;
-     P.pf_from = calc_pf ? (calc_gc ? 1 : 2) : 0;
-     P.n_angles = calc_pf ? n_angles : 0;
-     P.mu_user = s.mu_user;
-     P.accuracy = accuracy;
-     P.save_control = save_control;
-     if (save_control == 2) {
-          /* gather the caller's kernels through their row pointers */
-          int q, r;
-          if (!save1 || !*save1 || (n_qang > 0 && (!save2 || !*save2))) {
-               fprintf(stderr, "ERROR: save_control = 2 needs save1 and save2 from a "
-                       "save_control = 1 call\n");
-               scratch_free(&s);
-               return -1;
-          }
-          s.sv1 = lmieb_arr1((size_t) 4 * n);
-          s.sv2 = lmieb_arr1((size_t) 4 * n * (n_qang > 0 ? n_qang : 1));
-          for (q = 0; q < 4; ++q) {
-               memcpy(s.sv1 + (size_t) q * n, (*save1)[q], sizeof(double) * n);
-               if (n_qang > 0)
-                    for (r = 0; r < n; ++r)
-                         memcpy(s.sv2 + ((size_t) q * n + r) * n_qang, (*save2)[q][r],
-                                sizeof(double) * n_qang);
-          }
-          P.save1_in = s.sv1;
-          P.save2_in = s.sv2;
-          P.w2 = s.w2;
-     }
-
-     ncol = 1 + nd;
-     n_out = (size_t) ncol * 4 + (P.want_gc ? (size_t) ncol * 6 * n_coef_all : 0) +
-             (P.want_lc ? (size_t) ncol * 6 * n_coef_all : 0) +
-             (size_t) ncol * 6 * P.n_angles;
-     s.dev_out = lmieb_arr1(n_out);
-     scal = s.dev_out;
-     dgc = scal + ncol * 4;
-     dlc = dgc + (P.want_gc ? (size_t) ncol * 6 * n_coef_all : 0);
-     dpf = dlc + (P.want_lc ? (size_t) ncol * 6 * n_coef_all : 0);
-     memset(&R, 0, sizeof(R));
-     R.scal = scal;
-     R.gc = P.want_gc ? dgc : NULL;
-     R.lc = P.want_lc ? dlc : NULL;
-     R.pf = P.n_angles > 0 ? dpf : NULL;
-     if (save_control == 1) {
-          R.save1 = (*save1)[0];
-          R.save2 = (*save2)[0][0];
-     }
-     if (verbose)
-          fprintf(stderr, "lmie_b200: n_radii = %d, n1 = %d, n_qang = %d, n_derivs = %d (%d Mie, %d shape)\n",
-                  n, n1, n_qang, nd, nd1, nd2);
-     if (lmieb_device_solve(&P, &R)) {
-          fprintf(stderr, "ERROR: lmie_core_solution()\n");
-          scratch_free(&s);
-          return -1;
-     }
-
-     /* ---- scatter into the caller's arrays ---- */
-     *cext = scal[0];
-     *csca = scal[1];
-     *cbak = scal[2];
-     *g = scal[3];
-     for (k = 0; k < nd; ++k) {
-          cext_l[k] = scal[(1 + k) * 4 + 0];
-          csca_l[k] = scal[(1 + k) * 4 + 1];
-          cbak_l[k] = scal[(1 + k) * 4 + 2];
-          g_l[k] = scal[(1 + k) * 4 + 3];
-     }
-     if (gc) {
-          for (e = 0; e < 6; ++e)
-               memcpy(gc[e], dgc + (size_t) e * n_coef_all, sizeof(double) * n_coef_all);
-          for (k = 0; k < nd; ++k)
-               for (e = 0; e < 6; ++e)
-                    memcpy(gc_l[k][e], dgc + ((size_t) (1 + k) * 6 + e) * n_coef_all,
-                           sizeof(double) * n_coef_all);
-     }
-     if (lc) {
-          for (e = 0; e < 6; ++e)
-               memcpy(lc[e], dlc + (size_t) e * n_coef_all, sizeof(double) * n_coef_all);
-          for (k = 0; k < nd; ++k)
-               for (e = 0; e < 6; ++e)
-                    memcpy(lc_l[k][e], dlc + ((size_t) (1 + k) * 6 + e) * n_coef_all,
-                           sizeof(double) * n_coef_all);
-     }
-     if (calc_pf) {
-          for (e = 0; e < 6; ++e)
-               memcpy(pf[e], dpf + (size_t) e * n_angles, sizeof(double) * n_angles);
-          for (k = 0; k < nd; ++k)
-               for (e = 0; e < 6; ++e)
-                    memcpy(pf_l[k][e], dpf + ((size_t) (1 + k) * 6 + e) * n_angles,
-                           sizeof(double) * n_angles);
-     }
-     *n_coef = R.n_coef_out;
-
-     scratch_free(&s);
-     return 0;
+     if (rc == 0)
+          run_jobs(jobs, n_cases, 1, n_threads);
+     for (i = 0; i < n_cases; ++i)
+          job_free(&jobs[i]);
+     free(jobs); free(P); free(R); free(done);
+     return rc;
 }

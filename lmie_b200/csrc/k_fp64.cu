@@ -1,4 +1,5 @@
-// k_fp64.cu -- the FP64 kernels of the drop-in solve (sm_100a).
+// k_fp64.cu -- the FP64 kernels of the polydisperse solve (sm_100a), over a
+// batch of independent cases (one lmie_solution() is a batch of one).
 //
 //   k_gauss          Gauss-Legendre angles on [-1,1]        <- misc/rtutil_math.c:73-129,231-316
 //   k_recur<NC>      per-radius sequential recurrences (D_n, psi, chi)
@@ -12,9 +13,10 @@
 //                    quadratic forms, reduced over a radius group
 //                                                           <- src/lmie_core.c:658-791
 //   k_reduce_pf      fixed-order sum over radius groups
-//   k_normalize      2/Csca and lambda^2/2pi normalisation   <- src/lmie_schedule.c:1155-1199
-//   k_gsf_* / k_leg_* expansion coefficients over Gauss angles
-//                                                           <- misc/rtutil_scat_int.c:20-230,353-480,
+//   k_normalize_*    2/Csca and lambda^2/2pi normalisation   <- src/lmie_schedule.c:1155-1199
+//   k_exp_*          expansion coefficients over Gauss angles as a contraction
+//                    over (order tile x angle tile), basis functions generated
+//                    per tile from recurrence checkpoints  <- misc/rtutil_scat_int.c:20-230,353-480,
 //                                                              misc/rtutil_math.c:477-513,936-1017
 //   k_phase_user     phase matrix at the user's angles       <- misc/rtutil_scat_int.c:510-589,662-710
 //
@@ -25,6 +27,17 @@
 
 namespace {
 
+// case c with start[c] <= e < start[c + 1]
+__device__ __forceinline__ int find_case(const long long *__restrict__ start, int ncase, long long e) {
+    int lo = 0, hi = ncase - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (start[mid] <= e) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
 // ---------------------------------------------------------------------------
 // Gauss-Legendre nodes: one thread per root pair, Newton with the
 // second-order correction of Davis & Rabinowitz.  The initial guesses come
@@ -33,14 +46,16 @@ namespace {
 // reference's to the last bit -- at size parameters ~1000 the phase matrix
 // changes by ~1e-10 per ulp of a node.
 // ---------------------------------------------------------------------------
-__global__ void k_gauss(int n, const double *__restrict__ guess, const double *__restrict__ jr,
-                        double *mu, double *wq) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    int half = (n + 1) / 2;
-    if (i >= half) return;
+__global__ void k_gauss(int npairs, const int *__restrict__ pt, const int *__restrict__ pi,
+                        const int *__restrict__ ns, const long long *__restrict__ mo,
+                        const long long *__restrict__ go, const double *__restrict__ guess,
+                        const double *__restrict__ jr, double *mu, double *wq) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npairs) return;
+    const int t = pt[p], i = pi[p], n = ns[t];
     const double dn = (double) n;
     const double ib = (double) (n * (n + 1));
-    double y = guess[i], y_prev, pn, pm, pmm, t, d1, d2;
+    double y = guess[go[t] + i], y_prev, pn, pm, pmm, u, d1, d2;
     int it = 0;
     do {
         pm = 0.;
@@ -48,22 +63,23 @@ __global__ void k_gauss(int n, const double *__restrict__ guess, const double *_
         for (int j = 0; j < n; ++j) {
             pmm = pm;
             pm = pn;
-            t = __dmul_rn(y, pm);
-            pn = __dadd_rn(__dmul_rn(jr[j], __dsub_rn(t, pmm)), t);   // jr[j] = j / (j + 1.)
+            u = __dmul_rn(y, pm);
+            pn = __dadd_rn(__dmul_rn(jr[j], __dsub_rn(u, pmm)), u);   // jr[j] = j / (j + 1.)
         }
-        t = __dsub_rn(1., __dmul_rn(y, y));
-        d1 = __ddiv_rn(__dmul_rn(dn, __dsub_rn(pm, __dmul_rn(y, pn))), t);
-        d2 = __ddiv_rn(__dsub_rn(__dmul_rn(__dmul_rn(2., y), d1), __dmul_rn(ib, pn)), t);
+        u = __dsub_rn(1., __dmul_rn(y, y));
+        d1 = __ddiv_rn(__dmul_rn(dn, __dsub_rn(pm, __dmul_rn(y, pn))), u);
+        d2 = __ddiv_rn(__dsub_rn(__dmul_rn(__dmul_rn(2., y), d1), __dmul_rn(ib, pn)), u);
         y_prev = y;
-        t = __ddiv_rn(pn, d1);
-        y = __dsub_rn(y_prev, __dmul_rn(t, __dadd_rn(1., __ddiv_rn(__dmul_rn(t, d2), __dmul_rn(2., d1)))));
+        u = __ddiv_rn(pn, d1);
+        y = __dsub_rn(y_prev, __dmul_rn(u, __dadd_rn(1., __ddiv_rn(__dmul_rn(u, d2), __dmul_rn(2., d1)))));
     } while (fabs(__dsub_rn(y, y_prev)) > 2.220446049250313e-16 && ++it < 100);
     double de = __dmul_rn(dn, pm);
     de = __ddiv_rn(2., __dmul_rn(de, de));
-    mu[i] = -y;
-    mu[n - 1 - i] = y;
-    wq[i] = __dmul_rn(__dsub_rn(1., __dmul_rn(y, y)), de);
-    wq[n - 1 - i] = wq[i];
+    double *m = mu + mo[t], *w = m + n;   // pool entry: n nodes then n weights
+    m[i] = -y;
+    m[n - 1 - i] = y;
+    w[i] = __dmul_rn(__dsub_rn(1., __dmul_rn(y, y)), de);
+    w[n - 1 - i] = w[i];
 }
 
 // ---------------------------------------------------------------------------
@@ -75,28 +91,28 @@ __global__ void k_gauss(int n, const double *__restrict__ guess, const double *_
 // it coalesced.
 // ---------------------------------------------------------------------------
 template <int NC>
-__global__ void __launch_bounds__(64) k_recur(DevProblem P, int c0, int write_value,
-                                             double4 *__restrict__ rec) {
+__global__ void __launch_bounds__(64) k_recur(DevBatch B, int c0, int write_value, double4 *__restrict__ rec) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= P.n) return;
-    const int n = P.n;
-    const int n1 = P.n1r[r], n2 = P.n2r[r];
-    const double x = P.x[r];
+    if (r >= B.R) return;
+    const int R = B.R;
+    const DevCase &C = B.cs[B.rcase[r]];
+    const int n1 = B.n1r[r], n2 = B.n2r[r];
+    const double x = B.x[r];
     const double xinv = 1. / x;
-    const cplx m = P.m;
+    const cplx m = C.m;
     const cplx z = mk(m.re * x, m.im * x);
     const cplx zinv = cinv(z);
-    const size_t totp = (size_t) P.totp;
-    const size_t base = (size_t) P.offp[r];
+    const size_t totp = (size_t) B.totp;
+    const size_t base = (size_t) B.offp[r];
     double4 *R0 = rec + base;                         // value column
 
     double xl[NC > 0 ? NC : 1];
     cplx zl[NC > 0 ? NC : 1];
 #pragma unroll
     for (int k = 0; k < NC; ++k) {
-        const int kk = P.idx1[c0 + k];
-        xl[k] = P.xl[(size_t) (c0 + k) * n + r];
-        zl[k] = P.m_l[kk] * x + m * xl[k];
+        const int kk = B.idx1[c0 + k];
+        xl[k] = B.xl[(size_t) (c0 + k) * R + r];
+        zl[k] = B.m_l[C.ml_off + kk] * x + m * xl[k];
     }
 #define RC(k) (rec + (size_t) (1 + c0 + (k)) * totp + base)
 
@@ -235,27 +251,28 @@ __global__ void __launch_bounds__(64) k_recur(DevProblem P, int c0, int write_va
 constexpr int ABT = 128;
 
 template <int NC>
-__global__ void __launch_bounds__(ABT) k_abcoef(DevProblem P, int c0, int write_value,
+__global__ void __launch_bounds__(ABT) k_abcoef(DevBatch B, int c0, int write_value,
                                                 const int2 *__restrict__ tiles,
                                                 const double4 *__restrict__ rec,
                                                 double *__restrict__ coef, double *__restrict__ rsp) {
-    constexpr int C = 1 + NC;
-    __shared__ cplx sab[2 * C][ABT];
-    __shared__ double red[5 * C][ABT / 32];
+    constexpr int CC = 1 + NC;
+    __shared__ cplx sab[2 * CC][ABT];
+    __shared__ double red[5 * CC][ABT / 32];
     const int t = threadIdx.x;
     const int2 tile = tiles[blockIdx.x];
     const int r = tile.x, j0 = tile.y;
-    const int n1 = P.n1r[r];
+    const DevCase &C = B.cs[B.rcase[r]];
+    const int n1 = B.n1r[r];
     const int j = j0 + t;
     const bool valid = j <= n1;
     const bool owned = valid && t < ABT - 1;
-    const int n = P.n;
-    const double x = P.x[r];
+    const int R = B.R;
+    const double x = B.x[r];
     const double xinv = 1. / x;
-    const cplx m = P.m, minv = P.minv;
-    const size_t totp = (size_t) P.totp, tot = (size_t) P.tot;
-    const size_t base = (size_t) P.offp[r];
-    const double *fv1 = P.fv, *fv3 = P.fv + 2 * (P.n1 + 2), *fv4 = P.fv + 3 * (P.n1 + 2);
+    const cplx m = C.m, minv = C.minv;
+    const size_t totp = (size_t) B.totp, tot = (size_t) B.tot;
+    const size_t base = (size_t) B.offp[r];
+    const double *fv1 = B.fv, *fv3 = B.fv + 2 * (B.n1max + 2), *fv4 = B.fv + 3 * (B.n1max + 2);
 
     cplx a = mk(0., 0.), b = mk(0., 0.), al[NC > 0 ? NC : 1], bl[NC > 0 ? NC : 1];
     if (valid) {
@@ -282,8 +299,8 @@ __global__ void __launch_bounds__(ABT) k_abcoef(DevProblem P, int c0, int write_
                 const cplx Dl = mk(w.z, w.w);
                 const cplx zetal = mk(w.x, w.y), zetal_p = mk(wp.x, wp.y);
                 const double psil = w.x, psil_p = wp.x;
-                const double tl = tx * P.xl[(size_t) (c0 + k) * n + r];
-                const cplx ml = P.m_l[P.idx1[c0 + k]];
+                const double tl = tx * B.xl[(size_t) (c0 + k) * R + r];
+                const cplx ml = B.m_l[C.ml_off + B.idx1[c0 + k]];
                 const cplx c6 = Dl * minv - Dm2 * ml + tl;
                 al[k] = (c6 * psi + ca * psil - psil_p) * ida -
                         na * ((c6 * zeta + ca * zetal - zetal_p) * (ida * ida));
@@ -305,9 +322,9 @@ __global__ void __launch_bounds__(ABT) k_abcoef(DevProblem P, int c0, int write_
     }
     __syncthreads();
 
-    double acc[5 * C];
+    double acc[5 * CC];
 #pragma unroll
-    for (int q = 0; q < 5 * C; ++q) acc[q] = 0.;
+    for (int q = 0; q < 5 * CC; ++q) acc[q] = 0.;
     if (owned) {
         const double f1 = fv1[j], f4 = fv4[j];
         const double sgn = (j & 1) ? -1. : 1.;
@@ -325,7 +342,7 @@ __global__ void __launch_bounds__(ABT) k_abcoef(DevProblem P, int c0, int write_
         double2 *cf = (double2 *) coef;
         if (write_value) {
             const cplx cs = (a + b) * f4, cd = (a - b) * f4;
-            const size_t o = ((size_t) P.off[r] + j - 1) * 2;
+            const size_t o = ((size_t) B.off[r] + j - 1) * 2;
             cf[o] = make_double2(cs.re, cs.im);
             cf[o + 1] = make_double2(cd.re, cd.im);
         }
@@ -342,22 +359,22 @@ __global__ void __launch_bounds__(ABT) k_abcoef(DevProblem P, int c0, int write_
                        fv4[j] * (re_mulc(al[k], b) + re_mulc(a, bl[k]));
             }
             const cplx cs = (al[k] + bl[k]) * f4, cd = (al[k] - bl[k]) * f4;
-            const size_t o = (((size_t) (1 + c0 + k)) * tot + (size_t) P.off[r] + j - 1) * 2;
+            const size_t o = (((size_t) (1 + c0 + k)) * tot + (size_t) B.off[r] + j - 1) * 2;
             cf[o] = make_double2(cs.re, cs.im);
             cf[o + 1] = make_double2(cd.re, cd.im);
         }
     }
-    // block reduction of the 5*C tile sums (fixed order)
+    // block reduction of the 5*CC tile sums (fixed order)
 #pragma unroll
-    for (int q = 0; q < 5 * C; ++q) {
+    for (int q = 0; q < 5 * CC; ++q) {
         double v = acc[q];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
         if ((t & 31) == 0) red[q][t >> 5] = v;
     }
     __syncthreads();
-    const int ntiles = P.ntiles;
-    for (int q = t; q < 5 * C; q += ABT) {
+    const int ntiles = B.ntiles;
+    for (int q = t; q < 5 * CC; q += ABT) {
         double v = 0.;
 #pragma unroll
         for (int w = 0; w < ABT / 32; ++w) v += red[q][w];
@@ -368,20 +385,21 @@ __global__ void __launch_bounds__(ABT) k_abcoef(DevProblem P, int c0, int write_
     }
 }
 
-// Sum the tile partials of every radius in tile order: rs[(col*5+q)*n + r].
-__global__ void k_tile_reduce(int n, int ncol, int ntiles, const int *__restrict__ tstart,
+// Sum the tile partials of every radius in tile order: rs[(col*5+q)*R + r].
+__global__ void k_tile_reduce(int R, int ncol, int ntiles, const int *__restrict__ tstart,
                               const double *__restrict__ rsp, double *__restrict__ rs) {
     const size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (size_t) ncol * 5 * n) return;
-    const int r = (int) (i % n);
-    const size_t cq = i / n;
+    if (i >= (size_t) ncol * 5 * R) return;
+    const int r = (int) (i % R);
+    const size_t cq = i / R;
     double v = 0.;
     for (int tt = tstart[r]; tt < tstart[r + 1]; ++tt) v += rsp[cq * ntiles + tt];
-    rs[cq * n + r] = v;
+    rs[cq * R + r] = v;
 }
 
 // ---------------------------------------------------------------------------
-// K2: one block per output column; fixed-order block reduction over radii.
+// K2: one block per (case, output column); fixed-order block reduction over
+// the case's radii.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ double block_sum(double v, double *sh) {
     const int t = threadIdx.x;
@@ -396,25 +414,27 @@ __device__ __forceinline__ double block_sum(double v, double *sh) {
     return r;
 }
 
-__global__ void __launch_bounds__(256) k_reduce_scalars(DevProblem P, const double *__restrict__ rs,
+__global__ void __launch_bounds__(256) k_reduce_scalars(DevBatch B, const double *__restrict__ rs,
                                                         double *__restrict__ sums,
                                                         double *__restrict__ save1) {
     __shared__ double sh[256];
-    const int col = blockIdx.x;           // 0 = value, 1+kk = slot kk
-    const int n = P.n;
+    const int cidx = blockIdx.x;
+    const int col = blockIdx.y;           // 0 = value, 1+kk = slot kk
+    const DevCase &C = B.cs[cidx];
+    const int R = B.R;
     int kind = 0, c1 = 0;                 // 0 value, 1 index1, 2 index2
     if (col > 0) {
         const int kk = col - 1;
-        for (int k = 0; k < P.nd1; ++k)
-            if (P.idx1[k] == kk) { kind = 1; c1 = 1 + k; }
+        for (int k = 0; k < B.nd1; ++k)
+            if (B.idx1[k] == kk) { kind = 1; c1 = 1 + k; }
         if (kind == 0) kind = 2;
     }
     double acc[4] = {0., 0., 0., 0.};
-    for (int r = threadIdx.x; r < n; r += blockDim.x) {
-        const double f = P.w[r];
-        const double se = rs[r], ss = rs[(size_t) n + r];
-        const double sbr = rs[(size_t) 2 * n + r], sbi = rs[(size_t) 3 * n + r];
-        const double sg = rs[(size_t) 4 * n + r];
+    for (int r = C.r0 + threadIdx.x; r < C.r0 + C.nr; r += blockDim.x) {
+        const double f = B.w[r];
+        const double se = rs[r], ss = rs[(size_t) R + r];
+        const double sbr = rs[(size_t) 2 * R + r], sbi = rs[(size_t) 3 * R + r];
+        const double sg = rs[(size_t) 4 * R + r];
         const double bak = sbr * sbr + sbi * sbi;
         if (kind == 0) {
             acc[0] += f * se;
@@ -423,46 +443,46 @@ __global__ void __launch_bounds__(256) k_reduce_scalars(DevProblem P, const doub
             acc[3] += f * sg;
             if (save1) {
                 save1[r] = se;
-                save1[(size_t) n + r] = ss;
-                save1[(size_t) 2 * n + r] = bak;
-                save1[(size_t) 3 * n + r] = sg;
+                save1[(size_t) R + r] = ss;
+                save1[(size_t) 2 * R + r] = bak;
+                save1[(size_t) 3 * R + r] = sg;
             }
         } else if (kind == 1) {
-            const double fl = P.w[(size_t) col * n + r];
-            const double *q = rs + (size_t) c1 * 5 * n;
+            const double fl = B.w[(size_t) col * R + r];
+            const double *q = rs + (size_t) c1 * 5 * R;
             acc[0] += fl * se + f * q[r];
-            acc[1] += fl * ss + f * q[(size_t) n + r];
-            acc[2] += fl * bak + f * 2. * (sbr * q[(size_t) 2 * n + r] + sbi * q[(size_t) 3 * n + r]);
-            acc[3] += fl * sg + f * q[(size_t) 4 * n + r];
+            acc[1] += fl * ss + f * q[(size_t) R + r];
+            acc[2] += fl * bak + f * 2. * (sbr * q[(size_t) 2 * R + r] + sbi * q[(size_t) 3 * R + r]);
+            acc[3] += fl * sg + f * q[(size_t) 4 * R + r];
         } else {
-            const double fl = P.w[(size_t) col * n + r];
+            const double fl = B.w[(size_t) col * R + r];
             acc[0] += fl * se;
             acc[1] += fl * ss;
             acc[2] += fl * bak;
             acc[3] += fl * sg;
         }
     }
+    const int ncol = 1 + B.nd;
     for (int q = 0; q < 4; ++q) {
         double v = block_sum(acc[q], sh);
-        if (threadIdx.x == 0) sums[col * 4 + q] = v;
+        if (threadIdx.x == 0) sums[((size_t) cidx * ncol + col) * 4 + q] = v;
     }
 }
 
 // ---------------------------------------------------------------------------
 // K3: one thread per half-angle (mu_j < 0) and its mirror (-mu_j); a block
-// covers ANG_T half-angles and one radius group.  For every radius the
-// pi_n/tau_n recurrence runs in registers, the coefficient columns are
-// staged through shared memory ANG_KT orders at a time, and the quadratic
-// forms of S1, S2 are accumulated per thread in shared memory.
+// covers AP * ANG_T half-angles of one case and one radius group of it.  For
+// every radius the pi_n/tau_n recurrence runs in registers, the coefficient
+// columns are staged through shared memory ANG_KT orders at a time (the next
+// chunk prefetched into registers), and the quadratic forms of S1, S2 are
+// accumulated per thread in shared memory.
 // ---------------------------------------------------------------------------
 constexpr int ANG_T = 64;
 constexpr int ANG_KT = 64;
 
-// AP half-angle pairs per thread (AP = 2 when the accumulators fit), so one
-// staged coefficient feeds 8*AP FMAs and the AP pi/tau chains interleave.
 template <int NC1, int NC2, int AP>
-__global__ void __launch_bounds__(ANG_T) k_angular(DevProblem P, int c1base, int c2base, int first,
-                                                   const int *__restrict__ gstart,
+__global__ void __launch_bounds__(ANG_T) k_angular(DevBatch B, int c1base, int c2base, int first,
+                                                   const AngItem *__restrict__ items,
                                                    const double *__restrict__ coef,
                                                    double *__restrict__ part, double *__restrict__ save2) {
     constexpr int C1 = 1 + NC1;
@@ -472,20 +492,23 @@ __global__ void __launch_bounds__(ANG_T) k_angular(DevProblem P, int c1base, int
     double *fv2s = (double *) (cbuf + ANG_KT * C1);          // [ANG_KT]
     double *acc = fv2s + ANG_KT;                             // [AP][NS*2*4][ANG_T]
 
+    const AngItem it = items[blockIdx.x];
+    const DevCase &C = B.cs[it.c];
     const int tid = threadIdx.x;
-    const int g = blockIdx.y;
-    const int n = P.n;
-    const size_t tot = (size_t) P.tot;
-    const double *fv2 = P.fv + (P.n1 + 2);
+    const int R = B.R;
+    const int nh = C.nh, n_qang = C.n_qang;
+    const size_t tot = (size_t) B.tot;
+    const double *fv2 = B.fv + (B.n1max + 2);
+    const double *mup = B.mu_pool + C.mu_off;
     const double4 *cf = (const double4 *) coef;
     int jh[AP];
     bool act[AP];
     double mu[AP];
 #pragma unroll
     for (int a = 0; a < AP; ++a) {
-        jh[a] = (blockIdx.x * AP + a) * ANG_T + tid;
-        act[a] = jh[a] < P.nh;
-        mu[a] = act[a] ? P.mu[jh[a]] : 0.;
+        jh[a] = (it.xt * AP + a) * ANG_T + tid;
+        act[a] = jh[a] < nh;
+        mu[a] = act[a] ? mup[jh[a]] : 0.;
     }
     const bool any = act[0];
 
@@ -493,14 +516,13 @@ __global__ void __launch_bounds__(ANG_T) k_angular(DevProblem P, int c1base, int
 
     int slot1[NC1 > 0 ? NC1 : 1], slot2[NC2 > 0 ? NC2 : 1];
 #pragma unroll
-    for (int k = 0; k < NC1; ++k) slot1[k] = 1 + P.idx1[c1base + k];
+    for (int k = 0; k < NC1; ++k) slot1[k] = 1 + B.idx1[c1base + k];
 #pragma unroll
-    for (int k = 0; k < NC2; ++k) slot2[k] = 1 + P.idx2[c2base + k];
+    for (int k = 0; k < NC2; ++k) slot2[k] = 1 + B.idx2[c2base + k];
 
-    const int rbeg = gstart[g], rend = gstart[g + 1];
-    for (int r = rbeg; r < rend; ++r) {
-        const int n1 = P.n1r[r];
-        const size_t off = (size_t) P.off[r];
+    for (int r = it.rbeg; r < it.rend; ++r) {
+        const int n1 = B.n1r[r];
+        const size_t off = (size_t) B.off[r];
         cplx spA[AP][C1], smA[AP][C1], spB[AP][C1], smB[AP][C1];
         double p0[AP], p1[AP];
 #pragma unroll
@@ -574,12 +596,12 @@ __global__ void __launch_bounds__(ANG_T) k_angular(DevProblem P, int c1base, int
             if (t < kt) step(t, true);
         }
         if (!any) continue;
-        const double f = P.w[r], half_f = f * .5;
+        const double f = B.w[r], half_f = f * .5;
         double fl1[NC1 > 0 ? NC1 : 1], fl2[NC2 > 0 ? NC2 : 1];
 #pragma unroll
-        for (int k = 0; k < NC1; ++k) fl1[k] = P.w[(size_t) slot1[k] * n + r];
+        for (int k = 0; k < NC1; ++k) fl1[k] = B.w[(size_t) slot1[k] * R + r];
 #pragma unroll
-        for (int k = 0; k < NC2; ++k) fl2[k] = P.w[(size_t) slot2[k] * n + r];
+        for (int k = 0; k < NC2; ++k) fl2[k] = B.w[(size_t) slot2[k] * R + r];
 #pragma unroll
         for (int a = 0; a < AP; ++a) {
             if (!act[a]) continue;
@@ -598,9 +620,9 @@ __global__ void __launch_bounds__(ANG_T) k_angular(DevProblem P, int c1base, int
 #pragma unroll
                     for (int e = 0; e < 4; ++e) av[e * ANG_T] += f * pv[e];
                     if (save2) {
-                        const int jj = h ? P.n_qang - 1 - jh[a] : jh[a];
+                        const int jj = h ? n_qang - 1 - jh[a] : jh[a];
 #pragma unroll
-                        for (int e = 0; e < 4; ++e) save2[((size_t) e * n + r) * P.n_qang + jj] = pv[e];
+                        for (int e = 0; e < 4; ++e) save2[((size_t) e * R + r) * n_qang + jj] = pv[e];
                     }
                 }
 #pragma unroll
@@ -624,7 +646,8 @@ __global__ void __launch_bounds__(ANG_T) k_angular(DevProblem P, int c1base, int
             }
         }
     }
-    const int Q = 4 * (1 + P.nd);
+    const int Q = 4 * (1 + B.nd);
+    double *pc = part + C.part_off + (size_t) it.g * Q * n_qang;
 #pragma unroll
     for (int a = 0; a < AP; ++a) {
         if (!act[a]) continue;
@@ -634,56 +657,62 @@ __global__ void __launch_bounds__(ANG_T) k_angular(DevProblem P, int c1base, int
             const int slot = s == 0 ? 0 : (s <= NC1 ? slot1[s - 1] : slot2[s - 1 - NC1]);
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
-                const int jj = h ? P.n_qang - 1 - jh[a] : jh[a];
+                const int jj = h ? n_qang - 1 - jh[a] : jh[a];
 #pragma unroll
                 for (int e = 0; e < 4; ++e)
-                    part[((size_t) g * Q + slot * 4 + e) * P.n_qang + jj] = accA[(s * 8 + h * 4 + e) * ANG_T + tid];
+                    pc[(size_t) (slot * 4 + e) * n_qang + jj] = accA[(s * 8 + h * 4 + e) * ANG_T + tid];
             }
         }
     }
 }
 
-__global__ void k_reduce_pf(int n_groups, int Q, int n_qang, const double *__restrict__ part,
-                            double *__restrict__ pfacc) {
-    const size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (size_t) Q * n_qang) return;
+// pfacc[case][q][jj] = sum over the case's radius groups, in group order
+__global__ void k_reduce_pf(DevBatch B, long long total, const long long *__restrict__ start,
+                            const double *__restrict__ part, double *__restrict__ pfacc) {
+    const long long e = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= total) return;
+    const int c = find_case(start, B.ncase, e);
+    const DevCase &C = B.cs[c];
+    const long long local = e - start[c];
+    const size_t span = (size_t) 4 * (1 + B.nd) * C.n_qang;
     double s = 0.;
-    for (int g = 0; g < n_groups; ++g) s += part[(size_t) g * Q * n_qang + i];
-    pfacc[i] = s;
+    for (int g = 0; g < C.G; ++g) s += part[C.part_off + (size_t) g * span + local];
+    pfacc[C.pf_off + local] = s;
 }
 
-// save_control 2: re-weight stored per-radius kernels (src/lmie_schedule.c:1087-1124)
-__global__ void k_save_reweight_pf(DevProblem P, const double *__restrict__ save2,
+// save_control 2 (single case): re-weight stored per-radius kernels
+// (src/lmie_schedule.c:1087-1124)
+__global__ void k_save_reweight_pf(DevBatch B, int n_qang, const double *__restrict__ save2,
                                    const double *__restrict__ w2, double *__restrict__ pfacc) {
     const size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x;   // e*n_qang + jj
-    if (i >= (size_t) 4 * P.n_qang) return;
-    const int e = (int) (i / P.n_qang), jj = (int) (i % P.n_qang);
-    const int n = P.n;
+    if (i >= (size_t) 4 * n_qang) return;
+    const int e = (int) (i / n_qang), jj = (int) (i % n_qang);
+    const int n = B.R;
     double s = 0.;
-    for (int r = 0; r < n; ++r) s += save2[((size_t) e * n + r) * P.n_qang + jj] * P.w[r];
-    pfacc[(size_t) e * P.n_qang + jj] = s;
-    for (int k = 0; k < P.nd; ++k) {
+    for (int r = 0; r < n; ++r) s += save2[((size_t) e * n + r) * n_qang + jj] * B.w[r];
+    pfacc[(size_t) e * n_qang + jj] = s;
+    for (int k = 0; k < B.nd; ++k) {
         double v = 0.;
         bool idx2 = false;
-        for (int q = 0; q < P.nd2; ++q) idx2 |= P.idx2[q] == k;
+        for (int q = 0; q < B.nd2; ++q) idx2 |= B.idx2[q] == k;
         if (idx2)
-            for (int r = 0; r < n; ++r) v += save2[((size_t) e * n + r) * P.n_qang + jj] * w2[(size_t) k * n + r];
-        pfacc[((size_t) (1 + k) * 4 + e) * P.n_qang + jj] = v;
+            for (int r = 0; r < n; ++r) v += save2[((size_t) e * n + r) * n_qang + jj] * w2[(size_t) k * n + r];
+        pfacc[((size_t) (1 + k) * 4 + e) * n_qang + jj] = v;
     }
 }
 
-__global__ void k_save_reweight_scal(DevProblem P, const double *__restrict__ save1,
-                                     const double *__restrict__ w2, double *__restrict__ sums) {
+__global__ void k_save_reweight_scal(DevBatch B, const double *__restrict__ save1, const double *__restrict__ w2,
+                                     double *__restrict__ sums) {
     const int col = threadIdx.x;    // 0..nd
-    if (col > P.nd) return;
-    const int n = P.n;
+    if (col > B.nd) return;
+    const int n = B.R;
     double acc[4] = {0., 0., 0., 0.};
     bool on = col == 0;
     if (col > 0)
-        for (int q = 0; q < P.nd2; ++q) on |= P.idx2[q] == col - 1;
+        for (int q = 0; q < B.nd2; ++q) on |= B.idx2[q] == col - 1;
     if (on)
         for (int r = 0; r < n; ++r) {
-            const double a = col == 0 ? P.w[r] : w2[(size_t) (col - 1) * n + r];
+            const double a = col == 0 ? B.w[r] : w2[(size_t) (col - 1) * n + r];
             for (int q = 0; q < 4; ++q) acc[q] += save1[(size_t) q * n + r] * a;
         }
     for (int q = 0; q < 4; ++q) sums[col * 4 + q] = acc[q];
@@ -694,229 +723,252 @@ __global__ void k_save_reweight_scal(DevProblem P, const double *__restrict__ sa
 // lambda^2/(2 pi), Cbak additionally by 1/(8 pi), with the chain rule for
 // every derivative slot.
 // ---------------------------------------------------------------------------
-__global__ void k_normalize(DevProblem P, const double *__restrict__ sums, const double *__restrict__ pfacc,
-                            double *__restrict__ scal, double *__restrict__ pfn) {
-    const double csca = sums[1];
+__global__ void k_normalize_pf(DevBatch B, long long total, const long long *__restrict__ start,
+                               const double *__restrict__ sums, const double *__restrict__ pfacc,
+                               double *__restrict__ pfn) {
+    const long long e = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= total) return;
+    const int c = find_case(start, B.ncase, e);
+    const DevCase &C = B.cs[c];
+    const long long local = e - start[c];
+    const int q = (int) (local / C.n_qang), jj = (int) (local % C.n_qang);
+    const int slot = q / 4, el = q % 4;
+    const double *sm = sums + (size_t) c * (1 + B.nd) * 4;
+    const double csca = sm[1];
     const double a = 2. / csca;
-    const size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x;
-    const size_t npf = (size_t) 4 * (1 + P.nd) * P.n_qang;
-    if (i < npf) {
-        const int q = (int) (i / P.n_qang), jj = (int) (i % P.n_qang);
-        const int slot = q / 4, e = q % 4;
-        if (slot == 0) {
-            pfn[i] = pfacc[i] * a;
-        } else {
-            const double a_l = -a * sums[slot * 4 + 1] / csca;
-            pfn[i] = pfacc[i] * a + pfacc[(size_t) e * P.n_qang + jj] * a_l;
-        }
-    }
-    if (i == 0) {
-        const double lam = P.lambda;
-        const double b = lam * lam / (2. * LMIEB_PI);
-        const double g = sums[3];
-        for (int k = 0; k < P.nd; ++k) {
-            const double *s = sums + (1 + k) * 4;
-            const double a_l = -a * s[1] / csca;
-            const double b_l = 2. * P.lambda_l[k] * lam / (2. * LMIEB_PI);
-            double *o = scal + (1 + k) * 4;
-            o[0] = s[0] * b + sums[0] * b_l;
-            o[1] = s[1] * b + sums[1] * b_l;
-            o[2] = (s[2] * b + sums[2] * b_l) / (2. * 4. * LMIEB_PI);
-            o[3] = s[3] * a + g * a_l;
-        }
-        scal[0] = sums[0] * b;
-        scal[1] = sums[1] * b;
-        scal[2] = sums[2] * b / (2. * 4. * LMIEB_PI);
-        scal[3] = g / csca * 2.;
+    const double *pa = pfacc + C.pf_off;
+    if (slot == 0) {
+        pfn[C.pf_off + local] = pa[local] * a;
+    } else {
+        const double a_l = -a * sm[slot * 4 + 1] / csca;
+        pfn[C.pf_off + local] = pa[local] * a + pa[(size_t) el * C.n_qang + jj] * a_l;
     }
 }
 
+__global__ void k_normalize_scal(DevBatch B, const double *__restrict__ sums, double *__restrict__ scal) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= B.ncase) return;
+    const DevCase &C = B.cs[c];
+    const int ncol = 1 + B.nd;
+    const double *sm = sums + (size_t) c * ncol * 4;
+    double *o = scal + C.scal_off;
+    const double csca = sm[1];
+    const double a = 2. / csca;
+    const double lam = C.lambda;
+    const double b = lam * lam / (2. * LMIEB_PI);
+    const double g = sm[3];
+    for (int k = 0; k < B.nd; ++k) {
+        const double *s = sm + (1 + k) * 4;
+        const double a_l = -a * s[1] / csca;
+        const double b_l = 2. * B.lambda_l[C.ml_off + k] * lam / (2. * LMIEB_PI);
+        double *ok = o + (1 + k) * 4;
+        ok[0] = s[0] * b + sm[0] * b_l;
+        ok[1] = s[1] * b + sm[1] * b_l;
+        ok[2] = (s[2] * b + sm[2] * b_l) / (2. * 4. * LMIEB_PI);
+        ok[3] = s[3] * a + g * a_l;
+    }
+    o[0] = sm[0] * b;
+    o[1] = sm[1] * b;
+    o[2] = sm[2] * b / (2. * 4. * LMIEB_PI);
+    o[3] = g / csca * 2.;
+}
+
 // ---------------------------------------------------------------------------
-// K4: expansion of the normalised phase matrix over the Gauss angles, with
-// the mu-parity folding: the basis functions are tabulated at the positive
-// nodes in chunks of orders (state carried between chunks), then one warp per
-// (order, column) contracts over the nh node pairs.
-// ---------------------------------------------------------------------------
-// Per-order recurrence coefficients rc[8*l + q] (host-computed, l >= 3,
+// GSF / Legendre basis recurrences.  rc[8*l + q] (host-computed, l >= 3,
 // j = l - 1): p00_l = q0 mu p00_{l-1} - q1 p00_{l-2};
 // p02_l = q2 mu p02_{l-1} - q3 p02_{l-2};
 // p22_l = (q4 mu - q5) p22_{l-1} - q6 p22_{l-2}; p2m_l = (q4 mu + q5) p2m_{l-1} - q6 p2m_{l-2};
-// Legendre: p_l = q1 (mu p_{l-1} - p_{l-2}) + mu p_{l-1}.
-struct GsfRow {
-    double p00, p02, p22, p2m;
-};
-
-__device__ __forceinline__ GsfRow gsf_first(int l, double x) {
-    GsfRow o;
-    if (l == 0) {
-        o.p00 = 1.; o.p02 = 0.; o.p22 = 0.; o.p2m = 0.;
-    } else if (l == 1) {
-        o.p00 = x; o.p02 = 0.; o.p22 = 0.; o.p2m = 0.;
-    } else {
-        const double x2 = x * x;
-        o.p00 = (3. * x2 - 1.) / 2.;
-        o.p02 = .25 * sqrt(6.) * (x2 - 1.);
-        double t = 1. + x;
-        o.p22 = .25 * t * t;
-        t = 1. - x;
-        o.p2m = .25 * t * t;
-    }
-    return o;
+// Legendre: p_l = q1 (mu p_{l-1} - p_{l-2}) + mu p_{l-1} (q1 = 1/2 at l = 2).
+// Function f of the GSF set: 0 p00, 1 p0+2, 2 p2+2, 3 p2-2; Legendre: f = 0.
+// ---------------------------------------------------------------------------
+template <int KIND>
+__device__ __forceinline__ double basis_first(int f, int l, double x) {
+    if (KIND == 1) return l == 0 ? 1. : x;
+    if (l == 0) return f == 0 ? 1. : 0.;
+    if (l == 1) return f == 0 ? x : 0.;
+    const double x2 = x * x;
+    if (f == 0) return (3. * x2 - 1.) / 2.;
+    if (f == 1) return .25 * sqrt(6.) * (x2 - 1.);
+    double t = f == 2 ? 1. + x : 1. - x;
+    return .25 * t * t;
 }
 
-__device__ __forceinline__ GsfRow gsf_next(const double *c, double x, const GsfRow &cur, const GsfRow &prev) {
-    GsfRow o;
-    o.p00 = c[0] * x * cur.p00 - c[1] * prev.p00;
-    o.p02 = c[2] * x * cur.p02 - c[3] * prev.p02;
+template <int KIND>
+__device__ __forceinline__ double basis_step(int f, const double *c, double x, double cur, double prev) {
+    if (KIND == 1) {
+        const double b = x * cur;
+        return c[1] * (b - prev) + b;
+    }
+    if (f == 0) return c[0] * x * cur - c[1] * prev;
+    if (f == 1) return c[2] * x * cur - c[3] * prev;
     const double e = c[4] * x;
-    o.p22 = (e - c[5]) * cur.p22 - c[6] * prev.p22;
-    o.p2m = (e + c[5]) * cur.p2m - c[6] * prev.p2m;
-    return o;
+    return (f == 2 ? e - c[5] : e + c[5]) * cur - c[6] * prev;
 }
 
-// One thread per (positive node, basis function): the four recurrences are
-// independent, so each runs on its own thread; the per-order coefficients
-// are staged through shared memory GT_L orders at a time.
-constexpr int GT_T = 64;
-constexpr int GT_L = 128;
+// advance one basis function from order l-1 to l
+template <int KIND>
+__device__ __forceinline__ double basis_next(int f, int l, const double *rc, double x, double cur, double prev) {
+    const int first = KIND == 1 ? 2 : 3;
+    return l < first ? basis_first<KIND>(f, l, x) : basis_step<KIND>(f, rc + 8 * (size_t) l, x, cur, prev);
+}
 
-__global__ void __launch_bounds__(GT_T) k_gsf_table(int nh, const double *__restrict__ mu,
-                                                    const double *__restrict__ rc, int l0, int l1, int lc,
-                                                    double *__restrict__ st, double *__restrict__ tab) {
-    __shared__ double src[GT_L][8];
-    const int id = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool act = id < 4 * nh;
-    const int f = act ? id / nh : 0, i = act ? id - f * nh : 0;
-    const double x = act ? mu[nh + i] : 0.;
+// ---------------------------------------------------------------------------
+// K4a: one thread per (case, basis function, positive node) runs the
+// recurrence over all orders and checkpoints (p_{l-2}, p_{l-1}) at the start
+// of every EX_LT-order tile.
+// ---------------------------------------------------------------------------
+template <int KIND>
+__global__ void k_exp_ckpt(DevBatch B, long long total, const long long *__restrict__ start,
+                           double *__restrict__ ckpt) {
+    constexpr int NF = KIND == 0 ? 4 : 1;
+    const long long e = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= total) return;
+    const int c = find_case(start, B.ncase, e);
+    const DevCase &C = B.cs[c];
+    const long long local = e - start[c];
+    const int f = (int) (local / C.nh), i = (int) (local % C.nh);
+    const double x = B.mu_pool[C.mu_off + C.nh + i];
     double prev = 0., cur = 0.;
-    if (act && l0 > 0) {
-        prev = st[(size_t) f * nh + i];
-        cur = st[(size_t) (4 + f) * nh + i];
+    double *ck = ckpt + C.ck_off;
+    for (int l = 0; l < C.n_coef; ++l) {
+        if (l % EX_LT == 0) {
+            const size_t o = (((size_t) (l / EX_LT) * NF + f) * C.nh + i) * 2;
+            ck[o] = prev;
+            ck[o + 1] = cur;
+        }
+        const double v = basis_next<KIND>(f, l, B.rc, x, cur, prev);
+        prev = cur;
+        cur = v;
     }
-    double *out = tab + (size_t) f * lc * nh + i;
-    // p_l = (A x + s C5) p_{l-1} - C p_{l-2}
-    const int ia = f == 0 ? 0 : f == 1 ? 2 : 4;
-    const int ic = f == 0 ? 1 : f == 1 ? 3 : 6;
-    const double sb = f == 2 ? -1. : f == 3 ? 1. : 0.;
-    for (int c0 = l0; c0 < l1; c0 += GT_L) {
-        const int ct = min(GT_L, l1 - c0);
-        __syncthreads();
-        for (int q = threadIdx.x; q < 8 * ct; q += GT_T) src[q / 8][q % 8] = rc[8 * (size_t) c0 + q];
-        __syncthreads();
-        if (!act) continue;
-        for (int t = 0; t < ct; ++t) {
-            const int l = c0 + t;
-            double v;
-            if (l < 3) {
-                const GsfRow g = gsf_first(l, x);
-                v = f == 0 ? g.p00 : f == 1 ? g.p02 : f == 2 ? g.p22 : g.p2m;
-            } else {
-                v = (src[t][ia] * x + sb * src[t][5]) * cur - src[t][ic] * prev;
+}
+
+// ---------------------------------------------------------------------------
+// K4b: one block per (case, order tile, angle tile).  The basis functions of
+// the tile are generated into shared memory from the checkpoints, the
+// weighted phase-matrix moments of the tile's node pairs (mu-parity folding)
+// are staged next to them, and each output (order, column) is contracted
+// over the tile's EX_AT node pairs.  Raw per-tile sums go to exq.
+// ---------------------------------------------------------------------------
+constexpr int EX_T = 128;
+
+template <int KIND>
+__global__ void __launch_bounds__(EX_T) k_exp_tile(DevBatch B, const ExpItem *__restrict__ items,
+                                                   const double *__restrict__ pfn,
+                                                   const double *__restrict__ ckpt,
+                                                   double *__restrict__ exq) {
+    constexpr int NF = KIND == 0 ? 4 : 1;
+    extern __shared__ double sm[];
+    double *P = sm;                                        // [NF][EX_LT][EX_AT + 1]
+    double *Bv = P + NF * EX_LT * (EX_AT + 1);             // [ncol][12][EX_AT]
+    const ExpItem it = items[blockIdx.x];
+    const DevCase &C = B.cs[it.c];
+    const int nh = C.nh, nq = C.n_qang, ncf = C.n_coef;
+    const int ncol = 1 + B.nd;
+    const int l0 = it.lt * EX_LT, lt = min(EX_LT, ncf - l0);
+    const int i0 = it.at * EX_AT;
+    const double *mup = B.mu_pool + C.mu_off, *wqp = mup + nq;
+
+    // basis functions of the tile
+    for (int t = threadIdx.x; t < NF * EX_AT; t += EX_T) {
+        const int f = t / EX_AT, ia = t % EX_AT, i = i0 + ia;
+        double *Pf = P + (size_t) f * EX_LT * (EX_AT + 1) + ia;
+        if (i < nh) {
+            const double x = mup[nh + i];
+            const size_t o = (((size_t) it.lt * NF + f) * nh + i) * 2;
+            double prev = ckpt[C.ck_off + o], cur = ckpt[C.ck_off + o + 1];
+            for (int u = 0; u < lt; ++u) {
+                const double v = basis_next<KIND>(f, l0 + u, B.rc, x, cur, prev);
+                prev = cur;
+                cur = v;
+                Pf[u * (EX_AT + 1)] = v;
             }
-            prev = cur;
-            cur = v;
-            out[(size_t) (l - l0) * nh] = v;
-        }
-    }
-    if (!act) return;
-    st[(size_t) f * nh + i] = prev;
-    st[(size_t) (4 + f) * nh + i] = cur;
-}
-
-__global__ void k_leg_table(int nh, const double *__restrict__ mu, const double *__restrict__ rc, int l0,
-                            int l1, int lc, double *__restrict__ st, double *__restrict__ tab) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nh) return;
-    const double x = mu[nh + i];
-    double pm = 0., pc = 0.;
-    if (l0 > 0) { pm = st[i]; pc = st[(size_t) nh + i]; }
-    for (int l = l0; l < l1; ++l) {
-        double p;
-        if (l == 0) p = 1.;
-        else if (l == 1) p = x;
-        else {
-            const double b = x * pc;
-            p = rc[8 * (size_t) l + 1] * (b - pm) + b;
-        }
-        pm = pc;
-        pc = p;
-        tab[(size_t) (l - l0) * nh + i] = p;
-    }
-    st[i] = pm;
-    st[(size_t) nh + i] = pc;
-}
-
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
-
-// kind 0 (GSF) / 1 (Legendre): raw[(c*6+e)*n_coef + l] for l in [l0, l1)
-template <int KIND>
-__global__ void __launch_bounds__(256) k_expand_project(DevProblem P, int l0, int l1, int lc,
-                                                        const double *__restrict__ pfn,
-                                                        const double *__restrict__ tab,
-                                                        double *__restrict__ raw) {
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    const int nl = l1 - l0;
-    const int ncol = 1 + P.nd;
-    if (warp >= nl * ncol) return;
-    const int lr = warp % nl, c = warp / nl;
-    const int l = l0 + lr;
-    const int nh = P.nh, nq = P.n_qang;
-    const double s = (l & 1) ? -1. : 1.;
-    const double *F0 = pfn + ((size_t) c * 4 + 0) * nq, *F1 = pfn + ((size_t) c * 4 + 1) * nq;
-    const double *F2 = pfn + ((size_t) c * 4 + 2) * nq, *F3 = pfn + ((size_t) c * 4 + 3) * nq;
-    double acc[6] = {0., 0., 0., 0., 0., 0.};
-    for (int i = lane; i < nh; i += 32) {
-        const int i1 = nh - 1 - i, i2 = nh + i;
-        const double w = P.wq[i2];
-        const double u0 = F0[i1] * w, u1 = F1[i1] * w, u2 = F2[i1] * w, u3 = F3[i1] * w;
-        const double v0 = F0[i2] * w, v1 = F1[i2] * w, v2 = F2[i2] * w, v3 = F3[i2] * w;
-        if (KIND == 0) {
-            const double P00 = tab[(0 * (size_t) lc + lr) * nh + i];
-            const double P02 = tab[(1 * (size_t) lc + lr) * nh + i];
-            const double P22 = tab[(2 * (size_t) lc + lr) * nh + i];
-            const double P2m = tab[(3 * (size_t) lc + lr) * nh + i];
-            acc[0] += P00 * (u0 * s + v0);
-            acc[1] += P2m * (u0 + u1) * s + P22 * (v0 + v1);
-            acc[2] += P22 * (u0 - u1) * s + P2m * (v0 - v1);
-            acc[3] += P00 * (u1 * s + v1);
-            acc[4] += P02 * (u2 * s + v2);
-            acc[5] += P02 * (u3 * s + v3);
         } else {
-            const double Y = tab[(size_t) lr * nh + i];
-            acc[0] += Y * (u0 * s + v0);
-            acc[1] += Y * (u0 * s + v0);
-            acc[2] += Y * (u1 * s + v1);
-            acc[3] += Y * (u1 * s + v1);
-            acc[4] += Y * (u2 * s + v2);
-            acc[5] += Y * (u3 * s + v3);
+            for (int u = 0; u < lt; ++u) Pf[u * (EX_AT + 1)] = 0.;
         }
     }
+    // weighted moments of the node pairs: b1 at the mirror node -mu_i, b2 at +mu_i
+    for (int t = threadIdx.x; t < ncol * EX_AT; t += EX_T) {
+        const int col = t / EX_AT, ia = t % EX_AT, i = i0 + ia;
+        double *bv = Bv + (size_t) col * 12 * EX_AT + ia;
+        if (i < nh) {
+            const int i1 = nh - 1 - i, i2 = nh + i;
+            const double w = wqp[i2];
+            const double *F = pfn + C.pf_off + (size_t) col * 4 * nq;
+            const double u0 = F[i1] * w, u1 = F[nq + i1] * w, u2 = F[2 * nq + i1] * w, u3 = F[3 * nq + i1] * w;
+            const double v0 = F[i2] * w, v1 = F[nq + i2] * w, v2 = F[2 * nq + i2] * w, v3 = F[3 * nq + i2] * w;
+            if (KIND == 0) {
+                bv[0 * EX_AT] = u0; bv[1 * EX_AT] = u0 + u1; bv[2 * EX_AT] = u0 - u1;
+                bv[3 * EX_AT] = u1; bv[4 * EX_AT] = u2;      bv[5 * EX_AT] = u3;
+                bv[6 * EX_AT] = v0; bv[7 * EX_AT] = v0 + v1; bv[8 * EX_AT] = v0 - v1;
+                bv[9 * EX_AT] = v1; bv[10 * EX_AT] = v2;     bv[11 * EX_AT] = v3;
+            } else {
+                bv[0 * EX_AT] = u0; bv[1 * EX_AT] = u0; bv[2 * EX_AT] = u1;
+                bv[3 * EX_AT] = u1; bv[4 * EX_AT] = u2; bv[5 * EX_AT] = u3;
+                bv[6 * EX_AT] = v0; bv[7 * EX_AT] = v0; bv[8 * EX_AT] = v1;
+                bv[9 * EX_AT] = v1; bv[10 * EX_AT] = v2; bv[11 * EX_AT] = v3;
+            }
+        } else {
+            for (int q = 0; q < 12; ++q) bv[q * EX_AT] = 0.;
+        }
+    }
+    __syncthreads();
+    // contraction over the tile's node pairs
+    for (int t = threadIdx.x; t < ncol * lt; t += EX_T) {
+        const int col = t / lt, u = t % lt;
+        const int l = l0 + u;
+        const double s = (l & 1) ? -1. : 1.;
+        const double *bv = Bv + (size_t) col * 12 * EX_AT;
+        double acc[6] = {0., 0., 0., 0., 0., 0.};
+        if (KIND == 0) {
+            const double *P00 = P + (size_t) (0 * EX_LT + u) * (EX_AT + 1);
+            const double *P02 = P + (size_t) (1 * EX_LT + u) * (EX_AT + 1);
+            const double *P22 = P + (size_t) (2 * EX_LT + u) * (EX_AT + 1);
+            const double *P2m = P + (size_t) (3 * EX_LT + u) * (EX_AT + 1);
+#pragma unroll 4
+            for (int ia = 0; ia < EX_AT; ++ia) {
+                const double p00 = P00[ia], p02 = P02[ia], p22 = P22[ia], p2m = P2m[ia];
+                acc[0] += p00 * (bv[0 * EX_AT + ia] * s + bv[6 * EX_AT + ia]);
+                acc[1] += p2m * bv[1 * EX_AT + ia] * s + p22 * bv[7 * EX_AT + ia];
+                acc[2] += p22 * bv[2 * EX_AT + ia] * s + p2m * bv[8 * EX_AT + ia];
+                acc[3] += p00 * (bv[3 * EX_AT + ia] * s + bv[9 * EX_AT + ia]);
+                acc[4] += p02 * (bv[4 * EX_AT + ia] * s + bv[10 * EX_AT + ia]);
+                acc[5] += p02 * (bv[5 * EX_AT + ia] * s + bv[11 * EX_AT + ia]);
+            }
+        } else {
+            const double *Y = P + (size_t) u * (EX_AT + 1);
+#pragma unroll 4
+            for (int ia = 0; ia < EX_AT; ++ia) {
+                const double y = Y[ia];
 #pragma unroll
-    for (int e = 0; e < 6; ++e) acc[e] = warp_sum(acc[e]);
-    if (lane == 0) {
+                for (int e = 0; e < 6; ++e) acc[e] += y * (bv[e * EX_AT + ia] * s + bv[(6 + e) * EX_AT + ia]);
+            }
+        }
+        double *o = exq + C.ex_off + ((size_t) it.at * ncol + col) * 6 * ncf + l;
 #pragma unroll
-        for (int e = 0; e < 6; ++e) raw[((size_t) c * 6 + e) * P.n_coef + l] = acc[e];
+        for (int e = 0; e < 6; ++e) o[(size_t) e * ncf] = acc[e];
     }
 }
 
-// Recombination, (2l+1)/2 scaling, zeroed beta_0 derivative and the
-// truncation search (first l with |coef_0(l)| <= accuracy).
+// K4c: sum of the angle tiles in order, recombination, (2l+1)/2 scaling,
+// zeroed beta_0 derivative and the truncation search (first l with
+// |coef_0(l)| <= accuracy).
 template <int KIND>
-__global__ void k_expand_finalize(DevProblem P, double accuracy, const double *__restrict__ raw,
-                                  double *__restrict__ coefs, int *__restrict__ trunc) {
-    const size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x;
-    const int nc = P.n_coef;
-    if (i >= (size_t) (1 + P.nd) * nc) return;
-    const int c = (int) (i / nc), l = (int) (i % nc);
-    const double *rw = raw + (size_t) c * 6 * nc;
-    double v[6];
+__global__ void k_exp_final(DevBatch B, long long total, const long long *__restrict__ start,
+                            const double *__restrict__ exq, double *__restrict__ coefs, int *__restrict__ trunc) {
+    const long long e = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= total) return;
+    const int c = find_case(start, B.ncase, e);
+    const DevCase &C = B.cs[c];
+    const long long local = e - start[c];
+    const int ncf = C.n_coef, ncol = 1 + B.nd;
+    const int col = (int) (local / ncf), l = (int) (local % ncf);
+    const int nat = (C.nh + EX_AT - 1) / EX_AT;
+    double v[6] = {0., 0., 0., 0., 0., 0.};
+    for (int at = 0; at < nat; ++at) {
+        const double *q = exq + C.ex_off + ((size_t) at * ncol + col) * 6 * ncf + l;
 #pragma unroll
-    for (int e = 0; e < 6; ++e) v[e] = rw[(size_t) e * nc + l];
+        for (int k = 0; k < 6; ++k) v[k] += q[(size_t) k * ncf];
+    }
     if (KIND == 0) {
         const double t = v[1];
         v[1] = (t + v[2]) / 2.;
@@ -926,86 +978,52 @@ __global__ void k_expand_finalize(DevProblem P, double accuracy, const double *_
     }
     const double sc = (2. * l + 1.) / 2.;
 #pragma unroll
-    for (int e = 0; e < 6; ++e) v[e] *= sc;
-    if (c > 0 && l == 0) v[0] = 0.;
-    double *o = coefs + (size_t) c * 6 * nc;
+    for (int k = 0; k < 6; ++k) v[k] *= sc;
+    if (col > 0 && l == 0) v[0] = 0.;
+    double *o = coefs + (KIND == 0 ? C.gc_off : C.lc_off) + (size_t) col * 6 * ncf;
 #pragma unroll
-    for (int e = 0; e < 6; ++e) o[(size_t) e * nc + l] = v[e];
-    if (c == 0 && fabs(v[0]) <= accuracy) atomicMax(trunc, nc - l);
+    for (int k = 0; k < 6; ++k) o[(size_t) k * ncf + l] = v[k];
+    if (col == 0 && fabs(v[0]) <= C.accuracy) atomicMax(trunc + c, ncf - l);
 }
 
 // ---------------------------------------------------------------------------
 // K5: phase matrix at the user's angles from the truncated expansion; one
-// thread per user angle, one block column per output column.  The
-// coefficients and recurrence constants are staged through shared memory
-// PU_L orders at a time and read as broadcasts.
+// thread per (case, column, user angle).
 // ---------------------------------------------------------------------------
-constexpr int PU_T = 64;
-constexpr int PU_L = 256;
-
 template <int KIND>
-__global__ void __launch_bounds__(PU_T) k_phase_user(DevProblem P, const double *__restrict__ coefs,
-                                                     const int *__restrict__ trunc, const double *__restrict__ rc,
-                                                     const double *__restrict__ mu_user, double *__restrict__ out) {
-    __shared__ double scf[6][PU_L];
-    __shared__ double src[PU_L][8];
-    const int a = blockIdx.x * PU_T + threadIdx.x;
-    const int c = blockIdx.y;
-    const int na = P.n_angles;
-    const bool act = a < na;
-    const int ncf = P.n_coef;
-    const int nt = trunc[0] > 0 ? ncf - trunc[0] + 1 : ncf;
-    const double x = act ? mu_user[a] : 0.;
-    const double *cf = coefs + (size_t) c * 6 * ncf;
+__global__ void k_phase_user(DevBatch B, long long total, const long long *__restrict__ start,
+                             const double *__restrict__ coefs, const int *__restrict__ trunc,
+                             double *__restrict__ out) {
+    const long long e = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= total) return;
+    const int c = find_case(start, B.ncase, e);
+    const DevCase &C = B.cs[c];
+    const long long local = e - start[c];
+    const int na = C.n_angles, ncf = C.n_coef;
+    const int col = (int) (local / na), a = (int) (local % na);
+    const int nt = trunc[c] > 0 ? ncf - trunc[c] + 1 : ncf;
+    const double x = B.mu_user[C.mu_user_off + a];
+    const double *cf = coefs + (KIND == 0 ? C.gc_off : C.lc_off) + (size_t) col * 6 * ncf;
+    double *o = out + C.pf_out_off + (size_t) col * 6 * na;
     double s0 = 0., s1 = 0., s2 = 0., s3 = 0., s4 = 0., s5 = 0.;
-    GsfRow prev = {0., 0., 0., 0.}, cur = {0., 0., 0., 0.};
-    double pm = 0., pc = 0.;
-    for (int l0 = 0; l0 < nt; l0 += PU_L) {
-        const int lt = min(PU_L, nt - l0);
-        __syncthreads();
-        for (int i = threadIdx.x; i < 6 * lt; i += PU_T) {
-            const int e = i / lt, l = i - e * lt;
-            scf[e][l] = cf[(size_t) e * ncf + l0 + l];
-        }
-        for (int i = threadIdx.x; i < 8 * lt; i += PU_T) src[i / 8][i % 8] = rc[8 * (size_t) l0 + i];
-        __syncthreads();
-        if (!act) continue;
-        for (int t = 0; t < lt; ++t) {
-            const int l = l0 + t;
-            if (KIND == 0) {
-                const GsfRow nx = l < 3 ? gsf_first(l, x) : gsf_next(src[t], x, cur, prev);
-                prev = cur;
-                cur = nx;
-                s0 += scf[0][t] * cur.p00;
-                s3 += scf[3][t] * cur.p00;
-                if (l >= 2) {
-                    s4 += scf[4][t] * cur.p02;
-                    s5 += scf[5][t] * cur.p02;
-                    s1 += (scf[1][t] + scf[2][t]) * cur.p22;
-                    s2 += (scf[1][t] - scf[2][t]) * cur.p2m;
-                }
-            } else {
-                double p;
-                if (l == 0) p = 1.;
-                else if (l == 1) p = x;
-                else {
-                    const double b = x * pc;
-                    p = src[t][1] * (b - pm) + b;
-                }
-                pm = pc;
-                pc = p;
-                s0 += scf[0][t] * p;
-                s1 += scf[1][t] * p;
-                s2 += scf[2][t] * p;
-                s3 += scf[3][t] * p;
-                s4 += scf[4][t] * p;
-                s5 += scf[5][t] * p;
+    if (KIND == 0) {
+        double q[4] = {0., 0., 0., 0.}, p[4] = {0., 0., 0., 0.};
+        for (int l = 0; l < nt; ++l) {
+#pragma unroll
+            for (int f = 0; f < 4; ++f) {
+                const double v = basis_next<0>(f, l, B.rc, x, p[f], q[f]);
+                q[f] = p[f];
+                p[f] = v;
+            }
+            s0 += cf[l] * p[0];
+            s3 += cf[(size_t) 3 * ncf + l] * p[0];
+            if (l >= 2) {
+                s4 += cf[(size_t) 4 * ncf + l] * p[1];
+                s5 += cf[(size_t) 5 * ncf + l] * p[1];
+                s1 += (cf[(size_t) 1 * ncf + l] + cf[(size_t) 2 * ncf + l]) * p[2];
+                s2 += (cf[(size_t) 1 * ncf + l] - cf[(size_t) 2 * ncf + l]) * p[3];
             }
         }
-    }
-    if (!act) return;
-    double *o = out + (size_t) c * 6 * na;
-    if (KIND == 0) {
         o[a] = s0;
         o[(size_t) 3 * na + a] = s3;
         o[(size_t) 4 * na + a] = s4;
@@ -1013,6 +1031,18 @@ __global__ void __launch_bounds__(PU_T) k_phase_user(DevProblem P, const double 
         o[(size_t) 1 * na + a] = (s1 + s2) / 2.;
         o[(size_t) 2 * na + a] = (s1 - s2) / 2.;
     } else {
+        double pm = 0., pc = 0.;
+        for (int l = 0; l < nt; ++l) {
+            const double v = basis_next<1>(0, l, B.rc, x, pc, pm);
+            pm = pc;
+            pc = v;
+            s0 += cf[l] * v;
+            s1 += cf[(size_t) 1 * ncf + l] * v;
+            s2 += cf[(size_t) 2 * ncf + l] * v;
+            s3 += cf[(size_t) 3 * ncf + l] * v;
+            s4 += cf[(size_t) 4 * ncf + l] * v;
+            s5 += cf[(size_t) 5 * ncf + l] * v;
+        }
         o[a] = s0;
         o[(size_t) 1 * na + a] = s1;
         o[(size_t) 2 * na + a] = s2;
@@ -1032,8 +1062,8 @@ size_t angular_smem() {
 }
 
 template <int NC1, int NC2>
-int run_angular(cudaStream_t s, const DevProblem &P, int c1base, int c2base, int first, int G,
-                const int *gstart, const double *coef, double *part, double *save2) {
+int run_angular(cudaStream_t s, const DevBatch &B, int c1base, int c2base, int first, int nitems,
+                const AngItem *items, const double *coef, double *part, double *save2) {
     constexpr int AP = angular_ap<NC1, NC2>();
     const size_t sm = angular_smem<NC1, NC2>();
     static bool attr = false;
@@ -1042,23 +1072,47 @@ int run_angular(cudaStream_t s, const DevProblem &P, int c1base, int c2base, int
                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm));
         attr = true;
     }
-    dim3 grid(ceil_div(P.nh, ANG_T * AP), G);
-    k_angular<NC1, NC2, AP><<<grid, ANG_T, sm, s>>>(P, c1base, c2base, first, gstart, coef, part, save2);
+    k_angular<NC1, NC2, AP><<<nitems, ANG_T, sm, s>>>(B, c1base, c2base, first, items, coef, part, save2);
     LMIEB_CUDA_TRY(cudaGetLastError());
     return 0;
 }
 
 template <int NC1>
-int run_angular_nc2(cudaStream_t s, const DevProblem &P, int nc2, int c1base, int c2base, int first,
-                    int G, const int *gstart, const double *coef, double *part, double *save2) {
+int run_angular_nc2(cudaStream_t s, const DevBatch &B, int nc2, int c1base, int c2base, int first, int nitems,
+                    const AngItem *items, const double *coef, double *part, double *save2) {
     switch (nc2) {
-    case 0: return run_angular<NC1, 0>(s, P, c1base, c2base, first, G, gstart, coef, part, save2);
-    case 1: return run_angular<NC1, 1>(s, P, c1base, c2base, first, G, gstart, coef, part, save2);
-    case 2: return run_angular<NC1, 2>(s, P, c1base, c2base, first, G, gstart, coef, part, save2);
-    case 3: return run_angular<NC1, 3>(s, P, c1base, c2base, first, G, gstart, coef, part, save2);
-    case 4: return run_angular<NC1, 4>(s, P, c1base, c2base, first, G, gstart, coef, part, save2);
+    case 0: return run_angular<NC1, 0>(s, B, c1base, c2base, first, nitems, items, coef, part, save2);
+    case 1: return run_angular<NC1, 1>(s, B, c1base, c2base, first, nitems, items, coef, part, save2);
+    case 2: return run_angular<NC1, 2>(s, B, c1base, c2base, first, nitems, items, coef, part, save2);
+    case 3: return run_angular<NC1, 3>(s, B, c1base, c2base, first, nitems, items, coef, part, save2);
+    case 4: return run_angular<NC1, 4>(s, B, c1base, c2base, first, nitems, items, coef, part, save2);
     }
     return -1;
+}
+
+template <int KIND>
+int run_expand(cudaStream_t s, const DevBatch &B, long long nck, const long long *ck_start,
+               int nitems, const ExpItem *items, long long nfin, const long long *fin_start, const double *pfn,
+               double *ckpt, double *exq, double *coefs, int *trunc) {
+    constexpr int NF = KIND == 0 ? 4 : 1;
+    constexpr int SMAX = 200 * 1024;
+    const size_t sm = sizeof(double) * ((size_t) NF * EX_LT * (EX_AT + 1) + (size_t) (1 + B.nd) * 12 * EX_AT);
+    if (sm > (size_t) SMAX) {
+        fprintf(stderr, "ERROR: expansion tile needs %zu bytes of shared memory (too many derivatives)\n", sm);
+        return -1;
+    }
+    static bool attr = false;
+    if (!attr) {
+        LMIEB_CUDA_TRY(cudaFuncSetAttribute(k_exp_tile<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMAX));
+        attr = true;
+    }
+    k_exp_ckpt<KIND><<<ceil_div(nck, 128), 128, 0, s>>>(B, nck, ck_start, ckpt);
+    LMIEB_CUDA_TRY(cudaGetLastError());
+    k_exp_tile<KIND><<<nitems, EX_T, sm, s>>>(B, items, pfn, ckpt, exq);
+    LMIEB_CUDA_TRY(cudaGetLastError());
+    k_exp_final<KIND><<<ceil_div(nfin, 256), 256, 0, s>>>(B, nfin, fin_start, exq, coefs, trunc);
+    LMIEB_CUDA_TRY(cudaGetLastError());
+    return 0;
 }
 
 }  // namespace
@@ -1066,21 +1120,23 @@ int run_angular_nc2(cudaStream_t s, const DevProblem &P, int nc2, int c1base, in
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
-int launch_gauss(cudaStream_t s, int n, const double *guess, const double *jr, double *mu, double *wq) {
-    k_gauss<<<ceil_div((n + 1) / 2, 32), 32, 0, s>>>(n, guess, jr, mu, wq);
+int launch_gauss(cudaStream_t s, int npairs, const int *pt, const int *pi, const int *ns, const long long *mo,
+                 const long long *go, const double *guess, const double *jr, double *pool) {
+    if (npairs <= 0) return 0;
+    k_gauss<<<ceil_div(npairs, 32), 32, 0, s>>>(npairs, pt, pi, ns, mo, go, guess, jr, pool, pool);
     LMIEB_CUDA_TRY(cudaGetLastError());
     return 0;
 }
 
-int launch_coef(cudaStream_t s, const DevProblem &P, int nc, int c0, int write_value, const int2 *tiles,
+int launch_coef(cudaStream_t s, const DevBatch &B, int nc, int c0, int write_value, const int2 *tiles,
                 double4 *rec, double *coef, double *rsp) {
-    const unsigned rb = ceil_div(P.n, 64);
-    const unsigned tb = (unsigned) P.ntiles;
+    const unsigned rb = ceil_div(B.R, 64);
+    const unsigned tb = (unsigned) B.ntiles;
     switch (nc) {
 #define LMIEB_K1(NC_)                                                                                    \
     case NC_:                                                                                            \
-        k_recur<NC_><<<rb, 64, 0, s>>>(P, c0, write_value, rec);                                         \
-        k_abcoef<NC_><<<tb, ABT, 0, s>>>(P, c0, write_value, tiles, rec, coef, rsp);                    \
+        k_recur<NC_><<<rb, 64, 0, s>>>(B, c0, write_value, rec);                                         \
+        k_abcoef<NC_><<<tb, ABT, 0, s>>>(B, c0, write_value, tiles, rec, coef, rsp);                    \
         break;
     LMIEB_K1(0)
     LMIEB_K1(1)
@@ -1096,98 +1152,83 @@ int launch_coef(cudaStream_t s, const DevProblem &P, int nc, int c0, int write_v
     return 0;
 }
 
-int launch_tile_reduce(cudaStream_t s, const DevProblem &P, const int *tstart, const double *rsp, double *rs) {
-    const size_t nt = (size_t) (1 + P.nd1) * 5 * P.n;
-    k_tile_reduce<<<ceil_div(nt, 256), 256, 0, s>>>(P.n, 1 + P.nd1, P.ntiles, tstart, rsp, rs);
+int launch_tile_reduce(cudaStream_t s, const DevBatch &B, const int *tstart, const double *rsp, double *rs) {
+    const size_t nt = (size_t) (1 + B.nd1) * 5 * B.R;
+    k_tile_reduce<<<ceil_div(nt, 256), 256, 0, s>>>(B.R, 1 + B.nd1, B.ntiles, tstart, rsp, rs);
     LMIEB_CUDA_TRY(cudaGetLastError());
     return 0;
 }
 
-int launch_reduce_scalars(cudaStream_t s, const DevProblem &P, const double *rs, double *sums,
-                          double *save1) {
-    k_reduce_scalars<<<1 + P.nd, 256, 0, s>>>(P, rs, sums, save1);
+int launch_reduce_scalars(cudaStream_t s, const DevBatch &B, const double *rs, double *sums, double *save1) {
+    dim3 grid(B.ncase, 1 + B.nd);
+    k_reduce_scalars<<<grid, 256, 0, s>>>(B, rs, sums, save1);
     LMIEB_CUDA_TRY(cudaGetLastError());
     return 0;
 }
 
-int launch_angular(cudaStream_t s, const DevProblem &P, int nc1, int c1base, int nc2, int c2base,
-                   int first, int G, const int *gstart, const double *coef, double *part,
-                   double *save2) {
+int angular_angles_per_block(int nc1) { return ANG_T * (nc1 <= 2 ? 2 : 1); }
+
+int launch_angular(cudaStream_t s, const DevBatch &B, int nc1, int c1base, int nc2, int c2base, int first,
+                   int nitems, const AngItem *items, const double *coef, double *part, double *save2) {
+    if (nitems <= 0) return 0;
     switch (nc1) {
-    case 0: return run_angular_nc2<0>(s, P, nc2, c1base, c2base, first, G, gstart, coef, part, save2);
-    case 1: return run_angular_nc2<1>(s, P, nc2, c1base, c2base, first, G, gstart, coef, part, save2);
-    case 2: return run_angular_nc2<2>(s, P, nc2, c1base, c2base, first, G, gstart, coef, part, save2);
-    case 3: return run_angular_nc2<3>(s, P, nc2, c1base, c2base, first, G, gstart, coef, part, save2);
-    case 4: return run_angular_nc2<4>(s, P, nc2, c1base, c2base, first, G, gstart, coef, part, save2);
+    case 0: return run_angular_nc2<0>(s, B, nc2, c1base, c2base, first, nitems, items, coef, part, save2);
+    case 1: return run_angular_nc2<1>(s, B, nc2, c1base, c2base, first, nitems, items, coef, part, save2);
+    case 2: return run_angular_nc2<2>(s, B, nc2, c1base, c2base, first, nitems, items, coef, part, save2);
+    case 3: return run_angular_nc2<3>(s, B, nc2, c1base, c2base, first, nitems, items, coef, part, save2);
+    case 4: return run_angular_nc2<4>(s, B, nc2, c1base, c2base, first, nitems, items, coef, part, save2);
     }
     fprintf(stderr, "ERROR: launch_angular: bad chunk width %d\n", nc1);
     return -1;
 }
 
-int angular_angles_per_block(int nc1) { return ANG_T * (nc1 <= 2 ? 2 : 1); }
-
-int launch_reduce_pf(cudaStream_t s, const DevProblem &P, int G, const double *part, double *pfacc) {
-    const int Q = 4 * (1 + P.nd);
-    const size_t tot = (size_t) Q * P.n_qang;
-    k_reduce_pf<<<ceil_div(tot, 256), 256, 0, s>>>(G, Q, P.n_qang, part, pfacc);
+int launch_reduce_pf(cudaStream_t s, const DevBatch &B, long long total, const long long *start,
+                     const double *part, double *pfacc) {
+    if (total <= 0) return 0;
+    k_reduce_pf<<<ceil_div(total, 256), 256, 0, s>>>(B, total, start, part, pfacc);
     LMIEB_CUDA_TRY(cudaGetLastError());
     return 0;
 }
 
-int launch_save_reweight(cudaStream_t s, const DevProblem &P, const double *save1, const double *save2,
+int launch_save_reweight(cudaStream_t s, const DevBatch &B, int n_qang, const double *save1, const double *save2,
                          const double *w2, double *sums, double *pfacc) {
-    k_save_reweight_scal<<<1, 32 * ceil_div(1 + P.nd, 32), 0, s>>>(P, save1, w2, sums);
+    k_save_reweight_scal<<<1, 32 * ceil_div(1 + B.nd, 32), 0, s>>>(B, save1, w2, sums);
     LMIEB_CUDA_TRY(cudaGetLastError());
-    if (P.n_qang > 0) {
-        k_save_reweight_pf<<<ceil_div((size_t) 4 * P.n_qang, 128), 128, 0, s>>>(P, save2, w2, pfacc);
+    if (n_qang > 0) {
+        k_save_reweight_pf<<<ceil_div((size_t) 4 * n_qang, 128), 128, 0, s>>>(B, n_qang, save2, w2, pfacc);
         LMIEB_CUDA_TRY(cudaGetLastError());
     }
     return 0;
 }
 
-int launch_normalize(cudaStream_t s, const DevProblem &P, const double *sums, const double *pfacc,
-                     double *scal, double *pfn) {
-    const size_t npf = (size_t) 4 * (1 + P.nd) * P.n_qang;
-    k_normalize<<<ceil_div(npf > 0 ? npf : 1, 256), 256, 0, s>>>(P, sums, pfacc, scal, pfn);
-    LMIEB_CUDA_TRY(cudaGetLastError());
-    return 0;
-}
-
-int launch_expand(cudaStream_t s, const DevProblem &P, int kind, int lchunk, double accuracy,
-                  const double *pfn, double *state, double *tab, double *raw, double *coefs, int *trunc) {
-    const double *rc = P.rc;
-    const int nc = P.n_coef, ncol = 1 + P.nd;
-    LMIEB_CUDA_TRY(cudaMemsetAsync(trunc, 0, sizeof(int), s));
-    for (int l0 = 0; l0 < nc; l0 += lchunk) {
-        const int l1 = l0 + lchunk < nc ? l0 + lchunk : nc;
-        if (kind == 0)
-            k_gsf_table<<<ceil_div((size_t) 4 * P.nh, GT_T), GT_T, 0, s>>>(P.nh, P.mu, rc, l0, l1, lchunk, state, tab);
-        else
-            k_leg_table<<<ceil_div(P.nh, 32), 32, 0, s>>>(P.nh, P.mu, rc, l0, l1, lchunk, state, tab);
-        LMIEB_CUDA_TRY(cudaGetLastError());
-        const size_t warps = (size_t) (l1 - l0) * ncol;
-        if (kind == 0)
-            k_expand_project<0><<<ceil_div(warps * 32, 256), 256, 0, s>>>(P, l0, l1, lchunk, pfn, tab, raw);
-        else
-            k_expand_project<1><<<ceil_div(warps * 32, 256), 256, 0, s>>>(P, l0, l1, lchunk, pfn, tab, raw);
+int launch_normalize(cudaStream_t s, const DevBatch &B, long long total, const long long *start,
+                     const double *sums, const double *pfacc, double *scal, double *pfn) {
+    if (total > 0) {
+        k_normalize_pf<<<ceil_div(total, 256), 256, 0, s>>>(B, total, start, sums, pfacc, pfn);
         LMIEB_CUDA_TRY(cudaGetLastError());
     }
-    const size_t nt = (size_t) ncol * nc;
-    if (kind == 0)
-        k_expand_finalize<0><<<ceil_div(nt, 256), 256, 0, s>>>(P, accuracy, raw, coefs, trunc);
-    else
-        k_expand_finalize<1><<<ceil_div(nt, 256), 256, 0, s>>>(P, accuracy, raw, coefs, trunc);
+    k_normalize_scal<<<ceil_div(B.ncase, 128), 128, 0, s>>>(B, sums, scal);
     LMIEB_CUDA_TRY(cudaGetLastError());
     return 0;
 }
 
-int launch_phase_user(cudaStream_t s, const DevProblem &P, int kind, const double *coefs, const int *trunc,
-                      const double *mu_user, double *pf_out) {
-    dim3 grid(ceil_div(P.n_angles, PU_T), 1 + P.nd);
+int launch_expand(cudaStream_t s, const DevBatch &B, int kind, long long nck,
+                  const long long *ck_start, int nitems, const ExpItem *items, long long nfin,
+                  const long long *fin_start, const double *pfn, double *ckpt, double *exq,
+                  double *coefs, int *trunc) {
+    if (nitems <= 0) return 0;
     if (kind == 0)
-        k_phase_user<0><<<grid, PU_T, 0, s>>>(P, coefs, trunc, P.rc, mu_user, pf_out);
+        return run_expand<0>(s, B, nck, ck_start, nitems, items, nfin, fin_start, pfn, ckpt, exq, coefs, trunc);
+    return run_expand<1>(s, B, nck, ck_start, nitems, items, nfin, fin_start, pfn, ckpt, exq, coefs, trunc);
+}
+
+int launch_phase_user(cudaStream_t s, const DevBatch &B, int kind, long long total, const long long *start,
+                      const double *coefs, const int *trunc, double *pf_out) {
+    if (total <= 0) return 0;
+    if (kind == 0)
+        k_phase_user<0><<<ceil_div(total, 64), 64, 0, s>>>(B, total, start, coefs, trunc, pf_out);
     else
-        k_phase_user<1><<<grid, PU_T, 0, s>>>(P, coefs, trunc, P.rc, mu_user, pf_out);
+        k_phase_user<1><<<ceil_div(total, 64), 64, 0, s>>>(B, total, start, coefs, trunc, pf_out);
     LMIEB_CUDA_TRY(cudaGetLastError());
     return 0;
 }

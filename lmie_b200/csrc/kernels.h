@@ -1,78 +1,108 @@
-// kernels.h -- launch interface of the FP64 kernels of liblmie_b200 (k_fp64.cu),
-// used by the driver (driver.cu).
+// kernels.h -- launch interface of the FP64 kernels of liblmie_b200
+// (k_fp64.cu), used by the driver (driver.cu).
+//
+// Every kernel works on a batch of independent polydisperse cases: all radii
+// of all cases form one list, and a device case table gives each case its
+// parameters and its offsets into the concatenated arrays.  A single
+// lmie_solution() is a batch of one.
 #pragma once
 
 #include "dev_common.cuh"
 
-// Device view of one polydisperse problem (all pointers are device memory).
-struct DevProblem {
-    int n;                      // radii
-    int nd, nd1, nd2;
-    int n1;                     // global truncation
-    int n_qang, nh, n_coef;
-    int n_angles;
-    int save_control;
+// One case of a batch (device copy).  Offsets index the batch-wide arrays.
+struct DevCase {
     double lambda;
-    cplx m, minv, m2;
-    const cplx *m_l;            // [nd]
-    const double *lambda_l;     // [nd]
+    cplx m, minv;
+    double accuracy;            // expansion truncation threshold
+    int r0, nr;                 // radius range [r0, r0 + nr) in the batch lists
+    int n1, n_qang, nh, n_coef, n_angles;
+    int ml_off;                 // m_l / lambda_l of this case at [ml_off, ml_off + nd)
+    long long mu_off;           // Gauss nodes/weights in the node pool
+    long long pf_off;           // [Q][n_qang] block in pfacc / pfn (Q = 4 (1 + nd))
+    long long part_off;         // [G][Q][n_qang] block of angular partials
+    long long ck_off;           // recurrence checkpoints of the expansion
+    long long ex_off;           // [n_atile][ncol][6][n_coef] expansion partials
+    long long gc_off, lc_off;   // [ncol][6][n_coef] outputs
+    long long pf_out_off;       // [ncol][6][n_angles] output (user angles)
+    long long mu_user_off;      // user-angle cosines
+    int scal_off;               // [ncol][4] normalised cross sections and g
+    int G;                      // angular radius groups
+};
+
+struct DevBatch {
+    int ncase;
+    int R;                      // radii over all cases
+    int nd, nd1, nd2;           // derivative layout (uniform over the batch)
+    int n1max, ncmax;           // largest n1 and n_coef (table lengths)
+    const DevCase *cs;          // [ncase]
     const int *idx1, *idx2;     // [nd1], [nd2]
-    const double *x;            // [n]
-    const double *xl;           // [nd1*n]
-    const double *w;            // [(1+nd)*n]
-    const int *n1r, *n2r;       // [n]
-    const long long *off;       // [n+1] prefix sums of n1r
-    long long tot;              // off[n]
-    const long long *offp;      // [n+1] prefix sums of n1r + 1 (orders 0..n1 per radius)
-    long long totp;             // offp[n]
-    int ntiles;                 // order tiles of K1b over all radii
-    const double *fv;           // [4*(n1+2)]: fv1 | fv2 | fv3 | fv4
-    const double *mu, *wq;      // [n_qang] Gauss nodes (ascending) and weights
-    const double *gl_guess;     // [(n_qang+1)/2] Newton starting points for the nodes
-    const double *gl_jr;        // [n_qang] j / (j + 1.) for the Legendre recurrence of the nodes
-    const double *rc;           // [8*n_coef] per-order GSF/Legendre recurrence coefficients
+    const cplx *m_l;            // [ncase * nd]
+    const double *lambda_l;     // [ncase * nd]
+    const int *rcase;           // [R] case of each radius
+    const double *x;            // [R] size parameters
+    const double *xl;           // [nd1][R] d x / d p for index1 slot k
+    const double *w;            // [(1 + nd)][R] row 0: f = nr qw; row 1+kk: f_l (index1) or f_l2 (index2)
+    const int *n1r, *n2r;       // [R]
+    const long long *off;       // [R+1] prefix sums of n1r (coefficient storage)
+    const long long *offp;      // [R+1] prefix sums of n1r + 1 (recurrence storage)
+    long long tot, totp;
+    int ntiles;                 // K1b tiles over all radii
+    const double *fv;           // [4][n1max + 2]: fv1 | fv2 | fv3 | fv4
+    const double *rc;           // [8 * ncmax] GSF/Legendre recurrence coefficients per order
+    const double *mu_pool;      // Gauss pool: n nodes then n weights at DevCase.mu_off
+    const double *mu_user;      // user-angle cosines (DevCase.mu_user_off)
 };
 
 // Coefficient columns: column 0 = value, column 1+k = index1 slot k.  Entry
 // (col, off[r] + j - 1) holds {Re cs, Im cs, Re cd, Im cd} with
 // cs = fv4_j (a_j + b_j), cd = fv4_j (a_j - b_j).
-// Per-radius sums rs[(col*5 + q)*n + r], q: se, ss, Re sb, Im sb, sg.
+// Per-radius sums rs[(col*5 + q)*R + r], q: se, ss, Re sb, Im sb, sg.
 
-// guess[i]: cos(t_i + da / tan t_i), t_i = (4i+3) pi / (4n+2), computed on the host
-int launch_gauss(cudaStream_t s, int n, const double *guess, const double *jr, double *mu, double *wq);
+// Gauss-Legendre nodes of npairs root pairs: pair p belongs to order
+// n = ns[pt[p]] and is root pi[p]; that order's n nodes and then n weights
+// start at pool + mo[pt[p]], its host starting points at guess + go[pt[p]].
+int launch_gauss(cudaStream_t s, int npairs, const int *pt, const int *pi, const int *ns,
+                 const long long *mo, const long long *go, const double *guess, const double *jr,
+                 double *pool);
 
-// K1 for one chunk of nc tangent-linear columns starting at index1 slot c0:
-// sequential recurrences into rec, then a_n/b_n tiles (tiles[i] = {radius,
-// first order}) into coef and the tile partial sums rsp[(col*5+q)*ntiles + tile].
-int launch_coef(cudaStream_t s, const DevProblem &P, int nc, int c0, int write_value, const int2 *tiles,
+// K1 for one chunk of nc tangent-linear columns starting at index1 slot c0.
+int launch_coef(cudaStream_t s, const DevBatch &B, int nc, int c0, int write_value, const int2 *tiles,
                 double4 *rec, double *coef, double *rsp);
-// rs[(col*5+q)*n + r] = sum of the tile partials of radius r (tiles tstart[r]..tstart[r+1]-1)
-int launch_tile_reduce(cudaStream_t s, const DevProblem &P, const int *tstart, const double *rsp, double *rs);
+int launch_tile_reduce(cudaStream_t s, const DevBatch &B, const int *tstart, const double *rsp, double *rs);
 
-int launch_reduce_scalars(cudaStream_t s, const DevProblem &P, const double *rs,
-                          double *sums, double *save1);
+// K2: sums[case][(1+nd)][4] (unnormalised), save1 [4][R] for save_control 1
+int launch_reduce_scalars(cudaStream_t s, const DevBatch &B, const double *rs, double *sums, double *save1);
 
-int launch_angular(cudaStream_t s, const DevProblem &P, int nc1, int c1base, int nc2,
-                   int c2base, int first, int n_groups, const int *gstart,
-                   const double *coef, double *part, double *save2);
-
-// half-angles one K3 block covers for a chunk of nc1 index1 columns
+// K3 work item: one block of half-angles of one case over a radius range.
+struct AngItem {
+    int c, xt, g, rbeg, rend;
+};
 int angular_angles_per_block(int nc1);
-
-int launch_reduce_pf(cudaStream_t s, const DevProblem &P, int n_groups, const double *part,
-                     double *pfacc);
-
-int launch_save_reweight(cudaStream_t s, const DevProblem &P, const double *save1,
+int launch_angular(cudaStream_t s, const DevBatch &B, int nc1, int c1base, int nc2, int c2base, int first,
+                   int nitems, const AngItem *items, const double *coef, double *part, double *save2);
+// per-case element lists: element e of the flat index space belongs to the
+// case c with start[c] <= e < start[c+1] (start has ncase + 1 entries)
+int launch_reduce_pf(cudaStream_t s, const DevBatch &B, long long total, const long long *start,
+                     const double *part, double *pfacc);
+// save_control 2, batch of one case with n_qang angles
+int launch_save_reweight(cudaStream_t s, const DevBatch &B, int n_qang, const double *save1,
                          const double *save2, const double *w2, double *sums, double *pfacc);
+int launch_normalize(cudaStream_t s, const DevBatch &B, long long total, const long long *start,
+                     const double *sums, const double *pfacc, double *scal, double *pfn);
 
-int launch_normalize(cudaStream_t s, const DevProblem &P, const double *sums,
-                     const double *pfacc, double *scal_out, double *pfn);
+// K4: expansion over Gauss angles.  kind 0: GSF, 1: Legendre.
+constexpr int EX_LT = 64;       // orders per tile
+constexpr int EX_AT = 32;       // half-angles per tile
+struct ExpItem {
+    int c, lt, at;              // case, order tile, angle tile
+};
+// ck_start: flat (case, half-angle, function) checkpoint-thread index space;
+// fin_start: flat (case, column, order) index space of the finalisation.
+int launch_expand(cudaStream_t s, const DevBatch &B, int kind, long long nck,
+                  const long long *ck_start, int nitems, const ExpItem *items, long long nfin,
+                  const long long *fin_start, const double *pfn, double *ckpt, double *exq,
+                  double *coefs, int *trunc);
 
-// Expansion of the normalised phase matrix over Gauss angles.  kind 0: GSF
-// (alpha/beta coefficients), kind 1: Legendre.
-int launch_expand(cudaStream_t s, const DevProblem &P, int kind, int lchunk, double accuracy,
-                  const double *pfn, double *state, double *tab, double *raw, double *coefs,
-                  int *trunc);
-
-int launch_phase_user(cudaStream_t s, const DevProblem &P, int kind, const double *coefs,
-                      const int *trunc, const double *mu_user, double *pf_out);
+// K5: flat (case, column, user angle) index space.
+int launch_phase_user(cudaStream_t s, const DevBatch &B, int kind, long long total, const long long *start,
+                      const double *coefs, const int *trunc, double *pf_out);

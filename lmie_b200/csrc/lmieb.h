@@ -69,8 +69,15 @@ typedef struct {
      double *save2;             /* [4*n*n_qang] (save_control 1) or NULL */
 } lmieb_result;
 
-/* Runs the device solve.  Returns 0 or -1 (after printing "ERROR: ..."). */
+/* Runs the device solve of one problem.  Returns 0 or -1 (after printing
+ * "ERROR: ..."). */
 int lmieb_device_solve(const lmieb_problem *p, lmieb_result *r);
+
+/* Runs n problems as batches on the device.  All problems must share the
+ * derivative layout (nd, idx1, idx2), the requested outputs (want_gc,
+ * want_lc, pf_from) and use save_control 0 when n > 1.  The cases are cut
+ * into sub-batches that fit the device memory budget. */
+int lmieb_device_solve_batch(int n, const lmieb_problem *p, lmieb_result *r);
 
 /* Device timing of the last lmieb_device_solve (ms per stage), for bench.py. */
 int lmieb_last_timing(double *ms, int n);

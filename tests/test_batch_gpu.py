@@ -1,0 +1,67 @@
+"""lmie_solution_batch: many independent cases in batched device launches.
+
+Every case of a batch must give what lmie_solution gives for it alone, and
+what the reference gives: the batch changes only how work is grouped on the
+device (radius groups, summation order), so results agree to the parity
+tolerance."""
+import dataclasses
+
+import numpy as np
+import pytest
+
+import libs
+from cases import all_cases, small_cases
+from lmie_b200 import abi, workloads
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10
+
+
+def _assert_close(got, want, tol, label):
+    assert got.rc == 0, label
+    err = libs.compare(got, want)
+    assert err["n_coef"] <= 1, (label, got.n_coef, want.n_coef)
+    bad = {k: v for k, v in err.items() if k != "n_coef" and v > tol}
+    assert not bad, (label, bad)
+
+
+def test_batch_of_mixed_cases_matches_reference():
+    """Cases with different distributions, derivative layouts and output
+    flags in one call: grouped into compatible device batches."""
+    names = [n for n in small_cases() if n != "save1"] + ["example", "x1000_few_radii"]
+    cases = [all_cases()[n] for n in names]
+    got = abi.solve_batch(libs.product(), cases, n_threads=8)
+    for n, g in zip(names, got):
+        _assert_close(g, libs.golden(n), TOL, n)
+
+
+def test_uneven_batch_matches_single_solves():
+    """A slice of the seeded uneven workload (size parameters 0.2..1000)."""
+    cases = workloads.batched_uneven(96)
+    got = abi.solve_batch(libs.product(), cases, n_threads=8)
+    for i, (c, g) in enumerate(zip(cases, got)):
+        _assert_close(g, libs.run_product(c), 1e-12, f"case {i}")
+
+
+def test_uneven_batch_matches_oracle():
+    cases = [c for c in workloads.batched_uneven(64) if 2 * np.pi * c.r2 / c.lam < 60][:12]
+    assert len(cases) >= 6
+    got = abi.solve_batch(libs.product(), cases, n_threads=4)
+    for i, (c, g) in enumerate(zip(cases, got)):
+        _assert_close(g, libs.run_oracle(c), TOL, f"case {i}")
+
+
+def test_batch_with_save_control_case():
+    """A save_control case inside a batch is solved on its own."""
+    cases = [all_cases()["gamma"], all_cases()["save1"], all_cases()["c1"]]
+    got = abi.solve_batch(libs.product(), cases, n_threads=2)
+    for n, g in zip(["gamma", "save1", "c1"], got):
+        _assert_close(g, libs.golden(n), TOL, n)
+
+
+def test_batch_reports_bad_case():
+    cases = [all_cases()["c1"], dataclasses.replace(all_cases()["c1"], calc_gc=0, calc_lc=0)]
+    cases[1] = dataclasses.replace(cases[1], calc_pf=1)
+    got = abi.solve_batch(libs.product(), cases, n_threads=2)
+    assert got[0].rc == -1
