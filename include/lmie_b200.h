@@ -27,6 +27,34 @@ extern "C" {
 int lmie_solution_batch(int n_cases, lmie_in_data *in, lmie_out_data *out, int alloc_out,
                         int verbose, int n_threads);
 
+/* Arithmetic of the batched solve.
+ * LMIEB_PRECISION_FP64: every stage in FP64, the reference's arithmetic
+ *   (within 1e-10 of it); lmie_solution and lmie_solution_batch use it.
+ * LMIEB_PRECISION_TF32X3: the angular S1/S2 contraction runs on the tensor
+ *   cores with each operand split into two TF32 terms (lo*hi + hi*lo + hi*hi),
+ *   FP32 accumulation over segments of 64 orders and a double-float sum of
+ *   the segments; the Mie recurrences, a_n/b_n, the phase-matrix quadratic
+ *   forms, the radius sums, the normalisation and the expansions stay FP64.
+ *   The phase matrix then carries a relative error of a few 1e-7 of its
+ *   largest element.  Problems this mode does not cover (save_control != 0,
+ *   more than 4 index1 or 3 index2 derivative slots) run in FP64. */
+#define LMIEB_PRECISION_FP64 0
+#define LMIEB_PRECISION_TF32X3 1
+
+/* lmie_solution_batch with the arithmetic chosen by `precision`. */
+int lmie_solution_batch2(int n_cases, lmie_in_data *in, lmie_out_data *out, int alloc_out,
+                         int verbose, int n_threads, int precision);
+
+/* Checks the tensor-core contraction machinery on the device: a 128 x 64
+ * product over K orders (K a positive multiple of 16, at most 4096) of seeded
+ * random operands through the operand split, shared-memory layout,
+ * descriptors, tcgen05.mma issue and tensor-memory reads of the
+ * split-precision angular stage, with one FP32 accumulation over all of K
+ * (the stage itself sums segments of 64 orders in double-float), against an
+ * FP64 product on the host.  Writes the largest error relative to the
+ * largest element of the product.  Returns 0 or -1. */
+int lmieb_tc_selftest(int K, double *max_rel_err);
+
 /* Stages of one solve, timed with CUDA events when timing is on:
  * 0 upload, 1 Mie recurrences and coefficients (K1), 2 radius reduction of
  * the cross sections (K2), 3 angular accumulation (K3), 4 normalisation,

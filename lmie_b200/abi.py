@@ -275,16 +275,22 @@ def deriv_unit(*names: str) -> List[Dict[str, float]]:
     return [{n: 1.0} for n in names]
 
 
-def solve_batch(lib: C.CDLL, cases: Sequence[Case], n_threads: int = 8) -> List[Result]:
-    """Solve many cases with one lmie_solution_batch() call."""
+PRECISION_FP64 = 0      # LMIEB_PRECISION_FP64
+PRECISION_TF32X3 = 1    # LMIEB_PRECISION_TF32X3
+
+
+def solve_batch(lib: C.CDLL, cases: Sequence[Case], n_threads: int = 8,
+                precision: int = PRECISION_FP64) -> List[Result]:
+    """Solve many cases with one lmie_solution_batch2() call."""
     n = len(cases)
     blocks = [InputBlock(c) for c in cases]
     ins = (lmie_in_data * n)(*[b.s for b in blocks])
     outs = (lmie_out_data * n)()
-    f = lib.lmie_solution_batch
+    f = lib.lmie_solution_batch2
     f.restype = C.c_int
-    f.argtypes = [C.c_int, C.POINTER(lmie_in_data), C.POINTER(lmie_out_data), C.c_int, C.c_int, C.c_int]
-    rc = f(n, ins, outs, 1, 0, n_threads)
+    f.argtypes = [C.c_int, C.POINTER(lmie_in_data), C.POINTER(lmie_out_data), C.c_int, C.c_int, C.c_int,
+                  C.c_int]
+    rc = f(n, ins, outs, 1, 0, n_threads, precision)
     if rc != 0:
         return [Result(rc=rc) for _ in cases]
     res = []

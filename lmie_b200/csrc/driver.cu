@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "kernels.h"
+#include "tc_layout.cuh"
 #include "lmieb.h"
 #include "../../include/lmie_b200.h"
 
@@ -85,6 +86,9 @@ struct Plan {
     double *pfacc = nullptr, *pfn = nullptr, *ckpt = nullptr, *exq = nullptr;
     AngItem *ang = nullptr;
     int n_ang = 0;
+    int tc = 0;                 // K3 in split precision on the tensor cores
+    float *bop = nullptr;       // its B operand (tc_layout.cuh)
+    size_t bop_bytes = 0;
     ExpItem *ex = nullptr;
     int n_ex = 0;
     long long *pf_start = nullptr, *ck_gc = nullptr, *ck_lc = nullptr, *fin_start = nullptr, *pu_start = nullptr;
@@ -184,16 +188,20 @@ int run_kernels(Plan &L) {
     const DevBatch &B = L.B;
     stage(1);
     if (L.save_control != 2) {
+        if (L.tc) LMIEB_CUDA_TRY(cudaMemsetAsync(L.bop, 0, L.bop_bytes, s));
         for (int ch = 0; ch < (L.nd1c > 0 ? L.nd1c : 1); ++ch) {
             const int c0 = ch * 4;
             const int nc = std::max(0, std::min(4, B.nd1 - c0));
-            if (launch_coef(s, B, nc, c0, ch == 0, L.tiles, L.rec, L.coef, L.rsp)) return -1;
+            if (launch_coef(s, B, nc, c0, ch == 0, L.tiles, L.rec, L.coef, L.bop, L.rsp)) return -1;
         }
         if (launch_tile_reduce(s, B, L.tstart, L.rsp, L.rs)) return -1;
         stage(2);
         if (launch_reduce_scalars(s, B, L.rs, L.sums, L.save_control == 1 ? L.o_save1 : nullptr)) return -1;
         stage(3);
-        if (L.n_ang > 0) {
+        if (L.n_ang > 0 && L.tc) {
+            if (launch_angular_tc(s, B, L.n_ang, L.ang, L.bop, L.part, L.o_trunc + 2 * L.ncase)) return -1;
+            if (launch_reduce_pf(s, B, L.pf_total, L.pf_start, L.part, L.pfacc)) return -1;
+        } else if (L.n_ang > 0) {
             for (int t = 0; t < L.n_ang_launch; ++t) {
                 const int c1 = t * 4, c2 = t * 4;
                 const int nc1 = std::max(0, std::min(4, B.nd1 - c1));
@@ -391,10 +399,83 @@ int solve_sub(int ncase, const lmieb_problem *ps, lmieb_result *rs_out) {
     }
 
     // ---- angular work items (largest first), partial and pf offsets ----
+    bool any_ang = false;
+    for (int k = 0; k < ncase; ++k) any_ang |= cs[k].n_qang > 0;
+    L.tc = p0.precision == LMIEB_PRECISION_TF32X3 && L.save_control == 0 && any_ang && nd1 <= TC_MAX_NC1 &&
+           nd2 <= TC_MAX_ND2;
     std::vector<AngItem> ang;
     std::vector<long long> pf_start(ncase + 1, 0);
     long long part_total = 0;
-    {
+    // split precision: radius groups of tc_rg(nd1) radii, each with its B operand block
+    std::vector<int> tc_pos, tg_r0, tg_n, tg_nk;
+    std::vector<long long> tc_roff, tg_off;
+    long long bop_floats = 0;
+    if (L.tc) {
+        const int RG = tc_rg(nd1);
+        tc_pos.assign(R, 0);
+        tc_roff.assign(R, 0);
+        std::vector<int> cg0(ncase + 1, 0);
+        std::vector<double> wc(ncase, 0.);
+        double W = 0.;
+        for (int k = 0; k < ncase; ++k) {
+            const DevCase &C = cs[k];
+            cg0[k] = (int) tg_r0.size();
+            for (int r = C.r0; r < C.r0 + C.nr; r += RG) {
+                const int n = std::min(RG, C.r0 + C.nr - r);
+                int mx = 1;
+                for (int i = 0; i < n; ++i) {
+                    mx = std::max(mx, n1r[r + i]);
+                    tc_pos[r + i] = i;
+                    tc_roff[r + i] = bop_floats;
+                }
+                const int nk = (mx + TC_KC - 1) / TC_KC;
+                tg_r0.push_back(r);
+                tg_n.push_back(n);
+                tg_nk.push_back(nk);
+                tg_off.push_back(bop_floats);
+                bop_floats += (long long) nk * (TC_BSTAGE / 4);
+                wc[k] += nk + 1;                       // chunks, plus one for the group's epilogue
+            }
+            if (C.n_qang > 0) W += wc[k] * ((C.nh + TC_HALF - 1) / TC_HALF);
+        }
+        cg0[ncase] = (int) tg_r0.size();
+        const double wt = std::max(W / (2. * c.sms), 8.);    // chunks per item
+        std::vector<std::pair<double, AngItem>> tmp;
+        for (int k = 0; k < ncase; ++k) {
+            DevCase &C = cs[k];
+            pf_start[k + 1] = pf_start[k] + (long long) Q * C.n_qang;
+            C.pf_off = pf_start[k];
+            if (C.n_qang <= 0) { C.G = 0; continue; }
+            const int ng = cg0[k + 1] - cg0[k];
+            const int xt = (C.nh + TC_HALF - 1) / TC_HALF;
+            int G = (int) std::lround(wc[k] / wt);
+            G = std::max(1, std::min(G, ng));
+            std::vector<int> gs(G + 1, cg0[k + 1]);
+            gs[0] = cg0[k];
+            double run = 0.;
+            int gi = 1;
+            for (int g = cg0[k]; g < cg0[k + 1] && gi < G; ++g) {
+                run += tg_nk[g] + 1;
+                if (run * G >= wc[k] * gi) gs[gi++] = g + 1;
+            }
+            for (int g = 1; g <= G; ++g) gs[g] = std::max(gs[g], gs[g - 1]);
+            gs.erase(std::unique(gs.begin(), gs.end()), gs.end());   // every partial slot gets a range
+            G = (int) gs.size() - 1;
+            C.G = G;
+            C.part_off = part_total;
+            part_total += (long long) G * Q * C.n_qang;
+            for (int g = 0; g < G; ++g) {
+                double cost = 0.;
+                for (int gg = gs[g]; gg < gs[g + 1]; ++gg) cost += tg_nk[gg] + 1;
+                for (int t = 0; t < xt; ++t) tmp.push_back({cost, AngItem{k, t, g, gs[g], gs[g + 1]}});
+            }
+        }
+        std::stable_sort(tmp.begin(), tmp.end(), [](const std::pair<double, AngItem> &a,
+                                                    const std::pair<double, AngItem> &b) { return a.first > b.first; });
+        for (auto &e : tmp) ang.push_back(e.second);
+        L.pf_total = pf_start[ncase];
+        L.n_ang = (int) ang.size();
+    } else {
         const int per = angular_angles_per_block(std::min(nd1, 4));
         double W = 0.;
         std::vector<double> wc(ncase, 0.);
@@ -527,6 +608,8 @@ int solve_sub(int ncase, const lmieb_problem *ps, lmieb_result *rs_out) {
         add(tiles.size() * 8); add(fv.size() * 8); add(rc.size() * 8); add(ml.size() * 16); add(laml.size() * 8);
         add((size_t) nd1 * 4); add((size_t) nd2 * 4); add(mu_user.size() * 8);
         add(ang.size() * sizeof(AngItem)); add(ex.size() * sizeof(ExpItem));
+        add(tc_pos.size() * 4); add(tc_roff.size() * 8); add(tg_r0.size() * 4); add(tg_n.size() * 4);
+        add(tg_nk.size() * 4); add(tg_off.size() * 8);
         for (int q = 0; q < 5; ++q) add((size_t) (ncase + 1) * 8);
         add(gl_ns.size() * 4); add(gl_mo.size() * 8); add(gl_go.size() * 8); add(gl_pt.size() * 4);
         add(gl_pi.size() * 4); add(gl_guess.size() * 8); add(gl_jr.size() * 8);
@@ -535,7 +618,7 @@ int solve_sub(int ncase, const lmieb_problem *ps, lmieb_result *rs_out) {
     size_t out_bytes = 0;
     {
         auto add = [&](size_t b) { out_bytes += pad(b); };
-        add(o_scal * 8); add(o_gc * 8); add(o_lc * 8); add(o_pf * 8); add((size_t) 2 * ncase * 4);
+        add(o_scal * 8); add(o_gc * 8); add(o_lc * 8); add(o_pf * 8); add((size_t) (2 * ncase + 1) * 4);
         if (L.save_control == 1) { add((size_t) 4 * R * 8); add(n_save2 * 8); }
     }
     if (ensure_host(in_bytes + out_bytes)) return -1;
@@ -561,6 +644,12 @@ int solve_sub(int ncase, const lmieb_problem *ps, lmieb_result *rs_out) {
     double *h_mu = put(hp, ho, mu_user.data(), mu_user.size());
     AngItem *h_ang = put(hp, ho, ang.data(), ang.size());
     ExpItem *h_ex = put(hp, ho, ex.data(), ex.size());
+    int *h_tcpos = put(hp, ho, tc_pos.data(), tc_pos.size());
+    long long *h_tcroff = put(hp, ho, tc_roff.data(), tc_roff.size());
+    int *h_tgr0 = put(hp, ho, tg_r0.data(), tg_r0.size());
+    int *h_tgn = put(hp, ho, tg_n.data(), tg_n.size());
+    int *h_tgnk = put(hp, ho, tg_nk.data(), tg_nk.size());
+    long long *h_tgoff = put(hp, ho, tg_off.data(), tg_off.size());
     long long *h_pfs = put(hp, ho, pf_start.data(), pf_start.size());
     long long *h_ckg = put(hp, ho, ck_gc.data(), ck_gc.size());
     long long *h_ckl = put(hp, ho, ck_lc.data(), ck_lc.size());
@@ -593,7 +682,8 @@ int solve_sub(int ncase, const lmieb_problem *ps, lmieb_result *rs_out) {
         if (L.save_control != 2) {
             add((size_t) (1 + nd1) * (size_t) totp * 32);
             add((size_t) (1 + nd1) * 5 * (size_t) ntiles * 8);
-            add((size_t) (1 + nd1) * (size_t) tot * 32);
+            if (L.tc) add((size_t) bop_floats * 4);
+            else add((size_t) (1 + nd1) * (size_t) tot * 32);
             add((size_t) (1 + nd1) * 5 * (size_t) R * 8);
             add((size_t) part_total * 8);
         }
@@ -639,6 +729,14 @@ int solve_sub(int ncase, const lmieb_problem *ps, lmieb_result *rs_out) {
     B.rc = (const double *) dptr(h_rc);
     B.mu_pool = c.gl_pool;
     B.mu_user = (const double *) dptr(h_mu);
+    if (L.tc) {
+        B.tc_pos = (const int *) dptr(h_tcpos);
+        B.tc_roff = (const long long *) dptr(h_tcroff);
+        B.tg_r0 = (const int *) dptr(h_tgr0);
+        B.tg_n = (const int *) dptr(h_tgn);
+        B.tg_nk = (const int *) dptr(h_tgnk);
+        B.tg_off = (const long long *) dptr(h_tgoff);
+    }
     L.tiles = (int2 *) dptr(h_tiles);
     L.tstart = (int *) dptr(h_tstart);
     L.ang = (AngItem *) dptr(h_ang);
@@ -656,7 +754,12 @@ int solve_sub(int ncase, const lmieb_problem *ps, lmieb_result *rs_out) {
     if (L.save_control != 2) {
         L.rec = A.take<double4>((size_t) (1 + nd1) * (size_t) totp);
         L.rsp = A.take<double>((size_t) (1 + nd1) * 5 * (size_t) ntiles);
-        L.coef = A.take<double>((size_t) (1 + nd1) * (size_t) tot * 4);
+        if (L.tc) {
+            L.bop_bytes = (size_t) bop_floats * 4;
+            L.bop = A.take<float>((size_t) bop_floats);
+        } else {
+            L.coef = A.take<double>((size_t) (1 + nd1) * (size_t) tot * 4);
+        }
         L.rs = A.take<double>((size_t) (1 + nd1) * 5 * (size_t) R);
         L.part = A.take<double>((size_t) part_total);
     }
@@ -672,13 +775,13 @@ int solve_sub(int ncase, const lmieb_problem *ps, lmieb_result *rs_out) {
         L.o_gc = (double *) take(o_gc * 8);
         L.o_lc = (double *) take(o_lc * 8);
         L.o_pf = (double *) take(o_pf * 8);
-        L.o_trunc = (int *) take((size_t) 2 * ncase * 4);
+        L.o_trunc = (int *) take((size_t) (2 * ncase + 1) * 4);   // gc, lc truncations; error word
         if (L.save_control == 1) {
             L.o_save1 = (double *) take((size_t) 4 * R * 8);
             L.o_save2 = (double *) take(n_save2 * 8);
         }
     }
-    if (!L.sums || !L.pfn || !L.exq || (L.save_control != 2 && !L.part)) {
+    if (!L.sums || !L.pfn || !L.exq || (L.save_control != 2 && !L.part) || (L.tc && !L.bop)) {
         fprintf(stderr, "ERROR: lmie_b200: device arena too small\n");
         return -1;
     }
@@ -716,6 +819,10 @@ int solve_sub(int ncase, const lmieb_problem *ps, lmieb_result *rs_out) {
     const double *hl = (const double *) hostp(L.o_lc);
     const double *hpf = (const double *) hostp(L.o_pf);
     const int *htr = (const int *) hostp(L.o_trunc);
+    if (htr[2 * ncase]) {
+        fprintf(stderr, "ERROR: lmie_b200: the tensor-core angular stage timed out waiting for its pipeline\n");
+        return -1;
+    }
     for (int k = 0; k < ncase; ++k) {
         const DevCase &C = cs[k];
         lmieb_result &r = rs_out[k];
@@ -738,7 +845,8 @@ int check_uniform(int n, const lmieb_problem *p) {
     for (int k = 1; k < n; ++k) {
         bool same = p[k].nd == p[0].nd && p[k].nd1 == p[0].nd1 && p[k].nd2 == p[0].nd2 &&
                     p[k].want_gc == p[0].want_gc && p[k].want_lc == p[0].want_lc &&
-                    p[k].pf_from == p[0].pf_from && p[k].save_control == 0 && p[0].save_control == 0;
+                    p[k].pf_from == p[0].pf_from && p[k].save_control == 0 && p[0].save_control == 0 &&
+                    p[k].precision == p[0].precision;
         for (int q = 0; same && q < p[0].nd1; ++q) same = p[k].idx1[q] == p[0].idx1[q];
         for (int q = 0; same && q < p[0].nd2; ++q) same = p[k].idx2[q] == p[0].idx2[q];
         if (!same) {
@@ -876,5 +984,60 @@ extern "C" int lmieb_stream(void **stream) {
     std::lock_guard<std::mutex> lock(g_mu);
     if (ensure_ready()) return -1;
     *stream = (void *) g_ctx.stream;
+    return 0;
+}
+
+extern "C" int lmieb_tc_selftest(int K, double *max_rel_err) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    if (K <= 0 || K % TC_KC || K > 4096 || !max_rel_err) {
+        fprintf(stderr, "ERROR: lmieb_tc_selftest: K must be a positive multiple of %d, at most 4096\n", TC_KC);
+        return -1;
+    }
+    if (ensure_ready()) return -1;
+    const int M = TC_M, N = TC_NP;   // one product tile
+    std::vector<double> a((size_t) M * K), b((size_t) N * K), d((size_t) M * N), ref((size_t) M * N, 0.);
+    // seeded operands with the spread of magnitudes of the angular products
+    unsigned long long st = 0x9E3779B97F4A7C15ull;
+    auto rnd = [&]() {
+        st ^= st << 13; st ^= st >> 7; st ^= st << 17;
+        return (double) (st >> 11) * (1. / 9007199254740992.) * 2. - 1.;
+    };
+    for (int i = 0; i < M; ++i)
+        for (int k = 0; k < K; ++k) a[(size_t) i * K + k] = rnd() * (k + 1.);
+    for (int n = 0; n < N; ++n)
+        for (int k = 0; k < K; ++k) b[(size_t) n * K + k] = rnd() / (k + 1.) * exp(-4. * k / K);
+    double mx = 0.;
+    for (int i = 0; i < M; ++i)
+        for (int n = 0; n < N; ++n) {
+            double s = 0.;
+            for (int k = 0; k < K; ++k) s += a[(size_t) i * K + k] * b[(size_t) n * K + k];
+            ref[(size_t) i * N + n] = s;
+            mx = std::max(mx, fabs(s));
+        }
+    double *da = nullptr, *db = nullptr, *dd = nullptr;
+    int *derr = nullptr, herr = 0;
+    cudaStream_t s = g_ctx.stream;
+    int rc = -1;
+    if (cudaMalloc((void **) &da, a.size() * 8) == cudaSuccess && cudaMalloc((void **) &db, b.size() * 8) == cudaSuccess &&
+        cudaMalloc((void **) &dd, d.size() * 8) == cudaSuccess && cudaMalloc((void **) &derr, 4) == cudaSuccess &&
+        cudaMemcpyAsync(da, a.data(), a.size() * 8, cudaMemcpyHostToDevice, s) == cudaSuccess &&
+        cudaMemcpyAsync(db, b.data(), b.size() * 8, cudaMemcpyHostToDevice, s) == cudaSuccess &&
+        cudaMemsetAsync(derr, 0, 4, s) == cudaSuccess && launch_tc_selftest(s, K, da, db, dd, derr) == 0 &&
+        cudaMemcpyAsync(d.data(), dd, d.size() * 8, cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+        cudaMemcpyAsync(&herr, derr, 4, cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+        cudaStreamSynchronize(s) == cudaSuccess)
+        rc = 0;
+    cudaFree(da); cudaFree(db); cudaFree(dd); cudaFree(derr);
+    if (rc) {
+        fprintf(stderr, "ERROR: lmieb_tc_selftest: %s\n", cudaGetErrorString(cudaGetLastError()));
+        return -1;
+    }
+    if (herr) {
+        fprintf(stderr, "ERROR: lmieb_tc_selftest: the tensor-core pipeline timed out\n");
+        return -1;
+    }
+    double e = 0.;
+    for (size_t i = 0; i < d.size(); ++i) e = std::max(e, fabs(d[i] - ref[i]));
+    *max_rel_err = mx > 0. ? e / mx : e;
     return 0;
 }

@@ -5,6 +5,7 @@
 #define LMIEB_HOST_H
 
 #include "../../include/lmie_interface.h"
+#include "../../include/lmie_b200.h"
 #include "lmieb.h"
 
 #ifdef __cplusplus

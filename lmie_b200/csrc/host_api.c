@@ -725,12 +725,21 @@ static int jobs_compatible(const case_job *a, const case_job *b) {
 
 int lmie_solution_batch(int n_cases, lmie_in_data *in, lmie_out_data *out, int alloc_out,
                         int verbose, int n_threads) {
+     return lmie_solution_batch2(n_cases, in, out, alloc_out, verbose, n_threads, LMIEB_PRECISION_FP64);
+}
+
+int lmie_solution_batch2(int n_cases, lmie_in_data *in, lmie_out_data *out, int alloc_out,
+                         int verbose, int n_threads, int precision) {
      case_job *jobs;
      lmieb_problem *P;
      lmieb_result *R;
      int *done, i, k, rc = 0;
      if (n_cases <= 0)
           return 0;
+     if (precision != LMIEB_PRECISION_FP64 && precision != LMIEB_PRECISION_TF32X3) {
+          fprintf(stderr, "ERROR: lmie_solution_batch2(): unknown precision %d\n", precision);
+          return -1;
+     }
      if (alloc_out) {
           for (i = 0; i < n_cases; ++i) {
                int max_coef = lmie_calc_max_coef(in[i].lambda, in[i].dist_type, in[i].a1, in[i].a2,
@@ -762,6 +771,7 @@ int lmie_solution_batch(int n_cases, lmie_in_data *in, lmie_out_data *out, int a
                if (done[k] || (k != i && !jobs_compatible(&jobs[i], &jobs[k])))
                     continue;
                P[m] = jobs[k].P;
+               P[m].precision = precision;
                R[m] = jobs[k].R;
                done[k] = m + 1;
                ++m;

@@ -24,6 +24,7 @@
 #include <cstdio>
 
 #include "kernels.h"
+#include "tc_layout.cuh"
 
 namespace {
 
@@ -254,7 +255,8 @@ template <int NC>
 __global__ void __launch_bounds__(ABT) k_abcoef(DevBatch B, int c0, int write_value,
                                                 const int2 *__restrict__ tiles,
                                                 const double4 *__restrict__ rec,
-                                                double *__restrict__ coef, double *__restrict__ rsp) {
+                                                double *__restrict__ coef, float *__restrict__ bop,
+                                                double *__restrict__ rsp) {
     constexpr int CC = 1 + NC;
     __shared__ cplx sab[2 * CC][ABT];
     __shared__ double red[5 * CC][ABT / 32];
@@ -340,11 +342,17 @@ __global__ void __launch_bounds__(ABT) k_abcoef(DevBatch B, int c0, int write_va
             acc[4] = fv3[j] * (re_mulc(a, an) + re_mulc(b, bn)) + fv4[j] * re_mulc(a, b);
         }
         double2 *cf = (double2 *) coef;
+        const int tpos = bop ? B.tc_pos[r] : 0;
+        const long long troff = bop ? B.tc_roff[r] : 0;
         if (write_value) {
             const cplx cs = (a + b) * f4, cd = (a - b) * f4;
-            const size_t o = ((size_t) B.off[r] + j - 1) * 2;
-            cf[o] = make_double2(cs.re, cs.im);
-            cf[o + 1] = make_double2(cd.re, cd.im);
+            if (bop) {
+                tc_put_b(bop, troff, tpos, 1 + B.nd1, 0, j, cs.re, cs.im, cd.re, cd.im);
+            } else {
+                const size_t o = ((size_t) B.off[r] + j - 1) * 2;
+                cf[o] = make_double2(cs.re, cs.im);
+                cf[o + 1] = make_double2(cd.re, cd.im);
+            }
         }
 #pragma unroll
         for (int k = 0; k < NC; ++k) {
@@ -359,9 +367,13 @@ __global__ void __launch_bounds__(ABT) k_abcoef(DevBatch B, int c0, int write_va
                        fv4[j] * (re_mulc(al[k], b) + re_mulc(a, bl[k]));
             }
             const cplx cs = (al[k] + bl[k]) * f4, cd = (al[k] - bl[k]) * f4;
-            const size_t o = (((size_t) (1 + c0 + k)) * tot + (size_t) B.off[r] + j - 1) * 2;
-            cf[o] = make_double2(cs.re, cs.im);
-            cf[o + 1] = make_double2(cd.re, cd.im);
+            if (bop) {
+                tc_put_b(bop, troff, tpos, 1 + B.nd1, 1 + c0 + k, j, cs.re, cs.im, cd.re, cd.im);
+            } else {
+                const size_t o = (((size_t) (1 + c0 + k)) * tot + (size_t) B.off[r] + j - 1) * 2;
+                cf[o] = make_double2(cs.re, cs.im);
+                cf[o + 1] = make_double2(cd.re, cd.im);
+            }
         }
     }
     // block reduction of the 5*CC tile sums (fixed order)
@@ -1129,14 +1141,14 @@ int launch_gauss(cudaStream_t s, int npairs, const int *pt, const int *pi, const
 }
 
 int launch_coef(cudaStream_t s, const DevBatch &B, int nc, int c0, int write_value, const int2 *tiles,
-                double4 *rec, double *coef, double *rsp) {
+                double4 *rec, double *coef, float *bop, double *rsp) {
     const unsigned rb = ceil_div(B.R, 64);
     const unsigned tb = (unsigned) B.ntiles;
     switch (nc) {
 #define LMIEB_K1(NC_)                                                                                    \
     case NC_:                                                                                            \
         k_recur<NC_><<<rb, 64, 0, s>>>(B, c0, write_value, rec);                                         \
-        k_abcoef<NC_><<<tb, ABT, 0, s>>>(B, c0, write_value, tiles, rec, coef, rsp);                    \
+        k_abcoef<NC_><<<tb, ABT, 0, s>>>(B, c0, write_value, tiles, rec, coef, bop, rsp);               \
         break;
     LMIEB_K1(0)
     LMIEB_K1(1)

@@ -51,6 +51,11 @@ struct DevBatch {
     const double *rc;           // [8 * ncmax] GSF/Legendre recurrence coefficients per order
     const double *mu_pool;      // Gauss pool: n nodes then n weights at DevCase.mu_off
     const double *mu_user;      // user-angle cosines (DevCase.mu_user_off)
+    // split-precision K3 (tc_layout.cuh); null in the FP64 form
+    const int *tc_pos;          // [R] position of the radius in its group
+    const long long *tc_roff;   // [R] float offset of the radius' group in the B operand
+    const int *tg_r0, *tg_n, *tg_nk;   // per group: first radius, radii, chunks of TC_KC orders
+    const long long *tg_off;    // per group: float offset of its B operand block
 };
 
 // Coefficient columns: column 0 = value, column 1+k = index1 slot k.  Entry
@@ -66,8 +71,10 @@ int launch_gauss(cudaStream_t s, int npairs, const int *pt, const int *pi, const
                  double *pool);
 
 // K1 for one chunk of nc tangent-linear columns starting at index1 slot c0.
+// With bop set, the coefficients go to the tensor-core B operand
+// (tc_layout.cuh) instead of coef.
 int launch_coef(cudaStream_t s, const DevBatch &B, int nc, int c0, int write_value, const int2 *tiles,
-                double4 *rec, double *coef, double *rsp);
+                double4 *rec, double *coef, float *bop, double *rsp);
 int launch_tile_reduce(cudaStream_t s, const DevBatch &B, const int *tstart, const double *rsp, double *rs);
 
 // K2: sums[case][(1+nd)][4] (unnormalised), save1 [4][R] for save_control 1
@@ -80,6 +87,13 @@ struct AngItem {
 int angular_angles_per_block(int nc1);
 int launch_angular(cudaStream_t s, const DevBatch &B, int nc1, int c1base, int nc2, int c2base, int first,
                    int nitems, const AngItem *items, const double *coef, double *part, double *save2);
+// K3 in split precision on the tensor cores (k_tc.cu).  An item is one case
+// (c), 64 half-angles (xt), a partial slot (g) and the radius groups
+// [rbeg, rend).  err is set when a block gave up waiting.
+int launch_angular_tc(cudaStream_t s, const DevBatch &B, int nitems, const AngItem *items, const float *bop,
+                      double *part, int *err);
+// D[128 x 240] = A[128 x K] B[240 x K]^T through the same tensor-core path
+int launch_tc_selftest(cudaStream_t s, int K, const double *A, const double *Bm, double *D, int *err);
 // per-case element lists: element e of the flat index space belongs to the
 // case c with start[c] <= e < start[c+1] (start has ncase + 1 entries)
 int launch_reduce_pf(cudaStream_t s, const DevBatch &B, long long total, const long long *start,

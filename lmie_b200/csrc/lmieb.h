@@ -56,6 +56,8 @@ typedef struct {
      const double *save1_in;    /* [4*n]            save_control 2 */
      const double *save2_in;    /* [4*n*n_qang]     save_control 2 */
      const double *w2;          /* [nd*n] save_control 2: nr_l qw + nr qw_l per slot */
+
+     int precision;             /* LMIEB_PRECISION_* of include/lmie_b200.h */
 } lmieb_problem;
 
 /* Results, in device column order: column 0 = value, column 1+kk = slot kk. */

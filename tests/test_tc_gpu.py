@@ -1,0 +1,102 @@
+"""Split-precision (3xTF32) angular contraction on the tensor cores.
+
+lmie_solution_batch2(..., LMIEB_PRECISION_TF32X3) runs K3 through tcgen05.mma
+with each operand split into two TF32 terms; everything else stays FP64.  The
+FP64 form of the same library is the reference here: it is pinned to the
+reference implementation at 1e-10 by the parity tests.  The tolerances below
+are stated per output array as max|got - want| / max|want| (the error metric
+of the parity tests):
+  - cross sections, g, reff/veff ...: not touched by K3, identical to FP64;
+  - phase matrix (pf) and its expansions (gc, lc): <= 2e-6;
+  - their derivatives (pf_l, gc_l): <= 1e-4 -- a derivative of a quadratic
+    form cancels where the sums it is formed from do not, so the operand
+    precision (about 22 bits) shows there relative to the derivative's own
+    largest element.
+"""
+import ctypes as C
+import dataclasses
+
+import numpy as np
+import pytest
+
+import libs
+from cases import all_cases
+from lmie_b200 import abi, workloads
+
+pytestmark = pytest.mark.gpu
+
+SCALARS_TOL = 1e-13
+VALUE_TOL = 2e-6
+DERIV_TOL = 1e-4
+
+
+def _both(cases, n_threads=8):
+    lib = libs.product()
+    ref = abi.solve_batch(lib, cases, n_threads=n_threads, precision=abi.PRECISION_FP64)
+    got = abi.solve_batch(lib, cases, n_threads=n_threads, precision=abi.PRECISION_TF32X3)
+    return ref, got
+
+
+def _check(got, want, label):
+    assert got.rc == 0 and want.rc == 0, label
+    err = libs.compare(got, want)
+    scal = {k: v for k, v in err.items()
+            if k not in libs.ARRAYS and k != "n_coef" and v > SCALARS_TOL}
+    assert not scal, (label, scal)
+    for name in ("pf", "gc", "lc"):
+        if name in err:
+            assert err[name] <= VALUE_TOL, (label, name, err[name])
+    for name in ("pf_l", "gc_l", "lc_l"):
+        if name in err:
+            assert err[name] <= DERIV_TOL, (label, name, err[name])
+    return err
+
+
+@pytest.mark.parametrize("K", [16, 64, 256])
+def test_selftest_contraction(K):
+    """One 128 x 128 product through the same operand split, layout,
+    descriptors and tensor-memory reads, against FP64 on the host; a single
+    FP32 accumulation over K, so the bound grows with K."""
+    e = C.c_double(-1.)
+    assert libs.product().lmieb_tc_selftest(K, C.byref(e)) == 0
+    assert 0. <= e.value < 2e-8 * K + 5e-7, e.value
+
+
+def test_selftest_rejects_bad_k():
+    e = C.c_double(-1.)
+    assert libs.product().lmieb_tc_selftest(24, C.byref(e)) == -1
+
+
+@pytest.mark.parametrize("name", ["c1", "c2", "example", "x1000_few_radii"])
+def test_named_cases(name):
+    (ref,), (got,) = _both([all_cases()[name]])
+    _check(got, ref, name)
+
+
+def test_uneven_batch():
+    """A slice of the seeded uneven workload (size parameters up to ~1000,
+    derivatives of mr, mi, r_eff, v_eff)."""
+    cases = workloads.batched_uneven(192)
+    ref, got = _both(cases, n_threads=16)
+    for i, (g, r) in enumerate(zip(got, ref)):
+        _check(g, r, f"case {i}")
+
+
+def test_without_derivatives_and_legendre():
+    """nd = 0 (two operand rows per radius) and the Legendre expansion path."""
+    base = all_cases()["c2"]
+    cases = []
+    for lc in (0, 1):
+        cases.append(dataclasses.replace(base, derivs=[], calc_lc=lc, calc_gc=1 - lc))
+    ref, got = _both(cases)
+    for i, (g, r) in enumerate(zip(got, ref)):
+        _check(g, r, f"variant {i}")
+
+
+def test_split_mode_is_deterministic():
+    cases = workloads.batched_uneven(32)
+    lib = libs.product()
+    a = abi.solve_batch(lib, cases, n_threads=8, precision=abi.PRECISION_TF32X3)
+    b = abi.solve_batch(lib, cases, n_threads=8, precision=abi.PRECISION_TF32X3)
+    for x, y in zip(a, b):
+        assert np.array_equal(x.pf, y.pf) and np.array_equal(x.gc, y.gc)
