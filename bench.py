@@ -18,8 +18,15 @@ from disk.
          copies and the scatter into the caller's lmie_out_data are inside the
          timed region.
 
-A second measurement, `single_case`, is the reference's cloud-droplet case
-(2000 radii, x_max ~436, 4 derivatives) through lmie_solution().
+The same JSON line carries secondary measurements of the same run:
+  split_tf32x3  the batch with the angular contraction on the tensor cores
+                (lmie_solution_batch2(..., LMIEB_PRECISION_TF32X3)): device and
+                e2e solves/s, stage times, and its measured error against the
+                FP64 form per output array over a sample of the batch;
+  plain         the drop-in form: one lmie_solution() call per case (FP64),
+                e2e solves/s over a sample of the batch;
+  single_case   the reference's cloud-droplet case (2000 radii, x_max ~436,
+                4 derivatives) through lmie_solution().
 
 With N > 1 (torchrun, one process per GPU) every rank solves its own batch
 (independent cases, no data-path collective): weak scaling.
@@ -39,6 +46,8 @@ import sys
 import threading
 import time
 from pathlib import Path
+
+import numpy as np
 
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
@@ -136,15 +145,15 @@ class CBatch:
             mc = lib.lmie_calc_max_coef(c.lam, self.ins[i].dist_type, c.a1, c.a2, c.a3, c.r1, c.r2)
             lib.lmie_out_alloc(C.byref(self.ins[i]), C.byref(self.outs[i]), mc)
 
-    def solve_batch(self, n_threads: int) -> int:
-        f = self.lib.lmie_solution_batch
+    def solve_batch(self, n_threads: int, precision: int = abi.PRECISION_FP64) -> int:
+        f = self.lib.lmie_solution_batch2
         f.restype = C.c_int
         f.argtypes = [C.c_int, C.POINTER(abi.lmie_in_data), C.POINTER(abi.lmie_out_data), C.c_int,
-                      C.c_int, C.c_int]
-        return f(len(self.cases), self.ins, self.outs, 0, 0, n_threads)
+                      C.c_int, C.c_int, C.c_int]
+        return f(len(self.cases), self.ins, self.outs, 0, 0, n_threads, precision)
 
-    def solve_each(self, n_threads: int) -> int:
-        for i in range(len(self.cases)):
+    def solve_each(self, n_threads: int, count: int = -1) -> int:
+        for i in range(len(self.cases) if count < 0 else count):
             rc = self.lib.lmie_solution(C.byref(self.ins[i]), C.byref(self.outs[i]), 0, 0, n_threads, 0)
             if rc != 0:
                 return rc
@@ -188,6 +197,47 @@ def cpu_sample_rate(cases, budget_s: float) -> dict:
     return {"value": done / busy, "unit": UNIT, "cores": threads, "kind": kind,
             "sample": f"{done} of the {len(cases)} batch cases in seeded random order "
                       f"({busy:.1f} s), lmie_solution with n_threads={threads}, one case after another"}
+
+
+def _relmax(a, b) -> float:
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    den = float(np.max(np.abs(b))) if b.size else 0.0
+    num = float(np.max(np.abs(a - b))) if b.size else 0.0
+    return num / den if den > 0 else num
+
+
+def split_errors(lib, cases, n_threads: int) -> dict:
+    """Largest error of the split-precision form against the FP64 form over
+    `cases`, per output: max|split - fp64| / max|fp64| per case and array
+    (GSF/Legendre arrays over the shorter n_coef), then the worst case."""
+    ref = abi.solve_batch(lib, cases, n_threads=n_threads, precision=abi.PRECISION_FP64)
+    got = abi.solve_batch(lib, cases, n_threads=n_threads, precision=abi.PRECISION_TF32X3)
+    worst, n_same = {}, 0
+    for g, r in zip(got, ref):
+        if g.rc != 0 or r.rc != 0:
+            raise RuntimeError("solve failed while measuring the split-precision error")
+        err = {"cext": _relmax(g.scalars["cext"], r.scalars["cext"]), "g": _relmax(g.scalars["g"], r.scalars["g"])}
+        nc = min(g.n_coef, r.n_coef)
+        for name in ("gc", "pf", "gc_l", "pf_l"):
+            a, b = getattr(g, name), getattr(r, name)
+            if b is None:
+                continue
+            if name == "gc":
+                a, b = a[:, :nc], b[:, :nc]
+            elif name == "gc_l":
+                a, b = a[:, :, :nc], b[:, :, :nc]
+            err[name] = _relmax(a, b)
+        same_n = g.n_coef == r.n_coef
+        n_same += same_n
+        for k, v in err.items():
+            if k in ("pf", "pf_l") and not same_n:
+                k = k + "_truncated_differently"
+            worst[k] = max(worst.get(k, 0.0), float(v))
+    return {"cases": len(cases), "max_rel_err": worst, "cases_with_same_n_coef": n_same,
+            "metric": "max over cases of max|split - fp64| / max|fp64| per output array (gc over the "
+                      "shorter n_coef; pf where both forms kept the same number of coefficients, and "
+                      "separately where the truncation at `accuracy` differed)"}
 
 
 def run_reference_arm(args) -> int:
@@ -276,19 +326,74 @@ def run_b200(args) -> int:
         raise RuntimeError("device re-run failed")
     barrier()
     dev_ms = max_over_ranks(ms_total.value)
+    batch_stage_ms = {n: ms_stage[i] / args.steps for i, n in enumerate(lmie_b200.STAGES)}
+    ang_ms = ms_stage[3] / args.steps
+
+    # the same batch with the angular contraction on the tensor cores
+    tf32 = abi.PRECISION_TF32X3
+    for _ in range(2):
+        if batch.solve_batch(threads, tf32) != 0:
+            raise RuntimeError("lmie_solution_batch2 failed")
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        if batch.solve_batch(threads, tf32) != 0:
+            raise RuntimeError("lmie_solution_batch2 failed")
+    barrier()
+    split_e2e_s = max_over_ranks(time.perf_counter() - t0)
+    if lib.lmieb_rerun_device(1, 1, C.byref(ms_total), ms_stage) != 0:
+        raise RuntimeError("device re-run failed")
+    barrier()
+    if lib.lmieb_rerun_device(args.steps, 1, C.byref(ms_total), ms_stage) != 0:
+        raise RuntimeError("device re-run failed")
+    barrier()
+    split_dev_ms = max_over_ranks(ms_total.value)
     clk = clocks.stop()
+    split_stage_ms = {n: ms_stage[i] / args.steps for i, n in enumerate(lmie_b200.STAGES)}
+    split_ang_ms = ms_stage[3] / args.steps
 
     value = world * N_CASES * args.steps / (dev_ms * 1e-3)
     e2e = world * N_CASES * args.steps / e2e_s
-    batch_stage_ms = {n: ms_stage[i] / args.steps for i, n in enumerate(lmie_b200.STAGES)}
-    ang_ms = ms_stage[3] / args.steps
     peak = C.c_double()
     lib.lmieb_fp64_peak(C.byref(peak))
     achieved = flops[0] / (ang_ms * 1e-3) / 1e12 if ang_ms > 0 else None
 
-    # secondary: the single cloud-droplet case through lmie_solution()
-    single = None
+    # secondary: split-precision error, the plain per-case form, the single cloud-droplet case
+    single = split = plain = None
     if rank == 0:
+        errs = split_errors(lib, cases[:256], threads)
+        tf32_peak = None
+        peaks = ROOT / "MEASURED_PEAKS.json"
+        if peaks.exists():
+            try:
+                bf16 = json.loads(peaks.read_text()).get("bf16_tflops")
+                tf32_peak = float(bf16) / 2 if bf16 else None
+            except (ValueError, TypeError):
+                tf32_peak = None
+        tc_tflops = 3 * flops[0] / (split_ang_ms * 1e-3) / 1e12 if split_ang_ms > 0 else None
+        split = {
+            "value": world * N_CASES * args.steps / (split_dev_ms * 1e-3),
+            "e2e": world * N_CASES * args.steps / split_e2e_s, "unit": UNIT,
+            "ms_per_step": split_dev_ms / args.steps, "stage_ms": split_stage_ms,
+            "dtype": "f64 with tf32x3 angular contraction (fp32 accumulation in segments of 64 orders)",
+            "error_vs_fp64": errs,
+            "roofline": {
+                "kernel": "k_angular_tc (tcgen05.mma kind::tf32, 3 products per operand pair)",
+                "bound": "tensor", "achieved": tc_tflops, "peak": tf32_peak, "unit": "TFLOP/s",
+                "frac": (tc_tflops / tf32_peak) if (tc_tflops and tf32_peak) else None,
+                "peak_source": "dense tf32 = half of the measured bf16 burst in MEASURED_PEAKS.json",
+                "tensor_flops_per_launch": 3 * flops[0], "ms_per_launch": split_ang_ms},
+        }
+        n_plain = 256
+        plain_batch = CBatch(lib, cases[:n_plain])
+        plain_batch.solve_each(threads, 16)
+        t1 = time.perf_counter()
+        if plain_batch.solve_each(threads) != 0:
+            raise RuntimeError("lmie_solution failed")
+        plain_s = time.perf_counter() - t1
+        plain = {"value": n_plain / plain_s, "unit": UNIT, "dtype": "f64",
+                 "sample": f"the first {n_plain} cases of the batch, one lmie_solution() call each"}
+
         one = CBatch(lib, [single_case()])
         for _ in range(3):
             one.solve_each(1)
@@ -324,6 +429,8 @@ def run_b200(args) -> int:
                                "MEASURED_PEAKS.json holds HBM and BF16 only",
                 "flops_per_launch": flops[0], "ms_per_launch": ang_ms},
             "stage_ms": batch_stage_ms,
+            "split_tf32x3": split,
+            "plain": plain,
             "single_case": single,
             "clocks": clk,
         }
