@@ -45,6 +45,58 @@ int lmie_solution_batch(int n_cases, lmie_in_data *in, lmie_out_data *out, int a
 int lmie_solution_batch2(int n_cases, lmie_in_data *in, lmie_out_data *out, int alloc_out,
                          int verbose, int n_threads, int precision);
 
+/* ---- adjoint (reverse-mode) gradient of an output-weighted scalar ----
+ *
+ * A binned size distribution shared by all wavelengths: bin b spans
+ * [edges[b], edges[b+1]] (same length unit as the wavelengths), carries the
+ * number weight weight[b] (uniform number density inside the bin) and is
+ * integrated with n_quad Gauss-Legendre radii.  The quadrature radius r of
+ * bin b has the weight W_r = weight[b] q_r (q_r its Gauss weight); the
+ * distribution is normalised by N = sum_r W_r, as lmie_solution normalises
+ * n(r).  The reference cannot express such a distribution in one call; it is
+ * the per-radius SIZE_DIST_MONO solves combined with these weights. */
+typedef struct {
+     int n_bins;
+     int n_quad;
+     const double *edges;       /* [n_bins + 1], ascending, > 0 */
+     const double *weight;      /* [n_bins], > 0 */
+} lmie_bins;
+
+/* Loss weights of one wavelength: the loss is
+ *   L = c_cext Cext + c_csca Csca + c_g g
+ *       + sum_i (d_p11[i] P11(theta_i) + d_p12[i] P12(theta_i)),
+ * theta_i = i 180 / (n_angles - 1) degrees, with Cext, Csca, g and the phase
+ * matrix normalised as lmie_solution returns them (P11 = a1, P12 = b1, the
+ * elements pf[0] and pf[4] of its 6-element phase matrix).  The phase matrix
+ * is evaluated from the Mie sums at theta_i directly, which is what
+ * lmie_solution returns with accuracy = 0 (no truncation of the expansion).
+ * d_p11 / d_p12 may be NULL (zero weights). */
+typedef struct {
+     double c_cext, c_csca, c_g;
+     const double *d_p11;       /* [n_angles] */
+     const double *d_p12;       /* [n_angles] */
+} lmie_loss_weights;
+
+/* Reverse-mode gradient of L = sum over the n_lambda wavelengths of their
+ * losses, for the binned distribution `bins`, wavelength lambda[k] and
+ * m = mr[k] - i mi[k].  Returns the loss in *loss, dL/dmr[k] in grad_mr[k],
+ * dL/dmi[k] in grad_mi[k] and dL/dweight[b] in grad_weight[b] (any of the
+ * gradient pointers may be NULL).  If values is not NULL it receives per
+ * wavelength [Cext, Csca, g, P11(theta_0..), P12(theta_0..)]
+ * (3 + 2 n_angles doubles each).
+ *
+ * One forward sweep (Mie recurrences, coefficients, the phase matrix at the
+ * n_angles angles) and one reverse sweep in FP64: the derivative of the
+ * logarithmic derivative D_n(z) is taken in closed form (dD_n/dz =
+ * n(n+1)/z^2 - 1 - D_n^2, from the Riccati-Bessel equation), and the reverse
+ * sweep re-runs the recurrences from checkpoints stored every 64 orders
+ * instead of per-order arrays.  This entry point has no counterpart in the
+ * reference.  Returns 0 or -1. */
+int lmie_solution_adjoint(int n_lambda, const double *lambda, const double *mr, const double *mi,
+                          const lmie_bins *bins, int n_angles, const lmie_loss_weights *weights,
+                          double *loss, double *grad_mr, double *grad_mi, double *grad_weight,
+                          double *values);
+
 /* Checks the tensor-core contraction machinery on the device: a 128 x 64
  * product over K orders (K a positive multiple of 16, at most 4096) of seeded
  * random operands through the operand split, shared-memory layout,

@@ -48,3 +48,46 @@ def solve(case: abi.Case) -> abi.Result:
 N_STAGES = 9
 STAGES = ("upload", "mie_coefficients", "cross_sections", "angular", "normalise",
           "gsf_expansion", "legendre_expansion", "user_angles", "download")
+
+
+class lmie_bins(C.Structure):
+    _fields_ = [("n_bins", C.c_int), ("n_quad", C.c_int),
+                ("edges", C.POINTER(C.c_double)), ("weight", C.POINTER(C.c_double))]
+
+
+class lmie_loss_weights(C.Structure):
+    _fields_ = [("c_cext", C.c_double), ("c_csca", C.c_double), ("c_g", C.c_double),
+                ("d_p11", C.POINTER(C.c_double)), ("d_p12", C.POINTER(C.c_double))]
+
+
+def _dptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def adjoint(p) -> dict:
+    """lmie_solution_adjoint() on a workloads.AdjointProblem: the loss, its
+    gradient w.r.t. mr, mi (per wavelength) and the bin weights, and the
+    per-wavelength outputs [Cext, Csca, g, P11(theta), P12(theta)]."""
+    import numpy as np
+    lib = library()
+    f = lib.lmie_solution_adjoint
+    f.restype = C.c_int
+    f.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),
+                  C.POINTER(lmie_bins), C.c_int, C.POINTER(lmie_loss_weights), C.POINTER(C.c_double),
+                  C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    L, na = p.n_lambda, p.n_angles
+    bins = lmie_bins(p.n_bins, p.n_quad, _dptr(p.edges), _dptr(p.weight))
+    w = (lmie_loss_weights * L)()
+    for k in range(L):
+        w[k] = lmie_loss_weights(p.c[k, 0], p.c[k, 1], p.c[k, 2], _dptr(p.d11[k]), _dptr(p.d12[k]))
+    loss = C.c_double()
+    gmr, gmi = np.zeros(L), np.zeros(L)
+    gw = np.zeros(p.n_bins)
+    vals = np.zeros((L, 3 + 2 * na))
+    rc = f(L, _dptr(p.lam), _dptr(p.mr), _dptr(p.mi), C.byref(bins), na, w, C.byref(loss),
+           _dptr(gmr), _dptr(gmi), _dptr(gw), _dptr(vals))
+    if rc != 0:
+        raise RuntimeError("lmie_solution_adjoint failed")
+    return {"loss": loss.value, "grad_mr": gmr, "grad_mi": gmi, "grad_weight": gw,
+            "cext": vals[:, 0], "csca": vals[:, 1], "g": vals[:, 2],
+            "p11": vals[:, 3:3 + na], "p12": vals[:, 3 + na:]}

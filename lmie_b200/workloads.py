@@ -47,3 +47,54 @@ def batched_uneven(n_cases: int = 4096, seed: int = SEED, n_angles: int = 181) -
                           n_int2=n_r // 100, n_quad=100, n_angles=n_angles, accuracy=1e-7,
                           derivs=deriv_unit("mr", "mi", "a1", "a2")))
     return cases
+
+
+class AdjointProblem:
+    """Inputs of lmie_solution_adjoint: wavelengths with their refractive
+    indices, one binned size distribution and the loss weights."""
+
+    def __init__(self, lam, mr, mi, edges, weight, n_quad, n_angles, c, d11, d12):
+        self.lam = np.ascontiguousarray(lam, dtype=np.float64)
+        self.mr = np.ascontiguousarray(mr, dtype=np.float64)
+        self.mi = np.ascontiguousarray(mi, dtype=np.float64)
+        self.edges = np.ascontiguousarray(edges, dtype=np.float64)
+        self.weight = np.ascontiguousarray(weight, dtype=np.float64)
+        self.n_quad = int(n_quad)
+        self.n_angles = int(n_angles)
+        self.c = np.ascontiguousarray(c, dtype=np.float64)        # [n_lambda, 3]: c_cext, c_csca, c_g
+        self.d11 = np.ascontiguousarray(d11, dtype=np.float64)    # [n_lambda, n_angles]
+        self.d12 = np.ascontiguousarray(d12, dtype=np.float64)
+
+    @property
+    def n_lambda(self) -> int:
+        return len(self.lam)
+
+    @property
+    def n_bins(self) -> int:
+        return len(self.weight)
+
+    def replace(self, **kw) -> "AdjointProblem":
+        a = dict(lam=self.lam, mr=self.mr, mi=self.mi, edges=self.edges, weight=self.weight,
+                 n_quad=self.n_quad, n_angles=self.n_angles, c=self.c, d11=self.d11, d12=self.d12)
+        a.update(kw)
+        return AdjointProblem(**a)
+
+
+def adjoint_retrieval(n_lambda: int = 256, n_bins: int = 64, n_quad: int = 32, n_angles: int = 181,
+                      lam_range=(0.34, 2.25), r_range=(0.02, 20.0), seed: int = SEED) -> AdjointProblem:
+    """The retrieval workload: n_lambda wavelengths log-spaced over lam_range
+    (um) sharing one distribution of n_bins log-spaced bins over r_range (um)
+    with n_quad Gauss points each and seeded bin weights U(0.1, 1); per
+    wavelength mr ~ U[1.35, 1.6], mi ~ logU[1e-6, 0.05]; loss weights: c for
+    Cext, Csca, g ~ U(-1, 1) scaled to the magnitudes of those outputs, and
+    d for P11, P12 at each angle ~ U(-1, 1) / n_angles."""
+    rng = np.random.Generator(np.random.PCG64(seed + 5))
+    lam = np.exp(np.linspace(math.log(lam_range[0]), math.log(lam_range[1]), n_lambda))
+    edges = np.exp(np.linspace(math.log(r_range[0]), math.log(r_range[1]), n_bins + 1))
+    weight = rng.uniform(0.1, 1.0, n_bins)
+    mr = rng.uniform(1.35, 1.6, n_lambda)
+    mi = np.exp(rng.uniform(math.log(1e-6), math.log(0.05), n_lambda))
+    c = rng.uniform(-1.0, 1.0, (n_lambda, 3))
+    d11 = rng.uniform(-1.0, 1.0, (n_lambda, n_angles)) / n_angles
+    d12 = rng.uniform(-1.0, 1.0, (n_lambda, n_angles)) / n_angles
+    return AdjointProblem(lam, mr, mi, edges, weight, n_quad, n_angles, c, d11, d12)
