@@ -114,6 +114,15 @@ int lmieb_tc_selftest(int K, double *max_rel_err);
  * 8 download. */
 #define LMIEB_N_STAGES 9
 
+/* Host-side phases of the last lmie_solution_batch / lmie_solution_batch2
+ * call, wall-clock ms: 0 preparation of the cases (size distributions,
+ * derivative split, per-radius truncations; n_threads threads), 1 packing of
+ * the device inputs, 2 device work with its host<->device copies, 3 unpacking
+ * of the device outputs, 4 scatter into the callers' lmie_out_data.  Returns
+ * LMIEB_N_HOST. */
+#define LMIEB_N_HOST 5
+int lmieb_last_host_timing(double *ms, int n);
+
 /* Selects the GPU the library uses (default: the CUDA runtime's current
  * device).  Must precede the first solve; one process drives one GPU. */
 int lmieb_set_device(int device);

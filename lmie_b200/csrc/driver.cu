@@ -7,11 +7,14 @@
 // (src/lmie_schedule.c:942-1268); a batch of cases is the unit of work, and a
 // single lmie_solution() is a batch of one.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <atomic>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 #include "kernels.h"
@@ -54,9 +57,48 @@ struct Ctx {
     double *gl_pool = nullptr;
     size_t gl_cap = 0, gl_used = 0;
     std::vector<std::pair<int, long long>> gl_map;
+    // host-side phases of the last batch call (ms): prepare, pack, device and copies, unpack, finish
+    double host_ms[LMIEB_N_HOST] = {};
 };
 
 Ctx g_ctx;
+
+// fn(i) for every i in [0, n) on the host's cores (dynamic chunks of `grain`)
+template <class F>
+void parallel_for(int n, int grain, F &&fn) {
+    const int hw = (int) std::max(1u, std::thread::hardware_concurrency());
+    const int nt = std::min(std::min(hw, 32), (n + grain - 1) / grain);
+    if (nt <= 1) {
+        for (int i = 0; i < n; ++i) fn(i);
+        return;
+    }
+    std::atomic<int> next(0);
+    auto body = [&]() {
+        for (;;) {
+            const int i0 = next.fetch_add(grain);
+            if (i0 >= n) break;
+            for (int i = i0; i < std::min(n, i0 + grain); ++i) fn(i);
+        }
+    };
+    std::vector<std::thread> th;
+    for (int t = 1; t < nt; ++t) th.emplace_back(body);
+    body();
+    for (auto &t : th) t.join();
+}
+
+// memcpy of a large block on several host threads
+void par_memcpy(void *dst, const void *src, size_t bytes) {
+    constexpr size_t chunk = (size_t) 4 << 20;
+    const int n = (int) ((bytes + chunk - 1) / chunk);
+    parallel_for(n, 1, [&](int i) {
+        const size_t a = (size_t) i * chunk, b = std::min(bytes, a + chunk);
+        memcpy((char *) dst + a, (const char *) src + a, b - a);
+    });
+}
+
+double now_ms() {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
 std::mutex g_mu;
 int g_want_device = -1;
 
@@ -241,7 +283,7 @@ int run_kernels(Plan &L) {
 template <class T>
 T *put(char *hp, size_t &off, const T *src, size_t count) {
     T *at = (T *) (hp + off);
-    if (src && count) memcpy(at, src, count * sizeof(T));
+    if (src && count) par_memcpy(at, src, count * sizeof(T));
     off += pad(count * sizeof(T));
     return at;
 }
@@ -262,6 +304,7 @@ size_t case_bytes(const lmieb_problem &p) {
 // One sub-batch: ps[0..n).
 int solve_sub(int ncase, const lmieb_problem *ps, lmieb_result *rs_out) {
     Ctx &c = g_ctx;
+    const double t_pack = now_ms();
     Plan &L = *c.plan;
     L = Plan();
     const lmieb_problem &p0 = ps[0];
@@ -276,59 +319,79 @@ int solve_sub(int ncase, const lmieb_problem *ps, lmieb_result *rs_out) {
     L.nd1c = (nd1 + 3) / 4;
     L.n_ang_launch = std::max(1, std::max((nd1 + 3) / 4, (nd2 + 3) / 4));
 
-    // ---- case table and batch-wide per-radius arrays ----
+    // ---- case table and batch-wide per-radius arrays (filled per case in parallel) ----
     std::vector<DevCase> cs(ncase);
-    int R = 0, n1max = 1, ncmax = 1, nqmax = 0;
+    std::vector<int> cr0(ncase + 1, 0), ct0(ncase + 1, 0), cn1max(ncase, 1);
+    std::vector<long long> cs1(ncase + 1, 0), cs2(ncase, 0);
+    parallel_for(ncase, 16, [&](int k) {
+        const lmieb_problem &p = ps[k];
+        int t = 0, mx = 1;
+        long long a = 0, b = 0;
+        for (int i = 0; i < p.n; ++i) {
+            t += (p.n1r[i] + 126) / 127;
+            a += p.n1r[i];
+            b += p.n2r[i];
+            mx = std::max(mx, p.n1r[i]);
+        }
+        ct0[k + 1] = t;
+        cs1[k + 1] = a;
+        cs2[k] = b;
+        cn1max[k] = mx;
+    });
+    int ncmax = 1, nqmax = 0, n1max = 1;
     for (int k = 0; k < ncase; ++k) {
-        R += ps[k].n;
+        cr0[k + 1] = cr0[k] + ps[k].n;
+        ct0[k + 1] += ct0[k];
+        cs1[k + 1] += cs1[k];
         ncmax = std::max(ncmax, ps[k].n_coef);
         nqmax = std::max(nqmax, ps[k].n_qang);
-        for (int r = 0; r < ps[k].n; ++r) n1max = std::max(n1max, ps[k].n1r[r]);
+        n1max = std::max(n1max, cn1max[k]);
     }
+    const int R = cr0[ncase];
     std::vector<double> x(R), xl((size_t) std::max(nd1, 1) * R), w((size_t) ncol * R);
     std::vector<int> n1r(R), n2r(R), rcase(R), tstart(R + 1);
     std::vector<long long> off(R + 1), offp(R + 1);
-    std::vector<int2> tiles;
+    std::vector<int2> tiles(ct0[ncase]);
     std::vector<cplx> ml((size_t) std::max(1, ncase * nd));
     std::vector<double> laml((size_t) std::max(1, ncase * nd));
     off[0] = offp[0] = 0;
-    {
-        int r = 0;
-        for (int k = 0; k < ncase; ++k) {
-            const lmieb_problem &p = ps[k];
-            DevCase &C = cs[k];
-            memset(&C, 0, sizeof(C));
-            C.lambda = p.lambda;
-            C.m = mk(p.mr, -p.mi);
-            C.minv = 1. / C.m;
-            C.accuracy = p.accuracy;
-            C.r0 = r;
-            C.nr = p.n;
-            C.n1 = p.n1;
-            C.n_qang = p.n_qang;
-            C.nh = p.n_qang / 2;
-            C.n_coef = p.n_coef;
-            C.n_angles = L.pf_from ? p.n_angles : 0;
-            C.ml_off = k * nd;
-            for (int kk = 0; kk < nd; ++kk) {
-                ml[(size_t) k * nd + kk] = mk(p.mr_l[kk], -p.mi_l[kk]);
-                laml[(size_t) k * nd + kk] = p.lambda_l[kk];
-            }
-            for (int i = 0; i < p.n; ++i, ++r) {
-                x[r] = p.x[i];
-                for (int q = 0; q < nd1; ++q) xl[(size_t) q * R + r] = p.xl[(size_t) q * p.n + i];
-                for (int q = 0; q < ncol; ++q) w[(size_t) q * R + r] = p.w[(size_t) q * p.n + i];
-                n1r[r] = p.n1r[i];
-                n2r[r] = p.n2r[i];
-                rcase[r] = k;
-                off[r + 1] = off[r] + n1r[r];
-                offp[r + 1] = offp[r] + n1r[r] + 1;
-                tstart[r] = (int) tiles.size();
-                for (int j0 = 1; j0 <= n1r[r]; j0 += 127) tiles.push_back(make_int2(r, j0));
-            }
+    parallel_for(ncase, 16, [&](int k) {
+        const lmieb_problem &p = ps[k];
+        DevCase &C = cs[k];
+        memset(&C, 0, sizeof(C));
+        C.lambda = p.lambda;
+        C.m = mk(p.mr, -p.mi);
+        C.minv = 1. / C.m;
+        C.accuracy = p.accuracy;
+        C.r0 = cr0[k];
+        C.nr = p.n;
+        C.n1 = p.n1;
+        C.n_qang = p.n_qang;
+        C.nh = p.n_qang / 2;
+        C.n_coef = p.n_coef;
+        C.n_angles = L.pf_from ? p.n_angles : 0;
+        C.ml_off = k * nd;
+        for (int kk = 0; kk < nd; ++kk) {
+            ml[(size_t) k * nd + kk] = mk(p.mr_l[kk], -p.mi_l[kk]);
+            laml[(size_t) k * nd + kk] = p.lambda_l[kk];
         }
-    }
-    tstart[R] = (int) tiles.size();
+        long long o = cs1[k];
+        int t = ct0[k];
+        for (int i = 0, r = cr0[k]; i < p.n; ++i, ++r) {
+            x[r] = p.x[i];
+            for (int q = 0; q < nd1; ++q) xl[(size_t) q * R + r] = p.xl[(size_t) q * p.n + i];
+            for (int q = 0; q < ncol; ++q) w[(size_t) q * R + r] = p.w[(size_t) q * p.n + i];
+            n1r[r] = p.n1r[i];
+            n2r[r] = p.n2r[i];
+            rcase[r] = k;
+            o += n1r[r];
+            off[r + 1] = o;
+            offp[r + 1] = o + r + 1;
+            tstart[r] = t;
+            for (int j0 = 1; j0 <= n1r[r]; j0 += 127) tiles[t++] = make_int2(r, j0);
+        }
+    });
+    tstart[R] = ct0[ncase];
     const long long tot = off[R], totp = offp[R];
     const int ntiles = (int) tiles.size();
 
@@ -481,9 +544,7 @@ int solve_sub(int ncase, const lmieb_problem *ps, lmieb_result *rs_out) {
         std::vector<double> wc(ncase, 0.);
         for (int k = 0; k < ncase; ++k) {
             if (cs[k].n_qang <= 0) continue;
-            double s = 0.;
-            for (int r = cs[k].r0; r < cs[k].r0 + cs[k].nr; ++r) s += n1r[r];
-            wc[k] = s * cs[k].nh;
+            wc[k] = (double) (cs1[k + 1] - cs1[k]) * cs[k].nh;
             W += wc[k];
         }
         const double wt = std::max(W / (4. * c.sms), 64. * 2 * 64 * 16);   // work per block
@@ -582,10 +643,9 @@ int solve_sub(int ncase, const lmieb_problem *ps, lmieb_result *rs_out) {
         double fang = 0., frec = 0., fgsf = 0., fexp = 0.;
         for (int k = 0; k < ncase; ++k) {
             const DevCase &C = cs[k];
-            for (int r = C.r0; r < C.r0 + C.nr; ++r) {
-                fang += 8. * C.n_qang * n1r[r] * (1. + nd1);
-                frec += (14. * n2r[r] + 93. * n1r[r]) + nd1 * (16. * n2r[r] + 154. * n1r[r]);
-            }
+            const double s1 = (double) (cs1[k + 1] - cs1[k]), s2 = (double) cs2[k];
+            fang += 8. * C.n_qang * s1 * (1. + nd1);
+            frec += (14. * s2 + 93. * s1) + nd1 * (16. * s2 + 154. * s1);
             fgsf += 12. * C.n_coef * C.n_qang * ncol * ((L.want_gc ? 1 : 0) + (L.want_lc ? 1 : 0));
             fexp += 12. * C.n_angles * C.n_coef * ncol;
         }
@@ -787,6 +847,8 @@ int solve_sub(int ncase, const lmieb_problem *ps, lmieb_result *rs_out) {
     }
 
     // ---- run ----
+    const double t_dev = now_ms();
+    c.host_ms[1] += t_dev - t_pack;
     c.h2d += h_in_end;
     c.d2h += out_bytes;
     cudaStream_t s = c.stream;
@@ -811,6 +873,8 @@ int solve_sub(int ncase, const lmieb_problem *ps, lmieb_result *rs_out) {
         }
     }
     c.have_plan = true;
+    const double t_unpack = now_ms();
+    c.host_ms[2] += t_unpack - t_dev;
 
     // ---- unpack ----
     auto hostp = [&](void *d) { return h_out + ((char *) d - d_out); };
@@ -823,7 +887,7 @@ int solve_sub(int ncase, const lmieb_problem *ps, lmieb_result *rs_out) {
         fprintf(stderr, "ERROR: lmie_b200: the tensor-core angular stage timed out waiting for its pipeline\n");
         return -1;
     }
-    for (int k = 0; k < ncase; ++k) {
+    parallel_for(ncase, 8, [&](int k) {
         const DevCase &C = cs[k];
         lmieb_result &r = rs_out[k];
         memcpy(r.scal, hs + C.scal_off, (size_t) ncol * 4 * 8);
@@ -832,12 +896,13 @@ int solve_sub(int ncase, const lmieb_problem *ps, lmieb_result *rs_out) {
         if (L.pf_from && r.pf) memcpy(r.pf, hpf + C.pf_out_off, (size_t) ncol * 6 * C.n_angles * 8);
         const int t = L.want_lc ? htr[ncase + k] : (L.want_gc ? htr[k] : 0);
         r.n_coef_out = (L.want_gc || L.want_lc) ? (t > 0 ? C.n_coef - t + 1 : C.n_coef) : 0;
-    }
+    });
     if (L.save_control == 1) {
         lmieb_result &r = rs_out[0];
         if (r.save1) memcpy(r.save1, hostp(L.o_save1), (size_t) 4 * R * 8);
         if (r.save2 && L.n_qang0 > 0) memcpy(r.save2, hostp(L.o_save2), n_save2 * 8);
     }
+    c.host_ms[3] += now_ms() - t_unpack;
     return 0;
 }
 
@@ -867,6 +932,7 @@ extern "C" int lmieb_device_solve_batch(int n, const lmieb_problem *p, lmieb_res
     if (check_uniform(n, p)) return -1;
     Ctx &c = g_ctx;
     for (int i = 0; i < NSTAGE; ++i) c.stage_ms[i] = 0.;
+    for (int i = 1; i < 4; ++i) c.host_ms[i] = 0.;
     for (int i = 0; i < 4; ++i) c.work[i] = 0.;
     c.launches = 0;
     c.h2d = c.d2h = 0;
@@ -1040,4 +1106,15 @@ extern "C" int lmieb_tc_selftest(int K, double *max_rel_err) {
     for (size_t i = 0; i < d.size(); ++i) e = std::max(e, fabs(d[i] - ref[i]));
     *max_rel_err = mx > 0. ? e / mx : e;
     return 0;
+}
+
+extern "C" void lmieb_host_phase(int phase, double ms) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    if (phase >= 0 && phase < LMIEB_N_HOST) g_ctx.host_ms[phase] = ms;
+}
+
+extern "C" int lmieb_last_host_timing(double *ms, int n) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    for (int i = 0; i < n && i < LMIEB_N_HOST; ++i) ms[i] = g_ctx.host_ms[i];
+    return LMIEB_N_HOST;
 }

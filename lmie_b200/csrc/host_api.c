@@ -12,6 +12,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <time.h>
 
 #include "host.h"
 
@@ -634,6 +635,12 @@ int lmie_solution2_l(int calc_gc, int calc_lc, int calc_pf,
 
 /* ---- batches -------------------------------------------------------------- */
 
+static double wall_ms(void) {
+     struct timespec ts;
+     clock_gettime(CLOCK_MONOTONIC, &ts);
+     return ts.tv_sec * 1e3 + ts.tv_nsec * 1e-6;
+}
+
 static void job_from_struct(case_job *j, lmie_in_data *in, lmie_out_data *out, int verbose) {
      memset(j, 0, sizeof(*j));
      j->calc_gc = in->calc_gc; j->calc_lc = in->calc_lc; j->calc_pf = in->calc_pf;
@@ -734,6 +741,7 @@ int lmie_solution_batch2(int n_cases, lmie_in_data *in, lmie_out_data *out, int 
      lmieb_problem *P;
      lmieb_result *R;
      int *done, i, k, rc = 0;
+     double t0;
      if (n_cases <= 0)
           return 0;
      if (precision != LMIEB_PRECISION_FP64 && precision != LMIEB_PRECISION_TF32X3) {
@@ -756,7 +764,9 @@ int lmie_solution_batch2(int n_cases, lmie_in_data *in, lmie_out_data *out, int 
      done = (int *) calloc(n_cases, sizeof(int));
      for (i = 0; i < n_cases; ++i)
           job_from_struct(&jobs[i], &in[i], &out[i], verbose);
+     t0 = wall_ms();
      run_jobs(jobs, n_cases, 0, n_threads);
+     lmieb_host_phase(0, wall_ms() - t0);
      for (i = 0; i < n_cases; ++i)
           if (jobs[i].rc) {
                fprintf(stderr, "ERROR: lmie_solution_batch(): case %d\n", i);
@@ -789,8 +799,10 @@ int lmie_solution_batch2(int n_cases, lmie_in_data *in, lmie_out_data *out, int 
                     done[k] = -1;
                }
      }
+     t0 = wall_ms();
      if (rc == 0)
           run_jobs(jobs, n_cases, 1, n_threads);
+     lmieb_host_phase(4, wall_ms() - t0);
      for (i = 0; i < n_cases; ++i)
           job_free(&jobs[i]);
      free(jobs); free(P); free(R); free(done);

@@ -81,6 +81,10 @@ int lmieb_device_solve(const lmieb_problem *p, lmieb_result *r);
  * into sub-batches that fit the device memory budget. */
 int lmieb_device_solve_batch(int n, const lmieb_problem *p, lmieb_result *r);
 
+/* Records the time (ms) of host phase `phase` (0 prepare, 4 finish) of the
+ * current batch call; phases 1-3 are timed inside the device layer. */
+void lmieb_host_phase(int phase, double ms);
+
 /* Device timing of the last lmieb_device_solve (ms per stage), for bench.py. */
 int lmieb_last_timing(double *ms, int n);
 
