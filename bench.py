@@ -26,7 +26,13 @@ The same JSON line carries secondary measurements of the same run:
   plain         the drop-in form: one lmie_solution() call per case (FP64),
                 e2e solves/s over a sample of the batch;
   single_case   the reference's cloud-droplet case (2000 radii, x_max ~436,
-                4 derivatives) through lmie_solution().
+                4 derivatives) through lmie_solution();
+  adjoint       the retrieval workload (256 wavelengths sharing 64 bins x 32
+                Gauss radii, 181 angles) through lmie_solution_adjoint():
+                loss and gradient w.r.t. 512 refractive-index parameters and
+                64 bin weights per call, wavelength-solves/s, next to the
+                reference's forward mode on a sample of its per-radius
+                SIZE_DIST_MONO solves on the host cores.
 
 With N > 1 (torchrun, one process per GPU) every rank solves its own batch
 (independent cases, no data-path collective): weak scaling.
@@ -39,6 +45,7 @@ from __future__ import annotations
 import argparse
 import ctypes as C
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -240,6 +247,47 @@ def split_errors(lib, cases, n_threads: int) -> dict:
                       "separately where the truncation at `accuracy` differed)"}
 
 
+def adjoint_measurement(lib, steps: int) -> dict:
+    import lmie_b200
+    p = workloads.adjoint_retrieval()
+    for _ in range(2):
+        lmie_b200.adjoint(p)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        r = lmie_b200.adjoint(p)
+    dt = (time.perf_counter() - t0) / steps
+    # the reference's forward mode on a sample of the per-radius MONO solves
+    cpu_lib, kind = _cpu_library()
+    rng = np.random.Generator(np.random.PCG64(workloads.SEED))
+    n_sample, t_cpu = 0, 0.0
+    radii = np.exp(rng.uniform(math.log(p.edges[0]), math.log(p.edges[-1]), 64))
+    ks = rng.integers(0, p.n_lambda, 64)
+    for r_, k in zip(radii, ks):
+        case = abi.Case(dist="mono", lam=float(p.lam[k]), mr=float(p.mr[k]), mi=float(p.mi[k]), a1=float(r_),
+                        r1=float(r_), r2=float(r_), n_angles=p.n_angles, accuracy=0.0,
+                        derivs=abi.deriv_unit("mr", "mi"))
+        t1 = time.perf_counter()
+        res = abi.solve(cpu_lib, case, n_threads=1) if kind == "reference" else abi.solve(cpu_lib, case, kind="oracle")
+        t_cpu += time.perf_counter() - t1
+        if res.rc != 0:
+            raise RuntimeError("CPU MONO solve failed")
+        n_sample += 1
+    per_mono = t_cpu / n_sample
+    n_radii = p.n_bins * p.n_quad
+    return {
+        "workload": f"{p.n_lambda} wavelengths log-spaced 0.34-2.25 um, {p.n_bins} log-spaced bins over "
+                    f"0.02-20 um x {p.n_quad} Gauss radii, {p.n_angles} angles, seeded bin weights, mr, mi "
+                    "and loss weights; gradient w.r.t. 512 refractive-index parameters + 64 bin weights",
+        "ms_per_call": dt * 1e3, "value": p.n_lambda / dt, "unit": "wavelength-solves/s (loss + full gradient)",
+        "dtype": "f64", "loss": r["loss"],
+        "cpu_forward_mode": {
+            "value": 1.0 / (per_mono * n_radii), "unit": "wavelength-solves/s (loss + gradient, 1 core)",
+            "kind": kind, "cores": 1,
+            "sample": f"{n_sample} seeded per-radius SIZE_DIST_MONO solves (accuracy 0, mr/mi derivatives, "
+                      f"{p.n_angles} angles) at {per_mono * 1e3:.2f} ms each, times {n_radii} radii per wavelength"},
+    }
+
+
 def run_reference_arm(args) -> int:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -315,6 +363,9 @@ def run_b200(args) -> int:
             raise RuntimeError("lmie_solution_batch failed")
     barrier()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
+    hm = (C.c_double * 5)()
+    lib.lmieb_last_host_timing(hm, 5)
+    host_ms = dict(zip(("prepare", "pack", "device_and_copies", "unpack", "scatter"), list(hm)))
 
     # device: K re-runs of the resident batch, L2 flushed before each (untimed)
     ms_total = C.c_double()
@@ -359,7 +410,7 @@ def run_b200(args) -> int:
     achieved = flops[0] / (ang_ms * 1e-3) / 1e12 if ang_ms > 0 else None
 
     # secondary: split-precision error, the plain per-case form, the single cloud-droplet case
-    single = split = plain = None
+    single = split = plain = adj = None
     if rank == 0:
         errs = split_errors(lib, cases[:256], threads)
         tf32_peak = None
@@ -393,6 +444,7 @@ def run_b200(args) -> int:
         plain_s = time.perf_counter() - t1
         plain = {"value": n_plain / plain_s, "unit": UNIT, "dtype": "f64",
                  "sample": f"the first {n_plain} cases of the batch, one lmie_solution() call each"}
+        adj = adjoint_measurement(lib, 5)
 
         one = CBatch(lib, [single_case()])
         for _ in range(3):
@@ -429,8 +481,10 @@ def run_b200(args) -> int:
                                "MEASURED_PEAKS.json holds HBM and BF16 only",
                 "flops_per_launch": flops[0], "ms_per_launch": ang_ms},
             "stage_ms": batch_stage_ms,
+            "host_ms": host_ms,
             "split_tf32x3": split,
             "plain": plain,
+            "adjoint": adj,
             "single_case": single,
             "clocks": clk,
         }
@@ -443,13 +497,41 @@ def run_b200(args) -> int:
     return 0
 
 
+def run_profile(args) -> int:
+    """Only the device work of one path, `warmup` + `steps` times, for launch
+    lists and kernel captures under a profiler (prints no bench line)."""
+    import lmie_b200
+    lib = lmie_b200.library()
+    if args.profile == "adjoint":
+        p = workloads.adjoint_retrieval()
+        if args.cases < N_CASES:
+            p = workloads.adjoint_retrieval(n_lambda=max(1, 256 * args.cases // N_CASES))
+        for _ in range(args.warmup + args.steps):
+            lmie_b200.adjoint(p)
+        print(f"profiled adjoint: {p.n_lambda} wavelengths, {args.warmup} + {args.steps} calls")
+        return 0
+    precision = abi.PRECISION_TF32X3 if args.profile == "tf32x3" else abi.PRECISION_FP64
+    batch = CBatch(lib, workloads.batched_uneven(args.cases))
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup + args.steps):
+        if batch.solve_batch(threads, precision) != 0:
+            raise RuntimeError("lmie_solution_batch2 failed")
+    print(f"profiled {args.profile}: {args.cases} cases, {args.warmup} + {args.steps} batch calls")
+    return 0
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
+    ap.add_argument("--profile", choices=("fp64", "tf32x3", "adjoint"), default=None,
+                    help="run only this path's batch calls (for profilers); no bench line")
+    ap.add_argument("--cases", type=int, default=N_CASES, help="cases of the profiled batch")
     args = ap.parse_args(argv)
+    if args.profile:
+        return run_profile(args)
     if args.impl == "reference":
         return run_reference_arm(args)
     return run_b200(args)
