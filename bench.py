@@ -64,6 +64,10 @@ from lmie_b200 import abi, workloads  # noqa: E402
 METRIC = "polydisperse solves/s (+Jacobian)"
 UNIT = "solves/s"
 N_CASES = 4096
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_angular /
+# k_angular_tc launch on this workload: measured with ncu on a 256-case batch
+# of the same generator and scaled by the ratio of angular work (13.33).
+ANGULAR_TRAFFIC = {"fp64": 6.66e9, "tf32x3": 5.27e9}
 WORKLOAD = ("batched uneven: 4096 seeded cases (r_eff 0.05-20 um, v_eff 0.02-0.3, lambda 0.34-2.1 um, "
             "mr 1.33-1.60, mi 1e-8-0.1, gamma/log-normal, 100-2000 radii, x_max 0.2-1063), "
             "4 derivatives each (mr, mi, a1, a2), GSF + 181-angle phase matrix, FP64")
@@ -432,6 +436,7 @@ def run_b200(args) -> int:
                 "kernel": "k_angular_tc (tcgen05.mma kind::tf32, 3 products per operand pair)",
                 "bound": "tensor", "achieved": tc_tflops, "peak": tf32_peak, "unit": "TFLOP/s",
                 "frac": (tc_tflops / tf32_peak) if (tc_tflops and tf32_peak) else None,
+                "traffic": ANGULAR_TRAFFIC["tf32x3"],
                 "peak_source": "dense tf32 = half of the measured bf16 burst in MEASURED_PEAKS.json",
                 "tensor_flops_per_launch": 3 * flops[0], "ms_per_launch": split_ang_ms},
         }
@@ -476,7 +481,7 @@ def run_b200(args) -> int:
             "roofline": {
                 "kernel": "k_angular (S1/S2 accumulation + phase-matrix forms, FP64)",
                 "bound": "fp64", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
-                "frac": (achieved / peak.value) if achieved else None, "traffic": None,
+                "frac": (achieved / peak.value) if achieved else None, "traffic": ANGULAR_TRAFFIC["fp64"],
                 "peak_source": "live FP64 FMA microbenchmark (lmieb_fp64_peak); "
                                "MEASURED_PEAKS.json holds HBM and BF16 only",
                 "flops_per_launch": flops[0], "ms_per_launch": ang_ms},

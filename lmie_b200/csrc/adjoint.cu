@@ -57,6 +57,8 @@ struct Adj {
     const long long *off;          // [L*R+1] per-order offsets (n1 each)
     const long long *coff;         // [L*R+1] checkpoint offsets (ceil(n1/ADJ_K) each)
     const double *tab;             // [(n - 1) * nhu + h] -> {pi_n, tau_n}(mu_h), n = 1..n1max
+    const double *tabt;            // [h * n1max + n - 1] -> {pi_n, tau_n}(mu_h) (orders contiguous)
+    int n1max;
     const double *dw;              // [L][na][2] d11, d12
     const double *cw;              // [L][3] c_cext, c_csca, c_g
     cplx *cs, *cd;                 // per order: fv4 (a +- b)
@@ -342,11 +344,12 @@ __global__ void __launch_bounds__(ADJ_T) k_adj_back(Adj P) {
     __syncthreads();
     // transposed contraction over the angles, one order per thread
     for (int n = threadIdx.x + 1; n <= n1; n += ADJ_T) {
-        const double *tb = P.tab + (size_t) (n - 1) * 2 * P.nhu;
+        const double2 *tb = (const double2 *) P.tabt + (n - 1);   // consecutive threads, consecutive orders
         const double sg = (n & 1) ? 1. : -1.;
         cplx bs = mk(0., 0.), bd = mk(0., 0.);
         for (int hh = 0; hh < P.nhu; ++hh) {
-            const double pi = tb[2 * hh], tau = tb[2 * hh + 1];
+            const double2 pt = tb[(size_t) hh * P.n1max];
+            const double pi = pt.x, tau = pt.y;
             const double p = pi + tau, q = pi - tau;
             const cplx *sb = sbar + 4 * hh;
             bs = bs + sb[0] * p + sb[2] * (sg * q);
@@ -530,6 +533,12 @@ extern "C" int lmie_solution_adjoint(int n_lambda, const double *lambda, const d
             p1 = p2;
         }
     }
+    std::vector<double> tabt(tab.size());
+    for (int n = 1; n <= n1max; ++n)
+        for (int h = 0; h < nhu; ++h) {
+            tabt[((size_t) h * n1max + n - 1) * 2] = tab[((size_t) (n - 1) * nhu + h) * 2];
+            tabt[((size_t) h * n1max + n - 1) * 2 + 1] = tab[((size_t) (n - 1) * nhu + h) * 2 + 1];
+        }
     std::vector<double> dw((size_t) L * na * 2, 0.), cw((size_t) L * 3);
     for (int k = 0; k < L; ++k) {
         cw[(size_t) k * 3] = weights[k].c_cext;
@@ -553,6 +562,7 @@ extern "C" int lmie_solution_adjoint(int n_lambda, const double *lambda, const d
     const size_t i_x = add(x.data(), LR * 8), i_n1 = add(n1.data(), LR * 4), i_n2 = add(n2.data(), LR * 4);
     const size_t i_off = add(off.data(), (LR + 1) * 8), i_coff = add(coff.data(), (LR + 1) * 8);
     const size_t i_tab = add(tab.data(), tab.size() * 8), i_dw = add(dw.data(), dw.size() * 8);
+    const size_t i_tabt = add(tabt.data(), tabt.size() * 8);
     const size_t i_cw = add(cw.data(), cw.size() * 8);
     const size_t out_vals = (size_t) L * (3 + 2 * na) * 8, out_lw = (size_t) L * 8 * 8;
     const size_t out_g = (size_t) (2 * L + nb) * 8;
@@ -586,6 +596,8 @@ extern "C" int lmie_solution_adjoint(int n_lambda, const double *lambda, const d
     P.bstart = (const int *) dp(i_bs);
     P.x = (const double *) dp(i_x); P.n1 = (const int *) dp(i_n1); P.n2 = (const int *) dp(i_n2);
     P.off = (const long long *) dp(i_off); P.coff = (const long long *) dp(i_coff);
+    P.tabt = (const double *) dp(i_tabt);
+    P.n1max = n1max;
     P.tab = (const double *) dp(i_tab); P.dw = (const double *) dp(i_dw); P.cw = (const double *) dp(i_cw);
     char *o = d + in_bytes;
     P.vals = (double *) o; o += pad256(out_vals);
