@@ -59,7 +59,7 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-from lmie_b200 import abi, workloads  # noqa: E402
+from lmie_b200 import abi, shard, workloads  # noqa: E402
 
 METRIC = "polydisperse solves/s (+Jacobian)"
 UNIT = "solves/s"
@@ -344,8 +344,16 @@ def run_b200(args) -> int:
     if lib.lmieb_set_device(local) != 0:
         raise RuntimeError("lmieb_set_device failed")
     threads = max(1, (os.cpu_count() or 1) // max(1, world))
-    # every rank solves its own seeded batch (independent cases)
-    cases = workloads.batched_uneven(N_CASES, seed=workloads.SEED + rank)
+    if args.scaling == "weak":
+        # every rank solves its own seeded batch (independent cases)
+        cases = workloads.batched_uneven(N_CASES, seed=shard.weak_seed(workloads.SEED, rank))
+        n_job = world * N_CASES
+    else:
+        # the ranks split one batch into cost-balanced contiguous ranges
+        allc = workloads.batched_uneven(N_CASES)
+        a, b = shard.strong_slice(allc, rank, world)
+        cases = allc[a:b]
+        n_job = N_CASES
     batch = CBatch(lib, cases)
 
     for _ in range(args.warmup):
@@ -407,8 +415,8 @@ def run_b200(args) -> int:
     split_stage_ms = {n: ms_stage[i] / args.steps for i, n in enumerate(lmie_b200.STAGES)}
     split_ang_ms = ms_stage[3] / args.steps
 
-    value = world * N_CASES * args.steps / (dev_ms * 1e-3)
-    e2e = world * N_CASES * args.steps / e2e_s
+    value = n_job * args.steps / (dev_ms * 1e-3)
+    e2e = n_job * args.steps / e2e_s
     peak = C.c_double()
     lib.lmieb_fp64_peak(C.byref(peak))
     achieved = flops[0] / (ang_ms * 1e-3) / 1e12 if ang_ms > 0 else None
@@ -427,8 +435,8 @@ def run_b200(args) -> int:
                 tf32_peak = None
         tc_tflops = 3 * flops[0] / (split_ang_ms * 1e-3) / 1e12 if split_ang_ms > 0 else None
         split = {
-            "value": world * N_CASES * args.steps / (split_dev_ms * 1e-3),
-            "e2e": world * N_CASES * args.steps / split_e2e_s, "unit": UNIT,
+            "value": n_job * args.steps / (split_dev_ms * 1e-3),
+            "e2e": n_job * args.steps / split_e2e_s, "unit": UNIT,
             "ms_per_step": split_dev_ms / args.steps, "stage_ms": split_stage_ms,
             "dtype": "f64 with tf32x3 angular contraction (fp32 accumulation in segments of 64 orders)",
             "error_vs_fp64": errs,
@@ -469,10 +477,12 @@ def run_b200(args) -> int:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded generator, rank r uses seed + r)",
+            "scaling": args.scaling, "vs_baseline": None, "dtype": "f64",
+            "data": ("synthetic (seeded generator, rank r uses seed + r)" if args.scaling == "weak" else
+                     "synthetic (seeded generator, one batch split by estimated cost over the ranks)"),
             "config": {"workload": WORKLOAD, "n_cases": N_CASES, "n_derivs": 4,
-                       "parallelism": f"independent batches x{world}",
+                       "parallelism": (f"independent batches x{world}" if args.scaling == "weak" else
+                                       f"one batch in {world} cost-balanced case ranges"),
                        "l2": "flushed (256 MiB write) before every timed device step; "
                              "the batch's working set (~8 GB) exceeds L2 in any case"},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d.value),
@@ -534,6 +544,8 @@ def main(argv=None) -> int:
     ap.add_argument("--profile", choices=("fp64", "tf32x3", "adjoint"), default=None,
                     help="run only this path's batch calls (for profilers); no bench line")
     ap.add_argument("--cases", type=int, default=N_CASES, help="cases of the profiled batch")
+    ap.add_argument("--scaling", choices=("weak", "strong"), default="weak",
+                    help="weak: each rank its own 4096-case batch; strong: the ranks split one batch")
     args = ap.parse_args(argv)
     if args.profile:
         return run_profile(args)
