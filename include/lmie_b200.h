@@ -41,6 +41,13 @@ int lmie_solution_batch(int n_cases, lmie_in_data *in, lmie_out_data *out, int a
 #define LMIEB_PRECISION_FP64 0
 #define LMIEB_PRECISION_TF32X3 1
 
+/* Batch calls cut their cases into `chunks` parts (0: automatic -- one part
+ * per 640 cases, at most 6; 1: one part) and prepare, pack, unpack and
+ * scatter one part on the host while the device works on another.  With one
+ * part a whole batch that fits the device stays resident for
+ * lmieb_rerun_device.  Returns 0, or -1 for chunks < 0. */
+int lmieb_set_pipeline(int chunks);
+
 /* lmie_solution_batch with the arithmetic chosen by `precision`. */
 int lmie_solution_batch2(int n_cases, lmie_in_data *in, lmie_out_data *out, int alloc_out,
                          int verbose, int n_threads, int precision);
@@ -135,7 +142,9 @@ int lmieb_set_timing(int on);
 int lmieb_last_timing(double *ms, int n);
 
 /* Re-runs the device stages 1..7 of the last solve `reps` times on the
- * inputs still resident in device memory (no host work, no copies), each
+ * inputs still resident in device memory (no host work, no copies); only
+ * defined when that solve ran as one sub-batch (see lmieb_set_pipeline),
+ * else returns -1.  Each
  * repetition bracketed by CUDA events on the library's stream; with
  * flush_l2 a 256 MiB buffer is written before each repetition (outside the
  * timed interval).  Returns the summed device time in *ms_total and the

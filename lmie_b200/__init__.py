@@ -37,6 +37,7 @@ def library() -> C.CDLL:
                                           C.POINTER(C.c_int), C.POINTER(C.c_int)]
         lib.lmieb_tc_selftest.argtypes = [C.c_int, C.POINTER(C.c_double)]
         lib.lmieb_last_host_timing.argtypes = [C.POINTER(C.c_double), C.c_int]
+        lib.lmieb_set_pipeline.argtypes = [C.c_int]
         _lib = lib
     return _lib
 

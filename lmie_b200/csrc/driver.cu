@@ -34,15 +34,45 @@ inline size_t pad(size_t bytes) { return ((bytes ? bytes : 1) + 255) & ~(size_t)
 
 struct Plan;
 
+// Results of a submitted sub-batch still to be unpacked.
+struct Pending {
+    bool active = false;
+    long long ticket = -1;
+    int ncase = 0, ncol = 0, R = 0;
+    std::vector<DevCase> cs;
+    lmieb_result *rs = nullptr;
+    char *h_out = nullptr, *d_out = nullptr;     // host copy / device origin of the output block
+    int want_gc = 0, want_lc = 0, pf_from = 0, save_control = 0, n_qang0 = 0;
+    size_t n_save2 = 0;
+    double *o_scal = nullptr, *o_gc = nullptr, *o_lc = nullptr, *o_pf = nullptr;
+    double *o_save1 = nullptr, *o_save2 = nullptr;
+    int *o_trunc = nullptr;
+    double t_submit = 0.;
+};
+
+// One of two buffer sets: a sub-batch is packed into one while the device
+// still works on the other's.
+struct Slot {
+    char *dbuf = nullptr;
+    size_t dcap = 0;
+    char *hbuf = nullptr;
+    size_t hcap = 0;
+    Plan *plan = nullptr;
+    cudaEvent_t done = nullptr;
+    bool have_plan = false;
+    Pending pend;
+};
+
 struct Ctx {
     bool ready = false;
     int device = -1;
     int sms = 0;
     cudaStream_t stream = nullptr;
-    char *dbuf = nullptr;
-    size_t dcap = 0;
-    char *hbuf = nullptr;
-    size_t hcap = 0;
+    Slot slot[2];
+    int last_slot = -1;             // slot of the last submitted sub-batch
+    long long next_ticket = 0;
+    int submits = 0;                // sub-batches submitted since the counters were reset
+    std::vector<std::pair<long long, int>> finished;   // (ticket, rc) of recently collected sub-batches
     char *flush = nullptr;
     cudaEvent_t ev[NSTAGE + 1] = {};
     bool timing = false;
@@ -50,8 +80,6 @@ struct Ctx {
     double work[4] = {};            // algorithmic flops of the last solve (see lmieb_last_work)
     long long launches = 0;         // kernel launches of one device run of the last solve
     size_t h2d = 0, d2h = 0;        // bytes copied by the last solve
-    bool have_plan = false;
-    Plan *plan = nullptr;
     // Gauss-Legendre angles depend only on their number: computed once per n
     // into a device pool ([n nodes][n weights] per entry) and kept
     double *gl_pool = nullptr;
@@ -170,33 +198,34 @@ int ensure_ready() {
     c.sms = prop.multiProcessorCount;
     LMIEB_CUDA_TRY(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
     for (int i = 0; i <= NSTAGE; ++i) LMIEB_CUDA_TRY(cudaEventCreate(&c.ev[i]));
-    c.plan = new Plan();
+    for (Slot &S : c.slot) {
+        S.plan = new Plan();
+        LMIEB_CUDA_TRY(cudaEventCreateWithFlags(&S.done, cudaEventDisableTiming));
+    }
     c.ready = true;
     return 0;
 }
 
-int ensure_device(size_t bytes) {
-    Ctx &c = g_ctx;
-    if (bytes <= c.dcap) return 0;
-    if (c.dbuf) LMIEB_CUDA_TRY(cudaFree(c.dbuf));
-    c.dbuf = nullptr;
-    c.dcap = 0;
+int ensure_device(Slot &S, size_t bytes) {
+    if (bytes <= S.dcap) return 0;
+    if (S.dbuf) LMIEB_CUDA_TRY(cudaFree(S.dbuf));
+    S.dbuf = nullptr;
+    S.dcap = 0;
     size_t want = bytes + bytes / 4;
-    LMIEB_CUDA_TRY(cudaMalloc((void **) &c.dbuf, want));
-    c.dcap = want;
-    c.have_plan = false;
+    LMIEB_CUDA_TRY(cudaMalloc((void **) &S.dbuf, want));
+    S.dcap = want;
+    S.have_plan = false;
     return 0;
 }
 
-int ensure_host(size_t bytes) {
-    Ctx &c = g_ctx;
-    if (bytes <= c.hcap) return 0;
-    if (c.hbuf) LMIEB_CUDA_TRY(cudaFreeHost(c.hbuf));
-    c.hbuf = nullptr;
-    c.hcap = 0;
+int ensure_host(Slot &S, size_t bytes) {
+    if (bytes <= S.hcap) return 0;
+    if (S.hbuf) LMIEB_CUDA_TRY(cudaFreeHost(S.hbuf));
+    S.hbuf = nullptr;
+    S.hcap = 0;
     size_t want = bytes + bytes / 4;
-    LMIEB_CUDA_TRY(cudaMallocHost((void **) &c.hbuf, want));
-    c.hcap = want;
+    LMIEB_CUDA_TRY(cudaMallocHost((void **) &S.hbuf, want));
+    S.hcap = want;
     return 0;
 }
 
@@ -215,7 +244,7 @@ int ensure_gl_pool(size_t doubles) {
     }
     c.gl_pool = np;
     c.gl_cap = want;
-    c.have_plan = false;
+    for (Slot &S : c.slot) S.have_plan = false;   // their plans point at the old pool
     return 0;
 }
 
@@ -301,11 +330,13 @@ size_t case_bytes(const lmieb_problem &p) {
     return b;
 }
 
-// One sub-batch: ps[0..n).
-int solve_sub(int ncase, const lmieb_problem *ps, lmieb_result *rs_out) {
+// Packs one sub-batch ps[0..n) into slot S and queues its device work and the
+// download of its outputs; collect_slot() unpacks them.
+int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lmieb_result *rs_out) {
     Ctx &c = g_ctx;
     const double t_pack = now_ms();
-    Plan &L = *c.plan;
+    S.have_plan = false;
+    Plan &L = *S.plan;
     L = Plan();
     const lmieb_problem &p0 = ps[0];
     const int nd = p0.nd, nd1 = p0.nd1, nd2 = p0.nd2, ncol = 1 + nd;
@@ -681,8 +712,8 @@ int solve_sub(int ncase, const lmieb_problem *ps, lmieb_result *rs_out) {
         add(o_scal * 8); add(o_gc * 8); add(o_lc * 8); add(o_pf * 8); add((size_t) (2 * ncase + 1) * 4);
         if (L.save_control == 1) { add((size_t) 4 * R * 8); add(n_save2 * 8); }
     }
-    if (ensure_host(in_bytes + out_bytes)) return -1;
-    char *hp = c.hbuf;
+    if (ensure_host(S, in_bytes + out_bytes)) return -1;
+    char *hp = S.hbuf;
     size_t ho = 0;
     DevCase *h_cs = put(hp, ho, cs.data(), cs.size());
     double *h_x = put(hp, ho, x.data(), (size_t) R);
@@ -753,8 +784,8 @@ int solve_sub(int ncase, const lmieb_problem *ps, lmieb_result *rs_out) {
         add((size_t) ck_total * 8);
         add((size_t) ex_total * 8);
     }
-    if (ensure_device(dev_bytes)) return -1;
-    Arena A{c.dbuf, 0, c.dcap};
+    if (ensure_device(S, dev_bytes)) return -1;
+    Arena A{S.dbuf, 0, S.dcap};
     char *d_in = A.take<char>(h_in_end);
     char *d_out = A.take<char>(out_bytes);
     if (!d_in || !d_out) {
@@ -846,7 +877,7 @@ int solve_sub(int ncase, const lmieb_problem *ps, lmieb_result *rs_out) {
         return -1;
     }
 
-    // ---- run ----
+    // ---- queue: upload, kernels, download ----
     const double t_dev = now_ms();
     c.host_ms[1] += t_dev - t_pack;
     c.h2d += h_in_end;
@@ -863,8 +894,48 @@ int solve_sub(int ncase, const lmieb_problem *ps, lmieb_result *rs_out) {
     if (run_kernels(L)) return -1;
     LMIEB_CUDA_TRY(cudaMemcpyAsync(h_out, d_out, out_bytes, cudaMemcpyDeviceToHost, s));
     stage(NSTAGE);
-    LMIEB_CUDA_TRY(cudaStreamSynchronize(s));
+    LMIEB_CUDA_TRY(cudaEventRecord(S.done, s));
+    S.have_plan = true;
+    c.last_slot = (int) (&S - c.slot);
+
+    Pending &P = S.pend;
+    P.active = true;
+    P.ticket = ticket;
+    P.ncase = ncase;
+    P.ncol = ncol;
+    P.R = R;
+    P.cs.swap(cs);
+    P.rs = rs_out;
+    P.h_out = h_out;
+    P.d_out = d_out;
+    P.want_gc = L.want_gc;
+    P.want_lc = L.want_lc;
+    P.pf_from = L.pf_from;
+    P.save_control = L.save_control;
+    P.n_qang0 = L.n_qang0;
+    P.n_save2 = n_save2;
+    P.o_scal = L.o_scal;
+    P.o_gc = L.o_gc;
+    P.o_lc = L.o_lc;
+    P.o_pf = L.o_pf;
+    P.o_save1 = L.o_save1;
+    P.o_save2 = L.o_save2;
+    P.o_trunc = L.o_trunc;
+    P.t_submit = now_ms();
+    return 0;
+}
+
+// Waits for the slot's sub-batch and unpacks its outputs into the callers'
+// result arrays.
+int collect_slot(Slot &S) {
+    Ctx &c = g_ctx;
+    Pending &P = S.pend;
+    if (!P.active) return 0;
+    P.active = false;
+    LMIEB_CUDA_TRY(cudaEventSynchronize(S.done));
     LMIEB_CUDA_TRY(cudaGetLastError());
+    const double t_unpack = now_ms();
+    c.host_ms[2] += t_unpack - P.t_submit;
     if (c.timing) {
         for (int i = 0; i < NSTAGE; ++i) {
             float ms = 0.f;
@@ -872,38 +943,70 @@ int solve_sub(int ncase, const lmieb_problem *ps, lmieb_result *rs_out) {
             c.stage_ms[i] += ms;
         }
     }
-    c.have_plan = true;
-    const double t_unpack = now_ms();
-    c.host_ms[2] += t_unpack - t_dev;
-
-    // ---- unpack ----
-    auto hostp = [&](void *d) { return h_out + ((char *) d - d_out); };
-    const double *hs = (const double *) hostp(L.o_scal);
-    const double *hg = (const double *) hostp(L.o_gc);
-    const double *hl = (const double *) hostp(L.o_lc);
-    const double *hpf = (const double *) hostp(L.o_pf);
-    const int *htr = (const int *) hostp(L.o_trunc);
+    const int ncase = P.ncase, ncol = P.ncol;
+    auto hostp = [&](void *d) { return P.h_out + ((char *) d - P.d_out); };
+    const double *hs = (const double *) hostp(P.o_scal);
+    const double *hg = (const double *) hostp(P.o_gc);
+    const double *hl = (const double *) hostp(P.o_lc);
+    const double *hpf = (const double *) hostp(P.o_pf);
+    const int *htr = (const int *) hostp(P.o_trunc);
     if (htr[2 * ncase]) {
         fprintf(stderr, "ERROR: lmie_b200: the tensor-core angular stage timed out waiting for its pipeline\n");
         return -1;
     }
     parallel_for(ncase, 8, [&](int k) {
-        const DevCase &C = cs[k];
-        lmieb_result &r = rs_out[k];
+        const DevCase &C = P.cs[k];
+        lmieb_result &r = P.rs[k];
         memcpy(r.scal, hs + C.scal_off, (size_t) ncol * 4 * 8);
-        if (L.want_gc && r.gc) memcpy(r.gc, hg + C.gc_off, (size_t) ncol * 6 * C.n_coef * 8);
-        if (L.want_lc && r.lc) memcpy(r.lc, hl + C.lc_off, (size_t) ncol * 6 * C.n_coef * 8);
-        if (L.pf_from && r.pf) memcpy(r.pf, hpf + C.pf_out_off, (size_t) ncol * 6 * C.n_angles * 8);
-        const int t = L.want_lc ? htr[ncase + k] : (L.want_gc ? htr[k] : 0);
-        r.n_coef_out = (L.want_gc || L.want_lc) ? (t > 0 ? C.n_coef - t + 1 : C.n_coef) : 0;
+        if (P.want_gc && r.gc) memcpy(r.gc, hg + C.gc_off, (size_t) ncol * 6 * C.n_coef * 8);
+        if (P.want_lc && r.lc) memcpy(r.lc, hl + C.lc_off, (size_t) ncol * 6 * C.n_coef * 8);
+        if (P.pf_from && r.pf) memcpy(r.pf, hpf + C.pf_out_off, (size_t) ncol * 6 * C.n_angles * 8);
+        const int t = P.want_lc ? htr[ncase + k] : (P.want_gc ? htr[k] : 0);
+        r.n_coef_out = (P.want_gc || P.want_lc) ? (t > 0 ? C.n_coef - t + 1 : C.n_coef) : 0;
     });
-    if (L.save_control == 1) {
-        lmieb_result &r = rs_out[0];
-        if (r.save1) memcpy(r.save1, hostp(L.o_save1), (size_t) 4 * R * 8);
-        if (r.save2 && L.n_qang0 > 0) memcpy(r.save2, hostp(L.o_save2), n_save2 * 8);
+    if (P.save_control == 1) {
+        lmieb_result &r = P.rs[0];
+        if (r.save1) memcpy(r.save1, hostp(P.o_save1), (size_t) 4 * P.R * 8);
+        if (r.save2 && P.n_qang0 > 0) memcpy(r.save2, hostp(P.o_save2), P.n_save2 * 8);
     }
     c.host_ms[3] += now_ms() - t_unpack;
     return 0;
+}
+
+// Collects `ticket` if it is still pending, and remembers its status.
+int collect_ticket(long long ticket) {
+    Ctx &c = g_ctx;
+    for (Slot &S : c.slot)
+        if (S.pend.active && S.pend.ticket == ticket) {
+            const int rc = collect_slot(S);
+            c.finished.push_back({ticket, rc});
+            if (c.finished.size() > 64) c.finished.erase(c.finished.begin());
+            return rc;
+        }
+    for (auto &f : c.finished)
+        if (f.first == ticket) return f.second;
+    return 0;
+}
+
+// A free slot for the next sub-batch (the older pending one is collected).
+Slot &free_slot() {
+    Ctx &c = g_ctx;
+    Slot &S = c.slot[c.next_ticket & 1];
+    if (S.pend.active) collect_ticket(S.pend.ticket);
+    return S;
+}
+
+// Cases of p[0..n) that fit one sub-batch (at least one).
+int fit_sub(int n, const lmieb_problem *p) {
+    size_t bytes = 0;
+    int k = 0;
+    while (k < n) {
+        const size_t b = case_bytes(p[k]);
+        if (k > 0 && bytes + b > BATCH_BYTES) break;
+        bytes += b;
+        ++k;
+    }
+    return k;
 }
 
 int check_uniform(int n, const lmieb_problem *p) {
@@ -923,6 +1026,30 @@ int check_uniform(int n, const lmieb_problem *p) {
     return 0;
 }
 
+void reset_counters() {
+    Ctx &c = g_ctx;
+    for (int i = 0; i < NSTAGE; ++i) c.stage_ms[i] = 0.;
+    for (int i = 1; i < 4; ++i) c.host_ms[i] = 0.;
+    for (int i = 0; i < 4; ++i) c.work[i] = 0.;
+    c.launches = 0;
+    c.h2d = c.d2h = 0;
+    c.submits = 0;
+}
+
+// submits p[0..n) (one sub-batch); returns its ticket or -1
+long long submit_locked(int n, const lmieb_problem *p, lmieb_result *r) {
+    Ctx &c = g_ctx;
+    Slot &S = free_slot();
+    const long long t = c.next_ticket++;
+    ++c.submits;
+    if (submit_sub(S, t, n, p, r)) {
+        S.pend.active = false;
+        return -1;
+    }
+    if (c.timing && collect_ticket(t)) return -1;   // stage events are shared: one sub-batch at a time
+    return t;
+}
+
 }  // namespace
 
 extern "C" int lmieb_device_solve_batch(int n, const lmieb_problem *p, lmieb_result *r) {
@@ -930,30 +1057,38 @@ extern "C" int lmieb_device_solve_batch(int n, const lmieb_problem *p, lmieb_res
     if (n < 1) return 0;
     if (ensure_ready()) return -1;
     if (check_uniform(n, p)) return -1;
-    Ctx &c = g_ctx;
-    for (int i = 0; i < NSTAGE; ++i) c.stage_ms[i] = 0.;
-    for (int i = 1; i < 4; ++i) c.host_ms[i] = 0.;
-    for (int i = 0; i < 4; ++i) c.work[i] = 0.;
-    c.launches = 0;
-    c.h2d = c.d2h = 0;
-    c.have_plan = false;
-    // cut sub-batches by device working set
-    int k0 = 0, nsub = 0;
-    while (k0 < n) {
-        size_t bytes = 0;
-        int k1 = k0;
-        while (k1 < n) {
-            const size_t b = case_bytes(p[k1]);
-            if (k1 > k0 && bytes + b > BATCH_BYTES) break;
-            bytes += b;
-            ++k1;
-        }
-        if (solve_sub(k1 - k0, p + k0, r + k0)) return -1;
-        ++nsub;
-        k0 = k1;
+    reset_counters();
+    // sub-batches by device working set, each packed while the previous one runs
+    std::vector<long long> tickets;
+    int rc = 0;
+    for (int k0 = 0; k0 < n && rc == 0;) {
+        const int m = fit_sub(n - k0, p + k0);
+        const long long t = submit_locked(m, p + k0, r + k0);
+        if (t < 0) rc = -1;
+        else tickets.push_back(t);
+        k0 += m;
     }
-    if (nsub > 1) c.have_plan = false;   // re-running is only defined for one sub-batch
-    return 0;
+    for (long long t : tickets)
+        if (collect_ticket(t)) rc = -1;
+    return rc;
+}
+
+extern "C" long long lmieb_device_submit(int n, const lmieb_problem *p, lmieb_result *r, int first) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    if (n < 1) return -1;
+    if (ensure_ready()) return -1;
+    if (check_uniform(n, p)) return -1;
+    if (first) reset_counters();
+    return submit_locked(n, p, r);
+}
+
+extern "C" int lmieb_device_collect(long long ticket) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    return collect_ticket(ticket);
+}
+
+extern "C" int lmieb_device_fit(int n, const lmieb_problem *p) {
+    return n < 1 ? 0 : fit_sub(n, p);
 }
 
 extern "C" int lmieb_device_solve(const lmieb_problem *p, lmieb_result *r) {
@@ -988,7 +1123,8 @@ extern "C" int lmieb_last_timing(double *ms, int n) {
 extern "C" int lmieb_rerun_device(int reps, int flush_l2, double *ms_total, double *ms_stage) {
     std::lock_guard<std::mutex> lock(g_mu);
     Ctx &c = g_ctx;
-    if (!c.ready || !c.have_plan) {
+    // a re-run repeats the resident sub-batch, so the last call must have had exactly one
+    if (!c.ready || c.last_slot < 0 || !c.slot[c.last_slot].have_plan || c.submits != 1) {
         fprintf(stderr, "ERROR: lmieb_rerun_device: no single-sub-batch solve is resident on the device\n");
         return -1;
     }
@@ -1000,7 +1136,7 @@ extern "C" int lmieb_rerun_device(int reps, int flush_l2, double *ms_total, doub
     for (int i = 0; i < reps; ++i) {
         if (flush_l2) LMIEB_CUDA_TRY(cudaMemsetAsync(c.flush, i & 0xff, FLUSH_BYTES, c.stream));
         cudaEventRecord(e0, c.stream);
-        if (run_kernels(*c.plan)) { c.timing = was; return -1; }
+        if (run_kernels(*c.slot[c.last_slot].plan)) { c.timing = was; return -1; }
         cudaEventRecord(e1, c.stream);
         LMIEB_CUDA_TRY(cudaEventSynchronize(e1));
         float ms = 0.f;

@@ -735,13 +735,57 @@ int lmie_solution_batch(int n_cases, lmie_in_data *in, lmie_out_data *out, int a
      return lmie_solution_batch2(n_cases, in, out, alloc_out, verbose, n_threads, LMIEB_PRECISION_FP64);
 }
 
+static int g_pipeline = 0;
+
+int lmieb_set_pipeline(int chunks) {
+     if (chunks < 0)
+          return -1;
+     g_pipeline = chunks;
+     return 0;
+}
+
+/* Submitted device work of one chunk of cases: tickets with their ranges in
+ * the P/R arrays. */
+typedef struct {
+     long long *ticket;
+     int n;
+} chunk_tickets;
+
+/* Waits for a chunk's tickets, copies the results back to their jobs and
+ * scatters them into the callers' outputs. */
+static int finish_chunk(chunk_tickets *ct, case_job *jobs, int j0, int j1, const int *pos2job,
+                        const int *pbeg, const int *pend, lmieb_result *R, int n_threads, int ok,
+                        double *t_finish) {
+     int rc = ok ? 0 : -1, q, i;
+     double t0;
+     for (q = 0; q < ct->n; ++q)
+          if (lmieb_device_collect(ct->ticket[q])) {
+               fprintf(stderr, "ERROR: lmie_solution_batch(): device solve\n");
+               rc = -1;
+          }
+     if (rc == 0) {
+          for (q = 0; q < ct->n; ++q)
+               for (i = pbeg[q]; i < pend[q]; ++i)
+                    jobs[pos2job[i]].R = R[i];
+          t0 = wall_ms();
+          run_jobs(jobs + j0, j1 - j0, 1, n_threads);
+          *t_finish += wall_ms() - t0;
+     }
+     ct->n = 0;
+     return rc;
+}
+
 int lmie_solution_batch2(int n_cases, lmie_in_data *in, lmie_out_data *out, int alloc_out,
                          int verbose, int n_threads, int precision) {
      case_job *jobs;
      lmieb_problem *P;
      lmieb_result *R;
-     int *done, i, k, rc = 0;
-     double t0;
+     int *done, *pos2job, i, k, c, rc = 0, np = 0, chunks, per, first = 1;
+     long long *tk[2];
+     int *tb[2], *te[2];
+     chunk_tickets ct[2];
+     int cj0[2] = {0, 0}, cj1[2] = {0, 0};
+     double t0, t_prep = 0., t_fin = 0.;
      if (n_cases <= 0)
           return 0;
      if (precision != LMIEB_PRECISION_FP64 && precision != LMIEB_PRECISION_TF32X3) {
@@ -762,49 +806,91 @@ int lmie_solution_batch2(int n_cases, lmie_in_data *in, lmie_out_data *out, int 
      P = (lmieb_problem *) calloc(n_cases, sizeof(lmieb_problem));
      R = (lmieb_result *) calloc(n_cases, sizeof(lmieb_result));
      done = (int *) calloc(n_cases, sizeof(int));
+     pos2job = (int *) calloc(n_cases, sizeof(int));
+     for (c = 0; c < 2; ++c) {
+          tk[c] = (long long *) calloc(n_cases, sizeof(long long));
+          tb[c] = (int *) calloc(n_cases, sizeof(int));
+          te[c] = (int *) calloc(n_cases, sizeof(int));
+          ct[c].ticket = tk[c];
+          ct[c].n = 0;
+     }
      for (i = 0; i < n_cases; ++i)
           job_from_struct(&jobs[i], &in[i], &out[i], verbose);
-     t0 = wall_ms();
-     run_jobs(jobs, n_cases, 0, n_threads);
-     lmieb_host_phase(0, wall_ms() - t0);
-     for (i = 0; i < n_cases; ++i)
-          if (jobs[i].rc) {
-               fprintf(stderr, "ERROR: lmie_solution_batch(): case %d\n", i);
-               rc = -1;
-          }
-     /* device batches of compatible cases, in input order */
-     for (i = 0; rc == 0 && i < n_cases; ++i) {
-          int m = 0;
-          if (done[i])
-               continue;
-          for (k = i; k < n_cases; ++k) {
-               if (done[k] || (k != i && !jobs_compatible(&jobs[i], &jobs[k])))
-                    continue;
-               P[m] = jobs[k].P;
-               P[m].precision = precision;
-               R[m] = jobs[k].R;
-               done[k] = m + 1;
-               ++m;
-               if (jobs[i].P.save_control != 0)
-                    break;
-          }
-          if (lmieb_device_solve_batch(m, P, R)) {
-               fprintf(stderr, "ERROR: lmie_solution_batch(): device solve\n");
-               rc = -1;
-               break;
-          }
-          for (k = i; k < n_cases; ++k)
-               if (done[k] > 0) {
-                    jobs[k].R = R[done[k] - 1];
-                    done[k] = -1;
+
+     /* chunks of cases: chunk c is prepared and packed while the device works
+        on chunk c - 1, whose results are then unpacked and scattered */
+     chunks = g_pipeline > 0 ? g_pipeline : (n_cases / 640 < 6 ? (n_cases / 640 > 1 ? n_cases / 640 : 1) : 6);
+     if (chunks > n_cases)
+          chunks = n_cases;
+     per = (n_cases + chunks - 1) / chunks;
+     for (c = 0; c * per < n_cases; ++c) {
+          const int j0 = c * per, j1 = j0 + per < n_cases ? j0 + per : n_cases, s = c & 1, o = s ^ 1;
+          int q = 0;
+          t0 = wall_ms();
+          run_jobs(jobs + j0, j1 - j0, 0, n_threads);
+          t_prep += wall_ms() - t0;
+          for (i = j0; i < j1; ++i)
+               if (jobs[i].rc) {
+                    fprintf(stderr, "ERROR: lmie_solution_batch(): case %d\n", i);
+                    rc = -1;
                }
+          /* device batches of compatible cases of the chunk, in input order */
+          for (i = j0; rc == 0 && i < j1; ++i) {
+               int m = 0, base = np, off = 0;
+               if (done[i])
+                    continue;
+               for (k = i; k < j1; ++k) {
+                    if (done[k] || (k != i && !jobs_compatible(&jobs[i], &jobs[k])))
+                         continue;
+                    P[np] = jobs[k].P;
+                    P[np].precision = precision;
+                    R[np] = jobs[k].R;
+                    pos2job[np] = k;
+                    done[k] = 1;
+                    ++np;
+                    ++m;
+                    if (jobs[i].P.save_control != 0)
+                         break;
+               }
+               while (rc == 0 && off < m) {
+                    const int f = lmieb_device_fit(m - off, P + base + off);
+                    const long long t = lmieb_device_submit(f, P + base + off, R + base + off, first);
+                    first = 0;
+                    if (t < 0) {
+                         fprintf(stderr, "ERROR: lmie_solution_batch(): device solve\n");
+                         rc = -1;
+                         break;
+                    }
+                    tk[s][q] = t;
+                    tb[s][q] = base + off;
+                    te[s][q] = base + off + f;
+                    ++q;
+                    off += f;
+               }
+          }
+          ct[s].n = q;
+          cj0[s] = j0;
+          cj1[s] = j1;
+          /* the previous chunk's results */
+          if (ct[o].n && finish_chunk(&ct[o], jobs, cj0[o], cj1[o], pos2job, tb[o], te[o], R, n_threads,
+                                      rc == 0, &t_fin))
+               rc = -1;
+          if (rc != 0)
+               break;
      }
-     t0 = wall_ms();
-     if (rc == 0)
-          run_jobs(jobs, n_cases, 1, n_threads);
-     lmieb_host_phase(4, wall_ms() - t0);
+     for (c = 0; c < 2; ++c) {
+          const int s = ((n_cases + per - 1) / per - 1 + c) & 1;   /* the last chunk, then any other left */
+          if (ct[s].n && finish_chunk(&ct[s], jobs, cj0[s], cj1[s], pos2job, tb[s], te[s], R, n_threads,
+                                      rc == 0, &t_fin))
+               rc = -1;
+     }
+     lmieb_host_phase(0, t_prep);
+     lmieb_host_phase(4, t_fin);
      for (i = 0; i < n_cases; ++i)
           job_free(&jobs[i]);
-     free(jobs); free(P); free(R); free(done);
+     for (c = 0; c < 2; ++c) {
+          free(tk[c]); free(tb[c]); free(te[c]);
+     }
+     free(jobs); free(P); free(R); free(done); free(pos2job);
      return rc;
 }

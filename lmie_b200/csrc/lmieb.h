@@ -81,6 +81,17 @@ int lmieb_device_solve(const lmieb_problem *p, lmieb_result *r);
  * into sub-batches that fit the device memory budget. */
 int lmieb_device_solve_batch(int n, const lmieb_problem *p, lmieb_result *r);
 
+/* Pipelined form of lmieb_device_solve_batch for callers that overlap their
+ * own host work with the device: lmieb_device_fit gives how many of p[0..n)
+ * fit one sub-batch; lmieb_device_submit packs them and queues their device
+ * work (first != 0 resets the timing and work counters), returning a ticket
+ * (>= 0) or -1; lmieb_device_collect waits for a ticket and unpacks its
+ * results into the lmieb_result arrays given at submission (0 or -1).  Two
+ * sub-batches can be in flight; submitting a third collects the oldest. */
+int lmieb_device_fit(int n, const lmieb_problem *p);
+long long lmieb_device_submit(int n, const lmieb_problem *p, lmieb_result *r, int first);
+int lmieb_device_collect(long long ticket);
+
 /* Records the time (ms) of host phase `phase` (0 prepare, 4 finish) of the
  * current batch call; phases 1-3 are timed inside the device layer. */
 void lmieb_host_phase(int phase, double ms);
