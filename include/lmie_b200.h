@@ -144,12 +144,13 @@ int lmieb_last_timing(double *ms, int n);
 /* Re-runs the device stages 1..7 of the last solve `reps` times on the
  * inputs still resident in device memory (no host work, no copies); only
  * defined when that solve ran as one sub-batch (see lmieb_set_pipeline),
- * else returns -1.  Each
- * repetition bracketed by CUDA events on the library's stream; with
- * flush_l2 a 256 MiB buffer is written before each repetition (outside the
- * timed interval).  Returns the summed device time in *ms_total and the
- * summed per-stage times in ms_stage[0..LMIEB_N_STAGES-1] (either may be
- * NULL).  Returns 0 or -1. */
+ * else returns -1.  The kernel sequence is captured once per resident solve
+ * into a CUDA graph; each replay is bracketed by CUDA events on the
+ * library's stream, and with flush_l2 a 256 MiB buffer is written before each
+ * repetition (outside the timed interval).  Returns the summed device time of
+ * the replays in *ms_total, and in ms_stage[0..LMIEB_N_STAGES-1] the summed
+ * per-stage times of as many further runs launched kernel by kernel between
+ * events (either pointer may be NULL).  Returns 0 or -1. */
 int lmieb_rerun_device(int reps, int flush_l2, double *ms_total, double *ms_stage);
 
 /* Algorithmic work of the last solve: flops[0] angular S1/S2 contraction,

@@ -60,6 +60,7 @@ struct Slot {
     Plan *plan = nullptr;
     cudaEvent_t done = nullptr;
     bool have_plan = false;
+    cudaGraphExec_t graph = nullptr;   // the plan's kernel sequence, captured for re-runs
     Pending pend;
 };
 
@@ -206,6 +207,11 @@ int ensure_ready() {
     return 0;
 }
 
+void drop_graph(Slot &S) {
+    if (S.graph) cudaGraphExecDestroy(S.graph);
+    S.graph = nullptr;
+}
+
 int ensure_device(Slot &S, size_t bytes) {
     if (bytes <= S.dcap) return 0;
     if (S.dbuf) LMIEB_CUDA_TRY(cudaFree(S.dbuf));
@@ -244,7 +250,10 @@ int ensure_gl_pool(size_t doubles) {
     }
     c.gl_pool = np;
     c.gl_cap = want;
-    for (Slot &S : c.slot) S.have_plan = false;   // their plans point at the old pool
+    for (Slot &S : c.slot) {   // their plans point at the old pool
+        S.have_plan = false;
+        drop_graph(S);
+    }
     return 0;
 }
 
@@ -336,6 +345,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     Ctx &c = g_ctx;
     const double t_pack = now_ms();
     S.have_plan = false;
+    drop_graph(S);
     Plan &L = *S.plan;
     L = Plan();
     const lmieb_problem &p0 = ps[0];
@@ -1129,19 +1139,47 @@ extern "C" int lmieb_rerun_device(int reps, int flush_l2, double *ms_total, doub
         return -1;
     }
     if (flush_l2 && !c.flush) LMIEB_CUDA_TRY(cudaMalloc((void **) &c.flush, FLUSH_BYTES));
+    Slot &S = c.slot[c.last_slot];
     const bool was = c.timing;
-    c.timing = true;
+    // the plan's kernel sequence as one CUDA graph (captured once per plan)
+    if (!S.graph) {
+        c.timing = false;
+        cudaGraph_t g = nullptr;
+        LMIEB_CUDA_TRY(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
+        const int rc = run_kernels(*S.plan);
+        const cudaError_t ec = cudaStreamEndCapture(c.stream, &g);
+        c.timing = was;
+        if (rc || ec != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            fprintf(stderr, "ERROR: lmieb_rerun_device: graph capture failed (%s)\n", cudaGetErrorString(ec));
+            return -1;
+        }
+        const cudaError_t ei = cudaGraphInstantiate(&S.graph, g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) {
+            S.graph = nullptr;
+            fprintf(stderr, "ERROR: lmieb_rerun_device: %s\n", cudaGetErrorString(ei));
+            return -1;
+        }
+    }
     double total = 0., st[NSTAGE] = {};
     cudaEvent_t e0 = c.ev[0], e1 = c.ev[NSTAGE];
     for (int i = 0; i < reps; ++i) {
         if (flush_l2) LMIEB_CUDA_TRY(cudaMemsetAsync(c.flush, i & 0xff, FLUSH_BYTES, c.stream));
-        cudaEventRecord(e0, c.stream);
-        if (run_kernels(*c.slot[c.last_slot].plan)) { c.timing = was; return -1; }
-        cudaEventRecord(e1, c.stream);
+        LMIEB_CUDA_TRY(cudaEventRecord(e0, c.stream));
+        LMIEB_CUDA_TRY(cudaGraphLaunch(S.graph, c.stream));
+        LMIEB_CUDA_TRY(cudaEventRecord(e1, c.stream));
         LMIEB_CUDA_TRY(cudaEventSynchronize(e1));
         float ms = 0.f;
         cudaEventElapsedTime(&ms, e0, e1);
         total += ms;
+    }
+    // stage times: the same kernel sequence launched one by one between events
+    c.timing = true;
+    for (int i = 0; i < reps; ++i) {
+        if (flush_l2) LMIEB_CUDA_TRY(cudaMemsetAsync(c.flush, i & 0xff, FLUSH_BYTES, c.stream));
+        if (run_kernels(*S.plan)) { c.timing = was; return -1; }
+        LMIEB_CUDA_TRY(cudaEventSynchronize(c.ev[8]));
         for (int k = 1; k < 8; ++k) {
             float sm = 0.f;
             cudaEventElapsedTime(&sm, c.ev[k], c.ev[k + 1]);

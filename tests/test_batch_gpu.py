@@ -65,3 +65,45 @@ def test_batch_reports_bad_case():
     cases[1] = dataclasses.replace(cases[1], calc_pf=1)
     got = abi.solve_batch(libs.product(), cases, n_threads=2)
     assert got[0].rc == -1
+
+
+def test_rerun_replays_resident_batch_and_refuses_split_calls():
+    """lmieb_rerun_device replays the resident batch as a captured CUDA graph
+    only when the last call ran as one part."""
+    import ctypes as C
+    import lmie_b200
+    lib = lmie_b200.library()
+    cases = workloads.batched_uneven(64)
+    tot = C.c_double()
+    st = (C.c_double * lmie_b200.N_STAGES)()
+    try:
+        lib.lmieb_set_pipeline(1)
+        assert all(r.rc == 0 for r in abi.solve_batch(lib, cases, n_threads=4))
+        assert lib.lmieb_rerun_device(2, 0, C.byref(tot), st) == 0
+        assert tot.value > 0 and st[3] > 0
+        lib.lmieb_set_pipeline(4)
+        assert all(r.rc == 0 for r in abi.solve_batch(lib, cases, n_threads=4))
+        assert lib.lmieb_rerun_device(1, 0, C.byref(tot), st) == -1
+    finally:
+        lib.lmieb_set_pipeline(0)
+
+
+def test_pipelined_batch_matches_one_part():
+    """Cutting a batch into parts changes only how the work is scheduled: the
+    radius groups of the angular stage are planned per part, so the order of
+    the partial sums (not the arithmetic) can differ, at round-off level."""
+    import lmie_b200
+    lib = lmie_b200.library()
+    cases = workloads.batched_uneven(96)
+    try:
+        lib.lmieb_set_pipeline(1)
+        one = abi.solve_batch(lib, cases, n_threads=4)
+        lib.lmieb_set_pipeline(5)
+        many = abi.solve_batch(lib, cases, n_threads=4)
+    finally:
+        lib.lmieb_set_pipeline(0)
+    for i, (a, b) in enumerate(zip(one, many)):
+        assert a.rc == 0 and b.rc == 0 and a.n_coef == b.n_coef
+        err = libs.compare(b, a)
+        bad = {k: v for k, v in err.items() if v > 1e-13}
+        assert not bad, (i, bad)
