@@ -163,6 +163,16 @@ class CBatch:
                       C.c_int, C.c_int, C.c_int]
         return f(len(self.cases), self.ins, self.outs, 0, 0, n_threads, precision)
 
+    def autotune(self, n_threads: int, precision: int) -> dict:
+        f = self.lib.lmie_solution_autotune
+        f.restype = C.c_int
+        f.argtypes = [C.c_int, C.POINTER(abi.lmie_in_data), C.POINTER(abi.lmie_out_data), C.c_int, C.c_int,
+                      C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        ch, it, ms = C.c_int(), C.c_double(), C.c_double()
+        if f(len(self.cases), self.ins, self.outs, n_threads, precision, C.byref(ch), C.byref(it), C.byref(ms)):
+            raise RuntimeError("lmie_solution_autotune failed")
+        return {"pipeline_parts": ch.value, "angular_items_per_sm": it.value, "ms_per_call": ms.value}
+
     def solve_each(self, n_threads: int, count: int = -1) -> int:
         for i in range(len(self.cases) if count < 0 else count):
             rc = self.lib.lmie_solution(C.byref(self.ins[i]), C.byref(self.outs[i]), 0, 0, n_threads, 0)
@@ -356,6 +366,7 @@ def run_b200(args) -> int:
         n_job = N_CASES
     batch = CBatch(lib, cases)
 
+    tuned = batch.autotune(threads, abi.PRECISION_FP64)
     for _ in range(args.warmup):
         if batch.solve_batch(threads) != 0:
             raise RuntimeError("lmie_solution_batch failed")
@@ -398,7 +409,8 @@ def run_b200(args) -> int:
 
     # the same batch with the angular contraction on the tensor cores
     tf32 = abi.PRECISION_TF32X3
-    lib.lmieb_set_pipeline(0)
+    lib.lmieb_set_pipeline(tuned["pipeline_parts"])
+    tuned_tc = batch.autotune(threads, tf32)
     for _ in range(2):
         if batch.solve_batch(threads, tf32) != 0:
             raise RuntimeError("lmie_solution_batch2 failed")
@@ -419,7 +431,7 @@ def run_b200(args) -> int:
         raise RuntimeError("device re-run failed")
     barrier()
     split_dev_ms = max_over_ranks(ms_total.value)
-    lib.lmieb_set_pipeline(0)
+    lib.lmieb_set_pipeline(tuned["pipeline_parts"])
     clk = clocks.stop()
     split_stage_ms = {n: ms_stage[i] / args.steps for i, n in enumerate(lmie_b200.STAGES)}
     split_ang_ms = ms_stage[3] / args.steps
@@ -448,6 +460,7 @@ def run_b200(args) -> int:
             "e2e": n_job * args.steps / split_e2e_s, "unit": UNIT,
             "ms_per_step": split_dev_ms / args.steps, "stage_ms": split_stage_ms,
             "dtype": "f64 with tf32x3 angular contraction (fp32 accumulation in segments of 64 orders)",
+            "autotuned": tuned_tc,
             "error_vs_fp64": errs,
             "roofline": {
                 "kernel": "k_angular_tc (tcgen05.mma kind::tf32, 3 products per operand pair)",
@@ -492,6 +505,7 @@ def run_b200(args) -> int:
             "config": {"workload": WORKLOAD, "n_cases": N_CASES, "n_derivs": 4,
                        "parallelism": (f"independent batches x{world}" if args.scaling == "weak" else
                                        f"one batch in {world} cost-balanced case ranges"),
+                       "autotuned": tuned,
                        "l2": "flushed (256 MiB write) before every timed device step; "
                              "the batch's working set (~8 GB) exceeds L2 in any case"},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d.value),

@@ -38,6 +38,9 @@ def library() -> C.CDLL:
         lib.lmieb_tc_selftest.argtypes = [C.c_int, C.POINTER(C.c_double)]
         lib.lmieb_last_host_timing.argtypes = [C.POINTER(C.c_double), C.c_int]
         lib.lmieb_set_pipeline.argtypes = [C.c_int]
+        lib.lmieb_set_work_granularity.argtypes = [C.c_int, C.c_double]
+        lib.lmieb_get_work_granularity.argtypes = [C.c_int]
+        lib.lmieb_get_work_granularity.restype = C.c_double
         _lib = lib
     return _lib
 

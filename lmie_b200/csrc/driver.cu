@@ -92,6 +92,11 @@ struct Ctx {
 
 Ctx g_ctx;
 
+// Work items per SM the angular stage is cut into ([0] FP64 kernel, [1]
+// tensor-core kernel): finer items balance uneven cases, coarser ones cut the
+// per-item overhead; set by lmieb_set_work_granularity (the autotuner).
+double g_items_per_sm[2] = {4., 2.};
+
 // fn(i) for every i in [0, n) on the host's cores (dynamic chunks of `grain`)
 template <class F>
 void parallel_for(int n, int grain, F &&fn) {
@@ -543,7 +548,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
             if (C.n_qang > 0) W += wc[k] * ((C.nh + TC_HALF - 1) / TC_HALF);
         }
         cg0[ncase] = (int) tg_r0.size();
-        const double wt = std::max(W / (2. * c.sms), 8.);    // chunks per item
+        const double wt = std::max(W / (g_items_per_sm[1] * c.sms), 8.);    // chunks per item
         std::vector<std::pair<double, AngItem>> tmp;
         for (int k = 0; k < ncase; ++k) {
             DevCase &C = cs[k];
@@ -588,7 +593,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
             wc[k] = (double) (cs1[k + 1] - cs1[k]) * cs[k].nh;
             W += wc[k];
         }
-        const double wt = std::max(W / (4. * c.sms), 64. * 2 * 64 * 16);   // work per block
+        const double wt = std::max(W / (g_items_per_sm[0] * c.sms), 64. * 2 * 64 * 16);   // work per block
         std::vector<std::pair<double, AngItem>> tmp;
         for (int k = 0; k < ncase; ++k) {
             DevCase &C = cs[k];
@@ -1291,4 +1296,20 @@ extern "C" int lmieb_last_host_timing(double *ms, int n) {
     std::lock_guard<std::mutex> lock(g_mu);
     for (int i = 0; i < n && i < LMIEB_N_HOST; ++i) ms[i] = g_ctx.host_ms[i];
     return LMIEB_N_HOST;
+}
+
+extern "C" int lmieb_set_work_granularity(int precision, double items_per_sm) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    if ((precision != LMIEB_PRECISION_FP64 && precision != LMIEB_PRECISION_TF32X3) || !(items_per_sm >= 0.25) ||
+        items_per_sm > 64.) {
+        fprintf(stderr, "ERROR: lmieb_set_work_granularity: precision %d, items per SM %g\n", precision, items_per_sm);
+        return -1;
+    }
+    g_items_per_sm[precision == LMIEB_PRECISION_TF32X3 ? 1 : 0] = items_per_sm;
+    return 0;
+}
+
+extern "C" double lmieb_get_work_granularity(int precision) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    return g_items_per_sm[precision == LMIEB_PRECISION_TF32X3 ? 1 : 0];
 }

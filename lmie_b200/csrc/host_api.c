@@ -894,3 +894,52 @@ int lmie_solution_batch2(int n_cases, lmie_in_data *in, lmie_out_data *out, int 
      free(jobs); free(P); free(R); free(done); free(pos2job);
      return rc;
 }
+
+
+/* ---- autotuner ------------------------------------------------------------ */
+
+int lmie_solution_autotune(int n_cases, lmie_in_data *in, lmie_out_data *out, int n_threads, int precision,
+                           int *best_chunks, double *best_items, double *best_ms) {
+     static const int chunk_c[] = {1, 2, 4, 6};
+     static const double items_fp64[] = {2., 4., 8.}, items_tc[] = {1., 2., 4.};
+     const double *items = precision == LMIEB_PRECISION_TF32X3 ? items_tc : items_fp64;
+     const int keep = g_pipeline;
+     const double keep_items = lmieb_get_work_granularity(precision);
+     int a, b, r, bc = keep, rc = 0;
+     double bi = keep_items, bt = -1.;
+     if (n_cases < 1 || (precision != LMIEB_PRECISION_FP64 && precision != LMIEB_PRECISION_TF32X3)) {
+          fprintf(stderr, "ERROR: lmie_solution_autotune(): invalid arguments\n");
+          return -1;
+     }
+     for (a = 0; a < 4 && rc == 0; ++a) {
+          if (chunk_c[a] > 1 && n_cases < 2 * chunk_c[a])
+               continue;
+          for (b = 0; b < 3 && rc == 0; ++b) {
+               double t = 0.;
+               g_pipeline = chunk_c[a];
+               lmieb_set_work_granularity(precision, items[b]);
+               /* one call to settle the buffers, then the faster of two */
+               for (r = 0; r < 3 && rc == 0; ++r) {
+                    const double t0 = wall_ms();
+                    rc = lmie_solution_batch2(n_cases, in, out, 0, 0, n_threads, precision);
+                    const double dt = wall_ms() - t0;
+                    if (r == 1 || (r == 2 && dt < t))
+                         t = dt;
+               }
+               if (rc == 0 && (bt < 0. || t < bt)) {
+                    bt = t;
+                    bc = chunk_c[a];
+                    bi = items[b];
+               }
+          }
+     }
+     g_pipeline = rc == 0 ? bc : keep;
+     lmieb_set_work_granularity(precision, rc == 0 ? bi : keep_items);
+     if (best_chunks)
+          *best_chunks = g_pipeline;
+     if (best_items)
+          *best_items = lmieb_get_work_granularity(precision);
+     if (best_ms)
+          *best_ms = bt;
+     return rc;
+}

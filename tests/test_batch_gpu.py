@@ -107,3 +107,25 @@ def test_pipelined_batch_matches_one_part():
         err = libs.compare(b, a)
         bad = {k: v for k, v in err.items() if v > 1e-13}
         assert not bad, (i, bad)
+
+
+def test_autotune_picks_a_candidate_and_keeps_results():
+    import ctypes as C
+    import bench
+    import lmie_b200
+    lib = lmie_b200.library()
+    cases = workloads.batched_uneven(64)
+    ref = abi.solve_batch(lib, cases, n_threads=4)
+    b = bench.CBatch(lib, cases)
+    try:
+        got = b.autotune(4, abi.PRECISION_FP64)
+        assert got["pipeline_parts"] in (1, 2, 4, 6)
+        assert got["angular_items_per_sm"] in (2.0, 4.0, 8.0)
+        assert got["ms_per_call"] > 0
+        after = abi.solve_batch(lib, cases, n_threads=4)
+        for i, (a, r) in enumerate(zip(after, ref)):
+            err = libs.compare(a, r)
+            assert not {k: v for k, v in err.items() if v > 1e-13}, i
+    finally:
+        lib.lmieb_set_pipeline(0)
+        lib.lmieb_set_work_granularity(0, C.c_double(4.0))
