@@ -155,10 +155,7 @@ struct Plan {
     int ncase = 0;
     int nd1c = 0, n_ang_launch = 0;
     int want_gc = 0, want_lc = 0, pf_from = 0, save_control = 0, n_qang0 = 0;
-    int2 *tiles = nullptr;
-    int *tstart = nullptr;
-    double4 *rec = nullptr;
-    double *rsp = nullptr, *coef = nullptr, *rs = nullptr, *sums = nullptr, *part = nullptr;
+    double *ck = nullptr, *coef = nullptr, *rs = nullptr, *sums = nullptr, *part = nullptr;
     double *pfacc = nullptr, *pfn = nullptr, *ckpt = nullptr, *exq = nullptr;
     AngItem *ang = nullptr;
     int n_ang = 0;
@@ -277,9 +274,8 @@ int run_kernels(Plan &L) {
         for (int ch = 0; ch < (L.nd1c > 0 ? L.nd1c : 1); ++ch) {
             const int c0 = ch * 4;
             const int nc = std::max(0, std::min(4, B.nd1 - c0));
-            if (launch_coef(s, B, nc, c0, ch == 0, L.tiles, L.rec, L.coef, L.bop, L.rsp)) return -1;
+            if (launch_coef(s, B, nc, c0, ch == 0, L.ck, L.coef, L.bop, L.rs)) return -1;
         }
-        if (launch_tile_reduce(s, B, L.tstart, L.rsp, L.rs)) return -1;
         stage(2);
         if (launch_reduce_scalars(s, B, L.rs, L.sums, L.save_control == 1 ? L.o_save1 : nullptr)) return -1;
         stage(3);
@@ -336,7 +332,8 @@ size_t case_bytes(const lmieb_problem &p) {
     long long tot = 0;
     for (int r = 0; r < p.n; ++r) tot += p.n1r[r] + 1;
     const size_t ncol = 1 + p.nd;
-    size_t b = (size_t) tot * 32 * 2 * (1 + p.nd1);                    // rec + coef
+    size_t b = (size_t) tot * 32 * (1 + p.nd1);                        // coef
+    b += (size_t) (tot / K1_B + p.n) * 8 * k1_ck_width(std::min(p.nd1, 4));   // K1 checkpoints
     b += (size_t) p.n * (64 + 8 * ncol + 40 * (1 + p.nd1));           // per-radius arrays, sums
     b += (size_t) 4 * ncol * p.n_qang * 8 * 8;                        // partials (groups), pf, pfn
     b += (size_t) ncol * 6 * p.n_coef * 8 * (3 + (p.n_qang / 2 + 31) / 32);   // expansion partials + outputs
@@ -367,14 +364,15 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
 
     // ---- case table and batch-wide per-radius arrays (filled per case in parallel) ----
     std::vector<DevCase> cs(ncase);
-    std::vector<int> cr0(ncase + 1, 0), ct0(ncase + 1, 0), cn1max(ncase, 1);
+    std::vector<int> cr0(ncase + 1, 0), cn1max(ncase, 1);
+    std::vector<long long> ct0(ncase + 1, 0);      // K1 checkpoint blocks before each case
     std::vector<long long> cs1(ncase + 1, 0), cs2(ncase, 0);
     parallel_for(ncase, 16, [&](int k) {
         const lmieb_problem &p = ps[k];
-        int t = 0, mx = 1;
-        long long a = 0, b = 0;
+        int mx = 1;
+        long long a = 0, b = 0, t = 0;
         for (int i = 0; i < p.n; ++i) {
-            t += (p.n1r[i] + 126) / 127;
+            t += (p.n1r[i] + K1_B - 1) / K1_B;
             a += p.n1r[i];
             b += p.n2r[i];
             mx = std::max(mx, p.n1r[i]);
@@ -395,12 +393,11 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     }
     const int R = cr0[ncase];
     std::vector<double> x(R), xl((size_t) std::max(nd1, 1) * R), w((size_t) ncol * R);
-    std::vector<int> n1r(R), n2r(R), rcase(R), tstart(R + 1);
-    std::vector<long long> off(R + 1), offp(R + 1);
-    std::vector<int2> tiles(ct0[ncase]);
+    std::vector<int> n1r(R), n2r(R), rcase(R);
+    std::vector<long long> off(R + 1), ckoff(R + 1);
     std::vector<cplx> ml((size_t) std::max(1, ncase * nd));
     std::vector<double> laml((size_t) std::max(1, ncase * nd));
-    off[0] = offp[0] = 0;
+    off[0] = ckoff[0] = 0;
     parallel_for(ncase, 16, [&](int k) {
         const lmieb_problem &p = ps[k];
         DevCase &C = cs[k];
@@ -422,7 +419,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
             laml[(size_t) k * nd + kk] = p.lambda_l[kk];
         }
         long long o = cs1[k];
-        int t = ct0[k];
+        long long t = ct0[k];
         for (int i = 0, r = cr0[k]; i < p.n; ++i, ++r) {
             x[r] = p.x[i];
             for (int q = 0; q < nd1; ++q) xl[(size_t) q * R + r] = p.xl[(size_t) q * p.n + i];
@@ -432,14 +429,11 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
             rcase[r] = k;
             o += n1r[r];
             off[r + 1] = o;
-            offp[r + 1] = o + r + 1;
-            tstart[r] = t;
-            for (int j0 = 1; j0 <= n1r[r]; j0 += 127) tiles[t++] = make_int2(r, j0);
+            t += (n1r[r] + K1_B - 1) / K1_B;
+            ckoff[r + 1] = t;
         }
     });
-    tstart[R] = ct0[ncase];
-    const long long tot = off[R], totp = offp[R];
-    const int ntiles = (int) tiles.size();
+    const long long tot = off[R], ckn = ckoff[R];
 
     // ---- order tables ----
     std::vector<double> fv((size_t) 4 * (n1max + 2), 0.);
@@ -676,7 +670,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     {
         long long nl = 0;
         if (L.save_control != 2) {
-            nl += (long long) std::max(L.nd1c, 1) * 2 + 1 + 1;                  // K1a+K1b per chunk, tiles, K2
+            nl += (long long) std::max(L.nd1c, 1) + 1;                          // K1 per chunk, K2
             if (L.n_ang > 0) nl += L.n_ang_launch + 1;                          // K3 + group reduction
         } else {
             nl += 1 + (L.n_qang0 > 0);
@@ -710,8 +704,8 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         auto add = [&](size_t b) { in_bytes += pad(b); };
         add(cs.size() * sizeof(DevCase)); add((size_t) R * 8); add(xl.size() * 8); add(w.size() * 8);
         add((size_t) R * 4); add((size_t) R * 4); add((size_t) R * 4);
-        add((size_t) (R + 1) * 8); add((size_t) (R + 1) * 8); add((size_t) (R + 1) * 4);
-        add(tiles.size() * 8); add(fv.size() * 8); add(rc.size() * 8); add(ml.size() * 16); add(laml.size() * 8);
+        add((size_t) (R + 1) * 8); add((size_t) (R + 1) * 8);
+        add(fv.size() * 8); add(rc.size() * 8); add(ml.size() * 16); add(laml.size() * 8);
         add((size_t) nd1 * 4); add((size_t) nd2 * 4); add(mu_user.size() * 8);
         add(ang.size() * sizeof(AngItem)); add(ex.size() * sizeof(ExpItem));
         add(tc_pos.size() * 4); add(tc_roff.size() * 8); add(tg_r0.size() * 4); add(tg_n.size() * 4);
@@ -738,9 +732,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     int *h_n2r = put(hp, ho, n2r.data(), (size_t) R);
     int *h_rcase = put(hp, ho, rcase.data(), (size_t) R);
     long long *h_off = put(hp, ho, off.data(), (size_t) R + 1);
-    long long *h_offp = put(hp, ho, offp.data(), (size_t) R + 1);
-    int *h_tstart = put(hp, ho, tstart.data(), (size_t) R + 1);
-    int2 *h_tiles = put(hp, ho, tiles.data(), tiles.size());
+    long long *h_ckoff = put(hp, ho, ckoff.data(), (size_t) R + 1);
     double *h_fv = put(hp, ho, fv.data(), fv.size());
     double *h_rc = put(hp, ho, rc.data(), rc.size());
     cplx *h_ml = put(hp, ho, ml.data(), ml.size());
@@ -786,8 +778,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     {
         auto add = [&](size_t b) { dev_bytes += pad(b); };
         if (L.save_control != 2) {
-            add((size_t) (1 + nd1) * (size_t) totp * 32);
-            add((size_t) (1 + nd1) * 5 * (size_t) ntiles * 8);
+            add((size_t) ckn * 8 * k1_ck_width(std::min(nd1, 4)));
             if (L.tc) add((size_t) bop_floats * 4);
             else add((size_t) (1 + nd1) * (size_t) tot * 32);
             add((size_t) (1 + nd1) * 5 * (size_t) R * 8);
@@ -827,10 +818,9 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     B.n1r = (const int *) dptr(h_n1r);
     B.n2r = (const int *) dptr(h_n2r);
     B.off = (const long long *) dptr(h_off);
-    B.offp = (const long long *) dptr(h_offp);
+    B.ckoff = (const long long *) dptr(h_ckoff);
     B.tot = tot;
-    B.totp = totp;
-    B.ntiles = ntiles;
+    B.ckn = ckn;
     B.fv = (const double *) dptr(h_fv);
     B.rc = (const double *) dptr(h_rc);
     B.mu_pool = c.gl_pool;
@@ -843,8 +833,6 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         B.tg_nk = (const int *) dptr(h_tgnk);
         B.tg_off = (const long long *) dptr(h_tgoff);
     }
-    L.tiles = (int2 *) dptr(h_tiles);
-    L.tstart = (int *) dptr(h_tstart);
     L.ang = (AngItem *) dptr(h_ang);
     L.ex = (ExpItem *) dptr(h_ex);
     L.pf_start = (long long *) dptr(h_pfs);
@@ -858,8 +846,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         L.w2 = (double *) dptr(h_w2);
     }
     if (L.save_control != 2) {
-        L.rec = A.take<double4>((size_t) (1 + nd1) * (size_t) totp);
-        L.rsp = A.take<double>((size_t) (1 + nd1) * 5 * (size_t) ntiles);
+        L.ck = A.take<double>((size_t) ckn * k1_ck_width(std::min(nd1, 4)));
         if (L.tc) {
             L.bop_bytes = (size_t) bop_floats * 4;
             L.bop = A.take<float>((size_t) bop_floats);

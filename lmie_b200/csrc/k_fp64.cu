@@ -2,11 +2,10 @@
 // batch of independent cases (one lmie_solution() is a batch of one).
 //
 //   k_gauss          Gauss-Legendre angles on [-1,1]        <- misc/rtutil_math.c:73-129,231-316
-//   k_recur<NC>      per-radius sequential recurrences (D_n, psi, chi)
-//                                                           <- src/lmie_core.c:263-405
-//   k_abcoef<NC>     a_n, b_n, their tangent-linear forms, expansion
-//                    coefficients and per-radius sums, per (radius, order tile)
-//                                                           <- src/lmie_core.c:453-652
+//   k_mie<NC>        per radius: D_n, psi, chi recurrences (checkpointed
+//                    downward sweeps, replayed per block), a_n, b_n, their
+//                    tangent-linear forms, expansion coefficients and the
+//                    per-radius sums                        <- src/lmie_core.c:263-652
 //   k_reduce_scalars radius reduction of Cext/Csca/Cbak/g    <- src/lmie_core.c:537-611,
 //                                                              src/lmie_schedule.c:334-338
 //   k_angular<..>    S1/S2 accumulation over orders and the phase-matrix
@@ -84,15 +83,25 @@ __global__ void k_gauss(int npairs, const int *__restrict__ pt, const int *__res
 }
 
 // ---------------------------------------------------------------------------
-// K1a: one thread per radius runs the three recurrences that are sequential
-// in the order n -- D_n(mx) downward from n2, the psi ratio downward from n1,
-// then psi and chi upward -- and stores psi_j, chi_j, D_j (j = 0..n1) for the
-// value and the NC tangent-linear columns of this chunk.  Storage rec[col] is
-// order-contiguous per radius ({psi, chi, Re D, Im D} per order), so K1b reads
-// it coalesced.
+// K1: one thread per radius.  The downward recurrences -- D_n(mx) from n2 and
+// the psi ratio from n1, each with its tangent-linear columns -- keep only
+// their values at the top of every block of K1_B orders (checkpoints in ck);
+// the ascending pass replays each block from its checkpoint into local
+// arrays (the same operations, so the same values), runs psi and chi upward,
+// forms a_n, b_n and their tangent-linear columns, writes the expansion
+// coefficients fv4 (a +- b) (coef, or the tensor-core B operand) and sums the
+// per-radius cross sections rs[(col*5 + q)*R + r], q: se, ss, Re sb, Im sb, sg,
+// in order.  Follows src/lmie_core.c:298-370 (psi ratio, psi, chi), 386-440
+// (D), 455-510 (a, b and tangents), 515-590 (cross-section and asymmetry
+// sums per radius).
 // ---------------------------------------------------------------------------
+
 template <int NC>
-__global__ void __launch_bounds__(64) k_recur(DevBatch B, int c0, int write_value, double4 *__restrict__ rec) {
+__global__ void __launch_bounds__(64) k_mie(DevBatch B, int c0, int write_value, double *__restrict__ ck,
+                                            double *__restrict__ coef, float *__restrict__ bop,
+                                            double *__restrict__ rs) {
+    constexpr int CC = 1 + NC;
+    constexpr int CW = k1_ck_width(NC);               // D (2), D_l (2 NC), ratio (1), ratio_l (NC)
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= B.R) return;
     const int R = B.R;
@@ -100,28 +109,35 @@ __global__ void __launch_bounds__(64) k_recur(DevBatch B, int c0, int write_valu
     const int n1 = B.n1r[r], n2 = B.n2r[r];
     const double x = B.x[r];
     const double xinv = 1. / x;
-    const cplx m = C.m;
+    const cplx m = C.m, minv = C.minv;
     const cplx z = mk(m.re * x, m.im * x);
     const cplx zinv = cinv(z);
-    const size_t totp = (size_t) B.totp;
-    const size_t base = (size_t) B.offp[r];
-    double4 *R0 = rec + base;                         // value column
+    const int nb = (n1 + K1_B - 1) / K1_B;
+    double *ckr = ck + (size_t) B.ckoff[r] * CW;     // nb blocks of CW doubles
+    const double *fv1 = B.fv, *fv3 = B.fv + 2 * (B.n1max + 2), *fv4 = B.fv + 3 * (B.n1max + 2);
 
     double xl[NC > 0 ? NC : 1];
-    cplx zl[NC > 0 ? NC : 1];
+    cplx zl[NC > 0 ? NC : 1], ml[NC > 0 ? NC : 1];
 #pragma unroll
     for (int k = 0; k < NC; ++k) {
         const int kk = B.idx1[c0 + k];
         xl[k] = B.xl[(size_t) (c0 + k) * R + r];
-        zl[k] = B.m_l[C.ml_off + kk] * x + m * xl[k];
+        ml[k] = B.m_l[C.ml_off + kk];
+        zl[k] = ml[k] * x + m * xl[k];
     }
-#define RC(k) (rec + (size_t) (1 + c0 + (k)) * totp + base)
 
-    // D_n downward from D_{n2} = 0; orders 1..n1 kept
+    // ---- downward sweeps: checkpoints only ----
     {
         cplx D = mk(0., 0.), Dl[NC > 0 ? NC : 1];
 #pragma unroll
         for (int k = 0; k < NC; ++k) Dl[k] = mk(0., 0.);
+        for (int c = 0; c < nb; ++c)
+            if (c * K1_B + K1_B >= n2) {
+                double *q = ckr + (size_t) c * CW;
+                q[0] = q[1] = 0.;
+#pragma unroll
+                for (int k = 0; k < NC; ++k) q[2 + 2 * k] = q[3 + 2 * k] = 0.;
+            }
         for (int j = n2 - 1; j >= 1; --j) {
             const cplx c1 = (j + 1.) * zinv;
             const cplx ic2 = cinv(D + c1);
@@ -135,25 +151,29 @@ __global__ void __launch_bounds__(64) k_recur(DevBatch B, int c0, int write_valu
                     Dl[k] = c5 + (Dl[k] + c5) * ic4;
                 }
             }
-            if (j <= n1) {
-                if (write_value) ((double2 *) (R0 + j))[1] = make_double2(D.re, D.im);
+            if (j % K1_B == 0 && j / K1_B - 1 < nb) {
+                double *q = ckr + (size_t) (j / K1_B - 1) * CW;
+                q[0] = D.re;
+                q[1] = D.im;
 #pragma unroll
-                for (int k = 0; k < NC; ++k) ((double2 *) (RC(k) + j))[1] = make_double2(Dl[k].re, Dl[k].im);
+                for (int k = 0; k < NC; ++k) {
+                    q[2 + 2 * k] = Dl[k].re;
+                    q[3 + 2 * k] = Dl[k].im;
+                }
             }
         }
     }
-    // psi ratio r_j = psi_j / psi_{j-1} downward from r_{n1} = 0.  The value
-    // ratio is parked in the value's psi slot, or -- in chunks that do not
-    // write the value column -- in the chi slot of the chunk's first column,
-    // until the upward pass replaces it.
-    double *park = write_value ? &R0[0].x : &(rec + (size_t) (1 + c0) * totp + base)[0].y;
     {
         double rn = 0., rl[NC > 0 ? NC : 1];
 #pragma unroll
         for (int k = 0; k < NC; ++k) rl[k] = 0.;
-        park[(size_t) n1 * 4] = 0.;
+        for (int c = 0; c < nb; ++c)
+            if (c * K1_B + K1_B >= n1) {
+                double *q = ckr + (size_t) c * CW + 2 + 2 * NC;
+                q[0] = 0.;
 #pragma unroll
-        for (int k = 0; k < NC; ++k) RC(k)[n1].x = 0.;
+                for (int k = 0; k < NC; ++k) q[1 + k] = 0.;
+            }
         for (int j = n1 - 1; j >= 1; --j) {
             const double a1 = (2. * j + 1.) * xinv;
             const double rnew = 1. / (a1 - rn);
@@ -163,250 +183,190 @@ __global__ void __launch_bounds__(64) k_recur(DevBatch B, int c0, int write_valu
                 for (int k = 0; k < NC; ++k) rl[k] = -(a2 * xl[k] - rl[k]) * a3;
             }
             rn = rnew;
-            park[(size_t) j * 4] = rn;
+            if (j % K1_B == 0 && j / K1_B - 1 < nb) {
+                double *q = ckr + (size_t) (j / K1_B - 1) * CW + 2 + 2 * NC;
+                q[0] = rn;
 #pragma unroll
-            for (int k = 0; k < NC; ++k) RC(k)[j].x = rl[k];
-        }
-    }
-    // psi, chi upward
-    {
-        double sinx, cosx;
-        sincos(x, &sinx, &cosx);
-        double psi = sinx, chi_p = cosx, chi_c = xinv * cosx + sinx;
-        double psil[NC > 0 ? NC : 1], chil_p[NC > 0 ? NC : 1], chil_c[NC > 0 ? NC : 1];
-#pragma unroll
-        for (int k = 0; k < NC; ++k) {
-            psil[k] = xl[k] * cosx;
-            chil_p[k] = xl[k] * -sinx;
-            chil_c[k] = (-xinv * xinv) * xl[k] * cosx + xinv * chil_p[k] + xl[k] * cosx;
-        }
-        if (write_value) {
-            R0[0].x = psi;
-            R0[0].y = chi_p;
-        }
-#pragma unroll
-        for (int k = 0; k < NC; ++k) {
-            RC(k)[0].x = psil[k];
-            RC(k)[0].y = chil_p[k];
-        }
-        // the stored ratios are read back 8 orders at a time, so the loads of
-        // a group overlap instead of serialising on L2 latency
-        constexpr int G8 = 8;
-        double rbuf[G8], rlbuf[NC > 0 ? NC : 1][G8];
-        for (int j = 1; j <= n1; ++j) {
-            const int u = (j - 1) & (G8 - 1);
-            if (u == 0) {
-#pragma unroll
-                for (int v = 0; v < G8; ++v) {
-                    const int jv = j + v <= n1 ? j + v : n1;
-                    rbuf[v] = park[(size_t) jv * 4];
-#pragma unroll
-                    for (int k = 0; k < NC; ++k) rlbuf[k][v] = RC(k)[jv].x;
-                }
-            }
-            double rj = rbuf[0];
-#pragma unroll
-            for (int v = 1; v < G8; ++v)
-                if (u == v) rj = rbuf[v];
-#pragma unroll
-            for (int k = 0; k < NC; ++k) {
-                double rl = rlbuf[k][0];
-#pragma unroll
-                for (int v = 1; v < G8; ++v)
-                    if (u == v) rl = rlbuf[k][v];
-                psil[k] = rl * psi + rj * psil[k];
-                RC(k)[j].x = psil[k];
-                RC(k)[j].y = chil_c[k];
-            }
-            psi = rj * psi;
-            if (write_value) {
-                R0[j].x = psi;
-                R0[j].y = chi_c;
-            }
-            if (j < n1) {
-                const double a1 = (2. * j + 1.) * xinv;
-                const double chi_n = a1 * chi_c - chi_p;
-#pragma unroll
-                for (int k = 0; k < NC; ++k) {
-                    const double a2l = -a1 * xl[k] * xinv;
-                    const double chil_n = a2l * chi_c + a1 * chil_c[k] - chil_p[k];
-                    chil_p[k] = chil_c[k];
-                    chil_c[k] = chil_n;
-                }
-                chi_p = chi_c;
-                chi_c = chi_n;
+                for (int k = 0; k < NC; ++k) q[1 + k] = rl[k];
             }
         }
     }
-#undef RC
-}
 
-// ---------------------------------------------------------------------------
-// K1b: one block per (radius, tile of ABT-1 orders), one thread per order.
-// Forms a_n, b_n and their tangent-linear columns from the stored
-// recurrences, writes the expansion coefficients fv4 (a +- b) and reduces the
-// tile's contributions to the extinction, scattering, backscatter and
-// asymmetry sums (the last thread's order is the next tile's first; it is
-// computed only as the neighbour a_{j+1}, b_{j+1} of the asymmetry term).
-// ---------------------------------------------------------------------------
-constexpr int ABT = 128;
-
-template <int NC>
-__global__ void __launch_bounds__(ABT) k_abcoef(DevBatch B, int c0, int write_value,
-                                                const int2 *__restrict__ tiles,
-                                                const double4 *__restrict__ rec,
-                                                double *__restrict__ coef, float *__restrict__ bop,
-                                                double *__restrict__ rsp) {
-    constexpr int CC = 1 + NC;
-    __shared__ cplx sab[2 * CC][ABT];
-    __shared__ double red[5 * CC][ABT / 32];
-    const int t = threadIdx.x;
-    const int2 tile = tiles[blockIdx.x];
-    const int r = tile.x, j0 = tile.y;
-    const DevCase &C = B.cs[B.rcase[r]];
-    const int n1 = B.n1r[r];
-    const int j = j0 + t;
-    const bool valid = j <= n1;
-    const bool owned = valid && t < ABT - 1;
-    const int R = B.R;
-    const double x = B.x[r];
-    const double xinv = 1. / x;
-    const cplx m = C.m, minv = C.minv;
-    const size_t totp = (size_t) B.totp, tot = (size_t) B.tot;
-    const size_t base = (size_t) B.offp[r];
-    const double *fv1 = B.fv, *fv3 = B.fv + 2 * (B.n1max + 2), *fv4 = B.fv + 3 * (B.n1max + 2);
-
-    cplx a = mk(0., 0.), b = mk(0., 0.), al[NC > 0 ? NC : 1], bl[NC > 0 ? NC : 1];
-    if (valid) {
-        const double4 v = rec[base + j], vp = rec[base + j - 1];
-        const cplx D = mk(v.z, v.w);
-        const cplx zeta = mk(v.x, v.y), zeta_p = mk(vp.x, vp.y);
-        const double psi = v.x, psi_p = vp.x;
-        const double tt = j * xinv;
-        const cplx ca = D * minv + tt;
-        const cplx na = ca * psi - psi_p;
-        const cplx ida = cinv(ca * zeta - zeta_p);
-        a = na * ida;
-        const cplx cb = m * D + tt;
-        const cplx nb = cb * psi - psi_p;
-        const cplx idb = cinv(cb * zeta - zeta_p);
-        b = nb * idb;
-        if (NC > 0) {
-            const cplx Dm2 = D * (minv * minv);
-            const double tx = -tt * xinv;
-#pragma unroll
-            for (int k = 0; k < NC; ++k) {
-                const size_t cb_ = (size_t) (1 + c0 + k) * totp + base;
-                const double4 w = rec[cb_ + j], wp = rec[cb_ + j - 1];
-                const cplx Dl = mk(w.z, w.w);
-                const cplx zetal = mk(w.x, w.y), zetal_p = mk(wp.x, wp.y);
-                const double psil = w.x, psil_p = wp.x;
-                const double tl = tx * B.xl[(size_t) (c0 + k) * R + r];
-                const cplx ml = B.m_l[C.ml_off + B.idx1[c0 + k]];
-                const cplx c6 = Dl * minv - Dm2 * ml + tl;
-                al[k] = (c6 * psi + ca * psil - psil_p) * ida -
-                        na * ((c6 * zeta + ca * zetal - zetal_p) * (ida * ida));
-                const cplx c4 = ml * D + m * Dl + tl;
-                bl[k] = (c4 * psi + cb * psil - psil_p) * idb -
-                        nb * ((c4 * zeta + cb * zetal - zetal_p) * (idb * idb));
-            }
-        }
-    } else {
-#pragma unroll
-        for (int k = 0; k < NC; ++k) al[k] = bl[k] = mk(0., 0.);
-    }
-    sab[0][t] = a;
-    sab[1][t] = b;
+    // ---- ascending pass ----
+    double sinx, cosx;
+    sincos(x, &sinx, &cosx);
+    double psi_p = sinx, chi_p = cosx, chi_c = xinv * cosx + sinx;     // psi_0, chi_0, chi_1
+    double psil_p[NC > 0 ? NC : 1], chil_p[NC > 0 ? NC : 1], chil_c[NC > 0 ? NC : 1];
 #pragma unroll
     for (int k = 0; k < NC; ++k) {
-        sab[2 + 2 * k][t] = al[k];
-        sab[3 + 2 * k][t] = bl[k];
+        psil_p[k] = xl[k] * cosx;
+        chil_p[k] = xl[k] * -sinx;
+        chil_c[k] = (-xinv * xinv) * xl[k] * cosx + xinv * chil_p[k] + xl[k] * cosx;
     }
-    __syncthreads();
-
     double acc[5 * CC];
 #pragma unroll
     for (int q = 0; q < 5 * CC; ++q) acc[q] = 0.;
-    if (owned) {
-        const double f1 = fv1[j], f4 = fv4[j];
-        const double sgn = (j & 1) ? -1. : 1.;
-        acc[0] = f1 * (a.re + b.re);
-        acc[1] = f1 * (norm2(a) + norm2(b));
-        acc[2] = f1 * sgn * (a.re - b.re);
-        acc[3] = f1 * sgn * (a.im - b.im);
-        const bool gterm = j < n1;
-        cplx an = mk(0., 0.), bn = mk(0., 0.);
-        if (gterm) {
-            an = sab[0][t + 1];
-            bn = sab[1][t + 1];
-            acc[4] = fv3[j] * (re_mulc(a, an) + re_mulc(b, bn)) + fv4[j] * re_mulc(a, b);
-        }
-        double2 *cf = (double2 *) coef;
-        const int tpos = bop ? B.tc_pos[r] : 0;
-        const long long troff = bop ? B.tc_roff[r] : 0;
-        if (write_value) {
-            const cplx cs = (a + b) * f4, cd = (a - b) * f4;
-            if (bop) {
-                tc_put_b(bop, troff, tpos, 1 + B.nd1, 0, j, cs.re, cs.im, cd.re, cd.im);
-            } else {
-                const size_t o = ((size_t) B.off[r] + j - 1) * 2;
-                cf[o] = make_double2(cs.re, cs.im);
-                cf[o + 1] = make_double2(cd.re, cd.im);
-            }
-        }
+    cplx ap = mk(0., 0.), bp = mk(0., 0.), alp[NC > 0 ? NC : 1], blp[NC > 0 ? NC : 1];
 #pragma unroll
-        for (int k = 0; k < NC; ++k) {
-            double *q = acc + 5 * (1 + k);
-            q[0] = f1 * (al[k].re + bl[k].re);
-            q[1] = f1 * 2. * (re_mulc(a, al[k]) + re_mulc(b, bl[k]));
-            q[2] = f1 * sgn * (al[k].re - bl[k].re);
-            q[3] = f1 * sgn * (al[k].im - bl[k].im);
-            if (gterm) {
-                const cplx aln = sab[2 + 2 * k][t + 1], bln = sab[3 + 2 * k][t + 1];
-                q[4] = fv3[j] * (re_mulc(al[k], an) + re_mulc(a, aln) + re_mulc(bl[k], bn) + re_mulc(b, bln)) +
-                       fv4[j] * (re_mulc(al[k], b) + re_mulc(a, bl[k]));
+    for (int k = 0; k < NC; ++k) alp[k] = blp[k] = mk(0., 0.);
+    const cplx Dm2f = minv * minv;
+    const size_t tot = (size_t) B.tot, off = (size_t) B.off[r];
+    const int tpos = bop ? B.tc_pos[r] : 0;
+    const long long troff = bop ? B.tc_roff[r] : 0;
+    double4 *cf = (double4 *) coef;
+
+    cplx Dloc[K1_B], Dlloc[NC > 0 ? NC : 1][K1_B];
+    double rloc[K1_B], rlloc[NC > 0 ? NC : 1][K1_B];
+    for (int c = 0; c < nb; ++c) {
+        const int lo = c * K1_B + 1, hi = min(c * K1_B + K1_B, n1);
+        const double *q = ckr + (size_t) c * CW;
+        // replay D, D_l from the block's top (t <= n2) down to lo
+        {
+            const int t = min(c * K1_B + K1_B, n2);
+            cplx D = mk(q[0], q[1]), Dl[NC > 0 ? NC : 1];
+#pragma unroll
+            for (int k = 0; k < NC; ++k) Dl[k] = mk(q[2 + 2 * k], q[3 + 2 * k]);
+            if (t <= hi) {
+                Dloc[t - lo] = D;
+#pragma unroll
+                for (int k = 0; k < NC; ++k) Dlloc[k][t - lo] = Dl[k];
             }
-            const cplx cs = (al[k] + bl[k]) * f4, cd = (al[k] - bl[k]) * f4;
-            if (bop) {
-                tc_put_b(bop, troff, tpos, 1 + B.nd1, 1 + c0 + k, j, cs.re, cs.im, cd.re, cd.im);
-            } else {
-                const size_t o = (((size_t) (1 + c0 + k)) * tot + (size_t) B.off[r] + j - 1) * 2;
-                cf[o] = make_double2(cs.re, cs.im);
-                cf[o + 1] = make_double2(cd.re, cd.im);
+            for (int j = t - 1; j >= lo; --j) {
+                const cplx c1 = (j + 1.) * zinv;
+                const cplx ic2 = cinv(D + c1);
+                D = c1 - ic2;
+                if (NC > 0) {
+                    const cplx c3 = -c1 * zinv;
+                    const cplx ic4 = ic2 * ic2;
+#pragma unroll
+                    for (int k = 0; k < NC; ++k) {
+                        const cplx c5 = c3 * zl[k];
+                        Dl[k] = c5 + (Dl[k] + c5) * ic4;
+                    }
+                }
+                if (j <= hi) {
+                    Dloc[j - lo] = D;
+#pragma unroll
+                    for (int k = 0; k < NC; ++k) Dlloc[k][j - lo] = Dl[k];
+                }
             }
+        }
+        // replay the psi ratio and its tangents from the block's top (t = hi) down to lo
+        {
+            const double *qr = q + 2 + 2 * NC;
+            double rn = qr[0], rl[NC > 0 ? NC : 1];
+#pragma unroll
+            for (int k = 0; k < NC; ++k) rl[k] = qr[1 + k];
+            rloc[hi - lo] = rn;
+#pragma unroll
+            for (int k = 0; k < NC; ++k) rlloc[k][hi - lo] = rl[k];
+            for (int j = hi - 1; j >= lo; --j) {
+                const double a1 = (2. * j + 1.) * xinv;
+                const double rnew = 1. / (a1 - rn);
+                if (NC > 0) {
+                    const double a2 = -a1 * xinv, a3 = rnew * rnew;
+#pragma unroll
+                    for (int k = 0; k < NC; ++k) rl[k] = -(a2 * xl[k] - rl[k]) * a3;
+                }
+                rn = rnew;
+                rloc[j - lo] = rn;
+#pragma unroll
+                for (int k = 0; k < NC; ++k) rlloc[k][j - lo] = rl[k];
+            }
+        }
+        for (int j = lo; j <= hi; ++j) {
+            const double rj = rloc[j - lo];
+            const double psi = rj * psi_p;
+            double psil[NC > 0 ? NC : 1];
+#pragma unroll
+            for (int k = 0; k < NC; ++k) psil[k] = rlloc[k][j - lo] * psi_p + rj * psil_p[k];
+            const cplx D = Dloc[j - lo];
+            const cplx zeta = mk(psi, chi_c), zeta_p = mk(psi_p, chi_p);
+            const double tt = j * xinv;
+            const cplx ca = D * minv + tt;
+            const cplx na = ca * psi - psi_p;
+            const cplx ida = cinv(ca * zeta - zeta_p);
+            const cplx a = na * ida;
+            const cplx cb = m * D + tt;
+            const cplx nbq = cb * psi - psi_p;
+            const cplx idb = cinv(cb * zeta - zeta_p);
+            const cplx b = nbq * idb;
+            cplx al[NC > 0 ? NC : 1], bl[NC > 0 ? NC : 1];
+            if (NC > 0) {
+                const cplx Dm2 = D * Dm2f;
+                const double tx = -tt * xinv;
+#pragma unroll
+                for (int k = 0; k < NC; ++k) {
+                    const cplx Dl = Dlloc[k][j - lo];
+                    const cplx zetal = mk(psil[k], chil_c[k]), zetal_p = mk(psil_p[k], chil_p[k]);
+                    const double tl = tx * xl[k];
+                    const cplx c6 = Dl * minv - Dm2 * ml[k] + tl;
+                    al[k] = (c6 * psi + ca * psil[k] - psil_p[k]) * ida -
+                            na * ((c6 * zeta + ca * zetal - zetal_p) * (ida * ida));
+                    const cplx c4 = ml[k] * D + m * Dl + tl;
+                    bl[k] = (c4 * psi + cb * psil[k] - psil_p[k]) * idb -
+                            nbq * ((c4 * zeta + cb * zetal - zetal_p) * (idb * idb));
+                }
+            }
+            // sums of order j, and the asymmetry term of order j - 1 (it needs a_j, b_j)
+            const double f1 = fv1[j], f4 = fv4[j];
+            const double sgn = (j & 1) ? -1. : 1.;
+            acc[0] += f1 * (a.re + b.re);
+            acc[1] += f1 * (norm2(a) + norm2(b));
+            acc[2] += f1 * sgn * (a.re - b.re);
+            acc[3] += f1 * sgn * (a.im - b.im);
+            if (j >= 2) acc[4] += fv3[j - 1] * (re_mulc(ap, a) + re_mulc(bp, b)) + fv4[j - 1] * re_mulc(ap, bp);
+#pragma unroll
+            for (int k = 0; k < NC; ++k) {
+                double *qq = acc + 5 * (1 + k);
+                qq[0] += f1 * (al[k].re + bl[k].re);
+                qq[1] += f1 * 2. * (re_mulc(a, al[k]) + re_mulc(b, bl[k]));
+                qq[2] += f1 * sgn * (al[k].re - bl[k].re);
+                qq[3] += f1 * sgn * (al[k].im - bl[k].im);
+                if (j >= 2)
+                    qq[4] += fv3[j - 1] * (re_mulc(alp[k], a) + re_mulc(ap, al[k]) + re_mulc(blp[k], b) +
+                                           re_mulc(bp, bl[k])) +
+                             fv4[j - 1] * (re_mulc(alp[k], bp) + re_mulc(ap, blp[k]));
+            }
+            // expansion coefficients of order j
+            if (write_value) {
+                const cplx cs = (a + b) * f4, cd = (a - b) * f4;
+                if (bop) tc_put_b(bop, troff, tpos, 1 + B.nd1, 0, j, cs.re, cs.im, cd.re, cd.im);
+                else cf[off + j - 1] = make_double4(cs.re, cs.im, cd.re, cd.im);
+            }
+#pragma unroll
+            for (int k = 0; k < NC; ++k) {
+                const cplx cs = (al[k] + bl[k]) * f4, cd = (al[k] - bl[k]) * f4;
+                if (bop) tc_put_b(bop, troff, tpos, 1 + B.nd1, 1 + c0 + k, j, cs.re, cs.im, cd.re, cd.im);
+                else cf[(size_t) (1 + c0 + k) * tot + off + j - 1] = make_double4(cs.re, cs.im, cd.re, cd.im);
+            }
+            // upward: chi_{j+1} and its tangents; shift the previous order
+            const double a1 = (2. * j + 1.) * xinv;
+            const double chi_n = a1 * chi_c - chi_p;
+#pragma unroll
+            for (int k = 0; k < NC; ++k) {
+                const double a2l = -a1 * xl[k] * xinv;
+                const double chil_n = a2l * chi_c + a1 * chil_c[k] - chil_p[k];
+                chil_p[k] = chil_c[k];
+                chil_c[k] = chil_n;
+                psil_p[k] = psil[k];
+                alp[k] = al[k];
+                blp[k] = bl[k];
+            }
+            chi_p = chi_c;
+            chi_c = chi_n;
+            psi_p = psi;
+            ap = a;
+            bp = b;
         }
     }
-    // block reduction of the 5*CC tile sums (fixed order)
 #pragma unroll
     for (int q = 0; q < 5 * CC; ++q) {
-        double v = acc[q];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if ((t & 31) == 0) red[q][t >> 5] = v;
+        const int cc = q / 5, qq = q % 5;
+        if (cc == 0 && !write_value) continue;
+        const size_t col = cc == 0 ? 0 : (size_t) (1 + c0 + cc - 1);
+        rs[(col * 5 + qq) * R + r] = acc[q];
     }
-    __syncthreads();
-    const int ntiles = B.ntiles;
-    for (int q = t; q < 5 * CC; q += ABT) {
-        double v = 0.;
-#pragma unroll
-        for (int w = 0; w < ABT / 32; ++w) v += red[q][w];
-        const int c = q / 5, qq = q % 5;
-        if (c == 0 && !write_value) continue;
-        const size_t col = c == 0 ? 0 : (size_t) (1 + c0 + c - 1);
-        rsp[(col * 5 + qq) * ntiles + blockIdx.x] = v;
-    }
-}
-
-// Sum the tile partials of every radius in tile order: rs[(col*5+q)*R + r].
-__global__ void k_tile_reduce(int R, int ncol, int ntiles, const int *__restrict__ tstart,
-                              const double *__restrict__ rsp, double *__restrict__ rs) {
-    const size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (size_t) ncol * 5 * R) return;
-    const int r = (int) (i % R);
-    const size_t cq = i / R;
-    double v = 0.;
-    for (int tt = tstart[r]; tt < tstart[r + 1]; ++tt) v += rsp[cq * ntiles + tt];
-    rs[cq * R + r] = v;
 }
 
 // ---------------------------------------------------------------------------
@@ -1140,15 +1100,13 @@ int launch_gauss(cudaStream_t s, int npairs, const int *pt, const int *pi, const
     return 0;
 }
 
-int launch_coef(cudaStream_t s, const DevBatch &B, int nc, int c0, int write_value, const int2 *tiles,
-                double4 *rec, double *coef, float *bop, double *rsp) {
+int launch_coef(cudaStream_t s, const DevBatch &B, int nc, int c0, int write_value, double *ck, double *coef,
+                float *bop, double *rs) {
     const unsigned rb = ceil_div(B.R, 64);
-    const unsigned tb = (unsigned) B.ntiles;
     switch (nc) {
 #define LMIEB_K1(NC_)                                                                                    \
     case NC_:                                                                                            \
-        k_recur<NC_><<<rb, 64, 0, s>>>(B, c0, write_value, rec);                                         \
-        k_abcoef<NC_><<<tb, ABT, 0, s>>>(B, c0, write_value, tiles, rec, coef, bop, rsp);               \
+        k_mie<NC_><<<rb, 64, 0, s>>>(B, c0, write_value, ck, coef, bop, rs);                             \
         break;
     LMIEB_K1(0)
     LMIEB_K1(1)
@@ -1160,13 +1118,6 @@ int launch_coef(cudaStream_t s, const DevBatch &B, int nc, int c0, int write_val
         fprintf(stderr, "ERROR: launch_coef: bad chunk width %d\n", nc);
         return -1;
     }
-    LMIEB_CUDA_TRY(cudaGetLastError());
-    return 0;
-}
-
-int launch_tile_reduce(cudaStream_t s, const DevBatch &B, const int *tstart, const double *rsp, double *rs) {
-    const size_t nt = (size_t) (1 + B.nd1) * 5 * B.R;
-    k_tile_reduce<<<ceil_div(nt, 256), 256, 0, s>>>(B.R, 1 + B.nd1, B.ntiles, tstart, rsp, rs);
     LMIEB_CUDA_TRY(cudaGetLastError());
     return 0;
 }

@@ -10,7 +10,7 @@
 //     (pi_{k+1} = (2k+1)/k mu pi_k - (k+1)/k pi_{k-1}, one dependent FMA per
 //     order) and write rows 2h = (pi + tau)(mu_h) and 2h+1 = s_k (pi - tau)(mu_h)
 //     of A+, split into TF32 hi/lo, in the K-major core-matrix layout;
-//   - lane 0 of warp 2 brings the group's B chunks (written by K1b) with bulk
+//   - lane 0 of warp 2 brings the group's B chunks (written by K1) with bulk
 //     copies running ahead of the products, and issues tcgen05.mma kind::tf32
 //     (M 128, N 128, K 8): lo*hi + hi*lo + hi*hi into an FP32 accumulator in
 //     tensor memory;

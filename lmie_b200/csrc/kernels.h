@@ -9,6 +9,11 @@
 
 #include "dev_common.cuh"
 
+// K1 keeps its downward recurrences at the top of every block of K1_B orders.
+constexpr int K1_B = 16;
+// doubles per checkpoint block of a chunk of nc tangent-linear columns
+__host__ __device__ constexpr int k1_ck_width(int nc) { return 3 + 3 * nc; }
+
 // One case of a batch (device copy).  Offsets index the batch-wide arrays.
 struct DevCase {
     double lambda;
@@ -44,9 +49,8 @@ struct DevBatch {
     const double *w;            // [(1 + nd)][R] row 0: f = nr qw; row 1+kk: f_l (index1) or f_l2 (index2)
     const int *n1r, *n2r;       // [R]
     const long long *off;       // [R+1] prefix sums of n1r (coefficient storage)
-    const long long *offp;      // [R+1] prefix sums of n1r + 1 (recurrence storage)
-    long long tot, totp;
-    int ntiles;                 // K1b tiles over all radii
+    const long long *ckoff;     // [R+1] prefix sums of ceil(n1r / K1_B) (K1 checkpoint blocks)
+    long long tot, ckn;
     const double *fv;           // [4][n1max + 2]: fv1 | fv2 | fv3 | fv4
     const double *rc;           // [8 * ncmax] GSF/Legendre recurrence coefficients per order
     const double *mu_pool;      // Gauss pool: n nodes then n weights at DevCase.mu_off
@@ -73,9 +77,8 @@ int launch_gauss(cudaStream_t s, int npairs, const int *pt, const int *pi, const
 // K1 for one chunk of nc tangent-linear columns starting at index1 slot c0.
 // With bop set, the coefficients go to the tensor-core B operand
 // (tc_layout.cuh) instead of coef.
-int launch_coef(cudaStream_t s, const DevBatch &B, int nc, int c0, int write_value, const int2 *tiles,
-                double4 *rec, double *coef, float *bop, double *rsp);
-int launch_tile_reduce(cudaStream_t s, const DevBatch &B, const int *tstart, const double *rsp, double *rs);
+int launch_coef(cudaStream_t s, const DevBatch &B, int nc, int c0, int write_value, double *ck, double *coef,
+                float *bop, double *rs);
 
 // K2: sums[case][(1+nd)][4] (unnormalised), save1 [4][R] for save_control 1
 int launch_reduce_scalars(cudaStream_t s, const DevBatch &B, const double *rs, double *sums, double *save1);

@@ -1,5 +1,5 @@
 // tc_layout.cuh -- operand layout of the split-precision (3xTF32) angular
-// contraction on the tensor cores, shared by its producer (K1b, k_fp64.cu)
+// contraction on the tensor cores, shared by its producer (K1, k_fp64.cu)
 // and its consumer (k_tc.cu).
 //
 // Per case the S1/S2 sums are dense products over the orders k:
@@ -64,7 +64,7 @@ __device__ __forceinline__ void tc_split(double v, float &hi, float &lo) {
     lo = tc_tf32(f - h);
 }
 
-// K1b writer: S = cs and D = cd of order j (1-based) of the radius at
+// K1 writer: S = cs and D = cd of order j (1-based) of the radius at
 // position pos of its group, column col, into the group block at goff.
 __device__ __forceinline__ void tc_put_b(float *__restrict__ bop, long long goff, int pos, int c1, int col, int j,
                                          double sre, double sim, double dre, double dim) {
