@@ -54,6 +54,14 @@ int lmieb_set_pipeline(int chunks);
 int lmieb_set_work_granularity(int precision, double items_per_sm);
 double lmieb_get_work_granularity(int precision);
 
+/* Segment length of the tensor-core angular stage, in chunks of 16 orders:
+ * its hi*hi products accumulate in FP32 (which the tensor cores truncate)
+ * over one segment, then go into a running sum; shorter segments are more
+ * accurate and cost more sum traffic.  Default 2.  Returns 0, or -1 outside
+ * 1..64. */
+int lmieb_set_split_segment(int chunks);
+int lmieb_get_split_segment(void);
+
 /* Autotuner: solves the batch in[0..n_cases) (outputs in out, allocated by
  * the caller or a previous call) under each candidate pipeline depth
  * (1, 2, 4, 6 parts) and angular work granularity (2, 4, 8 items per SM for

@@ -41,6 +41,8 @@ def library() -> C.CDLL:
         lib.lmieb_set_work_granularity.argtypes = [C.c_int, C.c_double]
         lib.lmieb_get_work_granularity.argtypes = [C.c_int]
         lib.lmieb_get_work_granularity.restype = C.c_double
+        lib.lmieb_set_split_segment.argtypes = [C.c_int]
+        lib.lmieb_get_split_segment.argtypes = []
         _lib = lib
     return _lib
 

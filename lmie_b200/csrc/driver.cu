@@ -97,6 +97,10 @@ Ctx g_ctx;
 // per-item overhead; set by lmieb_set_work_granularity (the autotuner).
 double g_items_per_sm[2] = {4., 2.};
 
+// Orders (in chunks of TC_KC) per FP32 segment of the tensor-core stage's
+// hi*hi products; set by lmieb_set_split_segment.
+int g_tc_seg = 2;
+
 // fn(i) for every i in [0, n) on the host's cores (dynamic chunks of `grain`)
 template <class F>
 void parallel_for(int n, int grain, F &&fn) {
@@ -157,9 +161,12 @@ struct Plan {
     int want_gc = 0, want_lc = 0, pf_from = 0, save_control = 0, n_qang0 = 0;
     double *ck = nullptr, *coef = nullptr, *rs = nullptr, *sums = nullptr, *part = nullptr;
     double *pfacc = nullptr, *pfn = nullptr, *ckpt = nullptr, *exq = nullptr;
-    AngItem *ang = nullptr;
+    AngItem *ang = nullptr;     // K3 items (tensor-core items when tc)
     int n_ang = 0;
+    AngItem *ang64 = nullptr;   // with tc: FP64 K3 items of the cases kept off the tensor cores
+    int n_ang64 = 0;
     int tc = 0;                 // K3 in split precision on the tensor cores
+    int tc_seg = 2;             // its segment length (chunks)
     float *bop = nullptr;       // its B operand (tc_layout.cuh)
     size_t bop_bytes = 0;
     ExpItem *ex = nullptr;
@@ -279,20 +286,22 @@ int run_kernels(Plan &L) {
         stage(2);
         if (launch_reduce_scalars(s, B, L.rs, L.sums, L.save_control == 1 ? L.o_save1 : nullptr)) return -1;
         stage(3);
-        if (L.n_ang > 0 && L.tc) {
-            if (launch_angular_tc(s, B, L.n_ang, L.ang, L.bop, L.part, L.o_trunc + 2 * L.ncase)) return -1;
-            if (launch_reduce_pf(s, B, L.pf_total, L.pf_start, L.part, L.pfacc)) return -1;
-        } else if (L.n_ang > 0) {
+        const int n64 = L.tc ? L.n_ang64 : L.n_ang;
+        const AngItem *a64 = L.tc ? L.ang64 : L.ang;
+        if (L.tc && L.n_ang > 0 &&
+            launch_angular_tc(s, B, L.n_ang, L.ang, L.bop, L.part, L.tc_seg, L.o_trunc + 2 * L.ncase))
+            return -1;
+        if (n64 > 0) {
             for (int t = 0; t < L.n_ang_launch; ++t) {
                 const int c1 = t * 4, c2 = t * 4;
                 const int nc1 = std::max(0, std::min(4, B.nd1 - c1));
                 const int nc2 = std::max(0, std::min(4, B.nd2 - c2));
-                if (launch_angular(s, B, nc1, c1, nc2, c2, t == 0, L.n_ang, L.ang, L.coef, L.part,
+                if (launch_angular(s, B, nc1, c1, nc2, c2, t == 0, n64, a64, L.coef, L.part,
                                    L.save_control == 1 ? L.o_save2 : nullptr))
                     return -1;
             }
-            if (launch_reduce_pf(s, B, L.pf_total, L.pf_start, L.part, L.pfacc)) return -1;
         }
+        if ((L.n_ang > 0 || n64 > 0) && launch_reduce_pf(s, B, L.pf_total, L.pf_start, L.part, L.pfacc)) return -1;
     } else {
         stage(2);
         if (launch_save_reweight(s, B, L.n_qang0, L.save1_in, L.save2_in, L.w2, L.sums, L.pfacc)) return -1;
@@ -506,16 +515,37 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     for (int k = 0; k < ncase; ++k) any_ang |= cs[k].n_qang > 0;
     L.tc = p0.precision == LMIEB_PRECISION_TF32X3 && L.save_control == 0 && any_ang && nd1 <= TC_MAX_NC1 &&
            nd2 <= TC_MAX_ND2;
-    std::vector<AngItem> ang;
+    L.tc_seg = g_tc_seg;
+    // with split precision, cases below TC_MIN_N1 orders keep the FP64 K3: their
+    // linearised phase matrices cancel strongly on normalisation, and they cost little
+    std::vector<char> case_tc(ncase, 0);
+    for (int k = 0; k < ncase; ++k) case_tc[k] = L.tc && cs[k].n_qang > 0 && cs[k].n1 >= TC_MIN_N1;
+    std::vector<AngItem> ang, ang64;
     std::vector<long long> pf_start(ncase + 1, 0);
+    for (int k = 0; k < ncase; ++k) {
+        pf_start[k + 1] = pf_start[k] + (long long) Q * cs[k].n_qang;
+        cs[k].pf_off = pf_start[k];
+        cs[k].G = 0;
+    }
+    L.pf_total = pf_start[ncase];
     long long part_total = 0;
+    auto by_cost = [](const std::pair<double, AngItem> &a, const std::pair<double, AngItem> &b) {
+        return a.first > b.first;
+    };
+    // coefficient offsets of the radii whose coefficients K1 writes in FP64
+    // (all radii, or with split precision those of the FP64 cases)
+    std::vector<long long> coff(R + 1, 0);
+    for (int k = 0; k < ncase; ++k) {
+        const DevCase &C = cs[k];
+        for (int r = C.r0; r < C.r0 + C.nr; ++r) coff[r + 1] = coff[r] + (case_tc[k] ? 0 : n1r[r]);
+    }
     // split precision: radius groups of tc_rg(nd1) radii, each with its B operand block
     std::vector<int> tc_pos, tg_r0, tg_n, tg_nk;
     std::vector<long long> tc_roff, tg_off;
     long long bop_floats = 0;
     if (L.tc) {
         const int RG = tc_rg(nd1);
-        tc_pos.assign(R, 0);
+        tc_pos.assign(R, -1);
         tc_roff.assign(R, 0);
         std::vector<int> cg0(ncase + 1, 0);
         std::vector<double> wc(ncase, 0.);
@@ -523,6 +553,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         for (int k = 0; k < ncase; ++k) {
             const DevCase &C = cs[k];
             cg0[k] = (int) tg_r0.size();
+            if (!case_tc[k]) continue;
             for (int r = C.r0; r < C.r0 + C.nr; r += RG) {
                 const int n = std::min(RG, C.r0 + C.nr - r);
                 int mx = 1;
@@ -539,16 +570,14 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
                 bop_floats += (long long) nk * (TC_BSTAGE / 4);
                 wc[k] += nk + 1;                       // chunks, plus one for the group's epilogue
             }
-            if (C.n_qang > 0) W += wc[k] * ((C.nh + TC_HALF - 1) / TC_HALF);
+            W += wc[k] * ((C.nh + TC_HALF - 1) / TC_HALF);
         }
         cg0[ncase] = (int) tg_r0.size();
         const double wt = std::max(W / (g_items_per_sm[1] * c.sms), 8.);    // chunks per item
         std::vector<std::pair<double, AngItem>> tmp;
         for (int k = 0; k < ncase; ++k) {
             DevCase &C = cs[k];
-            pf_start[k + 1] = pf_start[k] + (long long) Q * C.n_qang;
-            C.pf_off = pf_start[k];
-            if (C.n_qang <= 0) { C.G = 0; continue; }
+            if (!case_tc[k]) continue;
             const int ng = cg0[k + 1] - cg0[k];
             const int xt = (C.nh + TC_HALF - 1) / TC_HALF;
             int G = (int) std::lround(wc[k] / wt);
@@ -573,17 +602,16 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
                 for (int t = 0; t < xt; ++t) tmp.push_back({cost, AngItem{k, t, g, gs[g], gs[g + 1]}});
             }
         }
-        std::stable_sort(tmp.begin(), tmp.end(), [](const std::pair<double, AngItem> &a,
-                                                    const std::pair<double, AngItem> &b) { return a.first > b.first; });
+        std::stable_sort(tmp.begin(), tmp.end(), by_cost);
         for (auto &e : tmp) ang.push_back(e.second);
-        L.pf_total = pf_start[ncase];
-        L.n_ang = (int) ang.size();
-    } else {
+    }
+    {
+        // FP64 K3 over the remaining cases: radius ranges of roughly equal sum of n1
         const int per = angular_angles_per_block(std::min(nd1, 4));
         double W = 0.;
         std::vector<double> wc(ncase, 0.);
         for (int k = 0; k < ncase; ++k) {
-            if (cs[k].n_qang <= 0) continue;
+            if (cs[k].n_qang <= 0 || case_tc[k]) continue;
             wc[k] = (double) (cs1[k + 1] - cs1[k]) * cs[k].nh;
             W += wc[k];
         }
@@ -591,13 +619,10 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         std::vector<std::pair<double, AngItem>> tmp;
         for (int k = 0; k < ncase; ++k) {
             DevCase &C = cs[k];
-            pf_start[k + 1] = pf_start[k] + (long long) Q * C.n_qang;
-            C.pf_off = pf_start[k];
-            if (C.n_qang <= 0) { C.G = 0; continue; }
+            if (C.n_qang <= 0 || case_tc[k]) continue;
             const int xt = (C.nh + per - 1) / per;
             int G = (int) std::lround(wc[k] / (xt * wt));
             G = std::max(1, std::min(G, C.nr));
-            // groups of roughly equal sum of n1 over the case's radii
             std::vector<int> gs(G + 1, C.r0 + C.nr);
             gs[0] = C.r0;
             const long long o0 = off[C.r0], ot = off[C.r0 + C.nr] - o0;
@@ -615,12 +640,12 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
                     tmp.push_back({cost, it});
                 }
         }
-        std::stable_sort(tmp.begin(), tmp.end(), [](const std::pair<double, AngItem> &a,
-                                                    const std::pair<double, AngItem> &b) { return a.first > b.first; });
-        for (auto &e : tmp) ang.push_back(e.second);
-        L.pf_total = pf_start[ncase];
-        L.n_ang = (int) ang.size();
+        std::stable_sort(tmp.begin(), tmp.end(), by_cost);
+        for (auto &e : tmp) (L.tc ? ang64 : ang).push_back(e.second);
     }
+    L.n_ang = (int) ang.size();
+    L.n_ang64 = (int) ang64.size();
+    const long long ctot = coff[R];
 
     // ---- expansion work items and offsets ----
     std::vector<ExpItem> ex;
@@ -671,7 +696,9 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         long long nl = 0;
         if (L.save_control != 2) {
             nl += (long long) std::max(L.nd1c, 1) + 1;                          // K1 per chunk, K2
-            if (L.n_ang > 0) nl += L.n_ang_launch + 1;                          // K3 + group reduction
+            if (L.tc) nl += (L.n_ang > 0) + (L.n_ang64 > 0 ? L.n_ang_launch : 0);   // K3
+            else nl += L.n_ang > 0 ? L.n_ang_launch : 0;
+            if (L.n_ang > 0 || L.n_ang64 > 0) nl += 1;                          // group reduction
         } else {
             nl += 1 + (L.n_qang0 > 0);
         }
@@ -707,7 +734,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         add((size_t) (R + 1) * 8); add((size_t) (R + 1) * 8);
         add(fv.size() * 8); add(rc.size() * 8); add(ml.size() * 16); add(laml.size() * 8);
         add((size_t) nd1 * 4); add((size_t) nd2 * 4); add(mu_user.size() * 8);
-        add(ang.size() * sizeof(AngItem)); add(ex.size() * sizeof(ExpItem));
+        add(ang.size() * sizeof(AngItem)); add(ang64.size() * sizeof(AngItem)); add(ex.size() * sizeof(ExpItem));
         add(tc_pos.size() * 4); add(tc_roff.size() * 8); add(tg_r0.size() * 4); add(tg_n.size() * 4);
         add(tg_nk.size() * 4); add(tg_off.size() * 8);
         for (int q = 0; q < 5; ++q) add((size_t) (ncase + 1) * 8);
@@ -731,7 +758,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     int *h_n1r = put(hp, ho, n1r.data(), (size_t) R);
     int *h_n2r = put(hp, ho, n2r.data(), (size_t) R);
     int *h_rcase = put(hp, ho, rcase.data(), (size_t) R);
-    long long *h_off = put(hp, ho, off.data(), (size_t) R + 1);
+    long long *h_off = put(hp, ho, coff.data(), (size_t) R + 1);
     long long *h_ckoff = put(hp, ho, ckoff.data(), (size_t) R + 1);
     double *h_fv = put(hp, ho, fv.data(), fv.size());
     double *h_rc = put(hp, ho, rc.data(), rc.size());
@@ -741,6 +768,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     int *h_i2 = put(hp, ho, p0.idx2, (size_t) nd2);
     double *h_mu = put(hp, ho, mu_user.data(), mu_user.size());
     AngItem *h_ang = put(hp, ho, ang.data(), ang.size());
+    AngItem *h_ang64 = put(hp, ho, ang64.data(), ang64.size());
     ExpItem *h_ex = put(hp, ho, ex.data(), ex.size());
     int *h_tcpos = put(hp, ho, tc_pos.data(), tc_pos.size());
     long long *h_tcroff = put(hp, ho, tc_roff.data(), tc_roff.size());
@@ -780,7 +808,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         if (L.save_control != 2) {
             add((size_t) ckn * 8 * k1_ck_width(std::min(nd1, 4)));
             if (L.tc) add((size_t) bop_floats * 4);
-            else add((size_t) (1 + nd1) * (size_t) tot * 32);
+            add((size_t) (1 + nd1) * (size_t) ctot * 32);
             add((size_t) (1 + nd1) * 5 * (size_t) R * 8);
             add((size_t) part_total * 8);
         }
@@ -819,7 +847,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     B.n2r = (const int *) dptr(h_n2r);
     B.off = (const long long *) dptr(h_off);
     B.ckoff = (const long long *) dptr(h_ckoff);
-    B.tot = tot;
+    B.tot = ctot;
     B.ckn = ckn;
     B.fv = (const double *) dptr(h_fv);
     B.rc = (const double *) dptr(h_rc);
@@ -834,6 +862,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         B.tg_off = (const long long *) dptr(h_tgoff);
     }
     L.ang = (AngItem *) dptr(h_ang);
+    L.ang64 = (AngItem *) dptr(h_ang64);
     L.ex = (ExpItem *) dptr(h_ex);
     L.pf_start = (long long *) dptr(h_pfs);
     L.ck_gc = (long long *) dptr(h_ckg);
@@ -850,9 +879,8 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         if (L.tc) {
             L.bop_bytes = (size_t) bop_floats * 4;
             L.bop = A.take<float>((size_t) bop_floats);
-        } else {
-            L.coef = A.take<double>((size_t) (1 + nd1) * (size_t) tot * 4);
         }
+        L.coef = A.take<double>((size_t) (1 + nd1) * (size_t) ctot * 4);
         L.rs = A.take<double>((size_t) (1 + nd1) * 5 * (size_t) R);
         L.part = A.take<double>((size_t) part_total);
     }
@@ -1294,6 +1322,21 @@ extern "C" int lmieb_set_work_granularity(int precision, double items_per_sm) {
     }
     g_items_per_sm[precision == LMIEB_PRECISION_TF32X3 ? 1 : 0] = items_per_sm;
     return 0;
+}
+
+extern "C" int lmieb_set_split_segment(int chunks) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    if (chunks < 1 || chunks > 64) {
+        fprintf(stderr, "ERROR: lmieb_set_split_segment: %d chunks (1..64)\n", chunks);
+        return -1;
+    }
+    g_tc_seg = chunks;
+    return 0;
+}
+
+extern "C" int lmieb_get_split_segment(void) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    return g_tc_seg;
 }
 
 extern "C" double lmieb_get_work_granularity(int precision) {

@@ -211,8 +211,10 @@ __global__ void __launch_bounds__(64) k_mie(DevBatch B, int c0, int write_value,
     for (int k = 0; k < NC; ++k) alp[k] = blp[k] = mk(0., 0.);
     const cplx Dm2f = minv * minv;
     const size_t tot = (size_t) B.tot, off = (size_t) B.off[r];
-    const int tpos = bop ? B.tc_pos[r] : 0;
-    const long long troff = bop ? B.tc_roff[r] : 0;
+    // split precision: the radii of tensor-core cases write the B operand
+    const int tpos = bop ? B.tc_pos[r] : -1;
+    const bool to_tc = tpos >= 0;
+    const long long troff = to_tc ? B.tc_roff[r] : 0;
     double4 *cf = (double4 *) coef;
 
     cplx Dloc[K1_B], Dlloc[NC > 0 ? NC : 1][K1_B];
@@ -331,13 +333,13 @@ __global__ void __launch_bounds__(64) k_mie(DevBatch B, int c0, int write_value,
             // expansion coefficients of order j
             if (write_value) {
                 const cplx cs = (a + b) * f4, cd = (a - b) * f4;
-                if (bop) tc_put_b(bop, troff, tpos, 1 + B.nd1, 0, j, cs.re, cs.im, cd.re, cd.im);
+                if (to_tc) tc_put_b(bop, troff, tpos, 1 + B.nd1, 0, j, cs.re, cs.im, cd.re, cd.im);
                 else cf[off + j - 1] = make_double4(cs.re, cs.im, cd.re, cd.im);
             }
 #pragma unroll
             for (int k = 0; k < NC; ++k) {
                 const cplx cs = (al[k] + bl[k]) * f4, cd = (al[k] - bl[k]) * f4;
-                if (bop) tc_put_b(bop, troff, tpos, 1 + B.nd1, 1 + c0 + k, j, cs.re, cs.im, cd.re, cd.im);
+                if (to_tc) tc_put_b(bop, troff, tpos, 1 + B.nd1, 1 + c0 + k, j, cs.re, cs.im, cd.re, cd.im);
                 else cf[(size_t) (1 + c0 + k) * tot + off + j - 1] = make_double4(cs.re, cs.im, cd.re, cd.im);
             }
             // upward: chi_{j+1} and its tangents; shift the previous order

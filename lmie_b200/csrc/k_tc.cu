@@ -6,28 +6,32 @@
 // of a radius group, over the orders.  A block owns one angle tile of one
 // case and a range of radius groups; per group, chunks of TC_KC orders flow
 // through shared memory:
-//   - warps 0-1 (one thread per half-angle) run the pi/tau recurrence in FP64
-//     (pi_{k+1} = (2k+1)/k mu pi_k - (k+1)/k pi_{k-1}, one dependent FMA per
-//     order) and write rows 2h = (pi + tau)(mu_h) and 2h+1 = s_k (pi - tau)(mu_h)
-//     of A+, split into TF32 hi/lo, in the K-major core-matrix layout;
-//   - lane 0 of warp 2 brings the group's B chunks (written by K1) with bulk
+//   - warps 0-3 (one thread per row; the two threads of a half-angle both run
+//     its recurrence) run the pi/tau recurrence in FP64 (pi_{k+1} =
+//     (2k+1)/k mu pi_k - (k+1)/k pi_{k-1}, one dependent FMA per order) and
+//     write row 2h = (pi + tau)(mu_h) or 2h+1 = s_k (pi - tau)(mu_h) of A+,
+//     split into TF32 hi/lo, in the K-major core-matrix layout;
+//   - lane 0 of warp 8 brings the group's B chunks (written by K1) with bulk
 //     copies running ahead of the products, and issues tcgen05.mma kind::tf32
-//     (M 128, N 128, K 8): lo*hi + hi*lo + hi*hi into an FP32 accumulator in
-//     tensor memory;
+//     (M 128, N 128, K 8): hi*hi into a segment accumulator F, lo*hi + hi*lo
+//     into a cross-term accumulator G of the group, both FP32 in tensor
+//     memory;
 //   - the FP32 accumulation of the tensor cores truncates, so its error grows
-//     with the number of products it sums: a segment of TC_SEG chunks opens a
-//     fresh accumulator (two buffers alternate), and warps 4-7 add each
-//     finished segment into a double-float running sum (hi + lo, both FP32,
-//     error-free two-sum) kept in tensor memory while the next segment is
-//     computed.  After a group's last segment they read the sums of their row
-//     (tensor-memory lane = row; sm of a row is in its pair row's lane, one
-//     shuffle away), form the phase-matrix quadratic forms and their
-//     linearisations per radius in FP64 (reference src/lmie_core.c:723-790)
-//     and accumulate them over the block's radii in registers.
+//     with the number of products it sums: the hi*hi products (the large
+//     ones) of a segment of `seg` chunks go into a fresh F (two buffers
+//     alternate), and warps 4-7 add each finished segment into an FP32
+//     running sum H while the next segment is computed; the cross terms are
+//     2^-11 of those, so their truncation stays below the hi*hi rounding over
+//     a whole group.  After a group's last segment warps 4-7 fold G into F,
+//     release G to the next group, read the sums of their row (tensor-memory
+//     lane = row; sm of a row is in its pair row's lane, one shuffle away),
+//     form the phase-matrix quadratic forms and their linearisations per
+//     radius in FP64 (reference src/lmie_core.c:723-790) and accumulate them
+//     over the block's radii in registers.
 // Partials go to the same per-group buffer as the FP64 K3.
 //
 // Tensor memory (512 columns): F0 [0,128) and F1 [128,256) segment
-// accumulators, H [256,384) and L [384,512) running sum.
+// accumulators, H [256,384) running sum, G [384,512) cross terms.
 //
 // Every wait is bounded (about 1 s of clock, or until another block has
 // failed); a block that gives up sets the error word, waits (bounded) for
@@ -40,25 +44,29 @@
 
 namespace {
 
-constexpr int TC_T = 256;                    // warps 0-1: A operand; 2: B copies and products;
-                                             // 3: idle; 4-7: segment sums and quadratic forms
+constexpr int TC_T = 288;                    // warps 0-3: A operand; 4-7: segment sums and quadratic
+                                             // forms; 8: B copies and products
+constexpr int TC_MMA_WARP = 8;
 constexpr int TC_ASTAGES = 3;                // A operand stages
 constexpr int TC_BSLOTS = 6;                 // B operand slots (bulk copies)
 constexpr int TC_BAHEAD = TC_BSLOTS - 2;     // chunks the B copies run ahead of the products
-constexpr int TC_SEG = 4;                    // chunks per accumulator segment
+constexpr int TC_MAX_GN = TC_NHALF / 2;      // radii of a group (tc_rg(0))
+constexpr int TC_MAX_NS = 1 + TC_MAX_NC1 + TC_MAX_ND2;
 // barriers: afull[TC_ASTAGES], adone[TC_ASTAGES], bfull[TC_BSLOTS], bdone[TC_BSLOTS], segfull[2],
-// segfree[2], fin
-constexpr int TC_NBAR = 2 * TC_ASTAGES + 2 * TC_BSLOTS + 4 + 1;
+// segfree[2], gfree, fin
+constexpr int TC_NBAR = 2 * TC_ASTAGES + 2 * TC_BSLOTS + 4 + 2;
 constexpr uint32_t TC_RING = TC_ASTAGES * TC_ASTAGE + TC_BSLOTS * TC_BSTAGE;
-constexpr uint32_t TC_SMEM = TC_RING + TC_NBAR * 8 + 16;
+constexpr uint32_t TC_WBUF = TC_MAX_GN * TC_MAX_NS * 8;   // a group's radius weights
+constexpr uint32_t TC_SMEM = TC_RING + TC_WBUF + TC_NBAR * 8 + 16;
 constexpr uint32_t TC_TMEM_COLS = 512;
-constexpr uint32_t TC_HCOL = 2 * TC_NP, TC_LCOL = 3 * TC_NP;   // running sum hi, lo
+constexpr uint32_t TC_HCOL = 2 * TC_NP, TC_GCOL = 3 * TC_NP;   // running sum, cross terms
 constexpr long long TC_WAIT_CYCLES = 1LL << 31;   // about 1 s
 
 static_assert(TC_ASTAGE % 1024 == 0 && TC_BSTAGE % 1024 == 0, "stages stay 1 KB aligned");
 constexpr uint32_t TC_STAGE = TC_ASTAGE + TC_BSTAGE;   // the self-test's single stage
 static_assert(TC_NP % 16 == 0 && TC_NP <= 256, "N of an M=128 tf32 MMA");
-static_assert(4 * TC_NP <= (int) TC_TMEM_COLS, "segment buffers and running sum");
+static_assert(4 * TC_NP <= (int) TC_TMEM_COLS, "segment buffers, running sum, cross terms");
+static_assert(TC_WBUF % 16 == 0, "barriers stay 8-byte aligned");
 static_assert(TC_SMEM <= 227 * 1024, "shared memory per block");
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -205,13 +213,36 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
-// barrier 1 over the 128 threads of warpgroup 0, OR-reducing v
-__device__ __forceinline__ int wg0_sync_or(int v) {
+// keeps uses of a tcgen05.ld result after the wait
+__device__ __forceinline__ void reg_after_wait(uint32_t &v) {
+    asm volatile("" : "+r"(v));
+}
+
+// The 3xTF32 products of one chunk (one thread).  a0/b0: shared addresses of
+// the chunk's A and B stages ([hi | lo] each); dF: tensor-memory column of the
+// hi*hi accumulator of the segment, dG: of the cross-term (lo*hi + hi*lo)
+// accumulator of the group; firstF / firstG: the chunk opens that accumulation.
+__device__ __forceinline__ void issue_chunk(uint32_t a0, uint32_t b0, uint32_t dF, uint32_t dG, bool firstF,
+                                            bool firstG) {
+    constexpr uint32_t idesc = idesc_tf32(TC_M, TC_NP);
+#pragma unroll
+    for (int ks = 0; ks < TC_KC / 8; ++ks) {
+        const uint32_t ao = a0 + ks * 2 * TC_LBO_A, bo = b0 + ks * 2 * TC_LBO_B;
+        const uint64_t ahi = sdesc(ao, TC_LBO_A, 128), alo = sdesc(ao + TC_APART, TC_LBO_A, 128);
+        const uint64_t bhi = sdesc(bo, TC_LBO_B, 128), blo = sdesc(bo + TC_BPART, TC_LBO_B, 128);
+        mma_tf32(dG, alo, bhi, idesc, (firstG && ks == 0) ? 0u : 1u);
+        mma_tf32(dG, ahi, blo, idesc, 1u);
+        mma_tf32(dF, ahi, bhi, idesc, (firstF && ks == 0) ? 0u : 1u);
+    }
+}
+
+// barrier 2 over the 128 threads of warps 4-7, OR-reducing v
+__device__ __forceinline__ int epi_sync_or(int v) {
     uint32_t r;
     asm volatile(
         "{\n\t.reg .pred p, q;\n\t"
         "setp.ne.u32 q, %1, 0;\n\t"
-        "bar.red.or.pred p, 1, 128, q;\n\t"
+        "bar.red.or.pred p, 2, 128, q;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(r)
         : "r"(v)
@@ -219,40 +250,20 @@ __device__ __forceinline__ int wg0_sync_or(int v) {
     return (int) r;
 }
 
-// keeps uses of a tcgen05.ld result after the wait
-__device__ __forceinline__ void reg_after_wait(uint32_t &v) {
-    asm volatile("" : "+r"(v));
-}
-
-// The 3xTF32 products of one chunk (one thread).  a0/b0: shared addresses of
-// the chunk's A and B stages ([hi | lo] each); d: tensor-memory column of the
-// accumulator; first: the chunk opens the accumulation.
-__device__ __forceinline__ void issue_chunk(uint32_t a0, uint32_t b0, uint32_t d, bool first) {
-    constexpr uint32_t idesc = idesc_tf32(TC_M, TC_NP);
-#pragma unroll
-    for (int ks = 0; ks < TC_KC / 8; ++ks) {
-        const uint32_t ao = a0 + ks * 2 * TC_LBO_A, bo = b0 + ks * 2 * TC_LBO_B;
-        const uint64_t ahi = sdesc(ao, TC_LBO_A, 128), alo = sdesc(ao + TC_APART, TC_LBO_A, 128);
-        const uint64_t bhi = sdesc(bo, TC_LBO_B, 128), blo = sdesc(bo + TC_BPART, TC_LBO_B, 128);
-        mma_tf32(d, alo, bhi, idesc, (first && ks == 0) ? 0u : 1u);
-        mma_tf32(d, ahi, blo, idesc, 1u);
-        mma_tf32(d, ahi, bhi, idesc, 1u);
-    }
-}
-
 template <int NC1>
 __global__ void __launch_bounds__(TC_T, 1) k_angular_tc(DevBatch B, const AngItem *__restrict__ items,
                                                         const float *__restrict__ bop, double *__restrict__ part,
-                                                        int *__restrict__ err) {
+                                                        int seg, int *__restrict__ err) {
     constexpr int C1 = 1 + NC1, CPR = 2 * C1;
     extern __shared__ __align__(1024) unsigned char smem[];
-    uint64_t *bars = (uint64_t *) (smem + TC_RING);
+    double *wsh = (double *) (smem + TC_RING);              // [TC_MAX_GN][TC_MAX_NS] weights of a group
+    uint64_t *bars = (uint64_t *) (smem + TC_RING + TC_WBUF);
     uint32_t *tmem_hold = (uint32_t *) (bars + TC_NBAR);
     const uint32_t sbase = smem_u32(smem), bring = sbase + TC_ASTAGES * TC_ASTAGE;
     const uint32_t afull0 = smem_u32(bars), adone0 = afull0 + 8 * TC_ASTAGES;
     const uint32_t bfull0 = adone0 + 8 * TC_ASTAGES, bdone0 = bfull0 + 8 * TC_BSLOTS;
     const uint32_t segfull0 = bdone0 + 8 * TC_BSLOTS, segfree0 = segfull0 + 16;
-    const uint32_t fin = segfree0 + 16;
+    const uint32_t gfree = segfree0 + 16, fin = gfree + 8;
 
     const int tid = threadIdx.x, warp = tid >> 5;
     const AngItem it = items[blockIdx.x];
@@ -267,7 +278,7 @@ __global__ void __launch_bounds__(TC_T, 1) k_angular_tc(DevBatch B, const AngIte
     if (s_skip) return;
     if (tid == 0) {
         for (int i = 0; i < TC_ASTAGES; ++i) {
-            mbar_init(afull0 + 8 * i, TC_HALF);
+            mbar_init(afull0 + 8 * i, TC_M);
             mbar_init(adone0 + 8 * i, 1);
         }
         for (int i = 0; i < TC_BSLOTS; ++i) {
@@ -278,6 +289,7 @@ __global__ void __launch_bounds__(TC_T, 1) k_angular_tc(DevBatch B, const AngIte
             mbar_init(segfull0 + 8 * i, 1);
             mbar_init(segfree0 + 8 * i, 128);
         }
+        mbar_init(gfree, 128);
         mbar_init(fin, 1);
         fence_mbar_init();
     }
@@ -288,15 +300,17 @@ __global__ void __launch_bounds__(TC_T, 1) k_angular_tc(DevBatch B, const AngIte
     const uint32_t tmem = *tmem_hold;
     int bad = 0;
 
-    if (tid < TC_HALF) {
-        // ---------------- warps 0-1: the A operand, rows 2h and 2h+1 ----------------
-        const int h = tid;
+    if (tid < TC_M) {
+        // ---------------- warps 0-3: the A operand, one row per thread ----------------
+        // row 2h = (pi + tau)(mu_h), row 2h+1 = s_k (pi - tau)(mu_h); both threads
+        // of a pair run the recurrence of half-angle h
+        const int row = tid, h = row >> 1, mirror = row & 1;
         const int gj = it.xt * TC_HALF + h;
         const bool gact = gj < nh;
         const double mu = gact ? B.mu_pool[C.mu_off + gj] : 0.;
         const double *fv2 = B.fv + (B.n1max + 2);          // (k + 1) / k
         const int fvmax = B.n1max + 1;
-        const int ro = (2 * h >> 3) * 32 + (2 * h & 7) * 4;   // float offset of row 2h in an order group
+        const int ro = (row >> 3) * 32 + (row & 7) * 4;    // float offset of the row in an order group
         int q = 0;
         for (int g = it.rbeg; g < it.rend && !bad; ++g) {
             const int nk = B.tg_nk[g];
@@ -311,16 +325,15 @@ __global__ void __launch_bounds__(TC_T, 1) k_angular_tc(DevBatch B, const AngIte
                 float *aw = (float *) (smem + s * TC_ASTAGE) + ro;
 #pragma unroll
                 for (int k4 = 0; k4 < TC_KC / 4; ++k4) {
-                    float ha[4], la[4], hb[4], lb[4];
+                    float hv[4], lv[4];
 #pragma unroll
                     for (int u = 0; u < 4; ++u) {
                         const int k = kc * TC_KC + k4 * 4 + u + 1;
                         const double f2 = fv2[min(k, fvmax)];
                         // tau_k = k mu pi_k - (k + 1) pi_{k-1}
                         const double tau = fma(kd * mu, p1, -(kd + 1.) * p0);
-                        const double tp = p1 + tau, tm = p1 - tau;
-                        tc_split(tp, ha[u], la[u]);
-                        tc_split((k & 1) ? tm : -tm, hb[u], lb[u]);
+                        const double v = mirror ? ((k & 1) ? p1 - tau : tau - p1) : p1 + tau;
+                        tc_split(v, hv[u], lv[u]);
                         const double pn = fma((1. + f2) * mu, p1, -f2 * p0);
                         p0 = p1;
                         p1 = pn;
@@ -328,33 +341,31 @@ __global__ void __launch_bounds__(TC_T, 1) k_angular_tc(DevBatch B, const AngIte
                     }
                     if (!gact) {
 #pragma unroll
-                        for (int u = 0; u < 4; ++u) ha[u] = la[u] = hb[u] = lb[u] = 0.f;
+                        for (int u = 0; u < 4; ++u) hv[u] = lv[u] = 0.f;
                     }
                     float *o = aw + k4 * (TC_M / 8) * 32;
-                    *(float4 *) o = make_float4(ha[0], ha[1], ha[2], ha[3]);
-                    *(float4 *) (o + 4) = make_float4(hb[0], hb[1], hb[2], hb[3]);
-                    *(float4 *) (o + TC_APART / 4) = make_float4(la[0], la[1], la[2], la[3]);
-                    *(float4 *) (o + TC_APART / 4 + 4) = make_float4(lb[0], lb[1], lb[2], lb[3]);
+                    *(float4 *) o = make_float4(hv[0], hv[1], hv[2], hv[3]);
+                    *(float4 *) (o + TC_APART / 4) = make_float4(lv[0], lv[1], lv[2], lv[3]);
                 }
                 fence_proxy_async();
                 mbar_arrive(afull0 + 8 * s);
             }
         }
-    } else if (warp == 2) {
-        // ---------------- warp 2, lane 0: B copies and the products ----------------
+    } else if (warp == TC_MMA_WARP) {
+        // ---------------- warp 8, lane 0: B copies and the products ----------------
         if ((tid & 31) == 0) {
             // B copies run TC_BAHEAD chunks ahead: chunk pq of the item is chunk pkc of group pg
             int pq = 0, pg = it.rbeg, pkc = 0, qtot = 0;
             for (int g = it.rbeg; g < it.rend; ++g) qtot += B.tg_nk[g];
             uint32_t ph_free = 0u;   // per F buffer b (bit b): parity of its next segfree phase
-            int q = 0, gs = 0;
-            for (int g = it.rbeg; g < it.rend && !bad; ++g) {
+            int q = 0, gs = 0, gi = 0;
+            for (int g = it.rbeg; g < it.rend && !bad; ++g, ++gi) {
                 const int nk = B.tg_nk[g];
                 for (int kc = 0; kc < nk; ++kc, ++q) {
                     const int s = q % TC_ASTAGES, sb = q % TC_BSLOTS;
                     const int b = gs & 1;
-                    const bool seg_first = kc % TC_SEG == 0;
-                    const bool seg_last = kc % TC_SEG == TC_SEG - 1 || kc == nk - 1;
+                    const bool seg_first = kc % seg == 0;
+                    const bool seg_last = kc % seg == seg - 1 || kc == nk - 1;
                     for (; pq <= q + TC_BAHEAD && pq < qtot && !bad; ++pq) {
                         const int ps = pq % TC_BSLOTS;
                         // the slot's previous chunk pq - TC_BSLOTS must have been consumed
@@ -385,8 +396,14 @@ __global__ void __launch_bounds__(TC_T, 1) k_angular_tc(DevBatch B, const AngIte
                         }
                         ph_free ^= 1u << b;
                     }
+                    if (kc == 0 && gi >= 1 && !mbar_wait(gfree, (gi - 1) & 1, err)) {
+                        // the previous group's cross terms must have been read
+                        bad = 1;
+                        break;
+                    }
                     tc_fence_after();
-                    issue_chunk(sbase + s * TC_ASTAGE, bring + sb * TC_BSTAGE, tmem + b * TC_NP, seg_first);
+                    issue_chunk(sbase + s * TC_ASTAGE, bring + sb * TC_BSTAGE, tmem + b * TC_NP, tmem + TC_GCOL,
+                                seg_first, kc == 0);
                     mma_commit(adone0 + 8 * s);
                     mma_commit(bdone0 + 8 * sb);
                     if (seg_last) {
@@ -402,6 +419,8 @@ __global__ void __launch_bounds__(TC_T, 1) k_angular_tc(DevBatch B, const AngIte
         }
     } else if (warp >= 4) {
         // ---------------- warps 4-7: segment sums, quadratic forms ----------------
+        // A warp whose wait fails skips the tensor-memory work from then on but
+        // keeps taking the barriers of the four warps, which stop together.
         const int t1 = tid - 128;                            // product row = tensor-memory lane
         const uint32_t trow = tmem + ((uint32_t) ((warp - 4) * 32) << 16);
         const int eh = t1 >> 1, emir = t1 & 1;
@@ -418,73 +437,83 @@ __global__ void __launch_bounds__(TC_T, 1) k_angular_tc(DevBatch B, const AngIte
             for (int e = 0; e < 4; ++e) racc[s][e] = 0.;
         uint32_t ph_seg = 0u;
         int gs = 0;
-        for (int g = it.rbeg; g < it.rend && !bad; ++g) {
+        for (int g = it.rbeg; g < it.rend; ++g) {
             const int gr0 = B.tg_r0[g], gn = B.tg_n[g], nk = B.tg_nk[g];
-            const int nseg = (nk + TC_SEG - 1) / TC_SEG;
+            const int nseg = (nk + seg - 1) / seg;
+            // the previous group's weights have been read by all four warps
+            if (epi_sync_or(bad || gn > TC_MAX_GN)) {
+                bad = 1;
+                break;
+            }
+            for (int i = t1; i < gn * NS; i += 128) {
+                const int p = i / NS, s = i - p * NS;
+                const int slot = s == 0 ? 0 : (s <= NC1 ? slot1[s - 1] : 1 + B.idx2[s - 1 - NC1]);
+                wsh[p * TC_MAX_NS + s] = B.w[(size_t) slot * R + gr0 + p];
+            }
+            epi_sync_or(0);
             for (int sg = 0; sg < nseg; ++sg, ++gs) {
                 const int b = gs & 1;
+                if (bad) continue;
                 // warp-uniform decision: the tensor-memory accesses below are warp-wide
                 const bool arrived = mbar_wait(segfull0 + 8 * b, (ph_seg >> b) & 1u, err);
                 if (__any_sync(0xffffffffu, !arrived)) {
                     bad = 1;
-                    break;
+                    continue;
                 }
                 ph_seg ^= 1u << b;
                 tc_fence_after();
                 const bool first = sg == 0;
                 if (sg < nseg - 1) {
-                    // running sum (H, L) += F_b, error-free in FP32
+                    // running sum H += F_b (FP32, round to nearest)
 #pragma unroll 1
                     for (int c0 = 0; c0 < TC_NP; c0 += 16) {
                         const uint32_t base = trow + c0;
-                        uint32_t f[16], hh[16], ll[16];
+                        uint32_t f[16], hh[16];
                         tmem_ld16(base + b * TC_NP, f);
-                        if (!first) {
-                            tmem_ld16(base + TC_HCOL, hh);
-                            tmem_ld16(base + TC_LCOL, ll);
-                        }
+                        if (!first) tmem_ld16(base + TC_HCOL, hh);
                         tmem_wait_ld();
 #pragma unroll
                         for (int i = 0; i < 16; ++i) {
                             reg_after_wait(f[i]);
-                            if (!first) {
-                                reg_after_wait(hh[i]);
-                                reg_after_wait(ll[i]);
-                            }
+                            if (!first) reg_after_wait(hh[i]);
                         }
 #pragma unroll
-                        for (int i = 0; i < 16; ++i) {
-                            const float fv = __uint_as_float(f[i]);
-                            if (first) {
-                                hh[i] = f[i];
-                                ll[i] = 0u;
-                            } else {
-                                const float hv = __uint_as_float(hh[i]);
-                                const float sv = __fadd_rn(hv, fv);
-                                const float bp = __fsub_rn(sv, hv);
-                                const float ap = __fsub_rn(sv, bp);
-                                const float e = __fadd_rn(__fsub_rn(hv, ap), __fsub_rn(fv, bp));
-                                hh[i] = __float_as_uint(sv);
-                                ll[i] = __float_as_uint(__fadd_rn(__uint_as_float(ll[i]), e));
-                            }
-                        }
+                        for (int i = 0; i < 16; ++i)
+                            hh[i] = first ? f[i]
+                                          : __float_as_uint(__fadd_rn(__uint_as_float(hh[i]), __uint_as_float(f[i])));
                         tmem_st16(base + TC_HCOL, hh);
-                        tmem_st16(base + TC_LCOL, ll);
                     }
                     tmem_wait_st();
                 } else {
-                    // last segment: the sums of every radius of the group, then the quadratic forms
+                    // last segment: fold the group's cross terms G into F_b and hand G
+                    // back to the products of the next group
+#pragma unroll 1
+                    for (int c0 = 0; c0 < TC_NP; c0 += 16) {
+                        const uint32_t base = trow + c0;
+                        uint32_t f[16], gg[16];
+                        tmem_ld16(base + b * TC_NP, f);
+                        tmem_ld16(base + TC_GCOL, gg);
+                        tmem_wait_ld();
+#pragma unroll
+                        for (int i = 0; i < 16; ++i) {
+                            reg_after_wait(f[i]);
+                            reg_after_wait(gg[i]);
+                            f[i] = __float_as_uint(__fadd_rn(__uint_as_float(f[i]), __uint_as_float(gg[i])));
+                        }
+                        tmem_st16(base + b * TC_NP, f);
+                    }
+                    tmem_wait_st();
+                    tc_fence_before();
+                    mbar_arrive(gfree);
+                    // the sums of every radius of the group, then the quadratic forms
                     for (int p = 0; p < gn; ++p) {
                         // columns of S (i < CPR) and D' (i >= CPR) of radius p
-                        uint32_t vf[2 * CPR], vh[2 * CPR], vl[2 * CPR];
+                        uint32_t vf[2 * CPR], vh[2 * CPR];
 #pragma unroll
                         for (int i = 0; i < 2 * CPR; i += 2) {
                             const uint32_t col = (i < CPR ? 0 : TC_NHALF - CPR) + p * CPR + i;
                             tmem_ld2(trow + b * TC_NP + col, vf[i], vf[i + 1]);
-                            if (!first) {
-                                tmem_ld2(trow + TC_HCOL + col, vh[i], vh[i + 1]);
-                                tmem_ld2(trow + TC_LCOL + col, vl[i], vl[i + 1]);
-                            }
+                            if (!first) tmem_ld2(trow + TC_HCOL + col, vh[i], vh[i + 1]);
                         }
                         tmem_wait_ld();
                         double v[2 * CPR];
@@ -494,15 +523,14 @@ __global__ void __launch_bounds__(TC_T, 1) k_angular_tc(DevBatch B, const AngIte
                             v[i] = (double) __uint_as_float(vf[i]);
                             if (!first) {
                                 reg_after_wait(vh[i]);
-                                reg_after_wait(vl[i]);
-                                v[i] += (double) __uint_as_float(vh[i]) + (double) __uint_as_float(vl[i]);
+                                v[i] += (double) __uint_as_float(vh[i]);
                             }
                         }
                         // sm of this row is the D' sum of its pair row (lane ^ 1)
 #pragma unroll
                         for (int i = CPR; i < 2 * CPR; ++i) v[i] = __shfl_xor_sync(0xffffffffu, v[i], 1);
-                        const int r = gr0 + p;
-                        const double f = B.w[r];
+                        const double *wp = wsh + p * TC_MAX_NS;
+                        const double f = wp[0];
                         // invariants of (sp, sm): |sp|^2, |sm|^2, Re(sp sm*), Im(sm sp*)
                         const double spr = v[0], spi = v[1], smr = v[CPR], smi = v[CPR + 1];
                         const double ia = spr * spr + spi * spi, ib = smr * smr + smi * smi;
@@ -513,7 +541,7 @@ __global__ void __launch_bounds__(TC_T, 1) k_angular_tc(DevBatch B, const AngIte
                         racc[0][3] += f * id;
 #pragma unroll
                         for (int k = 0; k < NC1; ++k) {
-                            const double fl = B.w[(size_t) slot1[k] * R + r];
+                            const double fl = wp[1 + k];
                             const double plr = v[2 + 2 * k], pli = v[3 + 2 * k];
                             const double mlr = v[CPR + 2 + 2 * k], mli = v[CPR + 3 + 2 * k];
                             const double da = 2. * (plr * spr + pli * spi), db = 2. * (mlr * smr + mli * smi);
@@ -527,7 +555,7 @@ __global__ void __launch_bounds__(TC_T, 1) k_angular_tc(DevBatch B, const AngIte
 #pragma unroll
                         for (int k = 0; k < TC_MAX_ND2; ++k) {
                             if (k < nd2) {
-                                const double fl = B.w[(size_t) (1 + B.idx2[k]) * R + r];
+                                const double fl = wp[1 + NC1 + k];
                                 racc[1 + NC1 + k][0] += fl * ia;
                                 racc[1 + NC1 + k][1] += fl * ib;
                                 racc[1 + NC1 + k][2] += fl * ic;
@@ -540,6 +568,7 @@ __global__ void __launch_bounds__(TC_T, 1) k_angular_tc(DevBatch B, const AngIte
                 mbar_arrive(segfree0 + 8 * b);
             }
         }
+        if (epi_sync_or(bad)) bad = 1;
         if (!bad && eact) {
             // phase-matrix elements: ((A + B) / 4, (A - B) / 4, -C / 2, D / 2)
             const int jj = emir ? n_qang - 1 - ej : ej;
@@ -611,7 +640,7 @@ __global__ void __launch_bounds__(128, 1) k_tc_selftest(int K, const double *__r
         __syncthreads();
         if (tid == 0) {
             tc_fence_after();
-            issue_chunk(a0, b0, tmem, kc == 0);
+            issue_chunk(a0, b0, tmem, tmem + TC_GCOL, kc == 0, kc == 0);
             mma_commit(done);
         }
         const int lbad = !mbar_wait(done, ph, err);
@@ -622,13 +651,16 @@ __global__ void __launch_bounds__(128, 1) k_tc_selftest(int K, const double *__r
         tc_fence_after();
         const uint32_t trow = tmem + ((uint32_t) (warp * 32) << 16);
         for (int c = 0; c < TC_NP; c += 2) {
-            uint32_t x, y;
+            uint32_t x, y, gx, gy;
             tmem_ld2(trow + c, x, y);
+            tmem_ld2(trow + TC_GCOL + c, gx, gy);
             tmem_wait_ld();
             reg_after_wait(x);
             reg_after_wait(y);
-            D[(size_t) tid * TC_NP + c] = __uint_as_float(x);
-            D[(size_t) tid * TC_NP + c + 1] = __uint_as_float(y);
+            reg_after_wait(gx);
+            reg_after_wait(gy);
+            D[(size_t) tid * TC_NP + c] = (double) __uint_as_float(x) + (double) __uint_as_float(gx);
+            D[(size_t) tid * TC_NP + c + 1] = (double) __uint_as_float(y) + (double) __uint_as_float(gy);
         }
     } else if (tid == 0) {
         atomicExch(err, 1);
@@ -643,14 +675,14 @@ __global__ void __launch_bounds__(128, 1) k_tc_selftest(int K, const double *__r
 
 template <int NC1>
 int launch_tc(cudaStream_t s, const DevBatch &B, int nitems, const AngItem *items, const float *bop, double *part,
-              int *err) {
+              int seg, int *err) {
     static bool attr = false;
     if (!attr) {
         LMIEB_CUDA_TRY(cudaFuncSetAttribute(k_angular_tc<NC1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int) TC_SMEM));
         attr = true;
     }
-    k_angular_tc<NC1><<<nitems, TC_T, TC_SMEM, s>>>(B, items, bop, part, err);
+    k_angular_tc<NC1><<<nitems, TC_T, TC_SMEM, s>>>(B, items, bop, part, seg, err);
     LMIEB_CUDA_TRY(cudaGetLastError());
     return 0;
 }
@@ -658,14 +690,18 @@ int launch_tc(cudaStream_t s, const DevBatch &B, int nitems, const AngItem *item
 }  // namespace
 
 int launch_angular_tc(cudaStream_t s, const DevBatch &B, int nitems, const AngItem *items, const float *bop,
-                      double *part, int *err) {
+                      double *part, int seg, int *err) {
     if (nitems <= 0) return 0;
+    if (seg < 1) {
+        fprintf(stderr, "ERROR: lmie_b200: tensor-core segment length %d < 1\n", seg);
+        return -1;
+    }
     switch (B.nd1) {
-        case 0: return launch_tc<0>(s, B, nitems, items, bop, part, err);
-        case 1: return launch_tc<1>(s, B, nitems, items, bop, part, err);
-        case 2: return launch_tc<2>(s, B, nitems, items, bop, part, err);
-        case 3: return launch_tc<3>(s, B, nitems, items, bop, part, err);
-        case 4: return launch_tc<4>(s, B, nitems, items, bop, part, err);
+        case 0: return launch_tc<0>(s, B, nitems, items, bop, part, seg, err);
+        case 1: return launch_tc<1>(s, B, nitems, items, bop, part, seg, err);
+        case 2: return launch_tc<2>(s, B, nitems, items, bop, part, seg, err);
+        case 3: return launch_tc<3>(s, B, nitems, items, bop, part, seg, err);
+        case 4: return launch_tc<4>(s, B, nitems, items, bop, part, seg, err);
     }
     fprintf(stderr, "ERROR: lmie_b200: tensor-core angular stage built for at most %d index1 columns\n", TC_MAX_NC1);
     return -1;

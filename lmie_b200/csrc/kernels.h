@@ -94,7 +94,7 @@ int launch_angular(cudaStream_t s, const DevBatch &B, int nc1, int c1base, int n
 // (c), 64 half-angles (xt), a partial slot (g) and the radius groups
 // [rbeg, rend).  err is set when a block gave up waiting.
 int launch_angular_tc(cudaStream_t s, const DevBatch &B, int nitems, const AngItem *items, const float *bop,
-                      double *part, int *err);
+                      double *part, int seg, int *err);
 // D[128 x 240] = A[128 x K] B[240 x K]^T through the same tensor-core path
 int launch_tc_selftest(cudaStream_t s, int K, const double *A, const double *Bm, double *D, int *err);
 // per-case element lists: element e of the flat index space belongs to the

@@ -38,6 +38,8 @@ constexpr uint32_t TC_LBO_A = (TC_M / 8) * 128;     // order-group stride of A
 constexpr uint32_t TC_LBO_B = (TC_NP / 8) * 128;    // order-group stride of B
 constexpr int TC_MAX_NC1 = 4;                       // index1 columns the kernel is built for
 constexpr int TC_MAX_ND2 = 3;                       // index2 slots the kernel is built for (accumulators in registers)
+// cases of fewer orders keep the FP64 angular stage in split-precision batches
+constexpr int TC_MIN_N1 = 16;
 
 // radii per group for nd1 index1 columns
 __host__ __device__ inline int tc_rg(int nd1) { return TC_NHALF / (2 * (1 + nd1)); }
