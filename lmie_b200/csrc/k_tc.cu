@@ -11,8 +11,9 @@
 //     (2k+1)/k mu pi_k - (k+1)/k pi_{k-1}, one dependent FMA per order) and
 //     write row 2h = (pi + tau)(mu_h) or 2h+1 = s_k (pi - tau)(mu_h) of A+,
 //     split into TF32 hi/lo, in the K-major core-matrix layout;
-//   - lane 0 of warp 8 brings the group's B chunks (written by K1) with bulk
-//     copies running ahead of the products, and issues tcgen05.mma kind::tf32
+//   - lane 0 of warp 9 brings the group's B chunks (written by K1) with bulk
+//     copies running ahead of the products; lane 0 of warp 8 issues
+//     tcgen05.mma kind::tf32
 //     (M 128, N 128, K 8): hi*hi into a segment accumulator F, lo*hi + hi*lo
 //     into a cross-term accumulator G of the group, both FP32 in tensor
 //     memory;
@@ -44,9 +45,9 @@
 
 namespace {
 
-constexpr int TC_T = 288;                    // warps 0-3: A operand; 4-7: segment sums and quadratic
-                                             // forms; 8: B copies and products
-constexpr int TC_MMA_WARP = 8;
+constexpr int TC_T = 320;                    // warps 0-3: A operand; 4-7: segment sums and quadratic
+                                             // forms; 8: products; 9: B copies
+constexpr int TC_MMA_WARP = 8, TC_COPY_WARP = 9;
 constexpr int TC_ASTAGES = 3;                // A operand stages
 constexpr int TC_BSLOTS = 6;                 // B operand slots (bulk copies)
 constexpr int TC_BAHEAD = TC_BSLOTS - 2;     // chunks the B copies run ahead of the products
@@ -225,11 +226,13 @@ __device__ __forceinline__ void reg_after_wait(uint32_t &v) {
 __device__ __forceinline__ void issue_chunk(uint32_t a0, uint32_t b0, uint32_t dF, uint32_t dG, bool firstF,
                                             bool firstG) {
     constexpr uint32_t idesc = idesc_tf32(TC_M, TC_NP);
+    // descriptor of the stage start; the start-address field (bits 0-13, in
+    // 16-byte units) of the other operand parts and K steps is an offset
+    const uint64_t da = sdesc(a0, TC_LBO_A, 128), db = sdesc(b0, TC_LBO_B, 128);
 #pragma unroll
     for (int ks = 0; ks < TC_KC / 8; ++ks) {
-        const uint32_t ao = a0 + ks * 2 * TC_LBO_A, bo = b0 + ks * 2 * TC_LBO_B;
-        const uint64_t ahi = sdesc(ao, TC_LBO_A, 128), alo = sdesc(ao + TC_APART, TC_LBO_A, 128);
-        const uint64_t bhi = sdesc(bo, TC_LBO_B, 128), blo = sdesc(bo + TC_BPART, TC_LBO_B, 128);
+        const uint64_t ahi = da + (uint64_t) ((ks * 2 * TC_LBO_A) >> 4), alo = ahi + (TC_APART >> 4);
+        const uint64_t bhi = db + (uint64_t) ((ks * 2 * TC_LBO_B) >> 4), blo = bhi + (TC_BPART >> 4);
         mma_tf32(dG, alo, bhi, idesc, (firstG && ks == 0) ? 0u : 1u);
         mma_tf32(dG, ahi, blo, idesc, 1u);
         mma_tf32(dF, ahi, bhi, idesc, (firstF && ks == 0) ? 0u : 1u);
@@ -317,6 +320,10 @@ __global__ void __launch_bounds__(TC_T, 1) k_angular_tc(DevBatch B, const AngIte
             double p0 = 0., p1 = 1., kd = 1.;              // pi_{k-1}, pi_k, k
             for (int kc = 0; kc < nk; ++kc, ++q) {
                 const int s = q % TC_ASTAGES;
+                // (k + 1) / k of the chunk's orders, loaded while the stage is still in use
+                double f2v[TC_KC];
+#pragma unroll
+                for (int u = 0; u < TC_KC; ++u) f2v[u] = __ldg(fv2 + min(kc * TC_KC + u + 1, fvmax));
                 // the stage's previous chunk must have been consumed by its products
                 if (q >= TC_ASTAGES && !mbar_wait(adone0 + 8 * s, ((q / TC_ASTAGES) - 1) & 1, err)) {
                     bad = 1;
@@ -329,7 +336,7 @@ __global__ void __launch_bounds__(TC_T, 1) k_angular_tc(DevBatch B, const AngIte
 #pragma unroll
                     for (int u = 0; u < 4; ++u) {
                         const int k = kc * TC_KC + k4 * 4 + u + 1;
-                        const double f2 = fv2[min(k, fvmax)];
+                        const double f2 = f2v[k4 * 4 + u];
                         // tau_k = k mu pi_k - (k + 1) pi_{k-1}
                         const double tau = fma(kd * mu, p1, -(kd + 1.) * p0);
                         const double v = mirror ? ((k & 1) ? p1 - tau : tau - p1) : p1 + tau;
@@ -351,39 +358,47 @@ __global__ void __launch_bounds__(TC_T, 1) k_angular_tc(DevBatch B, const AngIte
                 mbar_arrive(afull0 + 8 * s);
             }
         }
-    } else if (warp == TC_MMA_WARP) {
-        // ---------------- warp 8, lane 0: B copies and the products ----------------
+    } else if (warp == TC_COPY_WARP) {
+        // ---------------- warp 9, lane 0: B copies, up to TC_BSLOTS chunks ahead ----------------
         if ((tid & 31) == 0) {
-            // B copies run TC_BAHEAD chunks ahead: chunk pq of the item is chunk pkc of group pg
-            int pq = 0, pg = it.rbeg, pkc = 0, qtot = 0;
-            for (int g = it.rbeg; g < it.rend; ++g) qtot += B.tg_nk[g];
+            int pq = 0;
+            for (int g = it.rbeg; g < it.rend && !bad; ++g) {
+                const int nk = B.tg_nk[g];
+                const float *src = bop + B.tg_off[g];
+                for (int kc = 0; kc < nk; ++kc, ++pq) {
+                    const int ps = pq % TC_BSLOTS;
+                    // the slot's previous chunk pq - TC_BSLOTS must have been consumed
+                    if (pq >= TC_BSLOTS && !mbar_wait(bdone0 + 8 * ps, ((pq / TC_BSLOTS) - 1) & 1, err)) {
+                        bad = 1;
+                        break;
+                    }
+                    mbar_expect_tx(bfull0 + 8 * ps, TC_BSTAGE);
+                    const uint32_t dst = bring + ps * TC_BSTAGE;
+                    bulk_g2s(dst, src, TC_BPART, bfull0 + 8 * ps);
+                    bulk_g2s(dst + TC_BPART, src + TC_BPART / 4, TC_BPART, bfull0 + 8 * ps);
+                    src += TC_BSTAGE / 4;
+                }
+            }
+            // the copies in flight land before the block ends
+            const int q0 = pq > TC_BSLOTS ? pq - TC_BSLOTS : 0;
+            for (int c = q0; c < pq; ++c) mbar_wait(bfull0 + 8 * (c % TC_BSLOTS), (c / TC_BSLOTS) & 1, nullptr);
+        }
+    } else if (warp == TC_MMA_WARP) {
+        // ---------------- warp 8, lane 0: the products ----------------
+        if ((tid & 31) == 0) {
             uint32_t ph_free = 0u;   // per F buffer b (bit b): parity of its next segfree phase
             int q = 0, gs = 0, gi = 0;
+            int nk_next = it.rbeg < it.rend ? B.tg_nk[it.rbeg] : 0;
             for (int g = it.rbeg; g < it.rend && !bad; ++g, ++gi) {
-                const int nk = B.tg_nk[g];
+                const int nk = nk_next;
+                if (g + 1 < it.rend) nk_next = B.tg_nk[g + 1];
+                int sc = 0;                                  // chunk within the segment
                 for (int kc = 0; kc < nk; ++kc, ++q) {
                     const int s = q % TC_ASTAGES, sb = q % TC_BSLOTS;
                     const int b = gs & 1;
-                    const bool seg_first = kc % seg == 0;
-                    const bool seg_last = kc % seg == seg - 1 || kc == nk - 1;
-                    for (; pq <= q + TC_BAHEAD && pq < qtot && !bad; ++pq) {
-                        const int ps = pq % TC_BSLOTS;
-                        // the slot's previous chunk pq - TC_BSLOTS must have been consumed
-                        if (pq >= TC_BSLOTS && !mbar_wait(bdone0 + 8 * ps, ((pq / TC_BSLOTS) - 1) & 1, err)) {
-                            bad = 1;
-                            break;
-                        }
-                        mbar_expect_tx(bfull0 + 8 * ps, TC_BSTAGE);
-                        const float *src = bop + B.tg_off[pg] + (size_t) pkc * (TC_BSTAGE / 4);
-                        const uint32_t dst = bring + ps * TC_BSTAGE;
-                        bulk_g2s(dst, src, TC_BPART, bfull0 + 8 * ps);
-                        bulk_g2s(dst + TC_BPART, src + TC_BPART / 4, TC_BPART, bfull0 + 8 * ps);
-                        if (++pkc == B.tg_nk[pg]) {
-                            ++pg;
-                            pkc = 0;
-                        }
-                    }
-                    if (bad || !mbar_wait(afull0 + 8 * s, (q / TC_ASTAGES) & 1, err) ||
+                    const bool seg_first = sc == 0;
+                    const bool seg_last = sc == seg - 1 || kc == nk - 1;
+                    if (!mbar_wait(afull0 + 8 * s, (q / TC_ASTAGES) & 1, err) ||
                         !mbar_wait(bfull0 + 8 * sb, (q / TC_BSLOTS) & 1, err)) {
                         bad = 1;
                         break;
@@ -409,13 +424,15 @@ __global__ void __launch_bounds__(TC_T, 1) k_angular_tc(DevBatch B, const AngIte
                     if (seg_last) {
                         mma_commit(segfull0 + 8 * b);
                         ++gs;
+                        sc = 0;
+                    } else {
+                        ++sc;
                     }
                 }
             }
-            // all products of this thread have completed and all copies arrived
+            // all products of this thread have completed
             mma_commit(fin);
             mbar_wait(fin, 0u, nullptr);
-            for (int c = q; c < pq; ++c) mbar_wait(bfull0 + 8 * (c % TC_BSLOTS), (c / TC_BSLOTS) & 1, nullptr);
         }
     } else if (warp >= 4) {
         // ---------------- warps 4-7: segment sums, quadratic forms ----------------
