@@ -23,6 +23,8 @@ CSRC = HERE / "csrc"
 INCLUDE = HERE.parent / "include"
 OBJ = HERE / "_build"
 LIB = HERE / "liblmie_b200.so"
+CLI_SRC = HERE / "cli" / "calllmie.c"
+CLI = HERE / "calllmie"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
@@ -100,6 +102,12 @@ def build(force: bool = False, verbose: bool = False) -> Path:
              ["-cudart", "static", "-lm", "-lpthread", "-ldl", "-lrt",
               "-Xlinker", f"--version-script={vs}"])
         os.replace(tmp, LIB)
+    # the command-line driver, linked against the library next to it
+    if force or _stale(CLI, [CLI_SRC, LIB] + sorted(INCLUDE.glob("*.h"))):
+        tmp = CLI.with_suffix(".tmp")
+        _run(["gcc"] + CC_FLAGS + ["-I", str(INCLUDE), str(CLI_SRC), "-o", str(tmp), "-L", str(HERE),
+                                   "-llmie_b200", "-Wl,-rpath,$ORIGIN", "-lm"])
+        os.replace(tmp, CLI)
     return LIB
 
 
