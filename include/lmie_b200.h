@@ -48,7 +48,7 @@ int lmie_solution_batch(int n_cases, lmie_in_data *in, lmie_out_data *out, int a
  * lmieb_rerun_device.  Returns 0, or -1 for chunks < 0. */
 int lmieb_set_pipeline(int chunks);
 
-/* Work items per SM the angular stage of `precision` is cut into (default 4
+/* Work items per SM the angular stage of `precision` is cut into (default 32
  * for FP64, 2 for the tensor-core stage); results differ only in the order of
  * partial sums.  Returns 0 or -1. */
 int lmieb_set_work_granularity(int precision, double items_per_sm);
@@ -64,8 +64,8 @@ int lmieb_get_split_segment(void);
 
 /* Autotuner: solves the batch in[0..n_cases) (outputs in out, allocated by
  * the caller or a previous call) under each candidate pipeline depth
- * (1, 2, 4, 6 parts) and angular work granularity (2, 4, 8 items per SM for
- * FP64; 1, 2, 4 for the tensor-core stage), timing the public batch call on
+ * (1, 2, 4, 6 parts) and angular work granularity (8, 16, 32, 64 items per SM
+ * for FP64; 1, 2, 4 for the tensor-core stage), timing the public batch call on
  * the host clock, and keeps the fastest for later calls (lmieb_set_pipeline,
  * lmieb_set_work_granularity).  Reports the choice and its time (ms) through
  * the non-NULL pointers.  Returns 0 or -1. */

@@ -95,7 +95,7 @@ Ctx g_ctx;
 // Work items per SM the angular stage is cut into ([0] FP64 kernel, [1]
 // tensor-core kernel): finer items balance uneven cases, coarser ones cut the
 // per-item overhead; set by lmieb_set_work_granularity (the autotuner).
-double g_items_per_sm[2] = {4., 2.};
+double g_items_per_sm[2] = {32., 2.};
 
 // Orders (in chunks of TC_KC) per FP32 segment of the tensor-core stage's
 // hi*hi products; set by lmieb_set_split_segment.

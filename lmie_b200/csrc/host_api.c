@@ -901,8 +901,9 @@ int lmie_solution_batch2(int n_cases, lmie_in_data *in, lmie_out_data *out, int 
 int lmie_solution_autotune(int n_cases, lmie_in_data *in, lmie_out_data *out, int n_threads, int precision,
                            int *best_chunks, double *best_items, double *best_ms) {
      static const int chunk_c[] = {1, 2, 4, 6};
-     static const double items_fp64[] = {2., 4., 8.}, items_tc[] = {1., 2., 4.};
+     static const double items_fp64[] = {8., 16., 32., 64.}, items_tc[] = {1., 2., 4.};
      const double *items = precision == LMIEB_PRECISION_TF32X3 ? items_tc : items_fp64;
+     const int n_items = precision == LMIEB_PRECISION_TF32X3 ? 3 : 4;
      const int keep = g_pipeline;
      const double keep_items = lmieb_get_work_granularity(precision);
      int a, b, r, bc = keep, rc = 0;
@@ -914,7 +915,7 @@ int lmie_solution_autotune(int n_cases, lmie_in_data *in, lmie_out_data *out, in
      for (a = 0; a < 4 && rc == 0; ++a) {
           if (chunk_c[a] > 1 && n_cases < 2 * chunk_c[a])
                continue;
-          for (b = 0; b < 3 && rc == 0; ++b) {
+          for (b = 0; b < n_items && rc == 0; ++b) {
                double t = 0.;
                g_pipeline = chunk_c[a];
                lmieb_set_work_granularity(precision, items[b]);

@@ -449,9 +449,11 @@ __global__ void __launch_bounds__(256) k_reduce_scalars(DevBatch B, const double
 // every radius the pi_n/tau_n recurrence runs in registers, the coefficient
 // columns are staged through shared memory ANG_KT orders at a time (the next
 // chunk prefetched into registers), and the quadratic forms of S1, S2 are
-// accumulated per thread in shared memory.
+// accumulated per thread in shared memory.  One half-angle per thread (AP 1)
+// keeps the registers low enough for 12 resident warps per SM, which hides
+// the FP64 latencies better than two half-angles sharing coefficient loads.
 // ---------------------------------------------------------------------------
-constexpr int ANG_T = 64;
+constexpr int ANG_T = 128;
 constexpr int ANG_KT = 64;
 
 template <int NC1, int NC2, int AP>
@@ -1027,7 +1029,7 @@ __global__ void k_phase_user(DevBatch B, long long total, const long long *__res
 }
 
 template <int NC1, int NC2>
-constexpr int angular_ap() { return NC1 <= 2 ? 2 : 1; }
+constexpr int angular_ap() { return 1; }
 
 template <int NC1, int NC2>
 size_t angular_smem() {
@@ -1131,7 +1133,7 @@ int launch_reduce_scalars(cudaStream_t s, const DevBatch &B, const double *rs, d
     return 0;
 }
 
-int angular_angles_per_block(int nc1) { return ANG_T * (nc1 <= 2 ? 2 : 1); }
+int angular_angles_per_block(int) { return ANG_T; }
 
 int launch_angular(cudaStream_t s, const DevBatch &B, int nc1, int c1base, int nc2, int c2base, int first,
                    int nitems, const AngItem *items, const double *coef, double *part, double *save2) {

@@ -117,10 +117,11 @@ def test_autotune_picks_a_candidate_and_keeps_results():
     cases = workloads.batched_uneven(64)
     ref = abi.solve_batch(lib, cases, n_threads=4)
     b = bench.CBatch(lib, cases)
+    keep = lib.lmieb_get_work_granularity(abi.PRECISION_FP64)
     try:
         got = b.autotune(4, abi.PRECISION_FP64)
         assert got["pipeline_parts"] in (1, 2, 4, 6)
-        assert got["angular_items_per_sm"] in (2.0, 4.0, 8.0)
+        assert got["angular_items_per_sm"] in (8.0, 16.0, 32.0, 64.0)
         assert got["ms_per_call"] > 0
         after = abi.solve_batch(lib, cases, n_threads=4)
         for i, (a, r) in enumerate(zip(after, ref)):
@@ -128,4 +129,5 @@ def test_autotune_picks_a_candidate_and_keeps_results():
             assert not {k: v for k, v in err.items() if v > 1e-13}, i
     finally:
         lib.lmieb_set_pipeline(0)
+        lib.lmieb_set_work_granularity(abi.PRECISION_FP64, keep)
         lib.lmieb_set_work_granularity(0, C.c_double(4.0))
