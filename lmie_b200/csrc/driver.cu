@@ -15,6 +15,7 @@
 #include <atomic>
 #include <mutex>
 #include <thread>
+#include <unordered_map>
 #include <vector>
 
 #include "kernels.h"
@@ -58,6 +59,7 @@ struct Slot {
     char *hbuf = nullptr;
     size_t hcap = 0;
     Plan *plan = nullptr;
+    cudaStream_t stream = nullptr;     // the sub-batches of this slot (consecutive ones overlap)
     cudaEvent_t done = nullptr;
     bool have_plan = false;
     cudaGraphExec_t graph = nullptr;   // the plan's kernel sequence, captured for re-runs
@@ -85,7 +87,9 @@ struct Ctx {
     // into a device pool ([n nodes][n weights] per entry) and kept
     double *gl_pool = nullptr;
     size_t gl_cap = 0, gl_used = 0;
-    std::vector<std::pair<int, long long>> gl_map;
+    std::unordered_map<int, long long> gl_map;     // n -> pool offset
+    cudaEvent_t gl_ready = nullptr;                // after the last launch that added entries
+    bool gl_pending = false;
     // host-side phases of the last batch call (ms): prepare, pack, device and copies, unpack, finish
     double host_ms[LMIEB_N_HOST] = {};
 };
@@ -210,8 +214,10 @@ int ensure_ready() {
     for (int i = 0; i <= NSTAGE; ++i) LMIEB_CUDA_TRY(cudaEventCreate(&c.ev[i]));
     for (Slot &S : c.slot) {
         S.plan = new Plan();
+        LMIEB_CUDA_TRY(cudaStreamCreateWithFlags(&S.stream, cudaStreamNonBlocking));
         LMIEB_CUDA_TRY(cudaEventCreateWithFlags(&S.done, cudaEventDisableTiming));
     }
+    LMIEB_CUDA_TRY(cudaEventCreateWithFlags(&c.gl_ready, cudaEventDisableTiming));
     c.ready = true;
     return 0;
 }
@@ -252,6 +258,8 @@ int ensure_gl_pool(size_t doubles) {
     double *np = nullptr;
     LMIEB_CUDA_TRY(cudaMalloc((void **) &np, want * sizeof(double)));
     if (c.gl_pool) {
+        // entries may still be in the making on either slot's stream
+        LMIEB_CUDA_TRY(cudaDeviceSynchronize());
         LMIEB_CUDA_TRY(cudaMemcpyAsync(np, c.gl_pool, c.gl_used * sizeof(double), cudaMemcpyDeviceToDevice,
                                        c.stream));
         LMIEB_CUDA_TRY(cudaStreamSynchronize(c.stream));
@@ -271,9 +279,7 @@ inline void stage(int i) {
 }
 
 // The kernel sequence of one sub-batch on resident inputs (stages 1..7).
-int run_kernels(Plan &L) {
-    Ctx &c = g_ctx;
-    cudaStream_t s = c.stream;
+int run_kernels(Plan &L, cudaStream_t s) {
     const DevBatch &B = L.B;
     stage(1);
     if (L.save_control != 2) {
@@ -401,9 +407,20 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         n1max = std::max(n1max, cn1max[k]);
     }
     const int R = cr0[ncase];
-    std::vector<double> x(R), xl((size_t) std::max(nd1, 1) * R), w((size_t) ncol * R);
-    std::vector<int> n1r(R), n2r(R), rcase(R);
-    std::vector<long long> off(R + 1), ckoff(R + 1);
+    // per-radius arrays: every element is written below; kept between calls
+    // (calls are serialised) so that their pages are not faulted in and
+    // zeroed again for every sub-batch
+    static std::vector<double> x, xl, w;
+    static std::vector<int> n1r, n2r, rcase;
+    static std::vector<long long> off, ckoff;
+    x.resize(R);
+    xl.resize((size_t) std::max(nd1, 1) * R);
+    w.resize((size_t) ncol * R);
+    n1r.resize(R);
+    n2r.resize(R);
+    rcase.resize(R);
+    off.resize(R + 1);
+    ckoff.resize(R + 1);
     std::vector<cplx> ml((size_t) std::max(1, ncase * nd));
     std::vector<double> laml((size_t) std::max(1, ncase * nd));
     off[0] = ckoff[0] = 0;
@@ -478,18 +495,18 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     for (int j = 0; j < nqmax; ++j) gl_jr[j] = j / (j + 1.);
     {
         size_t need = c.gl_used;
+        std::unordered_map<int, long long> fresh;   // entries this batch adds
         for (int k = 0; k < ncase; ++k) {
             const int nq = cs[k].n_qang;
             if (nq <= 0) continue;
             long long at = -1;
-            for (auto &e : c.gl_map)
-                if (e.first == nq) at = e.second;
-            if (at < 0) {
-                for (size_t t = 0; t < gl_ns.size(); ++t)
-                    if (gl_ns[t] == nq) at = gl_mo[t];
-            }
+            const auto hit = c.gl_map.find(nq);
+            if (hit != c.gl_map.end()) at = hit->second;
+            const auto hit2 = fresh.find(nq);
+            if (hit2 != fresh.end()) at = hit2->second;
             if (at < 0) {
                 at = (long long) need;
+                fresh[nq] = at;
                 need += 2 * (size_t) nq;
                 const int ia = 4 * nq + 2, half = (nq + 1) / 2;
                 const double da = (nq - 1) / (8. * pow((double) nq, 3));
@@ -506,7 +523,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
             cs[k].mu_off = at;
         }
         if (ensure_gl_pool(need)) return -1;
-        for (size_t t = 0; t < gl_ns.size(); ++t) c.gl_map.push_back({gl_ns[t], gl_mo[t]});
+        for (size_t t = 0; t < gl_ns.size(); ++t) c.gl_map[gl_ns[t]] = gl_mo[t];
         c.gl_used = need;
     }
 
@@ -534,14 +551,20 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     };
     // coefficient offsets of the radii whose coefficients K1 writes in FP64
     // (all radii, or with split precision those of the FP64 cases)
-    std::vector<long long> coff(R + 1, 0);
+    static std::vector<long long> coff;
+    coff.resize(R + 1);
+    coff[0] = 0;
     for (int k = 0; k < ncase; ++k) {
         const DevCase &C = cs[k];
         for (int r = C.r0; r < C.r0 + C.nr; ++r) coff[r + 1] = coff[r] + (case_tc[k] ? 0 : n1r[r]);
     }
     // split precision: radius groups of tc_rg(nd1) radii, each with its B operand block
-    std::vector<int> tc_pos, tg_r0, tg_n, tg_nk;
-    std::vector<long long> tc_roff, tg_off;
+    static std::vector<int> tc_pos;
+    static std::vector<long long> tc_roff;
+    std::vector<int> tg_r0, tg_n, tg_nk;
+    std::vector<long long> tg_off;
+    tc_pos.clear();
+    tc_roff.clear();
     long long bop_floats = 0;
     if (L.tc) {
         const int RG = tc_rg(nd1);
@@ -912,16 +935,24 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     c.host_ms[1] += t_dev - t_pack;
     c.h2d += h_in_end;
     c.d2h += out_bytes;
-    cudaStream_t s = c.stream;
+    // Each slot has its own stream, so a sub-batch's copies and kernels overlap
+    // those of the previous one; with per-stage timing both use the context's
+    // stream (the stage events are shared) and run one after the other.
+    cudaStream_t s = c.timing ? c.stream : S.stream;
     stage(0);
     LMIEB_CUDA_TRY(cudaMemcpyAsync(d_in, hp, h_in_end, cudaMemcpyHostToDevice, s));
     LMIEB_CUDA_TRY(cudaMemsetAsync(d_out, 0, out_bytes, s));
-    if (!gl_pt.empty() &&
-        launch_gauss(s, (int) gl_pt.size(), (int *) dptr(h_gpt), (int *) dptr(h_gpi), (int *) dptr(h_gns),
-                     (long long *) dptr(h_gmo), (long long *) dptr(h_ggo), (double *) dptr(h_gguess),
-                     (double *) dptr(h_gjr), c.gl_pool))
-        return -1;
-    if (run_kernels(L)) return -1;
+    // Gauss-angle pool entries another sub-batch is still computing
+    if (c.gl_pending) LMIEB_CUDA_TRY(cudaStreamWaitEvent(s, c.gl_ready, 0));
+    if (!gl_pt.empty()) {
+        if (launch_gauss(s, (int) gl_pt.size(), (int *) dptr(h_gpt), (int *) dptr(h_gpi), (int *) dptr(h_gns),
+                         (long long *) dptr(h_gmo), (long long *) dptr(h_ggo), (double *) dptr(h_gguess),
+                         (double *) dptr(h_gjr), c.gl_pool))
+            return -1;
+        LMIEB_CUDA_TRY(cudaEventRecord(c.gl_ready, s));
+        c.gl_pending = true;
+    }
+    if (run_kernels(L, s)) return -1;
     LMIEB_CUDA_TRY(cudaMemcpyAsync(h_out, d_out, out_bytes, cudaMemcpyDeviceToHost, s));
     stage(NSTAGE);
     LMIEB_CUDA_TRY(cudaEventRecord(S.done, s));
@@ -1166,7 +1197,7 @@ extern "C" int lmieb_rerun_device(int reps, int flush_l2, double *ms_total, doub
         c.timing = false;
         cudaGraph_t g = nullptr;
         LMIEB_CUDA_TRY(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
-        const int rc = run_kernels(*S.plan);
+        const int rc = run_kernels(*S.plan, c.stream);
         const cudaError_t ec = cudaStreamEndCapture(c.stream, &g);
         c.timing = was;
         if (rc || ec != cudaSuccess) {
@@ -1198,7 +1229,7 @@ extern "C" int lmieb_rerun_device(int reps, int flush_l2, double *ms_total, doub
     c.timing = true;
     for (int i = 0; i < reps; ++i) {
         if (flush_l2) LMIEB_CUDA_TRY(cudaMemsetAsync(c.flush, i & 0xff, FLUSH_BYTES, c.stream));
-        if (run_kernels(*S.plan)) { c.timing = was; return -1; }
+        if (run_kernels(*S.plan, c.stream)) { c.timing = was; return -1; }
         LMIEB_CUDA_TRY(cudaEventSynchronize(c.ev[8]));
         for (int k = 1; k < 8; ++k) {
             float sm = 0.f;

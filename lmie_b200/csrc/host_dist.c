@@ -17,6 +17,7 @@
  */
 #include <float.h>
 #include <math.h>
+#include <pthread.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -153,6 +154,25 @@ void lmieb_gauss_leg(int n, double x1, double x2, double *x, double *w) {
      }
 }
 
+/* Gauss-Legendre nodes and weights on [-1, 1] ([x | w]), computed once per n
+ * up to GL_CACHE_MAX and kept: every case with the same n_quad reuses them. */
+#define GL_CACHE_MAX 4096
+static pthread_mutex_t gl_cache_mu = PTHREAD_MUTEX_INITIALIZER;
+static double *gl_cache[GL_CACHE_MAX + 1];
+
+static const double *gl_unit(int n) {
+     double *p;
+     if (n < 1 || n > GL_CACHE_MAX) return NULL;
+     pthread_mutex_lock(&gl_cache_mu);
+     p = gl_cache[n];
+     if (!p && (p = (double *) malloc(sizeof(double) * (size_t) n * 2)) != NULL) {
+          lmieb_gauss_leg(n, -1., 1., p, p + n);
+          gl_cache[n] = p;
+     }
+     pthread_mutex_unlock(&gl_cache_mu);
+     return p;
+}
+
 /* n_int equal sub-intervals of [r1, r2], n_quad nodes each; derivatives of
  * nodes and weights follow from those of the end points (r1_l may be NULL:
  * the lower end is fixed). */
@@ -160,10 +180,17 @@ static void interval_quad(int n_int, int n_quad, int nd, double r1, double r2,
                           const double *r1_l, const double *r2_l,
                           double *qx, double *qw, double *qx_l, double *qw_l) {
      int i, j, k, half = (n_quad + 1) / 2;
-     double *tx = (double *) malloc(sizeof(double) * (size_t) n_quad * 2);
-     double *tw = tx + n_quad;
+     const double *unit = gl_unit(n_quad);
+     double *own = NULL;
+     const double *tx, *tw;
      double step = (r2 - r1) / n_int;
-     lmieb_gauss_leg(n_quad, -1., 1., tx, tw);
+     if (!unit) {
+          own = (double *) malloc(sizeof(double) * (size_t) n_quad * 2);
+          lmieb_gauss_leg(n_quad, -1., 1., own, own + n_quad);
+          unit = own;
+     }
+     tx = unit;
+     tw = unit + n_quad;
      for (i = 0; i < n_int; ++i) {
           size_t base = (size_t) i * n_quad;
           double lo = r1 + i * step, hi = lo + step;
@@ -188,7 +215,7 @@ static void interval_quad(int n_int, int n_quad, int nd, double r1, double r2,
                }
           }
      }
-     free(tx);
+     free(own);
 }
 
 /* ---- distributions ---------------------------------------------------------
