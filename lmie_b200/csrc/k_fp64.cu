@@ -96,6 +96,59 @@ __global__ void k_gauss(int npairs, const int *__restrict__ pt, const int *__res
 // sums per radius).
 // ---------------------------------------------------------------------------
 
+// Split-precision operand of K1's radius.  The 8 floats of order j and column
+// slot cc -- e = 0..7: S hi re, S hi im, S lo re, S lo im, D' hi re, D' hi im,
+// D' lo re, D' lo im, with D' = s_j (a - b) fv4 -- are staged in the thread's
+// slot u = (j - 1) % 4 of shared memory, tcbuf[((u * CC + cc) * 8 + e) * T +
+// thread] (a warp's accesses hit consecutive banks); every 4 orders (and after
+// the last) they go out as 16-byte pieces of the K-major core-matrix layout of
+// tc_layout.cuh instead of 4-byte stores per order.
+template <int CC>
+__device__ __forceinline__ void tc_stage(float *tcbuf, int j, int cc, double sre, double sim, double dre,
+                                         double dim) {
+    const int T = blockDim.x, u = (j - 1) & 3;
+    const double sg = (j & 1) ? 1. : -1.;             // s_j of D'
+    float *p = tcbuf + (size_t) ((u * CC + cc) * 8) * T + threadIdx.x;
+    float h, l;
+    tc_split(sre, h, l); p[0] = h; p[2 * T] = l;
+    tc_split(sim, h, l); p[1 * T] = h; p[3 * T] = l;
+    tc_split(sg * dre, h, l); p[4 * T] = h; p[6 * T] = l;
+    tc_split(sg * dim, h, l); p[5 * T] = h; p[7 * T] = l;
+}
+
+// Writes the group of 4 orders that holds order j (orders after j in it are
+// zero) for the column slots this launch produces: slot 0 (the value) when
+// write_value, slots 1.. the tangent-linear columns c0 + 1...
+template <int CC>
+__device__ __forceinline__ void tc_flush(const float *tcbuf, float *__restrict__ rbase, int j, int pos, int c1,
+                                         int c0, int write_value) {
+    const int T = blockDim.x, last = (j - 1) & 3, k0 = (j - 1) - last;
+    const int kc = k0 / TC_KC, kk = k0 - kc * TC_KC;
+    float *base = rbase + (size_t) kc * (TC_BSTAGE / 4);
+    constexpr int P = TC_BPART / 4;
+#pragma unroll
+    for (int cc = 0; cc < CC; ++cc) {
+        if (cc == 0 && !write_value) continue;
+        const int col = cc == 0 ? 0 : c0 + cc;
+        const int n = (pos * c1 + col) * 2;
+        const int i0 = tc_idx(n, kk, TC_NP), d0 = tc_idx(TC_NHALF + n, kk, TC_NP);
+        float v[8][4];
+#pragma unroll
+        for (int e = 0; e < 8; ++e)
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                v[e][u] = u <= last ? tcbuf[(size_t) ((u * CC + cc) * 8 + e) * T + threadIdx.x] : 0.f;
+        *(float4 *) (base + i0) = make_float4(v[0][0], v[0][1], v[0][2], v[0][3]);
+        *(float4 *) (base + i0 + 4) = make_float4(v[1][0], v[1][1], v[1][2], v[1][3]);
+        *(float4 *) (base + P + i0) = make_float4(v[2][0], v[2][1], v[2][2], v[2][3]);
+        *(float4 *) (base + P + i0 + 4) = make_float4(v[3][0], v[3][1], v[3][2], v[3][3]);
+        *(float4 *) (base + d0) = make_float4(v[4][0], v[4][1], v[4][2], v[4][3]);
+        *(float4 *) (base + d0 + 4) = make_float4(v[5][0], v[5][1], v[5][2], v[5][3]);
+        *(float4 *) (base + P + d0) = make_float4(v[6][0], v[6][1], v[6][2], v[6][3]);
+        *(float4 *) (base + P + d0 + 4) = make_float4(v[7][0], v[7][1], v[7][2], v[7][3]);
+    }
+}
+
 template <int NC>
 __global__ void __launch_bounds__(64) k_mie(DevBatch B, int c0, int write_value, double *__restrict__ ck,
                                             double *__restrict__ coef, float *__restrict__ bop,
@@ -215,6 +268,7 @@ __global__ void __launch_bounds__(64) k_mie(DevBatch B, int c0, int write_value,
     const int tpos = bop ? B.tc_pos[r] : -1;
     const bool to_tc = tpos >= 0;
     const long long troff = to_tc ? B.tc_roff[r] : 0;
+    extern __shared__ float tcbuf[];                  // [4][1 + NC][8][blockDim.x] when bop is set
     double4 *cf = (double4 *) coef;
 
     cplx Dloc[K1_B], Dlloc[NC > 0 ? NC : 1][K1_B];
@@ -333,15 +387,17 @@ __global__ void __launch_bounds__(64) k_mie(DevBatch B, int c0, int write_value,
             // expansion coefficients of order j
             if (write_value) {
                 const cplx cs = (a + b) * f4, cd = (a - b) * f4;
-                if (to_tc) tc_put_b(bop, troff, tpos, 1 + B.nd1, 0, j, cs.re, cs.im, cd.re, cd.im);
+                if (to_tc) tc_stage<CC>(tcbuf, j, 0, cs.re, cs.im, cd.re, cd.im);
                 else cf[off + j - 1] = make_double4(cs.re, cs.im, cd.re, cd.im);
             }
 #pragma unroll
             for (int k = 0; k < NC; ++k) {
                 const cplx cs = (al[k] + bl[k]) * f4, cd = (al[k] - bl[k]) * f4;
-                if (to_tc) tc_put_b(bop, troff, tpos, 1 + B.nd1, 1 + c0 + k, j, cs.re, cs.im, cd.re, cd.im);
+                if (to_tc) tc_stage<CC>(tcbuf, j, 1 + k, cs.re, cs.im, cd.re, cd.im);
                 else cf[(size_t) (1 + c0 + k) * tot + off + j - 1] = make_double4(cs.re, cs.im, cd.re, cd.im);
             }
+            if (to_tc && (((j - 1) & 3) == 3 || j == n1))
+                tc_flush<CC>(tcbuf, bop + troff, j, tpos, 1 + B.nd1, c0, write_value);
             // upward: chi_{j+1} and its tangents; shift the previous order
             const double a1 = (2. * j + 1.) * xinv;
             const double chi_n = a1 * chi_c - chi_p;
@@ -1110,7 +1166,8 @@ int launch_coef(cudaStream_t s, const DevBatch &B, int nc, int c0, int write_val
     switch (nc) {
 #define LMIEB_K1(NC_)                                                                                    \
     case NC_:                                                                                            \
-        k_mie<NC_><<<rb, 64, 0, s>>>(B, c0, write_value, ck, coef, bop, rs);                             \
+        k_mie<NC_><<<rb, 64, bop ? 4 * 8 * (1 + NC_) * 64 * sizeof(float) : 0, s>>>(B, c0, write_value, ck,   \
+                                                                                  coef, bop, rs);        \
         break;
     LMIEB_K1(0)
     LMIEB_K1(1)

@@ -66,21 +66,4 @@ __device__ __forceinline__ void tc_split(double v, float &hi, float &lo) {
     lo = tc_tf32(f - h);
 }
 
-// K1 writer: S = cs and D = cd of order j (1-based) of the radius at
-// position pos of its group, column col, into the group block at goff.
-__device__ __forceinline__ void tc_put_b(float *__restrict__ bop, long long goff, int pos, int c1, int col, int j,
-                                         double sre, double sim, double dre, double dim) {
-    const int k = j - 1, kc = k / TC_KC, kk = k - kc * TC_KC;
-    float *base = bop + goff + (size_t) kc * (TC_BSTAGE / 4);
-    const int n = (pos * c1 + col) * 2;
-    const int i0 = tc_idx(n, kk, TC_NP), i1 = i0 + 4;    // n even: n + 1 is the next row of the core matrix
-    const int d0 = tc_idx(TC_NHALF + n, kk, TC_NP), d1 = d0 + 4;
-    const double sg = (j & 1) ? 1. : -1.;                // s_j of D'
-    constexpr int P = TC_BPART / 4;
-    float h, l;
-    tc_split(sre, h, l); base[i0] = h; base[P + i0] = l;
-    tc_split(sim, h, l); base[i1] = h; base[P + i1] = l;
-    tc_split(sg * dre, h, l); base[d0] = h; base[P + d0] = l;
-    tc_split(sg * dim, h, l); base[d1] = h; base[P + d1] = l;
-}
 #endif
