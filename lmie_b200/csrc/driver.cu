@@ -283,7 +283,6 @@ int run_kernels(Plan &L, cudaStream_t s) {
     const DevBatch &B = L.B;
     stage(1);
     if (L.save_control != 2) {
-        if (L.tc) LMIEB_CUDA_TRY(cudaMemsetAsync(L.bop, 0, L.bop_bytes, s));
         for (int ch = 0; ch < (L.nd1c > 0 ? L.nd1c : 1); ++ch) {
             const int c0 = ch * 4;
             const int nc = std::max(0, std::min(4, B.nd1 - c0));
@@ -580,12 +579,12 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
             for (int r = C.r0; r < C.r0 + C.nr; r += RG) {
                 const int n = std::min(RG, C.r0 + C.nr - r);
                 int mx = 1;
+                for (int i = 0; i < n; ++i) mx = std::max(mx, n1r[r + i]);
+                const int nk = (mx + TC_KC - 1) / TC_KC;
                 for (int i = 0; i < n; ++i) {
-                    mx = std::max(mx, n1r[r + i]);
-                    tc_pos[r + i] = i;
+                    tc_pos[r + i] = i + 256 * nk;
                     tc_roff[r + i] = bop_floats;
                 }
-                const int nk = (mx + TC_KC - 1) / TC_KC;
                 tg_r0.push_back(r);
                 tg_n.push_back(n);
                 tg_nk.push_back(nk);

@@ -121,31 +121,49 @@ __device__ __forceinline__ void tc_stage(float *tcbuf, int j, int cc, double sre
 // write_value, slots 1.. the tangent-linear columns c0 + 1...
 template <int CC>
 __device__ __forceinline__ void tc_flush(const float *tcbuf, float *__restrict__ rbase, int j, int pos, int c1,
-                                         int c0, int write_value) {
+                                         int c0, int write_value, int gnk) {
     const int T = blockDim.x, last = (j - 1) & 3, k0 = (j - 1) - last;
-    const int kc = k0 / TC_KC, kk = k0 - kc * TC_KC;
-    float *base = rbase + (size_t) kc * (TC_BSTAGE / 4);
     constexpr int P = TC_BPART / 4;
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
     for (int cc = 0; cc < CC; ++cc) {
         if (cc == 0 && !write_value) continue;
         const int col = cc == 0 ? 0 : c0 + cc;
         const int n = (pos * c1 + col) * 2;
-        const int i0 = tc_idx(n, kk, TC_NP), d0 = tc_idx(TC_NHALF + n, kk, TC_NP);
-        float v[8][4];
+        {
+            const int kc = k0 / TC_KC, kk = k0 - kc * TC_KC;
+            float *base = rbase + (size_t) kc * (TC_BSTAGE / 4);
+            const int i0 = tc_idx(n, kk, TC_NP), d0 = tc_idx(TC_NHALF + n, kk, TC_NP);
+            float v[8][4];
 #pragma unroll
-        for (int e = 0; e < 8; ++e)
+            for (int e = 0; e < 8; ++e)
 #pragma unroll
-            for (int u = 0; u < 4; ++u)
-                v[e][u] = u <= last ? tcbuf[(size_t) ((u * CC + cc) * 8 + e) * T + threadIdx.x] : 0.f;
-        *(float4 *) (base + i0) = make_float4(v[0][0], v[0][1], v[0][2], v[0][3]);
-        *(float4 *) (base + i0 + 4) = make_float4(v[1][0], v[1][1], v[1][2], v[1][3]);
-        *(float4 *) (base + P + i0) = make_float4(v[2][0], v[2][1], v[2][2], v[2][3]);
-        *(float4 *) (base + P + i0 + 4) = make_float4(v[3][0], v[3][1], v[3][2], v[3][3]);
-        *(float4 *) (base + d0) = make_float4(v[4][0], v[4][1], v[4][2], v[4][3]);
-        *(float4 *) (base + d0 + 4) = make_float4(v[5][0], v[5][1], v[5][2], v[5][3]);
-        *(float4 *) (base + P + d0) = make_float4(v[6][0], v[6][1], v[6][2], v[6][3]);
-        *(float4 *) (base + P + d0 + 4) = make_float4(v[7][0], v[7][1], v[7][2], v[7][3]);
+                for (int u = 0; u < 4; ++u)
+                    v[e][u] = u <= last ? tcbuf[(size_t) ((u * CC + cc) * 8 + e) * T + threadIdx.x] : 0.f;
+            *(float4 *) (base + i0) = make_float4(v[0][0], v[0][1], v[0][2], v[0][3]);
+            *(float4 *) (base + i0 + 4) = make_float4(v[1][0], v[1][1], v[1][2], v[1][3]);
+            *(float4 *) (base + P + i0) = make_float4(v[2][0], v[2][1], v[2][2], v[2][3]);
+            *(float4 *) (base + P + i0 + 4) = make_float4(v[3][0], v[3][1], v[3][2], v[3][3]);
+            *(float4 *) (base + d0) = make_float4(v[4][0], v[4][1], v[4][2], v[4][3]);
+            *(float4 *) (base + d0 + 4) = make_float4(v[5][0], v[5][1], v[5][2], v[5][3]);
+            *(float4 *) (base + P + d0) = make_float4(v[6][0], v[6][1], v[6][2], v[6][3]);
+            *(float4 *) (base + P + d0 + 4) = make_float4(v[7][0], v[7][1], v[7][2], v[7][3]);
+        }
+        // after the radius' last order: zeros up to the end of its group's chunks
+        // (the operand buffer is not cleared between solves)
+        for (int k = k0 + 4; k < gnk * TC_KC; k += 4) {
+            const int kc = k / TC_KC, kk = k - kc * TC_KC;
+            float *base = rbase + (size_t) kc * (TC_BSTAGE / 4);
+            const int i0 = tc_idx(n, kk, TC_NP), d0 = tc_idx(TC_NHALF + n, kk, TC_NP);
+            *(float4 *) (base + i0) = z;
+            *(float4 *) (base + i0 + 4) = z;
+            *(float4 *) (base + P + i0) = z;
+            *(float4 *) (base + P + i0 + 4) = z;
+            *(float4 *) (base + d0) = z;
+            *(float4 *) (base + d0 + 4) = z;
+            *(float4 *) (base + P + d0) = z;
+            *(float4 *) (base + P + d0 + 4) = z;
+        }
     }
 }
 
@@ -265,8 +283,9 @@ __global__ void __launch_bounds__(64) k_mie(DevBatch B, int c0, int write_value,
     const cplx Dm2f = minv * minv;
     const size_t tot = (size_t) B.tot, off = (size_t) B.off[r];
     // split precision: the radii of tensor-core cases write the B operand
-    const int tpos = bop ? B.tc_pos[r] : -1;
-    const bool to_tc = tpos >= 0;
+    const int tcode = bop ? B.tc_pos[r] : -1;
+    const bool to_tc = tcode >= 0;
+    const int tpos = tcode & 255, tgnk = tcode >> 8;   // position in the group, the group's chunks
     const long long troff = to_tc ? B.tc_roff[r] : 0;
     extern __shared__ float tcbuf[];                  // [4][1 + NC][8][blockDim.x] when bop is set
     double4 *cf = (double4 *) coef;
@@ -397,7 +416,7 @@ __global__ void __launch_bounds__(64) k_mie(DevBatch B, int c0, int write_value,
                 else cf[(size_t) (1 + c0 + k) * tot + off + j - 1] = make_double4(cs.re, cs.im, cd.re, cd.im);
             }
             if (to_tc && (((j - 1) & 3) == 3 || j == n1))
-                tc_flush<CC>(tcbuf, bop + troff, j, tpos, 1 + B.nd1, c0, write_value);
+                tc_flush<CC>(tcbuf, bop + troff, j, tpos, 1 + B.nd1, c0, write_value, j == n1 ? tgnk : 0);
             // upward: chi_{j+1} and its tangents; shift the previous order
             const double a1 = (2. * j + 1.) * xinv;
             const double chi_n = a1 * chi_c - chi_p;

@@ -56,7 +56,8 @@ struct DevBatch {
     const double *mu_pool;      // Gauss pool: n nodes then n weights at DevCase.mu_off
     const double *mu_user;      // user-angle cosines (DevCase.mu_user_off)
     // split-precision K3 (tc_layout.cuh); null in the FP64 form
-    const int *tc_pos;          // [R] position of the radius in its group
+    const int *tc_pos;          // [R] position of the radius in its group + 256 * the group's chunks
+                                //     (-1: the radius' case keeps the FP64 angular stage)
     const long long *tc_roff;   // [R] float offset of the radius' group in the B operand
     const int *tg_r0, *tg_n, *tg_nk;   // per group: first radius, radii, chunks of TC_KC orders
     const long long *tg_off;    // per group: float offset of its B operand block
