@@ -63,12 +63,13 @@ int lmieb_set_split_segment(int chunks);
 int lmieb_get_split_segment(void);
 
 /* Autotuner: solves the batch in[0..n_cases) (outputs in out, allocated by
- * the caller or a previous call) under each candidate pipeline depth
- * (1, 2, 4, 6 parts) and angular work granularity (8, 16, 32, 64 items per SM
- * for FP64; 1, 2, 4 for the tensor-core stage), timing the public batch call on
- * the host clock, and keeps the fastest for later calls (lmieb_set_pipeline,
- * lmieb_set_work_granularity).  Reports the choice and its time (ms) through
- * the non-NULL pointers.  Returns 0 or -1. */
+ * the caller or a previous call) repeatedly.  It first picks the angular work
+ * granularity (8, 16, 32, 64 items per SM for FP64; 1, 2, 4 for the
+ * tensor-core stage) by the device time of the kernels (per-stage CUDA events,
+ * one sub-batch), then the pipeline depth (1, 2, 4, 6 parts) by the wall time
+ * of the public batch call, and keeps both for later calls
+ * (lmieb_set_work_granularity, lmieb_set_pipeline).  Reports the choice and
+ * the best wall time (ms) through the non-NULL pointers.  Returns 0 or -1. */
 int lmie_solution_autotune(int n_cases, lmie_in_data *in, lmie_out_data *out, int n_threads, int precision,
                            int *best_chunks, double *best_items, double *best_ms);
 

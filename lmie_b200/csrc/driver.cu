@@ -1174,6 +1174,11 @@ extern "C" int lmieb_set_timing(int on) {
     return 0;
 }
 
+extern "C" int lmieb_timing_state(void) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    return g_ctx.timing ? 1 : 0;
+}
+
 extern "C" int lmieb_last_timing(double *ms, int n) {
     std::lock_guard<std::mutex> lock(g_mu);
     for (int i = 0; i < n && i < NSTAGE; ++i) ms[i] = g_ctx.stage_ms[i];

@@ -904,34 +904,57 @@ int lmie_solution_autotune(int n_cases, lmie_in_data *in, lmie_out_data *out, in
      static const double items_fp64[] = {8., 16., 32., 64.}, items_tc[] = {1., 2., 4.};
      const double *items = precision == LMIEB_PRECISION_TF32X3 ? items_tc : items_fp64;
      const int n_items = precision == LMIEB_PRECISION_TF32X3 ? 3 : 4;
-     const int keep = g_pipeline;
+     const int keep = g_pipeline, keep_timing = lmieb_timing_state();
      const double keep_items = lmieb_get_work_granularity(precision);
      int a, b, r, bc = keep, rc = 0;
-     double bi = keep_items, bt = -1.;
+     double bi = keep_items, bd = -1., bt = -1.;
      if (n_cases < 1 || (precision != LMIEB_PRECISION_FP64 && precision != LMIEB_PRECISION_TF32X3)) {
           fprintf(stderr, "ERROR: lmie_solution_autotune(): invalid arguments\n");
           return -1;
      }
+     /* 1. work granularity: only the device work depends on it, so it is
+      *    chosen by the device time of the kernels (per-stage CUDA events,
+      *    one sub-batch), which the host's load does not disturb */
+     g_pipeline = 1;
+     lmieb_set_timing(1);
+     for (b = 0; b < n_items && rc == 0; ++b) {
+          double d = -1.;
+          lmieb_set_work_granularity(precision, items[b]);
+          for (r = 0; r < 3 && rc == 0; ++r) {
+               double st[LMIEB_N_STAGES], dt = 0.;
+               int s;
+               rc = lmie_solution_batch2(n_cases, in, out, 0, 0, n_threads, precision);
+               lmieb_last_timing(st, LMIEB_N_STAGES);
+               for (s = 1; s < LMIEB_N_STAGES - 1; ++s)      /* kernels: stages between the copies */
+                    dt += st[s];
+               if (r > 0 && (d < 0. || dt < d))
+                    d = dt;
+          }
+          if (rc == 0 && (bd < 0. || d < bd)) {
+               bd = d;
+               bi = items[b];
+          }
+     }
+     lmieb_set_timing(keep_timing);
+     /* 2. pipeline depth: the overlap of host work with the device, by the
+      *    wall time of the public batch call (one call to settle the buffers,
+      *    then the faster of two) */
+     lmieb_set_work_granularity(precision, bi);
      for (a = 0; a < 4 && rc == 0; ++a) {
+          double t = -1.;
           if (chunk_c[a] > 1 && n_cases < 2 * chunk_c[a])
                continue;
-          for (b = 0; b < n_items && rc == 0; ++b) {
-               double t = 0.;
-               g_pipeline = chunk_c[a];
-               lmieb_set_work_granularity(precision, items[b]);
-               /* one call to settle the buffers, then the faster of two */
-               for (r = 0; r < 3 && rc == 0; ++r) {
-                    const double t0 = wall_ms();
-                    rc = lmie_solution_batch2(n_cases, in, out, 0, 0, n_threads, precision);
-                    const double dt = wall_ms() - t0;
-                    if (r == 1 || (r == 2 && dt < t))
-                         t = dt;
-               }
-               if (rc == 0 && (bt < 0. || t < bt)) {
-                    bt = t;
-                    bc = chunk_c[a];
-                    bi = items[b];
-               }
+          g_pipeline = chunk_c[a];
+          for (r = 0; r < 3 && rc == 0; ++r) {
+               const double t0 = wall_ms();
+               rc = lmie_solution_batch2(n_cases, in, out, 0, 0, n_threads, precision);
+               const double dt = wall_ms() - t0;
+               if (r > 0 && (t < 0. || dt < t))
+                    t = dt;
+          }
+          if (rc == 0 && (bt < 0. || t < bt)) {
+               bt = t;
+               bc = chunk_c[a];
           }
      }
      g_pipeline = rc == 0 ? bc : keep;

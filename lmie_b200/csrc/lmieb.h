@@ -98,6 +98,8 @@ void lmieb_host_phase(int phase, double ms);
 
 /* Device timing of the last lmieb_device_solve (ms per stage), for bench.py. */
 int lmieb_last_timing(double *ms, int n);
+/* whether per-stage timing is on (internal: not exported) */
+int lmieb_timing_state(void);
 
 #ifdef __cplusplus
 }
