@@ -261,6 +261,39 @@ def split_errors(lib, cases, n_threads: int) -> dict:
                       "separately where the truncation at `accuracy` differed)"}
 
 
+def precision_stress_measurement(lib, n_threads: int, n_cases: int = 8) -> dict:
+    """The large-particle configuration (size parameter up to 5000, 8000 radii,
+    10154 Gauss angles, four derivatives) on a sample of its cases: the split
+    form's error per output array against the FP64 form, and both forms'
+    throughput through the public batch call (wall clock, host buffers)."""
+    cases = workloads.precision_stress(n_cases)
+    lib.lmieb_set_pipeline(0)
+    out = {"workload": f"workloads.precision_stress: first {n_cases} of 256 seeded cases "
+                       "(gamma, r_eff 150-400 um, x_max 5000, 16x500 radii, 4 derivatives)"}
+    res = {}
+    for name, prec in (("fp64", abi.PRECISION_FP64), ("tf32x3", abi.PRECISION_TF32X3)):
+        abi.solve_batch(lib, cases[:1], n_threads=n_threads, precision=prec)   # settle buffers
+        t0 = time.perf_counter()
+        res[name] = abi.solve_batch(lib, cases, n_threads=n_threads, precision=prec)
+        out[name] = {"e2e": n_cases / (time.perf_counter() - t0), "unit": UNIT}
+    worst, same = {}, 0
+    for g, r in zip(res["tf32x3"], res["fp64"]):
+        if g.rc != 0 or r.rc != 0:
+            raise RuntimeError("precision-stress solve failed")
+        nc = min(g.n_coef, r.n_coef)
+        err = {"gc": _relmax(g.gc[:, :nc], r.gc[:, :nc]), "gc_l": _relmax(g.gc_l[:, :, :nc], r.gc_l[:, :, :nc])}
+        if g.n_coef == r.n_coef:
+            same += 1
+            err.update(pf=_relmax(g.pf, r.pf), pf_l=_relmax(g.pf_l, r.pf_l))
+        for k in ("cext", "csca", "cbak", "g"):
+            err[k] = _relmax(g.scalars[k], r.scalars[k])
+        for k, v in err.items():
+            worst[k] = max(worst.get(k, 0.0), float(v))
+    out["split_error_vs_fp64"] = {"max_rel_err": worst, "cases_with_same_n_coef": same,
+                                  "metric": "max over cases of max|split - fp64| / max|fp64| per output array"}
+    return out
+
+
 def adjoint_measurement(lib, steps: int) -> dict:
     import lmie_b200
     p = workloads.adjoint_retrieval()
@@ -443,7 +476,7 @@ def run_b200(args) -> int:
     achieved = flops[0] / (ang_ms * 1e-3) / 1e12 if ang_ms > 0 else None
 
     # secondary: split-precision error, the plain per-case form, the single cloud-droplet case
-    single = split = plain = adj = None
+    single = split = plain = adj = stress = None
     if rank == 0:
         errs = split_errors(lib, cases[:256], threads)
         tf32_peak = None
@@ -480,6 +513,7 @@ def run_b200(args) -> int:
         plain = {"value": n_plain / plain_s, "unit": UNIT, "dtype": "f64",
                  "sample": f"the first {n_plain} cases of the batch, one lmie_solution() call each"}
         adj = adjoint_measurement(lib, 5)
+        stress = precision_stress_measurement(lib, threads)
 
         one = CBatch(lib, [single_case()])
         for _ in range(3):
@@ -523,6 +557,7 @@ def run_b200(args) -> int:
             "split_tf32x3": split,
             "plain": plain,
             "adjoint": adj,
+            "precision_stress": stress,
             "single_case": single,
             "clocks": clk,
         }

@@ -49,6 +49,30 @@ def batched_uneven(n_cases: int = 4096, seed: int = SEED, n_angles: int = 181) -
     return cases
 
 
+def precision_stress(n_cases: int = 256, seed: int = SEED, n_angles: int = 181) -> List[Case]:
+    """Large particles: r_eff uniform in [150, 400] um, v_eff uniform in
+    [0.05, 0.2], wavelength uniform in [0.34, 0.55] um, mr uniform in
+    [1.31, 1.55], mi log-uniform in [1e-9, 1e-3]; gamma distribution on
+    [1e-3 r_eff, r2] with r2 = min(r_eff (1 + 10 v_eff), 5000 lambda / 2 pi), so
+    the size parameter reaches at most 5000 (n1 <= 5077, 10154 Gauss angles);
+    8000 radii (16 intervals of 500 Gauss points); derivatives w.r.t. mr, mi,
+    a1, a2."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    r_eff = rng.uniform(150.0, 400.0, n_cases)
+    v_eff = rng.uniform(0.05, 0.2, n_cases)
+    lam = rng.uniform(0.34, 0.55, n_cases)
+    mr = rng.uniform(1.31, 1.55, n_cases)
+    mi = np.exp(rng.uniform(math.log(1e-9), math.log(1e-3), n_cases))
+    cases = []
+    for i in range(n_cases):
+        r2 = min(r_eff[i] * (1.0 + 10.0 * v_eff[i]), 5000.0 * lam[i] / (2.0 * math.pi))
+        cases.append(Case(dist="gamma", lam=float(lam[i]), mr=float(mr[i]), mi=float(mi[i]),
+                          a1=float(r_eff[i]), a2=float(v_eff[i]), r1=float(1e-3 * r_eff[i]), r2=float(r2),
+                          n_int2=16, n_quad=500, n_angles=n_angles, accuracy=1e-7,
+                          derivs=deriv_unit("mr", "mi", "a1", "a2")))
+    return cases
+
+
 class AdjointProblem:
     """Inputs of lmie_solution_adjoint: wavelengths with their refractive
     indices, one binned size distribution and the loss weights."""
