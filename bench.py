@@ -418,9 +418,10 @@ def run_b200(args) -> int:
             raise RuntimeError("lmie_solution_batch failed")
     barrier()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
-    hm = (C.c_double * 5)()
-    lib.lmieb_last_host_timing(hm, 5)
-    host_ms = dict(zip(("prepare", "pack", "device_and_copies", "unpack", "scatter"), list(hm)))
+    hm = (C.c_double * 7)()
+    lib.lmieb_last_host_timing(hm, 7)
+    host_ms = dict(zip(("prepare", "pack", "device_and_copies", "unpack", "scatter", "device_span",
+                        "device_sum_of_parts"), list(hm)))
 
     # device: K re-runs of the whole batch resident on the device (one part, no
     # host/device overlap), L2 flushed before each (untimed)

@@ -150,9 +150,11 @@ int lmieb_tc_selftest(int K, double *max_rel_err);
  * call, wall-clock ms: 0 preparation of the cases (size distributions,
  * derivative split, per-radius truncations; n_threads threads), 1 packing of
  * the device inputs, 2 device work with its host<->device copies, 3 unpacking
- * of the device outputs, 4 scatter into the callers' lmie_out_data.  Returns
- * LMIEB_N_HOST. */
-#define LMIEB_N_HOST 5
+ * of the device outputs, 4 scatter into the callers' lmie_out_data; and on the
+ * device's clock (CUDA events): 5 the span from the first sub-batch's upload
+ * to the last one's download, 6 the sum of the sub-batches' own spans (more
+ * than 5 where consecutive sub-batches overlap).  Returns LMIEB_N_HOST. */
+#define LMIEB_N_HOST 7
 int lmieb_last_host_timing(double *ms, int n);
 
 /* Selects the GPU the library uses (default: the CUDA runtime's current

@@ -61,6 +61,7 @@ struct Slot {
     Plan *plan = nullptr;
     cudaStream_t stream = nullptr;     // the sub-batches of this slot (consecutive ones overlap)
     cudaEvent_t done = nullptr;
+    cudaEvent_t t_begin = nullptr, t_end = nullptr;   // device span of the sub-batch
     bool have_plan = false;
     cudaGraphExec_t graph = nullptr;   // the plan's kernel sequence, captured for re-runs
     Pending pend;
@@ -88,6 +89,7 @@ struct Ctx {
     double *gl_pool = nullptr;
     size_t gl_cap = 0, gl_used = 0;
     std::unordered_map<int, long long> gl_map;     // n -> pool offset
+    cudaEvent_t t_first = nullptr;                 // upload start of the call's first sub-batch
     cudaEvent_t gl_ready = nullptr;                // after the last launch that added entries
     bool gl_pending = false;
     // host-side phases of the last batch call (ms): prepare, pack, device and copies, unpack, finish
@@ -216,7 +218,10 @@ int ensure_ready() {
         S.plan = new Plan();
         LMIEB_CUDA_TRY(cudaStreamCreateWithFlags(&S.stream, cudaStreamNonBlocking));
         LMIEB_CUDA_TRY(cudaEventCreateWithFlags(&S.done, cudaEventDisableTiming));
+        LMIEB_CUDA_TRY(cudaEventCreate(&S.t_begin));
+        LMIEB_CUDA_TRY(cudaEventCreate(&S.t_end));
     }
+    LMIEB_CUDA_TRY(cudaEventCreate(&c.t_first));
     LMIEB_CUDA_TRY(cudaEventCreateWithFlags(&c.gl_ready, cudaEventDisableTiming));
     c.ready = true;
     return 0;
@@ -939,6 +944,8 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     // stream (the stage events are shared) and run one after the other.
     cudaStream_t s = c.timing ? c.stream : S.stream;
     stage(0);
+    LMIEB_CUDA_TRY(cudaEventRecord(S.t_begin, s));
+    if (c.submits == 1) LMIEB_CUDA_TRY(cudaEventRecord(c.t_first, s));
     LMIEB_CUDA_TRY(cudaMemcpyAsync(d_in, hp, h_in_end, cudaMemcpyHostToDevice, s));
     LMIEB_CUDA_TRY(cudaMemsetAsync(d_out, 0, out_bytes, s));
     // Gauss-angle pool entries another sub-batch is still computing
@@ -954,6 +961,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     if (run_kernels(L, s)) return -1;
     LMIEB_CUDA_TRY(cudaMemcpyAsync(h_out, d_out, out_bytes, cudaMemcpyDeviceToHost, s));
     stage(NSTAGE);
+    LMIEB_CUDA_TRY(cudaEventRecord(S.t_end, s));
     LMIEB_CUDA_TRY(cudaEventRecord(S.done, s));
     S.have_plan = true;
     c.last_slot = (int) (&S - c.slot);
@@ -996,6 +1004,11 @@ int collect_slot(Slot &S) {
     LMIEB_CUDA_TRY(cudaGetLastError());
     const double t_unpack = now_ms();
     c.host_ms[2] += t_unpack - P.t_submit;
+    {
+        float a = 0.f, b = 0.f;
+        if (cudaEventElapsedTime(&a, S.t_begin, S.t_end) == cudaSuccess) c.host_ms[6] += a;
+        if (cudaEventElapsedTime(&b, c.t_first, S.t_end) == cudaSuccess) c.host_ms[5] = std::max(c.host_ms[5], (double) b);
+    }
     if (c.timing) {
         for (int i = 0; i < NSTAGE; ++i) {
             float ms = 0.f;
@@ -1018,9 +1031,16 @@ int collect_slot(Slot &S) {
         const DevCase &C = P.cs[k];
         lmieb_result &r = P.rs[k];
         memcpy(r.scal, hs + C.scal_off, (size_t) ncol * 4 * 8);
-        if (P.want_gc && r.gc) memcpy(r.gc, hg + C.gc_off, (size_t) ncol * 6 * C.n_coef * 8);
-        if (P.want_lc && r.lc) memcpy(r.lc, hl + C.lc_off, (size_t) ncol * 6 * C.n_coef * 8);
-        if (P.pf_from && r.pf) memcpy(r.pf, hpf + C.pf_out_off, (size_t) ncol * 6 * C.n_angles * 8);
+        auto put = [&](double **rows, double *flat, const double *src, size_t len) {
+            if (rows) {
+                for (int i = 0; i < ncol * 6; ++i) memcpy(rows[i], src + (size_t) i * len, len * 8);
+            } else if (flat) {
+                memcpy(flat, src, (size_t) ncol * 6 * len * 8);
+            }
+        };
+        if (P.want_gc) put(r.gc_rows, r.gc, hg + C.gc_off, (size_t) C.n_coef);
+        if (P.want_lc) put(r.lc_rows, r.lc, hl + C.lc_off, (size_t) C.n_coef);
+        if (P.pf_from) put(r.pf_rows, r.pf, hpf + C.pf_out_off, (size_t) C.n_angles);
         const int t = P.want_lc ? htr[ncase + k] : (P.want_gc ? htr[k] : 0);
         r.n_coef_out = (P.want_gc || P.want_lc) ? (t > 0 ? C.n_coef - t + 1 : C.n_coef) : 0;
     });
@@ -1090,6 +1110,7 @@ void reset_counters() {
     Ctx &c = g_ctx;
     for (int i = 0; i < NSTAGE; ++i) c.stage_ms[i] = 0.;
     for (int i = 1; i < 4; ++i) c.host_ms[i] = 0.;
+    c.host_ms[5] = c.host_ms[6] = 0.;
     for (int i = 0; i < 4; ++i) c.work[i] = 0.;
     c.launches = 0;
     c.h2d = c.d2h = 0;

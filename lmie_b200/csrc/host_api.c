@@ -320,6 +320,7 @@ typedef struct {
      int n, nd, n_coef_all;
      double *qx, *qw, *nr, *qx_l, *qw_l, *nr_l;
      double *x, *xl, *w, *w2, *mu_user, *sv1, *sv2, *dev_out;
+     double **rows;             /* the caller's output rows, in device column order */
      int *n1r, *n2r, *idx1, *idx2;
      lmieb_problem P;
      lmieb_result R;
@@ -329,7 +330,8 @@ static void job_free(case_job *j) {
      free(j->qx); free(j->qw); free(j->nr); free(j->qx_l); free(j->qw_l); free(j->nr_l);
      free(j->x); free(j->xl); free(j->w); free(j->w2); free(j->mu_user);
      free(j->n1r); free(j->n2r); free(j->idx1); free(j->idx2); free(j->dev_out);
-     free(j->sv1); free(j->sv2);
+     free(j->sv1); free(j->sv2); free(j->rows);
+     j->rows = NULL;
      j->qx = j->qw = j->nr = j->qx_l = j->qw_l = j->nr_l = NULL;
      j->x = j->xl = j->w = j->w2 = j->mu_user = j->dev_out = j->sv1 = j->sv2 = NULL;
      j->n1r = j->n2r = j->idx1 = j->idx2 = NULL;
@@ -347,7 +349,6 @@ static int job_prepare(case_job *j) {
      lmieb_dist_in din;
      lmieb_dist_out dout;
      lmieb_moments_out mom;
-     size_t n_out;
 
      j->nd = nd;
      /* input check (reference src/lmie_interface.c:404-408) */
@@ -517,16 +518,25 @@ static int job_prepare(case_job *j) {
           j->P.save2_in = j->sv2;
           j->P.w2 = j->w2;
      }
+     /* results: the scalars in a small staging array, the expansions and the
+        phase matrix straight into the caller's rows */
      ncol = 1 + nd;
-     n_out = (size_t) ncol * 4 + (j->P.want_gc ? (size_t) ncol * 6 * j->n_coef_all : 0) +
-             (j->P.want_lc ? (size_t) ncol * 6 * j->n_coef_all : 0) + (size_t) ncol * 6 * j->P.n_angles;
-     j->dev_out = lmieb_arr1(n_out);
+     j->dev_out = lmieb_arr1((size_t) ncol * 4);
      memset(&j->R, 0, sizeof(j->R));
      j->R.scal = j->dev_out;
-     j->R.gc = j->P.want_gc ? j->R.scal + ncol * 4 : NULL;
-     j->R.lc = j->P.want_lc ? j->R.scal + ncol * 4 + (j->P.want_gc ? (size_t) ncol * 6 * j->n_coef_all : 0)
-                            : NULL;
-     j->R.pf = j->P.n_angles > 0 ? j->dev_out + n_out - (size_t) ncol * 6 * j->P.n_angles : NULL;
+     j->rows = (double **) calloc((size_t) 3 * ncol * 6, sizeof(double *));
+     for (k = 0; k < ncol * 6; ++k) {
+          const int col = k / 6, e = k % 6;
+          if (j->P.want_gc)
+               j->rows[k] = col == 0 ? j->gc[e] : j->gc_l[col - 1][e];
+          if (j->P.want_lc)
+               j->rows[ncol * 6 + k] = col == 0 ? j->lc[e] : j->lc_l[col - 1][e];
+          if (j->P.n_angles > 0)
+               j->rows[2 * ncol * 6 + k] = col == 0 ? j->pf[e] : j->pf_l[col - 1][e];
+     }
+     j->R.gc_rows = j->P.want_gc ? j->rows : NULL;
+     j->R.lc_rows = j->P.want_lc ? j->rows + ncol * 6 : NULL;
+     j->R.pf_rows = j->P.n_angles > 0 ? j->rows + 2 * ncol * 6 : NULL;
      if (j->save_control == 1) {
           j->R.save1 = (*j->save1)[0];
           j->R.save2 = (*j->save2)[0][0];
@@ -539,7 +549,7 @@ static int job_prepare(case_job *j) {
 
 /* Copies a solved case's results into the caller's arrays. */
 static void job_finish(case_job *j) {
-     int nd = j->nd, ncol = 1 + nd, nc = j->n_coef_all, k, e;
+     int nd = j->nd, k;
      const double *scal = j->R.scal;
      *j->cext = scal[0];
      *j->csca = scal[1];
@@ -551,30 +561,8 @@ static void job_finish(case_job *j) {
           j->cbak_l[k] = scal[(1 + k) * 4 + 2];
           j->g_l[k] = scal[(1 + k) * 4 + 3];
      }
-     if (j->gc) {
-          for (e = 0; e < 6; ++e)
-               memcpy(j->gc[e], j->R.gc + (size_t) e * nc, sizeof(double) * nc);
-          for (k = 0; k < nd; ++k)
-               for (e = 0; e < 6; ++e)
-                    memcpy(j->gc_l[k][e], j->R.gc + ((size_t) (1 + k) * 6 + e) * nc, sizeof(double) * nc);
-     }
-     if (j->lc) {
-          for (e = 0; e < 6; ++e)
-               memcpy(j->lc[e], j->R.lc + (size_t) e * nc, sizeof(double) * nc);
-          for (k = 0; k < nd; ++k)
-               for (e = 0; e < 6; ++e)
-                    memcpy(j->lc_l[k][e], j->R.lc + ((size_t) (1 + k) * 6 + e) * nc, sizeof(double) * nc);
-     }
-     if (j->calc_pf) {
-          int na = j->n_angles;
-          for (e = 0; e < 6; ++e)
-               memcpy(j->pf[e], j->R.pf + (size_t) e * na, sizeof(double) * na);
-          for (k = 0; k < nd; ++k)
-               for (e = 0; e < 6; ++e)
-                    memcpy(j->pf_l[k][e], j->R.pf + ((size_t) (1 + k) * 6 + e) * na, sizeof(double) * na);
-     }
+     /* gc, lc and pf were written into the caller's rows when unpacked */
      *j->n_coef = j->R.n_coef_out;
-     (void) ncol;
 }
 
 int lmie_solution2_l(int calc_gc, int calc_lc, int calc_pf,
@@ -684,14 +672,16 @@ static void *job_worker(void *arg) {
                break;
           if (p->stage == 0)
                p->jobs[i].rc = job_prepare(&p->jobs[i]);
+          else if (p->stage == 2)
+               job_free(&p->jobs[i]);
           else if (p->jobs[i].rc == 0)
                job_finish(&p->jobs[i]);
      }
      return NULL;
 }
 
-/* Runs stage 0 (prepare) or 1 (finish) of every job on up to n_threads host
- * threads. */
+/* Runs stage 0 (prepare), 1 (finish) or 2 (release the host scratch) of
+ * every job on up to n_threads host threads. */
 static void run_jobs(case_job *jobs, int n, int stage, int n_threads) {
      job_pool p;
      int t, nt = n_threads > 0 ? n_threads : 1;
@@ -886,8 +876,7 @@ int lmie_solution_batch2(int n_cases, lmie_in_data *in, lmie_out_data *out, int 
      }
      lmieb_host_phase(0, t_prep);
      lmieb_host_phase(4, t_fin);
-     for (i = 0; i < n_cases; ++i)
-          job_free(&jobs[i]);
+     run_jobs(jobs, n_cases, 2, n_threads);
      for (c = 0; c < 2; ++c) {
           free(tk[c]); free(tb[c]); free(te[c]);
      }

@@ -66,6 +66,10 @@ typedef struct {
      double *gc;                /* [(1+nd)*6*n_coef] or NULL */
      double *lc;                /* [(1+nd)*6*n_coef] or NULL */
      double *pf;                /* [(1+nd)*6*n_angles] or NULL */
+    /* When set, gc / lc / pf go straight to these rows instead ((1+nd)*6
+     * pointers each, row col*6+e of n_coef or n_angles doubles): the
+     * callers' own output rows. */
+    double **gc_rows, **lc_rows, **pf_rows;
      int n_coef_out;            /* truncated count (the reference's return value) */
      double *save1;             /* [4*n] (save_control 1) or NULL */
      double *save2;             /* [4*n*n_qang] (save_control 1) or NULL */
