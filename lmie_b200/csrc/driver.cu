@@ -13,11 +13,16 @@
 #include <cstdlib>
 #include <cstring>
 #include <atomic>
+#include <condition_variable>
+#include <functional>
 #include <mutex>
 #include <thread>
 #include <unordered_map>
 #include <vector>
 
+#include <unistd.h>
+
+#include "host_pool.h"
 #include "kernels.h"
 #include "tc_layout.cuh"
 #include "lmieb.h"
@@ -117,17 +122,33 @@ void parallel_for(int n, int grain, F &&fn) {
         return;
     }
     std::atomic<int> next(0);
-    auto body = [&]() {
+    const std::function<void()> body = [&]() {
         for (;;) {
             const int i0 = next.fetch_add(grain);
             if (i0 >= n) break;
             for (int i = i0; i < std::min(n, i0 + grain); ++i) fn(i);
         }
     };
-    std::vector<std::thread> th;
-    for (int t = 1; t < nt; ++t) th.emplace_back(body);
-    body();
-    for (auto &t : th) t.join();
+    host_pool().run(nt, body);
+}
+
+// fn(arg, i) for every i in [0, n) on up to n_threads host threads (the
+// case preparation and finishing of the C host layer)
+extern "C" void lmieb_host_parallel(int n, int n_threads, void (*fn)(void *, int), void *arg) {
+    const int nt = std::max(1, std::min(std::min(n_threads, 64), n));
+    if (nt <= 1) {
+        for (int i = 0; i < n; ++i) fn(arg, i);
+        return;
+    }
+    std::atomic<int> next(0);
+    const std::function<void()> body = [&]() {
+        for (;;) {
+            const int i = next.fetch_add(1);
+            if (i >= n) break;
+            fn(arg, i);
+        }
+    };
+    host_pool().run(nt, body);
 }
 
 // memcpy of a large block on several host threads

@@ -657,49 +657,25 @@ static void job_from_struct(case_job *j, lmie_in_data *in, lmie_out_data *out, i
 
 typedef struct {
      case_job *jobs;
-     int n, next, stage;
-     pthread_mutex_t mu;
+     int n, stage;
 } job_pool;
 
-static void *job_worker(void *arg) {
+static void job_stage(void *arg, int i) {
      job_pool *p = (job_pool *) arg;
-     for (;;) {
-          int i;
-          pthread_mutex_lock(&p->mu);
-          i = p->next++;
-          pthread_mutex_unlock(&p->mu);
-          if (i >= p->n)
-               break;
-          if (p->stage == 0)
-               p->jobs[i].rc = job_prepare(&p->jobs[i]);
-          else if (p->stage == 2)
-               job_free(&p->jobs[i]);
-          else if (p->jobs[i].rc == 0)
-               job_finish(&p->jobs[i]);
-     }
-     return NULL;
+     if (p->stage == 0)
+          p->jobs[i].rc = job_prepare(&p->jobs[i]);
+     else if (p->stage == 2)
+          job_free(&p->jobs[i]);
+     else if (p->jobs[i].rc == 0)
+          job_finish(&p->jobs[i]);
 }
 
 /* Runs stage 0 (prepare), 1 (finish) or 2 (release the host scratch) of
  * every job on up to n_threads host threads. */
 static void run_jobs(case_job *jobs, int n, int stage, int n_threads) {
      job_pool p;
-     int t, nt = n_threads > 0 ? n_threads : 1;
-     pthread_t th[64];
-     if (nt > 64)
-          nt = 64;
-     if (nt > n)
-          nt = n;
-     p.jobs = jobs; p.n = n; p.next = 0; p.stage = stage;
-     pthread_mutex_init(&p.mu, NULL);
-     for (t = 1; t < nt; ++t)
-          if (pthread_create(&th[t], NULL, job_worker, &p) != 0)
-               break;
-     nt = t;
-     job_worker(&p);
-     for (t = 1; t < nt; ++t)
-          pthread_join(th[t], NULL);
-     pthread_mutex_destroy(&p.mu);
+     p.jobs = jobs; p.n = n; p.stage = stage;
+     lmieb_host_parallel(n, n_threads > 0 ? n_threads : 1, job_stage, &p);
 }
 
 /* Two prepared cases can share a device batch when their derivative layout

@@ -102,6 +102,10 @@ void lmieb_host_phase(int phase, double ms);
 
 /* Device timing of the last lmieb_device_solve (ms per stage), for bench.py. */
 int lmieb_last_timing(double *ms, int n);
+
+/* fn(arg, i) for i in [0, n) on up to n_threads host threads of the library's
+ * pool (internal: not exported) */
+void lmieb_host_parallel(int n, int n_threads, void (*fn)(void *, int), void *arg);
 /* whether per-stage timing is on (internal: not exported) */
 int lmieb_timing_state(void);
 
