@@ -43,7 +43,9 @@ int lmie_solution_batch(int n_cases, lmie_in_data *in, lmie_out_data *out, int a
 
 /* Batch calls cut their cases into `chunks` parts (0: automatic -- one part
  * per 640 cases, at most 6; 1: one part) and prepare, pack, unpack and
- * scatter one part on the host while the device works on another.  With one
+ * scatter one part on the host while the device works on another; with three
+ * or more parts the first is a quarter and the last half the size of the
+ * others.  With one
  * part a whole batch that fits the device stays resident for
  * lmieb_rerun_device.  Returns 0, or -1 for chunks < 0. */
 int lmieb_set_pipeline(int chunks);
@@ -66,7 +68,7 @@ int lmieb_get_split_segment(void);
  * the caller or a previous call) repeatedly.  It first picks the angular work
  * granularity (8, 16, 32, 64 items per SM for FP64; 1, 2, 4 for the
  * tensor-core stage) by the device time of the kernels (per-stage CUDA events,
- * one sub-batch), then the pipeline depth (1, 2, 4, 6 parts) by the wall time
+ * one sub-batch), then the pipeline depth (1, 2, 3, 4, 6 parts) by the wall time
  * of the public batch call, and keeps both for later calls
  * (lmieb_set_work_granularity, lmieb_set_pipeline).  Reports the choice and
  * the best wall time (ms) through the non-NULL pointers.  Returns 0 or -1. */

@@ -741,12 +741,19 @@ static int finish_chunk(chunk_tickets *ct, case_job *jobs, int j0, int j1, const
      return rc;
 }
 
+/* relative size of chunk c of `chunks` (see lmie_solution_batch2) */
+static double chunk_weight(int c, int chunks) {
+     if (chunks < 3)
+          return 1.;
+     return c == 0 ? 0.25 : (c == chunks - 1 ? 0.5 : 1.);
+}
+
 int lmie_solution_batch2(int n_cases, lmie_in_data *in, lmie_out_data *out, int alloc_out,
                          int verbose, int n_threads, int precision) {
      case_job *jobs;
      lmieb_problem *P;
      lmieb_result *R;
-     int *done, *pos2job, i, k, c, rc = 0, np = 0, chunks, per, first = 1;
+     int *done, *pos2job, *bnd, i, k, c, rc = 0, np = 0, chunks, first = 1, n_last = 0;
      long long *tk[2];
      int *tb[2], *te[2];
      chunk_tickets ct[2];
@@ -788,9 +795,24 @@ int lmie_solution_batch2(int n_cases, lmie_in_data *in, lmie_out_data *out, int 
      chunks = g_pipeline > 0 ? g_pipeline : (n_cases / 640 < 6 ? (n_cases / 640 > 1 ? n_cases / 640 : 1) : 6);
      if (chunks > n_cases)
           chunks = n_cases;
-     per = (n_cases + chunks - 1) / chunks;
-     for (c = 0; c * per < n_cases; ++c) {
-          const int j0 = c * per, j1 = j0 + per < n_cases ? j0 + per : n_cases, s = c & 1, o = s ^ 1;
+     /* chunk boundaries: with three or more chunks the first is a quarter and
+        the last half the size of the others, so that the device starts after a
+        short preparation and the last results are unpacked soon after it ends */
+     bnd = (int *) calloc((size_t) chunks + 1, sizeof(int));
+     {
+          double wsum = 0., acc = 0.;
+          for (c = 0; c < chunks; ++c)
+               wsum += chunk_weight(c, chunks);
+          for (c = 0; c < chunks; ++c) {
+               acc += chunk_weight(c, chunks);
+               bnd[c + 1] = c + 1 == chunks ? n_cases : (int) (n_cases * (acc / wsum) + 0.5);
+               if (bnd[c + 1] < bnd[c] + 1)
+                    bnd[c + 1] = bnd[c] + 1;
+          }
+     }
+     for (c = 0; c < chunks && bnd[c] < n_cases; ++c) {
+          const int j0 = bnd[c], j1 = bnd[c + 1] < n_cases ? bnd[c + 1] : n_cases, s = c & 1, o = s ^ 1;
+          n_last = c;
           int q = 0;
           t0 = wall_ms();
           run_jobs(jobs + j0, j1 - j0, 0, n_threads);
@@ -845,7 +867,7 @@ int lmie_solution_batch2(int n_cases, lmie_in_data *in, lmie_out_data *out, int 
                break;
      }
      for (c = 0; c < 2; ++c) {
-          const int s = ((n_cases + per - 1) / per - 1 + c) & 1;   /* the last chunk, then any other left */
+          const int s = (n_last + c) & 1;   /* the last chunk, then any other left */
           if (ct[s].n && finish_chunk(&ct[s], jobs, cj0[s], cj1[s], pos2job, tb[s], te[s], R, n_threads,
                                       rc == 0, &t_fin))
                rc = -1;
@@ -853,6 +875,7 @@ int lmie_solution_batch2(int n_cases, lmie_in_data *in, lmie_out_data *out, int 
      lmieb_host_phase(0, t_prep);
      lmieb_host_phase(4, t_fin);
      run_jobs(jobs, n_cases, 2, n_threads);
+     free(bnd);
      for (c = 0; c < 2; ++c) {
           free(tk[c]); free(tb[c]); free(te[c]);
      }
@@ -865,7 +888,7 @@ int lmie_solution_batch2(int n_cases, lmie_in_data *in, lmie_out_data *out, int 
 
 int lmie_solution_autotune(int n_cases, lmie_in_data *in, lmie_out_data *out, int n_threads, int precision,
                            int *best_chunks, double *best_items, double *best_ms) {
-     static const int chunk_c[] = {1, 2, 4, 6};
+     static const int chunk_c[] = {1, 2, 3, 4, 6};
      static const double items_fp64[] = {8., 16., 32., 64.}, items_tc[] = {1., 2., 4.};
      const double *items = precision == LMIEB_PRECISION_TF32X3 ? items_tc : items_fp64;
      const int n_items = precision == LMIEB_PRECISION_TF32X3 ? 3 : 4;
@@ -905,7 +928,7 @@ int lmie_solution_autotune(int n_cases, lmie_in_data *in, lmie_out_data *out, in
       *    wall time of the public batch call (one call to settle the buffers,
       *    then the faster of two) */
      lmieb_set_work_granularity(precision, bi);
-     for (a = 0; a < 4 && rc == 0; ++a) {
+     for (a = 0; a < 5 && rc == 0; ++a) {
           double t = -1.;
           if (chunk_c[a] > 1 && n_cases < 2 * chunk_c[a])
                continue;
