@@ -294,6 +294,43 @@ def precision_stress_measurement(lib, n_threads: int, n_cases: int = 8) -> dict:
     return out
 
 
+def save_reweight_measurement(lib, reps: int = 10) -> dict:
+    """A retrieval loop on the cloud-droplet case without index1 derivatives:
+    one save_control 1 solve, then save_control 2 calls that re-weight its
+    per-radius kernels for new effective variances, the kernels staying on
+    the device between calls; also one call whose kernels changed (uploaded)."""
+    import dataclasses
+    case = dataclasses.replace(single_case(), derivs=abi.deriv_unit("a1", "a2"), save_control=1)
+    blk = abi.InputBlock(case)
+    out = abi.lmie_out_data()
+    t0 = time.perf_counter()
+    if lib.lmie_solution(C.byref(blk.s), C.byref(out), 1, 0, 16, 0) != 0:
+        raise RuntimeError("save_control 1 solve failed")
+    t_full = time.perf_counter() - t0
+    h0, m0 = C.c_longlong(), C.c_longlong()
+    lib.lmieb_save_cache_stats(C.byref(h0), C.byref(m0))
+    times = []
+    for i in range(reps):
+        blk2 = abi.InputBlock(dataclasses.replace(case, a2=0.1 + 0.002 * (i + 1), save_control=2))
+        t0 = time.perf_counter()
+        if lib.lmie_solution(C.byref(blk2.s), C.byref(out), 0, 0, 16, 0) != 0:
+            raise RuntimeError("save_control 2 solve failed")
+        times.append(time.perf_counter() - t0)
+    h1, m1 = C.c_longlong(), C.c_longlong()
+    lib.lmieb_save_cache_stats(C.byref(h1), C.byref(m1))
+    # one call whose kernels differ from the kept set (one value changed, then restored)
+    keep = out.save2[0][0][0]
+    out.save2[0][0][0] = keep * (1.0 + 2.0 ** -40)
+    t0 = time.perf_counter()
+    lib.lmie_solution(C.byref(blk2.s), C.byref(out), 0, 0, 16, 0)
+    t_miss = time.perf_counter() - t0
+    out.save2[0][0][0] = keep
+    return {"workload": "cloud droplet (gamma r_eff 10 um, 4x500 radii, 948 Gauss angles), derivatives a1, a2",
+            "save_control1_ms": t_full * 1e3, "save_control2_kept_ms": statistics.median(times) * 1e3,
+            "save_control2_uploaded_ms": t_miss * 1e3,
+            "kept_calls": h1.value - h0.value, "uploaded_calls": m1.value - m0.value}
+
+
 def adjoint_measurement(lib, steps: int) -> dict:
     import lmie_b200
     p = workloads.adjoint_retrieval()
@@ -477,7 +514,7 @@ def run_b200(args) -> int:
     achieved = flops[0] / (ang_ms * 1e-3) / 1e12 if ang_ms > 0 else None
 
     # secondary: split-precision error, the plain per-case form, the single cloud-droplet case
-    single = split = plain = adj = stress = None
+    single = split = plain = adj = stress = reweight = None
     if rank == 0:
         errs = split_errors(lib, cases[:256], threads)
         tf32_peak = None
@@ -515,6 +552,7 @@ def run_b200(args) -> int:
                  "sample": f"the first {n_plain} cases of the batch, one lmie_solution() call each"}
         adj = adjoint_measurement(lib, 5)
         stress = precision_stress_measurement(lib, threads)
+        reweight = save_reweight_measurement(lib)
 
         one = CBatch(lib, [single_case()])
         for _ in range(3):
@@ -559,6 +597,7 @@ def run_b200(args) -> int:
             "plain": plain,
             "adjoint": adj,
             "precision_stress": stress,
+            "save_reweight": reweight,
             "single_case": single,
             "clocks": clk,
         }

@@ -159,6 +159,16 @@ int lmieb_tc_selftest(int K, double *max_rel_err);
 #define LMIEB_N_HOST 7
 int lmieb_last_host_timing(double *ms, int n);
 
+/* save_control: the per-radius kernels (save1, save2) of the last
+ * save_control 1 solve, or of the last save_control 2 call whose kernels were
+ * not on the device, stay on the device.  A save_control 2 call hashes the
+ * kernels it is given (all of their values, through the caller's row
+ * pointers) and uploads them only when they differ from the kept set, so the
+ * re-weighting calls of a retrieval loop send the kernels once.  Reports how
+ * many save_control 2 calls found their kernels on the device (hits) and how
+ * many uploaded them (misses) since the library was loaded.  Returns 0. */
+int lmieb_save_cache_stats(long long *hits, long long *misses);
+
 /* Selects the GPU the library uses (default: the CUDA runtime's current
  * device).  Must precede the first solve; one process drives one GPU. */
 int lmieb_set_device(int device);

@@ -42,6 +42,7 @@ def library() -> C.CDLL:
         lib.lmieb_get_work_granularity.argtypes = [C.c_int]
         lib.lmieb_get_work_granularity.restype = C.c_double
         lib.lmieb_set_split_segment.argtypes = [C.c_int]
+        lib.lmieb_save_cache_stats.argtypes = [C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
         lib.lmieb_get_split_segment.argtypes = []
         _lib = lib
     return _lib

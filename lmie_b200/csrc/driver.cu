@@ -95,6 +95,20 @@ struct Ctx {
     size_t gl_cap = 0, gl_used = 0;
     std::unordered_map<int, long long> gl_map;     // n -> pool offset
     cudaEvent_t t_first = nullptr;                 // upload start of the call's first sub-batch
+    // save_control: the last per-radius kernels (save1, save2) seen, kept on
+    // the device and recognised by a hash of their contents, so that the
+    // re-weighting calls of a retrieval loop upload them once
+    struct {
+        double *d = nullptr;            // [4 R] save1 then [4 R max(nq, 1)] save2
+        size_t cap = 0;                 // doubles
+        unsigned long long key = 0;
+        int R = 0, nq = 0;
+        bool valid = false;
+        long long owner = -1;           // sub-batch whose kernels fill it
+        cudaEvent_t ready = nullptr;    // after the copy that filled it
+        bool pending = false;
+        long long hits = 0, misses = 0;
+    } save;
     cudaEvent_t gl_ready = nullptr;                // after the last launch that added entries
     bool gl_pending = false;
     // host-side phases of the last batch call (ms): prepare, pack, device and copies, unpack, finish
@@ -166,6 +180,31 @@ double now_ms() {
 }
 std::mutex g_mu;
 int g_want_device = -1;
+
+// Content hash of the save_control kernels: save1 as 4 rows of R, then (when
+// nq > 0) save2 as 4 R rows of nq, each row hashed on its own (in parallel),
+// the row hashes combined in order.  row(i) gives row i.
+inline unsigned long long mix64(unsigned long long h, unsigned long long w) {
+    h ^= w;
+    h *= 0x9E3779B97F4A7C15ull;
+    return h ^ (h >> 29);
+}
+
+template <class Row>
+unsigned long long save_hash(int R, int nq, Row row) {
+    const int nrows = 4 + (nq > 0 ? 4 * R : 0);
+    std::vector<unsigned long long> rh((size_t) nrows);
+    parallel_for(nrows, 64, [&](int i) {
+        const size_t len = i < 4 ? (size_t) R : (size_t) nq;
+        const unsigned long long *w = (const unsigned long long *) row(i);
+        unsigned long long h = 0x243F6A8885A308D3ull ^ len;
+        for (size_t k = 0; k < len; ++k) h = mix64(h, w[k]);
+        rh[i] = h;
+    });
+    unsigned long long h = mix64((unsigned long long) R, (unsigned long long) nq);
+    for (int i = 0; i < nrows; ++i) h = mix64(h, rh[i]);
+    return h;
+}
 
 struct Arena {
     char *base;
@@ -243,6 +282,7 @@ int ensure_ready() {
         LMIEB_CUDA_TRY(cudaEventCreate(&S.t_end));
     }
     LMIEB_CUDA_TRY(cudaEventCreate(&c.t_first));
+    LMIEB_CUDA_TRY(cudaEventCreateWithFlags(&c.save.ready, cudaEventDisableTiming));
     LMIEB_CUDA_TRY(cudaEventCreateWithFlags(&c.gl_ready, cudaEventDisableTiming));
     c.ready = true;
     return 0;
@@ -365,6 +405,25 @@ T *put(char *hp, size_t &off, const T *src, size_t count) {
     if (src && count) par_memcpy(at, src, count * sizeof(T));
     off += pad(count * sizeof(T));
     return at;
+}
+
+// Makes the save_control cache ready to be overwritten by stream s with a set
+// of R radii: waits for the work that may still read the old set, grows it.
+int save_fill(int R, size_t n_save2, cudaStream_t s) {
+    Ctx &c = g_ctx;
+    const size_t need = (size_t) 4 * R + n_save2;
+    (void) s;
+    LMIEB_CUDA_TRY(cudaDeviceSynchronize());
+    c.save.valid = false;
+    if (need > c.save.cap) {
+        if (c.save.d) LMIEB_CUDA_TRY(cudaFree(c.save.d));
+        c.save.d = nullptr;
+        c.save.cap = 0;
+        LMIEB_CUDA_TRY(cudaMalloc((void **) &c.save.d, need * sizeof(double)));
+        c.save.cap = need;
+        for (Slot &S : c.slot) drop_graph(S);   // a captured re-run may point at the old set
+    }
+    return 0;
 }
 
 // Device bytes one case needs beyond its inputs (for cutting sub-batches).
@@ -774,6 +833,19 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
 
     // ---- host staging: inputs then outputs ----
     const size_t n_save2 = (size_t) 4 * R * std::max(L.n_qang0, 1);
+    // save_control 2: the caller's kernels, unless the device still holds them
+    const int save_nq = p0.save2_rows ? L.n_qang0 : 0;
+    auto save_row = [&](int i) -> const double * {
+        return i < 4 ? p0.save1_rows[i] : p0.save2_rows[(i - 4) / R][(i - 4) % R];
+    };
+    bool save_hit = false;
+    unsigned long long save_key = 0;
+    if (L.save_control == 2) {
+        save_key = save_hash(R, save_nq, save_row);
+        save_hit = c.save.valid && c.save.key == save_key && c.save.R == R && c.save.nq == save_nq &&
+                   c.save.cap >= (size_t) 4 * R + n_save2;
+        ++(save_hit ? c.save.hits : c.save.misses);
+    }
     size_t in_bytes = 0;
     {
         auto add = [&](size_t b) { in_bytes += pad(b); };
@@ -788,7 +860,10 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         for (int q = 0; q < 5; ++q) add((size_t) (ncase + 1) * 8);
         add(gl_ns.size() * 4); add(gl_mo.size() * 8); add(gl_go.size() * 8); add(gl_pt.size() * 4);
         add(gl_pi.size() * 4); add(gl_guess.size() * 8); add(gl_jr.size() * 8);
-        if (L.save_control == 2) { add((size_t) 4 * R * 8); add(n_save2 * 8); add((size_t) std::max(nd, 1) * R * 8); }
+        if (L.save_control == 2) {
+            if (!save_hit) { add((size_t) 4 * R * 8); add(n_save2 * 8); }
+            add((size_t) std::max(nd, 1) * R * 8);
+        }
     }
     size_t out_bytes = 0;
     {
@@ -838,8 +913,17 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     double *h_gjr = put(hp, ho, gl_jr.data(), gl_jr.size());
     double *h_s1 = nullptr, *h_s2 = nullptr, *h_w2 = nullptr;
     if (L.save_control == 2) {
-        h_s1 = put(hp, ho, p0.save1_in, (size_t) 4 * R);
-        h_s2 = put(hp, ho, p0.save2_in, n_save2);
+        if (!save_hit) {
+            // gathered through the caller's row pointers
+            h_s1 = put(hp, ho, (const double *) nullptr, (size_t) 4 * R);
+            h_s2 = put(hp, ho, (const double *) nullptr, n_save2);
+            const int nrows = 4 + (save_nq > 0 ? 4 * R : 0);
+            parallel_for(nrows, 64, [&](int i) {
+                if (i < 4) memcpy(h_s1 + (size_t) i * R, save_row(i), (size_t) R * 8);
+                else memcpy(h_s2 + (size_t) (i - 4) * save_nq, save_row(i), (size_t) save_nq * 8);
+            });
+            if (save_nq == 0) memset(h_s2, 0, n_save2 * 8);
+        }
         h_w2 = put(hp, ho, p0.w2, (size_t) std::max(nd, 1) * R);
     }
     const size_t h_in_end = ho;
@@ -918,8 +1002,8 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     L.fin_start = (long long *) dptr(h_fin);
     L.pu_start = (long long *) dptr(h_pus);
     if (L.save_control == 2) {
-        L.save1_in = (double *) dptr(h_s1);
-        L.save2_in = (double *) dptr(h_s2);
+        L.save1_in = save_hit ? c.save.d : (double *) dptr(h_s1);
+        L.save2_in = save_hit ? c.save.d + (size_t) 4 * R : (double *) dptr(h_s2);
         L.w2 = (double *) dptr(h_w2);
     }
     if (L.save_control != 2) {
@@ -971,6 +1055,22 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     LMIEB_CUDA_TRY(cudaMemsetAsync(d_out, 0, out_bytes, s));
     // Gauss-angle pool entries another sub-batch is still computing
     if (c.gl_pending) LMIEB_CUDA_TRY(cudaStreamWaitEvent(s, c.gl_ready, 0));
+    if (L.save_control == 2 && save_hit && c.save.pending) LMIEB_CUDA_TRY(cudaStreamWaitEvent(s, c.save.ready, 0));
+    if (L.save_control == 2 && !save_hit) {
+        // keep this set of kernels on the device for the next re-weighting
+        // calls (replacing the previous set once nothing reads it any more)
+        if (save_fill(R, n_save2, s)) return -1;
+        LMIEB_CUDA_TRY(cudaMemcpyAsync(c.save.d, L.save1_in, (size_t) 4 * R * 8, cudaMemcpyDeviceToDevice, s));
+        LMIEB_CUDA_TRY(cudaMemcpyAsync(c.save.d + (size_t) 4 * R, L.save2_in, n_save2 * 8,
+                                       cudaMemcpyDeviceToDevice, s));
+        LMIEB_CUDA_TRY(cudaEventRecord(c.save.ready, s));
+        c.save.pending = true;
+        c.save.key = save_key;
+        c.save.R = R;
+        c.save.nq = save_nq;
+        c.save.valid = true;
+        c.save.owner = ticket;
+    }
     if (!gl_pt.empty()) {
         if (launch_gauss(s, (int) gl_pt.size(), (int *) dptr(h_gpt), (int *) dptr(h_gpi), (int *) dptr(h_gns),
                          (long long *) dptr(h_gmo), (long long *) dptr(h_ggo), (double *) dptr(h_gguess),
@@ -980,6 +1080,20 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         c.gl_pending = true;
     }
     if (run_kernels(L, s)) return -1;
+    if (L.save_control == 1) {
+        // the kernels this solve saves: kept on the device as well, recognised
+        // once their hash is known (when the sub-batch is collected)
+        if (save_fill(R, n_save2, s)) return -1;
+        LMIEB_CUDA_TRY(cudaMemcpyAsync(c.save.d, L.o_save1, (size_t) 4 * R * 8, cudaMemcpyDeviceToDevice, s));
+        LMIEB_CUDA_TRY(cudaMemcpyAsync(c.save.d + (size_t) 4 * R, L.o_save2, n_save2 * 8,
+                                       cudaMemcpyDeviceToDevice, s));
+        LMIEB_CUDA_TRY(cudaEventRecord(c.save.ready, s));
+        c.save.pending = true;
+        c.save.valid = false;
+        c.save.R = R;
+        c.save.nq = L.n_qang0;
+        c.save.owner = ticket;
+    }
     LMIEB_CUDA_TRY(cudaMemcpyAsync(h_out, d_out, out_bytes, cudaMemcpyDeviceToHost, s));
     stage(NSTAGE);
     LMIEB_CUDA_TRY(cudaEventRecord(S.t_end, s));
@@ -1065,6 +1179,17 @@ int collect_slot(Slot &S) {
         const int t = P.want_lc ? htr[ncase + k] : (P.want_gc ? htr[k] : 0);
         r.n_coef_out = (P.want_gc || P.want_lc) ? (t > 0 ? C.n_coef - t + 1 : C.n_coef) : 0;
     });
+    if (P.save_control == 1 && c.save.owner == P.ticket) {
+        // the set just saved: its hash, over the same rows a later
+        // save_control 2 call hashes through its row pointers
+        const double *h1 = (const double *) hostp(P.o_save1), *h2 = (const double *) hostp(P.o_save2);
+        const int R = P.R, nq = P.n_qang0;
+        c.save.key = save_hash(R, nq, [&](int i) -> const double * {
+            return i < 4 ? h1 + (size_t) i * R : h2 + (size_t) (i - 4) * nq;
+        });
+        c.save.nq = nq;
+        c.save.valid = true;
+    }
     if (P.save_control == 1) {
         lmieb_result &r = P.rs[0];
         if (r.save1) memcpy(r.save1, hostp(P.o_save1), (size_t) 4 * P.R * 8);
@@ -1213,6 +1338,13 @@ extern "C" int lmieb_set_device(int device) {
 extern "C" int lmieb_set_timing(int on) {
     std::lock_guard<std::mutex> lock(g_mu);
     g_ctx.timing = on != 0;
+    return 0;
+}
+
+extern "C" int lmieb_save_cache_stats(long long *hits, long long *misses) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    if (hits) *hits = g_ctx.save.hits;
+    if (misses) *misses = g_ctx.save.misses;
     return 0;
 }
 

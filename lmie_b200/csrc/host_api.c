@@ -464,7 +464,6 @@ static int job_prepare(case_job *j) {
           *j->save2 = lmieb_arr3(4, n, n_qang > 0 ? n_qang : 1);
      }
      if (j->save_control == 2) {
-          int q, r;
           if (!j->save1 || !*j->save1 || (n_qang > 0 && (!j->save2 || !*j->save2))) {
                fprintf(stderr, "ERROR: save_control = 2 needs save1 and save2 from a "
                        "save_control = 1 call\n");
@@ -477,16 +476,8 @@ static int job_prepare(case_job *j) {
                     j->w2[(size_t) kk * n + i] = j->nr_l[(size_t) i * nd + kk] * j->qw[i] +
                                                  j->nr[i] * j->qw_l[(size_t) i * nd + kk];
                }
-          /* gather the caller's kernels through their row pointers */
-          j->sv1 = lmieb_arr1((size_t) 4 * n);
-          j->sv2 = lmieb_arr1((size_t) 4 * n * (n_qang > 0 ? n_qang : 1));
-          for (q = 0; q < 4; ++q) {
-               memcpy(j->sv1 + (size_t) q * n, (*j->save1)[q], sizeof(double) * n);
-               if (n_qang > 0)
-                    for (r = 0; r < n; ++r)
-                         memcpy(j->sv2 + ((size_t) q * n + r) * n_qang, (*j->save2)[q][r],
-                                sizeof(double) * n_qang);
-          }
+          /* the caller's kernels are read through their row pointers by the
+             device layer, which keeps the last set it saw on the device */
      }
 
      /* user angles (reference misc/rtutil_scat_int.c:487-503,580) */
@@ -514,8 +505,8 @@ static int job_prepare(case_job *j) {
      j->P.accuracy = j->accuracy;
      j->P.save_control = j->save_control;
      if (j->save_control == 2) {
-          j->P.save1_in = j->sv1;
-          j->P.save2_in = j->sv2;
+          j->P.save1_rows = (const double *const *) *j->save1;
+          j->P.save2_rows = n_qang > 0 ? (const double *const *const *) *j->save2 : NULL;
           j->P.w2 = j->w2;
      }
      /* results: the scalars in a small staging array, the expansions and the

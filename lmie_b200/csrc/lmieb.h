@@ -53,8 +53,8 @@ typedef struct {
      double accuracy;
 
      int save_control;          /* 0, 1 or 2 */
-     const double *save1_in;    /* [4*n]            save_control 2 */
-     const double *save2_in;    /* [4*n*n_qang]     save_control 2 */
+     const double *const *save1_rows;            /* save_control 2: rows [4][n] */
+     const double *const *const *save2_rows;     /* save_control 2: rows [4][n][n_qang] (NULL if n_qang 0) */
      const double *w2;          /* [nd*n] save_control 2: nr_l qw + nr qw_l per slot */
 
      int precision;             /* LMIEB_PRECISION_* of include/lmie_b200.h */

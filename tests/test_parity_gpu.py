@@ -191,6 +191,63 @@ def _oracle_solve_prealloc(lib, blk, out, mc, case):
     return lib.oracle_solution(C.byref(blk.s), C.byref(out), 1)
 
 
+def _reweight(lib, kind, case, s1, s2):
+    """A save_control 2 solve of `case` on the kernels s1 [4, n], s2 [4, n, nq]
+    (numpy), handed over through row pointers as LMie callers do."""
+    blk = abi.InputBlock(case)
+    out = abi.lmie_out_data()
+    s1 = np.ascontiguousarray(s1)
+    s2 = np.ascontiguousarray(s2)
+    n = s2.shape[1]
+    rows1 = (abi.PD * 4)(*[s1[e].ctypes.data_as(abi.PD) for e in range(4)])
+    rows2 = [(abi.PD * n)(*[s2[e, r].ctypes.data_as(abi.PD) for r in range(n)]) for e in range(4)]
+    rows2p = (abi.PPD * 4)(*[C.cast(r, abi.PPD) for r in rows2])
+    out.save1 = C.cast(rows1, abi.PPD)
+    out.save2 = C.cast(rows2p, abi.PPPD)
+    if kind == "oracle":
+        mc = lib.oracle_calc_max_coef(case.lam, 4, case.a1, case.a2, 0.0, case.r1, case.r2)
+        rc = lib.oracle_solution(C.byref(blk.s), C.byref(out), 1)
+    else:
+        mc = lib.lmie_calc_max_coef(case.lam, 4, case.a1, case.a2, 0.0, case.r1, case.r2)
+        rc = lib.lmie_solution(C.byref(blk.s), C.byref(out), 1, 0, 1, 0)
+    assert rc == 0
+    return abi.read_output(case, out, mc)
+
+
+def _save_stats(lib):
+    h, m = C.c_longlong(), C.c_longlong()
+    lib.lmieb_save_cache_stats(C.byref(h), C.byref(m))
+    return h.value, m.value
+
+
+def test_save_control_kernels_stay_on_the_device():
+    """After a save_control 1 solve its kernels stay on the device: a
+    save_control 2 call given the same values (hashed through its row
+    pointers) uploads nothing; changed values are uploaded and kept in their
+    turn.  Every result against the oracle on the same kernels."""
+    lib, orc = libs.product(), libs.oracle()
+    case = all_cases()["save1"]
+    first = libs.run_product(case)
+    assert first.rc == 0
+    s1, s2 = first.save1, first.save2
+    new = dataclasses.replace(case, a2=0.25, save_control=2)
+    h0, m0 = _save_stats(lib)
+    got = _reweight(lib, "lmie", new, s1, s2)
+    assert _save_stats(lib) == (h0 + 1, m0)
+    _assert_parity(got, _reweight(orc, "oracle", new, s1, s2), label="kept kernels")
+    # changed kernels: uploaded, then kept
+    s2b = s2.copy()
+    s2b[1, 3, :] *= 1.5
+    got2 = _reweight(lib, "lmie", new, s1, s2b)
+    assert _save_stats(lib) == (h0 + 1, m0 + 1)
+    _assert_parity(got2, _reweight(orc, "oracle", new, s1, s2b), label="changed kernels")
+    assert not np.array_equal(got2.pf, got.pf)
+    new3 = dataclasses.replace(new, a2=0.3)
+    got3 = _reweight(lib, "lmie", new3, s1, s2b)
+    assert _save_stats(lib) == (h0 + 2, m0 + 1)
+    _assert_parity(got3, _reweight(orc, "oracle", new3, s1, s2b), label="kept changed kernels")
+
+
 def test_invalid_inputs_return_minus_one():
     lib = libs.product()
     assert abi.solve(lib, abi.Case(calc_gc=0, calc_lc=0, calc_pf=1)).rc == -1
