@@ -786,7 +786,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         DevCase &C = cs[k];
         C.mu_user_off = (long long) mu_user.size();
         for (int a = 0; a < C.n_angles; ++a) mu_user.push_back(ps[k].mu_user[a]);
-        pu_start[k + 1] = pu_start[k] + (long long) ncol * C.n_angles;
+        pu_start[k + 1] = pu_start[k] + (long long) ncol * ((C.n_angles + PU_T - 1) / PU_T);   // K5 blocks
         C.scal_off = (int) o_scal;
         o_scal += (size_t) ncol * 4;
         C.gc_off = (long long) o_gc;

@@ -1039,42 +1039,70 @@ __global__ void k_exp_final(DevBatch B, long long total, const long long *__rest
 
 // ---------------------------------------------------------------------------
 // K5: phase matrix at the user's angles from the truncated expansion; one
-// thread per (case, column, user angle).
+// block per (case, column, tile of PU_T user angles), one thread per angle.
+// The expansion coefficients and the recurrence coefficients of PU_T orders
+// at a time are staged in shared memory, which all threads of the block read.
 // ---------------------------------------------------------------------------
 template <int KIND>
-__global__ void k_phase_user(DevBatch B, long long total, const long long *__restrict__ start,
-                             const double *__restrict__ coefs, const int *__restrict__ trunc,
-                             double *__restrict__ out) {
-    const long long e = (long long) blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= total) return;
-    const int c = find_case(start, B.ncase, e);
+__global__ void __launch_bounds__(PU_T) k_phase_user(DevBatch B, const long long *__restrict__ start,
+                                                     const double *__restrict__ coefs,
+                                                     const int *__restrict__ trunc, double *__restrict__ out) {
+    __shared__ double cfs[6][PU_T], rcs[8 * PU_T];
+    const int c = find_case(start, B.ncase, blockIdx.x);
     const DevCase &C = B.cs[c];
-    const long long local = e - start[c];
     const int na = C.n_angles, ncf = C.n_coef;
-    const int col = (int) (local / na), a = (int) (local % na);
+    const int per = (na + PU_T - 1) / PU_T;
+    const int local = (int) (blockIdx.x - start[c]);
+    const int col = local / per, a = (local % per) * PU_T + threadIdx.x;
+    const bool act = a < na;
     const int nt = trunc[c] > 0 ? ncf - trunc[c] + 1 : ncf;
-    const double x = B.mu_user[C.mu_user_off + a];
+    const double x = act ? B.mu_user[C.mu_user_off + a] : 0.;
     const double *cf = coefs + (KIND == 0 ? C.gc_off : C.lc_off) + (size_t) col * 6 * ncf;
     double *o = out + C.pf_out_off + (size_t) col * 6 * na;
     double s0 = 0., s1 = 0., s2 = 0., s3 = 0., s4 = 0., s5 = 0.;
-    if (KIND == 0) {
-        double q[4] = {0., 0., 0., 0.}, p[4] = {0., 0., 0., 0.};
-        for (int l = 0; l < nt; ++l) {
+    double q[4] = {0., 0., 0., 0.}, p[4] = {0., 0., 0., 0.};
+    for (int l0 = 0; l0 < nt; l0 += PU_T) {
+        const int lt = min(PU_T, nt - l0);
+        __syncthreads();
+        for (int t = threadIdx.x; t < 6 * PU_T; t += PU_T) {
+            const int e = t / PU_T, u = t % PU_T;
+            cfs[e][u] = u < lt ? cf[(size_t) e * ncf + l0 + u] : 0.;
+        }
+        for (int t = threadIdx.x; t < 8 * lt; t += PU_T) rcs[t] = B.rc[8 * (size_t) l0 + t];
+        __syncthreads();
+        for (int u = 0; u < lt; ++u) {
+            const int l = l0 + u;
+            const double *rl = rcs + 8 * u;                       // recurrence coefficients of order l
+            if (KIND == 0) {
 #pragma unroll
-            for (int f = 0; f < 4; ++f) {
-                const double v = basis_next<0>(f, l, B.rc, x, p[f], q[f]);
-                q[f] = p[f];
-                p[f] = v;
-            }
-            s0 += cf[l] * p[0];
-            s3 += cf[(size_t) 3 * ncf + l] * p[0];
-            if (l >= 2) {
-                s4 += cf[(size_t) 4 * ncf + l] * p[1];
-                s5 += cf[(size_t) 5 * ncf + l] * p[1];
-                s1 += (cf[(size_t) 1 * ncf + l] + cf[(size_t) 2 * ncf + l]) * p[2];
-                s2 += (cf[(size_t) 1 * ncf + l] - cf[(size_t) 2 * ncf + l]) * p[3];
+                for (int f = 0; f < 4; ++f) {
+                    const double v = l < 3 ? basis_first<0>(f, l, x) : basis_step<0>(f, rl, x, p[f], q[f]);
+                    q[f] = p[f];
+                    p[f] = v;
+                }
+                s0 += cfs[0][u] * p[0];
+                s3 += cfs[3][u] * p[0];
+                if (l >= 2) {
+                    s4 += cfs[4][u] * p[1];
+                    s5 += cfs[5][u] * p[1];
+                    s1 += (cfs[1][u] + cfs[2][u]) * p[2];
+                    s2 += (cfs[1][u] - cfs[2][u]) * p[3];
+                }
+            } else {
+                const double v = l < 2 ? basis_first<1>(0, l, x) : basis_step<1>(0, rl, x, p[0], q[0]);
+                q[0] = p[0];
+                p[0] = v;
+                s0 += cfs[0][u] * v;
+                s1 += cfs[1][u] * v;
+                s2 += cfs[2][u] * v;
+                s3 += cfs[3][u] * v;
+                s4 += cfs[4][u] * v;
+                s5 += cfs[5][u] * v;
             }
         }
+    }
+    if (!act) return;
+    if (KIND == 0) {
         o[a] = s0;
         o[(size_t) 3 * na + a] = s3;
         o[(size_t) 4 * na + a] = s4;
@@ -1082,18 +1110,6 @@ __global__ void k_phase_user(DevBatch B, long long total, const long long *__res
         o[(size_t) 1 * na + a] = (s1 + s2) / 2.;
         o[(size_t) 2 * na + a] = (s1 - s2) / 2.;
     } else {
-        double pm = 0., pc = 0.;
-        for (int l = 0; l < nt; ++l) {
-            const double v = basis_next<1>(0, l, B.rc, x, pc, pm);
-            pm = pc;
-            pc = v;
-            s0 += cf[l] * v;
-            s1 += cf[(size_t) 1 * ncf + l] * v;
-            s2 += cf[(size_t) 2 * ncf + l] * v;
-            s3 += cf[(size_t) 3 * ncf + l] * v;
-            s4 += cf[(size_t) 4 * ncf + l] * v;
-            s5 += cf[(size_t) 5 * ncf + l] * v;
-        }
         o[a] = s0;
         o[(size_t) 1 * na + a] = s1;
         o[(size_t) 2 * na + a] = s2;
@@ -1269,9 +1285,9 @@ int launch_phase_user(cudaStream_t s, const DevBatch &B, int kind, long long tot
                       const double *coefs, const int *trunc, double *pf_out) {
     if (total <= 0) return 0;
     if (kind == 0)
-        k_phase_user<0><<<ceil_div(total, 64), 64, 0, s>>>(B, total, start, coefs, trunc, pf_out);
+        k_phase_user<0><<<(unsigned) total, PU_T, 0, s>>>(B, start, coefs, trunc, pf_out);
     else
-        k_phase_user<1><<<ceil_div(total, 64), 64, 0, s>>>(B, total, start, coefs, trunc, pf_out);
+        k_phase_user<1><<<(unsigned) total, PU_T, 0, s>>>(B, start, coefs, trunc, pf_out);
     LMIEB_CUDA_TRY(cudaGetLastError());
     return 0;
 }
