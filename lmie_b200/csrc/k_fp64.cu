@@ -918,6 +918,9 @@ __global__ void __launch_bounds__(EX_T) k_exp_tile(DevBatch B, const ExpItem *__
     const int l0 = it.lt * EX_LT, lt = min(EX_LT, ncf - l0);
     const int i0 = it.at * EX_AT;
     const double *mup = B.mu_pool + C.mu_off, *wqp = mup + nq;
+    double *rcs = Bv + (size_t) ncol * 12 * EX_AT;         // [8 EX_LT] recurrence coefficients of the tile
+    for (int t = threadIdx.x; t < 8 * lt; t += EX_T) rcs[t] = B.rc[8 * (size_t) l0 + t];
+    __syncthreads();
 
     // basis functions of the tile
     for (int t = threadIdx.x; t < NF * EX_AT; t += EX_T) {
@@ -927,8 +930,10 @@ __global__ void __launch_bounds__(EX_T) k_exp_tile(DevBatch B, const ExpItem *__
             const double x = mup[nh + i];
             const size_t o = (((size_t) it.lt * NF + f) * nh + i) * 2;
             double prev = ckpt[C.ck_off + o], cur = ckpt[C.ck_off + o + 1];
+            constexpr int first = KIND == 1 ? 2 : 3;
             for (int u = 0; u < lt; ++u) {
-                const double v = basis_next<KIND>(f, l0 + u, B.rc, x, cur, prev);
+                const int l = l0 + u;
+                const double v = l < first ? basis_first<KIND>(f, l, x) : basis_step<KIND>(f, rcs + 8 * u, x, cur, prev);
                 prev = cur;
                 cur = v;
                 Pf[u * (EX_AT + 1)] = v;
@@ -1163,7 +1168,8 @@ int run_expand(cudaStream_t s, const DevBatch &B, long long nck, const long long
                double *ckpt, double *exq, double *coefs, int *trunc) {
     constexpr int NF = KIND == 0 ? 4 : 1;
     constexpr int SMAX = 200 * 1024;
-    const size_t sm = sizeof(double) * ((size_t) NF * EX_LT * (EX_AT + 1) + (size_t) (1 + B.nd) * 12 * EX_AT);
+    const size_t sm = sizeof(double) * ((size_t) NF * EX_LT * (EX_AT + 1) + (size_t) (1 + B.nd) * 12 * EX_AT +
+                                        (size_t) 8 * EX_LT);
     if (sm > (size_t) SMAX) {
         fprintf(stderr, "ERROR: expansion tile needs %zu bytes of shared memory (too many derivatives)\n", sm);
         return -1;
