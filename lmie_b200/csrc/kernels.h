@@ -110,7 +110,7 @@ int launch_normalize(cudaStream_t s, const DevBatch &B, long long total, const l
 
 // K4: expansion over Gauss angles.  kind 0: GSF, 1: Legendre.
 constexpr int PU_T = 64;       // user angles per K5 block (and orders staged per step)
-constexpr int EX_LT = 64;       // orders per tile
+constexpr int EX_LT = 32;       // orders per tile
 constexpr int EX_AT = 32;       // half-angles per tile
 struct ExpItem {
     int c, lt, at;              // case, order tile, angle tile
