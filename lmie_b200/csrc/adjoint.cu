@@ -35,6 +35,7 @@
 #include "../../include/lmie_b200.h"
 
 extern "C" int lmieb_calc_n1(double x);
+extern "C" void lmieb_host_parallel(int n, int n_threads, void (*fn)(void *, int), void *arg);
 extern "C" int lmieb_calc_n2(int n1, double zr, double zi);
 extern "C" void lmieb_gauss_leg(int n, double x1, double x2, double *x, double *w);
 
@@ -502,13 +503,22 @@ extern "C" int lmie_solution_adjoint(int n_lambda, const double *lambda, const d
     std::vector<cplx> mm(L);
     off[0] = coff[0] = 0;
     int n1max = 1;
+    // size parameters and truncations, one wavelength per task on the host's threads
+    struct XJob { const double *rad, *lambda, *mr, *mi; double *x; int *n1, *n2; int R; } xj{
+        rad.data(), lambda, mr, mi, x.data(), n1.data(), n2.data(), R};
+    lmieb_host_parallel(L, 64, [](void *arg, int k) {
+        const XJob &j = *(const XJob *) arg;
+        for (int r = 0; r < j.R; ++r) {
+            const size_t t = (size_t) k * j.R + r;
+            j.x[t] = 2. * LMIEB_PI * j.rad[r] / j.lambda[k];
+            j.n1[t] = lmieb_calc_n1(j.x[t]);
+            j.n2[t] = lmieb_calc_n2(j.n1[t], j.mr[k] * j.x[t], -j.mi[k] * j.x[t]);
+        }
+    }, &xj);
     for (int k = 0; k < L; ++k) {
         mm[k] = mk(mr[k], -mi[k]);
         for (int r = 0; r < R; ++r) {
             const size_t t = (size_t) k * R + r;
-            x[t] = 2. * LMIEB_PI * rad[r] / lambda[k];
-            n1[t] = lmieb_calc_n1(x[t]);
-            n2[t] = lmieb_calc_n2(n1[t], mr[k] * x[t], -mi[k] * x[t]);
             n1max = std::max(n1max, n1[t]);
             off[t + 1] = off[t] + n1[t];
             coff[t + 1] = coff[t] + (n1[t] + ADJ_K - 1) / ADJ_K;
@@ -585,7 +595,11 @@ extern "C" int lmie_solution_adjoint(int n_lambda, const double *lambda, const d
         LMIEB_CUDA_TRY(cudaMallocHost((void **) &g_hbuf, in_bytes + out_bytes));
         g_hcap = in_bytes + out_bytes;
     }
-    for (const Piece &p : in) memcpy(g_hbuf + p.at, p.src, p.bytes);
+    struct CopyJob { const Piece *in; char *dst; } cj{in.data(), g_hbuf};
+    lmieb_host_parallel((int) in.size(), 16, [](void *arg, int i) {
+        const CopyJob &j = *(const CopyJob *) arg;
+        memcpy(j.dst + j.in[i].at, j.in[i].src, j.in[i].bytes);
+    }, &cj);
     char *d = g_dbuf;
     auto dp = [&](size_t i) { return (void *) (d + in[i].at); };
     Adj P;
