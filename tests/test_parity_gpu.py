@@ -281,3 +281,22 @@ def test_derivatives_against_central_differences():
         nc = min(up.n_coef, dn.n_coef, got.n_coef)
         fd = (up.gc[:, :nc] - dn.gc[:, :nc]) / (2 * h)
         assert libs.relmax(got.gc_l[d][:, 1:nc], fd[:, 1:]) < 1e-4, p
+
+
+def test_save_control_without_angular_outputs():
+    """save_control 1 and 2 with no expansion or phase matrix requested (only
+    the per-radius cross sections are saved): the kept kernels are save1
+    alone, and the re-weighted cross sections match the oracle."""
+    lib, orc = libs.product(), libs.oracle()
+    case = dataclasses.replace(all_cases()["save1"], calc_gc=0, calc_lc=0, calc_pf=0)
+    first = libs.run_product(case)
+    assert first.rc == 0
+    want_first = libs.run_oracle(case)
+    _assert_parity(first, want_first, label="save_control 1 without angles")
+    s1 = first.save1
+    s2 = np.zeros((4, s1.shape[1], 1))
+    new = dataclasses.replace(case, a2=0.25, save_control=2)
+    h0, m0 = _save_stats(lib)
+    got = _reweight(lib, "lmie", new, s1, s2)
+    assert _save_stats(lib) == (h0 + 1, m0)
+    _assert_parity(got, _reweight(orc, "oracle", new, s1, s2), label="re-weighted without angles")
