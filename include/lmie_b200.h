@@ -50,7 +50,7 @@ int lmie_solution_batch(int n_cases, lmie_in_data *in, lmie_out_data *out, int a
  * lmieb_rerun_device.  Returns 0, or -1 for chunks < 0. */
 int lmieb_set_pipeline(int chunks);
 
-/* Work items per SM the angular stage of `precision` is cut into (default 32
+/* Work items per SM the angular stage of `precision` is cut into (default 64
  * for FP64, 2 for the tensor-core stage); results differ only in the order of
  * partial sums.  Returns 0 or -1. */
 int lmieb_set_work_granularity(int precision, double items_per_sm);
@@ -66,7 +66,7 @@ int lmieb_get_split_segment(void);
 
 /* Autotuner: solves the batch in[0..n_cases) (outputs in out, allocated by
  * the caller or a previous call) repeatedly.  It first picks the angular work
- * granularity (8, 16, 32, 64 items per SM for FP64; 1, 2, 4 for the
+ * granularity (32, 64, 128, 256 items per SM for FP64; 1, 2, 4 for the
  * tensor-core stage) by the device time of the kernels (per-stage CUDA events,
  * one sub-batch), then the pipeline depth (1, 2, 3, 4, 6 parts) by the wall time
  * of the public batch call, and keeps both for later calls

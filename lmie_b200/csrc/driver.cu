@@ -120,7 +120,7 @@ Ctx g_ctx;
 // Work items per SM the angular stage is cut into ([0] FP64 kernel, [1]
 // tensor-core kernel): finer items balance uneven cases, coarser ones cut the
 // per-item overhead; set by lmieb_set_work_granularity (the autotuner).
-double g_items_per_sm[2] = {32., 2.};
+double g_items_per_sm[2] = {64., 2.};
 
 // Orders (in chunks of TC_KC) per FP32 segment of the tensor-core stage's
 // hi*hi products; set by lmieb_set_split_segment.
@@ -1525,7 +1525,7 @@ extern "C" int lmieb_last_host_timing(double *ms, int n) {
 extern "C" int lmieb_set_work_granularity(int precision, double items_per_sm) {
     std::lock_guard<std::mutex> lock(g_mu);
     if ((precision != LMIEB_PRECISION_FP64 && precision != LMIEB_PRECISION_TF32X3) || !(items_per_sm >= 0.25) ||
-        items_per_sm > 64.) {
+        items_per_sm > 256.) {
         fprintf(stderr, "ERROR: lmieb_set_work_granularity: precision %d, items per SM %g\n", precision, items_per_sm);
         return -1;
     }

@@ -880,7 +880,7 @@ int lmie_solution_batch2(int n_cases, lmie_in_data *in, lmie_out_data *out, int 
 int lmie_solution_autotune(int n_cases, lmie_in_data *in, lmie_out_data *out, int n_threads, int precision,
                            int *best_chunks, double *best_items, double *best_ms) {
      static const int chunk_c[] = {1, 2, 3, 4, 6};
-     static const double items_fp64[] = {8., 16., 32., 64.}, items_tc[] = {1., 2., 4.};
+     static const double items_fp64[] = {32., 64., 128., 256.}, items_tc[] = {1., 2., 4.};
      const double *items = precision == LMIEB_PRECISION_TF32X3 ? items_tc : items_fp64;
      const int n_items = precision == LMIEB_PRECISION_TF32X3 ? 3 : 4;
      const int keep = g_pipeline, keep_timing = lmieb_timing_state();

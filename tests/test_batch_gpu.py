@@ -121,7 +121,7 @@ def test_autotune_picks_a_candidate_and_keeps_results():
     try:
         got = b.autotune(4, abi.PRECISION_FP64)
         assert got["pipeline_parts"] in (1, 2, 3, 4, 6)
-        assert got["angular_items_per_sm"] in (8.0, 16.0, 32.0, 64.0)
+        assert got["angular_items_per_sm"] in (32.0, 64.0, 128.0, 256.0)
         assert got["ms_per_call"] > 0
         after = abi.solve_batch(lib, cases, n_threads=4)
         for i, (a, r) in enumerate(zip(after, ref)):
