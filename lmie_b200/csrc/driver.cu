@@ -167,7 +167,7 @@ extern "C" void lmieb_host_parallel(int n, int n_threads, void (*fn)(void *, int
 
 // memcpy of a large block on several host threads
 void par_memcpy(void *dst, const void *src, size_t bytes) {
-    constexpr size_t chunk = (size_t) 4 << 20;
+    const size_t chunk = std::max((size_t) 256 << 10, (bytes / 16 + 4095) & ~(size_t) 4095);
     const int n = (int) ((bytes + chunk - 1) / chunk);
     parallel_for(n, 1, [&](int i) {
         const size_t a = (size_t) i * chunk, b = std::min(bytes, a + chunk);
@@ -755,7 +755,8 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     const long long ctot = coff[R];
 
     // ---- expansion work items and offsets ----
-    std::vector<ExpItem> ex;
+    static std::vector<ExpItem> ex;          // kept between calls, like the per-radius arrays
+    ex.clear();
     std::vector<long long> ck_gc(ncase + 1, 0), ck_lc(ncase + 1, 0), fin_start(ncase + 1, 0);
     long long ck_total = 0, ex_total = 0;
     for (int k = 0; k < ncase; ++k) {
@@ -779,13 +780,23 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     L.n_ex = (int) ex.size();
 
     // ---- user angles and output offsets ----
+    // the user angles depend only on their number: one copy per distinct count
     std::vector<long long> pu_start(ncase + 1, 0);
     std::vector<double> mu_user;
+    std::unordered_map<int, long long> mu_at;
     size_t o_scal = 0, o_gc = 0, o_lc = 0, o_pf = 0;
     for (int k = 0; k < ncase; ++k) {
         DevCase &C = cs[k];
-        C.mu_user_off = (long long) mu_user.size();
-        for (int a = 0; a < C.n_angles; ++a) mu_user.push_back(ps[k].mu_user[a]);
+        if (C.n_angles > 0) {
+            const auto hit = mu_at.find(C.n_angles);
+            if (hit != mu_at.end()) {
+                C.mu_user_off = hit->second;
+            } else {
+                C.mu_user_off = (long long) mu_user.size();
+                mu_at[C.n_angles] = C.mu_user_off;
+                mu_user.insert(mu_user.end(), ps[k].mu_user, ps[k].mu_user + C.n_angles);
+            }
+        }
         pu_start[k + 1] = pu_start[k] + (long long) ncol * ((C.n_angles + PU_T - 1) / PU_T);   // K5 blocks
         C.scal_off = (int) o_scal;
         o_scal += (size_t) ncol * 4;
