@@ -49,7 +49,9 @@ typedef struct {
      int want_gc, want_lc;      /* expansions requested (reference: gc/lc pointers non-NULL) */
      int pf_from;               /* 0: no phase matrix, 1: from gc, 2: from lc */
      int n_angles;
-     const double *mu_user;     /* [n_angles] cos(theta_i) */
+     const double *mu_user;     /* [n_angles] cos(theta_i), theta_i = i 180/(n_angles-1) degrees:
+                                   a function of n_angles alone, so the device layer keeps
+                                   one copy per distinct count */
      double accuracy;
 
      int save_control;          /* 0, 1 or 2 */
