@@ -1,8 +1,9 @@
 /*
  * lmie_b200.h -- entry points of liblmie_b200.so beyond the reference's
- * interface (include/lmie_interface.h).  None of these has a counterpart in
- * the reference; they expose device timing and device-resident re-runs for
- * benchmarking, and device information.
+ * interface (include/lmie_interface.h): batched and split-precision solves,
+ * the adjoint, tuning, radius sharing over a group of GPUs (the reference's
+ * use_mpi), device timing and device-resident re-runs for benchmarking, and
+ * device information.
  */
 #ifndef LMIE_B200_H
 #define LMIE_B200_H
@@ -227,6 +228,57 @@ int lmieb_fp64_peak(double *tflops);
  * the results are in `out`.  Returns 0 or -1. */
 int lmie_cross_sections_noalloc(int n_radii, const double *radius, double lambda,
                                 double mr, double mi, double *out, void *stream);
+
+/* ---- radius sharing over processes, one per GPU ----------------------------
+ * Replaces the reference's MPI build of lmie_solution(..., use_mpi = 1), which
+ * deals the radii of one solve out to worker ranks round-robin and adds up
+ * their cross sections and phase-matrix integrals on the master
+ * (src/lmie_schedule.c:459-921, lmie_core_master / lmie_core_slave).  Here
+ * every process of a group drives its own GPU: process `rank` of `world`
+ * solves the radii i with i % world == rank (i in quadrature order), the
+ * group sums the integrals -- 4 (1 + n_derivs) (1 + n_qang) doubles, with
+ * n_qang = 0 without calc_gc and calc_lc, else lmie_calc_max_coef() -- and
+ * every process then finishes the solve (normalisation, expansions, phase
+ * matrix) and returns the whole result.  Every process of the group must make
+ * the same calls with the same inputs.  save_control must be 0. */
+
+/* In-place sum over the group of the `count` doubles at DEVICE address buf,
+ * which this process's solve has just written on `stream` (a cudaStream_t,
+ * already synchronised when the function is called).  The sum must be
+ * complete when the function returns; 0 means success. */
+typedef int (*lmieb_reduce_fn)(double *buf, long long count, void *stream, void *ctx);
+
+/* From this call on, lmie_solution() and lmie_solution2*() called with
+ * use_mpi != 0 share their radii with the group (rank, world), summing with
+ * reduce(buf, count, stream, ctx); use_mpi = 0 keeps the whole solve on this
+ * GPU.  world 1 with reduce NULL ends the sharing.  Returns 0 or -1. */
+int lmieb_set_radius_group(int rank, int world, lmieb_reduce_fn reduce, void *ctx);
+
+/* The same with the library's own NCCL all-reduce (FP64 sum over NVLink /
+ * NVSwitch), queued on the solve's stream between the integrals and the
+ * normalisation with no host synchronisation.  `id` is the 128-byte
+ * ncclUniqueId that one process of the group got from lmieb_nccl_unique_id()
+ * and sent to the others (over MPI, a file, a TCP store).  NCCL is loaded at
+ * run time (libnccl.so.2: the one already in the process, else the system's).
+ * Collective over the group.  Returns 0 or -1. */
+int lmieb_nccl_unique_id(void *id);
+int lmieb_set_radius_group_nccl(const void *id, int rank, int world);
+
+/* The group in use: *rank and *world (0 and 1 when none); returns 1 when
+ * use_mpi calls share their radii, else 0. */
+int lmieb_get_radius_group(int *rank, int *world);
+
+/* Two-call form for callers that sum on the host themselves (an
+ * MPI_Allreduce of doubles, say).  lmieb_partial_size() is the number of
+ * doubles of the integrals of `in`; lmieb_solution_partial() solves the radii
+ * i % world == rank of `in` and writes their integrals to acc; after the
+ * caller has summed acc over ranks 0..world-1, lmieb_solution_finish() fills
+ * `out` as lmie_solution(in, out, alloc_out, verbose, 0, 0) would.  Return
+ * -1 (size) or 0 / -1. */
+long long lmieb_partial_size(const lmie_in_data *in);
+int lmieb_solution_partial(lmie_in_data *in, int rank, int world, double *acc, int verbose);
+int lmieb_solution_finish(lmie_in_data *in, lmie_out_data *out, int alloc_out, const double *acc,
+                          int verbose);
 
 /* Name, SM count and compute capability of the device the library uses. */
 int lmieb_device_info(char *name, int len, int *sms, int *cc_major, int *cc_minor);

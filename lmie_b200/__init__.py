@@ -44,6 +44,7 @@ def library() -> C.CDLL:
         lib.lmieb_set_split_segment.argtypes = [C.c_int]
         lib.lmieb_save_cache_stats.argtypes = [C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
         lib.lmieb_get_split_segment.argtypes = []
+        abi.bind_group(lib)
         _lib = lib
     return _lib
 

@@ -21,6 +21,9 @@ PD = C.POINTER(C.c_double)
 PPD = C.POINTER(PD)
 PPPD = C.POINTER(PPD)
 
+# lmieb_reduce_fn (include/lmie_b200.h): int (*)(double *buf, long long count, void *stream, void *ctx)
+REDUCE_FN = C.CFUNCTYPE(C.c_int, PD, C.c_longlong, C.c_void_p, C.c_void_p)
+
 # enum size_dist_type (reference misc/rtutil_size_dist.h:22-34); order is ABI.
 SIZE_DIST = {
     "none": 0,
@@ -215,11 +218,13 @@ def n_qsize(case: Case) -> int:
     return case.n_int2 * case.n_quad
 
 
-def solve(lib: C.CDLL, case: Case, n_threads: int = 1, kind: str = "lmie") -> Result:
+def solve(lib: C.CDLL, case: Case, n_threads: int = 1, kind: str = "lmie", use_mpi: int = 0) -> Result:
     """Run one case through `lib` and copy every output into numpy arrays.
 
     kind "lmie": the library exports lmie_solution/lmie_out_free (the product
     and the reference); kind "oracle": oracle_solution/oracle_out_free.
+    use_mpi is lmie_solution's last argument (radius sharing with the
+    library's registered group).
     """
     blk = InputBlock(case)
     out = lmie_out_data()
@@ -232,7 +237,7 @@ def solve(lib: C.CDLL, case: Case, n_threads: int = 1, kind: str = "lmie") -> Re
     else:
         max_coef = lib.lmie_calc_max_coef(case.lam, blk.s.dist_type, case.a1, case.a2,
                                           case.a3, case.r1, case.r2)
-        rc = lib.lmie_solution(C.byref(blk.s), C.byref(out), 1, 0, n_threads, 0)
+        rc = lib.lmie_solution(C.byref(blk.s), C.byref(out), 1, 0, n_threads, use_mpi)
     if rc != 0:
         return Result(rc=rc)
     nq = n_qsize(case)
@@ -246,6 +251,59 @@ def solve(lib: C.CDLL, case: Case, n_threads: int = 1, kind: str = "lmie") -> Re
         lib.oracle_out_free(C.byref(out), 1 if case.n_derivs > 0 else 0)
     else:
         lib.lmie_out_free(C.byref(out), 1 if case.n_derivs > 0 else 0)
+    return res
+
+
+def _bind_share(lib: C.CDLL) -> None:
+    lib.lmieb_partial_size.restype = C.c_longlong
+    lib.lmieb_partial_size.argtypes = [C.POINTER(lmie_in_data)]
+    lib.lmieb_solution_partial.restype = C.c_int
+    lib.lmieb_solution_partial.argtypes = [C.POINTER(lmie_in_data), C.c_int, C.c_int, PD, C.c_int]
+    lib.lmieb_solution_finish.restype = C.c_int
+    lib.lmieb_solution_finish.argtypes = [C.POINTER(lmie_in_data), C.POINTER(lmie_out_data), C.c_int, PD,
+                                          C.c_int]
+
+
+def bind_group(lib: C.CDLL) -> None:
+    """Declares the radius-sharing entry points of include/lmie_b200.h."""
+    _bind_share(lib)
+    lib.lmieb_set_radius_group.restype = C.c_int
+    lib.lmieb_set_radius_group.argtypes = [C.c_int, C.c_int, REDUCE_FN, C.c_void_p]
+    lib.lmieb_nccl_unique_id.restype = C.c_int
+    lib.lmieb_nccl_unique_id.argtypes = [C.c_void_p]
+    lib.lmieb_set_radius_group_nccl.restype = C.c_int
+    lib.lmieb_set_radius_group_nccl.argtypes = [C.c_void_p, C.c_int, C.c_int]
+    lib.lmieb_get_radius_group.restype = C.c_int
+    lib.lmieb_get_radius_group.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int)]
+
+
+def solve_partial(lib: C.CDLL, case: Case, rank: int, world: int) -> np.ndarray:
+    """lmieb_solution_partial(): the integrals of the radii i % world == rank
+    of `case` (lmieb_partial_size() doubles, before normalisation)."""
+    _bind_share(lib)
+    blk = InputBlock(case)
+    acc = np.zeros(lib.lmieb_partial_size(C.byref(blk.s)), dtype=np.float64)
+    rc = lib.lmieb_solution_partial(C.byref(blk.s), rank, world, acc.ctypes.data_as(PD), 0)
+    if rc != 0:
+        raise RuntimeError(f"lmieb_solution_partial failed ({rc})")
+    return acc
+
+
+def solve_finish(lib: C.CDLL, case: Case, acc: np.ndarray) -> Result:
+    """lmieb_solution_finish(): the solve of `case` from the integrals summed
+    over all ranks."""
+    _bind_share(lib)
+    blk = InputBlock(case)
+    acc = np.ascontiguousarray(acc, dtype=np.float64)
+    if acc.size != lib.lmieb_partial_size(C.byref(blk.s)):
+        raise ValueError("acc has the wrong size for this case")
+    out = lmie_out_data()
+    max_coef = lib.lmie_calc_max_coef(case.lam, blk.s.dist_type, case.a1, case.a2, case.a3, case.r1, case.r2)
+    rc = lib.lmieb_solution_finish(C.byref(blk.s), C.byref(out), 1, acc.ctypes.data_as(PD), 0)
+    if rc != 0:
+        return Result(rc=rc)
+    res = read_output(case, out, max_coef)
+    lib.lmie_out_free(C.byref(out), 1 if case.n_derivs > 0 else 0)
     return res
 
 

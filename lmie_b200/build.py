@@ -38,7 +38,8 @@ def exported_symbols():
     names = []
     for h in sorted(INCLUDE.glob("*.h")):
         text = re.sub(r"/\*.*?\*/", " ", h.read_text(), flags=re.S)
-        for m in re.finditer(r"^[A-Za-z_][\w \*]*?\b([A-Za-z_]\w*)\s*\(", text, flags=re.M):
+        # (typedefs of function pointers declare no function)
+        for m in re.finditer(r"^(?!typedef\b)[A-Za-z_][\w \*]*?\b([A-Za-z_]\w*)\s*\(", text, flags=re.M):
             name = m.group(1)
             if name not in ("if", "while", "for", "return", "sizeof") and name not in names:
                 names.append(name)

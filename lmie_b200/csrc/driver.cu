@@ -20,6 +20,7 @@
 #include <unordered_map>
 #include <vector>
 
+#include <dlfcn.h>
 #include <unistd.h>
 
 #include "host_pool.h"
@@ -53,6 +54,9 @@ struct Pending {
     double *o_scal = nullptr, *o_gc = nullptr, *o_lc = nullptr, *o_pf = nullptr;
     double *o_save1 = nullptr, *o_save2 = nullptr;
     int *o_trunc = nullptr;
+    int acc_mode = 0;
+    double *o_acc = nullptr;           // LMIEB_ACC_PARTIAL: the integrals
+    size_t acc_n = 0;
     double t_submit = 0.;
 };
 
@@ -125,6 +129,28 @@ double g_items_per_sm[2] = {64., 2.};
 // Orders (in chunks of TC_KC) per FP32 segment of the tensor-core stage's
 // hi*hi products; set by lmieb_set_split_segment.
 int g_tc_seg = 2;
+
+// Radius sharing: the group lmie_solution(..., use_mpi != 0) shares its radii
+// with, and how the integrals are summed over it -- the caller's function, or
+// an NCCL all-reduce queued on the solve's stream.
+struct NcclUniqueId { char internal[128]; };    // ncclUniqueId
+struct Nccl {
+    void *lib = nullptr;
+    int (*get_unique_id)(NcclUniqueId *) = nullptr;
+    int (*comm_init_rank)(void **, int, NcclUniqueId, int) = nullptr;
+    int (*all_reduce)(const void *, void *, size_t, int, int, void *, cudaStream_t) = nullptr;
+    int (*comm_destroy)(void *) = nullptr;
+    const char *(*error_string)(int) = nullptr;
+};
+constexpr int NCCL_FLOAT64 = 8, NCCL_SUM = 0;   // ncclFloat64, ncclSum
+struct RadiusGroup {
+    int rank = 0, world = 1;
+    lmieb_reduce_fn fn = nullptr;
+    void *fn_ctx = nullptr;
+    void *comm = nullptr;                       // ncclComm_t of the built-in reduction
+    bool on = false;
+} g_group;
+Nccl g_nccl;
 
 // fn(i) for every i in [0, n) on the host's cores (dynamic chunks of `grain`)
 template <class F>
@@ -243,6 +269,10 @@ struct Plan {
     double *o_scal = nullptr, *o_gc = nullptr, *o_lc = nullptr, *o_pf = nullptr;
     int *o_trunc = nullptr;     // [2][ncase]: gc, lc
     double *o_save1 = nullptr, *o_save2 = nullptr;
+    int acc_mode = 0;           // LMIEB_ACC_* (radius sharing)
+    bool no_radii = false;      // this share has no radii: its integrals are zero
+    size_t acc_n = 0;           // doubles of sums + pfacc, one block
+    double *o_acc = nullptr;
     long long launches = 0;
 };
 
@@ -344,10 +374,17 @@ inline void stage(int i) {
     if (g_ctx.timing) cudaEventRecord(g_ctx.ev[i], g_ctx.stream);
 }
 
-// The kernel sequence of one sub-batch on resident inputs (stages 1..7).
-int run_kernels(Plan &L, cudaStream_t s) {
+// Stages 1..3 of a sub-batch: the radius integrals (sums, pfacc).
+int run_accumulate(Plan &L, cudaStream_t s) {
     const DevBatch &B = L.B;
     stage(1);
+    if (L.acc_mode == LMIEB_ACC_FINISH || L.no_radii) {
+        // summed integrals uploaded with the inputs, or none on this share
+        if (L.no_radii) LMIEB_CUDA_TRY(cudaMemsetAsync(L.sums, 0, L.acc_n * sizeof(double), s));
+        stage(2);
+        stage(3);
+        return 0;
+    }
     if (L.save_control != 2) {
         for (int ch = 0; ch < (L.nd1c > 0 ? L.nd1c : 1); ++ch) {
             const int c0 = ch * 4;
@@ -378,6 +415,12 @@ int run_kernels(Plan &L, cudaStream_t s) {
         if (launch_save_reweight(s, B, L.n_qang0, L.save1_in, L.save2_in, L.w2, L.sums, L.pfacc)) return -1;
         stage(3);
     }
+    return 0;
+}
+
+// Stages 4..7: normalisation, expansions, phase matrix at the user angles.
+int run_finish(Plan &L, cudaStream_t s) {
+    const DevBatch &B = L.B;
     stage(4);
     if (launch_normalize(s, B, L.pf_total, L.pf_start, L.sums, L.pfacc, L.o_scal, L.pfn)) return -1;
     LMIEB_CUDA_TRY(cudaMemsetAsync(L.o_trunc, 0, sizeof(int) * 2 * L.ncase, s));
@@ -396,6 +439,32 @@ int run_kernels(Plan &L, cudaStream_t s) {
         if (launch_phase_user(s, B, L.pf_from == 1 ? 0 : 1, L.pu_total, L.pu_start, cf, tr, L.o_pf)) return -1;
     }
     stage(8);
+    return 0;
+}
+
+// The kernel sequence of one sub-batch on resident inputs (stages 1..7).
+int run_kernels(Plan &L, cudaStream_t s) {
+    return run_accumulate(L, s) || run_finish(L, s) ? -1 : 0;
+}
+
+// Sums the integrals of a LMIEB_ACC_GROUP sub-batch over the radius group,
+// on stream s between run_accumulate and run_finish.
+int reduce_group(Plan &L, cudaStream_t s) {
+    const RadiusGroup &g = g_group;
+    if (g.comm) {
+        const int r = g_nccl.all_reduce(L.sums, L.sums, L.acc_n, NCCL_FLOAT64, NCCL_SUM, g.comm, s);
+        if (r != 0) {
+            fprintf(stderr, "ERROR: lmie_b200: ncclAllReduce: %s\n", g_nccl.error_string(r));
+            return -1;
+        }
+        return 0;
+    }
+    if (!g.fn) return 0;
+    LMIEB_CUDA_TRY(cudaStreamSynchronize(s));
+    if (g.fn(L.sums, (long long) L.acc_n, (void *) s, g.fn_ctx) != 0) {
+        fprintf(stderr, "ERROR: lmie_b200: the radius group's reduction failed\n");
+        return -1;
+    }
     return 0;
 }
 
@@ -460,6 +529,11 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     L.n_qang0 = p0.n_qang;
     L.nd1c = (nd1 + 3) / 4;
     L.n_ang_launch = std::max(1, std::max((nd1 + 3) / 4, (nd2 + 3) / 4));
+    L.acc_mode = p0.acc_mode;
+    if (L.acc_mode != LMIEB_ACC_WHOLE && (ncase != 1 || L.save_control != 0)) {
+        fprintf(stderr, "ERROR: lmie_b200: radius sharing needs a single case with save_control 0\n");
+        return -1;
+    }
 
     // ---- case table and batch-wide per-radius arrays (filled per case in parallel) ----
     std::vector<DevCase> cs(ncase);
@@ -491,6 +565,11 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         n1max = std::max(n1max, cn1max[k]);
     }
     const int R = cr0[ncase];
+    L.no_radii = R == 0 && (L.acc_mode == LMIEB_ACC_PARTIAL || L.acc_mode == LMIEB_ACC_GROUP);
+    if (R == 0 && L.acc_mode == LMIEB_ACC_WHOLE) {
+        fprintf(stderr, "ERROR: lmie_b200: a case without radii\n");
+        return -1;
+    }
     // per-radius arrays: every element is written below; kept between calls
     // (calls are serialised) so that their pages are not faulted in and
     // zeroed again for every sub-batch
@@ -614,8 +693,8 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     // ---- angular work items (largest first), partial and pf offsets ----
     bool any_ang = false;
     for (int k = 0; k < ncase; ++k) any_ang |= cs[k].n_qang > 0;
-    L.tc = p0.precision == LMIEB_PRECISION_TF32X3 && L.save_control == 0 && any_ang && nd1 <= TC_MAX_NC1 &&
-           nd2 <= TC_MAX_ND2;
+    L.tc = p0.precision == LMIEB_PRECISION_TF32X3 && L.save_control == 0 && any_ang && R > 0 &&
+           nd1 <= TC_MAX_NC1 && nd2 <= TC_MAX_ND2;
     L.tc_seg = g_tc_seg;
     // with split precision, cases below TC_MIN_N1 orders keep the FP64 K3: their
     // linearised phase matrices cancel strongly on normalisation, and they cost little
@@ -812,7 +891,11 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     // ---- launches per device run and algorithmic work ----
     {
         long long nl = 0;
-        if (L.save_control != 2) {
+        const bool solve = L.acc_mode != LMIEB_ACC_FINISH && !L.no_radii;
+        const bool finish = L.acc_mode != LMIEB_ACC_PARTIAL;
+        if (!solve) {
+            // integrals uploaded (or zero on an empty share)
+        } else if (L.save_control != 2) {
             nl += (long long) std::max(L.nd1c, 1) + 1;                          // K1 per chunk, K2
             if (L.tc) nl += (L.n_ang > 0) + (L.n_ang64 > 0 ? L.n_ang_launch : 0);   // K3
             else nl += L.n_ang > 0 ? L.n_ang_launch : 0;
@@ -820,10 +903,12 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         } else {
             nl += 1 + (L.n_qang0 > 0);
         }
-        nl += 1 + (L.pf_total > 0);                                              // normalisation
-        if (L.want_gc && L.n_ex > 0) nl += 3;
-        if (L.want_lc && L.n_ex > 0) nl += 3;
-        if (L.pf_from && L.pu_total > 0) nl += 1;
+        if (finish) {
+            nl += 1 + (L.pf_total > 0);                                          // normalisation
+            if (L.want_gc && L.n_ex > 0) nl += 3;
+            if (L.want_lc && L.n_ex > 0) nl += 3;
+            if (L.pf_from && L.pu_total > 0) nl += 1;
+        }
         L.launches = nl;
         double fang = 0., frec = 0., fgsf = 0., fexp = 0.;
         for (int k = 0; k < ncase; ++k) {
@@ -834,7 +919,8 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
             fgsf += 12. * C.n_coef * C.n_qang * ncol * ((L.want_gc ? 1 : 0) + (L.want_lc ? 1 : 0));
             fexp += 12. * C.n_angles * C.n_coef * ncol;
         }
-        if (L.save_control == 2) fang = frec = 0.;
+        if (L.save_control == 2 || !solve) fang = frec = 0.;
+        if (!finish) fgsf = fexp = 0.;
         c.work[0] += fang;
         c.work[1] += frec;
         c.work[2] += fgsf;
@@ -843,6 +929,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     }
 
     // ---- host staging: inputs then outputs ----
+    L.acc_n = (size_t) ncase * ncol * 4 + (size_t) L.pf_total;   // sums, then pfacc
     const size_t n_save2 = (size_t) 4 * R * std::max(L.n_qang0, 1);
     // save_control 2: the caller's kernels, unless the device still holds them
     const int save_nq = p0.save2_rows ? L.n_qang0 : 0;
@@ -875,12 +962,14 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
             if (!save_hit) { add((size_t) 4 * R * 8); add(n_save2 * 8); }
             add((size_t) std::max(nd, 1) * R * 8);
         }
+        if (L.acc_mode == LMIEB_ACC_FINISH) add((size_t) L.acc_n * 8);
     }
     size_t out_bytes = 0;
     {
         auto add = [&](size_t b) { out_bytes += pad(b); };
         add(o_scal * 8); add(o_gc * 8); add(o_lc * 8); add(o_pf * 8); add((size_t) (2 * ncase + 1) * 4);
         if (L.save_control == 1) { add((size_t) 4 * R * 8); add(n_save2 * 8); }
+        if (L.acc_mode == LMIEB_ACC_PARTIAL) add(L.acc_n * 8);
     }
     if (ensure_host(S, in_bytes + out_bytes)) return -1;
     char *hp = S.hbuf;
@@ -937,6 +1026,8 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         }
         h_w2 = put(hp, ho, p0.w2, (size_t) std::max(nd, 1) * R);
     }
+    double *h_acc = nullptr;
+    if (L.acc_mode == LMIEB_ACC_FINISH) h_acc = put(hp, ho, p0.acc_in, L.acc_n);
     const size_t h_in_end = ho;
     if (h_in_end > in_bytes) {
         fprintf(stderr, "ERROR: lmie_b200: staging layout mismatch\n");
@@ -948,15 +1039,14 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     size_t dev_bytes = in_bytes + out_bytes + 64 * 256;
     {
         auto add = [&](size_t b) { dev_bytes += pad(b); };
-        if (L.save_control != 2) {
+        if (L.save_control != 2 && L.acc_mode != LMIEB_ACC_FINISH) {
             add((size_t) ckn * 8 * k1_ck_width(std::min(nd1, 4)));
             if (L.tc) add((size_t) bop_floats * 4);
             add((size_t) (1 + nd1) * (size_t) ctot * 32);
             add((size_t) (1 + nd1) * 5 * (size_t) R * 8);
             add((size_t) part_total * 8);
         }
-        add((size_t) ncase * ncol * 4 * 8);
-        add((size_t) L.pf_total * 8);
+        add(L.acc_n * 8);                                        // sums + pfacc
         add((size_t) L.pf_total * 8);
         add((size_t) ck_total * 8);
         add((size_t) ex_total * 8);
@@ -1017,7 +1107,8 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         L.save2_in = save_hit ? c.save.d + (size_t) 4 * R : (double *) dptr(h_s2);
         L.w2 = (double *) dptr(h_w2);
     }
-    if (L.save_control != 2) {
+    const bool solve = L.save_control != 2 && L.acc_mode != LMIEB_ACC_FINISH;
+    if (solve) {
         L.ck = A.take<double>((size_t) ckn * k1_ck_width(std::min(nd1, 4)));
         if (L.tc) {
             L.bop_bytes = (size_t) bop_floats * 4;
@@ -1027,8 +1118,9 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         L.rs = A.take<double>((size_t) (1 + nd1) * 5 * (size_t) R);
         L.part = A.take<double>((size_t) part_total);
     }
-    L.sums = A.take<double>((size_t) ncase * ncol * 4);
-    L.pfacc = A.take<double>((size_t) L.pf_total);
+    // the integrals in one block, so that a radius group sums them in one call
+    L.sums = L.acc_mode == LMIEB_ACC_FINISH ? (double *) dptr(h_acc) : A.take<double>(L.acc_n);
+    L.pfacc = L.sums ? L.sums + (size_t) ncase * ncol * 4 : nullptr;
     L.pfn = A.take<double>((size_t) L.pf_total);
     L.ckpt = A.take<double>((size_t) ck_total);
     L.exq = A.take<double>((size_t) ex_total);
@@ -1044,8 +1136,9 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
             L.o_save1 = (double *) take((size_t) 4 * R * 8);
             L.o_save2 = (double *) take(n_save2 * 8);
         }
+        if (L.acc_mode == LMIEB_ACC_PARTIAL) L.o_acc = (double *) take(L.acc_n * 8);
     }
-    if (!L.sums || !L.pfn || !L.exq || (L.save_control != 2 && !L.part) || (L.tc && !L.bop)) {
+    if (!L.sums || !L.pfn || !L.exq || (solve && !L.part) || (L.tc && !L.bop)) {
         fprintf(stderr, "ERROR: lmie_b200: device arena too small\n");
         return -1;
     }
@@ -1090,7 +1183,15 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         LMIEB_CUDA_TRY(cudaEventRecord(c.gl_ready, s));
         c.gl_pending = true;
     }
-    if (run_kernels(L, s)) return -1;
+    if (run_accumulate(L, s)) return -1;
+    if (L.acc_mode == LMIEB_ACC_PARTIAL) {
+        // this share's integrals are the result
+        LMIEB_CUDA_TRY(cudaMemcpyAsync(L.o_acc, L.sums, L.acc_n * 8, cudaMemcpyDeviceToDevice, s));
+        for (int i = 4; i < NSTAGE; ++i) stage(i);
+    } else {
+        if (L.acc_mode == LMIEB_ACC_GROUP && reduce_group(L, s)) return -1;
+        if (run_finish(L, s)) return -1;
+    }
     if (L.save_control == 1) {
         // the kernels this solve saves: kept on the device as well, recognised
         // once their hash is known (when the sub-batch is collected)
@@ -1135,6 +1236,9 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     P.o_save1 = L.o_save1;
     P.o_save2 = L.o_save2;
     P.o_trunc = L.o_trunc;
+    P.acc_mode = L.acc_mode;
+    P.o_acc = L.o_acc;
+    P.acc_n = L.acc_n;
     P.t_submit = now_ms();
     return 0;
 }
@@ -1201,6 +1305,8 @@ int collect_slot(Slot &S) {
         c.save.nq = nq;
         c.save.valid = true;
     }
+    if (P.acc_mode == LMIEB_ACC_PARTIAL && P.rs[0].acc)
+        memcpy(P.rs[0].acc, hostp(P.o_acc), P.acc_n * 8);
     if (P.save_control == 1) {
         lmieb_result &r = P.rs[0];
         if (r.save1) memcpy(r.save1, hostp(P.o_save1), (size_t) 4 * P.R * 8);
@@ -1359,6 +1465,108 @@ extern "C" int lmieb_save_cache_stats(long long *hits, long long *misses) {
     return 0;
 }
 
+namespace {
+
+// Loads NCCL (the libnccl.so.2 already in the process, or the system's) and
+// resolves the entry points of the built-in group reduction.
+int nccl_load() {
+    Nccl &n = g_nccl;
+    if (n.lib) return 0;
+    void *lib = dlopen("libnccl.so.2", RTLD_NOW | RTLD_LOCAL);
+    if (!lib) {
+        fprintf(stderr, "ERROR: lmie_b200: cannot load NCCL (%s)\n", dlerror());
+        return -1;
+    }
+    Nccl t;
+    t.get_unique_id = (decltype(t.get_unique_id)) dlsym(lib, "ncclGetUniqueId");
+    t.comm_init_rank = (decltype(t.comm_init_rank)) dlsym(lib, "ncclCommInitRank");
+    t.all_reduce = (decltype(t.all_reduce)) dlsym(lib, "ncclAllReduce");
+    t.comm_destroy = (decltype(t.comm_destroy)) dlsym(lib, "ncclCommDestroy");
+    t.error_string = (decltype(t.error_string)) dlsym(lib, "ncclGetErrorString");
+    if (!t.get_unique_id || !t.comm_init_rank || !t.all_reduce || !t.comm_destroy || !t.error_string) {
+        fprintf(stderr, "ERROR: lmie_b200: libnccl.so.2 lacks an entry point\n");
+        dlclose(lib);
+        return -1;
+    }
+    t.lib = lib;
+    n = t;
+    return 0;
+}
+
+// Ends the current radius group (and its NCCL communicator).
+void group_release() {
+    if (g_group.comm) {
+        cudaDeviceSynchronize();                 // no solve may still use it
+        g_nccl.comm_destroy(g_group.comm);
+    }
+    g_group = RadiusGroup();
+}
+
+}  // namespace
+
+extern "C" int lmieb_set_radius_group(int rank, int world, lmieb_reduce_fn reduce, void *ctx) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    if (world < 1 || rank < 0 || rank >= world || (world > 1 && !reduce)) {
+        fprintf(stderr, "ERROR: lmieb_set_radius_group: rank %d of %d%s\n", rank, world,
+                world > 1 && !reduce ? " without a reduction" : "");
+        return -1;
+    }
+    group_release();
+    g_group.rank = rank;
+    g_group.world = world;
+    g_group.fn = reduce;
+    g_group.fn_ctx = ctx;
+    g_group.on = reduce != nullptr;
+    return 0;
+}
+
+extern "C" int lmieb_nccl_unique_id(void *id) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    if (!id || nccl_load()) return -1;
+    NcclUniqueId u;
+    const int r = g_nccl.get_unique_id(&u);
+    if (r != 0) {
+        fprintf(stderr, "ERROR: lmie_b200: ncclGetUniqueId: %s\n", g_nccl.error_string(r));
+        return -1;
+    }
+    memcpy(id, &u, sizeof(u));
+    return 0;
+}
+
+extern "C" int lmieb_set_radius_group_nccl(const void *id, int rank, int world) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    if (!id || world < 1 || rank < 0 || rank >= world) {
+        fprintf(stderr, "ERROR: lmieb_set_radius_group_nccl: rank %d of %d\n", rank, world);
+        return -1;
+    }
+    if (ensure_ready() || nccl_load()) return -1;
+    group_release();
+    NcclUniqueId u;
+    memcpy(&u, id, sizeof(u));
+    int prev = -1;
+    LMIEB_CUDA_TRY(cudaGetDevice(&prev));
+    LMIEB_CUDA_TRY(cudaSetDevice(g_ctx.device));     // the communicator lives on the library's GPU
+    void *comm = nullptr;
+    const int r = g_nccl.comm_init_rank(&comm, world, u, rank);
+    LMIEB_CUDA_TRY(cudaSetDevice(prev));
+    if (r != 0) {
+        fprintf(stderr, "ERROR: lmie_b200: ncclCommInitRank: %s\n", g_nccl.error_string(r));
+        return -1;
+    }
+    g_group.rank = rank;
+    g_group.world = world;
+    g_group.comm = comm;
+    g_group.on = true;
+    return 0;
+}
+
+extern "C" int lmieb_get_radius_group(int *rank, int *world) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    if (rank) *rank = g_group.rank;
+    if (world) *world = g_group.world;
+    return g_group.on ? 1 : 0;
+}
+
 extern "C" int lmieb_timing_state(void) {
     std::lock_guard<std::mutex> lock(g_mu);
     return g_ctx.timing ? 1 : 0;
@@ -1374,7 +1582,8 @@ extern "C" int lmieb_rerun_device(int reps, int flush_l2, double *ms_total, doub
     std::lock_guard<std::mutex> lock(g_mu);
     Ctx &c = g_ctx;
     // a re-run repeats the resident sub-batch, so the last call must have had exactly one
-    if (!c.ready || c.last_slot < 0 || !c.slot[c.last_slot].have_plan || c.submits != 1) {
+    if (!c.ready || c.last_slot < 0 || !c.slot[c.last_slot].have_plan || c.submits != 1 ||
+        c.slot[c.last_slot].plan->acc_mode != LMIEB_ACC_WHOLE) {
         fprintf(stderr, "ERROR: lmieb_rerun_device: no single-sub-batch solve is resident on the device\n");
         return -1;
     }

@@ -322,6 +322,10 @@ typedef struct {
      double *x, *xl, *w, *w2, *mu_user, *sv1, *sv2, *dev_out;
      double **rows;             /* the caller's output rows, in device column order */
      int *n1r, *n2r, *idx1, *idx2;
+     /* radius sharing (lmieb.h): the mode and this process's share */
+     int acc_mode, share_rank, share_world;
+     const double *acc_in;
+     double *acc_out;
      lmieb_problem P;
      lmieb_result R;
 } case_job;
@@ -335,6 +339,32 @@ static void job_free(case_job *j) {
      j->qx = j->qw = j->nr = j->qx_l = j->qw_l = j->nr_l = NULL;
      j->x = j->xl = j->w = j->w2 = j->mu_user = j->dev_out = j->sv1 = j->sv2 = NULL;
      j->n1r = j->n2r = j->idx1 = j->idx2 = NULL;
+}
+
+/* Keeps radius i of a prepared case when i % share_world == share_rank (the
+ * reference's MPI master deals its radii out to the workers the same way,
+ * src/lmie_schedule.c:574-597), none when finishing from summed integrals.
+ * Returns the number kept. */
+static int share_radii(case_job *j, int n, int nd, int nd1) {
+     const int w = j->share_world, r0 = j->share_rank;
+     const int m = j->acc_mode == LMIEB_ACC_FINISH ? 0 : (n > r0 ? (n - r0 + w - 1) / w : 0);
+     const size_t mm = m > 0 ? (size_t) m : 1;
+     double *x = lmieb_arr1(mm), *xl = lmieb_arr1(mm * (nd1 > 0 ? nd1 : 1)), *wt = lmieb_arr1(mm * (1 + nd));
+     int *n1r = (int *) calloc(mm, sizeof(int)), *n2r = (int *) calloc(mm, sizeof(int));
+     int t, k;
+     for (t = 0; t < m; ++t) {
+          const int i = r0 + t * w;
+          x[t] = j->x[i];
+          n1r[t] = j->n1r[i];
+          n2r[t] = j->n2r[i];
+          for (k = 0; k < nd1; ++k)
+               xl[(size_t) k * m + t] = j->xl[(size_t) k * n + i];
+          for (k = 0; k <= nd; ++k)
+               wt[(size_t) k * m + t] = j->w[(size_t) k * n + i];
+     }
+     free(j->x); free(j->xl); free(j->w); free(j->n1r); free(j->n2r);
+     j->x = x; j->xl = xl; j->w = wt; j->n1r = n1r; j->n2r = n2r;
+     return m;
 }
 
 /* Host steps before the Mie core (reference src/lmie_interface.c:404-451,
@@ -458,6 +488,14 @@ static int job_prepare(case_job *j) {
           }
      }
 
+     if (j->acc_mode != LMIEB_ACC_WHOLE) {
+          if (j->save_control != 0) {
+               fprintf(stderr, "ERROR: radius sharing (use_mpi) needs save_control = 0\n");
+               return -1;
+          }
+          n = share_radii(j, n, nd, nd1);
+     }
+
      /* save_control: allocate / gather the per-radius kernels */
      if (j->save_control == 1) {
           *j->save1 = lmieb_arr2(4, n);
@@ -504,6 +542,8 @@ static int job_prepare(case_job *j) {
      j->P.mu_user = j->mu_user;
      j->P.accuracy = j->accuracy;
      j->P.save_control = j->save_control;
+     j->P.acc_mode = j->acc_mode;
+     j->P.acc_in = j->acc_in;
      if (j->save_control == 2) {
           j->P.save1_rows = (const double *const *) *j->save1;
           j->P.save2_rows = n_qang > 0 ? (const double *const *const *) *j->save2 : NULL;
@@ -525,9 +565,12 @@ static int job_prepare(case_job *j) {
           if (j->P.n_angles > 0)
                j->rows[2 * ncol * 6 + k] = col == 0 ? j->pf[e] : j->pf_l[col - 1][e];
      }
-     j->R.gc_rows = j->P.want_gc ? j->rows : NULL;
-     j->R.lc_rows = j->P.want_lc ? j->rows + ncol * 6 : NULL;
-     j->R.pf_rows = j->P.n_angles > 0 ? j->rows + 2 * ncol * 6 : NULL;
+     if (j->acc_mode != LMIEB_ACC_PARTIAL) {
+          j->R.gc_rows = j->P.want_gc ? j->rows : NULL;
+          j->R.lc_rows = j->P.want_lc ? j->rows + ncol * 6 : NULL;
+          j->R.pf_rows = j->P.n_angles > 0 ? j->rows + 2 * ncol * 6 : NULL;
+     }
+     j->R.acc = j->acc_out;
      if (j->save_control == 1) {
           j->R.save1 = (*j->save1)[0];
           j->R.save2 = (*j->save2)[0][0];
@@ -582,8 +625,11 @@ int lmie_solution2_l(int calc_gc, int calc_lc, int calc_pf,
      case_job j;
      int rc;
      (void) n_threads;
-     (void) use_mpi;
      memset(&j, 0, sizeof(j));
+     /* use_mpi: the radii are shared with the registered group (the
+        reference's MPI path, src/lmie_schedule.c:1125-1152) */
+     if (use_mpi && lmieb_get_radius_group(&j.share_rank, &j.share_world))
+          j.acc_mode = LMIEB_ACC_GROUP;
      j.calc_gc = calc_gc; j.calc_lc = calc_lc; j.calc_pf = calc_pf; j.dist_type = dist_type;
      j.n_int1 = n_int1; j.n_int2 = n_int2; j.n_quad = n_quad; j.n_angles = n_angles;
      j.n_derivs = n_derivs; j.save_control = save_control;
@@ -685,6 +731,76 @@ static int jobs_compatible(const case_job *a, const case_job *b) {
           if (a->P.idx2[q] != b->P.idx2[q])
                return 0;
      return 1;
+}
+
+/* ---- radius sharing, two-call form ---------------------------------------- */
+
+long long lmieb_partial_size(const lmie_in_data *in) {
+     const int nd = in->n_derivs > 0 ? in->n_derivs : 0;
+     const int nq = (in->calc_gc || in->calc_lc) ?
+                    lmie_calc_max_coef(in->lambda, in->dist_type, in->a1, in->a2, in->a3, in->r1, in->r2) : 0;
+     return 4LL * (1 + nd) * (1 + nq);
+}
+
+/* One device solve of `in` into `out` in radius-sharing mode acc_mode. */
+static int share_solve(lmie_in_data *in, lmie_out_data *out, int acc_mode, int rank, int world,
+                       const double *acc_in, double *acc_out, int verbose) {
+     case_job j;
+     int rc;
+     job_from_struct(&j, in, out, verbose);
+     j.acc_mode = acc_mode;
+     j.share_rank = rank;
+     j.share_world = world;
+     j.acc_in = acc_in;
+     j.acc_out = acc_out;
+     rc = job_prepare(&j);
+     if (rc == 0 && 4LL * (1 + j.P.nd) * (1 + j.P.n_qang) != lmieb_partial_size(in)) {
+          fprintf(stderr, "ERROR: radius sharing: the integrals of this case are not "
+                  "lmieb_partial_size() doubles (were out's gc / lc arrays set by hand?)\n");
+          rc = -1;
+     }
+     if (rc == 0 && lmieb_device_solve(&j.P, &j.R)) {
+          fprintf(stderr, "ERROR: lmie_core_solution()\n");
+          rc = -1;
+     }
+     if (rc == 0 && acc_mode == LMIEB_ACC_FINISH)
+          job_finish(&j);
+     job_free(&j);
+     return rc;
+}
+
+int lmieb_solution_partial(lmie_in_data *in, int rank, int world, double *acc, int verbose) {
+     lmie_out_data out;
+     int rc;
+     if (world < 1 || rank < 0 || rank >= world || !acc) {
+          fprintf(stderr, "ERROR: lmieb_solution_partial(): rank %d of %d%s\n", rank, world,
+                  acc ? "" : ", acc NULL");
+          return -1;
+     }
+     /* scratch for the host-side outputs (moments, r1, r2, ...) */
+     memset(&out, 0, sizeof(out));
+     if (lmie_out_alloc(in, &out, lmie_calc_max_coef(in->lambda, in->dist_type, in->a1, in->a2,
+                                                     in->a3, in->r1, in->r2))) {
+          fprintf(stderr, "ERROR: lmie_out_alloc()\n");
+          return -1;
+     }
+     rc = share_solve(in, &out, LMIEB_ACC_PARTIAL, rank, world, NULL, acc, verbose);
+     lmie_out_free(&out, in->n_derivs > 0);
+     return rc;
+}
+
+int lmieb_solution_finish(lmie_in_data *in, lmie_out_data *out, int alloc_out, const double *acc,
+                          int verbose) {
+     if (!acc) {
+          fprintf(stderr, "ERROR: lmieb_solution_finish(): acc NULL\n");
+          return -1;
+     }
+     if (alloc_out && lmie_out_alloc(in, out, lmie_calc_max_coef(in->lambda, in->dist_type, in->a1,
+                                                                 in->a2, in->a3, in->r1, in->r2))) {
+          fprintf(stderr, "ERROR: lmie_out_alloc()\n");
+          return -1;
+     }
+     return share_solve(in, out, LMIEB_ACC_FINISH, 0, 1, acc, NULL, verbose);
 }
 
 int lmie_solution_batch(int n_cases, lmie_in_data *in, lmie_out_data *out, int alloc_out,

@@ -60,7 +60,23 @@ typedef struct {
      const double *w2;          /* [nd*n] save_control 2: nr_l qw + nr qw_l per slot */
 
      int precision;             /* LMIEB_PRECISION_* of include/lmie_b200.h */
+
+     /* radius sharing over a group of processes (include/lmie_b200.h): the
+        radii above are this process's share (n may be 0), and acc_mode says
+        how far the device goes.  The integrals ("acc") of a case are
+        4 (1+nd) (1 + n_qang) doubles: Cext, Csca, |S_back|^2, g sums per column,
+        then the phase-matrix sums, rows col*4+e of n_qang, all before
+        normalisation.  save_control must be 0 and the batch one case. */
+     int acc_mode;              /* LMIEB_ACC_* */
+     const double *acc_in;      /* LMIEB_ACC_FINISH: the group's summed integrals */
 } lmieb_problem;
+
+enum {
+     LMIEB_ACC_WHOLE = 0,       /* the whole solve */
+     LMIEB_ACC_PARTIAL = 1,     /* the share's integrals only, to lmieb_result.acc */
+     LMIEB_ACC_FINISH = 2,      /* no radii: finish from acc_in */
+     LMIEB_ACC_GROUP = 3        /* the share's integrals, summed over the registered group, finished */
+};
 
 /* Results, in device column order: column 0 = value, column 1+kk = slot kk. */
 typedef struct {
@@ -75,6 +91,7 @@ typedef struct {
      int n_coef_out;            /* truncated count (the reference's return value) */
      double *save1;             /* [4*n] (save_control 1) or NULL */
      double *save2;             /* [4*n*n_qang] (save_control 1) or NULL */
+     double *acc;               /* LMIEB_ACC_PARTIAL: the integrals (lmieb_problem) */
 } lmieb_result;
 
 /* Runs the device solve of one problem.  Returns 0 or -1 (after printing

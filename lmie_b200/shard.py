@@ -1,17 +1,26 @@
-"""Cases over ranks: one process per GPU, no data-path collective.
+"""Work over ranks, one process per GPU.
 
-Polydisperse cases are independent, so N GPUs either solve their own batches
-(weak scaling: rank r's batch is generated from seed + r) or split one batch
-(strong scaling: contiguous case ranges of balanced estimated cost).  The only
-collectives are the timing barrier and the max over ranks of the timed
-interval, which bench.py issues through torch.distributed.
+Cases: polydisperse cases are independent, so N GPUs either solve their own
+batches (weak scaling: rank r's batch is generated from seed + r) or split
+one batch (strong scaling: contiguous case ranges of balanced estimated
+cost), with no data-path collective; the only collectives are the timing
+barrier and the max over ranks of the timed interval, which bench.py issues
+through torch.distributed.
+
+Radii: one large case can be shared by a group of GPUs (the reference's
+use_mpi, src/lmie_schedule.c:459-921): each rank solves its share of the
+radii, one FP64 all-reduce sums the integrals, and every rank finishes.  The
+library sums either with its own NCCL all-reduce on the solve's stream
+(`use_nccl_group`) or through a callback (`use_torch_group`, torch.distributed).
 """
 from __future__ import annotations
 
+import ctypes as C
 import math
+import sys
 from typing import List, Sequence, Tuple
 
-from .abi import Case
+from .abi import Case, REDUCE_FN
 
 
 def case_cost(case: Case) -> float:
@@ -54,3 +63,76 @@ def strong_slice(cases: Sequence[Case], rank: int, world: int) -> Tuple[int, int
 def weak_seed(seed: int, rank: int) -> int:
     """Seed of rank `rank`'s own batch under weak scaling."""
     return seed + rank
+
+
+# ---- radius sharing --------------------------------------------------------
+
+class _DeviceDoubles:
+    """`count` doubles at a device address, as torch sees them through the
+    CUDA array interface (no copy)."""
+
+    def __init__(self, addr: int, count: int):
+        self.__cuda_array_interface__ = {"shape": (count,), "typestr": "<f8", "data": (addr, False),
+                                         "version": 3, "strides": None}
+
+
+def device_doubles(addr: int, count: int):
+    import torch
+    return torch.as_tensor(_DeviceDoubles(addr, count), device="cuda")
+
+
+def torch_reducer(group=None, wrap=device_doubles):
+    """A lmieb_reduce_fn that sums the library's integrals over the
+    torch.distributed `group` (all_reduce, SUM) and returns once the sum is in
+    place.  `wrap(address, count)` turns the buffer into a tensor: device
+    memory by default; tests on CPU ranks pass a host wrapper."""
+    import torch
+    import torch.distributed as dist
+
+    def fn(buf, count, stream, ctx):
+        try:
+            t = wrap(C.cast(buf, C.c_void_p).value, int(count))
+            dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+            if t.is_cuda:
+                torch.cuda.synchronize(t.device)
+            return 0
+        except Exception as e:  # reported to the library as a failed reduction
+            print(f"ERROR: lmie_b200 radius-group reduction: {e}", file=sys.stderr)
+            return -1
+
+    return REDUCE_FN(fn)
+
+
+def use_torch_group(lib, group=None):
+    """Makes the library share the radii of lmie_solution(..., use_mpi=1)
+    calls with the ranks of the torch.distributed `group`.  Returns the
+    callback object, which must stay alive while it is registered."""
+    import torch.distributed as dist
+    cb = torch_reducer(group)
+    if lib.lmieb_set_radius_group(dist.get_rank(group), dist.get_world_size(group), cb, None) != 0:
+        raise RuntimeError("lmieb_set_radius_group failed")
+    return cb
+
+
+def use_nccl_group(lib, group=None) -> None:
+    """The same with the library's own NCCL all-reduce (no host round trip):
+    rank 0 of `group` creates the NCCL id, the group's collective sends it to
+    the others, and every rank joins the communicator."""
+    import torch.distributed as dist
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    uid = (C.c_char * 128)()
+    ok = rank != 0 or lib.lmieb_nccl_unique_id(uid) == 0
+    obj = [bytes(uid) if ok else b""] if rank == 0 else [None]
+    src = 0 if group is None else dist.get_global_rank(group, 0)
+    dist.broadcast_object_list(obj, src=src, group=group)
+    if len(obj[0]) != 128:
+        raise RuntimeError("lmieb_nccl_unique_id failed on rank 0")
+    uid = (C.c_char * 128).from_buffer_copy(obj[0])
+    if lib.lmieb_set_radius_group_nccl(uid, rank, world) != 0:
+        raise RuntimeError("lmieb_set_radius_group_nccl failed")
+
+
+def leave_group(lib) -> None:
+    """Ends radius sharing: use_mpi calls solve every radius here again."""
+    if lib.lmieb_set_radius_group(0, 1, REDUCE_FN(), None) != 0:
+        raise RuntimeError("lmieb_set_radius_group failed")
