@@ -289,9 +289,14 @@ int lmie_solution2(int calc_gc, int calc_lc, int calc_pf,
                              save1, save2, verbose, n_threads, use_mpi);
 }
 
+/* The reference's MPI workers wait here for radii from the master
+ * (src/lmie_interface.c:514-526).  Radius groups here are symmetric: every
+ * process calls lmie_solution(..., use_mpi = 1) with the same inputs after
+ * joining the group (lmieb_set_radius_group*), so there is no worker loop. */
 int lmie_solution_slave(void) {
-     fprintf(stderr, "ERROR: lmie_solution_slave(): this library is built without MPI; "
-             "distribute cases over GPUs with lmie_solution_batch instead\n");
+     fprintf(stderr, "ERROR: lmie_solution_slave(): no master/worker protocol in this library; "
+             "call lmie_solution(..., use_mpi = 1) on every process of a radius group "
+             "(lmieb_set_radius_group_nccl) instead\n");
      return -1;
 }
 
