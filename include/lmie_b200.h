@@ -32,9 +32,10 @@ int lmie_solution_batch(int n_cases, lmie_in_data *in, lmie_out_data *out, int a
  * LMIEB_PRECISION_FP64: every stage in FP64, the reference's arithmetic
  *   (within 1e-10 of it); lmie_solution and lmie_solution_batch use it.
  * LMIEB_PRECISION_TF32X3: the angular S1/S2 contraction runs on the tensor
- *   cores with each operand split into two TF32 terms (lo*hi + hi*lo + hi*hi),
- *   FP32 accumulation over segments of 64 orders and a double-float sum of
- *   the segments; the Mie recurrences, a_n/b_n, the phase-matrix quadratic
+ *   cores with each operand split into two TF32 terms (lo*hi + hi*lo + hi*hi):
+ *   the hi*hi products accumulate in FP32 over segments of 32 orders
+ *   (lmieb_set_split_segment) added into an FP32 running sum, the cross terms
+ *   over a radius group; the Mie recurrences, a_n/b_n, the phase-matrix quadratic
  *   forms, the radius sums, the normalisation and the expansions stay FP64.
  *   The phase matrix then carries a relative error of a few 1e-7 of its
  *   largest element.  Problems this mode does not cover (save_control != 0,
@@ -69,7 +70,8 @@ int lmieb_get_split_segment(void);
  * the caller or a previous call) repeatedly.  It first picks the angular work
  * granularity (32, 64, 128, 256 items per SM for FP64; 1, 2, 4 for the
  * tensor-core stage) by the device time of the kernels (per-stage CUDA events,
- * one sub-batch), then the pipeline depth (1, 2, 3, 4, 6 parts) by the wall time
+ * one sub-batch) plus the host time of packing the work items, then the
+ * pipeline depth (1, 2, 3, 4, 6 parts) by the wall time
  * of the public batch call, and keeps both for later calls
  * (lmieb_set_work_granularity, lmieb_set_pipeline).  Reports the choice and
  * the best wall time (ms) through the non-NULL pointers.  Returns 0 or -1. */

@@ -699,25 +699,34 @@ static void job_from_struct(case_job *j, lmie_in_data *in, lmie_out_data *out, i
 
 typedef struct {
      case_job *jobs;
-     int n, stage;
+     lmie_in_data *in;          /* stage 0: the cases' inputs and outputs */
+     lmie_out_data *out;
+     int n, stage, verbose;
 } job_pool;
 
 static void job_stage(void *arg, int i) {
      job_pool *p = (job_pool *) arg;
-     if (p->stage == 0)
+     if (p->stage == 0) {
+          job_from_struct(&p->jobs[i], &p->in[i], &p->out[i], p->verbose);
           p->jobs[i].rc = job_prepare(&p->jobs[i]);
-     else if (p->stage == 2)
+     } else if (p->stage == 2) {
           job_free(&p->jobs[i]);
-     else if (p->jobs[i].rc == 0)
+     } else if (p->jobs[i].rc == 0) {
           job_finish(&p->jobs[i]);
+     }
 }
 
-/* Runs stage 0 (prepare), 1 (finish) or 2 (release the host scratch) of
- * every job on up to n_threads host threads. */
-static void run_jobs(case_job *jobs, int n, int stage, int n_threads) {
+/* Runs stage 0 (set up from in/out and prepare), 1 (finish) or 2 (release
+ * the host scratch) of every job on up to n_threads host threads. */
+static void run_jobs_io(case_job *jobs, lmie_in_data *in, lmie_out_data *out, int verbose, int n, int stage,
+                        int n_threads) {
      job_pool p;
-     p.jobs = jobs; p.n = n; p.stage = stage;
+     p.jobs = jobs; p.in = in; p.out = out; p.verbose = verbose; p.n = n; p.stage = stage;
      lmieb_host_parallel(n, n_threads > 0 ? n_threads : 1, job_stage, &p);
+}
+
+static void run_jobs(case_job *jobs, int n, int stage, int n_threads) {
+     run_jobs_io(jobs, NULL, NULL, 0, n, stage, n_threads);
 }
 
 /* Two prepared cases can share a device batch when their derivative layout
@@ -849,6 +858,9 @@ static int finish_chunk(chunk_tickets *ct, case_job *jobs, int j0, int j1, const
           run_jobs(jobs + j0, j1 - j0, 1, n_threads);
           *t_finish += wall_ms() - t0;
      }
+     /* the chunk's host scratch is no longer referenced: released here, while
+        the device still works on the next chunk */
+     run_jobs(jobs + j0, j1 - j0, 2, n_threads);
      ct->n = 0;
      return rc;
 }
@@ -865,7 +877,7 @@ int lmie_solution_batch2(int n_cases, lmie_in_data *in, lmie_out_data *out, int 
      case_job *jobs;
      lmieb_problem *P;
      lmieb_result *R;
-     int *done, *pos2job, *bnd, i, k, c, rc = 0, np = 0, chunks, first = 1, n_last = 0;
+     int *done, *pos2job, *bnd, i, k, c, rc = 0, np = 0, chunks, first = 1, n_last = 0, prepared = 0;
      long long *tk[2];
      int *tb[2], *te[2];
      chunk_tickets ct[2];
@@ -887,7 +899,8 @@ int lmie_solution_batch2(int n_cases, lmie_in_data *in, lmie_out_data *out, int 
                }
           }
      }
-     jobs = (case_job *) calloc(n_cases, sizeof(case_job));
+     /* every job is set up (zeroed first) by its chunk's preparation */
+     jobs = (case_job *) malloc((size_t) n_cases * sizeof(case_job));
      P = (lmieb_problem *) calloc(n_cases, sizeof(lmieb_problem));
      R = (lmieb_result *) calloc(n_cases, sizeof(lmieb_result));
      done = (int *) calloc(n_cases, sizeof(int));
@@ -899,9 +912,6 @@ int lmie_solution_batch2(int n_cases, lmie_in_data *in, lmie_out_data *out, int 
           ct[c].ticket = tk[c];
           ct[c].n = 0;
      }
-     for (i = 0; i < n_cases; ++i)
-          job_from_struct(&jobs[i], &in[i], &out[i], verbose);
-
      /* chunks of cases: chunk c is prepared and packed while the device works
         on chunk c - 1, whose results are then unpacked and scattered */
      chunks = g_pipeline > 0 ? g_pipeline : (n_cases / 640 < 6 ? (n_cases / 640 > 1 ? n_cases / 640 : 1) : 6);
@@ -927,7 +937,8 @@ int lmie_solution_batch2(int n_cases, lmie_in_data *in, lmie_out_data *out, int 
           n_last = c;
           int q = 0;
           t0 = wall_ms();
-          run_jobs(jobs + j0, j1 - j0, 0, n_threads);
+          run_jobs_io(jobs + j0, in + j0, out + j0, verbose, j1 - j0, 0, n_threads);
+          prepared = j1;
           t_prep += wall_ms() - t0;
           for (i = j0; i < j1; ++i)
                if (jobs[i].rc) {
@@ -986,7 +997,8 @@ int lmie_solution_batch2(int n_cases, lmie_in_data *in, lmie_out_data *out, int 
      }
      lmieb_host_phase(0, t_prep);
      lmieb_host_phase(4, t_fin);
-     run_jobs(jobs, n_cases, 2, n_threads);
+     if (rc != 0)      /* chunks given up before their finish (job_free is idempotent) */
+          run_jobs(jobs, prepared, 2, n_threads);
      free(bnd);
      for (c = 0; c < 2; ++c) {
           free(tk[c]); free(tb[c]); free(te[c]);
@@ -1012,9 +1024,10 @@ int lmie_solution_autotune(int n_cases, lmie_in_data *in, lmie_out_data *out, in
           fprintf(stderr, "ERROR: lmie_solution_autotune(): invalid arguments\n");
           return -1;
      }
-     /* 1. work granularity: only the device work depends on it, so it is
-      *    chosen by the device time of the kernels (per-stage CUDA events,
-      *    one sub-batch), which the host's load does not disturb */
+     /* 1. work granularity: it sets the device work and the host's packing
+      *    of the work items (finer items, longer lists), so it is chosen by
+      *    the kernels' device time (per-stage CUDA events, one sub-batch,
+      *    undisturbed by the host's load) plus the packing time */
      g_pipeline = 1;
      lmieb_set_timing(1);
      for (b = 0; b < n_items && rc == 0; ++b) {
@@ -1023,10 +1036,13 @@ int lmie_solution_autotune(int n_cases, lmie_in_data *in, lmie_out_data *out, in
           for (r = 0; r < 3 && rc == 0; ++r) {
                double st[LMIEB_N_STAGES], dt = 0.;
                int s;
+               double hm[LMIEB_N_HOST];
                rc = lmie_solution_batch2(n_cases, in, out, 0, 0, n_threads, precision);
                lmieb_last_timing(st, LMIEB_N_STAGES);
                for (s = 1; s < LMIEB_N_STAGES - 1; ++s)      /* kernels: stages between the copies */
                     dt += st[s];
+               lmieb_last_host_timing(hm, LMIEB_N_HOST);
+               dt += hm[1];                                   /* packing */
                if (r > 0 && (d < 0. || dt < d))
                     d = dt;
           }
