@@ -34,6 +34,8 @@ namespace {
 constexpr int NSTAGE = LMIEB_N_STAGES;
 constexpr size_t FLUSH_BYTES = (size_t) 256 << 20;     // > 126 MB L2
 constexpr size_t BATCH_BYTES = (size_t) 24 << 30;      // device working set of one sub-batch
+constexpr int MAX_PIECES = 16;                         // results come back in up to 16 pieces of cases
+constexpr size_t PIECE_BYTES = (size_t) 8 << 20;       // of about 8 MB or more
 
 // Every staged array starts on a 256-byte boundary and takes at least one
 // 256-byte block, so empty arrays never alias their neighbours.
@@ -57,6 +59,7 @@ struct Pending {
     int acc_mode = 0;
     double *o_acc = nullptr;           // LMIEB_ACC_PARTIAL: the integrals
     size_t acc_n = 0;
+    std::vector<int> piece;            // case ranges [piece[p], piece[p+1]) of the result copies
     double t_submit = 0.;
 };
 
@@ -70,6 +73,7 @@ struct Slot {
     Plan *plan = nullptr;
     cudaStream_t stream = nullptr;     // the sub-batches of this slot (consecutive ones overlap)
     cudaEvent_t done = nullptr;
+    cudaEvent_t piece[MAX_PIECES] = {};  // after the copy of each piece of the results
     cudaEvent_t t_begin = nullptr, t_end = nullptr;   // device span of the sub-batch
     bool have_plan = false;
     cudaGraphExec_t graph = nullptr;   // the plan's kernel sequence, captured for re-runs
@@ -308,6 +312,7 @@ int ensure_ready() {
         S.plan = new Plan();
         LMIEB_CUDA_TRY(cudaStreamCreateWithFlags(&S.stream, cudaStreamNonBlocking));
         LMIEB_CUDA_TRY(cudaEventCreateWithFlags(&S.done, cudaEventDisableTiming));
+        for (cudaEvent_t &e : S.piece) LMIEB_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         LMIEB_CUDA_TRY(cudaEventCreate(&S.t_begin));
         LMIEB_CUDA_TRY(cudaEventCreate(&S.t_end));
     }
@@ -1206,7 +1211,47 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         c.save.nq = L.n_qang0;
         c.save.owner = ticket;
     }
-    LMIEB_CUDA_TRY(cudaMemcpyAsync(h_out, d_out, out_bytes, cudaMemcpyDeviceToHost, s));
+    // The results come back in pieces of consecutive cases, each followed by
+    // an event, so that the host unpacks one piece while the next is copied.
+    // First the small tail of the block (truncations and error word,
+    // save_control kernels, integrals), then per piece its slices of the
+    // cross sections, expansions and phase matrices.
+    std::vector<int> piece(1, 0);
+    {
+        const char *misc = (const char *) L.o_trunc;
+        const size_t moff = (size_t) (misc - d_out);
+        LMIEB_CUDA_TRY(cudaMemcpyAsync(h_out + moff, misc, out_bytes - moff, cudaMemcpyDeviceToHost, s));
+        const int np = (int) std::max<size_t>(1, std::min<size_t>(MAX_PIECES, out_bytes / PIECE_BYTES));
+        const double per = (double) (o_scal + o_gc + o_lc + o_pf) / np;
+        double run = 0.;
+        for (int k = 0; k < ncase; ++k) {
+            const DevCase &C = cs[k];
+            run += ncol * (4. + 6. * (C.n_angles + (L.want_gc ? C.n_coef : 0) + (L.want_lc ? C.n_coef : 0)));
+            if ((k + 1 == ncase || run >= per * (double) piece.size()) && (int) piece.size() <= np)
+                piece.push_back(k + 1);
+        }
+        if (piece.back() != ncase) piece.back() = ncase;
+        auto ends = [&](int k, size_t &sc, size_t &g, size_t &l, size_t &f) {
+            if (k == ncase) { sc = o_scal; g = o_gc; l = o_lc; f = o_pf; return; }
+            sc = (size_t) cs[k].scal_off; g = (size_t) cs[k].gc_off; l = (size_t) cs[k].lc_off;
+            f = (size_t) cs[k].pf_out_off;
+        };
+        auto down = [&](double *base, size_t a, size_t b) -> cudaError_t {
+            if (b <= a) return cudaSuccess;
+            const size_t off = (size_t) ((char *) (base + a) - d_out);
+            return cudaMemcpyAsync(h_out + off, base + a, (b - a) * 8, cudaMemcpyDeviceToHost, s);
+        };
+        for (size_t p = 0; p + 1 < piece.size(); ++p) {
+            size_t s0, g0, l0, f0, s1, g1, l1, f1;
+            ends(piece[p], s0, g0, l0, f0);
+            ends(piece[p + 1], s1, g1, l1, f1);
+            LMIEB_CUDA_TRY(down(L.o_scal, s0, s1));
+            LMIEB_CUDA_TRY(down(L.o_gc, g0, g1));
+            LMIEB_CUDA_TRY(down(L.o_lc, l0, l1));
+            LMIEB_CUDA_TRY(down(L.o_pf, f0, f1));
+            LMIEB_CUDA_TRY(cudaEventRecord(S.piece[p], s));
+        }
+    }
     stage(NSTAGE);
     LMIEB_CUDA_TRY(cudaEventRecord(S.t_end, s));
     LMIEB_CUDA_TRY(cudaEventRecord(S.done, s));
@@ -1239,6 +1284,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     P.acc_mode = L.acc_mode;
     P.o_acc = L.o_acc;
     P.acc_n = L.acc_n;
+    P.piece.swap(piece);
     P.t_submit = now_ms();
     return 0;
 }
@@ -1250,10 +1296,51 @@ int collect_slot(Slot &S) {
     Pending &P = S.pend;
     if (!P.active) return 0;
     P.active = false;
-    LMIEB_CUDA_TRY(cudaEventSynchronize(S.done));
+    // the first piece of the results (and the truncations, error word, kept kernels)
+    LMIEB_CUDA_TRY(cudaEventSynchronize(S.piece[0]));
     LMIEB_CUDA_TRY(cudaGetLastError());
     const double t_unpack = now_ms();
-    c.host_ms[2] += t_unpack - P.t_submit;
+    double waited = 0.;                 // unpacking waits for later pieces
+    const int ncase = P.ncase, ncol = P.ncol;
+    auto hostp = [&](void *d) { return P.h_out + ((char *) d - P.d_out); };
+    const double *hs = (const double *) hostp(P.o_scal);
+    const double *hg = (const double *) hostp(P.o_gc);
+    const double *hl = (const double *) hostp(P.o_lc);
+    const double *hpf = (const double *) hostp(P.o_pf);
+    const int *htr = (const int *) hostp(P.o_trunc);
+    if (htr[2 * ncase]) {
+        LMIEB_CUDA_TRY(cudaEventSynchronize(S.done));   // no copy may still write the staging
+        fprintf(stderr, "ERROR: lmie_b200: the tensor-core angular stage timed out waiting for its pipeline\n");
+        return -1;
+    }
+    for (size_t p = 0; p + 1 < P.piece.size(); ++p) {
+        if (p > 0) {
+            const double tw = now_ms();
+            LMIEB_CUDA_TRY(cudaEventSynchronize(S.piece[p]));
+            waited += now_ms() - tw;
+        }
+        const int k0 = P.piece[p];
+        parallel_for(P.piece[p + 1] - k0, 8, [&](int i) {
+            const int k = k0 + i;
+            const DevCase &C = P.cs[k];
+            lmieb_result &r = P.rs[k];
+            memcpy(r.scal, hs + C.scal_off, (size_t) ncol * 4 * 8);
+            auto put = [&](double **rows, double *flat, const double *src, size_t len) {
+                if (rows) {
+                    for (int i = 0; i < ncol * 6; ++i) memcpy(rows[i], src + (size_t) i * len, len * 8);
+                } else if (flat) {
+                    memcpy(flat, src, (size_t) ncol * 6 * len * 8);
+                }
+            };
+            if (P.want_gc) put(r.gc_rows, r.gc, hg + C.gc_off, (size_t) C.n_coef);
+            if (P.want_lc) put(r.lc_rows, r.lc, hl + C.lc_off, (size_t) C.n_coef);
+            if (P.pf_from) put(r.pf_rows, r.pf, hpf + C.pf_out_off, (size_t) C.n_angles);
+            const int t = P.want_lc ? htr[ncase + k] : (P.want_gc ? htr[k] : 0);
+            r.n_coef_out = (P.want_gc || P.want_lc) ? (t > 0 ? C.n_coef - t + 1 : C.n_coef) : 0;
+        });
+    }
+    LMIEB_CUDA_TRY(cudaEventSynchronize(S.done));
+    c.host_ms[2] += t_unpack - P.t_submit + waited;
     {
         float a = 0.f, b = 0.f;
         if (cudaEventElapsedTime(&a, S.t_begin, S.t_end) == cudaSuccess) c.host_ms[6] += a;
@@ -1266,34 +1353,6 @@ int collect_slot(Slot &S) {
             c.stage_ms[i] += ms;
         }
     }
-    const int ncase = P.ncase, ncol = P.ncol;
-    auto hostp = [&](void *d) { return P.h_out + ((char *) d - P.d_out); };
-    const double *hs = (const double *) hostp(P.o_scal);
-    const double *hg = (const double *) hostp(P.o_gc);
-    const double *hl = (const double *) hostp(P.o_lc);
-    const double *hpf = (const double *) hostp(P.o_pf);
-    const int *htr = (const int *) hostp(P.o_trunc);
-    if (htr[2 * ncase]) {
-        fprintf(stderr, "ERROR: lmie_b200: the tensor-core angular stage timed out waiting for its pipeline\n");
-        return -1;
-    }
-    parallel_for(ncase, 8, [&](int k) {
-        const DevCase &C = P.cs[k];
-        lmieb_result &r = P.rs[k];
-        memcpy(r.scal, hs + C.scal_off, (size_t) ncol * 4 * 8);
-        auto put = [&](double **rows, double *flat, const double *src, size_t len) {
-            if (rows) {
-                for (int i = 0; i < ncol * 6; ++i) memcpy(rows[i], src + (size_t) i * len, len * 8);
-            } else if (flat) {
-                memcpy(flat, src, (size_t) ncol * 6 * len * 8);
-            }
-        };
-        if (P.want_gc) put(r.gc_rows, r.gc, hg + C.gc_off, (size_t) C.n_coef);
-        if (P.want_lc) put(r.lc_rows, r.lc, hl + C.lc_off, (size_t) C.n_coef);
-        if (P.pf_from) put(r.pf_rows, r.pf, hpf + C.pf_out_off, (size_t) C.n_angles);
-        const int t = P.want_lc ? htr[ncase + k] : (P.want_gc ? htr[k] : 0);
-        r.n_coef_out = (P.want_gc || P.want_lc) ? (t > 0 ? C.n_coef - t + 1 : C.n_coef) : 0;
-    });
     if (P.save_control == 1 && c.save.owner == P.ticket) {
         // the set just saved: its hash, over the same rows a later
         // save_control 2 call hashes through its row pointers
@@ -1312,7 +1371,7 @@ int collect_slot(Slot &S) {
         if (r.save1) memcpy(r.save1, hostp(P.o_save1), (size_t) 4 * P.R * 8);
         if (r.save2 && P.n_qang0 > 0) memcpy(r.save2, hostp(P.o_save2), P.n_save2 * 8);
     }
-    c.host_ms[3] += now_ms() - t_unpack;
+    c.host_ms[3] += now_ms() - t_unpack - waited;
     return 0;
 }
 
