@@ -540,8 +540,8 @@ __global__ void __launch_bounds__(ANG_T) k_angular(DevBatch B, int c1base, int c
     constexpr int NS = 1 + NC1 + NC2;
     extern __shared__ double4 smem4[];
     double4 *cbuf = smem4;                                   // [ANG_KT][C1] {cs, cd}
-    double *fv2s = (double *) (cbuf + ANG_KT * C1);          // [ANG_KT]
-    double *acc = fv2s + ANG_KT;                             // [AP][NS*2*4][ANG_T]
+    double *gks = (double *) (cbuf + ANG_KT * C1);           // [ANG_KT] (2k+1)/k
+    double *acc = gks + ANG_KT;                              // [AP][NS*2*4][ANG_T]
 
     const AngItem it = items[blockIdx.x];
     const DevCase &C = B.cs[it.c];
@@ -571,6 +571,25 @@ __global__ void __launch_bounds__(ANG_T) k_angular(DevBatch B, int c1base, int c
 #pragma unroll
     for (int k = 0; k < NC2; ++k) slot2[k] = 1 + B.idx2[c2base + k];
 
+    // The next chunk's coefficients are loaded into registers while the
+    // current chunk is consumed from shared memory.
+    constexpr int PF = (ANG_KT * C1 + ANG_T - 1) / ANG_T;
+    double4 pre[PF];
+    double pre_fv = 0.;
+    auto fetch = [&](size_t off, int n1, int k0) {
+        const int kt = min(ANG_KT, n1 - k0);
+#pragma unroll
+        for (int u = 0; u < PF; ++u) {
+            const int idx = tid + u * ANG_T;
+            if (idx < kt * C1) {
+                const int t = idx / C1, c = idx - t * C1;
+                const size_t col = c == 0 ? 0 : (size_t) (c1base + c);
+                pre[u] = cf[col * tot + off + k0 + t];
+            }
+        }
+        if (tid < kt) pre_fv = fv2[k0 + tid + 1];
+    };
+
     for (int r = it.rbeg; r < it.rend; ++r) {
         const int n1 = B.n1r[r];
         const size_t off = (size_t) B.off[r];
@@ -584,25 +603,7 @@ __global__ void __launch_bounds__(ANG_T) k_angular(DevBatch B, int c1base, int c
             for (int c = 0; c < C1; ++c) spA[a][c] = smA[a][c] = spB[a][c] = smB[a][c] = mk(0., 0.);
         }
         double kd = 1.;
-        // the next chunk's coefficients are loaded into registers while the
-        // current chunk is consumed from shared memory
-        constexpr int PF = (ANG_KT * C1 + ANG_T - 1) / ANG_T;
-        double4 pre[PF];
-        double pre_fv = 0.;
-        auto fetch = [&](int k0) {
-            const int kt = min(ANG_KT, n1 - k0);
-#pragma unroll
-            for (int u = 0; u < PF; ++u) {
-                const int idx = tid + u * ANG_T;
-                if (idx < kt * C1) {
-                    const int t = idx / C1, c = idx - t * C1;
-                    const size_t col = c == 0 ? 0 : (size_t) (c1base + c);
-                    pre[u] = cf[col * tot + off + k0 + t];
-                }
-            }
-            if (tid < kt) pre_fv = fv2[k0 + tid + 1];
-        };
-        fetch(0);
+        fetch(off, n1, 0);
         for (int k0 = 0; k0 < n1; k0 += ANG_KT) {
             const int kt = min(ANG_KT, n1 - k0);
             __syncthreads();
@@ -611,16 +612,23 @@ __global__ void __launch_bounds__(ANG_T) k_angular(DevBatch B, int c1base, int c
                 const int idx = tid + u * ANG_T;
                 if (idx < kt * C1) cbuf[idx] = pre[u];
             }
-            if (tid < kt) fv2s[tid] = pre_fv;
+            if (tid < kt) gks[tid] = 1. + pre_fv;
             __syncthreads();
-            if (k0 + ANG_KT < n1) fetch(k0 + ANG_KT);
+            if (k0 + ANG_KT < n1) fetch(off, n1, k0 + ANG_KT);
             if (!any) continue;
-            // orders k = k0 + t + 1: t even <-> k odd <-> mirror sign +1
+            // orders k = k0 + t + 1: t even <-> k odd <-> mirror sign +1.  With
+            // t2 = mu pi_k - pi_{k-1}: tau_k = k t2 - pi_{k-1} and
+            // pi_{k+1} = mu pi_k + (k+1)/k t2 = (2k+1)/k t2 + pi_{k-1}
+            // (the reference's a1 + fv2 a2, src/lmie_core.c:674-689, in three FMAs)
             auto step = [&](int t, bool odd) {
+                const double gk = gks[t];
 #pragma unroll
                 for (int a = 0; a < AP; ++a) {
-                    const double t1 = mu[a] * p1[a], t2 = t1 - p0[a], tau = kd * t2 - p0[a];
+                    const double t2 = fma(mu[a], p1[a], -p0[a]), tau = fma(kd, t2, -p0[a]);
                     const double tp = p1[a] + tau, tm = p1[a] - tau;
+                    const double pn = fma(gk, t2, p0[a]);
+                    p0[a] = p1[a];
+                    p1[a] = pn;
 #pragma unroll
                     for (int c = 0; c < C1; ++c) {
                         const double4 v = cbuf[t * C1 + c];
@@ -634,8 +642,6 @@ __global__ void __launch_bounds__(ANG_T) k_angular(DevBatch B, int c1base, int c
                             smB[a][c].re -= tp * v.z;  smB[a][c].im -= tp * v.w;
                         }
                     }
-                    p0[a] = p1[a];
-                    p1[a] = t1 + fv2s[t] * t2;
                 }
                 kd += 1.;
             };
