@@ -874,10 +874,39 @@ __device__ __forceinline__ double basis_next(int f, int l, const double *rc, dou
 // recurrence over all orders and checkpoints (p_{l-2}, p_{l-1}) at the start
 // of every EX_LT-order tile.
 // ---------------------------------------------------------------------------
+// one chain: function F of the set at node x over all n_coef orders
+template <int KIND, int F>
+__device__ __forceinline__ void ckpt_chain(const DevCase &C, int i, double x, const double *__restrict__ rc,
+                                           double *__restrict__ ck) {
+    constexpr int NF = KIND == 0 ? 4 : 1;
+    constexpr int first = KIND == 1 ? 2 : 3;
+    double prev = 0., cur = 0.;
+    for (int lb = 0; lb < C.n_coef; lb += EX_LT) {
+        const size_t o = (((size_t) (lb / EX_LT) * NF + F) * C.nh + i) * 2;
+        ck[o] = prev;
+        ck[o + 1] = cur;
+        const int le = min(C.n_coef, lb + EX_LT);
+        int l = lb;
+        for (; l < le && l < first; ++l) {
+            const double v = basis_first<KIND>(F, l, x);
+            prev = cur;
+            cur = v;
+        }
+        // the recurrence coefficients do not depend on the chain: unrolled,
+        // with the function fixed, their loads are issued ahead of the
+        // dependent steps
+#pragma unroll 8
+        for (; l < le; ++l) {
+            const double v = basis_step<KIND>(F, rc + 8 * (size_t) l, x, cur, prev);
+            prev = cur;
+            cur = v;
+        }
+    }
+}
+
 template <int KIND>
 __global__ void k_exp_ckpt(DevBatch B, long long total, const long long *__restrict__ start,
                            double *__restrict__ ckpt) {
-    constexpr int NF = KIND == 0 ? 4 : 1;
     const long long e = (long long) blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= total) return;
     const int c = find_case(start, B.ncase, e);
@@ -885,18 +914,12 @@ __global__ void k_exp_ckpt(DevBatch B, long long total, const long long *__restr
     const long long local = e - start[c];
     const int f = (int) (local / C.nh), i = (int) (local % C.nh);
     const double x = B.mu_pool[C.mu_off + C.nh + i];
-    double prev = 0., cur = 0.;
     double *ck = ckpt + C.ck_off;
-    for (int l = 0; l < C.n_coef; ++l) {
-        if (l % EX_LT == 0) {
-            const size_t o = (((size_t) (l / EX_LT) * NF + f) * C.nh + i) * 2;
-            ck[o] = prev;
-            ck[o + 1] = cur;
-        }
-        const double v = basis_next<KIND>(f, l, B.rc, x, cur, prev);
-        prev = cur;
-        cur = v;
-    }
+    if (KIND == 1) ckpt_chain<KIND, 0>(C, i, x, B.rc, ck);
+    else if (f == 0) ckpt_chain<KIND, 0>(C, i, x, B.rc, ck);
+    else if (f == 1) ckpt_chain<KIND, 1>(C, i, x, B.rc, ck);
+    else if (f == 2) ckpt_chain<KIND, 2>(C, i, x, B.rc, ck);
+    else ckpt_chain<KIND, 3>(C, i, x, B.rc, ck);
 }
 
 // ---------------------------------------------------------------------------
@@ -906,10 +929,12 @@ __global__ void k_exp_ckpt(DevBatch B, long long total, const long long *__restr
 // are staged next to them, and each output (order, column) is contracted
 // over the tile's EX_AT node pairs.  Raw per-tile sums go to exq.
 // ---------------------------------------------------------------------------
-constexpr int EX_T = 128;
+// threads of a K4b block: one per (order, column) of the contraction, at
+// least 128 (the basis phase) and at most EX_TMAX
+constexpr int EX_TMAX = 256;
 
 template <int KIND>
-__global__ void __launch_bounds__(EX_T) k_exp_tile(DevBatch B, const ExpItem *__restrict__ items,
+__global__ void __launch_bounds__(EX_TMAX) k_exp_tile(DevBatch B, const ExpItem *__restrict__ items,
                                                    const double *__restrict__ pfn,
                                                    const double *__restrict__ ckpt,
                                                    double *__restrict__ exq) {
@@ -925,11 +950,11 @@ __global__ void __launch_bounds__(EX_T) k_exp_tile(DevBatch B, const ExpItem *__
     const int i0 = it.at * EX_AT;
     const double *mup = B.mu_pool + C.mu_off, *wqp = mup + nq;
     double *rcs = Bv + (size_t) ncol * 12 * EX_AT;         // [8 EX_LT] recurrence coefficients of the tile
-    for (int t = threadIdx.x; t < 8 * lt; t += EX_T) rcs[t] = B.rc[8 * (size_t) l0 + t];
+    for (int t = threadIdx.x; t < 8 * lt; t += blockDim.x) rcs[t] = B.rc[8 * (size_t) l0 + t];
     __syncthreads();
 
     // basis functions of the tile
-    for (int t = threadIdx.x; t < NF * EX_AT; t += EX_T) {
+    for (int t = threadIdx.x; t < NF * EX_AT; t += blockDim.x) {
         const int f = t / EX_AT, ia = t % EX_AT, i = i0 + ia;
         double *Pf = P + (size_t) f * EX_LT * (EX_AT + 1) + ia;
         if (i < nh) {
@@ -949,7 +974,7 @@ __global__ void __launch_bounds__(EX_T) k_exp_tile(DevBatch B, const ExpItem *__
         }
     }
     // weighted moments of the node pairs: b1 at the mirror node -mu_i, b2 at +mu_i
-    for (int t = threadIdx.x; t < ncol * EX_AT; t += EX_T) {
+    for (int t = threadIdx.x; t < ncol * EX_AT; t += blockDim.x) {
         const int col = t / EX_AT, ia = t % EX_AT, i = i0 + ia;
         double *bv = Bv + (size_t) col * 12 * EX_AT + ia;
         if (i < nh) {
@@ -975,7 +1000,7 @@ __global__ void __launch_bounds__(EX_T) k_exp_tile(DevBatch B, const ExpItem *__
     }
     __syncthreads();
     // contraction over the tile's node pairs
-    for (int t = threadIdx.x; t < ncol * lt; t += EX_T) {
+    for (int t = threadIdx.x; t < ncol * lt; t += blockDim.x) {
         const int col = t / lt, u = t % lt;
         const int l = l0 + u;
         const double s = (l & 1) ? -1. : 1.;
@@ -1187,7 +1212,8 @@ int run_expand(cudaStream_t s, const DevBatch &B, long long nck, const long long
     }
     k_exp_ckpt<KIND><<<ceil_div(nck, 128), 128, 0, s>>>(B, nck, ck_start, ckpt);
     LMIEB_CUDA_TRY(cudaGetLastError());
-    k_exp_tile<KIND><<<nitems, EX_T, sm, s>>>(B, items, pfn, ckpt, exq);
+    const int nt = std::min(EX_TMAX, std::max(128, ((1 + B.nd) * EX_LT + 31) / 32 * 32));
+    k_exp_tile<KIND><<<nitems, nt, sm, s>>>(B, items, pfn, ckpt, exq);
     LMIEB_CUDA_TRY(cudaGetLastError());
     k_exp_final<KIND><<<ceil_div(nfin, 256), 256, 0, s>>>(B, nfin, fin_start, exq, coefs, trunc);
     LMIEB_CUDA_TRY(cudaGetLastError());
