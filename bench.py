@@ -67,7 +67,7 @@ N_CASES = 4096
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_angular /
 # k_angular_tc launch on this workload: measured with ncu on a 256-case batch
 # of the same generator and scaled by the ratio of angular work (13.33).
-ANGULAR_TRAFFIC = {"fp64": 9.89e9, "tf32x3": 5.15e9}
+ANGULAR_TRAFFIC = {"fp64": 12.21e9, "tf32x3": 5.15e9}
 WORKLOAD = ("batched uneven: 4096 seeded cases (r_eff 0.05-20 um, v_eff 0.02-0.3, lambda 0.34-2.1 um, "
             "mr 1.33-1.60, mi 1e-8-0.1, gamma/log-normal, 100-2000 radii, x_max 0.2-1063), "
             "4 derivatives each (mr, mi, a1, a2), GSF + 181-angle phase matrix, FP64")
