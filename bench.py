@@ -530,7 +530,7 @@ def run_b200(args) -> int:
             "value": n_job * args.steps / (split_dev_ms * 1e-3),
             "e2e": n_job * args.steps / split_e2e_s, "unit": UNIT,
             "ms_per_step": split_dev_ms / args.steps, "stage_ms": split_stage_ms,
-            "dtype": "f64 with tf32x3 angular contraction (fp32 accumulation in segments of 64 orders)",
+            "dtype": "f64 with tf32x3 angular contraction (fp32 accumulation in segments of 32 orders)",
             "autotuned": tuned_tc,
             "error_vs_fp64": errs,
             "roofline": {

@@ -139,7 +139,8 @@ int lmie_solution_adjoint(int n_lambda, const double *lambda, const double *mr, 
  * random operands through the operand split, shared-memory layout,
  * descriptors, tcgen05.mma issue and tensor-memory reads of the
  * split-precision angular stage, with one FP32 accumulation over all of K
- * (the stage itself sums segments of 64 orders in double-float), against an
+ * (the stage itself accumulates segments of 32 orders into a running sum),
+ * against an
  * FP64 product on the host.  Writes the largest error relative to the
  * largest element of the product.  Returns 0 or -1. */
 int lmieb_tc_selftest(int K, double *max_rel_err);
