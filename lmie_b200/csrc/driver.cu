@@ -881,7 +881,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
                 mu_user.insert(mu_user.end(), ps[k].mu_user, ps[k].mu_user + C.n_angles);
             }
         }
-        pu_start[k + 1] = pu_start[k] + (long long) ncol * ((C.n_angles + PU_T - 1) / PU_T);   // K5 blocks
+        pu_start[k + 1] = pu_start[k] + (C.n_angles + PU_T - 1) / PU_T;   // K5 blocks (all columns)
         C.scal_off = (int) o_scal;
         o_scal += (size_t) ncol * 4;
         C.gc_off = (long long) o_gc;

@@ -1075,83 +1075,108 @@ __global__ void k_exp_final(DevBatch B, long long total, const long long *__rest
 
 // ---------------------------------------------------------------------------
 // K5: phase matrix at the user's angles from the truncated expansion; one
-// block per (case, column, tile of PU_T user angles), one thread per angle.
-// The expansion coefficients and the recurrence coefficients of PU_T orders
-// at a time are staged in shared memory, which all threads of the block read.
+// block per (case, tile of PU_T user angles), one thread per angle.  The
+// basis functions of an order are generated once per angle and used by up to
+// CG columns at a time; the expansion coefficients of those columns (GSF:
+// with the a2 +- a3 pair combined) and the recurrence coefficients of PU_T
+// orders at a time are staged in shared memory, which all threads read.
 // ---------------------------------------------------------------------------
-template <int KIND>
+template <int KIND, int CG>
 __global__ void __launch_bounds__(PU_T) k_phase_user(DevBatch B, const long long *__restrict__ start,
                                                      const double *__restrict__ coefs,
                                                      const int *__restrict__ trunc, double *__restrict__ out) {
-    __shared__ double cfs[6][PU_T], rcs[8 * PU_T];
+    __shared__ double cfs[CG][6][PU_T], rcs[8 * PU_T];
     const int c = find_case(start, B.ncase, blockIdx.x);
     const DevCase &C = B.cs[c];
-    const int na = C.n_angles, ncf = C.n_coef;
-    const int per = (na + PU_T - 1) / PU_T;
+    const int na = C.n_angles, ncf = C.n_coef, ncol = 1 + B.nd;
     const int local = (int) (blockIdx.x - start[c]);
-    const int col = local / per, a = (local % per) * PU_T + threadIdx.x;
+    const int a = local * PU_T + threadIdx.x;
     const bool act = a < na;
     const int nt = trunc[c] > 0 ? ncf - trunc[c] + 1 : ncf;
     const double x = act ? B.mu_user[C.mu_user_off + a] : 0.;
-    const double *cf = coefs + (KIND == 0 ? C.gc_off : C.lc_off) + (size_t) col * 6 * ncf;
-    double *o = out + C.pf_out_off + (size_t) col * 6 * na;
-    double s0 = 0., s1 = 0., s2 = 0., s3 = 0., s4 = 0., s5 = 0.;
-    double q[4] = {0., 0., 0., 0.}, p[4] = {0., 0., 0., 0.};
-    for (int l0 = 0; l0 < nt; l0 += PU_T) {
-        const int lt = min(PU_T, nt - l0);
-        __syncthreads();
-        for (int t = threadIdx.x; t < 6 * PU_T; t += PU_T) {
-            const int e = t / PU_T, u = t % PU_T;
-            cfs[e][u] = u < lt ? cf[(size_t) e * ncf + l0 + u] : 0.;
-        }
-        for (int t = threadIdx.x; t < 8 * lt; t += PU_T) rcs[t] = B.rc[8 * (size_t) l0 + t];
-        __syncthreads();
-        for (int u = 0; u < lt; ++u) {
-            const int l = l0 + u;
-            const double *rl = rcs + 8 * u;                       // recurrence coefficients of order l
-            if (KIND == 0) {
+    const double *cf0 = coefs + (KIND == 0 ? C.gc_off : C.lc_off);
+    for (int g0 = 0; g0 < ncol; g0 += CG) {
+        const int ng = min(CG, ncol - g0);
+        double s[CG][6];
 #pragma unroll
-                for (int f = 0; f < 4; ++f) {
-                    const double v = l < 3 ? basis_first<0>(f, l, x) : basis_step<0>(f, rl, x, p[f], q[f]);
-                    q[f] = p[f];
-                    p[f] = v;
+        for (int g = 0; g < CG; ++g)
+#pragma unroll
+            for (int e = 0; e < 6; ++e) s[g][e] = 0.;
+        double q[4] = {0., 0., 0., 0.}, p[4] = {0., 0., 0., 0.};
+        for (int l0 = 0; l0 < nt; l0 += PU_T) {
+            const int lt = min(PU_T, nt - l0);
+            __syncthreads();
+            for (int t = threadIdx.x; t < ng * PU_T; t += PU_T) {
+                const int g = t / PU_T, u = t % PU_T;
+                const double *cf = cf0 + (size_t) (g0 + g) * 6 * ncf + l0 + u;
+                double v[6] = {0., 0., 0., 0., 0., 0.};
+                if (u < lt)
+#pragma unroll
+                    for (int e = 0; e < 6; ++e) v[e] = cf[(size_t) e * ncf];
+                if (KIND == 0) {
+                    const double a2 = v[1], a3 = v[2];
+                    v[1] = a2 + a3;
+                    v[2] = a2 - a3;
                 }
-                s0 += cfs[0][u] * p[0];
-                s3 += cfs[3][u] * p[0];
-                if (l >= 2) {
-                    s4 += cfs[4][u] * p[1];
-                    s5 += cfs[5][u] * p[1];
-                    s1 += (cfs[1][u] + cfs[2][u]) * p[2];
-                    s2 += (cfs[1][u] - cfs[2][u]) * p[3];
+#pragma unroll
+                for (int e = 0; e < 6; ++e) cfs[g][e][u] = v[e];
+            }
+            for (int t = threadIdx.x; t < 8 * lt; t += PU_T) rcs[t] = B.rc[8 * (size_t) l0 + t];
+            __syncthreads();
+            for (int u = 0; u < lt; ++u) {
+                const int l = l0 + u;
+                const double *rl = rcs + 8 * u;                       // recurrence coefficients of order l
+                if (KIND == 0) {
+#pragma unroll
+                    for (int f = 0; f < 4; ++f) {
+                        const double v = l < 3 ? basis_first<0>(f, l, x) : basis_step<0>(f, rl, x, p[f], q[f]);
+                        q[f] = p[f];
+                        p[f] = v;
+                    }
+#pragma unroll
+                    for (int g = 0; g < CG; ++g) {
+                        s[g][0] += cfs[g][0][u] * p[0];
+                        s[g][3] += cfs[g][3][u] * p[0];
+                        if (l >= 2) {
+                            s[g][4] += cfs[g][4][u] * p[1];
+                            s[g][5] += cfs[g][5][u] * p[1];
+                            s[g][1] += cfs[g][1][u] * p[2];
+                            s[g][2] += cfs[g][2][u] * p[3];
+                        }
+                    }
+                } else {
+                    const double v = l < 2 ? basis_first<1>(0, l, x) : basis_step<1>(0, rl, x, p[0], q[0]);
+                    q[0] = p[0];
+                    p[0] = v;
+#pragma unroll
+                    for (int g = 0; g < CG; ++g)
+#pragma unroll
+                        for (int e = 0; e < 6; ++e) s[g][e] += cfs[g][e][u] * v;
                 }
-            } else {
-                const double v = l < 2 ? basis_first<1>(0, l, x) : basis_step<1>(0, rl, x, p[0], q[0]);
-                q[0] = p[0];
-                p[0] = v;
-                s0 += cfs[0][u] * v;
-                s1 += cfs[1][u] * v;
-                s2 += cfs[2][u] * v;
-                s3 += cfs[3][u] * v;
-                s4 += cfs[4][u] * v;
-                s5 += cfs[5][u] * v;
             }
         }
-    }
-    if (!act) return;
-    if (KIND == 0) {
-        o[a] = s0;
-        o[(size_t) 3 * na + a] = s3;
-        o[(size_t) 4 * na + a] = s4;
-        o[(size_t) 5 * na + a] = s5;
-        o[(size_t) 1 * na + a] = (s1 + s2) / 2.;
-        o[(size_t) 2 * na + a] = (s1 - s2) / 2.;
-    } else {
-        o[a] = s0;
-        o[(size_t) 1 * na + a] = s1;
-        o[(size_t) 2 * na + a] = s2;
-        o[(size_t) 3 * na + a] = s3;
-        o[(size_t) 4 * na + a] = s4;
-        o[(size_t) 5 * na + a] = -s5;
+        if (act) {
+#pragma unroll
+            for (int g = 0; g < CG; ++g) {
+                if (g >= ng) break;
+                double *o = out + C.pf_out_off + (size_t) (g0 + g) * 6 * na;
+                if (KIND == 0) {
+                    o[a] = s[g][0];
+                    o[(size_t) 3 * na + a] = s[g][3];
+                    o[(size_t) 4 * na + a] = s[g][4];
+                    o[(size_t) 5 * na + a] = s[g][5];
+                    o[(size_t) 1 * na + a] = (s[g][1] + s[g][2]) / 2.;
+                    o[(size_t) 2 * na + a] = (s[g][1] - s[g][2]) / 2.;
+                } else {
+                    o[a] = s[g][0];
+                    o[(size_t) 1 * na + a] = s[g][1];
+                    o[(size_t) 2 * na + a] = s[g][2];
+                    o[(size_t) 3 * na + a] = s[g][3];
+                    o[(size_t) 4 * na + a] = s[g][4];
+                    o[(size_t) 5 * na + a] = -s[g][5];
+                }
+            }
+        }
     }
 }
 
@@ -1322,10 +1347,17 @@ int launch_expand(cudaStream_t s, const DevBatch &B, int kind, long long nck,
 int launch_phase_user(cudaStream_t s, const DevBatch &B, int kind, long long total, const long long *start,
                       const double *coefs, const int *trunc, double *pf_out) {
     if (total <= 0) return 0;
-    if (kind == 0)
-        k_phase_user<0><<<(unsigned) total, PU_T, 0, s>>>(B, start, coefs, trunc, pf_out);
-    else
-        k_phase_user<1><<<(unsigned) total, PU_T, 0, s>>>(B, start, coefs, trunc, pf_out);
+    const int ncol = 1 + B.nd;
+    const unsigned nb = (unsigned) total;
+    if (kind == 0) {
+        if (ncol == 1) k_phase_user<0, 1><<<nb, PU_T, 0, s>>>(B, start, coefs, trunc, pf_out);
+        else if (ncol <= 3) k_phase_user<0, 3><<<nb, PU_T, 0, s>>>(B, start, coefs, trunc, pf_out);
+        else k_phase_user<0, 5><<<nb, PU_T, 0, s>>>(B, start, coefs, trunc, pf_out);
+    } else {
+        if (ncol == 1) k_phase_user<1, 1><<<nb, PU_T, 0, s>>>(B, start, coefs, trunc, pf_out);
+        else if (ncol <= 3) k_phase_user<1, 3><<<nb, PU_T, 0, s>>>(B, start, coefs, trunc, pf_out);
+        else k_phase_user<1, 5><<<nb, PU_T, 0, s>>>(B, start, coefs, trunc, pf_out);
+    }
     LMIEB_CUDA_TRY(cudaGetLastError());
     return 0;
 }

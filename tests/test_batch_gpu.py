@@ -109,6 +109,24 @@ def test_pipelined_batch_matches_one_part():
         assert not bad, (i, bad)
 
 
+def test_results_in_pieces_match_single_solves():
+    """A one-part batch whose results (about 40 MB) come back in several
+    pieces of cases, each unpacked while the next is copied: every case as
+    when solved alone."""
+    import lmie_b200
+    lib = lmie_b200.library()
+    cases = workloads.batched_uneven(512)
+    try:
+        lib.lmieb_set_pipeline(1)
+        got = abi.solve_batch(lib, cases, n_threads=8)
+    finally:
+        lib.lmieb_set_pipeline(0)
+    for i in range(0, len(cases), 7):
+        _assert_close(got[i], libs.run_product(cases[i]), 1e-12, f"case {i}")
+    for i, g in enumerate(got):
+        assert g.rc == 0 and np.isfinite(g.gc).all() and np.isfinite(g.pf).all(), i
+
+
 def test_autotune_picks_a_candidate_and_keeps_results():
     import ctypes as C
     import bench
