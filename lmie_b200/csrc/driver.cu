@@ -714,8 +714,30 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     }
     L.pf_total = pf_start[ncase];
     long long part_total = 0;
-    auto by_cost = [](const std::pair<double, AngItem> &a, const std::pair<double, AngItem> &b) {
-        return a.first > b.first;
+    // Items go out largest first, so that the long ones do not end the stage
+    // alone.  The order only schedules the work (every item writes its own
+    // partial-sum slot, reduced in group order), so cost classes of 2^(1/4)
+    // are enough: a counting sort, stable within a class.
+    auto largest_first = [](const std::vector<std::pair<double, AngItem>> &tmp, std::vector<AngItem> &out) {
+        constexpr int NB = 256;
+        static std::vector<unsigned char> cls;
+        cls.resize(tmp.size());
+        size_t cnt[NB] = {};
+        for (size_t i = 0; i < tmp.size(); ++i) {
+            const double c = tmp[i].first;
+            int b = 0;
+            if (c > 1.) {
+                int ex;
+                const double m = frexp(c, &ex);              // c = m 2^ex, m in [0.5, 1)
+                b = std::min(NB - 1, 4 * ex + (int) ((m - .5) * 8.));
+            }
+            cls[i] = (unsigned char) (NB - 1 - b);           // largest class first
+            ++cnt[cls[i]];
+        }
+        size_t at[NB], run = out.size();
+        for (int b = 0; b < NB; ++b) { at[b] = run; run += cnt[b]; }
+        out.resize(run);
+        for (size_t i = 0; i < tmp.size(); ++i) out[at[cls[i]]++] = tmp[i].second;
     };
     // coefficient offsets of the radii whose coefficients K1 writes in FP64
     // (all radii, or with split precision those of the FP64 cases)
@@ -793,8 +815,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
                 for (int t = 0; t < xt; ++t) tmp.push_back({cost, AngItem{k, t, g, gs[g], gs[g + 1]}});
             }
         }
-        std::stable_sort(tmp.begin(), tmp.end(), by_cost);
-        for (auto &e : tmp) ang.push_back(e.second);
+        largest_first(tmp, ang);
     }
     {
         // FP64 K3 over the remaining cases: radius ranges of roughly equal sum of n1
@@ -831,8 +852,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
                     tmp.push_back({cost, it});
                 }
         }
-        std::stable_sort(tmp.begin(), tmp.end(), by_cost);
-        for (auto &e : tmp) (L.tc ? ang64 : ang).push_back(e.second);
+        largest_first(tmp, L.tc ? ang64 : ang);
     }
     L.n_ang = (int) ang.size();
     L.n_ang64 = (int) ang64.size();

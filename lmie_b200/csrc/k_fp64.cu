@@ -940,8 +940,9 @@ __global__ void __launch_bounds__(EX_TMAX) k_exp_tile(DevBatch B, const ExpItem 
                                                    double *__restrict__ exq) {
     constexpr int NF = KIND == 0 ? 4 : 1;
     extern __shared__ double sm[];
+    constexpr int NM = KIND == 0 ? 8 : 6;                  // folded moments per column and node pair
     double *P = sm;                                        // [NF][EX_LT][EX_AT + 1]
-    double *Bv = P + NF * EX_LT * (EX_AT + 1);             // [ncol][12][EX_AT]
+    double *Bv = P + NF * EX_LT * (EX_AT + 1);             // [ncol][NM][EX_AT][2 order parities]
     const ExpItem it = items[blockIdx.x];
     const DevCase &C = B.cs[it.c];
     const int nh = C.nh, nq = C.n_qang, ncf = C.n_coef;
@@ -949,7 +950,7 @@ __global__ void __launch_bounds__(EX_TMAX) k_exp_tile(DevBatch B, const ExpItem 
     const int l0 = it.lt * EX_LT, lt = min(EX_LT, ncf - l0);
     const int i0 = it.at * EX_AT;
     const double *mup = B.mu_pool + C.mu_off, *wqp = mup + nq;
-    double *rcs = Bv + (size_t) ncol * 12 * EX_AT;         // [8 EX_LT] recurrence coefficients of the tile
+    double *rcs = Bv + (size_t) ncol * NM * EX_AT * 2;     // [8 EX_LT] recurrence coefficients of the tile
     for (int t = threadIdx.x; t < 8 * lt; t += blockDim.x) rcs[t] = B.rc[8 * (size_t) l0 + t];
     __syncthreads();
 
@@ -973,29 +974,43 @@ __global__ void __launch_bounds__(EX_TMAX) k_exp_tile(DevBatch B, const ExpItem 
             for (int u = 0; u < lt; ++u) Pf[u * (EX_AT + 1)] = 0.;
         }
     }
-    // weighted moments of the node pairs: b1 at the mirror node -mu_i, b2 at +mu_i
+    // weighted moments of the node pairs (u* at the mirror node -mu_i, v* at
+    // +mu_i), folded for either order parity: s = (-1)^l multiplies the mirror
+    // node's terms.  The two parities sit side by side, so the lanes of a warp
+    // (consecutive orders) read one 16-byte pair.
     for (int t = threadIdx.x; t < ncol * EX_AT; t += blockDim.x) {
         const int col = t / EX_AT, ia = t % EX_AT, i = i0 + ia;
-        double *bv = Bv + (size_t) col * 12 * EX_AT + ia;
+        double u0 = 0., u1 = 0., u2 = 0., u3 = 0., v0 = 0., v1 = 0., v2 = 0., v3 = 0.;
         if (i < nh) {
             const int i1 = nh - 1 - i, i2 = nh + i;
             const double w = wqp[i2];
             const double *F = pfn + C.pf_off + (size_t) col * 4 * nq;
-            const double u0 = F[i1] * w, u1 = F[nq + i1] * w, u2 = F[2 * nq + i1] * w, u3 = F[3 * nq + i1] * w;
-            const double v0 = F[i2] * w, v1 = F[nq + i2] * w, v2 = F[2 * nq + i2] * w, v3 = F[3 * nq + i2] * w;
+            u0 = F[i1] * w; u1 = F[nq + i1] * w; u2 = F[2 * nq + i1] * w; u3 = F[3 * nq + i1] * w;
+            v0 = F[i2] * w; v1 = F[nq + i2] * w; v2 = F[2 * nq + i2] * w; v3 = F[3 * nq + i2] * w;
+        }
+        double *bv = Bv + ((size_t) col * NM * EX_AT + ia) * 2;
+#pragma unroll
+        for (int p = 0; p < 2; ++p) {
+            const double sg = p ? -1. : 1.;
             if (KIND == 0) {
-                bv[0 * EX_AT] = u0; bv[1 * EX_AT] = u0 + u1; bv[2 * EX_AT] = u0 - u1;
-                bv[3 * EX_AT] = u1; bv[4 * EX_AT] = u2;      bv[5 * EX_AT] = u3;
-                bv[6 * EX_AT] = v0; bv[7 * EX_AT] = v0 + v1; bv[8 * EX_AT] = v0 - v1;
-                bv[9 * EX_AT] = v1; bv[10 * EX_AT] = v2;     bv[11 * EX_AT] = v3;
+                // acc0 = p00 m0; acc1 = p2-2 m1 + p2+2 m2; acc2 = p2+2 m3 + p2-2 m4;
+                // acc3 = p00 m5; acc4 = p0+2 m6; acc5 = p0+2 m7
+                bv[(0 * EX_AT) * 2 + p] = sg * u0 + v0;
+                bv[(1 * EX_AT) * 2 + p] = sg * (u0 + u1);
+                bv[(2 * EX_AT) * 2 + p] = v0 + v1;
+                bv[(3 * EX_AT) * 2 + p] = sg * (u0 - u1);
+                bv[(4 * EX_AT) * 2 + p] = v0 - v1;
+                bv[(5 * EX_AT) * 2 + p] = sg * u1 + v1;
+                bv[(6 * EX_AT) * 2 + p] = sg * u2 + v2;
+                bv[(7 * EX_AT) * 2 + p] = sg * u3 + v3;
             } else {
-                bv[0 * EX_AT] = u0; bv[1 * EX_AT] = u0; bv[2 * EX_AT] = u1;
-                bv[3 * EX_AT] = u1; bv[4 * EX_AT] = u2; bv[5 * EX_AT] = u3;
-                bv[6 * EX_AT] = v0; bv[7 * EX_AT] = v0; bv[8 * EX_AT] = v1;
-                bv[9 * EX_AT] = v1; bv[10 * EX_AT] = v2; bv[11 * EX_AT] = v3;
+                bv[(0 * EX_AT) * 2 + p] = sg * u0 + v0;
+                bv[(1 * EX_AT) * 2 + p] = sg * u0 + v0;
+                bv[(2 * EX_AT) * 2 + p] = sg * u1 + v1;
+                bv[(3 * EX_AT) * 2 + p] = sg * u1 + v1;
+                bv[(4 * EX_AT) * 2 + p] = sg * u2 + v2;
+                bv[(5 * EX_AT) * 2 + p] = sg * u3 + v3;
             }
-        } else {
-            for (int q = 0; q < 12; ++q) bv[q * EX_AT] = 0.;
         }
     }
     __syncthreads();
@@ -1003,8 +1018,7 @@ __global__ void __launch_bounds__(EX_TMAX) k_exp_tile(DevBatch B, const ExpItem 
     for (int t = threadIdx.x; t < ncol * lt; t += blockDim.x) {
         const int col = t / lt, u = t % lt;
         const int l = l0 + u;
-        const double s = (l & 1) ? -1. : 1.;
-        const double *bv = Bv + (size_t) col * 12 * EX_AT;
+        const double *bv = Bv + (size_t) col * NM * EX_AT * 2 + (l & 1);
         double acc[6] = {0., 0., 0., 0., 0., 0.};
         if (KIND == 0) {
             const double *P00 = P + (size_t) (0 * EX_LT + u) * (EX_AT + 1);
@@ -1014,20 +1028,24 @@ __global__ void __launch_bounds__(EX_TMAX) k_exp_tile(DevBatch B, const ExpItem 
 #pragma unroll 4
             for (int ia = 0; ia < EX_AT; ++ia) {
                 const double p00 = P00[ia], p02 = P02[ia], p22 = P22[ia], p2m = P2m[ia];
-                acc[0] += p00 * (bv[0 * EX_AT + ia] * s + bv[6 * EX_AT + ia]);
-                acc[1] += p2m * bv[1 * EX_AT + ia] * s + p22 * bv[7 * EX_AT + ia];
-                acc[2] += p22 * bv[2 * EX_AT + ia] * s + p2m * bv[8 * EX_AT + ia];
-                acc[3] += p00 * (bv[3 * EX_AT + ia] * s + bv[9 * EX_AT + ia]);
-                acc[4] += p02 * (bv[4 * EX_AT + ia] * s + bv[10 * EX_AT + ia]);
-                acc[5] += p02 * (bv[5 * EX_AT + ia] * s + bv[11 * EX_AT + ia]);
+                const double *m = bv + 2 * ia;
+                acc[0] += p00 * m[0 * EX_AT * 2];
+                acc[1] += p2m * m[1 * EX_AT * 2];
+                acc[1] += p22 * m[2 * EX_AT * 2];
+                acc[2] += p22 * m[3 * EX_AT * 2];
+                acc[2] += p2m * m[4 * EX_AT * 2];
+                acc[3] += p00 * m[5 * EX_AT * 2];
+                acc[4] += p02 * m[6 * EX_AT * 2];
+                acc[5] += p02 * m[7 * EX_AT * 2];
             }
         } else {
             const double *Y = P + (size_t) u * (EX_AT + 1);
 #pragma unroll 4
             for (int ia = 0; ia < EX_AT; ++ia) {
                 const double y = Y[ia];
+                const double *m = bv + 2 * ia;
 #pragma unroll
-                for (int e = 0; e < 6; ++e) acc[e] += y * (bv[e * EX_AT + ia] * s + bv[(6 + e) * EX_AT + ia]);
+                for (int e = 0; e < 6; ++e) acc[e] += y * m[e * EX_AT * 2];
             }
         }
         double *o = exq + C.ex_off + ((size_t) it.at * ncol + col) * 6 * ncf + l;
@@ -1224,7 +1242,8 @@ int run_expand(cudaStream_t s, const DevBatch &B, long long nck, const long long
                double *ckpt, double *exq, double *coefs, int *trunc) {
     constexpr int NF = KIND == 0 ? 4 : 1;
     constexpr int SMAX = 200 * 1024;
-    const size_t sm = sizeof(double) * ((size_t) NF * EX_LT * (EX_AT + 1) + (size_t) (1 + B.nd) * 12 * EX_AT +
+    constexpr int NM = KIND == 0 ? 8 : 6;
+    const size_t sm = sizeof(double) * ((size_t) NF * EX_LT * (EX_AT + 1) + (size_t) (1 + B.nd) * NM * EX_AT * 2 +
                                         (size_t) 8 * EX_LT);
     if (sm > (size_t) SMAX) {
         fprintf(stderr, "ERROR: expansion tile needs %zu bytes of shared memory (too many derivatives)\n", sm);
