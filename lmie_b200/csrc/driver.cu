@@ -860,14 +860,19 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
 
     // ---- expansion work items and offsets ----
     static std::vector<ExpItem> ex;          // kept between calls, like the per-radius arrays
-    ex.clear();
     std::vector<long long> ck_gc(ncase + 1, 0), ck_lc(ncase + 1, 0), fin_start(ncase + 1, 0);
+    std::vector<long long> exb(ncase + 1, 0);           // first item of each case
     long long ck_total = 0, ex_total = 0;
+    auto ex_tiles = [&](const DevCase &C, int &nlt, int &nat) {
+        const bool on = (L.want_gc || L.want_lc) && C.n_qang > 0;
+        nlt = on ? (C.n_coef + EX_LT - 1) / EX_LT : 0;
+        nat = on ? (C.nh + EX_AT - 1) / EX_AT : 0;
+        return on;
+    };
     for (int k = 0; k < ncase; ++k) {
         DevCase &C = cs[k];
-        const bool on = (L.want_gc || L.want_lc) && C.n_qang > 0;
-        const int nlt = on ? (C.n_coef + EX_LT - 1) / EX_LT : 0;
-        const int nat = on ? (C.nh + EX_AT - 1) / EX_AT : 0;
+        int nlt, nat;
+        const bool on = ex_tiles(C, nlt, nat);
         ck_gc[k + 1] = ck_gc[k] + (on ? 4LL * C.nh : 0);
         ck_lc[k + 1] = ck_lc[k] + (on ? 1LL * C.nh : 0);
         fin_start[k + 1] = fin_start[k] + (on ? (long long) ncol * C.n_coef : 0);
@@ -875,9 +880,16 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         ck_total += (long long) nlt * 4 * C.nh * 2;
         C.ex_off = ex_total;
         ex_total += (long long) nat * ncol * 6 * C.n_coef;
-        for (int lt = 0; lt < nlt; ++lt)
-            for (int at = 0; at < nat; ++at) ex.push_back(ExpItem{k, lt, at});
+        exb[k + 1] = exb[k] + (long long) nlt * nat;
     }
+    ex.resize((size_t) exb[ncase]);
+    parallel_for(ncase, 16, [&](int k) {
+        int nlt, nat;
+        ex_tiles(cs[k], nlt, nat);
+        ExpItem *e = ex.data() + exb[k];
+        for (int lt = 0; lt < nlt; ++lt)
+            for (int at = 0; at < nat; ++at) *e++ = ExpItem{k, lt, at};
+    });
     L.nck_gc = ck_gc[ncase];
     L.nck_lc = ck_lc[ncase];
     L.nfin = fin_start[ncase];
