@@ -376,8 +376,39 @@ static int share_radii(case_job *j, int n, int nd, int nd1) {
  * src/lmie_schedule.c:1004-1072, src/lmie_core.c:263-292): size distribution,
  * moments, derivative split, per-radius size parameters and truncation,
  * user angles; fills j->P and points j->R at the output staging. */
+/* cos(theta_i) of n equally spaced user angles theta_i = i 180/(n-1) degrees
+ * (the reference's arithmetic, misc/rtutil_scat_int.c:487-503) */
+static void user_cosines_fill(int n, double *mu) {
+     const double d = 180. / (n - 1);
+     int i;
+     for (i = 0; i < n; ++i)
+          mu[i] = cos((i * d) * (M_PI / 180.0));
+}
+
+/* The cosines of one count, computed once per count up to MU_CACHE_MAX and
+ * kept: the cases of a batch share their user angles.  NULL above the limit
+ * (the caller fills its own array). */
+#define MU_CACHE_MAX 4096
+static pthread_mutex_t mu_cache_mu = PTHREAD_MUTEX_INITIALIZER;
+static double *mu_cache[MU_CACHE_MAX + 1];
+
+static const double *user_cosines(int n) {
+     double *p;
+     if (n < 1 || n > MU_CACHE_MAX)
+          return NULL;
+     pthread_mutex_lock(&mu_cache_mu);
+     p = mu_cache[n];
+     if (!p && (p = (double *) malloc(sizeof(double) * (size_t) n)) != NULL) {
+          user_cosines_fill(n, p);
+          mu_cache[n] = p;
+     }
+     pthread_mutex_unlock(&mu_cache_mu);
+     return p;
+}
+
 static int job_prepare(case_job *j) {
      int n, nd = j->n_derivs > 0 ? j->n_derivs : 0, nd1 = 0, nd2 = 0, i, k;
+     const double *mu_user = NULL;
      int n1, n_qang, ncol;
      double x2;
      double complex m;
@@ -523,13 +554,17 @@ static int job_prepare(case_job *j) {
              device layer, which keeps the last set it saw on the device */
      }
 
-     /* user angles (reference misc/rtutil_scat_int.c:487-503,580) */
+     /* user angles (reference misc/rtutil_scat_int.c:487-503,580): the
+        caller's theta, and their cosines shared by every case of that count */
      if (j->calc_pf) {
           double d = 180. / (j->n_angles - 1);
-          j->mu_user = lmieb_arr1(j->n_angles);
-          for (i = 0; i < j->n_angles; ++i) {
+          for (i = 0; i < j->n_angles; ++i)
                j->theta[i] = i * d;
-               j->mu_user[i] = cos(j->theta[i] * (M_PI / 180.0));
+          mu_user = user_cosines(j->n_angles);
+          if (!mu_user) {
+               j->mu_user = lmieb_arr1(j->n_angles);
+               user_cosines_fill(j->n_angles, j->mu_user);
+               mu_user = j->mu_user;
           }
      }
 
@@ -544,7 +579,7 @@ static int job_prepare(case_job *j) {
      j->P.want_gc = j->gc != NULL; j->P.want_lc = j->lc != NULL;
      j->P.pf_from = j->calc_pf ? (j->calc_gc ? 1 : 2) : 0;
      j->P.n_angles = j->calc_pf ? j->n_angles : 0;
-     j->P.mu_user = j->mu_user;
+     j->P.mu_user = mu_user;
      j->P.accuracy = j->accuracy;
      j->P.save_control = j->save_control;
      j->P.acc_mode = j->acc_mode;
