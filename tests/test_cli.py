@@ -109,6 +109,9 @@ def test_cli_help_and_version(tmp_path):
     (["-dist", "gamma", "2", "0.1", "0.01", "6", "-lambda", "0.5", "-m", "1.3", "0", "-n_int2", "1"], "-n_quad"),
     (["-dist", "mono", "1", "-lambda", "0.5", "-m", "1.3", "0", "-n_int2", "1", "-n_quad", "1",
       "-check_cbak", "1e-5"], "must use -pf when using -check_cbak"),
+    (["-dist", "mono", "1", "-lambda", "0.5", "-m", "1.3", "0", "-n_int2", "1", "-n_quad", "1",
+      "-check_g", "1e-5"], "must use -pf when using -check_g"),
+    (["-dist", "modified_power_law", "-3", "0.1", "2", "-lambda", "0.5", "-m", "1.3", "0"], "-n_int1"),
     (["-dist", "nosuch"], "invalid distribution name"),
     (["-dist_l", "0"], "must specify -dist before -dist_l"),
     (["-m_l", "1", "0"], "Must specifiy -derivs"),
