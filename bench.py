@@ -195,29 +195,77 @@ def _cpu_library():
     return lib, "port"
 
 
-def cpu_sample_rate(cases, budget_s: float) -> dict:
-    """Solves/s of the CPU implementation over a bounded sample of `cases`
-    (taken in a seeded order from the whole batch, so sizes are represented)."""
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
+def _seeded_order(n: int):
+    import random
+    order = list(range(n))
+    random.Random(workloads.SEED).shuffle(order)
+    return order
+
+
+def _cpu_solve(lib, kind, case, n_threads):
+    r = abi.solve(lib, case, n_threads=n_threads) if kind == "reference" else abi.solve(lib, case, kind="oracle")
+    if r.rc != 0:
+        raise RuntimeError("CPU solve failed")
+
+
+def cpu_radius_parallel(cases, order, budget_s: float) -> dict:
+    """The reference's own threading: one case after another, each
+    lmie_solution() spreading its radii over all host threads."""
     lib, kind = _cpu_library()
     threads = os.cpu_count() if kind == "reference" else 1
-    import random
-    order = list(range(len(cases)))
-    random.Random(workloads.SEED).shuffle(order)
-    t_start = time.perf_counter()
-    done, busy = 0, 0.0
+    t0 = time.perf_counter()
+    done = 0
     for i in order:
-        c = cases[i]
-        t0 = time.perf_counter()
-        r = abi.solve(lib, c, n_threads=threads) if kind == "reference" else abi.solve(lib, c, kind="oracle")
-        busy += time.perf_counter() - t0
-        if r.rc != 0:
-            raise RuntimeError("CPU solve failed")
+        _cpu_solve(lib, kind, cases[i], threads)
         done += 1
-        if time.perf_counter() - t_start > budget_s:
+        if time.perf_counter() - t0 > budget_s:
             break
-    return {"value": done / busy, "unit": UNIT, "cores": threads, "kind": kind,
-            "sample": f"{done} of the {len(cases)} batch cases in seeded random order "
-                      f"({busy:.1f} s), lmie_solution with n_threads={threads}, one case after another"}
+    wall = time.perf_counter() - t0
+    return {"value": done / wall, "unit": UNIT, "cores": threads, "kind": kind, "cases": done, "seconds": wall,
+            "mode": f"radius-parallel: one case after another, lmie_solution(n_threads={threads})"}
+
+
+def cpu_case_parallel(cases, order) -> dict:
+    """One case per host thread: every host thread takes the next case of
+    `order` and solves it with lmie_solution(n_threads=1) (ctypes releases the
+    interpreter lock during the call); wall time until all are done."""
+    import concurrent.futures as cf
+    lib, kind = _cpu_library()
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(max_workers=threads) as ex:
+        list(ex.map(lambda i: _cpu_solve(lib, kind, cases[i], 1), order))
+    wall = time.perf_counter() - t0
+    return {"value": len(order) / wall, "unit": UNIT, "cores": threads, "kind": kind, "cases": len(order),
+            "seconds": wall, "mode": "case-parallel: one case per host thread, lmie_solution(n_threads=1)"}
+
+
+def cpu_baseline(cases, budget_s: float = 20.0) -> dict:
+    """The CPU implementation on the host cores in both of its parallel forms
+    over bounded samples of the batch (seeded order, so sizes are
+    represented); the faster one is the baseline value."""
+    order = _seeded_order(len(cases))
+    radius = cpu_radius_parallel(cases, order, budget_s / 2)
+    n_case = max(len(order) // 16, min(len(order), int(radius["value"] * budget_s / 2)))
+    case = cpu_case_parallel(cases, order[:n_case])
+    best = max((radius, case), key=lambda v: v["value"])
+    return {"value": best["value"], "unit": UNIT, "cores": best["cores"], "kind": best["kind"],
+            "cpu_model": cpu_model(),
+            "sample": f"{best['cases']} of the {len(cases)} batch cases in seeded random order "
+                      f"({best['seconds']:.1f} s), {best['mode']}",
+            "variants": {"radius_parallel": radius, "case_parallel": case}}
 
 
 def _relmax(a, b) -> float:
@@ -372,21 +420,57 @@ def adjoint_measurement(lib, steps: int) -> dict:
     }
 
 
+def bench_config(world: int, scaling: str) -> dict:
+    return {"workload": WORKLOAD, "n_cases": N_CASES, "n_derivs": 4,
+            "parallelism": (f"independent batches x{world}" if scaling == "weak" else
+                            f"one batch in {world} cost-balanced case ranges"),
+            "l2": "flushed (256 MiB write) before every timed device step; "
+                  "the batch's working set (~8 GB) exceeds L2 in any case"}
+
+
+REF_STEP_CASES = 256
+
+
 def run_reference_arm(args) -> int:
+    """The reference's CPU lmie_solution on the host cores.  Step i solves the
+    REF_STEP_CASES cases at positions [i m, (i + 1) m) of the batch's seeded
+    order (wrapping around), one case per host thread (the faster of the
+    reference's two parallel forms on this workload, both measured in the
+    warm-up); steps and ms_per_step are the ones that ran."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     cases = workloads.batched_uneven(N_CASES)
-    budget = max(10.0, 3.0 * args.steps)
-    cpu = cpu_sample_rate(cases, budget)
-    value = cpu["value"]
+    order = _seeded_order(N_CASES)
+    m = REF_STEP_CASES
+
+    def step_cases(i):
+        return [order[(i * m + j) % N_CASES] for j in range(m)]
+
+    radius = None
+    for w in range(args.warmup):
+        if w == 0:
+            radius = cpu_radius_parallel(cases, step_cases(w), 10.0)
+        else:
+            cpu_case_parallel(cases, step_cases(w))
+    times = []
+    for i in range(args.steps):
+        times.append(cpu_case_parallel(cases, step_cases(args.warmup + i))["seconds"])
+    total = sum(times)
+    value = m * args.steps / total
+    lib, kind = _cpu_library()
+    threads = os.cpu_count() or 1
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": N_CASES / value * 1e3,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded generator)",
-        "config": {"workload": WORKLOAD, "n_cases": N_CASES, "n_derivs": 4},
-        "cpu_baseline": cpu,
+        "config": bench_config(args.gpus, "weak"),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "cpu_model": cpu_model(),
+                         "sample": f"{args.steps} steps of {m} cases each ({m * args.steps} solves, "
+                                   f"{total:.1f} s) taken in the batch's seeded order, one case per host "
+                                   "thread, lmie_solution(n_threads=1)",
+                         "variants": {"radius_parallel": radius}},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -541,15 +625,14 @@ def run_b200(args) -> int:
                 "peak_source": "dense tf32 = half of the measured bf16 burst in MEASURED_PEAKS.json",
                 "tensor_flops_per_launch": 3 * flops[0], "ms_per_launch": split_ang_ms},
         }
-        n_plain = 256
-        plain_batch = CBatch(lib, cases[:n_plain])
-        plain_batch.solve_each(threads, 16)
+        # the plain form on the same cases as the batched numbers
+        batch.solve_each(threads, 16)
         t1 = time.perf_counter()
-        if plain_batch.solve_each(threads) != 0:
+        if batch.solve_each(threads) != 0:
             raise RuntimeError("lmie_solution failed")
         plain_s = time.perf_counter() - t1
-        plain = {"value": n_plain / plain_s, "unit": UNIT, "dtype": "f64",
-                 "sample": f"the first {n_plain} cases of the batch, one lmie_solution() call each"}
+        plain = {"value": len(cases) / plain_s, "unit": UNIT, "dtype": "f64",
+                 "sample": f"all {len(cases)} cases of the batch, one lmie_solution() call each"}
         adj = adjoint_measurement(lib, 5)
         stress = precision_stress_measurement(lib, threads)
         reweight = save_reweight_measurement(lib)
@@ -568,19 +651,15 @@ def run_b200(args) -> int:
                   "stage_ms": {n: ms_stage[i] / 10 for i, n in enumerate(lmie_b200.STAGES)}}
 
     if rank == 0:
-        cpu = cpu_sample_rate(cases, 20.0) if world == 1 else None
+        cpu = cpu_baseline(cases, 20.0) if world == 1 else None
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
             "scaling": args.scaling, "vs_baseline": None, "dtype": "f64",
             "data": ("synthetic (seeded generator, rank r uses seed + r)" if args.scaling == "weak" else
                      "synthetic (seeded generator, one batch split by estimated cost over the ranks)"),
-            "config": {"workload": WORKLOAD, "n_cases": N_CASES, "n_derivs": 4,
-                       "parallelism": (f"independent batches x{world}" if args.scaling == "weak" else
-                                       f"one batch in {world} cost-balanced case ranges"),
-                       "autotuned": tuned,
-                       "l2": "flushed (256 MiB write) before every timed device step; "
-                             "the batch's working set (~8 GB) exceeds L2 in any case"},
+            "config": bench_config(world, args.scaling),
+            "autotuned": tuned,
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d.value),
                     "d2h_bytes_per_step": int(d2h.value), "host_threads": threads},
             "gpu_launches": int(launches.value) * args.steps,

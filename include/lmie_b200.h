@@ -221,6 +221,9 @@ int lmieb_fp64_peak(double *tflops);
  *
  * Limits: 1 <= n_radii <= 1024 and size parameters 0 < 2 pi r / lambda <= 900;
  * larger requests return -1 with an ERROR line (out-of-range radii get NaN).
+ * The truncation orders n1, n2 of every radius are computed on the host with
+ * the same formulas and libm as in lmie_solution (the radii are copied to the
+ * host, the orders back into the static array below).
  * The work uses a fixed 24 MiB scratch array compiled into the library, which
  * every GPU that loads the library keeps until the process exits; no call
  * allocates or frees device memory.  All calls on a device share that array:

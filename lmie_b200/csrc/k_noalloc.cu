@@ -13,14 +13,24 @@
 //
 // Limits: at most NA_MAX_RADII = 1024 radii per call and size parameters
 // 0 < x = 2 pi r / lambda <= NA_MAX_X = 900 (so n1(x) < NA_MAX_ORDER = 1024);
-// the scratch is 3 * 1024 * 1024 doubles = 24 MiB, and every GPU that loads
-// this library holds it until the process exits.
+// the scratch is 3 * 1024 * 1024 doubles = 24 MiB plus the truncation orders
+// of 1024 radii, and every GPU that loads this library holds it until the
+// process exits.
+//
+// The truncation orders n1, n2 of every radius (reference
+// src/lmie_core.c:18-38) are computed on the host with the host's libm, as
+// everywhere else in this library, and copied into the static array: the
+// device's pow may differ from the host's in the last place and move an
+// (int) cast across an integer.
 #include <cmath>
 #include <cstdio>
 #include <mutex>
 
 #include "dev_common.cuh"
 #include "../../include/lmie_b200.h"
+
+extern "C" int lmieb_calc_n1(double x);
+extern "C" int lmieb_calc_n2(int n1, double zr, double zi);
 
 namespace {
 
@@ -33,12 +43,15 @@ constexpr int NA_MAX_DEVICES = 64;
 // [j * NA_MAX_RADII + i], then D_j (complex) at
 // [NA_MAX_ORDER * NA_MAX_RADII + 2 * (j * NA_MAX_RADII + i)].
 static __device__ __align__(256) double g_noalloc_scratch[(size_t) 3 * NA_MAX_ORDER * NA_MAX_RADII];
+// (n1, n2) of every radius of the call, written by the host before the kernel.
+static __device__ __align__(256) int2 g_noalloc_trunc[NA_MAX_RADII];
 // Index + 1 of a radius whose size parameter is out of range (0: none).
 static __device__ __align__(256) int g_noalloc_error;
 
 struct DeviceSlot {
     bool ready = false;
     double *scratch = nullptr;   // device address of g_noalloc_scratch on this device
+    int2 *trunc = nullptr;       // device address of g_noalloc_trunc on this device
     int *error = nullptr;        // device address of g_noalloc_error on this device
 };
 DeviceSlot g_slots[NA_MAX_DEVICES];
@@ -46,23 +59,22 @@ std::mutex g_slots_mu;
 
 __global__ void __launch_bounds__(128) k_cross_sections_static(int n, const double *__restrict__ radius,
                                                                double lambda, cplx m, cplx minv,
+                                                               const int2 *__restrict__ trunc,
                                                                double *__restrict__ scr, int *err,
                                                                double *__restrict__ out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double x = 2. * LMIEB_PI * radius[i] / lambda;
-    if (!(x > 0.) || !(x <= NA_MAX_X)) {
+    const int2 nn = trunc[i];
+    const int n1 = nn.x, n2 = nn.y;
+    if (!(x > 0.) || !(x <= NA_MAX_X) || n1 < 1 || n1 >= NA_MAX_ORDER || n2 < n1) {
         // out of range: record it, write NaN, touch no scratch
         atomicMax(err, i + 1);
         const double nan = __longlong_as_double(0x7ff8000000000000LL);
         for (int q = 0; q < 4; ++q) out[(size_t) q * n + i] = nan;
         return;
     }
-    const int n1 = (int) (x + 4.05 * pow(x, 1. / 3.) + 8);
     const cplx z = mk(m.re * x, m.im * x);
-    const double az = hypot(z.re, z.im);
-    const double t2 = n1 > az ? (double) n1 : az;
-    const int n2 = (int) (t2 + 6.40 * pow(t2, 1. / 3.) + 8);
     const double xinv = 1. / x;
     const cplx zinv = 1. / z;
     double *R = scr;
@@ -140,6 +152,7 @@ int device_slot(DeviceSlot **slot) {
     DeviceSlot &s = g_slots[dev];
     if (!s.ready) {
         LMIEB_CUDA_TRY(cudaGetSymbolAddress((void **) &s.scratch, g_noalloc_scratch));
+        LMIEB_CUDA_TRY(cudaGetSymbolAddress((void **) &s.trunc, g_noalloc_trunc));
         LMIEB_CUDA_TRY(cudaGetSymbolAddress((void **) &s.error, g_noalloc_error));
         s.ready = true;
     }
@@ -168,9 +181,25 @@ extern "C" int lmie_cross_sections_noalloc(int n_radii, const double *radius, do
     if (device_slot(&slot)) return -1;
     cudaStream_t s = (cudaStream_t) stream;
     const cplx m = mk(mr, -mi);
+    // truncation orders on the host (host libm), through arrays on this
+    // thread's stack: the radii come down, n1 and n2 go up into the static array
+    double rad[NA_MAX_RADII];
+    int2 nn[NA_MAX_RADII];
+    LMIEB_CUDA_TRY(cudaMemcpyAsync(rad, radius, sizeof(double) * n_radii, cudaMemcpyDeviceToHost, s));
+    LMIEB_CUDA_TRY(cudaStreamSynchronize(s));
+    for (int i = 0; i < n_radii; ++i) {
+        const double x = 2. * LMIEB_PI * rad[i] / lambda;
+        nn[i] = make_int2(0, 0);
+        if (x > 0. && x <= NA_MAX_X) {
+            const int n1 = lmieb_calc_n1(x);
+            nn[i] = make_int2(n1, lmieb_calc_n2(n1, mr * x, -mi * x));
+        }
+    }
+    LMIEB_CUDA_TRY(cudaMemcpyAsync(slot->trunc, nn, sizeof(int2) * n_radii, cudaMemcpyHostToDevice, s));
     LMIEB_CUDA_TRY(cudaMemsetAsync(slot->error, 0, sizeof(int), s));
     k_cross_sections_static<<<ceil_div(n_radii, 128), 128, 0, s>>>(n_radii, radius, lambda, m, 1. / m,
-                                                                    slot->scratch, slot->error, out);
+                                                                    slot->trunc, slot->scratch, slot->error,
+                                                                    out);
     LMIEB_CUDA_TRY(cudaGetLastError());
     int bad = 0;
     LMIEB_CUDA_TRY(cudaMemcpyAsync(&bad, slot->error, sizeof(int), cudaMemcpyDeviceToHost, s));

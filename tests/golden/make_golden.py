@@ -17,6 +17,7 @@ from __future__ import annotations
 
 import dataclasses
 import json
+import os
 import re
 import subprocess
 import sys
@@ -31,7 +32,7 @@ sys.path.insert(0, str(ROOT / "tests"))
 from cases import all_cases, example_case  # noqa: E402
 import libs  # noqa: E402
 
-REF_TREE = Path("/root/reference")
+REF_TREE = Path(os.environ.get("LMIE_REFERENCE", "/root/reference"))
 OUT = ROOT / "tests" / "golden"
 
 

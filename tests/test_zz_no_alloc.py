@@ -61,6 +61,25 @@ def test_noalloc_matches_lmie_solution_on_two_calls():
             assert libs.relmax(got[q], want[q]) < TOL, (lam, name)
 
 
+def test_noalloc_dense_size_parameters():
+    """Size parameters packed densely over (0, 900], 1024 radii per call: the
+    truncation orders are the host's at every one of them, so the results
+    are lmie_solution's (one batch call of SIZE_DIST_MONO cases)."""
+    lib = _lib()
+    lam, mr, mi = 0.55, 1.38, 3e-4
+    x = np.concatenate([np.geomspace(1e-3, 900.0, 1024), np.linspace(0.45, 900.0, 1024)])
+    radii = x * lam / (2.0 * np.pi)
+    cases = [abi.Case(dist="mono", lam=lam, mr=mr, mi=mi, a1=float(r), r1=float(r), r2=float(r),
+                      calc_gc=0, calc_pf=0) for r in radii]
+    res = abi.solve_batch(libs.product(), cases, n_threads=8)
+    want = np.array([[r.scalars[k] for r in res] for k in NAMES])
+    assert all(r.rc == 0 for r in res)
+    for part in (slice(0, 1024), slice(1024, 2048)):
+        got = _via_noalloc(lib, lam, mr, mi, radii[part])
+        for q, name in enumerate(NAMES):
+            assert libs.relmax(got[q], want[q, part]) < TOL, name
+
+
 def test_noalloc_rejects_requests_beyond_its_limits():
     import torch
     lib = _lib()
