@@ -12,19 +12,27 @@ expansion and 181-angle phase matrix.  Inputs are synthetic; nothing is read
 from disk.
 
   value  device time of the batch on inputs resident in HBM (the L2 is
-         flushed before every step), solves/s over all ranks;
-  e2e    the same batch through the public C call lmie_solution_batch() on
+         flushed before every step), solves/s over all ranks, with the
+         angular S1/S2 contraction as an exact fixed-point sum on the int8
+         tensor cores (lmie_solution_batch2(..., LMIEB_PRECISION_INT8): every
+         output within 1e-9 of the FP64 form and the same truncation n_coef,
+         cases near the truncation threshold solved again in FP64);
+  e2e    the same batch through the public C call lmie_solution_batch2() on
          host buffers: host preparation, the host->device and device->host
          copies and the scatter into the caller's lmie_out_data are inside the
          timed region.
 
 The same JSON line carries secondary measurements of the same run:
-  split_tf32x3  the batch with the angular contraction on the tensor cores
-                (lmie_solution_batch2(..., LMIEB_PRECISION_TF32X3)): device and
-                e2e solves/s, stage times, and its measured error against the
-                FP64 form per output array over a sample of the batch;
+  int8_error_vs_fp64  the headline form's error against the FP64 form over
+                the whole batch, per output array and per derivative slice;
+  fp64          the same batch in FP64 throughout (lmie_solution_batch):
+                device and e2e solves/s, stage times, roofline of its K3;
+  split_tf32x3  the batch with the angular contraction in 3xTF32 on the
+                tensor cores (LMIEB_PRECISION_TF32X3, FP32 accumulation):
+                device and e2e solves/s, stage times, and its measured error
+                against the FP64 form per output array over a sample;
   plain         the drop-in form: one lmie_solution() call per case (FP64),
-                e2e solves/s over a sample of the batch;
+                e2e solves/s over every case of the batch;
   single_case   the reference's cloud-droplet case (2000 radii, x_max ~436,
                 4 derivatives) through lmie_solution();
   adjoint       the retrieval workload (256 wavelengths sharing 64 bins x 32
@@ -37,8 +45,8 @@ The same JSON line carries secondary measurements of the same run:
 With N > 1 (torchrun, one process per GPU) every rank solves its own batch
 (independent cases, no data-path collective): weak scaling.
 `--impl reference` times the reference's own CPU lmie_solution (compiled from
-its sources into oracle/_ref) on all host cores over a bounded sample of the
-same cases, on rank 0 only.
+its sources into oracle/_ref) on all host cores, one case per host thread,
+in steps of 256 of the same cases, on rank 0 only.
 """
 from __future__ import annotations
 
@@ -67,10 +75,10 @@ N_CASES = 4096
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_angular /
 # k_angular_tc launch on this workload: measured with ncu on a 256-case batch
 # of the same generator and scaled by the ratio of angular work (13.33).
-ANGULAR_TRAFFIC = {"fp64": 12.21e9, "tf32x3": 5.15e9}
+ANGULAR_TRAFFIC = {"fp64": 12.21e9, "tf32x3": 5.15e9, "int8": None}
 WORKLOAD = ("batched uneven: 4096 seeded cases (r_eff 0.05-20 um, v_eff 0.02-0.3, lambda 0.34-2.1 um, "
             "mr 1.33-1.60, mi 1e-8-0.1, gamma/log-normal, 100-2000 radii, x_max 0.2-1063), "
-            "4 derivatives each (mr, mi, a1, a2), GSF + 181-angle phase matrix, FP64")
+            "4 derivatives each (mr, mi, a1, a2), GSF + 181-angle phase matrix")
 
 
 def single_case() -> abi.Case:
@@ -311,34 +319,37 @@ def split_errors(lib, cases, n_threads: int) -> dict:
 
 def precision_stress_measurement(lib, n_threads: int, n_cases: int = 8) -> dict:
     """The large-particle configuration (size parameter up to 5000, 8000 radii,
-    10154 Gauss angles, four derivatives) on a sample of its cases: the split
-    form's error per output array against the FP64 form, and both forms'
-    throughput through the public batch call (wall clock, host buffers)."""
+    10154 Gauss angles, four derivatives) on a sample of its cases: each
+    tensor-core form's error per output array against the FP64 form, and the
+    forms' throughput through the public batch call (wall clock, host
+    buffers)."""
     cases = workloads.precision_stress(n_cases)
     lib.lmieb_set_pipeline(0)
     out = {"workload": f"workloads.precision_stress: first {n_cases} of 256 seeded cases "
                        "(gamma, r_eff 150-400 um, x_max 5000, 16x500 radii, 4 derivatives)"}
     res = {}
-    for name, prec in (("fp64", abi.PRECISION_FP64), ("tf32x3", abi.PRECISION_TF32X3)):
+    forms = (("fp64", abi.PRECISION_FP64), ("tf32x3", abi.PRECISION_TF32X3), ("int8", abi.PRECISION_INT8))
+    for name, prec in forms:
         abi.solve_batch(lib, cases[:1], n_threads=n_threads, precision=prec)   # settle buffers
         t0 = time.perf_counter()
         res[name] = abi.solve_batch(lib, cases, n_threads=n_threads, precision=prec)
         out[name] = {"e2e": n_cases / (time.perf_counter() - t0), "unit": UNIT}
-    worst, same = {}, 0
-    for g, r in zip(res["tf32x3"], res["fp64"]):
-        if g.rc != 0 or r.rc != 0:
-            raise RuntimeError("precision-stress solve failed")
-        nc = min(g.n_coef, r.n_coef)
-        err = {"gc": _relmax(g.gc[:, :nc], r.gc[:, :nc]), "gc_l": _relmax(g.gc_l[:, :, :nc], r.gc_l[:, :, :nc])}
-        if g.n_coef == r.n_coef:
-            same += 1
-            err.update(pf=_relmax(g.pf, r.pf), pf_l=_relmax(g.pf_l, r.pf_l))
-        for k in ("cext", "csca", "cbak", "g"):
-            err[k] = _relmax(g.scalars[k], r.scalars[k])
-        for k, v in err.items():
-            worst[k] = max(worst.get(k, 0.0), float(v))
-    out["split_error_vs_fp64"] = {"max_rel_err": worst, "cases_with_same_n_coef": same,
-                                  "metric": "max over cases of max|split - fp64| / max|fp64| per output array"}
+    for name in ("tf32x3", "int8"):
+        worst, same = {}, 0
+        for g, r in zip(res[name], res["fp64"]):
+            if g.rc != 0 or r.rc != 0:
+                raise RuntimeError("precision-stress solve failed")
+            nc = min(g.n_coef, r.n_coef)
+            err = {"gc": _relmax(g.gc[:, :nc], r.gc[:, :nc]), "gc_l": _relmax(g.gc_l[:, :, :nc], r.gc_l[:, :, :nc])}
+            if g.n_coef == r.n_coef:
+                same += 1
+                err.update(pf=_relmax(g.pf, r.pf), pf_l=_relmax(g.pf_l, r.pf_l))
+            for k in ("cext", "csca", "cbak", "g"):
+                err[k] = _relmax(g.scalars[k], r.scalars[k])
+            for k, v in err.items():
+                worst[k] = max(worst.get(k, 0.0), float(v))
+        out[name]["error_vs_fp64"] = {"max_rel_err": worst, "cases_with_same_n_coef": same,
+                                      "metric": "max over cases of max|form - fp64| / max|fp64| per output array"}
     return out
 
 
@@ -477,6 +488,52 @@ def run_reference_arm(args) -> int:
     return 0
 
 
+def int8_errors(lib, cases, n_threads: int) -> dict:
+    """The int8 fixed-point form against the FP64 form over `cases`: per
+    output array max|int8 - fp64| / max|fp64|, per derivative slice the same
+    over the slice's own maximum, the truncations that agree, the cases
+    solved again in FP64."""
+    ref = abi.solve_batch(lib, cases, n_threads=n_threads, precision=abi.PRECISION_FP64)
+    got = abi.solve_batch(lib, cases, n_threads=n_threads, precision=abi.PRECISION_INT8)
+    redo = C.c_longlong()
+    lib.lmieb_last_redo(C.byref(redo))
+    worst, n_same = {}, 0
+    for g, r in zip(got, ref):
+        if g.rc != 0 or r.rc != 0:
+            raise RuntimeError("solve failed while measuring the int8 error")
+        n_same += g.n_coef == r.n_coef
+        err = {k: _relmax(g.scalars[k], r.scalars[k]) for k in ("cext", "csca", "cbak", "g")}
+        for name in ("gc", "pf", "gc_l", "pf_l"):
+            a, b = getattr(g, name), getattr(r, name)
+            if b is None:
+                continue
+            if a.shape != b.shape:
+                raise RuntimeError("int8 and fp64 outputs differ in shape")
+            err[name] = _relmax(a, b)
+            if name.endswith("_l"):
+                sl = 0.0
+                for i in range(b.shape[0]):
+                    for e in range(b.shape[1]):
+                        m = float(np.max(np.abs(b[i, e])))
+                        if m > 0:
+                            sl = max(sl, float(np.max(np.abs(a[i, e] - b[i, e]))) / m)
+                err[name + "_per_slice"] = sl
+        for k, v in err.items():
+            worst[k] = max(worst.get(k, 0.0), float(v))
+    return {"cases": len(cases), "max_rel_err": worst, "cases_with_same_n_coef": n_same,
+            "solved_again_in_fp64": int(redo.value),
+            "metric": "max over cases of max|int8 - fp64| / max|fp64| per output array (*_per_slice: per "
+                      "derivative and element over that slice's own maximum)"}
+
+
+def _peaks() -> dict:
+    peaks = ROOT / "MEASURED_PEAKS.json"
+    try:
+        return json.loads(peaks.read_text()) if peaks.exists() else {}
+    except ValueError:
+        return {}
+
+
 def run_b200(args) -> int:
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -505,6 +562,8 @@ def run_b200(args) -> int:
 
     import lmie_b200
     lib = lmie_b200.library()
+    lib.lmieb_last_redo.argtypes = [C.POINTER(C.c_longlong)]
+    lib.lmieb_last_int8_kernel.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double)]
     if lib.lmieb_set_device(local) != 0:
         raise RuntimeError("lmieb_set_device failed")
     threads = max(1, (os.cpu_count() or 1) // max(1, world))
@@ -520,111 +579,103 @@ def run_b200(args) -> int:
         n_job = N_CASES
     batch = CBatch(lib, cases)
 
-    tuned = batch.autotune(threads, abi.PRECISION_FP64)
-    for _ in range(args.warmup):
-        if batch.solve_batch(threads) != 0:
-            raise RuntimeError("lmie_solution_batch failed")
-    flops = (C.c_double * 4)()
-    launches = C.c_longlong()
-    h2d, d2h = C.c_size_t(), C.c_size_t()
+    def measure(precision: int, steps: int, warmup: int) -> dict:
+        """One arithmetic form: autotuned public batch calls on host buffers
+        (e2e), then the resident batch re-run on the device with the L2
+        flushed before every step (value), with stage times and work."""
+        tuned = batch.autotune(threads, precision)
+        for _ in range(warmup):
+            if batch.solve_batch(threads, precision) != 0:
+                raise RuntimeError("lmie_solution_batch2 failed")
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            if batch.solve_batch(threads, precision) != 0:
+                raise RuntimeError("lmie_solution_batch2 failed")
+        barrier()
+        e2e_s = max_over_ranks(time.perf_counter() - t0)
+        hm = (C.c_double * 7)()
+        lib.lmieb_last_host_timing(hm, 7)
+        lib.lmieb_set_pipeline(1)
+        if batch.solve_batch(threads, precision) != 0:
+            raise RuntimeError("lmie_solution_batch2 failed")
+        flops = (C.c_double * 4)()
+        launches = C.c_longlong()
+        h2d, d2h = C.c_size_t(), C.c_size_t()
+        lib.lmieb_last_work(flops, C.byref(launches), C.byref(h2d), C.byref(d2h))
+        redo = C.c_longlong()
+        lib.lmieb_last_redo(C.byref(redo))
+        ms_total = C.c_double()
+        ms_stage = (C.c_double * lmie_b200.N_STAGES)()
+        if lib.lmieb_rerun_device(1, 1, C.byref(ms_total), ms_stage) != 0:
+            raise RuntimeError("device re-run failed (batch did not fit one sub-batch)")
+        barrier()
+        if lib.lmieb_rerun_device(steps, 1, C.byref(ms_total), ms_stage) != 0:
+            raise RuntimeError("device re-run failed")
+        barrier()
+        dev_ms = max_over_ranks(ms_total.value)
+        ops, k3 = C.c_double(), C.c_double()
+        lib.lmieb_last_int8_kernel(C.byref(ops), C.byref(k3))
+        lib.lmieb_set_pipeline(tuned["pipeline_parts"])
+        return {"value": n_job * steps / (dev_ms * 1e-3), "e2e": n_job * steps / e2e_s, "unit": UNIT,
+                "ms_per_step": dev_ms / steps,
+                "stage_ms": {n: ms_stage[i] / steps for i, n in enumerate(lmie_b200.STAGES)},
+                "host_ms": dict(zip(("prepare", "pack", "device_and_copies", "unpack", "scatter", "device_span",
+                                     "device_sum_of_parts"), list(hm))),
+                "autotuned": tuned, "flops": list(flops), "launches": int(launches.value),
+                "h2d": int(h2d.value), "d2h": int(d2h.value), "solved_again_in_fp64": int(redo.value),
+                "int8_ops": ops.value, "int8_kernel_ms": k3.value / steps}
 
     clocks = ClockSampler(local)
     clocks.start()
-
-    # e2e: K public batch calls on host buffers
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        if batch.solve_batch(threads) != 0:
-            raise RuntimeError("lmie_solution_batch failed")
-    barrier()
-    e2e_s = max_over_ranks(time.perf_counter() - t0)
-    hm = (C.c_double * 7)()
-    lib.lmieb_last_host_timing(hm, 7)
-    host_ms = dict(zip(("prepare", "pack", "device_and_copies", "unpack", "scatter", "device_span",
-                        "device_sum_of_parts"), list(hm)))
-
-    # device: K re-runs of the whole batch resident on the device (one part, no
-    # host/device overlap), L2 flushed before each (untimed)
-    lib.lmieb_set_pipeline(1)
-    if batch.solve_batch(threads) != 0:
-        raise RuntimeError("lmie_solution_batch failed")
-    lib.lmieb_last_work(flops, C.byref(launches), C.byref(h2d), C.byref(d2h))
-    ms_total = C.c_double()
-    ms_stage = (C.c_double * lmie_b200.N_STAGES)()
-    if lib.lmieb_rerun_device(1, 1, C.byref(ms_total), ms_stage) != 0:
-        raise RuntimeError("device re-run failed (batch did not fit one sub-batch)")
-    barrier()
-    if lib.lmieb_rerun_device(args.steps, 1, C.byref(ms_total), ms_stage) != 0:
-        raise RuntimeError("device re-run failed")
-    barrier()
-    dev_ms = max_over_ranks(ms_total.value)
-    batch_stage_ms = {n: ms_stage[i] / args.steps for i, n in enumerate(lmie_b200.STAGES)}
-    ang_ms = ms_stage[3] / args.steps
-
-    # the same batch with the angular contraction on the tensor cores
-    tf32 = abi.PRECISION_TF32X3
-    lib.lmieb_set_pipeline(tuned["pipeline_parts"])
-    tuned_tc = batch.autotune(threads, tf32)
-    for _ in range(2):
-        if batch.solve_batch(threads, tf32) != 0:
-            raise RuntimeError("lmie_solution_batch2 failed")
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        if batch.solve_batch(threads, tf32) != 0:
-            raise RuntimeError("lmie_solution_batch2 failed")
-    barrier()
-    split_e2e_s = max_over_ranks(time.perf_counter() - t0)
-    lib.lmieb_set_pipeline(1)
-    if batch.solve_batch(threads, tf32) != 0:
-        raise RuntimeError("lmie_solution_batch2 failed")
-    if lib.lmieb_rerun_device(1, 1, C.byref(ms_total), ms_stage) != 0:
-        raise RuntimeError("device re-run failed")
-    barrier()
-    if lib.lmieb_rerun_device(args.steps, 1, C.byref(ms_total), ms_stage) != 0:
-        raise RuntimeError("device re-run failed")
-    barrier()
-    split_dev_ms = max_over_ranks(ms_total.value)
-    lib.lmieb_set_pipeline(tuned["pipeline_parts"])
+    m8 = measure(abi.PRECISION_INT8, args.steps, args.warmup)
+    m64 = measure(abi.PRECISION_FP64, args.steps, 2)
+    mtf = measure(abi.PRECISION_TF32X3, max(3, args.steps // 2), 2)
     clk = clocks.stop()
-    split_stage_ms = {n: ms_stage[i] / args.steps for i, n in enumerate(lmie_b200.STAGES)}
-    split_ang_ms = ms_stage[3] / args.steps
 
-    value = n_job * args.steps / (dev_ms * 1e-3)
-    e2e = n_job * args.steps / e2e_s
-    peak = C.c_double()
-    lib.lmieb_fp64_peak(C.byref(peak))
-    achieved = flops[0] / (ang_ms * 1e-3) / 1e12 if ang_ms > 0 else None
+    peaks = _peaks()
+    bf16 = peaks.get("bf16_tflops")
+    fp64_peak = C.c_double()
+    lib.lmieb_fp64_peak(C.byref(fp64_peak))
+    f_ang = m8["flops"][0]
+    k3_ms = m8["int8_kernel_ms"]
+    tops = m8["int8_ops"] / (k3_ms * 1e-3) / 1e12 if k3_ms > 0 else None
+    int8_peak = 2.0 * float(bf16) if bf16 else None
+    roofline = {
+        "kernel": "k_angular_oz (S1/S2 contraction as exact int8 fixed point: tcgen05.mma kind::i8, A digits in "
+                  "tensor memory, 21 digit products per chunk of 32 orders, int32 accumulation)",
+        "bound": "tensor", "achieved": tops, "peak": int8_peak, "unit": "TOPS",
+        "frac": (tops / int8_peak) if (tops and int8_peak) else None,
+        "traffic": ANGULAR_TRAFFIC.get("int8"),
+        "peak_source": "dense int8 = 2x the measured bf16 burst in MEASURED_PEAKS.json (of measured)",
+        "ops_per_launch": m8["int8_ops"], "ms_per_launch": k3_ms,
+        "fp64_equivalent_tflops": f_ang / (k3_ms * 1e-3) / 1e12 if k3_ms > 0 else None,
+        "fp64_equivalent_note": "algorithmic S1/S2 flops (8 per angle, order, radius, Mie column) per second "
+                                "of this kernel, against the FP64 FMA peak below",
+        "fp64_fma_peak_tflops": fp64_peak.value}
+    ang64 = m64["stage_ms"]["angular"]
+    fp64 = {k: m64[k] for k in ("value", "e2e", "unit", "ms_per_step", "stage_ms", "host_ms", "autotuned")}
+    fp64["roofline"] = {
+        "kernel": "k_angular (S1/S2 accumulation + phase-matrix forms, FP64)", "bound": "fp64",
+        "achieved": m64["flops"][0] / (ang64 * 1e-3) / 1e12 if ang64 > 0 else None, "peak": fp64_peak.value,
+        "unit": "TFLOP/s", "traffic": ANGULAR_TRAFFIC["fp64"],
+        "frac": (m64["flops"][0] / (ang64 * 1e-3) / 1e12 / fp64_peak.value) if ang64 > 0 else None,
+        "peak_source": "live FP64 FMA microbenchmark (lmieb_fp64_peak)"}
 
-    # secondary: split-precision error, the plain per-case form, the single cloud-droplet case
-    single = split = plain = adj = stress = reweight = None
+    single = split = plain = adj = stress = reweight = errs8 = None
     if rank == 0:
-        errs = split_errors(lib, cases[:256], threads)
-        tf32_peak = None
-        peaks = ROOT / "MEASURED_PEAKS.json"
-        if peaks.exists():
-            try:
-                bf16 = json.loads(peaks.read_text()).get("bf16_tflops")
-                tf32_peak = float(bf16) / 2 if bf16 else None
-            except (ValueError, TypeError):
-                tf32_peak = None
-        tc_tflops = 3 * flops[0] / (split_ang_ms * 1e-3) / 1e12 if split_ang_ms > 0 else None
-        split = {
-            "value": n_job * args.steps / (split_dev_ms * 1e-3),
-            "e2e": n_job * args.steps / split_e2e_s, "unit": UNIT,
-            "ms_per_step": split_dev_ms / args.steps, "stage_ms": split_stage_ms,
-            "dtype": "f64 with tf32x3 angular contraction (fp32 accumulation in segments of 32 orders)",
-            "autotuned": tuned_tc,
-            "error_vs_fp64": errs,
-            "roofline": {
-                "kernel": "k_angular_tc (tcgen05.mma kind::tf32, 3 products per operand pair)",
-                "bound": "tensor", "achieved": tc_tflops, "peak": tf32_peak, "unit": "TFLOP/s",
-                "frac": (tc_tflops / tf32_peak) if (tc_tflops and tf32_peak) else None,
-                "traffic": ANGULAR_TRAFFIC["tf32x3"],
-                "peak_source": "dense tf32 = half of the measured bf16 burst in MEASURED_PEAKS.json",
-                "tensor_flops_per_launch": 3 * flops[0], "ms_per_launch": split_ang_ms},
-        }
+        errs8 = int8_errors(lib, cases, threads)
+        split = {k: mtf[k] for k in ("value", "e2e", "unit", "ms_per_step", "stage_ms", "autotuned")}
+        split["dtype"] = "f64 with tf32x3 angular contraction (fp32 accumulation in segments of 32 orders)"
+        split["error_vs_fp64"] = split_errors(lib, cases[:256], threads)
+        tang = mtf["stage_ms"]["angular"]
+        tc_tflops = 3 * m64["flops"][0] / (tang * 1e-3) / 1e12 if tang > 0 else None
+        split["roofline"] = {
+            "kernel": "k_angular_tc (tcgen05.mma kind::tf32, 3 products per operand pair)", "bound": "tensor",
+            "achieved": tc_tflops, "peak": float(bf16) / 2 if bf16 else None, "unit": "TFLOP/s",
+            "frac": (tc_tflops / (float(bf16) / 2)) if (tc_tflops and bf16) else None,
+            "traffic": ANGULAR_TRAFFIC["tf32x3"],
+            "peak_source": "dense tf32 = half of the measured bf16 burst in MEASURED_PEAKS.json"}
         # the plain form on the same cases as the batched numbers
         batch.solve_each(threads, 16)
         t1 = time.perf_counter()
@@ -644,6 +695,8 @@ def run_b200(args) -> int:
         for _ in range(10):
             one.solve_each(1)
         single_e2e = 10 / (time.perf_counter() - t1)
+        ms_total = C.c_double()
+        ms_stage = (C.c_double * lmie_b200.N_STAGES)()
         lib.lmieb_rerun_device(2, 1, C.byref(ms_total), ms_stage)
         lib.lmieb_rerun_device(10, 1, C.byref(ms_total), ms_stage)
         single = {"workload": "cloud droplet: gamma r_eff=10um v_eff=0.1, 4x500 radii, x_max~436, 4 derivatives",
@@ -653,25 +706,24 @@ def run_b200(args) -> int:
     if rank == 0:
         cpu = cpu_baseline(cases, 20.0) if world == 1 else None
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
-            "scaling": args.scaling, "vs_baseline": None, "dtype": "f64",
+            "metric": METRIC, "value": m8["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": m8["ms_per_step"], "higher_is_better": True,
+            "scaling": args.scaling, "vs_baseline": None,
+            "dtype": "f64 (angular contraction as exact int8 fixed point, within 1e-9 of f64)",
             "data": ("synthetic (seeded generator, rank r uses seed + r)" if args.scaling == "weak" else
                      "synthetic (seeded generator, one batch split by estimated cost over the ranks)"),
             "config": bench_config(world, args.scaling),
-            "autotuned": tuned,
-            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d.value),
-                    "d2h_bytes_per_step": int(d2h.value), "host_threads": threads},
-            "gpu_launches": int(launches.value) * args.steps,
-            "roofline": {
-                "kernel": "k_angular (S1/S2 accumulation + phase-matrix forms, FP64)",
-                "bound": "fp64", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
-                "frac": (achieved / peak.value) if achieved else None, "traffic": ANGULAR_TRAFFIC["fp64"],
-                "peak_source": "live FP64 FMA microbenchmark (lmieb_fp64_peak); "
-                               "MEASURED_PEAKS.json holds HBM and BF16 only",
-                "flops_per_launch": flops[0], "ms_per_launch": ang_ms},
-            "stage_ms": batch_stage_ms,
-            "host_ms": host_ms,
+            "path": "lmie_solution_batch2(..., LMIEB_PRECISION_INT8)",
+            "autotuned": m8["autotuned"],
+            "e2e": {"value": m8["e2e"], "unit": UNIT, "h2d_bytes_per_step": m8["h2d"],
+                    "d2h_bytes_per_step": m8["d2h"], "host_threads": threads},
+            "gpu_launches": m8["launches"] * args.steps,
+            "roofline": roofline,
+            "stage_ms": m8["stage_ms"],
+            "host_ms": m8["host_ms"],
+            "solved_again_in_fp64_per_step": m8["solved_again_in_fp64"],
+            "int8_error_vs_fp64": errs8,
+            "fp64": fp64,
             "split_tf32x3": split,
             "plain": plain,
             "adjoint": adj,
@@ -702,7 +754,7 @@ def run_profile(args) -> int:
             lmie_b200.adjoint(p)
         print(f"profiled adjoint: {p.n_lambda} wavelengths, {args.warmup} + {args.steps} calls")
         return 0
-    precision = abi.PRECISION_TF32X3 if args.profile == "tf32x3" else abi.PRECISION_FP64
+    precision = {"tf32x3": abi.PRECISION_TF32X3, "int8": abi.PRECISION_INT8}.get(args.profile, abi.PRECISION_FP64)
     lib.lmieb_set_pipeline(1)            # one sub-batch: the launches the device-time `value` measures
     batch = CBatch(lib, workloads.batched_uneven(args.cases))
     threads = os.cpu_count() or 1
@@ -719,7 +771,7 @@ def main(argv=None) -> int:
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
-    ap.add_argument("--profile", choices=("fp64", "tf32x3", "adjoint"), default=None,
+    ap.add_argument("--profile", choices=("fp64", "tf32x3", "int8", "adjoint"), default=None,
                     help="run only this path's batch calls (for profilers); no bench line")
     ap.add_argument("--cases", type=int, default=N_CASES, help="cases of the profiled batch")
     ap.add_argument("--scaling", choices=("weak", "strong"), default="weak",

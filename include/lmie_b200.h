@@ -42,6 +42,20 @@ int lmie_solution_batch(int n_cases, lmie_in_data *in, lmie_out_data *out, int a
  *   more than 4 index1 or 3 index2 derivative slots) run in FP64. */
 #define LMIEB_PRECISION_FP64 0
 #define LMIEB_PRECISION_TF32X3 1
+/* LMIEB_PRECISION_INT8: the angular S1/S2 contraction runs on the int8 tensor
+ *   cores as an exact fixed-point sum: each operand value is scaled by powers
+ *   of two (per order, per angle row, per operand column) to 46 fractional
+ *   bits and split into six signed 8-bit digits; the 21 digit products that
+ *   carry the result are summed exactly in int32 and combined in FP64.  The
+ *   contraction carries about 1e-12 of the largest term of its row and column
+ *   (FP64: about 1e-16); everything else is the FP64 form's arithmetic.  A case
+ *   whose truncation n_coef could depend on that difference -- some
+ *   |beta_l| (l < n_coef) within the contraction's error bound of `accuracy`
+ *   -- is solved again in FP64 within the same call, so n_coef is always the
+ *   FP64 form's.  Problems this mode does not cover (save_control != 0, more
+ *   than 4 index1 or 3 index2 derivative slots) and cases of fewer than 16 or
+ *   more than 5120 orders run in FP64. */
+#define LMIEB_PRECISION_INT8 2
 
 /* Batch calls cut their cases into `chunks` parts (0: automatic -- one part
  * per 640 cases, at most 6; 1: one part) and prepare, pack, unpack and
@@ -77,6 +91,13 @@ int lmieb_get_split_segment(void);
  * the best wall time (ms) through the non-NULL pointers.  Returns 0 or -1. */
 int lmie_solution_autotune(int n_cases, lmie_in_data *in, lmie_out_data *out, int n_threads, int precision,
                            int *best_chunks, double *best_items, double *best_ms);
+
+/* One 128 x 64 product of the LMIEB_PRECISION_INT8 contraction (K orders, a
+ * positive multiple of 32 up to 5120; seeded operands growing like the
+ * angular products) against long-double sums on the host: the largest error
+ * of an element relative to max|a_i.| max|b_n.| of its row and column.
+ * Returns 0 or -1. */
+int lmieb_oz_selftest(int K, double *max_rel_err);
 
 /* lmie_solution_batch with the arithmetic chosen by `precision`. */
 int lmie_solution_batch2(int n_cases, lmie_in_data *in, lmie_out_data *out, int alloc_out,
@@ -186,8 +207,9 @@ int lmieb_last_timing(double *ms, int n);
 
 /* Re-runs the device stages 1..7 of the last solve `reps` times on the
  * inputs still resident in device memory (no host work, no copies); only
- * defined when that solve ran as one sub-batch (see lmieb_set_pipeline),
- * else returns -1.  The kernel sequence is captured once per resident solve
+ * defined when that solve ran as one sub-batch (see lmieb_set_pipeline) --
+ * with LMIEB_PRECISION_INT8, one sub-batch and the FP64 re-solve of its
+ * uncertain cases, re-run one after the other -- else returns -1.  The kernel sequence is captured once per resident solve
  * into a CUDA graph; each replay is bracketed by CUDA events on the
  * library's stream, and with flush_l2 a 256 MiB buffer is written before each
  * repetition (outside the timed interval).  Returns the summed device time of
@@ -202,6 +224,18 @@ int lmieb_rerun_device(int reps, int flush_l2, double *ms_total, double *ms_stag
  * issues; and the bytes the last solve copied host-to-device and back.  Any
  * pointer may be NULL. */
 int lmieb_last_work(double *flops, long long *launches, size_t *h2d, size_t *d2h);
+
+/* Cases of the last batch call that LMIEB_PRECISION_INT8 solved again in
+ * FP64 because their truncation n_coef was not certain at the fixed-point
+ * contraction's error.  Returns 0. */
+int lmieb_last_redo(long long *cases);
+
+/* The LMIEB_PRECISION_INT8 product kernel of the last solve: the
+ * tensor-core operations it runs (2 per 8-bit multiply-add) and, after
+ * lmieb_rerun_device, its device time summed over the re-runs' stage-timed
+ * passes (ms; CUDA events around its launch).  Either pointer may be NULL.
+ * Returns 0. */
+int lmieb_last_int8_kernel(double *tensor_ops, double *ms);
 
 /* Measures the FP64 FMA throughput of the device (TFLOP/s) with a short
  * register-resident microbenchmark on the library's stream. */

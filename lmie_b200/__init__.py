@@ -36,6 +36,7 @@ def library() -> C.CDLL:
         lib.lmieb_device_info.argtypes = [C.c_char_p, C.c_int, C.POINTER(C.c_int),
                                           C.POINTER(C.c_int), C.POINTER(C.c_int)]
         lib.lmieb_tc_selftest.argtypes = [C.c_int, C.POINTER(C.c_double)]
+        lib.lmieb_oz_selftest.argtypes = [C.c_int, C.POINTER(C.c_double)]
         lib.lmieb_last_host_timing.argtypes = [C.POINTER(C.c_double), C.c_int]
         lib.lmieb_set_pipeline.argtypes = [C.c_int]
         lib.lmieb_set_work_granularity.argtypes = [C.c_int, C.c_double]

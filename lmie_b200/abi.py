@@ -335,6 +335,7 @@ def deriv_unit(*names: str) -> List[Dict[str, float]]:
 
 PRECISION_FP64 = 0      # LMIEB_PRECISION_FP64
 PRECISION_TF32X3 = 1    # LMIEB_PRECISION_TF32X3
+PRECISION_INT8 = 2      # LMIEB_PRECISION_INT8
 
 
 def solve_batch(lib: C.CDLL, cases: Sequence[Case], n_threads: int = 8,

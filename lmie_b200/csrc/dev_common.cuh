@@ -62,3 +62,16 @@ __host__ __device__ __forceinline__ cplx operator/(cplx a, double s) { return mk
     } while (0)
 
 static inline unsigned int ceil_div(size_t a, size_t b) { return (unsigned int) ((a + b - 1) / b); }
+
+#ifdef __CUDACC__
+// case c with start[c] <= e < start[c + 1] (start: ncase + 1 ascending offsets)
+static __device__ __forceinline__ int find_case(const long long *__restrict__ start, int ncase, long long e) {
+    int lo = 0, hi = ncase - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (start[mid] <= e) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+#endif

@@ -25,6 +25,7 @@
 
 #include "host_pool.h"
 #include "kernels.h"
+#include "oz_layout.cuh"
 #include "tc_layout.cuh"
 #include "lmieb.h"
 #include "../../include/lmie_b200.h"
@@ -61,6 +62,8 @@ struct Pending {
     size_t acc_n = 0;
     std::vector<int> piece;            // case ranges [piece[p], piece[p+1]) of the result copies
     double t_submit = 0.;
+    const lmieb_problem *ps = nullptr; // the problems (alive until the call that submitted them returns)
+    int precision = 0;
 };
 
 // One of two buffer sets: a sub-batch is packed into one while the device
@@ -89,12 +92,17 @@ struct Ctx {
     int last_slot = -1;             // slot of the last submitted sub-batch
     long long next_ticket = 0;
     int submits = 0;                // sub-batches submitted since the counters were reset
+    int call_slot[2] = {-1, -1};    // slots of the first two sub-batches since then
+    long long redo = 0;             // INT8 cases solved again in FP64 since then
     std::vector<std::pair<long long, int>> finished;   // (ticket, rc) of recently collected sub-batches
     char *flush = nullptr;
     cudaEvent_t ev[NSTAGE + 1] = {};
     bool timing = false;
     double stage_ms[NSTAGE] = {};
     double work[4] = {};            // algorithmic flops of the last solve (see lmieb_last_work)
+    double tensor_ops = 0.;         // tensor-core operations (2 per multiply-add) its int8 products run
+    cudaEvent_t k3[2] = {};         // with timing: around the int8 product kernel
+    double k3_ms = 0.;
     long long launches = 0;         // kernel launches of one device run of the last solve
     size_t h2d = 0, d2h = 0;        // bytes copied by the last solve
     // Gauss-Legendre angles depend only on their number: computed once per n
@@ -126,9 +134,14 @@ struct Ctx {
 Ctx g_ctx;
 
 // Work items per SM the angular stage is cut into ([0] FP64 kernel, [1]
-// tensor-core kernel): finer items balance uneven cases, coarser ones cut the
-// per-item overhead; set by lmieb_set_work_granularity (the autotuner).
-double g_items_per_sm[2] = {64., 2.};
+// TF32 tensor-core kernel, [2] int8 tensor-core kernel): finer items balance
+// uneven cases, coarser ones cut the per-item overhead; set by
+// lmieb_set_work_granularity (the autotuner).
+double g_items_per_sm[3] = {64., 2., 2.};
+
+int prec_slot(int precision) {
+    return precision == LMIEB_PRECISION_TF32X3 ? 1 : (precision == LMIEB_PRECISION_INT8 ? 2 : 0);
+}
 
 // Orders (in chunks of TC_KC) per FP32 segment of the tensor-core stage's
 // hi*hi products; set by lmieb_set_split_segment.
@@ -265,6 +278,14 @@ struct Plan {
     int tc_seg = 2;             // its segment length (chunks)
     float *bop = nullptr;       // its B operand (tc_layout.cuh)
     size_t bop_bytes = 0;
+    int oz = 0;                 // K3 as the int8 fixed-point contraction (oz_layout.cuh)
+    unsigned char *bop8 = nullptr;   // its B operand digits
+    signed char *rowexp = nullptr;   // its row exponents
+    int *colexp = nullptr;      // its column exponents
+    long long *bcorr = nullptr; // its bias terms of the digit combination
+    long long *rx_start = nullptr;   // (case, half-angle) index space of the row exponents
+    long long n_rx = 0;
+    int n_groups = 0;
     ExpItem *ex = nullptr;
     int n_ex = 0;
     long long *pf_start = nullptr, *ck_gc = nullptr, *ck_lc = nullptr, *fin_start = nullptr, *pu_start = nullptr;
@@ -317,6 +338,8 @@ int ensure_ready() {
         LMIEB_CUDA_TRY(cudaEventCreate(&S.t_end));
     }
     LMIEB_CUDA_TRY(cudaEventCreate(&c.t_first));
+    LMIEB_CUDA_TRY(cudaEventCreate(&c.k3[0]));
+    LMIEB_CUDA_TRY(cudaEventCreate(&c.k3[1]));
     LMIEB_CUDA_TRY(cudaEventCreateWithFlags(&c.save.ready, cudaEventDisableTiming));
     LMIEB_CUDA_TRY(cudaEventCreateWithFlags(&c.gl_ready, cudaEventDisableTiming));
     c.ready = true;
@@ -399,11 +422,20 @@ int run_accumulate(Plan &L, cudaStream_t s) {
         stage(2);
         if (launch_reduce_scalars(s, B, L.rs, L.sums, L.save_control == 1 ? L.o_save1 : nullptr)) return -1;
         stage(3);
-        const int n64 = L.tc ? L.n_ang64 : L.n_ang;
-        const AngItem *a64 = L.tc ? L.ang64 : L.ang;
+        const bool tcx = L.tc || L.oz;
+        const int n64 = tcx ? L.n_ang64 : L.n_ang;
+        const AngItem *a64 = tcx ? L.ang64 : L.ang;
         if (L.tc && L.n_ang > 0 &&
             launch_angular_tc(s, B, L.n_ang, L.ang, L.bop, L.part, L.tc_seg, L.o_trunc + 2 * L.ncase))
             return -1;
+        if (L.oz && L.n_ang > 0) {
+            if (launch_oz_operands(s, B, L.n_rx, L.rx_start, L.rowexp, L.n_groups, L.coef, L.bop8, L.colexp,
+                                   L.bcorr))
+                return -1;
+            if (g_ctx.timing) LMIEB_CUDA_TRY(cudaEventRecord(g_ctx.k3[0], s));
+            if (launch_angular_oz(s, B, L.n_ang, L.ang, L.bop8, L.part, L.o_trunc + 2 * L.ncase)) return -1;
+            if (g_ctx.timing) LMIEB_CUDA_TRY(cudaEventRecord(g_ctx.k3[1], s));
+        }
         if (n64 > 0) {
             for (int t = 0; t < L.n_ang_launch; ++t) {
                 const int c1 = t * 4, c2 = t * 4;
@@ -429,13 +461,14 @@ int run_finish(Plan &L, cudaStream_t s) {
     stage(4);
     if (launch_normalize(s, B, L.pf_total, L.pf_start, L.sums, L.pfacc, L.o_scal, L.pfn)) return -1;
     LMIEB_CUDA_TRY(cudaMemsetAsync(L.o_trunc, 0, sizeof(int) * 2 * L.ncase, s));
+    LMIEB_CUDA_TRY(cudaMemsetAsync(L.o_trunc + 2 * L.ncase + 1, 0, sizeof(int) * 4 * L.ncase, s));
     stage(5);
     if (L.want_gc && launch_expand(s, B, 0, L.nck_gc, L.ck_gc, L.n_ex, L.ex, L.nfin, L.fin_start, L.pfn,
-                                   L.ckpt, L.exq, L.o_gc, L.o_trunc))
+                                   L.ckpt, L.exq, L.o_gc, L.o_trunc, L.o_trunc + 2 * L.ncase + 1))
         return -1;
     stage(6);
     if (L.want_lc && launch_expand(s, B, 1, L.nck_lc, L.ck_lc, L.n_ex, L.ex, L.nfin, L.fin_start, L.pfn,
-                                   L.ckpt, L.exq, L.o_lc, L.o_trunc + L.ncase))
+                                   L.ckpt, L.exq, L.o_lc, L.o_trunc + L.ncase, L.o_trunc + 4 * L.ncase + 1))
         return -1;
     stage(7);
     if (L.pf_from) {
@@ -511,6 +544,11 @@ size_t case_bytes(const lmieb_problem &p) {
     b += (size_t) 4 * ncol * p.n_qang * 8 * 8;                        // partials (groups), pf, pfn
     b += (size_t) ncol * 6 * p.n_coef * 8 * (3 + (p.n_qang / 2 + 31) / 32);   // expansion partials + outputs
     b += (size_t) 4 * (p.n_qang / 2) * (p.n_coef / EX_LT + 1) * 16;   // checkpoints
+    if (p.precision == LMIEB_PRECISION_INT8) {
+        // B operand digits (groups padded to whole chunks), row exponents
+        b += (size_t) (tot + (size_t) p.n * OZ_KC) * OZ_BSTAGE / (OZ_KC * oz_rg(std::min(p.nd1, OZ_MAX_NC1)));
+        b += (size_t) (p.n_qang / 2 + 1) * (tot / std::max(p.n, 1) / OZ_KC + 2) * 2;
+    }
     return b;
 }
 
@@ -701,10 +739,17 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     L.tc = p0.precision == LMIEB_PRECISION_TF32X3 && L.save_control == 0 && any_ang && R > 0 &&
            nd1 <= TC_MAX_NC1 && nd2 <= TC_MAX_ND2;
     L.tc_seg = g_tc_seg;
+    L.oz = p0.precision == LMIEB_PRECISION_INT8 && L.save_control == 0 && any_ang && R > 0 &&
+           nd1 <= OZ_MAX_NC1 && nd2 <= OZ_MAX_ND2;
     // with split precision, cases below TC_MIN_N1 orders keep the FP64 K3: their
     // linearised phase matrices cancel strongly on normalisation, and they cost little
-    std::vector<char> case_tc(ncase, 0);
+    std::vector<char> case_tc(ncase, 0), case_oz(ncase, 0);
     for (int k = 0; k < ncase; ++k) case_tc[k] = L.tc && cs[k].n_qang > 0 && cs[k].n1 >= TC_MIN_N1;
+    // the int8 stage takes the cases of at least OZ_MIN_N1 orders whose radius
+    // groups fit its exact int32 sums (OZ_MAX_NK chunks)
+    for (int k = 0; k < ncase; ++k)
+        case_oz[k] = L.oz && cs[k].n_qang > 0 && cs[k].n1 >= OZ_MIN_N1 &&
+                     (cn1max[k] + OZ_KC - 1) / OZ_KC <= OZ_MAX_NK;
     std::vector<AngItem> ang, ang64;
     std::vector<long long> pf_start(ncase + 1, 0);
     for (int k = 0; k < ncase; ++k) {
@@ -817,13 +862,87 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         }
         largest_first(tmp, ang);
     }
+    // int8 fixed point: radius groups of oz_rg(nd1) radii, each with its B
+    // operand digits; row-exponent tables per case
+    long long bop8_bytes = 0, rx_bytes = 0;
+    int nkx_all = 0;
+    std::vector<long long> rx_start(ncase + 1, 0);
+    if (L.oz) {
+        const int RG = oz_rg(nd1);
+        std::vector<int> cg0(ncase + 1, 0);
+        std::vector<double> wc(ncase, 0.);
+        double W = 0.;
+        for (int k = 0; k < ncase; ++k) {
+            DevCase &C = cs[k];
+            cg0[k] = (int) tg_r0.size();
+            rx_start[k + 1] = rx_start[k];
+            if (!case_oz[k]) continue;
+            C.nkx = (cn1max[k] + OZ_KC - 1) / OZ_KC;
+            C.rx_off = rx_bytes;
+            C.trunc_band = C.accuracy > 0. ? OZ_TRUNC_BAND : 0.;
+            rx_bytes += (long long) C.nh * C.nkx * 2;
+            rx_start[k + 1] += C.nh;
+            nkx_all = std::max(nkx_all, C.nkx);
+            for (int r = C.r0; r < C.r0 + C.nr; r += RG) {
+                const int n = std::min(RG, C.r0 + C.nr - r);
+                int mx = 1;
+                for (int i = 0; i < n; ++i) mx = std::max(mx, n1r[r + i]);
+                const int nk = (mx + OZ_KC - 1) / OZ_KC;
+                tg_r0.push_back(r);
+                tg_n.push_back(n);
+                tg_nk.push_back(nk);
+                tg_off.push_back(bop8_bytes);
+                bop8_bytes += (long long) nk * OZ_BSTAGE;
+                wc[k] += nk + 1;                       // chunks, plus one for the group's epilogue
+            }
+            W += wc[k] * ((C.nh + OZ_HALF - 1) / OZ_HALF);
+        }
+        cg0[ncase] = (int) tg_r0.size();
+        L.n_groups = (int) tg_r0.size();
+        L.n_rx = rx_start[ncase];
+        const double wt = std::max(W / (g_items_per_sm[2] * c.sms), 8.);    // chunks per item
+        std::vector<std::pair<double, AngItem>> tmp;
+        for (int k = 0; k < ncase; ++k) {
+            DevCase &C = cs[k];
+            if (!case_oz[k]) continue;
+            const int ng = cg0[k + 1] - cg0[k];
+            const int xt = (C.nh + OZ_HALF - 1) / OZ_HALF;
+            int G = (int) std::lround(wc[k] / wt);
+            G = std::max(1, std::min(G, ng));
+            std::vector<int> gs(G + 1, cg0[k + 1]);
+            gs[0] = cg0[k];
+            double run = 0.;
+            int gi = 1;
+            for (int g = cg0[k]; g < cg0[k + 1] && gi < G; ++g) {
+                run += tg_nk[g] + 1;
+                if (run * G >= wc[k] * gi) gs[gi++] = g + 1;
+            }
+            for (int g = 1; g <= G; ++g) gs[g] = std::max(gs[g], gs[g - 1]);
+            gs.erase(std::unique(gs.begin(), gs.end()), gs.end());   // every partial slot gets a range
+            G = (int) gs.size() - 1;
+            C.G = G;
+            C.part_off = part_total;
+            part_total += (long long) G * Q * C.n_qang;
+            for (int g = 0; g < G; ++g) {
+                double cost = 0.;
+                for (int gg = gs[g]; gg < gs[g + 1]; ++gg) cost += tg_nk[gg] + 1;
+                for (int t = 0; t < xt; ++t) tmp.push_back({cost, AngItem{k, t, g, gs[g], gs[g + 1]}});
+            }
+        }
+        largest_first(tmp, ang);
+    }
+    std::vector<double> oz_f2;
+    if (L.oz) {
+        oz_f2.assign((size_t) OZ_KC * nkx_all + 2, 0.);
+        for (size_t k = 1; k < oz_f2.size(); ++k) oz_f2[k] = (k + 1.) / (double) k;
+    }
     {
         // FP64 K3 over the remaining cases: radius ranges of roughly equal sum of n1
         const int per = angular_angles_per_block(std::min(nd1, 4));
         double W = 0.;
         std::vector<double> wc(ncase, 0.);
         for (int k = 0; k < ncase; ++k) {
-            if (cs[k].n_qang <= 0 || case_tc[k]) continue;
+            if (cs[k].n_qang <= 0 || case_tc[k] || case_oz[k]) continue;
             wc[k] = (double) (cs1[k + 1] - cs1[k]) * cs[k].nh;
             W += wc[k];
         }
@@ -831,7 +950,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         std::vector<std::pair<double, AngItem>> tmp;
         for (int k = 0; k < ncase; ++k) {
             DevCase &C = cs[k];
-            if (C.n_qang <= 0 || case_tc[k]) continue;
+            if (C.n_qang <= 0 || case_tc[k] || case_oz[k]) continue;
             const int xt = (C.nh + per - 1) / per;
             int G = (int) std::lround(wc[k] / (xt * wt));
             G = std::max(1, std::min(G, C.nr));
@@ -852,7 +971,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
                     tmp.push_back({cost, it});
                 }
         }
-        largest_first(tmp, L.tc ? ang64 : ang);
+        largest_first(tmp, (L.tc || L.oz) ? ang64 : ang);
     }
     L.n_ang = (int) ang.size();
     L.n_ang64 = (int) ang64.size();
@@ -935,6 +1054,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         } else if (L.save_control != 2) {
             nl += (long long) std::max(L.nd1c, 1) + 1;                          // K1 per chunk, K2
             if (L.tc) nl += (L.n_ang > 0) + (L.n_ang64 > 0 ? L.n_ang_launch : 0);   // K3
+            else if (L.oz) nl += (L.n_ang > 0 ? 3 : 0) + (L.n_ang64 > 0 ? L.n_ang_launch : 0);   // operands, K3
             else nl += L.n_ang > 0 ? L.n_ang_launch : 0;
             if (L.n_ang > 0 || L.n_ang64 > 0) nl += 1;                          // group reduction
         } else {
@@ -959,6 +1079,13 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         if (L.save_control == 2 || !solve) fang = frec = 0.;
         if (!finish) fgsf = fexp = 0.;
         c.work[0] += fang;
+        if (L.oz) {
+            // OZ_NPROD products of M x N x K per chunk of every (angle tile, group) pair
+            double chunks = 0.;
+            for (const AngItem &a : ang)
+                for (int gg = a.rbeg; gg < a.rend; ++gg) chunks += tg_nk[gg];
+            c.tensor_ops += 2. * OZ_NPROD * (double) OZ_M * OZ_NP * OZ_KC * chunks;
+        }
         c.work[1] += frec;
         c.work[2] += fgsf;
         c.work[3] += fexp;
@@ -991,7 +1118,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         add((size_t) nd1 * 4); add((size_t) nd2 * 4); add(mu_user.size() * 8);
         add(ang.size() * sizeof(AngItem)); add(ang64.size() * sizeof(AngItem)); add(ex.size() * sizeof(ExpItem));
         add(tc_pos.size() * 4); add(tc_roff.size() * 8); add(tg_r0.size() * 4); add(tg_n.size() * 4);
-        add(tg_nk.size() * 4); add(tg_off.size() * 8);
+        add(tg_nk.size() * 4); add(tg_off.size() * 8); add(oz_f2.size() * 8); add(rx_start.size() * 8);
         for (int q = 0; q < 5; ++q) add((size_t) (ncase + 1) * 8);
         add(gl_ns.size() * 4); add(gl_mo.size() * 8); add(gl_go.size() * 8); add(gl_pt.size() * 4);
         add(gl_pi.size() * 4); add(gl_guess.size() * 8); add(gl_jr.size() * 8);
@@ -1004,7 +1131,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     size_t out_bytes = 0;
     {
         auto add = [&](size_t b) { out_bytes += pad(b); };
-        add(o_scal * 8); add(o_gc * 8); add(o_lc * 8); add(o_pf * 8); add((size_t) (2 * ncase + 1) * 4);
+        add(o_scal * 8); add(o_gc * 8); add(o_lc * 8); add(o_pf * 8); add((size_t) (6 * ncase + 1) * 4);
         if (L.save_control == 1) { add((size_t) 4 * R * 8); add(n_save2 * 8); }
         if (L.acc_mode == LMIEB_ACC_PARTIAL) add(L.acc_n * 8);
     }
@@ -1036,6 +1163,8 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     int *h_tgn = put(hp, ho, tg_n.data(), tg_n.size());
     int *h_tgnk = put(hp, ho, tg_nk.data(), tg_nk.size());
     long long *h_tgoff = put(hp, ho, tg_off.data(), tg_off.size());
+    double *h_ozf2 = put(hp, ho, oz_f2.data(), oz_f2.size());
+    long long *h_rxs = put(hp, ho, rx_start.data(), rx_start.size());
     long long *h_pfs = put(hp, ho, pf_start.data(), pf_start.size());
     long long *h_ckg = put(hp, ho, ck_gc.data(), ck_gc.size());
     long long *h_ckl = put(hp, ho, ck_lc.data(), ck_lc.size());
@@ -1079,6 +1208,12 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         if (L.save_control != 2 && L.acc_mode != LMIEB_ACC_FINISH) {
             add((size_t) ckn * 8 * k1_ck_width(std::min(nd1, 4)));
             if (L.tc) add((size_t) bop_floats * 4);
+            if (L.oz) {
+                add((size_t) bop8_bytes);
+                add((size_t) rx_bytes);
+                add((size_t) L.n_groups * OZ_NP * 4);
+                add((size_t) L.n_groups * OZ_NP * 16);
+            }
             add((size_t) (1 + nd1) * (size_t) ctot * 32);
             add((size_t) (1 + nd1) * 5 * (size_t) R * 8);
             add((size_t) part_total * 8);
@@ -1123,9 +1258,9 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     B.rc = (const double *) dptr(h_rc);
     B.mu_pool = c.gl_pool;
     B.mu_user = (const double *) dptr(h_mu);
-    if (L.tc) {
-        B.tc_pos = (const int *) dptr(h_tcpos);
-        B.tc_roff = (const long long *) dptr(h_tcroff);
+    if (L.tc || L.oz) {
+        B.tc_pos = L.tc ? (const int *) dptr(h_tcpos) : nullptr;
+        B.tc_roff = L.tc ? (const long long *) dptr(h_tcroff) : nullptr;
         B.tg_r0 = (const int *) dptr(h_tgr0);
         B.tg_n = (const int *) dptr(h_tgn);
         B.tg_nk = (const int *) dptr(h_tgnk);
@@ -1151,6 +1286,17 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
             L.bop_bytes = (size_t) bop_floats * 4;
             L.bop = A.take<float>((size_t) bop_floats);
         }
+        if (L.oz) {
+            L.bop8 = A.take<unsigned char>((size_t) bop8_bytes);
+            L.rowexp = A.take<signed char>((size_t) rx_bytes);
+            L.colexp = A.take<int>((size_t) L.n_groups * OZ_NP);
+            L.bcorr = A.take<long long>((size_t) L.n_groups * OZ_NP * 2);
+            B.oz_bcorr = L.bcorr;
+            L.rx_start = (long long *) dptr(h_rxs);
+            B.oz_f2 = (const double *) dptr(h_ozf2);
+            B.oz_rowexp = L.rowexp;
+            B.oz_colexp = L.colexp;
+        }
         L.coef = A.take<double>((size_t) (1 + nd1) * (size_t) ctot * 4);
         L.rs = A.take<double>((size_t) (1 + nd1) * 5 * (size_t) R);
         L.part = A.take<double>((size_t) part_total);
@@ -1168,14 +1314,16 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         L.o_gc = (double *) take(o_gc * 8);
         L.o_lc = (double *) take(o_lc * 8);
         L.o_pf = (double *) take(o_pf * 8);
-        L.o_trunc = (int *) take((size_t) (2 * ncase + 1) * 4);   // gc, lc truncations; error word
+        // gc, lc truncations; error word; gc, lc truncation bands
+        L.o_trunc = (int *) take((size_t) (6 * ncase + 1) * 4);
         if (L.save_control == 1) {
             L.o_save1 = (double *) take((size_t) 4 * R * 8);
             L.o_save2 = (double *) take(n_save2 * 8);
         }
         if (L.acc_mode == LMIEB_ACC_PARTIAL) L.o_acc = (double *) take(L.acc_n * 8);
     }
-    if (!L.sums || !L.pfn || !L.exq || (solve && !L.part) || (L.tc && !L.bop)) {
+    if (!L.sums || !L.pfn || !L.exq || (solve && !L.part) || (L.tc && !L.bop) ||
+        (L.oz && solve && (!L.bop8 || !L.rowexp || !L.colexp || !L.bcorr))) {
         fprintf(stderr, "ERROR: lmie_b200: device arena too small\n");
         return -1;
     }
@@ -1318,7 +1466,31 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     P.acc_n = L.acc_n;
     P.piece.swap(piece);
     P.t_submit = now_ms();
+    P.ps = ps;
+    P.precision = p0.precision;
     return 0;
+}
+
+long long submit_locked(int n, const lmieb_problem *p, lmieb_result *r);
+int collect_ticket(long long ticket);
+int fit_sub(int n, const lmieb_problem *p);
+
+// INT8 cases whose truncation n_coef is not certain at the contraction's
+// error: some |beta_l| (l up to the truncation) lies within the band of
+// `accuracy` (k_exp_final's band outputs).  They are solved again in FP64 by
+// the caller of collect_slot.
+void uncertain_truncations(const Pending &P, const int *htr, std::vector<int> &out) {
+    if (P.precision != LMIEB_PRECISION_INT8 || !(P.want_gc || P.want_lc)) return;
+    const int ncase = P.ncase;
+    const int *tr = P.want_lc ? htr + ncase : htr;
+    const int *band = htr + 2 * ncase + 1 + (P.want_lc ? 2 * ncase : 0);
+    for (int k = 0; k < ncase; ++k) {
+        const DevCase &C = P.cs[k];
+        if (!(C.trunc_band > 0.)) continue;
+        auto idx = [&](int v) { return v > 0 ? C.n_coef - v : C.n_coef; };
+        const int ti = idx(tr[k]), ui = idx(band[2 * k]), wi = idx(band[2 * k + 1]);
+        if (ui < ti || wi > ti) out.push_back(k);
+    }
 }
 
 // Waits for the slot's sub-batch and unpacks its outputs into the callers'
@@ -1342,7 +1514,7 @@ int collect_slot(Slot &S) {
     const int *htr = (const int *) hostp(P.o_trunc);
     if (htr[2 * ncase]) {
         LMIEB_CUDA_TRY(cudaEventSynchronize(S.done));   // no copy may still write the staging
-        fprintf(stderr, "ERROR: lmie_b200: the tensor-core angular stage timed out waiting for its pipeline\n");
+        fprintf(stderr, "ERROR: lmie_b200: a tensor-core angular stage timed out waiting for its pipeline\n");
         return -1;
     }
     for (size_t p = 0; p + 1 < P.piece.size(); ++p) {
@@ -1403,7 +1575,31 @@ int collect_slot(Slot &S) {
         if (r.save1) memcpy(r.save1, hostp(P.o_save1), (size_t) 4 * P.R * 8);
         if (r.save2 && P.n_qang0 > 0) memcpy(r.save2, hostp(P.o_save2), P.n_save2 * 8);
     }
+    std::vector<int> redo;
+    uncertain_truncations(P, htr, redo);
     c.host_ms[3] += now_ms() - t_unpack - waited;
+    if (!redo.empty()) {
+        // the uncertain cases again in FP64, into the same results (the slot's
+        // staging is no longer read, so the re-solve may reuse it)
+        // (P may be reused by the re-solve's sub-batch: keep what is needed)
+        lmieb_result *const rs = P.rs;
+        std::vector<lmieb_problem> q;
+        std::vector<lmieb_result> r;
+        for (int k : redo) {
+            q.push_back(P.ps[k]);
+            q.back().precision = LMIEB_PRECISION_FP64;
+            r.push_back(rs[k]);
+        }
+        c.redo += (long long) redo.size();
+        for (int k0 = 0; k0 < (int) q.size();) {
+            const int m = fit_sub((int) q.size() - k0, q.data() + k0);
+            const long long t = submit_locked(m, q.data() + k0, r.data() + k0);
+            if (t < 0 || collect_ticket(t)) return -1;
+            k0 += m;
+        }
+        // the arrays went straight to the callers' storage; the counts come back here
+        for (size_t i = 0; i < redo.size(); ++i) rs[redo[i]].n_coef_out = r[i].n_coef_out;
+    }
     return 0;
 }
 
@@ -1469,6 +1665,9 @@ void reset_counters() {
     c.launches = 0;
     c.h2d = c.d2h = 0;
     c.submits = 0;
+    c.call_slot[0] = c.call_slot[1] = -1;
+    c.redo = 0;
+    c.tensor_ops = 0.;
 }
 
 // submits p[0..n) (one sub-batch); returns its ticket or -1
@@ -1476,6 +1675,7 @@ long long submit_locked(int n, const lmieb_problem *p, lmieb_result *r) {
     Ctx &c = g_ctx;
     Slot &S = free_slot();
     const long long t = c.next_ticket++;
+    if (c.submits < 2) c.call_slot[c.submits] = (int) (&S - c.slot);
     ++c.submits;
     if (submit_sub(S, t, n, p, r)) {
         S.pend.active = false;
@@ -1672,17 +1872,24 @@ extern "C" int lmieb_last_timing(double *ms, int n) {
 extern "C" int lmieb_rerun_device(int reps, int flush_l2, double *ms_total, double *ms_stage) {
     std::lock_guard<std::mutex> lock(g_mu);
     Ctx &c = g_ctx;
-    // a re-run repeats the resident sub-batch, so the last call must have had exactly one
-    if (!c.ready || c.last_slot < 0 || !c.slot[c.last_slot].have_plan || c.submits != 1 ||
-        c.slot[c.last_slot].plan->acc_mode != LMIEB_ACC_WHOLE) {
+    // a re-run repeats the resident sub-batches of the last call: exactly one,
+    // or an INT8 sub-batch and the FP64 re-solve of its uncertain cases
+    const int ns = c.submits;
+    bool ok = c.ready && (ns == 1 || (ns == 2 && c.redo > 0 && c.call_slot[0] != c.call_slot[1]));
+    for (int i = 0; ok && i < ns; ++i) {
+        const int si = c.call_slot[i];
+        ok = si >= 0 && c.slot[si].have_plan && c.slot[si].plan->acc_mode == LMIEB_ACC_WHOLE;
+    }
+    if (!ok) {
         fprintf(stderr, "ERROR: lmieb_rerun_device: no single-sub-batch solve is resident on the device\n");
         return -1;
     }
     if (flush_l2 && !c.flush) LMIEB_CUDA_TRY(cudaMalloc((void **) &c.flush, FLUSH_BYTES));
-    Slot &S = c.slot[c.last_slot];
     const bool was = c.timing;
-    // the plan's kernel sequence as one CUDA graph (captured once per plan)
-    if (!S.graph) {
+    // each plan's kernel sequence as one CUDA graph (captured once per plan)
+    for (int i = 0; i < ns; ++i) {
+        Slot &S = c.slot[c.call_slot[i]];
+        if (S.graph) continue;
         c.timing = false;
         cudaGraph_t g = nullptr;
         LMIEB_CUDA_TRY(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
@@ -1702,28 +1909,35 @@ extern "C" int lmieb_rerun_device(int reps, int flush_l2, double *ms_total, doub
             return -1;
         }
     }
-    double total = 0., st[NSTAGE] = {};
+    double total = 0., st[NSTAGE] = {}, k3 = 0.;
     cudaEvent_t e0 = c.ev[0], e1 = c.ev[NSTAGE];
     for (int i = 0; i < reps; ++i) {
         if (flush_l2) LMIEB_CUDA_TRY(cudaMemsetAsync(c.flush, i & 0xff, FLUSH_BYTES, c.stream));
         LMIEB_CUDA_TRY(cudaEventRecord(e0, c.stream));
-        LMIEB_CUDA_TRY(cudaGraphLaunch(S.graph, c.stream));
+        for (int j = 0; j < ns; ++j) LMIEB_CUDA_TRY(cudaGraphLaunch(c.slot[c.call_slot[j]].graph, c.stream));
         LMIEB_CUDA_TRY(cudaEventRecord(e1, c.stream));
         LMIEB_CUDA_TRY(cudaEventSynchronize(e1));
         float ms = 0.f;
         cudaEventElapsedTime(&ms, e0, e1);
         total += ms;
     }
-    // stage times: the same kernel sequence launched one by one between events
+    // stage times: the same kernel sequences launched one by one between events
     c.timing = true;
     for (int i = 0; i < reps; ++i) {
         if (flush_l2) LMIEB_CUDA_TRY(cudaMemsetAsync(c.flush, i & 0xff, FLUSH_BYTES, c.stream));
-        if (run_kernels(*S.plan, c.stream)) { c.timing = was; return -1; }
-        LMIEB_CUDA_TRY(cudaEventSynchronize(c.ev[8]));
-        for (int k = 1; k < 8; ++k) {
-            float sm = 0.f;
-            cudaEventElapsedTime(&sm, c.ev[k], c.ev[k + 1]);
-            st[k] += sm;
+        for (int j = 0; j < ns; ++j) {
+            const Plan &PL = *c.slot[c.call_slot[j]].plan;
+            if (run_kernels(*c.slot[c.call_slot[j]].plan, c.stream)) { c.timing = was; return -1; }
+            LMIEB_CUDA_TRY(cudaEventSynchronize(c.ev[8]));
+            for (int k = 1; k < 8; ++k) {
+                float sm = 0.f;
+                cudaEventElapsedTime(&sm, c.ev[k], c.ev[k + 1]);
+                st[k] += sm;
+            }
+            if (PL.oz && PL.n_ang > 0) {
+                float km = 0.f;
+                if (cudaEventElapsedTime(&km, c.k3[0], c.k3[1]) == cudaSuccess) k3 += km;
+            }
         }
     }
     c.timing = was;
@@ -1731,6 +1945,20 @@ extern "C" int lmieb_rerun_device(int reps, int flush_l2, double *ms_total, doub
     if (ms_total) *ms_total = total;
     if (ms_stage)
         for (int k = 0; k < NSTAGE; ++k) ms_stage[k] = st[k];
+    c.k3_ms = k3;
+    return 0;
+}
+
+extern "C" int lmieb_last_redo(long long *cases) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    if (cases) *cases = g_ctx.redo;
+    return 0;
+}
+
+extern "C" int lmieb_last_int8_kernel(double *tensor_ops, double *ms) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    if (tensor_ops) *tensor_ops = g_ctx.tensor_ops;
+    if (ms) *ms = g_ctx.k3_ms;
     return 0;
 }
 
@@ -1822,6 +2050,73 @@ extern "C" int lmieb_tc_selftest(int K, double *max_rel_err) {
     return 0;
 }
 
+extern "C" int lmieb_oz_selftest(int K, double *max_rel_err) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    if (K <= 0 || K % OZ_KC || K > OZ_KC * OZ_MAX_NK || !max_rel_err) {
+        fprintf(stderr, "ERROR: lmieb_oz_selftest: K must be a positive multiple of %d, at most %d\n", OZ_KC,
+                OZ_KC * OZ_MAX_NK);
+        return -1;
+    }
+    if (ensure_ready()) return -1;
+    const int M = OZ_M, N = OZ_NP;   // one product tile
+    std::vector<double> a((size_t) M * K), b((size_t) N * K), d((size_t) M * N), ref((size_t) M * N, 0.);
+    // seeded operands with the growth of the angular products in k: A ~ k^2,
+    // B ~ 1/k with a decaying tail, both spanning orders of magnitude over rows
+    unsigned long long st = 0x9E3779B97F4A7C15ull;
+    auto rnd = [&]() {
+        st ^= st << 13; st ^= st >> 7; st ^= st << 17;
+        return (double) (st >> 11) * (1. / 9007199254740992.) * 2. - 1.;
+    };
+    for (int i = 0; i < M; ++i)
+        for (int k = 0; k < K; ++k) a[(size_t) i * K + k] = rnd() * (k + 1.) * (k + 2.) * exp2(-(i % 17));
+    for (int n = 0; n < N; ++n)
+        for (int k = 0; k < K; ++k) b[(size_t) n * K + k] = rnd() / (k + 1.) * exp(-4. * k / K) * exp2(n % 23 - 11);
+    // reference sums in long double; the error of each element against the
+    // largest |a_ik b_nk| of its row and column pair
+    double worst = 0.;
+    for (int i = 0; i < M; ++i)
+        for (int n = 0; n < N; ++n) {
+            long double sum = 0.L;
+            for (int k = 0; k < K; ++k) sum += (long double) a[(size_t) i * K + k] * b[(size_t) n * K + k];
+            ref[(size_t) i * N + n] = (double) sum;
+        }
+    double *da = nullptr, *db = nullptr, *dd = nullptr;
+    int *derr = nullptr, herr = 0;
+    cudaStream_t s = g_ctx.stream;
+    int rc = -1;
+    if (cudaMalloc((void **) &da, a.size() * 8) == cudaSuccess && cudaMalloc((void **) &db, b.size() * 8) == cudaSuccess &&
+        cudaMalloc((void **) &dd, d.size() * 8) == cudaSuccess && cudaMalloc((void **) &derr, 4) == cudaSuccess &&
+        cudaMemcpyAsync(da, a.data(), a.size() * 8, cudaMemcpyHostToDevice, s) == cudaSuccess &&
+        cudaMemcpyAsync(db, b.data(), b.size() * 8, cudaMemcpyHostToDevice, s) == cudaSuccess &&
+        cudaMemsetAsync(derr, 0, 4, s) == cudaSuccess && launch_oz_selftest(s, K, da, db, dd, derr) == 0 &&
+        cudaMemcpyAsync(d.data(), dd, d.size() * 8, cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+        cudaMemcpyAsync(&herr, derr, 4, cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+        cudaStreamSynchronize(s) == cudaSuccess)
+        rc = 0;
+    cudaFree(da); cudaFree(db); cudaFree(dd); cudaFree(derr);
+    if (rc) {
+        fprintf(stderr, "ERROR: lmieb_oz_selftest: %s\n", cudaGetErrorString(cudaGetLastError()));
+        return -1;
+    }
+    if (herr) {
+        fprintf(stderr, "ERROR: lmieb_oz_selftest: the tensor-core pipeline timed out\n");
+        return -1;
+    }
+    for (int i = 0; i < M; ++i)
+        for (int n = 0; n < N; ++n) {
+            double ma = 0., mb = 0.;
+            for (int k = 0; k < K; ++k) {
+                ma = std::max(ma, fabs(a[(size_t) i * K + k]));
+                mb = std::max(mb, fabs(b[(size_t) n * K + k]));
+            }
+            const double scale = ma * mb;
+            const double e = fabs(d[(size_t) i * N + n] - ref[(size_t) i * N + n]);
+            worst = std::max(worst, scale > 0. ? e / scale : e);
+        }
+    *max_rel_err = worst;
+    return 0;
+}
+
 extern "C" void lmieb_host_phase(int phase, double ms) {
     std::lock_guard<std::mutex> lock(g_mu);
     if (phase >= 0 && phase < LMIEB_N_HOST) g_ctx.host_ms[phase] = ms;
@@ -1835,12 +2130,12 @@ extern "C" int lmieb_last_host_timing(double *ms, int n) {
 
 extern "C" int lmieb_set_work_granularity(int precision, double items_per_sm) {
     std::lock_guard<std::mutex> lock(g_mu);
-    if ((precision != LMIEB_PRECISION_FP64 && precision != LMIEB_PRECISION_TF32X3) || !(items_per_sm >= 0.25) ||
-        items_per_sm > 256.) {
+    if ((precision != LMIEB_PRECISION_FP64 && precision != LMIEB_PRECISION_TF32X3 &&
+         precision != LMIEB_PRECISION_INT8) || !(items_per_sm >= 0.25) || items_per_sm > 256.) {
         fprintf(stderr, "ERROR: lmieb_set_work_granularity: precision %d, items per SM %g\n", precision, items_per_sm);
         return -1;
     }
-    g_items_per_sm[precision == LMIEB_PRECISION_TF32X3 ? 1 : 0] = items_per_sm;
+    g_items_per_sm[prec_slot(precision)] = items_per_sm;
     return 0;
 }
 
@@ -1861,5 +2156,5 @@ extern "C" int lmieb_get_split_segment(void) {
 
 extern "C" double lmieb_get_work_granularity(int precision) {
     std::lock_guard<std::mutex> lock(g_mu);
-    return g_items_per_sm[precision == LMIEB_PRECISION_TF32X3 ? 1 : 0];
+    return g_items_per_sm[prec_slot(precision)];
 }

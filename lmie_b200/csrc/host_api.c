@@ -920,7 +920,8 @@ int lmie_solution_batch2(int n_cases, lmie_in_data *in, lmie_out_data *out, int 
      double t0, t_prep = 0., t_fin = 0.;
      if (n_cases <= 0)
           return 0;
-     if (precision != LMIEB_PRECISION_FP64 && precision != LMIEB_PRECISION_TF32X3) {
+     if (precision != LMIEB_PRECISION_FP64 && precision != LMIEB_PRECISION_TF32X3 &&
+         precision != LMIEB_PRECISION_INT8) {
           fprintf(stderr, "ERROR: lmie_solution_batch2(): unknown precision %d\n", precision);
           return -1;
      }
@@ -1049,13 +1050,15 @@ int lmie_solution_autotune(int n_cases, lmie_in_data *in, lmie_out_data *out, in
                            int *best_chunks, double *best_items, double *best_ms) {
      static const int chunk_c[] = {1, 2, 3, 4, 6};
      static const double items_fp64[] = {32., 64., 128., 256.}, items_tc[] = {1., 2., 4.};
-     const double *items = precision == LMIEB_PRECISION_TF32X3 ? items_tc : items_fp64;
-     const int n_items = precision == LMIEB_PRECISION_TF32X3 ? 3 : 4;
+     const int tensor = precision == LMIEB_PRECISION_TF32X3 || precision == LMIEB_PRECISION_INT8;
+     const double *items = tensor ? items_tc : items_fp64;
+     const int n_items = tensor ? 3 : 4;
      const int keep = g_pipeline, keep_timing = lmieb_timing_state();
      const double keep_items = lmieb_get_work_granularity(precision);
      int a, b, r, bc = keep, rc = 0;
      double bi = keep_items, bd = -1., bt = -1.;
-     if (n_cases < 1 || (precision != LMIEB_PRECISION_FP64 && precision != LMIEB_PRECISION_TF32X3)) {
+     if (n_cases < 1 || (precision != LMIEB_PRECISION_FP64 && precision != LMIEB_PRECISION_TF32X3 &&
+                         precision != LMIEB_PRECISION_INT8)) {
           fprintf(stderr, "ERROR: lmie_solution_autotune(): invalid arguments\n");
           return -1;
      }

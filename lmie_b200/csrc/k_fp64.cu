@@ -27,17 +27,6 @@
 
 namespace {
 
-// case c with start[c] <= e < start[c + 1]
-__device__ __forceinline__ int find_case(const long long *__restrict__ start, int ncase, long long e) {
-    int lo = 0, hi = ncase - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (start[mid] <= e) lo = mid;
-        else hi = mid - 1;
-    }
-    return lo;
-}
-
 // ---------------------------------------------------------------------------
 // Gauss-Legendre nodes: one thread per root pair, Newton with the
 // second-order correction of Davis & Rabinowitz.  The initial guesses come
@@ -1059,7 +1048,8 @@ __global__ void __launch_bounds__(EX_TMAX) k_exp_tile(DevBatch B, const ExpItem 
 // |coef_0(l)| <= accuracy).
 template <int KIND>
 __global__ void k_exp_final(DevBatch B, long long total, const long long *__restrict__ start,
-                            const double *__restrict__ exq, double *__restrict__ coefs, int *__restrict__ trunc) {
+                            const double *__restrict__ exq, double *__restrict__ coefs, int *__restrict__ trunc,
+                            int *__restrict__ band) {
     const long long e = (long long) blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= total) return;
     const int c = find_case(start, B.ncase, e);
@@ -1089,6 +1079,13 @@ __global__ void k_exp_final(DevBatch B, long long total, const long long *__rest
 #pragma unroll
     for (int k = 0; k < 6; ++k) o[(size_t) k * ncf + l] = v[k];
     if (col == 0 && fabs(v[0]) <= C.accuracy) atomicMax(trunc + c, ncf - l);
+    if (col == 0 && C.trunc_band > 0.) {
+        // where |beta_l| first comes within the band of `accuracy` from above and
+        // from below: the truncation is certain when neither lies on another l
+        const double d = C.trunc_band * (2. * l + 1.);
+        if (fabs(v[0]) <= C.accuracy + d) atomicMax(band + 2 * c, ncf - l);
+        if (fabs(v[0]) <= C.accuracy - d) atomicMax(band + 2 * c + 1, ncf - l);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1239,7 +1236,7 @@ int run_angular_nc2(cudaStream_t s, const DevBatch &B, int nc2, int c1base, int 
 template <int KIND>
 int run_expand(cudaStream_t s, const DevBatch &B, long long nck, const long long *ck_start,
                int nitems, const ExpItem *items, long long nfin, const long long *fin_start, const double *pfn,
-               double *ckpt, double *exq, double *coefs, int *trunc) {
+               double *ckpt, double *exq, double *coefs, int *trunc, int *band) {
     constexpr int NF = KIND == 0 ? 4 : 1;
     constexpr int SMAX = 200 * 1024;
     constexpr int NM = KIND == 0 ? 8 : 6;
@@ -1259,7 +1256,7 @@ int run_expand(cudaStream_t s, const DevBatch &B, long long nck, const long long
     const int nt = std::min(EX_TMAX, std::max(128, ((1 + B.nd) * EX_LT + 31) / 32 * 32));
     k_exp_tile<KIND><<<nitems, nt, sm, s>>>(B, items, pfn, ckpt, exq);
     LMIEB_CUDA_TRY(cudaGetLastError());
-    k_exp_final<KIND><<<ceil_div(nfin, 256), 256, 0, s>>>(B, nfin, fin_start, exq, coefs, trunc);
+    k_exp_final<KIND><<<ceil_div(nfin, 256), 256, 0, s>>>(B, nfin, fin_start, exq, coefs, trunc, band);
     LMIEB_CUDA_TRY(cudaGetLastError());
     return 0;
 }
@@ -1356,11 +1353,12 @@ int launch_normalize(cudaStream_t s, const DevBatch &B, long long total, const l
 int launch_expand(cudaStream_t s, const DevBatch &B, int kind, long long nck,
                   const long long *ck_start, int nitems, const ExpItem *items, long long nfin,
                   const long long *fin_start, const double *pfn, double *ckpt, double *exq,
-                  double *coefs, int *trunc) {
+                  double *coefs, int *trunc, int *band) {
     if (nitems <= 0) return 0;
     if (kind == 0)
-        return run_expand<0>(s, B, nck, ck_start, nitems, items, nfin, fin_start, pfn, ckpt, exq, coefs, trunc);
-    return run_expand<1>(s, B, nck, ck_start, nitems, items, nfin, fin_start, pfn, ckpt, exq, coefs, trunc);
+        return run_expand<0>(s, B, nck, ck_start, nitems, items, nfin, fin_start, pfn, ckpt, exq, coefs, trunc,
+                             band);
+    return run_expand<1>(s, B, nck, ck_start, nitems, items, nfin, fin_start, pfn, ckpt, exq, coefs, trunc, band);
 }
 
 int launch_phase_user(cudaStream_t s, const DevBatch &B, int kind, long long total, const long long *start,

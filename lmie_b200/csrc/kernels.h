@@ -32,6 +32,10 @@ struct DevCase {
     long long mu_user_off;      // user-angle cosines
     int scal_off;               // [ncol][4] normalised cross sections and g
     int G;                      // angular radius groups
+    int nkx;                    // int8 K3: chunks of OZ_KC orders its row exponents cover
+    long long rx_off;           // int8 K3: its row exponents ([nh][nkx][2] bytes)
+    double trunc_band;          // > 0: K4 records where |beta_l| comes within trunc_band (2l + 1)
+                                // of `accuracy` (band[2c], band[2c + 1]; see launch_expand)
 };
 
 struct DevBatch {
@@ -60,7 +64,12 @@ struct DevBatch {
                                 //     (-1: the radius' case keeps the FP64 angular stage)
     const long long *tc_roff;   // [R] float offset of the radius' group in the B operand
     const int *tg_r0, *tg_n, *tg_nk;   // per group: first radius, radii, chunks of TC_KC orders
-    const long long *tg_off;    // per group: float offset of its B operand block
+    const long long *tg_off;    // per group: float offset of its B operand block (int8 K3: byte offset)
+    // int8 fixed-point K3 (oz_layout.cuh); null in the other forms
+    const double *oz_f2;        // [OZ_KC * max chunks + 2]: (k + 1) / k
+    const signed char *oz_rowexp;   // row exponents (DevCase.rx_off)
+    const int *oz_colexp;       // [group][OZ_NP] column exponents
+    const long long *oz_bcorr;  // [group][OZ_NP][2] bias terms of the digit combination
 };
 
 // Coefficient columns: column 0 = value, column 1+k = index1 slot k.  Entry
@@ -98,6 +107,18 @@ int launch_angular_tc(cudaStream_t s, const DevBatch &B, int nitems, const AngIt
                       double *part, int seg, int *err);
 // D[128 x 240] = A[128 x K] B[240 x K]^T through the same tensor-core path
 int launch_tc_selftest(cudaStream_t s, int K, const double *A, const double *Bm, double *D, int *err);
+// K3 as an exact fixed-point contraction on the int8 tensor cores (k_oz.cu):
+// the row exponents (thread per (case, half-angle) of the flat index space
+// row_start) and the B operand digits and column exponents (block per radius
+// group) from K1's FP64 coefficient columns, then the products; items as for
+// launch_angular_tc.  bcorr: [group][OZ_NP][2] terms of the combination.
+int launch_oz_operands(cudaStream_t s, const DevBatch &B, long long nrow, const long long *row_start,
+                       signed char *rowexp, int ngroups, const double *coef, unsigned char *bop, int *colexp,
+                       long long *bcorr);
+int launch_angular_oz(cudaStream_t s, const DevBatch &B, int nitems, const AngItem *items, const unsigned char *bop,
+                      double *part, int *err);
+// D[128 x OZ_NP] = A[128 x K] B[OZ_NP x K]^T through the same fixed-point path
+int launch_oz_selftest(cudaStream_t s, int K, const double *A, const double *Bm, double *D, int *err);
 // per-case element lists: element e of the flat index space belongs to the
 // case c with start[c] <= e < start[c+1] (start has ncase + 1 entries)
 int launch_reduce_pf(cudaStream_t s, const DevBatch &B, long long total, const long long *start,
@@ -108,7 +129,11 @@ int launch_save_reweight(cudaStream_t s, const DevBatch &B, int n_qang, const do
 int launch_normalize(cudaStream_t s, const DevBatch &B, long long total, const long long *start,
                      const double *sums, const double *pfacc, double *scal, double *pfn);
 
-// K4: expansion over Gauss angles.  kind 0: GSF, 1: Legendre.
+// K4: expansion over Gauss angles.  kind 0: GSF, 1: Legendre.  trunc[c] gets
+// n_coef - l for the first l with |beta_l| <= accuracy (0: none); for cases
+// with a truncation band d_l = C.trunc_band (2l + 1), band[2c] and band[2c+1]
+// get n_coef - l for the first l with |beta_l| <= accuracy + d_l and
+// <= accuracy - d_l.
 constexpr int PU_T = 64;       // user angles per K5 block (and orders staged per step)
 constexpr int EX_LT = 32;       // orders per tile
 constexpr int EX_AT = 32;       // half-angles per tile
@@ -120,7 +145,7 @@ struct ExpItem {
 int launch_expand(cudaStream_t s, const DevBatch &B, int kind, long long nck,
                   const long long *ck_start, int nitems, const ExpItem *items, long long nfin,
                   const long long *fin_start, const double *pfn, double *ckpt, double *exq,
-                  double *coefs, int *trunc);
+                  double *coefs, int *trunc, int *band);
 
 // K5: flat (case, column, user angle) index space.
 int launch_phase_user(cudaStream_t s, const DevBatch &B, int kind, long long total, const long long *start,

@@ -1,0 +1,197 @@
+"""Fixed-point angular contraction on the int8 tensor cores
+(lmie_solution_batch2(..., LMIEB_PRECISION_INT8)).
+
+Every operand value is scaled by powers of two and split into six signed
+8-bit digits whose products are summed exactly in int32 (tcgen05.mma
+kind::i8); everything else is the FP64 form's arithmetic.  The FP64 form of
+the same library is the reference here: it is pinned to the reference
+implementation at 1e-10 by the parity tests.  The contract checked below:
+  - the truncation n_coef is the FP64 form's in every case: cases whose
+    |beta_l| come within the contraction's error band of `accuracy` are
+    solved again in FP64 within the same call;
+  - cross sections, g, reff/veff ...: identical to FP64 (not touched);
+  - every output array (gc, lc, pf and their derivatives) within 1e-9 of FP64
+    as max|got - want| / max|want|, and every derivative slice (one
+    derivative, one element) within 1e-8 of its own maximum -- the split-
+    precision target is 1e-6, so these bounds leave three orders of margin
+    over what the contraction carries (measured: 6e-12 per array, 2e-10 per
+    slice over the 4096-case uneven workload).
+"""
+import ctypes as C
+import dataclasses
+
+import numpy as np
+import pytest
+
+import libs
+from cases import all_cases
+from lmie_b200 import abi, workloads
+
+pytestmark = pytest.mark.gpu
+
+SCALARS_TOL = 1e-13
+ARRAY_TOL = 1e-9
+SLICE_TOL = 1e-8
+# the band of the re-solve: |beta_l(int8) - beta_l(FP64)| <= BAND (2l + 1)
+# (oz_layout.cuh OZ_TRUNC_BAND); the measured bound is checked against it
+BAND = 5e-13
+
+
+def _lib():
+    lib = libs.product()
+    lib.lmieb_last_redo.restype = C.c_int
+    lib.lmieb_last_redo.argtypes = [C.POINTER(C.c_longlong)]
+    lib.lmieb_oz_selftest.restype = C.c_int
+    lib.lmieb_oz_selftest.argtypes = [C.c_int, C.POINTER(C.c_double)]
+    return lib
+
+
+def _redo(lib):
+    n = C.c_longlong(-1)
+    assert lib.lmieb_last_redo(C.byref(n)) == 0
+    return n.value
+
+
+def _both(cases, n_threads=16):
+    lib = _lib()
+    ref = abi.solve_batch(lib, cases, n_threads=n_threads, precision=abi.PRECISION_FP64)
+    got = abi.solve_batch(lib, cases, n_threads=n_threads, precision=abi.PRECISION_INT8)
+    return ref, got, _redo(lib)
+
+
+def _slices(a, b):
+    worst = 0.0
+    for i in range(b.shape[0]):
+        for e in range(b.shape[1]):
+            m = float(np.max(np.abs(b[i, e])))
+            if m > 0:
+                worst = max(worst, float(np.max(np.abs(a[i, e] - b[i, e]))) / m)
+    return worst
+
+
+def _check(got, want, label):
+    assert got.rc == 0 and want.rc == 0, label
+    assert got.n_coef == want.n_coef, (label, got.n_coef, want.n_coef)
+    err = libs.compare(got, want)
+    scal = {k: v for k, v in err.items() if k not in libs.ARRAYS and k != "n_coef" and v > SCALARS_TOL}
+    assert not scal, (label, scal)
+    for name in ("gc", "lc", "pf", "gc_l", "lc_l", "pf_l"):
+        if name in err:
+            assert err[name] <= ARRAY_TOL, (label, name, err[name])
+    for name in ("gc_l", "lc_l", "pf_l"):
+        a, b = getattr(got, name), getattr(want, name)
+        if b is not None:
+            s = _slices(a, b)
+            assert s <= SLICE_TOL, (label, name, s)
+    return err
+
+
+@pytest.mark.parametrize("K", [32, 256, 5120])
+def test_selftest_contraction(K):
+    """One 128 x 64 product through the same scaling, digit slices, tensor
+    memory, products and exact combination, against long-double sums: the
+    error of each element relative to max|a_i.| max|b_n.|."""
+    e = C.c_double(-1.)
+    assert _lib().lmieb_oz_selftest(K, C.byref(e)) == 0
+    assert 0. <= e.value < 1e-11, e.value
+
+
+def test_selftest_rejects_bad_k():
+    e = C.c_double(-1.)
+    assert _lib().lmieb_oz_selftest(48, C.byref(e)) == -1
+    assert _lib().lmieb_oz_selftest(32 * 161, C.byref(e)) == -1
+
+
+@pytest.mark.parametrize("name", ["c1", "c2", "example", "x1000_few_radii", "nine_derivs", "lognormal_gc_lc"])
+def test_named_cases(name):
+    (ref,), (got,), _ = _both([all_cases()[name]])
+    _check(got, ref, name)
+
+
+def test_uneven_workload_every_case():
+    """The whole 4096-case uneven workload (size parameters up to ~1000,
+    derivatives of mr, mi, r_eff, v_eff): the same n_coef in every case and
+    every array and derivative slice within the bounds."""
+    cases = workloads.batched_uneven(4096)
+    ref, got, redo = _both(cases)
+    for i, (g, r) in enumerate(zip(got, ref)):
+        _check(g, r, f"case {i}")
+    # the re-solve is rare: the band is a few 1e-13 (2l + 1) wide
+    assert 0 <= redo < len(cases) // 50, redo
+
+
+def test_expansion_error_within_the_band():
+    """With accuracy 0 nothing is truncated: the expansion coefficients of
+    1024 cases against FP64, the bound the re-solve band relies on, with a
+    factor of two to spare."""
+    cases = [dataclasses.replace(c, accuracy=0.) for c in workloads.batched_uneven(1024)]
+    ref, got, redo = _both(cases)
+    assert redo == 0
+    worst = 0.
+    for g, r in zip(got, ref):
+        assert g.n_coef == r.n_coef
+        ell = np.arange(r.gc.shape[1])
+        worst = max(worst, float(np.max(np.abs(g.gc[0] - r.gc[0]) / (2 * ell + 1))))
+    assert worst <= BAND / 2, worst
+
+
+def test_truncation_at_the_threshold_is_solved_in_fp64():
+    """A case whose accuracy is set to one of its own |beta_l|: the truncation
+    sits exactly at the threshold, the case is solved again in FP64, and its
+    outputs are the FP64 form's bit for bit."""
+    base = all_cases()["c2"]
+    lib = _lib()
+    (full,) = abi.solve_batch(lib, [dataclasses.replace(base, accuracy=0.)], precision=abi.PRECISION_FP64)
+    beta = np.abs(full.gc[0])
+    # the first |beta_l| <= 1e-7: every earlier one is larger, so an accuracy
+    # equal to it puts the truncation exactly on the threshold
+    l0 = int(np.argmax(beta <= 1e-7))
+    assert l0 > 0 and beta[l0] > 0
+    case = dataclasses.replace(base, accuracy=float(beta[l0]))
+    (ref,), (got,), redo = _both([case])
+    assert redo == 1
+    assert got.n_coef == ref.n_coef
+    for name in ("gc", "pf", "gc_l", "pf_l"):
+        assert np.array_equal(getattr(got, name), getattr(ref, name)), name
+
+
+def test_precision_stress_large_particles():
+    """Size parameter 5000 (n1 = 5077, 10154 Gauss angles, 8000 radii, four
+    derivatives): 159 chunks per radius group, near the exact-sum limit."""
+    cases = workloads.precision_stress(2)
+    ref, got, _ = _both(cases)
+    for i, (g, r) in enumerate(zip(got, ref)):
+        _check(g, r, f"case {i}")
+
+
+def test_small_particles_keep_the_fp64_angular_stage():
+    """Cases under 16 orders run the FP64 K3 in an int8 batch, mixed with
+    tensor-core cases: their results are the FP64 form's to round-off."""
+    tiny = [dataclasses.replace(c, r2=c.lam * 0.35, r1=c.lam * 0.001) for c in workloads.batched_uneven(6)]
+    cases = tiny[:3] + workloads.batched_uneven(12)[6:] + tiny[3:]
+    ref, got, _ = _both(cases)
+    for i in list(range(3)) + list(range(len(cases) - 3, len(cases))):
+        err = libs.compare(got[i], ref[i])
+        assert got[i].n_coef == ref[i].n_coef, i
+        assert not {k: v for k, v in err.items() if v > 1e-12}, (i, err)
+    for i in range(3, len(cases) - 3):
+        _check(got[i], ref[i], f"case {i}")
+
+
+def test_int8_mode_is_deterministic():
+    cases = workloads.batched_uneven(64)
+    lib = _lib()
+    a = abi.solve_batch(lib, cases, n_threads=8, precision=abi.PRECISION_INT8)
+    b = abi.solve_batch(lib, cases, n_threads=8, precision=abi.PRECISION_INT8)
+    for x, y in zip(a, b):
+        assert np.array_equal(x.pf, y.pf) and np.array_equal(x.gc, y.gc) and np.array_equal(x.gc_l, y.gc_l)
+
+
+def test_without_derivatives_and_legendre():
+    """nd = 0 (two operand rows per radius, 16 radii per group) and the
+    Legendre expansion path."""
+    base = all_cases()["c2"]
+    cases = [dataclasses.replace(base, derivs=[], calc_lc=lc, calc_gc=1 - lc) for lc in (0, 1)]
+    ref, got, _ = _both(cases)
+    for i, (g, r) in enumerate(zip(got, ref)):
+        _check(g, r, f"variant {i}")

@@ -1,20 +1,27 @@
 """Split-precision (3xTF32) angular contraction on the tensor cores.
 
 lmie_solution_batch2(..., LMIEB_PRECISION_TF32X3) runs K3 through tcgen05.mma
-with each operand split into two TF32 terms; everything else stays FP64 (and
-cases under 16 orders keep the FP64 K3).  The FP64 form of the same library is
-the reference here: it is pinned to the reference implementation at 1e-10 by
-the parity tests.  The tolerances are stated per output array as
-max|got - want| / max|want| (the error metric of the parity tests):
+with each operand split into two TF32 terms and FP32 accumulation;
+everything else stays FP64 (and cases under 16 orders keep the FP64 K3).  The
+FP64 form of the same library is the reference here: it is pinned to the
+reference implementation at 1e-10 by the parity tests.
+
+This form's contract is narrower than the int8 form's (test_oz_gpu.py, which
+meets every bound on every case):
   - cross sections, g, reff/veff ...: not touched by K3, identical to FP64;
-  - expansions (gc, lc, gc_l, lc_l) over the shorter n_coef: <= 1e-6;
-  - the phase matrix at the user angles (pf, pf_l): <= 1e-6 where both forms
-    kept the same number of coefficients.  n_coef is the first l with
-    |beta_l| <= accuracy; with accuracy 1e-7 the split form's coefficients
-    (a few 1e-7 of beta_0 of noise) may cross the threshold at another l, and
-    pf, summed from the kept coefficients, then differs by the dropped or
-    added terms, which is a property of the truncation rule, not of the
-    contraction (checked separately with accuracy 0).
+  - expansions (gc, lc, gc_l, lc_l) over the shorter n_coef: <= 1e-6 of each
+    array's largest element;
+  - the truncation n_coef is NOT the FP64 form's in general: it is the first
+    l with |beta_l| <= accuracy, and the FP32-accumulated contraction leaves
+    1e-6 .. 4e-5 of absolute noise on the tail beta_l while the FP64 tail
+    passes the 1e-7 threshold within a few 1e-9 (measured over 256 seeded
+    uneven cases: 119 kept the FP64 n_coef).  Where the truncations differ
+    the user-angle phase matrix, summed from the kept coefficients, differs
+    by the dropped or added terms (up to 3e-6 of pf's largest element and
+    2.4e-4 of pf_l's): test_truncation_differences_are_bounded bounds it
+    on every case rather than skipping those cases;
+  - with accuracy 0 (no truncation) the phase matrix at the user angles
+    carries only the contraction's error: <= 1e-6 on every case.
 One named case is held to a looser bound on its linearised arrays: eight
 radii at x ~ 1000 (x1000_few_radii), where no averaging over a size
 distribution hides the operand split's ~22 bits in a derivative of a
@@ -85,14 +92,29 @@ def test_named_cases(name, deriv_tol):
 
 def test_uneven_batch():
     """A slice of the seeded uneven workload (size parameters up to ~1000,
-    derivatives of mr, mi, r_eff, v_eff)."""
+    derivatives of mr, mi, r_eff, v_eff): the bounds above on every case
+    whose truncation agrees with FP64."""
     cases = workloads.batched_uneven(192)
     ref, got = _both(cases, n_threads=16)
-    same = 0
     for i, (g, r) in enumerate(zip(got, ref)):
         _check(g, r, f"case {i}")
-        same += g.n_coef == r.n_coef
-    assert same >= len(cases) // 4, same
+
+
+def test_truncation_differences_are_bounded():
+    """Every case of the slice, including those whose truncation differs: the
+    user-angle phase matrix within 1e-5 of its largest element and its
+    linearisations within 5e-3 -- the dropped or added tail terms (measured
+    on this slice: 3.0e-6 and 2.4e-4), which is why this form does not meet
+    the 1e-6 target and the int8 form does."""
+    cases = workloads.batched_uneven(192)
+    ref, got = _both(cases, n_threads=16)
+    differ = 0
+    for i, (g, r) in enumerate(zip(got, ref)):
+        assert g.rc == 0 and r.rc == 0, i
+        differ += g.n_coef != r.n_coef
+        assert libs.relmax(g.pf, r.pf) <= 1e-5, (i, libs.relmax(g.pf, r.pf))
+        assert libs.relmax(g.pf_l, r.pf_l) <= 5e-3, (i, libs.relmax(g.pf_l, r.pf_l))
+    assert 0 < differ < len(cases), differ
 
 
 def test_pf_with_untruncated_expansion():
