@@ -44,11 +44,11 @@ int lmie_solution_batch(int n_cases, lmie_in_data *in, lmie_out_data *out, int a
 #define LMIEB_PRECISION_TF32X3 1
 /* LMIEB_PRECISION_INT8: the angular S1/S2 contraction runs on the int8 tensor
  *   cores as an exact fixed-point sum: each operand value is scaled by powers
- *   of two (per order, per angle row, per operand column) to 46 fractional
+ *   of two (per order, per angle row, per operand column) to 47 fractional
  *   bits and split into six signed 8-bit digits; the 21 digit products that
- *   carry the result are summed exactly in int32 and combined in FP64.  The
- *   contraction carries about 1e-12 of the largest term of its row and column
- *   (FP64: about 1e-16); everything else is the FP64 form's arithmetic.  A case
+ *   carry the result are summed exactly in int32 and combined in FP64.  Each
+ *   product carries about 2^-46 of the largest term of its row and column
+ *   (FP64: 2^-53); everything else is the FP64 form's arithmetic.  A case
  *   whose truncation n_coef could depend on that difference -- some
  *   |beta_l| (l < n_coef) within the contraction's error bound of `accuracy`
  *   -- is solved again in FP64 within the same call, so n_coef is always the
@@ -98,6 +98,19 @@ int lmie_solution_autotune(int n_cases, lmie_in_data *in, lmie_out_data *out, in
  * of an element relative to max|a_i.| max|b_n.| of its row and column.
  * Returns 0 or -1. */
 int lmieb_oz_selftest(int K, double *max_rel_err);
+
+/* The same with the product waits bounded by wait_cycles (1 .. 2^31 SM clock
+ * cycles; lmieb_oz_selftest uses 2^31, about a second) and, when withhold is
+ * nonzero, the first chunk's products never issued: the wait for them runs
+ * out, the kernel releases its tensor memory, sets its error word and returns,
+ * and the call returns -1 with the device still usable -- the failure path of
+ * the product kernel's bounded waits, taken without a fault. */
+int lmieb_oz_selftest_wait(int K, long long wait_cycles, int withhold, double *max_rel_err);
+
+/* Device memory: out[0] free and out[1] total bytes of the current device
+ * (cudaMemGetInfo), out[2] device bytes and out[3] pinned host bytes the
+ * library holds (arenas, staging buffers, pools).  Returns 0 or -1. */
+int lmieb_memory(long long out[4]);
 
 /* lmie_solution_batch with the arithmetic chosen by `precision`. */
 int lmie_solution_batch2(int n_cases, lmie_in_data *in, lmie_out_data *out, int alloc_out,
@@ -262,8 +275,8 @@ int lmieb_fp64_peak(double *tflops);
  * every GPU that loads the library keeps until the process exits; no call
  * allocates or frees device memory.  All calls on a device share that array:
  * calls that overlap on the GPU (other threads, other streams) race on it.
- * The first call on a device looks up the array's device address, so make it
- * before any stream capture.  Runs on the calling thread's current device on
+ * The first call on a device looks up the array's device address; every call
+ * copies the radii to the host and waits for `stream`.  Runs on the calling thread's current device on
  * `stream` (a cudaStream_t; NULL for the default stream) and returns after
  * the results are in `out`.  Returns 0 or -1. */
 int lmie_cross_sections_noalloc(int n_radii, const double *radius, double lambda,

@@ -105,6 +105,11 @@ struct Ctx {
     double k3_ms = 0.;
     long long launches = 0;         // kernel launches of one device run of the last solve
     size_t h2d = 0, d2h = 0;        // bytes copied by the last solve
+    // radius groups: whether this process's solve has entered the group's
+    // reduction, and the block a failed solve reduces instead of its own
+    bool group_joined = false;
+    double *gfail = nullptr;
+    size_t gfail_cap = 0;
     // Gauss-Legendre angles depend only on their number: computed once per n
     // into a device pool ([n nodes][n weights] per entry) and kept
     double *gl_pool = nullptr;
@@ -346,30 +351,65 @@ int ensure_ready() {
     return 0;
 }
 
+// Host-side fault injection (tests of the failure paths; no GPU fault is
+// involved): while the environment variable LMIEB_FAULT holds a site name --
+// "alloc" (the device arena), "pinned" (the pinned staging buffer), "h2d" (a
+// sub-batch's input upload) or "graph" (instantiating a captured kernel
+// sequence), several separated by commas -- that step fails as its CUDA call
+// would (the arena and the staging buffer are released first, as when a
+// larger one cannot be had), and the error propagates as -1.
+bool fault_injected(const char *site);
+}  // namespace
+
+// the injector for the host code of host_api.c ("prepare": a case's host
+// preparation)
+extern "C" int lmieb_fault_injected(const char *site) { return fault_injected(site) ? 1 : 0; }
+
+namespace {
+bool fault_injected(const char *site) {
+    const char *v = getenv("LMIEB_FAULT");
+    if (!v || !*v) return false;
+    const size_t n = strlen(site);
+    for (const char *p = v; *p;) {
+        const char *e = strchr(p, ',');
+        const size_t len = e ? (size_t) (e - p) : strlen(p);
+        if (len == n && strncmp(p, site, n) == 0) {
+            fprintf(stderr, "ERROR: lmie_b200: injected failure at \"%s\" (LMIEB_FAULT)\n", site);
+            return true;
+        }
+        if (!e) break;
+        p = e + 1;
+    }
+    return false;
+}
+
 void drop_graph(Slot &S) {
     if (S.graph) cudaGraphExecDestroy(S.graph);
     S.graph = nullptr;
 }
 
 int ensure_device(Slot &S, size_t bytes) {
-    if (bytes <= S.dcap) return 0;
+    const bool fail = fault_injected("alloc");
+    if (bytes <= S.dcap && !fail) return 0;
+    S.have_plan = false;
+    drop_graph(S);
     if (S.dbuf) LMIEB_CUDA_TRY(cudaFree(S.dbuf));
     S.dbuf = nullptr;
     S.dcap = 0;
     size_t want = bytes + bytes / 4;
-    LMIEB_CUDA_TRY(cudaMalloc((void **) &S.dbuf, want));
+    LMIEB_CUDA_TRY(fail ? cudaErrorMemoryAllocation : cudaMalloc((void **) &S.dbuf, want));
     S.dcap = want;
-    S.have_plan = false;
     return 0;
 }
 
 int ensure_host(Slot &S, size_t bytes) {
-    if (bytes <= S.hcap) return 0;
+    const bool fail = fault_injected("pinned");
+    if (bytes <= S.hcap && !fail) return 0;
     if (S.hbuf) LMIEB_CUDA_TRY(cudaFreeHost(S.hbuf));
     S.hbuf = nullptr;
     S.hcap = 0;
     size_t want = bytes + bytes / 4;
-    LMIEB_CUDA_TRY(cudaMallocHost((void **) &S.hbuf, want));
+    LMIEB_CUDA_TRY(fail ? cudaErrorMemoryAllocation : cudaMallocHost((void **) &S.hbuf, want));
     S.hcap = want;
     return 0;
 }
@@ -485,12 +525,13 @@ int run_kernels(Plan &L, cudaStream_t s) {
     return run_accumulate(L, s) || run_finish(L, s) ? -1 : 0;
 }
 
-// Sums the integrals of a LMIEB_ACC_GROUP sub-batch over the radius group,
-// on stream s between run_accumulate and run_finish.
-int reduce_group(Plan &L, cudaStream_t s) {
+// In-place sum over the radius group of `count` doubles at device address
+// buf, written on stream s: the library's NCCL all-reduce queued on s, or the
+// caller's reduction on the synchronised buffer.
+int group_reduce(double *buf, size_t count, cudaStream_t s) {
     const RadiusGroup &g = g_group;
     if (g.comm) {
-        const int r = g_nccl.all_reduce(L.sums, L.sums, L.acc_n, NCCL_FLOAT64, NCCL_SUM, g.comm, s);
+        const int r = g_nccl.all_reduce(buf, buf, count, NCCL_FLOAT64, NCCL_SUM, g.comm, s);
         if (r != 0) {
             fprintf(stderr, "ERROR: lmie_b200: ncclAllReduce: %s\n", g_nccl.error_string(r));
             return -1;
@@ -499,11 +540,48 @@ int reduce_group(Plan &L, cudaStream_t s) {
     }
     if (!g.fn) return 0;
     LMIEB_CUDA_TRY(cudaStreamSynchronize(s));
-    if (g.fn(L.sums, (long long) L.acc_n, (void *) s, g.fn_ctx) != 0) {
+    if (g.fn(buf, (long long) count, (void *) s, g.fn_ctx) != 0) {
         fprintf(stderr, "ERROR: lmie_b200: the radius group's reduction failed\n");
         return -1;
     }
     return 0;
+}
+
+// Sums the integrals of a LMIEB_ACC_GROUP sub-batch over the radius group,
+// on stream s between run_accumulate and run_finish.  The block carries one
+// more double, the number of processes whose solve failed before the
+// reduction (zero here, one from each failed process: group_abort); if it
+// is not zero after the sum, the error word tells the host to return -1.
+int reduce_group(Plan &L, cudaStream_t s) {
+    g_ctx.group_joined = true;
+    LMIEB_CUDA_TRY(cudaMemsetAsync(L.sums + L.acc_n, 0, sizeof(double), s));
+    if (group_reduce(L.sums, L.acc_n + 1, s)) return -1;
+    return launch_group_flag(s, L.sums + L.acc_n, L.o_trunc + 2 * L.ncase);
+}
+
+// A process of the radius group whose solve failed before the group's
+// reduction still takes part in it, with zero integrals and a failure mark in
+// the extra slot, so that the other processes are not left waiting in theirs
+// and fail as well.  `acc_n`: the integrals of the solve, 4 (1 + n_derivs)
+// (1 + n_qang), the same on every process.  Returns -1 (the solve failed).
+int group_abort(size_t acc_n) {
+    Ctx &c = g_ctx;
+    if (!g_group.on || c.group_joined) return -1;
+    c.group_joined = true;
+    if (ensure_ready()) return -1;
+    if (acc_n + 1 > c.gfail_cap) {
+        if (c.gfail) cudaFree(c.gfail);
+        c.gfail = nullptr;
+        c.gfail_cap = 0;
+        LMIEB_CUDA_TRY(cudaMalloc((void **) &c.gfail, (acc_n + 1) * sizeof(double)));
+        c.gfail_cap = acc_n + 1;
+    }
+    static const double one = 1.;
+    LMIEB_CUDA_TRY(cudaMemsetAsync(c.gfail, 0, acc_n * sizeof(double), c.stream));
+    LMIEB_CUDA_TRY(cudaMemcpyAsync(c.gfail + acc_n, &one, sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    if (group_reduce(c.gfail, acc_n + 1, c.stream) == 0) cudaStreamSynchronize(c.stream);
+    fprintf(stderr, "ERROR: lmie_b200: this process's share of the radius group failed; the group was told\n");
+    return -1;
 }
 
 template <class T>
@@ -548,6 +626,7 @@ size_t case_bytes(const lmieb_problem &p) {
         // B operand digits (groups padded to whole chunks), row exponents
         b += (size_t) (tot + (size_t) p.n * OZ_KC) * OZ_BSTAGE / (OZ_KC * oz_rg(std::min(p.nd1, OZ_MAX_NC1)));
         b += (size_t) (p.n_qang / 2 + 1) * (tot / std::max(p.n, 1) / OZ_KC + 2) * 2;
+        b += (size_t) p.n * (1 + p.nd1) * 16;                          // exponents K1 tracks
     }
     return b;
 }
@@ -1213,12 +1292,13 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
                 add((size_t) rx_bytes);
                 add((size_t) L.n_groups * OZ_NP * 4);
                 add((size_t) L.n_groups * OZ_NP * 16);
+                add((size_t) (1 + nd1) * R * 16);
             }
             add((size_t) (1 + nd1) * (size_t) ctot * 32);
             add((size_t) (1 + nd1) * 5 * (size_t) R * 8);
             add((size_t) part_total * 8);
         }
-        add(L.acc_n * 8);                                        // sums + pfacc
+        add((L.acc_n + 1) * 8);                                  // sums + pfacc + the group's failure count
         add((size_t) L.pf_total * 8);
         add((size_t) ck_total * 8);
         add((size_t) ex_total * 8);
@@ -1290,6 +1370,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
             L.bop8 = A.take<unsigned char>((size_t) bop8_bytes);
             L.rowexp = A.take<signed char>((size_t) rx_bytes);
             L.colexp = A.take<int>((size_t) L.n_groups * OZ_NP);
+            B.oz_radexp = A.take<int>((size_t) (1 + nd1) * R * 4);
             L.bcorr = A.take<long long>((size_t) L.n_groups * OZ_NP * 2);
             B.oz_bcorr = L.bcorr;
             L.rx_start = (long long *) dptr(h_rxs);
@@ -1302,7 +1383,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         L.part = A.take<double>((size_t) part_total);
     }
     // the integrals in one block, so that a radius group sums them in one call
-    L.sums = L.acc_mode == LMIEB_ACC_FINISH ? (double *) dptr(h_acc) : A.take<double>(L.acc_n);
+    L.sums = L.acc_mode == LMIEB_ACC_FINISH ? (double *) dptr(h_acc) : A.take<double>(L.acc_n + 1);
     L.pfacc = L.sums ? L.sums + (size_t) ncase * ncol * 4 : nullptr;
     L.pfn = A.take<double>((size_t) L.pf_total);
     L.ckpt = A.take<double>((size_t) ck_total);
@@ -1340,7 +1421,8 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     stage(0);
     LMIEB_CUDA_TRY(cudaEventRecord(S.t_begin, s));
     if (c.submits == 1) LMIEB_CUDA_TRY(cudaEventRecord(c.t_first, s));
-    LMIEB_CUDA_TRY(cudaMemcpyAsync(d_in, hp, h_in_end, cudaMemcpyHostToDevice, s));
+    LMIEB_CUDA_TRY(fault_injected("h2d") ? cudaErrorInvalidValue
+                                         : cudaMemcpyAsync(d_in, hp, h_in_end, cudaMemcpyHostToDevice, s));
     LMIEB_CUDA_TRY(cudaMemsetAsync(d_out, 0, out_bytes, s));
     // Gauss-angle pool entries another sub-batch is still computing
     if (c.gl_pending) LMIEB_CUDA_TRY(cudaStreamWaitEvent(s, c.gl_ready, 0));
@@ -1514,7 +1596,10 @@ int collect_slot(Slot &S) {
     const int *htr = (const int *) hostp(P.o_trunc);
     if (htr[2 * ncase]) {
         LMIEB_CUDA_TRY(cudaEventSynchronize(S.done));   // no copy may still write the staging
-        fprintf(stderr, "ERROR: lmie_b200: a tensor-core angular stage timed out waiting for its pipeline\n");
+        if (htr[2 * ncase] == 2)
+            fprintf(stderr, "ERROR: lmie_b200: a process of the radius group failed before the group's sum\n");
+        else
+            fprintf(stderr, "ERROR: lmie_b200: a tensor-core angular stage timed out waiting for its pipeline\n");
         return -1;
     }
     for (size_t p = 0; p + 1 < P.piece.size(); ++p) {
@@ -1727,7 +1812,23 @@ extern "C" int lmieb_device_fit(int n, const lmieb_problem *p) {
 }
 
 extern "C" int lmieb_device_solve(const lmieb_problem *p, lmieb_result *r) {
-    return lmieb_device_solve_batch(1, p, r);
+    if (p->acc_mode == LMIEB_ACC_GROUP) {
+        std::lock_guard<std::mutex> lock(g_mu);
+        g_ctx.group_joined = false;
+    }
+    const int rc = lmieb_device_solve_batch(1, p, r);
+    if (rc && p->acc_mode == LMIEB_ACC_GROUP) {
+        // failed before the group's reduction: join it with a failure mark
+        std::lock_guard<std::mutex> lock(g_mu);
+        if (!g_ctx.group_joined) group_abort((size_t) 4 * (1 + p->nd) * (1 + p->n_qang));
+    }
+    return rc;
+}
+
+extern "C" int lmieb_group_abort(int n_derivs, int n_qang) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    g_ctx.group_joined = false;
+    return group_abort((size_t) 4 * (1 + n_derivs) * (1 + n_qang));
 }
 
 // ---------------------------------------------------------------------------
@@ -1901,7 +2002,7 @@ extern "C" int lmieb_rerun_device(int reps, int flush_l2, double *ms_total, doub
             fprintf(stderr, "ERROR: lmieb_rerun_device: graph capture failed (%s)\n", cudaGetErrorString(ec));
             return -1;
         }
-        const cudaError_t ei = cudaGraphInstantiate(&S.graph, g, 0);
+        const cudaError_t ei = fault_injected("graph") ? cudaErrorInvalidValue : cudaGraphInstantiate(&S.graph, g, 0);
         cudaGraphDestroy(g);
         if (ei != cudaSuccess) {
             S.graph = nullptr;
@@ -2050,11 +2151,36 @@ extern "C" int lmieb_tc_selftest(int K, double *max_rel_err) {
     return 0;
 }
 
-extern "C" int lmieb_oz_selftest(int K, double *max_rel_err) {
+extern "C" int lmieb_memory(long long out[4]) {
     std::lock_guard<std::mutex> lock(g_mu);
-    if (K <= 0 || K % OZ_KC || K > OZ_KC * OZ_MAX_NK || !max_rel_err) {
-        fprintf(stderr, "ERROR: lmieb_oz_selftest: K must be a positive multiple of %d, at most %d\n", OZ_KC,
-                OZ_KC * OZ_MAX_NK);
+    if (!out || ensure_ready()) return -1;
+    size_t fr = 0, tot = 0;
+    LMIEB_CUDA_TRY(cudaMemGetInfo(&fr, &tot));
+    const Ctx &c = g_ctx;
+    long long dev = (long long) (c.gl_cap * sizeof(double) + c.save.cap * sizeof(double));
+    if (c.flush) dev += (long long) FLUSH_BYTES;
+    long long pin = 0;
+    for (const Slot &S : c.slot) {
+        dev += (long long) S.dcap;
+        pin += (long long) S.hcap;
+    }
+    out[0] = (long long) fr;
+    out[1] = (long long) tot;
+    out[2] = dev;
+    out[3] = pin;
+    return 0;
+}
+
+extern "C" int lmieb_oz_selftest(int K, double *max_rel_err) {
+    return lmieb_oz_selftest_wait(K, LMIEB_WAIT_CYCLES, 0, max_rel_err);
+}
+
+extern "C" int lmieb_oz_selftest_wait(int K, long long wait_cycles, int withhold, double *max_rel_err) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    if (K <= 0 || K % OZ_KC || K > OZ_KC * OZ_MAX_NK || !max_rel_err || wait_cycles < 1 ||
+        wait_cycles > LMIEB_WAIT_CYCLES) {
+        fprintf(stderr, "ERROR: lmieb_oz_selftest: K must be a positive multiple of %d, at most %d; "
+                "the wait limit 1 .. %lld cycles\n", OZ_KC, OZ_KC * OZ_MAX_NK, (long long) LMIEB_WAIT_CYCLES);
         return -1;
     }
     if (ensure_ready()) return -1;
@@ -2088,7 +2214,8 @@ extern "C" int lmieb_oz_selftest(int K, double *max_rel_err) {
         cudaMalloc((void **) &dd, d.size() * 8) == cudaSuccess && cudaMalloc((void **) &derr, 4) == cudaSuccess &&
         cudaMemcpyAsync(da, a.data(), a.size() * 8, cudaMemcpyHostToDevice, s) == cudaSuccess &&
         cudaMemcpyAsync(db, b.data(), b.size() * 8, cudaMemcpyHostToDevice, s) == cudaSuccess &&
-        cudaMemsetAsync(derr, 0, 4, s) == cudaSuccess && launch_oz_selftest(s, K, da, db, dd, derr) == 0 &&
+        cudaMemsetAsync(derr, 0, 4, s) == cudaSuccess &&
+        launch_oz_selftest(s, K, da, db, dd, derr, wait_cycles, withhold) == 0 &&
         cudaMemcpyAsync(d.data(), dd, d.size() * 8, cudaMemcpyDeviceToHost, s) == cudaSuccess &&
         cudaMemcpyAsync(&herr, derr, 4, cudaMemcpyDeviceToHost, s) == cudaSuccess &&
         cudaStreamSynchronize(s) == cudaSuccess)

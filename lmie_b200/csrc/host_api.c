@@ -687,7 +687,11 @@ int lmie_solution2_l(int calc_gc, int calc_lc, int calc_pf,
      j.cext_l = cext_l; j.csca_l = csca_l; j.cbak_l = cbak_l; j.g_l = g_l;
      j.gc_l = gc_l; j.lc_l = lc_l; j.pf_l = pf_l;
      j.save1 = save1; j.save2 = save2;
-     rc = job_prepare(&j);
+     rc = lmieb_fault_injected("prepare") ? -1 : job_prepare(&j);
+     if (rc != 0 && j.acc_mode == LMIEB_ACC_GROUP)
+          /* the other processes of the group must not wait for this one */
+          lmieb_group_abort(n_derivs, (calc_gc || calc_lc) ?
+                            lmie_calc_max_coef(lambda, dist_type, a1, a2, a3, r1, r2) : 0);
      if (rc == 0 && lmieb_device_solve(&j.P, &j.R)) {
           fprintf(stderr, "ERROR: lmie_core_solution()\n");
           rc = -1;

@@ -156,6 +156,17 @@ __device__ __forceinline__ void tc_flush(const float *tcbuf, float *__restrict__
     }
 }
 
+// m[c] = max(m[c], biased exponent of component c + ek) over the normal
+// values among (Re cs, Im cs, Re cd, Im cd)
+__device__ __forceinline__ void oz_track(int (&m)[4], cplx cs, cplx cd, int ek) {
+    const double v[4] = {cs.re, cs.im, cd.re, cd.im};
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const int ex = (__double2hiint(v[c]) >> 20) & 0x7FF;
+        m[c] = max(m[c], ex ? ex + ek : 0);
+    }
+}
+
 template <int NC>
 __global__ void __launch_bounds__(64) k_mie(DevBatch B, int c0, int write_value, double *__restrict__ ck,
                                             double *__restrict__ coef, float *__restrict__ bop,
@@ -278,6 +289,12 @@ __global__ void __launch_bounds__(64) k_mie(DevBatch B, int c0, int write_value,
     const long long troff = to_tc ? B.tc_roff[r] : 0;
     extern __shared__ float tcbuf[];                  // [4][1 + NC][8][blockDim.x] when bop is set
     double4 *cf = (double4 *) coef;
+    // int8 form: the largest (biased exponent + e_k) of each column and
+    // component, the column exponents of the fixed-point B operand
+    int *const rx = B.oz_radexp;
+    int mxe[CC][4];
+#pragma unroll
+    for (int q = 0; q < 4 * CC; ++q) mxe[q / 4][q % 4] = 0;
 
     cplx Dloc[K1_B], Dlloc[NC > 0 ? NC : 1][K1_B];
     double rloc[K1_B], rlloc[NC > 0 ? NC : 1][K1_B];
@@ -393,16 +410,19 @@ __global__ void __launch_bounds__(64) k_mie(DevBatch B, int c0, int write_value,
                              fv4[j - 1] * (re_mulc(alp[k], bp) + re_mulc(ap, blp[k]));
             }
             // expansion coefficients of order j
+            const int ek = 32 - __clz(2 * j - 1);
             if (write_value) {
                 const cplx cs = (a + b) * f4, cd = (a - b) * f4;
                 if (to_tc) tc_stage<CC>(tcbuf, j, 0, cs.re, cs.im, cd.re, cd.im);
                 else cf[off + j - 1] = make_double4(cs.re, cs.im, cd.re, cd.im);
+                if (rx) oz_track(mxe[0], cs, cd, ek);
             }
 #pragma unroll
             for (int k = 0; k < NC; ++k) {
                 const cplx cs = (al[k] + bl[k]) * f4, cd = (al[k] - bl[k]) * f4;
                 if (to_tc) tc_stage<CC>(tcbuf, j, 1 + k, cs.re, cs.im, cd.re, cd.im);
                 else cf[(size_t) (1 + c0 + k) * tot + off + j - 1] = make_double4(cs.re, cs.im, cd.re, cd.im);
+                if (rx) oz_track(mxe[1 + k], cs, cd, ek);
             }
             if (to_tc && (((j - 1) & 3) == 3 || j == n1))
                 tc_flush<CC>(tcbuf, bop + troff, j, tpos, 1 + B.nd1, c0, write_value, j == n1 ? tgnk : 0);
@@ -432,6 +452,14 @@ __global__ void __launch_bounds__(64) k_mie(DevBatch B, int c0, int write_value,
         if (cc == 0 && !write_value) continue;
         const size_t col = cc == 0 ? 0 : (size_t) (1 + c0 + cc - 1);
         rs[(col * 5 + qq) * R + r] = acc[q];
+    }
+    if (rx) {
+#pragma unroll
+        for (int cc = 0; cc < CC; ++cc) {
+            if (cc == 0 && !write_value) continue;
+            const size_t col = cc == 0 ? 0 : (size_t) (1 + c0 + cc - 1);
+            *(int4 *) (rx + (col * R + r) * 4) = make_int4(mxe[cc][0], mxe[cc][1], mxe[cc][2], mxe[cc][3]);
+        }
     }
 }
 
@@ -1270,6 +1298,19 @@ int launch_gauss(cudaStream_t s, int npairs, const int *pt, const int *pi, const
                  const long long *go, const double *guess, const double *jr, double *pool) {
     if (npairs <= 0) return 0;
     k_gauss<<<ceil_div(npairs, 32), 32, 0, s>>>(npairs, pt, pi, ns, mo, go, guess, jr, pool, pool);
+    LMIEB_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+namespace {
+// the radius group's failure count after its sum: nonzero -> error word 2
+__global__ void k_group_flag(const double *__restrict__ failed, int *__restrict__ err) {
+    if (*failed != 0.) *err = 2;
+}
+}  // namespace
+
+int launch_group_flag(cudaStream_t s, const double *failed, int *err) {
+    k_group_flag<<<1, 1, 0, s>>>(failed, err);
     LMIEB_CUDA_TRY(cudaGetLastError());
     return 0;
 }

@@ -75,7 +75,8 @@ static_assert(OZ_NP % 16 == 0 && OZ_NP >= 16 && OZ_NP <= 256, "N of an M=128 kin
 static_assert(OZ_ACOL + OZ_ASTAGES * OZ_ACOLS <= OZ_TMEM_COLS, "accumulators and A stages in tensor memory");
 static_assert(OZ_WBUF % 16 == 0 && OZ_CBUF % 16 == 0, "barriers stay 8-byte aligned");
 static_assert(OZ_SMEM <= 227 * 1024, "shared memory per block");
-static_assert(OZ_FRAC == 8 * (OZ_ND - 1) + 6, "digit weights: the top digit holds |V| / 2^40 <= 32");
+// |V| <= 2^(OZ_FRAC - 1) must stay inside the six balanced digits (-0x808080808080 .. 0x7f7f7f7f7f7f)
+static_assert(OZ_FRAC - 1 <= 8 * OZ_ND - 2, "digit weights: the top digit holds |V| / 2^40 <= 64");
 static_assert(OZ_ND == 6, "oz_combine splits the six diagonals into two int64 halves");
 
 // instruction descriptor of kind::i8: D int32, A unsigned 8-bit, B signed 8-bit, both K-major
@@ -182,19 +183,17 @@ __global__ void k_oz_rowexp(DevBatch B, long long total, const long long *__rest
 // ---------------------------------------------------------------------------
 // B operand of the radius groups: block per group, thread per operand row
 // n = tid % 64 (S re, S im, ..., then D' re, D' im, ...) and every fourth
-// block of 16 orders.  Pass 1 finds the column exponents f_n (largest
-// ilogb(|v| 2^e_k) + 2 over the column), pass 2 writes the digit slices of
-// every chunk and sums the row's digits per slice; rows and orders without a
-// value get zero.
+// block of 16 orders.  The column exponent f_n (largest ilogb(|v| 2^e_k) + 2
+// over the column) comes from the exponents K1 tracked while it wrote the
+// coefficients; the kernel writes the digit slices of every chunk and sums
+// the row's digits per slice; rows and orders without a value get zero.
 // ---------------------------------------------------------------------------
 constexpr int OZ_BOP_T = 256;
 constexpr int OZ_BOP_J = OZ_BOP_T / OZ_NP;            // threads per row
-constexpr int OZ_F_NONE = -100000;
 
 __global__ void __launch_bounds__(OZ_BOP_T) k_oz_bop(DevBatch B, const double *__restrict__ coef,
                                                       unsigned char *__restrict__ bop, int *__restrict__ colexp,
                                                       long long *__restrict__ bcorr) {
-    __shared__ int fx[OZ_NP];
     __shared__ int sb[OZ_ND][OZ_NP];                  // sums of each digit slice over the group's orders
     const int g = blockIdx.x, tid = threadIdx.x;
     const int r0 = B.tg_r0[g], gn = B.tg_n[g], nk = B.tg_nk[g];
@@ -205,33 +204,20 @@ __global__ void __launch_bounds__(OZ_BOP_T) k_oz_bop(DevBatch B, const double *_
     const bool real = rp < P, dpart = n >= OZ_NHALF;
     const double *cf = coef + comp;                   // component `comp` of the double4 entries
     const size_t tot = (size_t) B.tot;
-    if (tid < OZ_NP) fx[tid] = OZ_F_NONE;
     for (int i = tid; i < OZ_ND * OZ_NP; i += OZ_BOP_T) sb[i / OZ_NP][i % OZ_NP] = 0;
-    int n1 = 0;
+    int n1 = 0, f = 0;
     size_t base = 0;
     if (real) {
         const int p = rp / C1, col = rp - p * C1, r = r0 + p;
         n1 = B.n1r[r];
         base = ((size_t) col * tot + B.off[r]) * 4;
+        // largest biased exponent + e_k: f = that - 1021 (0: the column is zero)
+        const int m = B.oz_radexp[((size_t) col * B.R + r) * 4 + comp];
+        f = m ? max(m - 1021, -900) : 0;
     }
-    __syncthreads();
-    // pass 1: the column exponent from the exponent fields (normal values)
-    {
-        int m = OZ_F_NONE;
-        for (int blk = j0; blk < 2 * nk && blk * 16 < n1; blk += OZ_BOP_J)
-#pragma unroll 4
-            for (int u = 0; u < 16; ++u) {
-                const int k = blk * 16 + u + 1;
-                if (k > n1) break;
-                const int ex = (__double2hiint(__ldg(cf + base + (size_t) (k - 1) * 4)) >> 20) & 0x7FF;
-                if (ex) m = max(m, ex - 1021 + oz_ek(k));
-            }
-        if (m != OZ_F_NONE) atomicMax(&fx[n], m);
-    }
-    __syncthreads();
-    const int f = fx[n] == OZ_F_NONE ? 0 : max(fx[n], -900);
     if (j0 == 0) colexp[(size_t) g * OZ_NP + n] = f;
-    // pass 2: digits, 16 orders at a time
+    __syncthreads();
+    // digits, 16 orders at a time
     int ds[OZ_ND] = {0, 0, 0, 0, 0, 0};
     unsigned char *rb = bop + B.tg_off[g] + (n >> 3) * 128 + (n & 7) * 16;
     for (int blk = j0; blk < 2 * nk; blk += OZ_BOP_J) {
@@ -283,7 +269,7 @@ __global__ void __launch_bounds__(OZ_BOP_T) k_oz_bop(DevBatch B, const double *_
 // tensor memory at column acol (warp-wide).  sg = +1 (row 2h) or -1 (its
 // mirror); sp / sm: the scales of odd / even orders (the mirror row carries
 // s_k); FIRST: the case's first chunk, whose orders 1..16 have their own
-// exponents (gsc = 2^(46 - g_r), 0 for an inactive row).
+// exponents (gsc = 2^(OZ_FRAC - g_r), 0 for an inactive row).
 template <bool FIRST>
 __device__ __forceinline__ void oz_produce_chunk(const double *__restrict__ f2, double mu, double sg, double sp,
                                                  double sm, double gsc, double &kmu, double &k1, double &p0,
@@ -305,7 +291,7 @@ __device__ __forceinline__ void oz_produce_chunk(const double *__restrict__ f2, 
         for (int u = 0; u < 16; ++u) {
             double sc = (u & 1) ? sm : sp;
             if (FIRST && hf == 0) {
-                // 2^(46 - e_k - g_r) with e_k = ceil(log2 2k), k = u + 1 (compile-time)
+                // 2^(OZ_FRAC - e_k - g_r) with e_k = ceil(log2 2k), k = u + 1 (compile-time)
                 constexpr double inv[5] = {0.5, 0.25, 0.125, 0.0625, 0.03125};
                 const int ek = u == 0 ? 1 : (u == 1 ? 2 : (u < 4 ? 3 : (u < 8 ? 4 : 5)));
                 sc = (u & 1) ? sg * gsc * inv[ek - 1] : gsc * inv[ek - 1];
@@ -450,7 +436,7 @@ __global__ void __launch_bounds__(OZ_T, 1) k_angular_oz(DevBatch B, const AngIte
             double p0 = 0., p1 = 1., kmu = mu, k1 = 2.;        // pi_{k-1}, pi_k, k mu, k + 1
             for (int kc = 0; kc < nk; ++kc, ++q) {
                 const int s = q % OZ_ASTAGES;
-                // the chunk's scale 2^(46 - e_k - g_r) (0 past the case's angles: zero
+                // the chunk's scale 2^(OZ_FRAC - e_k - g_r) (0 past the case's angles: zero
                 // digits); the mirror row carries s_k, +1 for odd k, -1 for even k
                 const double gsc = gact ? oz_pow2(OZ_FRAC - gr) : 0.;
                 const double sp = gsc * oz_pow2(-oz_ec(kc));
@@ -566,8 +552,8 @@ __global__ void __launch_bounds__(OZ_T, 1) k_angular_oz(DevBatch B, const AngIte
                 const int slot = s == 0 ? 0 : (s <= NC1 ? slot1[s - 1] : 1 + B.idx2[s - 1 - NC1]);
                 wsh[p * OZ_MAX_NS + s] = B.w[(size_t) slot * R + gr0 + p];
             }
-            // column scales with the row-independent 2^-28 of the combination (2^-12, 2^-16)
-            if (t1 < OZ_NP) csh[t1] = oz_pow2(B.oz_colexp[(size_t) g * OZ_NP + t1] - 28);
+            // column scales with the row-independent factor of the combination
+            if (t1 < OZ_NP) csh[t1] = oz_pow2(B.oz_colexp[(size_t) g * OZ_NP + t1] + OZ_CSHIFT);
             // the scales of this row and of its pair row (which holds this row's sm)
             const double rsc = oz_pow2(eact ? (int) gtab[2 * (nk - 1)] : 0);
             const double rsp = __shfl_xor_sync(0xffffffffu, rsc, 1);
@@ -689,11 +675,15 @@ __global__ void __launch_bounds__(OZ_T, 1) k_angular_oz(DevBatch B, const AngIte
 // OZ_MAX_NK chunks; one block of 128 threads, the per-chunk, row and column
 // scaling, digit slices (A in tensor memory, B in shared memory),
 // descriptors, products, accumulators and exact combination of the product
-// kernel.
+// kernel.  Its waits for the products give up after `wait_cycles`; with
+// `withhold` the first chunk's products are never issued, so that wait runs
+// out: the block then releases its tensor memory and sets *err (the failure
+// path of the product kernel, without a fault).
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(128, 1) k_oz_selftest(int K, const double *__restrict__ A,
                                                          const double *__restrict__ Bm, double *__restrict__ D,
-                                                         int *__restrict__ err) {
+                                                         int *__restrict__ err, long long wait_cycles,
+                                                         int withhold) {
     extern __shared__ __align__(1024) unsigned char smem[];
     uint64_t *bars = (uint64_t *) (smem + OZ_BSTAGE);
     uint32_t *tmem_hold = (uint32_t *) (bars + 2);
@@ -757,12 +747,12 @@ __global__ void __launch_bounds__(128, 1) k_oz_selftest(int K, const double *__r
         fence_proxy_async();
         tc_fence_before();
         __syncthreads();
-        if (tid == 0) {
+        if (tid == 0 && !(withhold && kc == 0)) {
             tc_fence_after();
             issue_chunk_i8(tmem + OZ_ACOL, b0, tmem, kc == 0);
             mma_commit(done);
         }
-        const int lbad = !mbar_wait(done, ph, err);
+        const int lbad = !mbar_wait_for(done, ph, err, wait_cycles);
         ph ^= 1u;
         bad = __syncthreads_or(lbad);
         tc_fence_after();
@@ -790,7 +780,7 @@ __global__ void __launch_bounds__(128, 1) k_oz_selftest(int K, const double *__r
                     col[d] = a[d][i];
                 }
                 D[(size_t) tid * OZ_NP + c + i] =
-                    oz_combine(col, kB[c + i][0], kB[c + i][1], oz_pow2(gA + fB[c + i] - 28));
+                    oz_combine(col, kB[c + i][0], kB[c + i][1], oz_pow2(gA + fB[c + i] + OZ_CSHIFT));
             }
         }
     } else if (tid == 0) {
@@ -848,14 +838,15 @@ int launch_angular_oz(cudaStream_t s, const DevBatch &B, int nitems, const AngIt
     return -1;
 }
 
-int launch_oz_selftest(cudaStream_t s, int K, const double *A, const double *Bm, double *D, int *err) {
+int launch_oz_selftest(cudaStream_t s, int K, const double *A, const double *Bm, double *D, int *err,
+                       long long wait_cycles, int withhold) {
     static bool attr = false;
     const int smem = (int) (OZ_BSTAGE + 64);
     if (!attr) {
         LMIEB_CUDA_TRY(cudaFuncSetAttribute(k_oz_selftest, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         attr = true;
     }
-    k_oz_selftest<<<1, 128, smem, s>>>(K, A, Bm, D, err);
+    k_oz_selftest<<<1, 128, smem, s>>>(K, A, Bm, D, err, wait_cycles, withhold);
     LMIEB_CUDA_TRY(cudaGetLastError());
     return 0;
 }

@@ -9,6 +9,9 @@
 
 #include "dev_common.cuh"
 
+// limit of every bounded wait of the tensor-core kernels (~1 s at 1.96 GHz), in SM clock cycles
+constexpr long long LMIEB_WAIT_CYCLES = 1LL << 31;
+
 // K1 keeps its downward recurrences at the top of every block of K1_B orders.
 constexpr int K1_B = 16;
 // doubles per checkpoint block of a chunk of nc tangent-linear columns
@@ -69,6 +72,9 @@ struct DevBatch {
     const double *oz_f2;        // [OZ_KC * max chunks + 2]: (k + 1) / k
     const signed char *oz_rowexp;   // row exponents (DevCase.rx_off)
     const int *oz_colexp;       // [group][OZ_NP] column exponents
+    int *oz_radexp;             // [1 + nd1][R][4]: per radius, coefficient column and component, the
+                                //     largest (biased exponent + e_k) over the orders, 0 if no normal
+                                //     value (written by K1)
     const long long *oz_bcorr;  // [group][OZ_NP][2] bias terms of the digit combination
 };
 
@@ -118,7 +124,10 @@ int launch_oz_operands(cudaStream_t s, const DevBatch &B, long long nrow, const 
 int launch_angular_oz(cudaStream_t s, const DevBatch &B, int nitems, const AngItem *items, const unsigned char *bop,
                       double *part, int *err);
 // D[128 x OZ_NP] = A[128 x K] B[OZ_NP x K]^T through the same fixed-point path
-int launch_oz_selftest(cudaStream_t s, int K, const double *A, const double *Bm, double *D, int *err);
+// *err = 2 if the radius group's failure count *failed is not zero
+int launch_group_flag(cudaStream_t s, const double *failed, int *err);
+int launch_oz_selftest(cudaStream_t s, int K, const double *A, const double *Bm, double *D, int *err,
+                       long long wait_cycles, int withhold);
 // per-case element lists: element e of the flat index space belongs to the
 // case c with start[c] <= e < start[c+1] (start has ncase + 1 entries)
 int launch_reduce_pf(cudaStream_t s, const DevBatch &B, long long total, const long long *start,

@@ -98,6 +98,17 @@ typedef struct {
  * "ERROR: ..."). */
 int lmieb_device_solve(const lmieb_problem *p, lmieb_result *r);
 
+/* A process of the registered radius group whose lmie_solution(use_mpi) fails
+ * on the host before its device solve: takes part in the group's reduction
+ * with a failure mark (4 (1 + n_derivs) (1 + n_qang) zero integrals and a
+ * count of 1), so that the other processes return -1 too instead of waiting.
+ * Returns -1. */
+int lmieb_group_abort(int n_derivs, int n_qang);
+
+/* 1 while the environment variable LMIEB_FAULT names `site` (host-side fault
+ * injection for the tests of the failure paths), else 0. */
+int lmieb_fault_injected(const char *site);
+
 /* Runs n problems as batches on the device.  All problems must share the
  * derivative layout (nd, idx1, idx2), the requested outputs (want_gc,
  * want_lc, pf_from) and use save_control 0 when n > 1.  The cases are cut

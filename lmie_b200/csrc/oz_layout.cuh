@@ -7,7 +7,7 @@
 // rows 2h / 2h+1 = (pi_k + tau_k)(mu_h) / s_k (pi_k - tau_k)(mu_h), columns
 // the real and imaginary parts of S = fv4 (a + b) and D' = s_k fv4 (a - b) of
 // the radii of a group.  Here every operand value becomes a signed integer of
-// 46 fractional bits and the integer products are summed exactly:
+// 47 fractional bits and the integer products are summed exactly:
 //   - order k gets the power of two 2^e_k, e_k = ceil(log2 2k) (constant over
 //     each chunk of 32 orders after the first: 6 + the chunk's bit length):
 //     A+ is divided by it and Bop multiplied by it (|pi +- tau| grows like k^2
@@ -15,24 +15,24 @@
 //     power of two, g_r and f_n, the smallest that bring every value of the
 //     row (orders up to the group's last chunk) or of the column to at most
 //     1/2 in magnitude;
-//   - the scaled value x becomes V = round(x 2^46), |V| <= 2^45, written as
+//   - the scaled value x becomes V = round(x 2^47), |V| <= 2^46, written as
 //     six balanced base-256 digits d_0 (most significant) .. d_5 in [-128, 128),
 //     V = sum_i d_i 2^(8 (5 - i)): one int8 slice per digit;
 //   - the product of A digit i and B digit j has the weight 2^(8 (10 - i - j));
 //     the 21 products with i + j < 6 are summed by tcgen05.mma kind::i8 into
 //     six int32 accumulators, one per diagonal i + j; the dropped products
-//     (i + j >= 6) are below 2^-43 of the largest term;
+//     (i + j >= 6) are below 2^-46 of the largest term each;
 //   - B digits are signed bytes; A digits are stored as the unsigned bytes
 //     d + 128 (no conversion after the extraction below), so diagonal d also
 //     sums 128 times the B digits j <= d over the group's orders, which the
 //     combination removes with the column's digit sums (exact: every int32
 //     sum stays below 6 * 255 * 128 * 5120 < 2^31 for groups of up to 5120
 //     orders);
-//   - C = 2^(g_r + f_n - 12) sum_d 2^(-8 d) ACC_d, formed exactly in int64
+//   - C = 2^(g_r + f_n - 14) sum_d 2^(-8 d) ACC_d, formed exactly in int64
 //     halves and FP64.
-// The contraction then carries ~1e-12 of the largest term of each row and
-// column instead of FP64's ~1e-16 (measured on a model of it against 80-bit
-// sums: 1.2e-12 at x = 1000, 1.8e-12 at x = 3000).
+// Each product then carries ~2^-46 of the largest term of its row and column
+// (rounding of the two values and the dropped digit products) instead of
+// FP64's 2^-53.
 //
 // Layout of one chunk (OZ_KC orders) of the B operand in memory: OZ_ND
 // slices, slice s holding digit s of every row, each slice in the tensor
@@ -62,7 +62,10 @@ constexpr int OZ_MAX_NC1 = 4;                        // index1 columns the kerne
 constexpr int OZ_MAX_ND2 = 3;                        // index2 slots the kernel is built for
 constexpr int OZ_MAX_NK = 160;                       // chunks per group (5120 orders: int32 sums exact)
 constexpr int OZ_MIN_N1 = 16;                        // smaller cases keep the FP64 angular stage
-constexpr int OZ_FRAC = 46;                          // fractional bits of the fixed-point values
+constexpr int OZ_FRAC = 47;                          // fractional bits of the fixed-point values
+// exponent of the combination's row- and column-independent factor:
+// V_A V_B = 2^80 sum_d 2^(-8 d) ACC_d, and oz_value returns 2^16 of that sum
+constexpr int OZ_CSHIFT = 80 - 2 * OZ_FRAC - 16;
 // Bound on |beta_l(int8) - beta_l(FP64)| / (2l + 1) of the expansion
 // coefficients (measured: at most 1.8e-13 over 1024 seeded uneven cases): a
 // case with some |beta_l| within OZ_TRUNC_BAND (2l + 1) of `accuracy` before
@@ -102,7 +105,7 @@ __host__ __device__ inline int oz_ek(int k) {
 // 2^e as a double, -1022 <= e <= 1023
 __device__ __forceinline__ double oz_pow2(int e) { return __hiloint2double((1023 + e) << 20, 0); }
 
-// The digits of V = round(x s) for |x s| <= 2^45: t = x s + 1.5 2^52 + B, with
+// The digits of V = round(x s) for |x s| <= 2^46: t = x s + 1.5 2^52 + B, with
 // B = 0x80 in each of the six low bytes, is an integer in [2^52, 2^53) formed
 // with one rounding, so the low 48 bits of its significand are V + B exactly
 // (0 < V + B < 2^48), and byte i of V + B is digit 5 - i plus 128 (adding 128

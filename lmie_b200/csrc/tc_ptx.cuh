@@ -10,7 +10,6 @@ namespace {
 
 // Every mbarrier wait gives up after this many clock cycles (about 1 s at
 // the B200's clock), or earlier once another block has set the error word.
-constexpr long long LMIEB_WAIT_CYCLES = 1LL << 31;
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
     return (uint32_t) __cvta_generic_to_shared(p);
@@ -59,14 +58,18 @@ __device__ __forceinline__ bool mbar_try_park(uint32_t bar, uint32_t parity) {
 }
 
 // Bounded wait for the phase with the given parity to complete.  Gives up
-// after LMIEB_WAIT_CYCLES, or early once another block has set the error word.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, const int *err) {
+// after `limit` cycles, or early once another block has set the error word.
+__device__ __forceinline__ bool mbar_wait_for(uint32_t bar, uint32_t parity, const int *err, long long limit) {
     if (mbar_try(bar, parity)) return true;
     const long long t0 = clock64();
     for (;;) {
         if (mbar_try_park(bar, parity)) return true;
-        if (clock64() - t0 > LMIEB_WAIT_CYCLES || (err && *(volatile const int *) err)) return false;
+        if (clock64() - t0 > limit || (err && *(volatile const int *) err)) return false;
     }
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, const int *err) {
+    return mbar_wait_for(bar, parity, err, LMIEB_WAIT_CYCLES);
 }
 
 __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {

@@ -16,6 +16,7 @@ forward-mode outputs of each radius, the bin weights analytically.
 from __future__ import annotations
 
 import ctypes as C
+from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 
@@ -57,8 +58,10 @@ def per_radius(p, k: int, r: float):
     return v, d
 
 
-def solve(p) -> dict:
-    """Loss, gradients and per-wavelength outputs by forward mode."""
+def solve(p, threads: int = 1) -> dict:
+    """Loss, gradients and per-wavelength outputs by forward mode; the
+    per-radius solves run on `threads` host threads (the oracle keeps no
+    state between calls)."""
     rad, q, binof = radii(p)
     W = p.weight[binof] * q
     N = W.sum()
@@ -66,8 +69,12 @@ def solve(p) -> dict:
     out = {"loss": 0.0, "grad_mr": np.zeros(L), "grad_mi": np.zeros(L), "grad_weight": np.zeros(nb),
            "cext": np.zeros(L), "csca": np.zeros(L), "g": np.zeros(L),
            "p11": np.zeros((L, na)), "p12": np.zeros((L, na))}
+    pool = ThreadPoolExecutor(threads) if threads > 1 else None
     for k in range(L):
-        vs = [per_radius(p, k, r) for r in rad]
+        if pool is None:
+            vs = [per_radius(p, k, r) for r in rad]
+        else:
+            vs = list(pool.map(lambda r: per_radius(p, k, r), rad))
         ce = np.array([v[0][0] for v in vs]); cs = np.array([v[0][1] for v in vs])
         gg = np.array([v[0][2] for v in vs])
         p11 = np.array([v[0][3] for v in vs]); p12 = np.array([v[0][4] for v in vs])
@@ -100,4 +107,6 @@ def solve(p) -> dict:
         out["loss"] += loss
         out["cext"][k], out["csca"][k], out["g"][k] = Cext, Csca, g
         out["p11"][k], out["p12"][k] = P11, P12
+    if pool is not None:
+        pool.shutdown()
     return out

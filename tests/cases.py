@@ -100,5 +100,27 @@ def all_cases() -> Dict[str, Case]:
     return d
 
 
+# cases of the seeded 4096-case uneven workload (workloads.batched_uneven)
+# whose largest size parameter is above 500, spread over 502 .. 1063
+UNEVEN_LARGE_X = (3278, 1168, 4034, 2007, 2343, 2904, 517, 2963)
+
+
+def large_cases() -> Dict[str, Case]:
+    """Cases at the sizes the benchmark runs, pinned to the reference's own
+    outputs (seconds of reference CPU time each): the large-particle
+    configuration with every output (size parameter up to 5000, n1 = 5077,
+    10154 Gauss angles, n_coef ~ 10^4; 8 radii instead of 8000, since each
+    radius' work is the same) and eight cases of the uneven workload with
+    size parameters from 502 to 1063."""
+    from lmie_b200 import workloads
+    d = {"x5000_full": Case(dist="gamma", lam=0.5, mr=1.33, mi=1e-4, a1=300.0, a2=0.1, r1=350.0,
+                            r2=398.0, n_int2=1, n_quad=8, n_angles=181, accuracy=1e-7,
+                            derivs=deriv_unit("mr", "mi", "a1", "a2"))}
+    uneven = workloads.batched_uneven(4096)
+    for i in UNEVEN_LARGE_X:
+        d[f"uneven_{i}"] = uneven[i]
+    return d
+
+
 def case_names() -> List[str]:
     return list(all_cases().keys())

@@ -11,7 +11,10 @@ Writes
                     thread, full double precision) for each case of
                     tests/cases.py, together with the case definition;
   example_out.npz   the values printed in the reference's golden output
-                    examples/example.out (7 significant digits), parsed.
+                    examples/example.out (7 significant digits), parsed;
+  ref_<case>.npz    likewise for the cases of tests/cases.py large_cases()
+                    (size parameters 500 - 5000; about half a minute of
+                    reference CPU time in all).
 """
 from __future__ import annotations
 
@@ -29,7 +32,7 @@ ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT))
 sys.path.insert(0, str(ROOT / "tests"))
 
-from cases import all_cases, example_case  # noqa: E402
+from cases import all_cases, example_case, large_cases  # noqa: E402
 import libs  # noqa: E402
 
 REF_TREE = Path(os.environ.get("LMIE_REFERENCE", "/root/reference"))
@@ -97,7 +100,7 @@ def main() -> int:
     OUT.mkdir(parents=True, exist_ok=True)
     np.savez_compressed(OUT / "example_out.npz",
                         **parse_example_out(REF_TREE / "examples" / "example.out"))
-    for name, case in all_cases().items():
+    for name, case in {**all_cases(), **large_cases()}.items():
         res = libs.run_reference(case, n_threads=1)
         assert res is not None and res.rc == 0, name
         d = libs.result_to_npz(res)

@@ -52,6 +52,22 @@ def test_adjoint_matches_forward_mode(r_max, tol):
         assert rel(got[name], want[name]) <= 1e-8, (name, got[name], want[name])
 
 
+def test_adjoint_full_distribution():
+    """The benchmark's distribution -- 64 log-spaced bins x 32 Gauss radii
+    over 0.02 - 20 um, 181 angles -- on four wavelengths from 0.34 to
+    2.25 um (size parameters up to 370), against the forward-mode oracle
+    over all 2048 radii of each wavelength; tolerances as at x ~ 300 above."""
+    p = workloads.adjoint_retrieval(n_lambda=4)
+    assert p.n_bins == 64 and p.n_quad == 32 and p.n_angles == 181
+    got = lmie_b200.adjoint(p)
+    want = adjoint_oracle.solve(p, threads=16)
+    assert abs(got["loss"] - want["loss"]) <= 1e-8 * abs(want["loss"]), (got["loss"], want["loss"])
+    for name in ("cext", "csca", "g"):
+        assert rel(got[name], want[name]) <= 1e-10, (name, rel(got[name], want[name]))
+    for name in ("p11", "p12", "grad_mr", "grad_mi", "grad_weight"):
+        assert rel(got[name], want[name]) <= 1e-8, (name, rel(got[name], want[name]))
+
+
 def _fd(loss, p, name, idx, rel_h):
     """Central difference with Richardson extrapolation (steps h and h/2):
     weakly absorbing particles of large size parameter have sharp resonances

@@ -36,6 +36,16 @@ def test_oracle_matches_reference_fixtures(name):
     _check(got, want, TOL)
 
 
+@pytest.mark.parametrize("name", ["x5000_full", "uneven_2963"])
+def test_oracle_matches_reference_at_large_size(name):
+    """Size parameters 5000 (n_coef 10156, every output) and 1063 (2200
+    radii of the uneven workload): a few seconds of oracle time each."""
+    from cases import large_cases
+    got = libs.run_oracle(large_cases()[name])
+    assert got.rc == 0
+    _check(got, libs.golden(name), TOL)
+
+
 def test_oracle_matches_example_out():
     """7 significant digits of examples/example.out (value and the 4
     derivatives: mr, mi, a1, a2)."""
@@ -91,7 +101,8 @@ def test_fixture_cases_are_current():
     """The fixtures were generated from the case definitions in tests/cases.py."""
     import dataclasses
     import json
-    for name, case in all_cases().items():
+    from cases import large_cases
+    for name, case in {**all_cases(), **large_cases()}.items():
         with np.load(libs.GOLDEN / f"ref_{name}.npz") as z:
             assert json.loads(str(z["case"])) == json.loads(
                 json.dumps(dataclasses.asdict(case), sort_keys=True)), name

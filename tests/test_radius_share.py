@@ -169,8 +169,9 @@ def test_group_callback_as_rank_0_of_two():
     seen = []
 
     def add_rank1(buf, count, stream, ctx):
+        # the integrals, then the group's failure count (rank 1 did not fail)
         t = shard.device_doubles(C.cast(buf, C.c_void_p).value, int(count))
-        t.add_(torch.from_numpy(other).to(t.device))
+        t[:other.size].add_(torch.from_numpy(other).to(t.device))
         torch.cuda.synchronize(t.device)
         seen.append(int(count))
         return 0
@@ -181,7 +182,7 @@ def test_group_callback_as_rank_0_of_two():
         got = abi.solve(lib, case, use_mpi=1)
     finally:
         shard.leave_group(lib)
-    assert seen == [other.size]
+    assert seen == [other.size + 1]
     _assert_close(got, libs.golden("c2"), label="c2")
     # without use_mpi the group is not used
     assert lib.lmieb_set_radius_group(0, 2, cb, None) == 0
@@ -189,8 +190,60 @@ def test_group_callback_as_rank_0_of_two():
         whole = abi.solve(lib, case, use_mpi=0)
     finally:
         shard.leave_group(lib)
-    assert seen == [other.size]
+    assert seen == [other.size + 1]
     _assert_identical(whole, libs.run_product(case))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("site", ["prepare", "alloc", "h2d"])
+def test_group_failure_is_shared(site):
+    """A process whose solve fails before the group's sum -- on the host
+    (preparation) or on the device side (arena, upload; injected by
+    LMIEB_FAULT) -- still takes part in the sum, once, with zero integrals
+    and a failure count of 1, so no process is left waiting; a healthy
+    process whose sum carries a peer's failure returns -1 as well; and the
+    group works again afterwards."""
+    import os
+    import torch
+    lib = _lib()
+    case = all_cases()["c2"]
+    n = abi.solve_partial(lib, case, 1, 2).size          # the integrals
+    calls = []
+
+    def record(buf, count, stream, ctx):
+        t = shard.device_doubles(C.cast(buf, C.c_void_p).value, int(count))
+        torch.cuda.synchronize(t.device)
+        calls.append((int(count), float(t[-1]), float(t[:-1].abs().sum())))
+        return 0
+
+    cb = abi.REDUCE_FN(record)
+    assert lib.lmieb_set_radius_group(1, 2, cb, None) == 0
+    try:
+        os.environ["LMIEB_FAULT"] = site
+        try:
+            failed = abi.solve(lib, case, use_mpi=1)
+        finally:
+            os.environ.pop("LMIEB_FAULT", None)
+        assert failed.rc == -1
+        assert calls == [(n + 1, 1.0, 0.0)], calls
+    finally:
+        shard.leave_group(lib)
+
+    # a healthy rank 0 whose peer failed: the peer's block is zeros and a 1
+    def peer_failed(buf, count, stream, ctx):
+        t = shard.device_doubles(C.cast(buf, C.c_void_p).value, int(count))
+        t[-1] += 1.0
+        torch.cuda.synchronize(t.device)
+        return 0
+
+    cb2 = abi.REDUCE_FN(peer_failed)
+    assert lib.lmieb_set_radius_group(0, 2, cb2, None) == 0
+    try:
+        assert abi.solve(lib, case, use_mpi=1).rc == -1
+    finally:
+        shard.leave_group(lib)
+    # and the library keeps working
+    _assert_identical(abi.solve(lib, case), libs.run_product(case))
 
 
 @pytest.mark.gpu
