@@ -958,7 +958,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
             if (!case_oz[k]) continue;
             C.nkx = (cn1max[k] + OZ_KC - 1) / OZ_KC;
             C.rx_off = rx_bytes;
-            C.trunc_band = C.accuracy > 0. ? OZ_TRUNC_BAND : 0.;
+            C.trunc_band = C.accuracy > 0. ? oz_trunc_band(cn1max[k]) : 0.;
             rx_bytes += (long long) C.nh * C.nkx * 2;
             rx_start[k + 1] += C.nh;
             nkx_all = std::max(nkx_all, C.nkx);

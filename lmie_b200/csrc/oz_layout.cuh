@@ -67,10 +67,14 @@ constexpr int OZ_FRAC = 47;                          // fractional bits of the f
 // V_A V_B = 2^80 sum_d 2^(-8 d) ACC_d, and oz_value returns 2^16 of that sum
 constexpr int OZ_CSHIFT = 80 - 2 * OZ_FRAC - 16;
 // Bound on |beta_l(int8) - beta_l(FP64)| / (2l + 1) of the expansion
-// coefficients (measured: at most 1.8e-13 over 1024 seeded uneven cases): a
-// case with some |beta_l| within OZ_TRUNC_BAND (2l + 1) of `accuracy` before
-// its truncation point is solved again in FP64.
-constexpr double OZ_TRUNC_BAND = 5e-13;
+// coefficients near the truncation threshold (|beta_l| within 1e-9 .. 1e-5 of
+// 2l + 1), for a case whose radii reach n1 orders: measured at most 8e-14 up
+// to ~1100 orders (the 4096 seeded uneven cases, x <= 1063) and up to 2.6e-12
+// beyond (x from 1500 to 5000, 4 to 8000 radii).  The two forms' own rounding
+// differs by this much (the FP64 form and the reference differ by as much).
+// A case with some |beta_l| within oz_trunc_band (2l + 1) of `accuracy`
+// before its truncation point is solved again in FP64.
+__host__ __device__ inline double oz_trunc_band(int n1) { return n1 <= 1152 ? 2.5e-13 : 5e-12; }
 // 1.5 * 2^52 + 0x808080808080: see oz_digits
 constexpr double OZ_MAGIC = 6896688841130112.0;
 
