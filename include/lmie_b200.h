@@ -293,12 +293,19 @@ int lmie_cross_sections_noalloc(int n_radii, const double *radius, double lambda
  * n_qang = 0 without calc_gc and calc_lc, else lmie_calc_max_coef() -- and
  * every process then finishes the solve (normalisation, expansions, phase
  * matrix) and returns the whole result.  Every process of the group must make
- * the same calls with the same inputs.  save_control must be 0. */
+ * the same calls with the same inputs.  save_control must be 0.
+ * The summed block carries one double more: the number of processes whose
+ * solve failed before the sum.  A process that fails there (host preparation,
+ * device memory, upload, a kernel) still takes part in the sum with zero
+ * integrals and a count of 1, and returns -1; every process whose sum holds
+ * a nonzero count returns -1 as well -- none is left waiting in the group's
+ * collective. */
 
-/* In-place sum over the group of the `count` doubles at DEVICE address buf,
- * which this process's solve has just written on `stream` (a cudaStream_t,
- * already synchronised when the function is called).  The sum must be
- * complete when the function returns; 0 means success. */
+/* In-place sum over the group of the `count` doubles at DEVICE address buf
+ * (the integrals, then the failure count), which this process's solve has
+ * just written on `stream` (a cudaStream_t, already synchronised when the
+ * function is called).  The sum must be complete when the function returns;
+ * 0 means success. */
 typedef int (*lmieb_reduce_fn)(double *buf, long long count, void *stream, void *ctx);
 
 /* From this call on, lmie_solution() and lmie_solution2*() called with

@@ -14,22 +14,27 @@
 //   - k_angular_oz: a block owns one angle tile of one case and a range of its
 //     radius groups; per group, chunks of OZ_KC orders flow through the
 //     pipeline:
-//       * warps 0-3 (one thread per row) run the pi/tau recurrence in FP64 and
-//         write the row's six digit slices of the chunk into tensor memory
-//         (two stages);
+//       * warps 10-13 (one thread per row) run the pi/tau recurrence in FP64
+//         and hand the row values over in tensor memory, half a chunk at a
+//         time;
+//       * warps 0-3 (one thread per row, the row's tensor-memory lane) turn
+//         them into the row's six digit slices in tensor memory (two stages);
 //       * lane 0 of warp 9 brings the group's B chunks into shared memory with
 //         bulk copies running ahead of the products;
 //       * lane 0 of warp 8 issues the 21 digit products of a chunk,
 //         tcgen05.mma kind::i8 with A in tensor memory and B in shared memory
 //         (M 128, N OZ_NP, K 32, int32 accumulation in tensor memory), one
 //         accumulator per digit diagonal;
-//       * after a group's last chunk warps 4-7 read the six accumulators of
-//         their row (tensor-memory lane = row), form C exactly (int64 halves,
-//         then FP64) into a shared-memory buffer and hand the accumulators
-//         back, so the next group's products start; then, from the buffer,
-//         the phase-matrix quadratic forms and their linearisations per
-//         radius (reference src/lmie_core.c:723-790; sm of a row is in its
-//         pair row), accumulated over the block's radii in registers.
+//       * after a group's last chunk warps 4-7 (S columns) and 0-3 (D'
+//         columns) read the six accumulators of their row (tensor-memory
+//         lane = row), form C exactly (int64 halves, then FP64) into a
+//         shared-memory buffer and hand the accumulators back, so the next
+//         group's products start;
+//       * warps 14-17 form, from the buffer and while the next group's
+//         products run, the phase-matrix quadratic forms and their
+//         linearisations per radius (reference src/lmie_core.c:723-790; sm of
+//         a row is in its pair row), accumulated over the block's radii in
+//         registers.
 // The integer sums are exact, so nothing is drained during a group.
 // Partials go to the same per-group buffer as the FP64 K3.
 //
@@ -49,26 +54,35 @@
 
 namespace {
 
-constexpr int OZ_T = 320;                     // warps 0-3: A operand; 4-7: sums and quadratic forms;
-                                              // 8: products; 9: B copies
-constexpr int OZ_MMA_WARP = 8, OZ_COPY_WARP = 9;
+constexpr int OZ_T = 576;                     // warps 0-3: A digits, D' sums; 4-7: S sums; 8: products;
+                                              // 9: B copies; 10-13: recurrence; 14-17: quadratic forms
+constexpr int OZ_MMA_WARP = 8, OZ_COPY_WARP = 9, OZ_RECUR_WARP = 10, OZ_QUAD_WARP = 14;
 constexpr int OZ_ASTAGES = 2;                 // A operand stages (tensor memory)
 constexpr int OZ_BSLOTS = 4;                  // B operand slots (bulk copies)
 constexpr int OZ_MAX_GN = OZ_NHALF / 2;       // radii of a group (oz_rg(0))
 constexpr int OZ_MAX_NS = 1 + OZ_MAX_NC1 + OZ_MAX_ND2;
 constexpr uint32_t OZ_ACOLS = OZ_ND * OZ_KC / 4;                 // tensor-memory columns of an A stage
 constexpr uint32_t OZ_ACOL = OZ_ND * OZ_NP;                      // first A stage column
-// barriers: afull[OZ_ASTAGES], adone[OZ_ASTAGES], bfull[OZ_BSLOTS], bdone[OZ_BSLOTS], accfull, accfree,
-// qdone, fin
-constexpr int OZ_NBAR = 2 * OZ_ASTAGES + 2 * OZ_BSLOTS + 4;
+// barriers: afull[OZ_ASTAGES], adone[OZ_ASTAGES], bfull[OZ_BSLOTS], bdone[OZ_BSLOTS], vfull, vfree,
+// accfull, accfree, qdone, hready[2], hfree[2], fin
+constexpr int OZ_NBAR = 2 * OZ_ASTAGES + 2 * OZ_BSLOTS + 10;
 constexpr uint32_t OZ_RING = OZ_BSLOTS * OZ_BSTAGE;
-constexpr uint32_t OZ_HBUF = OZ_NP * OZ_M * 16;            // a group's sums as (U, L) [column][row]
+constexpr int OZ_HB = OZ_NP * OZ_M;                         // doubles of one sums buffer
+constexpr uint32_t OZ_HBUF = 2 * OZ_HB * 8;                 // two groups' sums, unscaled, [column][row]
 constexpr uint32_t OZ_WBUF = OZ_MAX_GN * OZ_MAX_NS * 8;     // a group's radius weights
 constexpr uint32_t OZ_CBUF = OZ_NP * 8;                     // a group's column scales
 constexpr uint32_t OZ_KBUF = OZ_NP * 16;                    // a group's bias terms of the combination
 constexpr uint32_t OZ_FBUF = (OZ_KC * OZ_MAX_NK + 8) * 8;   // (k + 1) / k of the case's orders
-constexpr uint32_t OZ_SMEM = OZ_RING + OZ_HBUF + OZ_WBUF + OZ_CBUF + OZ_KBUF + OZ_FBUF + OZ_NBAR * 8 + 16;
+// shared-memory offsets
+constexpr uint32_t OZ_O_HBUF = OZ_RING, OZ_O_WBUF = OZ_O_HBUF + OZ_HBUF;
+constexpr uint32_t OZ_O_CBUF = OZ_O_WBUF + OZ_WBUF, OZ_O_KBUF = OZ_O_CBUF + OZ_CBUF;
+constexpr uint32_t OZ_O_FBUF = OZ_O_KBUF + OZ_KBUF, OZ_O_BARS = OZ_O_FBUF + OZ_FBUF;
+constexpr uint32_t OZ_SMEM = OZ_O_BARS + OZ_NBAR * 8 + 16;
 constexpr uint32_t OZ_TMEM_COLS = 512;
+// half a chunk of row values (16 doubles per lane) handed from the recurrence
+// warps to the digit warps, after the A stages
+constexpr uint32_t OZ_VCOL = OZ_ACOL + OZ_ASTAGES * OZ_ACOLS;
+static_assert(OZ_VCOL + 32 <= OZ_TMEM_COLS, "row-value columns in tensor memory");
 
 static_assert(OZ_BSTAGE % 1024 == 0, "stages stay 1 KB aligned");
 static_assert(OZ_NP % 16 == 0 && OZ_NP >= 16 && OZ_NP <= 256, "N of an M=128 kind::i8 product");
@@ -140,14 +154,48 @@ __device__ __forceinline__ longlong2 oz_halves(const uint32_t (&a)[OZ_ND], long 
     return make_longlong2(U, L);
 }
 
-__device__ __forceinline__ double oz_value(longlong2 h, double scale) {
+// U + 2^-24 L with one rounding (the scale that follows is a power of two)
+__device__ __forceinline__ double oz_unscaled(longlong2 h) {
     const double dU = __longlong_as_double(h.x + 0x4338000000000000LL) - 6755399441055744.0;
     const double dL = __longlong_as_double(h.y + 0x4338000000000000LL) - 6755399441055744.0;
-    return fma(dL, 5.9604644775390625e-08, dU) * scale;   // 2^-24
+    return fma(dL, 5.9604644775390625e-08, dU);   // 2^-24
 }
+
+__device__ __forceinline__ double oz_value(longlong2 h, double scale) { return oz_unscaled(h) * scale; }
 
 __device__ __forceinline__ double oz_combine(const uint32_t (&a)[OZ_ND], long long cU, long long cL, double scale) {
     return oz_value(oz_halves(a, cU, cL), scale);
+}
+
+// The exact sums of `ncol` columns from c0 on (multiples of 4) of this
+// thread's lane: six accumulators per column from tensor memory (taddr: the
+// lane's column c0 of diagonal 0), bias terms ks[2 c], ks[2 c + 1], unscaled
+// values to hb[c OZ_M] (warp-wide; the bias terms are loaded ahead of the
+// stores, which the compiler could not move them past).
+__device__ __forceinline__ void oz_read_sums(uint32_t taddr, int c0, int ncol, const long long *ks, double *hb) {
+#pragma unroll 1
+    for (int c = c0; c < c0 + ncol; c += 4) {
+        long long kU[4], kL[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            kU[i] = ks[2 * (c + i)];
+            kL[i] = ks[2 * (c + i) + 1];
+        }
+        uint32_t a[OZ_ND][4];
+#pragma unroll
+        for (int d = 0; d < OZ_ND; ++d) tmem_ld4(taddr + d * OZ_NP + (c - c0), a[d]);
+        tmem_wait_ld();
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            uint32_t col[OZ_ND];
+#pragma unroll
+            for (int d = 0; d < OZ_ND; ++d) {
+                reg_after_wait(a[d][i]);
+                col[d] = a[d][i];
+            }
+            hb[(c + i) * OZ_M] = oz_unscaled(oz_halves(col, kU[i], kL[i]));
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -264,54 +312,61 @@ __global__ void __launch_bounds__(OZ_BOP_T) k_oz_bop(DevBatch B, const double *_
     }
 }
 
-// One chunk of a product row (producer thread): runs the pi/tau recurrence
-// over the chunk's OZ_KC orders and stores the row's six digit slices to
-// tensor memory at column acol (warp-wide).  sg = +1 (row 2h) or -1 (its
-// mirror); sp / sm: the scales of odd / even orders (the mirror row carries
-// s_k); FIRST: the case's first chunk, whose orders 1..16 have their own
-// exponents (gsc = 2^(OZ_FRAC - g_r), 0 for an inactive row).
-template <bool FIRST>
-__device__ __forceinline__ void oz_produce_chunk(const double *__restrict__ f2, double mu, double sg, double sp,
-                                                 double sm, double gsc, double &kmu, double &k1, double &p0,
-                                                 double &p1, uint32_t acol) {
+// The pi/tau recurrence of one product row over 16 orders (recurrence
+// thread): the row's values (pi_k + sg tau_k) into v; sg = +1 (row 2h) or -1
+// (its mirror).
+__device__ __forceinline__ void oz_recur_half(const double *__restrict__ f2, double mu, double sg, double &kmu,
+                                              double &k1, double &p0, double &p1, double (&v)[16]) {
+    // the (k + 1) / k of eight orders at a time ahead of the dependent steps
 #pragma unroll
-    for (int hf = 0; hf < 2; ++hf) {
-        // the recurrence over the 16 orders of this half (one dependent FMA per
-        // order), then the 16 independent digit extractions, then the slices
-        double v[16];
+    for (int u0 = 0; u0 < 16; u0 += 8) {
+        double f[8];
 #pragma unroll
-        for (int u = 0; u < 16; ++u) {
+        for (int u = 0; u < 8; ++u) f[u] = f2[u0 + u];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
             const double pk = p1;
             double tau;
-            oz_step(mu, f2[hf * 16 + u], kmu, k1, p0, p1, tau);
-            v[u] = fma(sg, tau, pk);
+            oz_step(mu, f[u], kmu, k1, p0, p1, tau);
+            v[u0 + u] = fma(sg, tau, pk);
         }
-        uint32_t lo[16], hi[16];
-#pragma unroll
-        for (int u = 0; u < 16; ++u) {
-            double sc = (u & 1) ? sm : sp;
-            if (FIRST && hf == 0) {
-                // 2^(OZ_FRAC - e_k - g_r) with e_k = ceil(log2 2k), k = u + 1 (compile-time)
-                constexpr double inv[5] = {0.5, 0.25, 0.125, 0.0625, 0.03125};
-                const int ek = u == 0 ? 1 : (u == 1 ? 2 : (u < 4 ? 3 : (u < 8 ? 4 : 5)));
-                sc = (u & 1) ? sg * gsc * inv[ek - 1] : gsc * inv[ek - 1];
-            }
-            oz_digits(v[u], sc, lo[u], hi[u]);
-        }
-        uint32_t w[OZ_ND][4];
-#pragma unroll
-        for (int qd = 0; qd < 4; ++qd) {
-            uint32_t s6[OZ_ND];
-            const uint32_t l4[4] = {lo[4 * qd], lo[4 * qd + 1], lo[4 * qd + 2], lo[4 * qd + 3]};
-            const uint32_t h4[4] = {hi[4 * qd], hi[4 * qd + 1], hi[4 * qd + 2], hi[4 * qd + 3]};
-            oz_slices4_biased(l4, h4, s6);
-#pragma unroll
-            for (int sl = 0; sl < OZ_ND; ++sl) w[sl][qd] = s6[sl];
-        }
-#pragma unroll
-        for (int sl = 0; sl < OZ_ND; ++sl)
-            tmem_st4(acol + sl * (OZ_KC / 4) + hf * 4, w[sl][0], w[sl][1], w[sl][2], w[sl][3]);
     }
+}
+
+// Half hf (orders 16 hf .. 16 hf + 15) of a chunk of one product row (digit
+// thread): the row values vb[u], their digits and the row's six
+// digit slices stored to tensor memory at column acol (warp-wide).  sp / sm:
+// the scales of odd / even orders (the mirror row carries s_k); FIRST: the
+// case's first chunk, whose orders 1..16 have their own exponents
+// (gsc = 2^(OZ_FRAC - g_r), 0 for an inactive row).
+template <bool FIRST>
+__device__ __forceinline__ void oz_digit_half(const double (&vb)[16], int hf, double sg, double sp, double sm,
+                                              double gsc, uint32_t acol) {
+    uint32_t lo[16], hi[16];
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+        double sc = (u & 1) ? sm : sp;
+        if (FIRST && hf == 0) {
+            // 2^(OZ_FRAC - e_k - g_r) with e_k = ceil(log2 2k), k = u + 1 (compile-time)
+            constexpr double inv[5] = {0.5, 0.25, 0.125, 0.0625, 0.03125};
+            const int ek = u == 0 ? 1 : (u == 1 ? 2 : (u < 4 ? 3 : (u < 8 ? 4 : 5)));
+            sc = (u & 1) ? sg * gsc * inv[ek - 1] : gsc * inv[ek - 1];
+        }
+        oz_digits(vb[u], sc, lo[u], hi[u]);
+    }
+    uint32_t w[OZ_ND][4];
+#pragma unroll
+    for (int qd = 0; qd < 4; ++qd) {
+        uint32_t s6[OZ_ND];
+        const uint32_t l4[4] = {lo[4 * qd], lo[4 * qd + 1], lo[4 * qd + 2], lo[4 * qd + 3]};
+        const uint32_t h4[4] = {hi[4 * qd], hi[4 * qd + 1], hi[4 * qd + 2], hi[4 * qd + 3]};
+        oz_slices4_biased(l4, h4, s6);
+#pragma unroll
+        for (int sl = 0; sl < OZ_ND; ++sl) w[sl][qd] = s6[sl];
+    }
+#pragma unroll
+    for (int sl = 0; sl < OZ_ND; ++sl)
+        tmem_st4(acol + sl * (OZ_KC / 4) + hf * 4, w[sl][0], w[sl][1], w[sl][2], w[sl][3]);
 }
 
 // barrier 2 over the 128 threads of warps 4-7, OR-reducing v
@@ -337,17 +392,19 @@ __global__ void __launch_bounds__(OZ_T, 1) k_angular_oz(DevBatch B, const AngIte
                                                         double *__restrict__ part, int *__restrict__ err) {
     constexpr int C1 = 1 + NC1, CPR = 2 * C1;
     extern __shared__ __align__(1024) unsigned char smem[];
-    longlong2 *hbuf = (longlong2 *) (smem + OZ_RING);                  // [OZ_NP][OZ_M] sums of a group (U, L)
-    double *wsh = (double *) (smem + OZ_RING + OZ_HBUF);               // [OZ_MAX_GN][OZ_MAX_NS] weights
-    double *csh = (double *) (smem + OZ_RING + OZ_HBUF + OZ_WBUF);     // [OZ_NP] column scales
-    long long *ksh = (long long *) (smem + OZ_RING + OZ_HBUF + OZ_WBUF + OZ_CBUF);   // [OZ_NP][2] bias terms
-    double *f2s = (double *) (smem + OZ_RING + OZ_HBUF + OZ_WBUF + OZ_CBUF + OZ_KBUF);   // [k] (k + 1) / k
-    uint64_t *bars = (uint64_t *) (smem + OZ_RING + OZ_HBUF + OZ_WBUF + OZ_CBUF + OZ_KBUF + OZ_FBUF);
+    double *hbuf = (double *) (smem + OZ_O_HBUF);            // [2][OZ_NP][OZ_M] sums of a group, unscaled
+    double *wsh = (double *) (smem + OZ_O_WBUF);             // [OZ_MAX_GN][OZ_MAX_NS] weights
+    double *csh = (double *) (smem + OZ_O_CBUF);             // [OZ_NP] column scales
+    long long *ksh = (long long *) (smem + OZ_O_KBUF);       // [OZ_NP][2] bias terms
+    double *f2s = (double *) (smem + OZ_O_FBUF);             // [k] (k + 1) / k
+    uint64_t *bars = (uint64_t *) (smem + OZ_O_BARS);
     uint32_t *tmem_hold = (uint32_t *) (bars + OZ_NBAR);
     const uint32_t bring = smem_u32(smem);
     const uint32_t afull0 = smem_u32(bars), adone0 = afull0 + 8 * OZ_ASTAGES;
     const uint32_t bfull0 = adone0 + 8 * OZ_ASTAGES, bdone0 = bfull0 + 8 * OZ_BSLOTS;
-    const uint32_t accfull = bdone0 + 8 * OZ_BSLOTS, accfree = accfull + 8, qdone = accfree + 8, fin = qdone + 8;
+    const uint32_t vfull = bdone0 + 8 * OZ_BSLOTS, vfree = vfull + 8;
+    const uint32_t accfull = vfree + 8, accfree = accfull + 8, qdone = accfree + 8;
+    const uint32_t hready0 = qdone + 8, hfree0 = hready0 + 16, fin = hfree0 + 16;
 
     const int tid = threadIdx.x, warp = tid >> 5;
     const AngItem it = items[blockIdx.x];
@@ -369,9 +426,15 @@ __global__ void __launch_bounds__(OZ_T, 1) k_angular_oz(DevBatch B, const AngIte
             mbar_init(bfull0 + 8 * i, 1);
             mbar_init(bdone0 + 8 * i, 1);
         }
+        mbar_init(vfull, OZ_M);
+        mbar_init(vfree, OZ_M);
         mbar_init(accfull, 1);
         mbar_init(accfree, 256);
         mbar_init(qdone, 128);
+        for (int i = 0; i < 2; ++i) {
+            mbar_init(hready0 + 8 * i, 256);
+            mbar_init(hfree0 + 8 * i, 128);
+        }
         mbar_init(fin, 1);
         fence_mbar_init();
     }
@@ -386,44 +449,32 @@ __global__ void __launch_bounds__(OZ_T, 1) k_angular_oz(DevBatch B, const AngIte
     int bad = 0;
 
     if (tid < OZ_M) {
-        // ---------------- warps 0-3: the A operand, one row (lane) per thread ----------------
+        // ---------------- warps 0-3: the A digits, one row (lane) per thread ----------------
         const int row = tid, h = row >> 1, mirror = row & 1;
         const int gj = it.xt * OZ_HALF + h;
         const bool gact = gj < nh;
-        const double mu = gact ? B.mu_pool[C.mu_off + gj] : 0.;
         const signed char *gtab = B.oz_rowexp + C.rx_off + (size_t) (gact ? gj : 0) * C.nkx * 2 + mirror;
         const uint32_t tlane = tmem + ((uint32_t) (warp * 32) << 16);
         const double sg = mirror ? -1. : 1.;
-        // The producers take the D' columns of a group's finished sums out of
+        // The digit warps take the D' columns of a group's finished sums out of
         // tensor memory (the epilogue warps take the S columns): once the
         // epilogue has read the previous group's sums from the buffer, after
         // the group's last products.  Returns nonzero when a wait gave up.
         auto take = [&](int gh) -> int {
             const int g = it.rbeg + gh, ncol = B.tg_n[g] * CPR;
+            // the bias terms of the group are staged, the buffer's previous
+            // group (gh - 2) has been through the quadratic forms
+            const int b = gh & 1;
             bool ok = gh == 0 || mbar_wait(qdone, (gh - 1) & 1, err);
+            ok = ok && (gh < 2 || mbar_wait(hfree0 + 8 * b, ((gh >> 1) - 1) & 1, err));
             ok = ok && mbar_wait(accfull, gh & 1, err);
+            double *hb = hbuf + b * OZ_HB;
             if (__any_sync(0xffffffffu, !ok)) return 1;
             tc_fence_after();
-#pragma unroll 1
-            for (int c0 = OZ_NHALF; c0 < OZ_NP; c0 += 16) {
-                if ((c0 & (OZ_NHALF - 1)) >= ncol) continue;
-                uint32_t a[OZ_ND][16];
-#pragma unroll
-                for (int d = 0; d < OZ_ND; ++d) tmem_ld16(tlane + d * OZ_NP + c0, a[d]);
-                tmem_wait_ld();
-#pragma unroll
-                for (int i = 0; i < 16; ++i) {
-                    uint32_t col[OZ_ND];
-#pragma unroll
-                    for (int d = 0; d < OZ_ND; ++d) {
-                        reg_after_wait(a[d][i]);
-                        col[d] = a[d][i];
-                    }
-                    hbuf[(c0 + i) * OZ_M + row] = oz_halves(col, ksh[2 * (c0 + i)], ksh[2 * (c0 + i) + 1]);
-                }
-            }
+            oz_read_sums(tlane + OZ_NHALF, OZ_NHALF, (ncol + 3) & ~3, ksh, hb + row);
             tc_fence_before();
             mbar_arrive(accfree);
+            mbar_arrive(hready0 + 8 * b);
             return 0;
         };
         int q = 0, gi = 0, hold_next = 0;
@@ -433,7 +484,6 @@ __global__ void __launch_bounds__(OZ_T, 1) k_angular_oz(DevBatch B, const AngIte
         for (int g = it.rbeg; g < it.rend && !bad; ++g, ++gi) {
             const int nk = B.tg_nk[g];
             const int gr = gact ? (int) gtab[2 * (nk - 1)] : 0;
-            double p0 = 0., p1 = 1., kmu = mu, k1 = 2.;        // pi_{k-1}, pi_k, k mu, k + 1
             for (int kc = 0; kc < nk; ++kc, ++q) {
                 const int s = q % OZ_ASTAGES;
                 // the chunk's scale 2^(OZ_FRAC - e_k - g_r) (0 past the case's angles: zero
@@ -452,13 +502,34 @@ __global__ void __launch_bounds__(OZ_T, 1) k_angular_oz(DevBatch B, const AngIte
                     bad = 1;
                     break;
                 }
-                tc_fence_after();
                 const uint32_t acol = tlane + OZ_ACOL + s * OZ_ACOLS;
-                const double *f2 = f2s + kc * OZ_KC + 1;
-                if (kc == 0)
-                    oz_produce_chunk<true>(f2, mu, sg, sp, sm, gsc, kmu, k1, p0, p1, acol);
-                else
-                    oz_produce_chunk<false>(f2, mu, sg, sp, sm, gsc, kmu, k1, p0, p1, acol);
+#pragma unroll 1
+                for (int hf = 0; hf < 2 && !bad; ++hf) {
+                    // this half's row values from the recurrence warps
+                    if (__any_sync(0xffffffffu, !mbar_wait(vfull, (2 * q + hf) & 1, err))) {
+                        bad = 1;
+                        break;
+                    }
+                    tc_fence_after();
+                    uint32_t w[32];
+                    tmem_ld16(tlane + OZ_VCOL, *(uint32_t(*)[16]) w);
+                    tmem_ld16(tlane + OZ_VCOL + 16, *(uint32_t(*)[16]) (w + 16));
+                    tmem_wait_ld();
+                    tc_fence_before();
+                    mbar_arrive(vfree);
+                    double v[16];
+#pragma unroll
+                    for (int u = 0; u < 16; ++u) {
+                        reg_after_wait(w[2 * u]);
+                        reg_after_wait(w[2 * u + 1]);
+                        v[u] = __hiloint2double((int) w[2 * u + 1], (int) w[2 * u]);
+                    }
+                    if (kc == 0 && hf == 0)
+                        oz_digit_half<true>(v, 0, sg, sp, sm, gsc, acol);
+                    else
+                        oz_digit_half<false>(v, hf, sg, sp, sm, gsc, acol);
+                }
+                if (bad) break;
                 tmem_wait_st();
                 tc_fence_before();
                 sgrp[s] = gi;
@@ -466,6 +537,149 @@ __global__ void __launch_bounds__(OZ_T, 1) k_angular_oz(DevBatch B, const AngIte
             }
         }
         while (!bad && hold_next < it.rend - it.rbeg) bad = take(hold_next++);
+    } else if (warp >= OZ_QUAD_WARP) {
+        // ---------------- warps 14-17: quadratic forms, one row per thread ----------------
+        // A warp whose wait fails keeps taking the barriers of the four warps,
+        // which stop together.
+        const int t1 = tid - OZ_QUAD_WARP * 32;              // product row
+        const int eh = t1 >> 1, emir = t1 & 1;
+        const int ej = it.xt * OZ_HALF + eh;
+        const bool eact = ej < nh;
+        const signed char *gtab = B.oz_rowexp + C.rx_off + (size_t) (eact ? ej : 0) * C.nkx * 2 + emir;
+        int slot1[NC1 > 0 ? NC1 : 1];
+#pragma unroll
+        for (int k = 0; k < NC1; ++k) slot1[k] = 1 + B.idx1[k];
+        // per column set: f-weighted sums over radii of the four invariants
+        double racc[1 + NC1 + OZ_MAX_ND2][4];
+#pragma unroll
+        for (int s = 0; s < 1 + NC1 + OZ_MAX_ND2; ++s)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) racc[s][e] = 0.;
+        int gi = 0;
+        for (int g = it.rbeg; g < it.rend; ++g, ++gi) {
+            const int gr0 = B.tg_r0[g], gn = B.tg_n[g], nk = B.tg_nk[g];
+            // the previous group's weights and scales have been read by all four warps
+            if (oz_epi_sync_or(bad || gn > OZ_MAX_GN)) {
+                bad = 1;
+                break;
+            }
+            for (int i = t1; i < gn * NS; i += 128) {
+                const int p = i / NS, s = i - p * NS;
+                const int slot = s == 0 ? 0 : (s <= NC1 ? slot1[s - 1] : 1 + B.idx2[s - 1 - NC1]);
+                wsh[p * OZ_MAX_NS + s] = B.w[(size_t) slot * R + gr0 + p];
+            }
+            // column scales with the row-independent factor of the combination
+            if (t1 < OZ_NP) csh[t1] = oz_pow2(B.oz_colexp[(size_t) g * OZ_NP + t1] + OZ_CSHIFT);
+            // the scales of this row and of its pair row (which holds this row's sm)
+            const double rsc = oz_pow2(eact ? (int) gtab[2 * (nk - 1)] : 0);
+            const double rsp = __shfl_xor_sync(0xffffffffu, rsc, 1);
+            oz_epi_sync_or(0);
+            // both halves of the group's sums are in its buffer
+            const double *hb = hbuf + (gi & 1) * OZ_HB;
+            if (__any_sync(0xffffffffu, !mbar_wait(hready0 + 8 * (gi & 1), (gi >> 1) & 1, err))) {
+                bad = 1;
+                continue;
+            }
+            for (int p = 0; p < gn; ++p) {
+                // columns of S (i < CPR, this row) and D' (i >= CPR, the pair row: sm)
+                double v[2 * CPR];
+#pragma unroll
+                for (int i = 0; i < CPR; ++i) {
+                    const int cs = p * CPR + i, cd = OZ_NHALF + p * CPR + i;
+                    v[i] = hb[cs * OZ_M + t1] * (rsc * csh[cs]);
+                    v[CPR + i] = hb[cd * OZ_M + (t1 ^ 1)] * (rsp * csh[cd]);
+                }
+                const double *wp = wsh + p * OZ_MAX_NS;
+                const double f = wp[0];
+                // invariants of (sp, sm): |sp|^2, |sm|^2, Re(sp sm*), Im(sm sp*)
+                const double spr = v[0], spi = v[1], smr = v[CPR], smi = v[CPR + 1];
+                const double ia = spr * spr + spi * spi, ib = smr * smr + smi * smi;
+                const double ic = spr * smr + spi * smi, id = smi * spr - smr * spi;
+                racc[0][0] += f * ia;
+                racc[0][1] += f * ib;
+                racc[0][2] += f * ic;
+                racc[0][3] += f * id;
+#pragma unroll
+                for (int k = 0; k < NC1; ++k) {
+                    const double fl = wp[1 + k];
+                    const double plr = v[2 + 2 * k], pli = v[3 + 2 * k];
+                    const double mlr = v[CPR + 2 + 2 * k], mli = v[CPR + 3 + 2 * k];
+                    const double da = 2. * (plr * spr + pli * spi), db = 2. * (mlr * smr + mli * smi);
+                    const double dc = plr * smr + pli * smi + spr * mlr + spi * mli;
+                    const double dd = mli * spr - mlr * spi + smi * plr - smr * pli;
+                    racc[1 + k][0] += fl * ia + f * da;
+                    racc[1 + k][1] += fl * ib + f * db;
+                    racc[1 + k][2] += fl * ic + f * dc;
+                    racc[1 + k][3] += fl * id + f * dd;
+                }
+#pragma unroll
+                for (int k = 0; k < OZ_MAX_ND2; ++k) {
+                    if (k < nd2) {
+                        const double fl = wp[1 + NC1 + k];
+                        racc[1 + NC1 + k][0] += fl * ia;
+                        racc[1 + NC1 + k][1] += fl * ib;
+                        racc[1 + NC1 + k][2] += fl * ic;
+                        racc[1 + NC1 + k][3] += fl * id;
+                    }
+                }
+            }
+            // the buffer is free for the group after next
+            mbar_arrive(hfree0 + 8 * (gi & 1));
+        }
+        if (oz_epi_sync_or(bad)) bad = 1;
+        if (!bad && eact) {
+            // phase-matrix elements: ((A + B) / 4, (A - B) / 4, -C / 2, D / 2)
+            const int jj = emir ? n_qang - 1 - ej : ej;
+            const int Q = 4 * (1 + B.nd);
+            double *pc = part + C.part_off + (size_t) it.g * Q * n_qang;
+#pragma unroll
+            for (int s = 0; s < 1 + NC1 + OZ_MAX_ND2; ++s) {
+                if (s >= NS) break;
+                const int slot = s == 0 ? 0 : (s <= NC1 ? slot1[s - 1] : 1 + B.idx2[s - 1 - NC1]);
+                double *o = pc + (size_t) slot * 4 * n_qang + jj;
+                o[0] = .25 * (racc[s][0] + racc[s][1]);
+                o[(size_t) n_qang] = .25 * (racc[s][0] - racc[s][1]);
+                o[(size_t) 2 * n_qang] = -.5 * racc[s][2];
+                o[(size_t) 3 * n_qang] = .5 * racc[s][3];
+            }
+        }
+    } else if (warp >= OZ_RECUR_WARP) {
+        // ---------------- warps 10-13: the pi/tau recurrence, one row per thread ----------------
+        // row = tensor-memory lane of the warp (its quarter of the lanes)
+        const int row = (warp & 3) * 32 + (tid & 31), h = row >> 1, mirror = row & 1;
+        const uint32_t tlane = tmem + ((uint32_t) ((warp & 3) * 32) << 16);
+        const int gj = it.xt * OZ_HALF + h;
+        const double mu = gj < nh ? B.mu_pool[C.mu_off + gj] : 0.;
+        const double sg = mirror ? -1. : 1.;
+        int hc = 0;                                          // halves handed over
+        for (int g = it.rbeg; g < it.rend && !bad; ++g) {
+            const int nk = B.tg_nk[g];
+            double p0 = 0., p1 = 1., kmu = mu, k1 = 2.;        // pi_{k-1}, pi_k, k mu, k + 1
+            for (int kc = 0; kc < nk && !bad; ++kc) {
+#pragma unroll 1
+                for (int hf = 0; hf < 2; ++hf, ++hc) {
+                    double v[16];
+                    oz_recur_half(f2s + kc * OZ_KC + hf * 16 + 1, mu, sg, kmu, k1, p0, p1, v);
+                    // the digit warps have read the previous half
+                    if (__any_sync(0xffffffffu, !(hc == 0 || mbar_wait(vfree, (hc - 1) & 1, err)))) {
+                        bad = 1;
+                        break;
+                    }
+                    tc_fence_after();
+                    uint32_t w[32];
+#pragma unroll
+                    for (int u = 0; u < 16; ++u) {
+                        w[2 * u] = (uint32_t) __double2loint(v[u]);
+                        w[2 * u + 1] = (uint32_t) __double2hiint(v[u]);
+                    }
+                    tmem_st16(tlane + OZ_VCOL, *(const uint32_t(*)[16]) w);
+                    tmem_st16(tlane + OZ_VCOL + 16, *(const uint32_t(*)[16]) (w + 16));
+                    tmem_wait_st();
+                    tc_fence_before();
+                    mbar_arrive(vfull);
+                }
+            }
+        }
     } else if (warp == OZ_COPY_WARP) {
         // ---------------- warp 9, lane 0: B copies, up to OZ_BSLOTS chunks ahead ----------------
         if ((tid & 31) == 0) {
@@ -521,143 +735,41 @@ __global__ void __launch_bounds__(OZ_T, 1) k_angular_oz(DevBatch B, const AngIte
         __syncwarp();
         mbar_wait(fin, 0u, nullptr);
     } else if (warp >= 4) {
-        // ---------------- warps 4-7: sums, quadratic forms ----------------
-        // A warp whose wait fails skips the tensor-memory work from then on but
-        // keeps taking the barriers of the four warps, which stop together.
+        // ---------------- warps 4-7: the S sums of each group ----------------
         const int t1 = tid - 128;                            // product row = tensor-memory lane
         const uint32_t trow = tmem + ((uint32_t) ((warp - 4) * 32) << 16);
-        const int eh = t1 >> 1, emir = t1 & 1;
-        const int ej = it.xt * OZ_HALF + eh;
-        const bool eact = ej < nh;
-        const signed char *gtab = B.oz_rowexp + C.rx_off + (size_t) (eact ? ej : 0) * C.nkx * 2 + emir;
-        int slot1[NC1 > 0 ? NC1 : 1];
-#pragma unroll
-        for (int k = 0; k < NC1; ++k) slot1[k] = 1 + B.idx1[k];
-        // per column set: f-weighted sums over radii of the four invariants
-        double racc[1 + NC1 + OZ_MAX_ND2][4];
-#pragma unroll
-        for (int s = 0; s < 1 + NC1 + OZ_MAX_ND2; ++s)
-#pragma unroll
-            for (int e = 0; e < 4; ++e) racc[s][e] = 0.;
         int gi = 0;
-        for (int g = it.rbeg; g < it.rend; ++g, ++gi) {
-            const int gr0 = B.tg_r0[g], gn = B.tg_n[g], nk = B.tg_nk[g];
-            // the previous group's weights, scales and sums have been read by all four warps
-            if (oz_epi_sync_or(bad || gn > OZ_MAX_GN)) {
+        for (int g = it.rbeg; g < it.rend && !bad; ++g, ++gi) {
+            const int ncol = B.tg_n[g] * CPR;                 // used columns of each half
+            // every reader has staged its bias terms of this group, the
+            // buffer's previous group has been through the quadratic forms,
+            // and this group's products are done (warp-uniform: the
+            // tensor-memory accesses below are warp-wide)
+            const int b = gi & 1;
+            bool ok = gi == 0 || mbar_wait(qdone, (gi - 1) & 1, err);
+            ok = ok && (gi < 2 || mbar_wait(hfree0 + 8 * b, ((gi >> 1) - 1) & 1, err));
+            ok = ok && mbar_wait(accfull, gi & 1, err);
+            double *hb = hbuf + b * OZ_HB;
+            if (__any_sync(0xffffffffu, !ok)) {
                 bad = 1;
                 break;
             }
-            for (int i = t1; i < gn * NS; i += 128) {
-                const int p = i / NS, s = i - p * NS;
-                const int slot = s == 0 ? 0 : (s <= NC1 ? slot1[s - 1] : 1 + B.idx2[s - 1 - NC1]);
-                wsh[p * OZ_MAX_NS + s] = B.w[(size_t) slot * R + gr0 + p];
-            }
-            // column scales with the row-independent factor of the combination
-            if (t1 < OZ_NP) csh[t1] = oz_pow2(B.oz_colexp[(size_t) g * OZ_NP + t1] + OZ_CSHIFT);
-            // the scales of this row and of its pair row (which holds this row's sm)
-            const double rsc = oz_pow2(eact ? (int) gtab[2 * (nk - 1)] : 0);
-            const double rsp = __shfl_xor_sync(0xffffffffu, rsc, 1);
-            oz_epi_sync_or(0);
-            // warp-uniform decision: the tensor-memory accesses below are warp-wide
-            const bool arrived = mbar_wait(accfull, gi & 1, err);
-            if (__any_sync(0xffffffffu, !arrived)) {
-                bad = 1;
-                continue;
-            }
             tc_fence_after();
-            // the exact sums of the group's used S columns into the buffer as int64
-            // halves, 16 columns at a time (the producers take the D' columns);
-            // the accumulators go back right after
-            const int ncol = gn * CPR;                       // used columns of each half
-#pragma unroll 1
-            for (int c0 = 0; c0 < OZ_NHALF; c0 += 16) {
-                if (c0 >= ncol) continue;
-                uint32_t a[OZ_ND][16];
-#pragma unroll
-                for (int d = 0; d < OZ_ND; ++d) tmem_ld16(trow + d * OZ_NP + c0, a[d]);
-                tmem_wait_ld();
-#pragma unroll
-                for (int i = 0; i < 16; ++i) {
-                    uint32_t col[OZ_ND];
-#pragma unroll
-                    for (int d = 0; d < OZ_ND; ++d) {
-                        reg_after_wait(a[d][i]);
-                        col[d] = a[d][i];
-                    }
-                    hbuf[(c0 + i) * OZ_M + t1] = oz_halves(col, ksh[2 * (c0 + i)], ksh[2 * (c0 + i) + 1]);
-                }
-            }
-            // hand the accumulators to the next group's products; both halves of
-            // the sums are in the buffer once the producers have taken theirs
+            // the exact sums of the group's used S columns into the buffer
+            // (the digit warps take the D' columns); the accumulators go back
+            // right after
+            oz_read_sums(trow, 0, (ncol + 3) & ~3, ksh, hb + t1);
             tc_fence_before();
             mbar_arrive(accfree);
+            mbar_arrive(hready0 + 8 * b);
+            // once both halves are out (the digit warps no longer read the bias
+            // terms), the next group's bias terms
             if (__any_sync(0xffffffffu, !mbar_wait(accfree, gi & 1, err))) {
                 bad = 1;
-                continue;
+                break;
             }
-            for (int p = 0; p < gn; ++p) {
-                // columns of S (i < CPR, this row) and D' (i >= CPR, the pair row: sm)
-                double v[2 * CPR];
-#pragma unroll
-                for (int i = 0; i < CPR; ++i) {
-                    const int cs = p * CPR + i, cd = OZ_NHALF + p * CPR + i;
-                    v[i] = oz_value(hbuf[cs * OZ_M + t1], rsc * csh[cs]);
-                    v[CPR + i] = oz_value(hbuf[cd * OZ_M + (t1 ^ 1)], rsp * csh[cd]);
-                }
-                const double *wp = wsh + p * OZ_MAX_NS;
-                const double f = wp[0];
-                // invariants of (sp, sm): |sp|^2, |sm|^2, Re(sp sm*), Im(sm sp*)
-                const double spr = v[0], spi = v[1], smr = v[CPR], smi = v[CPR + 1];
-                const double ia = spr * spr + spi * spi, ib = smr * smr + smi * smi;
-                const double ic = spr * smr + spi * smi, id = smi * spr - smr * spi;
-                racc[0][0] += f * ia;
-                racc[0][1] += f * ib;
-                racc[0][2] += f * ic;
-                racc[0][3] += f * id;
-#pragma unroll
-                for (int k = 0; k < NC1; ++k) {
-                    const double fl = wp[1 + k];
-                    const double plr = v[2 + 2 * k], pli = v[3 + 2 * k];
-                    const double mlr = v[CPR + 2 + 2 * k], mli = v[CPR + 3 + 2 * k];
-                    const double da = 2. * (plr * spr + pli * spi), db = 2. * (mlr * smr + mli * smi);
-                    const double dc = plr * smr + pli * smi + spr * mlr + spi * mli;
-                    const double dd = mli * spr - mlr * spi + smi * plr - smr * pli;
-                    racc[1 + k][0] += fl * ia + f * da;
-                    racc[1 + k][1] += fl * ib + f * db;
-                    racc[1 + k][2] += fl * ic + f * dc;
-                    racc[1 + k][3] += fl * id + f * dd;
-                }
-#pragma unroll
-                for (int k = 0; k < OZ_MAX_ND2; ++k) {
-                    if (k < nd2) {
-                        const double fl = wp[1 + NC1 + k];
-                        racc[1 + NC1 + k][0] += fl * ia;
-                        racc[1 + NC1 + k][1] += fl * ib;
-                        racc[1 + NC1 + k][2] += fl * ic;
-                        racc[1 + NC1 + k][3] += fl * id;
-                    }
-                }
-            }
-            // the buffer is free for the next group: its bias terms, then done
             if (g + 1 < it.rend) ksh[t1] = B.oz_bcorr[(size_t) (g + 1) * 2 * OZ_NP + t1];
             mbar_arrive(qdone);
-        }
-        if (oz_epi_sync_or(bad)) bad = 1;
-        if (!bad && eact) {
-            // phase-matrix elements: ((A + B) / 4, (A - B) / 4, -C / 2, D / 2)
-            const int jj = emir ? n_qang - 1 - ej : ej;
-            const int Q = 4 * (1 + B.nd);
-            double *pc = part + C.part_off + (size_t) it.g * Q * n_qang;
-#pragma unroll
-            for (int s = 0; s < 1 + NC1 + OZ_MAX_ND2; ++s) {
-                if (s >= NS) break;
-                const int slot = s == 0 ? 0 : (s <= NC1 ? slot1[s - 1] : 1 + B.idx2[s - 1 - NC1]);
-                double *o = pc + (size_t) slot * 4 * n_qang + jj;
-                o[0] = .25 * (racc[s][0] + racc[s][1]);
-                o[(size_t) n_qang] = .25 * (racc[s][0] - racc[s][1]);
-                o[(size_t) 2 * n_qang] = -.5 * racc[s][2];
-                o[(size_t) 3 * n_qang] = .5 * racc[s][3];
-            }
         }
     }
     if (bad) atomicExch(err, 1);
