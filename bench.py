@@ -73,9 +73,11 @@ METRIC = "polydisperse solves/s (+Jacobian)"
 UNIT = "solves/s"
 N_CASES = 4096
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_angular /
-# k_angular_tc launch on this workload: measured with ncu on a 256-case batch
-# of the same generator and scaled by the ratio of angular work (13.33).
-ANGULAR_TRAFFIC = {"fp64": 12.21e9, "tf32x3": 5.15e9, "int8": None}
+# k_angular_tc / k_angular_oz launch on this workload: measured with ncu on a
+# 256-case batch of the same generator and scaled by the ratio of angular work
+# (13.33; 13.0 in chunks of the int8 product: 317.6 MB -> 4.13 GB, about the
+# B operand digits read once).
+ANGULAR_TRAFFIC = {"fp64": 12.21e9, "tf32x3": 5.15e9, "int8": 4.13e9}
 WORKLOAD = ("batched uneven: 4096 seeded cases (r_eff 0.05-20 um, v_eff 0.02-0.3, lambda 0.34-2.1 um, "
             "mr 1.33-1.60, mi 1e-8-0.1, gamma/log-normal, 100-2000 radii, x_max 0.2-1063), "
             "4 derivatives each (mr, mi, a1, a2), GSF + 181-angle phase matrix")
