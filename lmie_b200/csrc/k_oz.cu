@@ -14,11 +14,11 @@
 //   - k_angular_oz: a block owns one angle tile of one case and a range of its
 //     radius groups; per group, chunks of OZ_KC orders flow through the
 //     pipeline:
-//       * warps 10-13 (one thread per row) run the pi/tau recurrence in FP64
-//         and hand the row values over in tensor memory, half a chunk at a
-//         time;
+//       * warps 10-13 (one thread per row) run the pi/tau recurrence in FP64,
+//         scale the row values and extract their digits (one FMA each), and
+//         hand the digit words over in tensor memory, half a chunk at a time;
 //       * warps 0-3 (one thread per row, the row's tensor-memory lane) turn
-//         them into the row's six digit slices in tensor memory (two stages);
+//         them into the row's six digit slices of the A stage (two stages);
 //       * lane 0 of warp 9 brings the group's B chunks into shared memory with
 //         bulk copies running ahead of the products;
 //       * lane 0 of warp 8 issues the 21 digit products of a chunk,
@@ -333,16 +333,15 @@ __device__ __forceinline__ void oz_recur_half(const double *__restrict__ f2, dou
     }
 }
 
-// Half hf (orders 16 hf .. 16 hf + 15) of a chunk of one product row (digit
-// thread): the row values vb[u], their digits and the row's six
-// digit slices stored to tensor memory at column acol (warp-wide).  sp / sm:
-// the scales of odd / even orders (the mirror row carries s_k); FIRST: the
-// case's first chunk, whose orders 1..16 have their own exponents
-// (gsc = 2^(OZ_FRAC - g_r), 0 for an inactive row).
+// The digits of half hf (orders 16 hf .. 16 hf + 15) of a chunk of one
+// product row (recurrence thread): w[2u], w[2u + 1] = the low and high words
+// of oz_digits of row value v[u].  sp / sm: the scales of odd / even orders
+// (the mirror row carries s_k); FIRST: the case's first chunk, whose orders
+// 1..16 have their own exponents (gsc = 2^(OZ_FRAC - g_r), 0 for an inactive
+// row).
 template <bool FIRST>
-__device__ __forceinline__ void oz_digit_half(const double (&vb)[16], int hf, double sg, double sp, double sm,
-                                              double gsc, uint32_t acol) {
-    uint32_t lo[16], hi[16];
+__device__ __forceinline__ void oz_digit_words(const double (&v)[16], int hf, double sg, double sp, double sm,
+                                               double gsc, uint32_t (&w)[32]) {
 #pragma unroll
     for (int u = 0; u < 16; ++u) {
         double sc = (u & 1) ? sm : sp;
@@ -352,14 +351,19 @@ __device__ __forceinline__ void oz_digit_half(const double (&vb)[16], int hf, do
             const int ek = u == 0 ? 1 : (u == 1 ? 2 : (u < 4 ? 3 : (u < 8 ? 4 : 5)));
             sc = (u & 1) ? sg * gsc * inv[ek - 1] : gsc * inv[ek - 1];
         }
-        oz_digits(vb[u], sc, lo[u], hi[u]);
+        oz_digits(v[u], sc, w[2 * u], w[2 * u + 1]);
     }
+}
+
+// The row's six digit slices of half hf of a chunk from its digit words
+// (digit thread), stored to tensor memory at column acol (warp-wide).
+__device__ __forceinline__ void oz_store_slices(const uint32_t (&dw)[32], int hf, uint32_t acol) {
     uint32_t w[OZ_ND][4];
 #pragma unroll
     for (int qd = 0; qd < 4; ++qd) {
         uint32_t s6[OZ_ND];
-        const uint32_t l4[4] = {lo[4 * qd], lo[4 * qd + 1], lo[4 * qd + 2], lo[4 * qd + 3]};
-        const uint32_t h4[4] = {hi[4 * qd], hi[4 * qd + 1], hi[4 * qd + 2], hi[4 * qd + 3]};
+        const uint32_t l4[4] = {dw[8 * qd], dw[8 * qd + 2], dw[8 * qd + 4], dw[8 * qd + 6]};
+        const uint32_t h4[4] = {dw[8 * qd + 1], dw[8 * qd + 3], dw[8 * qd + 5], dw[8 * qd + 7]};
         oz_slices4_biased(l4, h4, s6);
 #pragma unroll
         for (int sl = 0; sl < OZ_ND; ++sl) w[sl][qd] = s6[sl];
@@ -449,17 +453,13 @@ __global__ void __launch_bounds__(OZ_T, 1) k_angular_oz(DevBatch B, const AngIte
     int bad = 0;
 
     if (tid < OZ_M) {
-        // ---------------- warps 0-3: the A digits, one row (lane) per thread ----------------
-        const int row = tid, h = row >> 1, mirror = row & 1;
-        const int gj = it.xt * OZ_HALF + h;
-        const bool gact = gj < nh;
-        const signed char *gtab = B.oz_rowexp + C.rx_off + (size_t) (gact ? gj : 0) * C.nkx * 2 + mirror;
+        // ---------------- warps 0-3: the A digit slices, one row (lane) per thread ----------------
+        const int row = tid;
         const uint32_t tlane = tmem + ((uint32_t) (warp * 32) << 16);
-        const double sg = mirror ? -1. : 1.;
         // The digit warps take the D' columns of a group's finished sums out of
-        // tensor memory (the epilogue warps take the S columns): once the
-        // epilogue has read the previous group's sums from the buffer, after
-        // the group's last products.  Returns nonzero when a wait gave up.
+        // tensor memory (warps 4-7 take the S columns): once the quadratic
+        // forms are done with the buffer's previous group, after the group's
+        // last products.  Returns nonzero when a wait gave up.
         auto take = [&](int gh) -> int {
             const int g = it.rbeg + gh, ncol = B.tg_n[g] * CPR;
             // the bias terms of the group are staged, the buffer's previous
@@ -483,14 +483,8 @@ __global__ void __launch_bounds__(OZ_T, 1) k_angular_oz(DevBatch B, const AngIte
         for (int i = 0; i < OZ_ASTAGES; ++i) sgrp[i] = 0;
         for (int g = it.rbeg; g < it.rend && !bad; ++g, ++gi) {
             const int nk = B.tg_nk[g];
-            const int gr = gact ? (int) gtab[2 * (nk - 1)] : 0;
             for (int kc = 0; kc < nk; ++kc, ++q) {
                 const int s = q % OZ_ASTAGES;
-                // the chunk's scale 2^(OZ_FRAC - e_k - g_r) (0 past the case's angles: zero
-                // digits); the mirror row carries s_k, +1 for odd k, -1 for even k
-                const double gsc = gact ? oz_pow2(OZ_FRAC - gr) : 0.;
-                const double sp = gsc * oz_pow2(-oz_ec(kc));
-                const double sm = mirror ? -sp : sp;
                 // the stage's previous chunk must have been consumed by its products,
                 // which reach its group once the sums of every earlier group are out;
                 // warp-uniform decisions: the tensor-memory accesses are warp-wide
@@ -517,17 +511,9 @@ __global__ void __launch_bounds__(OZ_T, 1) k_angular_oz(DevBatch B, const AngIte
                     tmem_wait_ld();
                     tc_fence_before();
                     mbar_arrive(vfree);
-                    double v[16];
 #pragma unroll
-                    for (int u = 0; u < 16; ++u) {
-                        reg_after_wait(w[2 * u]);
-                        reg_after_wait(w[2 * u + 1]);
-                        v[u] = __hiloint2double((int) w[2 * u + 1], (int) w[2 * u]);
-                    }
-                    if (kc == 0 && hf == 0)
-                        oz_digit_half<true>(v, 0, sg, sp, sm, gsc, acol);
-                    else
-                        oz_digit_half<false>(v, hf, sg, sp, sm, gsc, acol);
+                    for (int u = 0; u < 32; ++u) reg_after_wait(w[u]);
+                    oz_store_slices(w, hf, acol);
                 }
                 if (bad) break;
                 tmem_wait_st();
@@ -649,29 +635,36 @@ __global__ void __launch_bounds__(OZ_T, 1) k_angular_oz(DevBatch B, const AngIte
         const int row = (warp & 3) * 32 + (tid & 31), h = row >> 1, mirror = row & 1;
         const uint32_t tlane = tmem + ((uint32_t) ((warp & 3) * 32) << 16);
         const int gj = it.xt * OZ_HALF + h;
-        const double mu = gj < nh ? B.mu_pool[C.mu_off + gj] : 0.;
+        const bool gact = gj < nh;
+        const double mu = gact ? B.mu_pool[C.mu_off + gj] : 0.;
+        const signed char *gtab = B.oz_rowexp + C.rx_off + (size_t) (gact ? gj : 0) * C.nkx * 2 + mirror;
         const double sg = mirror ? -1. : 1.;
         int hc = 0;                                          // halves handed over
         for (int g = it.rbeg; g < it.rend && !bad; ++g) {
             const int nk = B.tg_nk[g];
+            const int gr = gact ? (int) gtab[2 * (nk - 1)] : 0;
             double p0 = 0., p1 = 1., kmu = mu, k1 = 2.;        // pi_{k-1}, pi_k, k mu, k + 1
             for (int kc = 0; kc < nk && !bad; ++kc) {
+                // the chunk's scale 2^(OZ_FRAC - e_k - g_r) (0 past the case's angles: zero
+                // digits); the mirror row carries s_k, +1 for odd k, -1 for even k
+                const double gsc = gact ? oz_pow2(OZ_FRAC - gr) : 0.;
+                const double sp = gsc * oz_pow2(-oz_ec(kc));
+                const double sm = mirror ? -sp : sp;
 #pragma unroll 1
                 for (int hf = 0; hf < 2; ++hf, ++hc) {
                     double v[16];
                     oz_recur_half(f2s + kc * OZ_KC + hf * 16 + 1, mu, sg, kmu, k1, p0, p1, v);
+                    uint32_t w[32];
+                    if (kc == 0 && hf == 0)
+                        oz_digit_words<true>(v, 0, sg, sp, sm, gsc, w);
+                    else
+                        oz_digit_words<false>(v, hf, sg, sp, sm, gsc, w);
                     // the digit warps have read the previous half
                     if (__any_sync(0xffffffffu, !(hc == 0 || mbar_wait(vfree, (hc - 1) & 1, err)))) {
                         bad = 1;
                         break;
                     }
                     tc_fence_after();
-                    uint32_t w[32];
-#pragma unroll
-                    for (int u = 0; u < 16; ++u) {
-                        w[2 * u] = (uint32_t) __double2loint(v[u]);
-                        w[2 * u + 1] = (uint32_t) __double2hiint(v[u]);
-                    }
                     tmem_st16(tlane + OZ_VCOL, *(const uint32_t(*)[16]) w);
                     tmem_st16(tlane + OZ_VCOL + 16, *(const uint32_t(*)[16]) (w + 16));
                     tmem_wait_st();
