@@ -745,6 +745,13 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         }
     });
     const long long tot = off[R], ckn = ckoff[R];
+    // K1 launch order: cases by their largest n1, largest first, each from its
+    // largest radius down, so that the longest recurrences start first
+    std::vector<int> k1ord(ncase);
+    std::vector<long long> k1pre(ncase + 1, 0);
+    for (int k = 0; k < ncase; ++k) k1ord[k] = k;
+    std::stable_sort(k1ord.begin(), k1ord.end(), [&](int a, int b) { return cn1max[a] > cn1max[b]; });
+    for (int k = 0; k < ncase; ++k) k1pre[k + 1] = k1pre[k] + ps[k1ord[k]].n;
 
     // ---- order tables ----
     std::vector<double> fv((size_t) 4 * (n1max + 2), 0.);
@@ -1199,6 +1206,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         add(tc_pos.size() * 4); add(tc_roff.size() * 8); add(tg_r0.size() * 4); add(tg_n.size() * 4);
         add(tg_nk.size() * 4); add(tg_off.size() * 8); add(oz_f2.size() * 8); add(rx_start.size() * 8);
         for (int q = 0; q < 5; ++q) add((size_t) (ncase + 1) * 8);
+        add((size_t) ncase * 4); add((size_t) (ncase + 1) * 8);             // K1 launch order
         add(gl_ns.size() * 4); add(gl_mo.size() * 8); add(gl_go.size() * 8); add(gl_pt.size() * 4);
         add(gl_pi.size() * 4); add(gl_guess.size() * 8); add(gl_jr.size() * 8);
         if (L.save_control == 2) {
@@ -1224,6 +1232,8 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     int *h_n1r = put(hp, ho, n1r.data(), (size_t) R);
     int *h_n2r = put(hp, ho, n2r.data(), (size_t) R);
     int *h_rcase = put(hp, ho, rcase.data(), (size_t) R);
+    int *h_k1ord = put(hp, ho, k1ord.data(), (size_t) ncase);
+    long long *h_k1pre = put(hp, ho, k1pre.data(), (size_t) ncase + 1);
     long long *h_off = put(hp, ho, coff.data(), (size_t) R + 1);
     long long *h_ckoff = put(hp, ho, ckoff.data(), (size_t) R + 1);
     double *h_fv = put(hp, ho, fv.data(), fv.size());
@@ -1325,6 +1335,8 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     B.m_l = (const cplx *) dptr(h_ml);
     B.lambda_l = (const double *) dptr(h_laml);
     B.rcase = (const int *) dptr(h_rcase);
+    B.k1ord = (const int *) dptr(h_k1ord);
+    B.k1pre = (const long long *) dptr(h_k1pre);
     B.x = (const double *) dptr(h_x);
     B.xl = (const double *) dptr(h_xl);
     B.w = (const double *) dptr(h_w);

@@ -173,8 +173,15 @@ __global__ void __launch_bounds__(64) k_mie(DevBatch B, int c0, int write_value,
                                             double *__restrict__ rs) {
     constexpr int CC = 1 + NC;
     constexpr int CW = k1_ck_width(NC);               // D (2), D_l (2 NC), ratio (1), ratio_l (NC)
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= B.R) return;
+    // thread t takes the radius of rank t in the launch order: cases in the
+    // order k1ord, each from its largest radius down
+    const long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= B.R) return;
+    const int kc = find_case(B.k1pre, B.ncase, t);
+    const int r = [&] {
+        const DevCase &Ck = B.cs[B.k1ord[kc]];
+        return Ck.r0 + Ck.nr - 1 - (int) (t - B.k1pre[kc]);
+    }();
     const int R = B.R;
     const DevCase &C = B.cs[B.rcase[r]];
     const int n1 = B.n1r[r], n2 = B.n2r[r];

@@ -51,6 +51,8 @@ struct DevBatch {
     const cplx *m_l;            // [ncase * nd]
     const double *lambda_l;     // [ncase * nd]
     const int *rcase;           // [R] case of each radius
+    const int *k1ord;           // [ncase] K1's order of the cases (largest n1 first)
+    const long long *k1pre;     // [ncase + 1] radii of the cases before each in that order
     const double *x;            // [R] size parameters
     const double *xl;           // [nd1][R] d x / d p for index1 slot k
     const double *w;            // [(1 + nd)][R] row 0: f = nr qw; row 1+kk: f_l (index1) or f_l2 (index2)
