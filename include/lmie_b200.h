@@ -107,6 +107,16 @@ int lmieb_oz_selftest(int K, double *max_rel_err);
  * the product kernel's bounded waits, taken without a fault. */
 int lmieb_oz_selftest_wait(int K, long long wait_cycles, int withhold, double *max_rel_err);
 
+/* Graph replay of the product path: a sub-batch whose kernel sequence is the
+ * same as the previous one on its slot -- the same structure of cases,
+ * radii, orders and angles in the same device arena, as in retrieval loops
+ * that change the refractive index or the size-distribution weights between
+ * calls -- runs as one CUDA graph, captured the second time the sequence
+ * comes.  Counts of the sequences captured and replayed since the library was
+ * loaded (timing mode, radius groups and save_control launch kernel by
+ * kernel).  Returns 0. */
+int lmieb_graph_stats(long long *captures, long long *replays);
+
 /* Device memory: out[0] free and out[1] total bytes of the current device
  * (cudaMemGetInfo), out[2] device bytes and out[3] pinned host bytes the
  * library holds (arenas, staging buffers, pools).  Returns 0 or -1. */

@@ -149,3 +149,38 @@ def test_autotune_picks_a_candidate_and_keeps_results():
         lib.lmieb_set_pipeline(0)
         lib.lmieb_set_work_granularity(abi.PRECISION_FP64, keep)
         lib.lmieb_set_work_granularity(0, C.c_double(4.0))
+
+
+def test_repeated_plan_is_replayed_as_a_graph():
+    """A solve whose structure repeats (here the refractive index changes
+    between calls, the radii, orders and angles do not) is captured the
+    second time it comes to a slot (the library alternates two) and replayed
+    from then on; the replayed results are the kernel-by-kernel ones bit for
+    bit, and a changed structure goes back to launching kernel by kernel."""
+    import ctypes as C
+    lib = libs.product()
+    lib.lmieb_graph_stats.argtypes = [C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
+    def stats():
+        a, b = C.c_longlong(), C.c_longlong()
+        lib.lmieb_graph_stats(C.byref(a), C.byref(b))
+        return a.value, b.value
+    base = all_cases()["c2"]
+    variants = [dataclasses.replace(base, mr=1.335 + 0.01 * i, mi=1e-6 * (1 + i)) for i in range(4)]
+    # kernel by kernel: the first sight of each (a different structure in between)
+    other = all_cases()["gamma"]
+    first = []
+    for v in variants:
+        first.append(libs.run_product(v))
+        libs.run_product(other)
+    c0, r0 = stats()
+    # the same structure call after call: captured once, then replayed
+    again = [libs.run_product(v) for v in variants + variants]
+    c1, r1 = stats()
+    assert 1 <= c1 - c0 <= 2 and r1 - r0 >= 2 * len(variants) - 2, (c0, r0, c1, r1)
+    for a, b in zip(first + first, again):
+        assert a.n_coef == b.n_coef and a.scalars == b.scalars
+        for name in ("gc", "pf", "gc_l", "pf_l"):
+            assert np.array_equal(getattr(a, name), getattr(b, name)), name
+    # another structure: launched kernel by kernel again
+    libs.run_product(other)
+    assert stats() == (c1, r1)
