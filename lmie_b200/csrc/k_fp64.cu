@@ -957,6 +957,190 @@ __global__ void k_exp_ckpt(DevBatch B, long long total, const long long *__restr
 // least 128 (the basis phase) and at most EX_TMAX
 constexpr int EX_TMAX = 256;
 
+// D (8 x 8, two values per thread) += A (8 x 4, one value) B (4 x 8, one value)
+// in FP64 on the tensor cores
+__device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+// ---------------------------------------------------------------------------
+// K4b of the GSF expansion on the FP64 tensor cores: one block of 4 warps per
+// (case, order tile, angle tile).  For each order parity the 16 orders of
+// that parity form an M = 16 product over K = the tile's EX_AT node pairs:
+// the basis functions against the folded moments of that parity.  Each
+// function feeds two outputs per column (N = 2 ncol): p00 -> (e0: m0, e3: m5),
+// p0+2 -> (e4: m6, e5: m7), p2+2 -> (e1: m2, e2: m3) and p2-2 -> (e1: m1,
+// e2: m4), the last two into the same accumulators (the sums of the FP64
+// kernel, k_exp_tile<0>, in another order).  Basis and moments are staged in
+// the m8n8k4 fragment order, so every operand load of a warp reads 32
+// consecutive doubles.  Warp w takes parity w & 1 and the orders
+// 8 (w >> 1) .. + 7 of it.
+// ---------------------------------------------------------------------------
+constexpr int EX_NB = 4;                 // n-blocks of 8 outputs: up to 16 columns
+constexpr int EX_KS = EX_AT / 4;         // k-steps of 4 node pairs
+// one fragment (32 lanes) every EX_SEG doubles: a warp's fragment load reads
+// 32 consecutive doubles, and the staging stores of a warp (4 lanes of each
+// of 8 k-steps) fall on distinct bank pairs
+constexpr int EX_SEG = 36;
+constexpr int EX_AF = 4 * 2 * 2 * EX_KS * EX_SEG;   // basis fragments: [f][parity][m-block][k-step]
+
+// doubles of the moment fragments: [parity][4 function slots][n-block][k-step]
+__host__ __device__ inline int ex_bf_size(int ncol) { return 2 * 4 * ((2 * ncol + 7) / 8) * EX_KS * EX_SEG; }
+
+// GSF function F of one node pair over the orders of a tile (u < lt, zeros
+// after), into its fragment positions (order u = par + 2 m: block par,
+// m >> 3, row m & 7); the recurrence coefficients' loads of the fully
+// unrolled steps do not depend on the chain and go ahead of it.
+template <int F>
+__device__ __forceinline__ void gsf_tile_chain(double *af, const double *rcs, double x, double prev, double cur,
+                                               int l0, int lt) {
+    if (lt == EX_LT && l0 >= 3) {
+#pragma unroll
+        for (int u = 0; u < EX_LT; ++u) {
+            const double v = basis_step<0>(F, rcs + 8 * u, x, cur, prev);
+            prev = cur;
+            cur = v;
+            af[(((u & 1) * 2 + (u >> 4)) * EX_KS) * EX_SEG + (((u >> 1) & 7) << 2)] = v;
+        }
+        return;
+    }
+    for (int u = 0; u < EX_LT; ++u) {
+        double v = 0.;
+        if (u < lt) {
+            const int l = l0 + u;
+            v = l < 3 ? basis_first<0>(F, l, x) : basis_step<0>(F, rcs + 8 * u, x, cur, prev);
+            prev = cur;
+            cur = v;
+        }
+        af[(((u & 1) * 2 + (u >> 4)) * EX_KS) * EX_SEG + (((u >> 1) & 7) << 2)] = v;
+    }
+}
+
+__global__ void __launch_bounds__(128) k_exp_tile_gsf(DevBatch B, const ExpItem *__restrict__ items,
+                                                     const double *__restrict__ pfn,
+                                                     const double *__restrict__ ckpt, double *__restrict__ exq) {
+    extern __shared__ double sm[];
+    const ExpItem it = items[blockIdx.x];
+    const DevCase &C = B.cs[it.c];
+    const int nh = C.nh, nq = C.n_qang, ncf = C.n_coef;
+    const int ncol = 1 + B.nd, nbn = (2 * ncol + 7) >> 3;
+    const int l0 = it.lt * EX_LT, lt = min(EX_LT, ncf - l0);
+    const int i0 = it.at * EX_AT;
+    const double *mup = B.mu_pool + C.mu_off, *wqp = mup + nq;
+    double *Af = sm;                                       // basis fragments
+    double *Bf = Af + EX_AF;                               // moment fragments
+    double *rcs = Bf + ex_bf_size(ncol);                   // [8 EX_LT] recurrence coefficients
+    for (int t = threadIdx.x; t < 8 * lt; t += blockDim.x) rcs[t] = B.rc[8 * (size_t) l0 + t];
+    __syncthreads();
+    // basis functions of the tile, thread per (function, node pair): order
+    // u = par + 2 (8 mb + m) is row m of block (par, mb); node pair ia is
+    // column ia & 3 of k-step ia >> 2
+    {
+        const int f = threadIdx.x >> 5, ia = threadIdx.x & 31, i = i0 + ia;
+        double *af = Af + (size_t) f * (2 * 2 * EX_KS * EX_SEG) + (ia >> 2) * EX_SEG + (ia & 3);
+        double prev = 0., cur = 0., x = 0.;
+        if (i < nh) {
+            x = mup[nh + i];
+            const size_t o = (((size_t) it.lt * 4 + f) * nh + i) * 2;
+            prev = ckpt[C.ck_off + o];
+            cur = ckpt[C.ck_off + o + 1];
+        }
+        // warp-uniform function: one specialised chain each
+        if (f == 0) gsf_tile_chain<0>(af, rcs, x, prev, cur, l0, i < nh ? lt : 0);
+        else if (f == 1) gsf_tile_chain<1>(af, rcs, x, prev, cur, l0, i < nh ? lt : 0);
+        else if (f == 2) gsf_tile_chain<2>(af, rcs, x, prev, cur, l0, i < nh ? lt : 0);
+        else gsf_tile_chain<3>(af, rcs, x, prev, cur, l0, i < nh ? lt : 0);
+    }
+    // weighted moments of the node pairs, folded for either order parity
+    // (s = (-1)^l multiplies the mirror node's terms), into the fragment of
+    // each (function slot, output): slot 0 p00 (m0, m5), 1 p2+2 (m2, m3),
+    // 2 p2-2 (m1, m4), 3 p0+2 (m6, m7); column n = 2 col + output
+    // (columns past ncol are left as they are: they only reach outputs that
+    // are not kept; node pairs past the case's angles get zeros)
+    for (int t = threadIdx.x; t < ncol * EX_AT; t += blockDim.x) {
+        const int col = t / EX_AT, ia = t % EX_AT, i = i0 + ia;
+        double u0 = 0., u1 = 0., u2 = 0., u3 = 0., v0 = 0., v1 = 0., v2 = 0., v3 = 0.;
+        if (i < nh) {
+            const int i1 = nh - 1 - i, i2 = nh + i;
+            const double w = wqp[i2];
+            const double *F = pfn + C.pf_off + (size_t) col * 4 * nq;
+            u0 = F[i1] * w; u1 = F[nq + i1] * w; u2 = F[2 * nq + i1] * w; u3 = F[3 * nq + i1] * w;
+            v0 = F[i2] * w; v1 = F[nq + i2] * w; v2 = F[2 * nq + i2] * w; v3 = F[3 * nq + i2] * w;
+        }
+        const int ks = ia >> 2, k = ia & 3;
+#pragma unroll
+        for (int par = 0; par < 2; ++par) {
+            const double sg = par ? -1. : 1.;
+            const double m[8] = {sg * u0 + v0, sg * (u0 + u1), v0 + v1, sg * (u0 - u1),
+                                 v0 - v1,      sg * u1 + v1,   sg * u2 + v2, sg * u3 + v3};
+            // (slot, output) -> moment
+            const int mom[4][2] = {{0, 5}, {2, 3}, {1, 4}, {6, 7}};
+#pragma unroll
+            for (int slot = 0; slot < 4; ++slot)
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    const int n = 2 * col + j, nb = n >> 3, nl = n & 7;
+                    Bf[(((par * 4 + slot) * nbn + nb) * EX_KS + ks) * EX_SEG + (nl << 2) + k] = m[mom[slot][j]];
+                }
+        }
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int par = warp & 1, mb = warp >> 1;
+    double acc[3][EX_NB][2];
+#pragma unroll
+    for (int g = 0; g < 3; ++g)
+#pragma unroll
+        for (int nb = 0; nb < EX_NB; ++nb) acc[g][nb][0] = acc[g][nb][1] = 0.;
+    const double *a0 = Af + ((0 * 2 + par) * 2 + mb) * EX_KS * EX_SEG + lane;   // function 0 (p00)
+    constexpr int AF = 2 * 2 * EX_KS * EX_SEG;                                   // stride of a function
+    const double *b0 = Bf + (size_t) par * 4 * nbn * EX_KS * EX_SEG + lane;
+    const int BS = nbn * EX_KS * EX_SEG;                                          // stride of a slot
+#pragma unroll 2
+    for (int ks = 0; ks < EX_KS; ++ks) {
+        const double a00 = a0[ks * EX_SEG], a02 = a0[AF + ks * EX_SEG];
+        const double a22 = a0[2 * AF + ks * EX_SEG], a2m = a0[3 * AF + ks * EX_SEG];
+#pragma unroll
+        for (int nb = 0; nb < EX_NB; ++nb) {
+            if (nb >= nbn) break;
+            const double *bb = b0 + (nb * EX_KS + ks) * EX_SEG;
+            dmma(acc[0][nb][0], acc[0][nb][1], a00, bb[0]);
+            dmma(acc[1][nb][0], acc[1][nb][1], a22, bb[BS]);
+            dmma(acc[1][nb][0], acc[1][nb][1], a2m, bb[2 * BS]);
+            dmma(acc[2][nb][0], acc[2][nb][1], a02, bb[3 * BS]);
+        }
+    }
+    __syncthreads();
+    // accumulators: row m = lane >> 2 (order), columns 2 (lane & 3) + {0, 1}:
+    // one column, its two outputs; staged as [col][6][EX_LT] in Af's space
+    double *S = Af;
+    {
+        const int u = par + 2 * (8 * mb + (lane >> 2));
+#pragma unroll
+        for (int nb = 0; nb < EX_NB; ++nb) {
+            if (nb >= nbn) break;
+            const int col = 4 * nb + (lane & 3);
+            if (col < ncol) {
+                double *sc = S + (size_t) col * 6 * EX_LT + u;
+                sc[0 * EX_LT] = acc[0][nb][0];
+                sc[3 * EX_LT] = acc[0][nb][1];
+                sc[1 * EX_LT] = acc[1][nb][0];
+                sc[2 * EX_LT] = acc[1][nb][1];
+                sc[4 * EX_LT] = acc[2][nb][0];
+                sc[5 * EX_LT] = acc[2][nb][1];
+            }
+        }
+    }
+    __syncthreads();
+    double *out = exq + C.ex_off + (size_t) it.at * ncol * 6 * ncf;
+    for (int t = threadIdx.x; t < ncol * 6 * lt; t += blockDim.x) {
+        const int ce = t / lt, u = t - ce * lt;
+        out[(size_t) ce * ncf + l0 + u] = S[(size_t) ce * EX_LT + u];
+    }
+}
+
 template <int KIND>
 __global__ void __launch_bounds__(EX_TMAX) k_exp_tile(DevBatch B, const ExpItem *__restrict__ items,
                                                    const double *__restrict__ pfn,
@@ -994,8 +1178,9 @@ __global__ void __launch_bounds__(EX_TMAX) k_exp_tile(DevBatch B, const ExpItem 
                 cur = v;
                 Pf[u * (EX_AT + 1)] = v;
             }
+            for (int u = lt; u < EX_LT; ++u) Pf[u * (EX_AT + 1)] = 0.;
         } else {
-            for (int u = 0; u < lt; ++u) Pf[u * (EX_AT + 1)] = 0.;
+            for (int u = 0; u < EX_LT; ++u) Pf[u * (EX_AT + 1)] = 0.;
         }
     }
     // weighted moments of the node pairs (u* at the mirror node -mu_i, v* at
@@ -1288,8 +1473,20 @@ int run_expand(cudaStream_t s, const DevBatch &B, long long nck, const long long
     }
     k_exp_ckpt<KIND><<<ceil_div(nck, 128), 128, 0, s>>>(B, nck, ck_start, ckpt);
     LMIEB_CUDA_TRY(cudaGetLastError());
-    const int nt = std::min(EX_TMAX, std::max(128, ((1 + B.nd) * EX_LT + 31) / 32 * 32));
-    k_exp_tile<KIND><<<nitems, nt, sm, s>>>(B, items, pfn, ckpt, exq);
+    const int ncol = 1 + B.nd;
+    if (KIND == 0 && 2 * ncol <= 8 * EX_NB) {
+        // the GSF contraction on the FP64 tensor cores
+        const size_t smm = sizeof(double) * ((size_t) EX_AF + ex_bf_size(ncol) + (size_t) 8 * EX_LT);
+        static bool attr_mma = false;
+        if (!attr_mma) {
+            LMIEB_CUDA_TRY(cudaFuncSetAttribute(k_exp_tile_gsf, cudaFuncAttributeMaxDynamicSharedMemorySize, SMAX));
+            attr_mma = true;
+        }
+        if (nitems > 0) k_exp_tile_gsf<<<nitems, 128, smm, s>>>(B, items, pfn, ckpt, exq);
+    } else {
+        const int nt = std::min(EX_TMAX, std::max(128, (ncol * EX_LT + 31) / 32 * 32));
+        k_exp_tile<KIND><<<nitems, nt, sm, s>>>(B, items, pfn, ckpt, exq);
+    }
     LMIEB_CUDA_TRY(cudaGetLastError());
     k_exp_final<KIND><<<ceil_div(nfin, 256), 256, 0, s>>>(B, nfin, fin_start, exq, coefs, trunc, band);
     LMIEB_CUDA_TRY(cudaGetLastError());
