@@ -90,9 +90,10 @@ struct Ctx {
     int device = -1;
     int sms = 0;
     cudaStream_t stream = nullptr;
-    Slot slot[2];
+    Slot slot[3];                   // two alternating slots; the third runs the FP64 re-solves
     int last_slot = -1;             // slot of the last submitted sub-batch
     long long next_ticket = 0;
+    long long redo_ticket = 1LL << 62;   // tickets of the re-solve slot (their own range)
     int submits = 0;                // sub-batches submitted since the counters were reset
     int call_slot[2] = {-1, -1};    // slots of the first two sub-batches since then
     long long redo = 0;             // INT8 cases solved again in FP64 since then
@@ -1666,6 +1667,34 @@ int collect_slot(Slot &S) {
             fprintf(stderr, "ERROR: lmie_b200: a tensor-core angular stage timed out waiting for its pipeline\n");
         return -1;
     }
+    // Cases whose truncation the int8 contraction's error could have moved
+    // are solved again in FP64.  They go to the re-solve slot now, so that
+    // the device runs them while the host unpacks this sub-batch; their
+    // results replace these cases' when they are collected below.
+    std::vector<int> redo;
+    std::vector<lmieb_problem> rq;
+    std::vector<lmieb_result> rr;
+    lmieb_result *const rs_keep = P.rs;
+    int redo_early = 0;
+    uncertain_truncations(P, htr, redo);
+    if (!redo.empty()) {
+        for (int k : redo) {
+            rq.push_back(P.ps[k]);
+            rq.back().precision = LMIEB_PRECISION_FP64;
+            rr.push_back(rs_keep[k]);
+        }
+        c.redo += (long long) redo.size();
+        Slot &R3 = c.slot[2];
+        if (!c.timing && !R3.pend.active) {
+            redo_early = fit_sub((int) rq.size(), rq.data());
+            if (c.submits < 2) c.call_slot[c.submits] = 2;
+            ++c.submits;
+            if (submit_sub(R3, c.redo_ticket++, redo_early, rq.data(), rr.data())) {
+                R3.pend.active = false;
+                return -1;
+            }
+        }
+    }
     for (size_t p = 0; p + 1 < P.piece.size(); ++p) {
         if (p > 0) {
             const double tw = now_ms();
@@ -1724,30 +1753,21 @@ int collect_slot(Slot &S) {
         if (r.save1) memcpy(r.save1, hostp(P.o_save1), (size_t) 4 * P.R * 8);
         if (r.save2 && P.n_qang0 > 0) memcpy(r.save2, hostp(P.o_save2), P.n_save2 * 8);
     }
-    std::vector<int> redo;
-    uncertain_truncations(P, htr, redo);
     c.host_ms[3] += now_ms() - t_unpack - waited;
     if (!redo.empty()) {
-        // the uncertain cases again in FP64, into the same results (the slot's
-        // staging is no longer read, so the re-solve may reuse it)
-        // (P may be reused by the re-solve's sub-batch: keep what is needed)
-        lmieb_result *const rs = P.rs;
-        std::vector<lmieb_problem> q;
-        std::vector<lmieb_result> r;
-        for (int k : redo) {
-            q.push_back(P.ps[k]);
-            q.back().precision = LMIEB_PRECISION_FP64;
-            r.push_back(rs[k]);
-        }
-        c.redo += (long long) redo.size();
-        for (int k0 = 0; k0 < (int) q.size();) {
-            const int m = fit_sub((int) q.size() - k0, q.data() + k0);
-            const long long t = submit_locked(m, q.data() + k0, r.data() + k0);
+        // the re-solve submitted above, then any cases left over (more than
+        // one sub-batch, or timing mode) one sub-batch at a time; the slot's
+        // staging is no longer read, so these may reuse it (P too: what is
+        // needed was kept)
+        if (redo_early > 0 && collect_slot(c.slot[2])) return -1;
+        for (int k0 = redo_early; k0 < (int) rq.size();) {
+            const int m = fit_sub((int) rq.size() - k0, rq.data() + k0);
+            const long long t = submit_locked(m, rq.data() + k0, rr.data() + k0);
             if (t < 0 || collect_ticket(t)) return -1;
             k0 += m;
         }
         // the arrays went straight to the callers' storage; the counts come back here
-        for (size_t i = 0; i < redo.size(); ++i) rs[redo[i]].n_coef_out = r[i].n_coef_out;
+        for (size_t i = 0; i < redo.size(); ++i) rs_keep[redo[i]].n_coef_out = rr[i].n_coef_out;
     }
     return 0;
 }
