@@ -294,6 +294,9 @@ struct Plan {
     long long *bcorr = nullptr; // its bias terms of the digit combination
     long long *rx_start = nullptr;   // (case, half-angle) index space of the row exponents
     long long n_rx = 0;
+    unsigned char *aop = nullptr;    // its A operand digits, every (case, angle tile, chunk)
+    long long *a_start = nullptr;    // (case, tile row) index space of the A operand
+    long long n_arow = 0;
     int n_groups = 0;
     ExpItem *ex = nullptr;
     int n_ex = 0;
@@ -473,8 +476,8 @@ int run_accumulate(Plan &L, cudaStream_t s) {
             launch_angular_tc(s, B, L.n_ang, L.ang, L.bop, L.part, L.tc_seg, L.o_trunc + 2 * L.ncase))
             return -1;
         if (L.oz && L.n_ang > 0) {
-            if (launch_oz_operands(s, B, L.n_rx, L.rx_start, L.rowexp, L.n_groups, L.coef, L.bop8, L.colexp,
-                                   L.bcorr))
+            if (launch_oz_operands(s, B, L.n_rx, L.rx_start, L.rowexp, L.n_arow, L.a_start, L.aop, L.n_groups,
+                                   L.coef, L.bop8, L.colexp, L.bcorr))
                 return -1;
             if (g_ctx.timing) LMIEB_CUDA_TRY(cudaEventRecord(g_ctx.k3[0], s));
             if (launch_angular_oz(s, B, L.n_ang, L.ang, L.bop8, L.part, L.o_trunc + 2 * L.ncase)) return -1;
@@ -668,6 +671,7 @@ size_t case_bytes(const lmieb_problem &p) {
         b += (size_t) (tot + (size_t) p.n * OZ_KC) * OZ_BSTAGE / (OZ_KC * oz_rg(std::min(p.nd1, OZ_MAX_NC1)));
         b += (size_t) (p.n_qang / 2 + 1) * (tot / std::max(p.n, 1) / OZ_KC + 2) * 2;
         b += (size_t) p.n * (1 + p.nd1) * 16;                          // exponents K1 tracks
+        b += (size_t) ((p.n_qang / 2 + OZ_HALF - 1) / OZ_HALF) * ((p.n1 + OZ_KC - 1) / OZ_KC) * OZ_ACHUNK;   // A operand
     }
     return b;
 }
@@ -990,9 +994,9 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     }
     // int8 fixed point: radius groups of oz_rg(nd1) radii, each with its B
     // operand digits; row-exponent tables per case
-    long long bop8_bytes = 0, rx_bytes = 0;
+    long long bop8_bytes = 0, rx_bytes = 0, aop_bytes = 0;
     int nkx_all = 0;
-    std::vector<long long> rx_start(ncase + 1, 0);
+    std::vector<long long> rx_start(ncase + 1, 0), a_start(ncase + 1, 0);
     if (L.oz) {
         const int RG = oz_rg(nd1);
         std::vector<int> cg0(ncase + 1, 0);
@@ -1002,12 +1006,18 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
             DevCase &C = cs[k];
             cg0[k] = (int) tg_r0.size();
             rx_start[k + 1] = rx_start[k];
+            a_start[k + 1] = a_start[k];
             if (!case_oz[k]) continue;
             C.nkx = (cn1max[k] + OZ_KC - 1) / OZ_KC;
             C.rx_off = rx_bytes;
             C.trunc_band = C.accuracy > 0. ? oz_trunc_band(cn1max[k]) : 0.;
             rx_bytes += (long long) C.nh * C.nkx * 2;
             rx_start[k + 1] += C.nh;
+            // the A operand of each angle tile and chunk
+            const int ntile = (C.nh + OZ_HALF - 1) / OZ_HALF;
+            C.a_off = aop_bytes;
+            aop_bytes += (long long) ntile * C.nkx * OZ_ACHUNK;
+            a_start[k + 1] += (long long) ntile * OZ_M;
             nkx_all = std::max(nkx_all, C.nkx);
             for (int r = C.r0; r < C.r0 + C.nr; r += RG) {
                 const int n = std::min(RG, C.r0 + C.nr - r);
@@ -1026,6 +1036,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         cg0[ncase] = (int) tg_r0.size();
         L.n_groups = (int) tg_r0.size();
         L.n_rx = rx_start[ncase];
+        L.n_arow = a_start[ncase];
         const double wt = std::max(W / (g_items_per_sm[2] * c.sms), 8.);    // chunks per item
         std::vector<std::pair<double, AngItem>> tmp;
         for (int k = 0; k < ncase; ++k) {
@@ -1245,6 +1256,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         add(ang.size() * sizeof(AngItem)); add(ang64.size() * sizeof(AngItem)); add(ex.size() * sizeof(ExpItem));
         add(tc_pos.size() * 4); add(tc_roff.size() * 8); add(tg_r0.size() * 4); add(tg_n.size() * 4);
         add(tg_nk.size() * 4); add(tg_off.size() * 8); add(oz_f2.size() * 8); add(rx_start.size() * 8);
+        add(a_start.size() * 8);
         for (int q = 0; q < 5; ++q) add((size_t) (ncase + 1) * 8);
         add((size_t) ncase * 4); add((size_t) (ncase + 1) * 8);             // K1 launch order
         add(gl_ns.size() * 4); add(gl_mo.size() * 8); add(gl_go.size() * 8); add(gl_pt.size() * 4);
@@ -1294,6 +1306,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     long long *h_tgoff = put(hp, ho, tg_off.data(), tg_off.size());
     double *h_ozf2 = put(hp, ho, oz_f2.data(), oz_f2.size());
     long long *h_rxs = put(hp, ho, rx_start.data(), rx_start.size());
+    long long *h_axs = put(hp, ho, a_start.data(), a_start.size());
     long long *h_pfs = put(hp, ho, pf_start.data(), pf_start.size());
     long long *h_ckg = put(hp, ho, ck_gc.data(), ck_gc.size());
     long long *h_ckl = put(hp, ho, ck_lc.data(), ck_lc.size());
@@ -1343,6 +1356,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
                 add((size_t) L.n_groups * OZ_NP * 4);
                 add((size_t) L.n_groups * OZ_NP * 16);
                 add((size_t) (1 + nd1) * R * 16);
+                add((size_t) aop_bytes);
             }
             add((size_t) (1 + nd1) * (size_t) ctot * 32);
             add((size_t) (1 + nd1) * 5 * (size_t) R * 8);
@@ -1426,6 +1440,9 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
             L.bcorr = A.take<long long>((size_t) L.n_groups * OZ_NP * 2);
             B.oz_bcorr = L.bcorr;
             L.rx_start = (long long *) dptr(h_rxs);
+            L.aop = A.take<unsigned char>((size_t) aop_bytes);
+            L.a_start = (long long *) dptr(h_axs);
+            B.oz_aop = L.aop;
             B.oz_f2 = (const double *) dptr(h_ozf2);
             B.oz_rowexp = L.rowexp;
             B.oz_colexp = L.colexp;
@@ -1456,7 +1473,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         if (L.acc_mode == LMIEB_ACC_PARTIAL) L.o_acc = (double *) take(L.acc_n * 8);
     }
     if (!L.sums || !L.pfn || !L.exq || (solve && !L.part) || (L.tc && !L.bop) ||
-        (L.oz && solve && (!L.bop8 || !L.rowexp || !L.colexp || !L.bcorr))) {
+        (L.oz && solve && (!L.bop8 || !L.rowexp || !L.colexp || !L.bcorr || (aop_bytes && !L.aop)))) {
         fprintf(stderr, "ERROR: lmie_b200: device arena too small\n");
         return -1;
     }

@@ -8,17 +8,19 @@
 //   - k_oz_rowexp: per half-angle, the row exponents g_r of both of its rows
 //     for every chunk count a group of its case can have (running maxima of
 //     |pi +- tau| 2^-e_k along the same recurrence the product kernel runs);
+//   - k_oz_aop: per product row of every angle tile, the pi/tau recurrence
+//     over the case's orders and the row's six digit slices of every chunk
+//     (the A operand is the same for all radius groups of the case);
 //   - k_oz_bop: per radius group, the column exponents f_n and the six digit
 //     slices of the B operand, chunk by chunk, from K1's FP64 coefficient
 //     columns;
 //   - k_angular_oz: a block owns one angle tile of one case and a range of its
 //     radius groups; per group, chunks of OZ_KC orders flow through the
 //     pipeline:
-//       * warps 10-13 (one thread per row) run the pi/tau recurrence in FP64,
-//         scale the row values and extract their digits (one FMA each), and
-//         hand the digit words over in tensor memory, half a chunk at a time;
-//       * warps 0-3 (one thread per row, the row's tensor-memory lane) turn
-//         them into the row's six digit slices of the A stage (two stages);
+//       * warps 0-3 (one thread per row, the row's tensor-memory lane) load
+//         the chunk's A digit slices of their row -- formed once per (case,
+//         angle tile, chunk) by k_oz_aop -- and store them into the A stage
+//         in tensor memory (two stages);
 //       * lane 0 of warp 9 brings the group's B chunks into shared memory with
 //         bulk copies running ahead of the products;
 //       * lane 0 of warp 8 issues the 21 digit products of a chunk,
@@ -30,7 +32,7 @@
 //         lane = row), form C exactly (int64 halves, then FP64) into a
 //         shared-memory buffer and hand the accumulators back, so the next
 //         group's products start;
-//       * warps 14-17 form, from the buffer and while the next group's
+//       * warps 10-13 form, from the buffer and while the next group's
 //         products run, the phase-matrix quadratic forms and their
 //         linearisations per radius (reference src/lmie_core.c:723-790; sm of
 //         a row is in its pair row), accumulated over the block's radii in
@@ -54,35 +56,31 @@
 
 namespace {
 
-constexpr int OZ_T = 576;                     // warps 0-3: A digits, D' sums; 4-7: S sums; 8: products;
-                                              // 9: B copies; 10-13: recurrence; 14-17: quadratic forms
-constexpr int OZ_MMA_WARP = 8, OZ_COPY_WARP = 9, OZ_RECUR_WARP = 10, OZ_QUAD_WARP = 14;
+constexpr int OZ_T = 448;                     // warps 0-3: A stages, D' sums; 4-7: S sums; 8: products;
+                                              // 9: B copies; 10-13: quadratic forms
+constexpr int OZ_MMA_WARP = 8, OZ_COPY_WARP = 9, OZ_QUAD_WARP = 10;
 constexpr int OZ_ASTAGES = 2;                 // A operand stages (tensor memory)
 constexpr int OZ_BSLOTS = 4;                  // B operand slots (bulk copies)
 constexpr int OZ_MAX_GN = OZ_NHALF / 2;       // radii of a group (oz_rg(0))
 constexpr int OZ_MAX_NS = 1 + OZ_MAX_NC1 + OZ_MAX_ND2;
 constexpr uint32_t OZ_ACOLS = OZ_ND * OZ_KC / 4;                 // tensor-memory columns of an A stage
 constexpr uint32_t OZ_ACOL = OZ_ND * OZ_NP;                      // first A stage column
-// barriers: afull[OZ_ASTAGES], adone[OZ_ASTAGES], bfull[OZ_BSLOTS], bdone[OZ_BSLOTS], vfull, vfree,
-// accfull, accfree, qdone, hready[2], hfree[2], fin
-constexpr int OZ_NBAR = 2 * OZ_ASTAGES + 2 * OZ_BSLOTS + 10;
+// barriers: afull[OZ_ASTAGES], adone[OZ_ASTAGES], bfull[OZ_BSLOTS], bdone[OZ_BSLOTS], accfull, accfree,
+// qdone, hready[2], hfree[2], fin
+constexpr int OZ_NBAR = 2 * OZ_ASTAGES + 2 * OZ_BSLOTS + 8;
 constexpr uint32_t OZ_RING = OZ_BSLOTS * OZ_BSTAGE;
 constexpr int OZ_HB = OZ_NP * OZ_M;                         // doubles of one sums buffer
 constexpr uint32_t OZ_HBUF = 2 * OZ_HB * 8;                 // two groups' sums, unscaled, [column][row]
 constexpr uint32_t OZ_WBUF = OZ_MAX_GN * OZ_MAX_NS * 8;     // a group's radius weights
 constexpr uint32_t OZ_CBUF = OZ_NP * 8;                     // a group's column scales
 constexpr uint32_t OZ_KBUF = OZ_NP * 16;                    // a group's bias terms of the combination
-constexpr uint32_t OZ_FBUF = (OZ_KC * OZ_MAX_NK + 8) * 8;   // (k + 1) / k of the case's orders
 // shared-memory offsets
 constexpr uint32_t OZ_O_HBUF = OZ_RING, OZ_O_WBUF = OZ_O_HBUF + OZ_HBUF;
 constexpr uint32_t OZ_O_CBUF = OZ_O_WBUF + OZ_WBUF, OZ_O_KBUF = OZ_O_CBUF + OZ_CBUF;
-constexpr uint32_t OZ_O_FBUF = OZ_O_KBUF + OZ_KBUF, OZ_O_BARS = OZ_O_FBUF + OZ_FBUF;
+constexpr uint32_t OZ_O_BARS = OZ_O_KBUF + OZ_KBUF;
 constexpr uint32_t OZ_SMEM = OZ_O_BARS + OZ_NBAR * 8 + 16;
 constexpr uint32_t OZ_TMEM_COLS = 512;
-// half a chunk of row values (16 doubles per lane) handed from the recurrence
-// warps to the digit warps, after the A stages
-constexpr uint32_t OZ_VCOL = OZ_ACOL + OZ_ASTAGES * OZ_ACOLS;
-static_assert(OZ_VCOL + 32 <= OZ_TMEM_COLS, "row-value columns in tensor memory");
+
 
 static_assert(OZ_BSTAGE % 1024 == 0, "stages stay 1 KB aligned");
 static_assert(OZ_NP % 16 == 0 && OZ_NP >= 16 && OZ_NP <= 256, "N of an M=128 kind::i8 product");
@@ -373,6 +371,64 @@ __device__ __forceinline__ void oz_store_slices(const uint32_t (&dw)[32], int hf
         tmem_st4(acol + sl * (OZ_KC / 4) + hf * 4, w[sl][0], w[sl][1], w[sl][2], w[sl][3]);
 }
 
+// ---------------------------------------------------------------------------
+// A operand: thread per product row of every angle tile of every case (flat
+// index space `start`, OZ_M rows per tile): the pi/tau recurrence over the
+// case's orders; each chunk's row values scaled by 2^(OZ_FRAC - e_k - g_r),
+// g_r the row's exponent over all the case's orders (the largest entry of its
+// table), their digits and the row's six digit slices, OZ_AROW bytes per
+// chunk, to aop[C.a_off + ((tile nkx + chunk) OZ_M + row) OZ_AROW].  Rows past
+// the case's angles get the digits of zero.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_oz_aop(DevBatch B, long long total, const long long *__restrict__ start,
+                                                unsigned char *__restrict__ aop) {
+    const long long e = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= total) return;
+    const int c = find_case(start, B.ncase, e);
+    const DevCase &C = B.cs[c];
+    const long long q = e - start[c];
+    const int t = (int) (q / OZ_M), row = (int) (q % OZ_M);
+    const int h = t * OZ_HALF + (row >> 1), mirror = row & 1;
+    const bool gact = h < C.nh;
+    const double mu = gact ? B.mu_pool[C.mu_off + h] : 0.;
+    const double sg = mirror ? -1. : 1.;
+    const int gr = gact ? (int) B.oz_rowexp[C.rx_off + ((size_t) h * C.nkx + C.nkx - 1) * 2 + mirror] : 0;
+    const double gsc = gact ? oz_pow2(OZ_FRAC - gr) : 0.;
+    uint4 *dst = (uint4 *) (aop + C.a_off + ((size_t) t * C.nkx * OZ_M + row) * OZ_AROW);
+    double p0 = 0., p1 = 1., kmu = mu, k1 = 2.;        // pi_{k-1}, pi_k, k mu, k + 1
+    for (int kc = 0; kc < C.nkx; ++kc) {
+        // the chunk's scale 2^(OZ_FRAC - e_k - g_r); the mirror row carries s_k
+        const double sp = gsc * oz_pow2(-oz_ec(kc));
+        const double sm = mirror ? -sp : sp;
+        uint32_t w[OZ_ND][8];
+#pragma unroll
+        for (int hf = 0; hf < 2; ++hf) {
+            double v[16];
+            oz_recur_half(B.oz_f2 + kc * OZ_KC + hf * 16 + 1, mu, sg, kmu, k1, p0, p1, v);
+            uint32_t dw[32];
+            if (kc == 0 && hf == 0)
+                oz_digit_words<true>(v, 0, sg, sp, sm, gsc, dw);
+            else
+                oz_digit_words<false>(v, hf, sg, sp, sm, gsc, dw);
+#pragma unroll
+            for (int qd = 0; qd < 4; ++qd) {
+                uint32_t s6[OZ_ND];
+                const uint32_t l4[4] = {dw[8 * qd], dw[8 * qd + 2], dw[8 * qd + 4], dw[8 * qd + 6]};
+                const uint32_t h4[4] = {dw[8 * qd + 1], dw[8 * qd + 3], dw[8 * qd + 5], dw[8 * qd + 7]};
+                oz_slices4_biased(l4, h4, s6);
+#pragma unroll
+                for (int sl = 0; sl < OZ_ND; ++sl) w[sl][hf * 4 + qd] = s6[sl];
+            }
+        }
+        uint4 *dc = dst + (size_t) kc * (OZ_ACHUNK / 16);
+#pragma unroll
+        for (int sl = 0; sl < OZ_ND; ++sl) {
+            dc[2 * sl] = make_uint4(w[sl][0], w[sl][1], w[sl][2], w[sl][3]);
+            dc[2 * sl + 1] = make_uint4(w[sl][4], w[sl][5], w[sl][6], w[sl][7]);
+        }
+    }
+}
+
 // barrier 2 over the 128 threads of warps 4-7, OR-reducing v
 __device__ __forceinline__ int oz_epi_sync_or(int v) {
     uint32_t r;
@@ -400,14 +456,12 @@ __global__ void __launch_bounds__(OZ_T, 1) k_angular_oz(DevBatch B, const AngIte
     double *wsh = (double *) (smem + OZ_O_WBUF);             // [OZ_MAX_GN][OZ_MAX_NS] weights
     double *csh = (double *) (smem + OZ_O_CBUF);             // [OZ_NP] column scales
     long long *ksh = (long long *) (smem + OZ_O_KBUF);       // [OZ_NP][2] bias terms
-    double *f2s = (double *) (smem + OZ_O_FBUF);             // [k] (k + 1) / k
     uint64_t *bars = (uint64_t *) (smem + OZ_O_BARS);
     uint32_t *tmem_hold = (uint32_t *) (bars + OZ_NBAR);
     const uint32_t bring = smem_u32(smem);
     const uint32_t afull0 = smem_u32(bars), adone0 = afull0 + 8 * OZ_ASTAGES;
     const uint32_t bfull0 = adone0 + 8 * OZ_ASTAGES, bdone0 = bfull0 + 8 * OZ_BSLOTS;
-    const uint32_t vfull = bdone0 + 8 * OZ_BSLOTS, vfree = vfull + 8;
-    const uint32_t accfull = vfree + 8, accfree = accfull + 8, qdone = accfree + 8;
+    const uint32_t accfull = bdone0 + 8 * OZ_BSLOTS, accfree = accfull + 8, qdone = accfree + 8;
     const uint32_t hready0 = qdone + 8, hfree0 = hready0 + 16, fin = hfree0 + 16;
 
     const int tid = threadIdx.x, warp = tid >> 5;
@@ -430,8 +484,6 @@ __global__ void __launch_bounds__(OZ_T, 1) k_angular_oz(DevBatch B, const AngIte
             mbar_init(bfull0 + 8 * i, 1);
             mbar_init(bdone0 + 8 * i, 1);
         }
-        mbar_init(vfull, OZ_M);
-        mbar_init(vfree, OZ_M);
         mbar_init(accfull, 1);
         mbar_init(accfree, 256);
         mbar_init(qdone, 128);
@@ -443,8 +495,7 @@ __global__ void __launch_bounds__(OZ_T, 1) k_angular_oz(DevBatch B, const AngIte
         fence_mbar_init();
     }
     if (warp == 0) tmem_alloc(smem_u32(tmem_hold), OZ_TMEM_COLS);
-    // (k + 1) / k for the orders of the case's largest group; the first group's bias terms
-    for (int k = tid; k <= C.nkx * OZ_KC; k += OZ_T) f2s[k] = B.oz_f2[k];
+    // the first group's bias terms
     if (tid < 2 * OZ_NP) ksh[tid] = B.oz_bcorr[(size_t) it.rbeg * 2 * OZ_NP + tid];
     tc_fence_before();
     __syncthreads();
@@ -456,6 +507,8 @@ __global__ void __launch_bounds__(OZ_T, 1) k_angular_oz(DevBatch B, const AngIte
         // ---------------- warps 0-3: the A digit slices, one row (lane) per thread ----------------
         const int row = tid;
         const uint32_t tlane = tmem + ((uint32_t) (warp * 32) << 16);
+        // this row's A digit slices: chunk kc of the item's angle tile at arow + kc OZ_ACHUNK
+        const uint4 *arow = (const uint4 *) (B.oz_aop + C.a_off + ((size_t) it.xt * C.nkx * OZ_M + row) * OZ_AROW);
         // The digit warps take the D' columns of a group's finished sums out of
         // tensor memory (warps 4-7 take the S columns): once the quadratic
         // forms are done with the buffer's previous group, after the group's
@@ -491,31 +544,24 @@ __global__ void __launch_bounds__(OZ_T, 1) k_angular_oz(DevBatch B, const AngIte
                 if (q >= OZ_ASTAGES)
                     while (!bad && hold_next < sgrp[s]) bad = take(hold_next++);
                 if (bad) break;
+                // the chunk's digit slices of this row, loaded before the wait
+                const uint4 *ac = arow + (size_t) kc * (OZ_ACHUNK / 16);
+                uint4 a[2 * OZ_ND];
+#pragma unroll
+                for (int i = 0; i < 2 * OZ_ND; ++i) a[i] = ac[i];
                 const bool ok = q < OZ_ASTAGES || mbar_wait(adone0 + 8 * s, ((q / OZ_ASTAGES) - 1) & 1, err);
                 if (__any_sync(0xffffffffu, !ok)) {
                     bad = 1;
                     break;
                 }
+                tc_fence_after();
                 const uint32_t acol = tlane + OZ_ACOL + s * OZ_ACOLS;
-#pragma unroll 1
-                for (int hf = 0; hf < 2 && !bad; ++hf) {
-                    // this half's row values from the recurrence warps
-                    if (__any_sync(0xffffffffu, !mbar_wait(vfull, (2 * q + hf) & 1, err))) {
-                        bad = 1;
-                        break;
-                    }
-                    tc_fence_after();
-                    uint32_t w[32];
-                    tmem_ld16(tlane + OZ_VCOL, *(uint32_t(*)[16]) w);
-                    tmem_ld16(tlane + OZ_VCOL + 16, *(uint32_t(*)[16]) (w + 16));
-                    tmem_wait_ld();
-                    tc_fence_before();
-                    mbar_arrive(vfree);
 #pragma unroll
-                    for (int u = 0; u < 32; ++u) reg_after_wait(w[u]);
-                    oz_store_slices(w, hf, acol);
+                for (int sl = 0; sl < OZ_ND; ++sl) {
+                    tmem_st4(acol + sl * (OZ_KC / 4), a[2 * sl].x, a[2 * sl].y, a[2 * sl].z, a[2 * sl].w);
+                    tmem_st4(acol + sl * (OZ_KC / 4) + 4, a[2 * sl + 1].x, a[2 * sl + 1].y, a[2 * sl + 1].z,
+                             a[2 * sl + 1].w);
                 }
-                if (bad) break;
                 tmem_wait_st();
                 tc_fence_before();
                 sgrp[s] = gi;
@@ -543,7 +589,7 @@ __global__ void __launch_bounds__(OZ_T, 1) k_angular_oz(DevBatch B, const AngIte
             for (int e = 0; e < 4; ++e) racc[s][e] = 0.;
         int gi = 0;
         for (int g = it.rbeg; g < it.rend; ++g, ++gi) {
-            const int gr0 = B.tg_r0[g], gn = B.tg_n[g], nk = B.tg_nk[g];
+            const int gr0 = B.tg_r0[g], gn = B.tg_n[g];
             // the previous group's weights and scales have been read by all four warps
             if (oz_epi_sync_or(bad || gn > OZ_MAX_GN)) {
                 bad = 1;
@@ -557,7 +603,7 @@ __global__ void __launch_bounds__(OZ_T, 1) k_angular_oz(DevBatch B, const AngIte
             // column scales with the row-independent factor of the combination
             if (t1 < OZ_NP) csh[t1] = oz_pow2(B.oz_colexp[(size_t) g * OZ_NP + t1] + OZ_CSHIFT);
             // the scales of this row and of its pair row (which holds this row's sm)
-            const double rsc = oz_pow2(eact ? (int) gtab[2 * (nk - 1)] : 0);
+            const double rsc = oz_pow2(eact ? (int) gtab[2 * (C.nkx - 1)] : 0);
             const double rsp = __shfl_xor_sync(0xffffffffu, rsc, 1);
             oz_epi_sync_or(0);
             // both halves of the group's sums are in its buffer
@@ -627,50 +673,6 @@ __global__ void __launch_bounds__(OZ_T, 1) k_angular_oz(DevBatch B, const AngIte
                 o[(size_t) n_qang] = .25 * (racc[s][0] - racc[s][1]);
                 o[(size_t) 2 * n_qang] = -.5 * racc[s][2];
                 o[(size_t) 3 * n_qang] = .5 * racc[s][3];
-            }
-        }
-    } else if (warp >= OZ_RECUR_WARP) {
-        // ---------------- warps 10-13: the pi/tau recurrence, one row per thread ----------------
-        // row = tensor-memory lane of the warp (its quarter of the lanes)
-        const int row = (warp & 3) * 32 + (tid & 31), h = row >> 1, mirror = row & 1;
-        const uint32_t tlane = tmem + ((uint32_t) ((warp & 3) * 32) << 16);
-        const int gj = it.xt * OZ_HALF + h;
-        const bool gact = gj < nh;
-        const double mu = gact ? B.mu_pool[C.mu_off + gj] : 0.;
-        const signed char *gtab = B.oz_rowexp + C.rx_off + (size_t) (gact ? gj : 0) * C.nkx * 2 + mirror;
-        const double sg = mirror ? -1. : 1.;
-        int hc = 0;                                          // halves handed over
-        for (int g = it.rbeg; g < it.rend && !bad; ++g) {
-            const int nk = B.tg_nk[g];
-            const int gr = gact ? (int) gtab[2 * (nk - 1)] : 0;
-            double p0 = 0., p1 = 1., kmu = mu, k1 = 2.;        // pi_{k-1}, pi_k, k mu, k + 1
-            for (int kc = 0; kc < nk && !bad; ++kc) {
-                // the chunk's scale 2^(OZ_FRAC - e_k - g_r) (0 past the case's angles: zero
-                // digits); the mirror row carries s_k, +1 for odd k, -1 for even k
-                const double gsc = gact ? oz_pow2(OZ_FRAC - gr) : 0.;
-                const double sp = gsc * oz_pow2(-oz_ec(kc));
-                const double sm = mirror ? -sp : sp;
-#pragma unroll 1
-                for (int hf = 0; hf < 2; ++hf, ++hc) {
-                    double v[16];
-                    oz_recur_half(f2s + kc * OZ_KC + hf * 16 + 1, mu, sg, kmu, k1, p0, p1, v);
-                    uint32_t w[32];
-                    if (kc == 0 && hf == 0)
-                        oz_digit_words<true>(v, 0, sg, sp, sm, gsc, w);
-                    else
-                        oz_digit_words<false>(v, hf, sg, sp, sm, gsc, w);
-                    // the digit warps have read the previous half
-                    if (__any_sync(0xffffffffu, !(hc == 0 || mbar_wait(vfree, (hc - 1) & 1, err)))) {
-                        bad = 1;
-                        break;
-                    }
-                    tc_fence_after();
-                    tmem_st16(tlane + OZ_VCOL, *(const uint32_t(*)[16]) w);
-                    tmem_st16(tlane + OZ_VCOL + 16, *(const uint32_t(*)[16]) (w + 16));
-                    tmem_wait_st();
-                    tc_fence_before();
-                    mbar_arrive(vfull);
-                }
             }
         }
     } else if (warp == OZ_COPY_WARP) {
@@ -916,10 +918,14 @@ int launch_oz(cudaStream_t s, const DevBatch &B, int nitems, const AngItem *item
 }  // namespace
 
 int launch_oz_operands(cudaStream_t s, const DevBatch &B, long long nrow, const long long *row_start,
-                       signed char *rowexp, int ngroups, const double *coef, unsigned char *bop, int *colexp,
-                       long long *bcorr) {
+                       signed char *rowexp, long long narow, const long long *arow_start, unsigned char *aop,
+                       int ngroups, const double *coef, unsigned char *bop, int *colexp, long long *bcorr) {
     if (nrow > 0) {
         k_oz_rowexp<<<ceil_div(nrow, 128), 128, 0, s>>>(B, nrow, row_start, rowexp);
+        LMIEB_CUDA_TRY(cudaGetLastError());
+    }
+    if (narow > 0) {
+        k_oz_aop<<<ceil_div(narow, 128), 128, 0, s>>>(B, narow, arow_start, aop);
         LMIEB_CUDA_TRY(cudaGetLastError());
     }
     if (ngroups > 0) {

@@ -37,6 +37,7 @@ struct DevCase {
     int G;                      // angular radius groups
     int nkx;                    // int8 K3: chunks of OZ_KC orders its row exponents cover
     long long rx_off;           // int8 K3: its row exponents ([nh][nkx][2] bytes)
+    long long a_off;            // int8 K3: its A operand digits ([tile][nkx][OZ_M rows][OZ_AROW bytes])
     double trunc_band;          // > 0: K4 records where |beta_l| comes within trunc_band (2l + 1)
                                 // of `accuracy` (band[2c], band[2c + 1]; see launch_expand)
 };
@@ -74,6 +75,7 @@ struct DevBatch {
     const double *oz_f2;        // [OZ_KC * max chunks + 2]: (k + 1) / k
     const signed char *oz_rowexp;   // row exponents (DevCase.rx_off)
     const int *oz_colexp;       // [group][OZ_NP] column exponents
+    const unsigned char *oz_aop;   // A operand digits of every angle tile (DevCase.a_off)
     int *oz_radexp;             // [1 + nd1][R][4]: per radius, coefficient column and component, the
                                 //     largest (biased exponent + e_k) over the orders, 0 if no normal
                                 //     value (written by K1)
@@ -121,7 +123,8 @@ int launch_tc_selftest(cudaStream_t s, int K, const double *A, const double *Bm,
 // group) from K1's FP64 coefficient columns, then the products; items as for
 // launch_angular_tc.  bcorr: [group][OZ_NP][2] terms of the combination.
 int launch_oz_operands(cudaStream_t s, const DevBatch &B, long long nrow, const long long *row_start,
-                       signed char *rowexp, int ngroups, const double *coef, unsigned char *bop, int *colexp,
+                       signed char *rowexp, long long narow, const long long *arow_start, unsigned char *aop,
+                       int ngroups, const double *coef, unsigned char *bop, int *colexp,
                        long long *bcorr);
 int launch_angular_oz(cudaStream_t s, const DevBatch &B, int nitems, const AngItem *items, const unsigned char *bop,
                       double *part, int *err);

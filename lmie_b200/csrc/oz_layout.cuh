@@ -13,8 +13,8 @@
 //     A+ is divided by it and Bop multiplied by it (|pi +- tau| grows like k^2
 //     at the poles, fv4 (a +- b) falls like 1/k), and each row r and column n gets its own
 //     power of two, g_r and f_n, the smallest that bring every value of the
-//     row (orders up to the group's last chunk) or of the column to at most
-//     1/2 in magnitude;
+//     row (all orders of its case) or of the column to at most 1/2 in
+//     magnitude;
 //   - the scaled value x becomes V = round(x 2^47), |V| <= 2^46, written as
 //     six balanced base-256 digits d_0 (most significant) .. d_5 in [-128, 128),
 //     V = sum_i d_i 2^(8 (5 - i)): one int8 slice per digit;
@@ -33,6 +33,13 @@
 // Each product then carries ~2^-46 of the largest term of its row and column
 // (rounding of the two values and the dropped digit products) instead of
 // FP64's 2^-53.
+//
+// The A operand of a chunk of an angle tile is the same for every radius
+// group of its case (the row exponent g_r is taken over all the case's
+// orders): it is formed once per (case, tile, chunk) into memory, product
+// row by product row, OZ_AROW bytes each -- slice s at 32 s, order 4 j + u
+// in byte u of its 32-bit word j -- and the product kernel stores it into
+// tensor memory as it is.
 //
 // Layout of one chunk (OZ_KC orders) of the B operand in memory: OZ_ND
 // slices, slice s holding digit s of every row, each slice in the tensor
@@ -62,6 +69,8 @@ constexpr int OZ_MAX_NC1 = 4;                        // index1 columns the kerne
 constexpr int OZ_MAX_ND2 = 3;                        // index2 slots the kernel is built for
 constexpr int OZ_MAX_NK = 160;                       // chunks per group (5120 orders: int32 sums exact)
 constexpr int OZ_MIN_N1 = 16;                        // smaller cases keep the FP64 angular stage
+constexpr int OZ_AROW = OZ_ND * OZ_KC;               // bytes of one product row of an A chunk (six slices)
+constexpr int OZ_ACHUNK = OZ_M * OZ_AROW;            // bytes of one A chunk of an angle tile
 constexpr int OZ_FRAC = 47;                          // fractional bits of the fixed-point values
 // exponent of the combination's row- and column-independent factor:
 // V_A V_B = 2^80 sum_d 2^(-8 d) ACC_d, and oz_value returns 2^16 of that sum
