@@ -4,7 +4,7 @@
 // The S1/S2 sums over orders (reference src/lmie_core.c:658-721) of one case
 // are the product A+ [S | D'] of 128 rows (64 half-angles of a tile and their
 // mirrors, interleaved) by the OZ_NP operand rows of a radius group, over the
-// orders.  Three kernels:
+// orders.  Four kernels:
 //   - k_oz_rowexp: per half-angle, the row exponents g_r of both of its rows
 //     for every chunk count a group of its case can have (running maxima of
 //     |pi +- tau| 2^-e_k along the same recurrence the product kernel runs);
@@ -353,32 +353,17 @@ __device__ __forceinline__ void oz_digit_words(const double (&v)[16], int hf, do
     }
 }
 
-// The row's six digit slices of half hf of a chunk from its digit words
-// (digit thread), stored to tensor memory at column acol (warp-wide).
-__device__ __forceinline__ void oz_store_slices(const uint32_t (&dw)[32], int hf, uint32_t acol) {
-    uint32_t w[OZ_ND][4];
-#pragma unroll
-    for (int qd = 0; qd < 4; ++qd) {
-        uint32_t s6[OZ_ND];
-        const uint32_t l4[4] = {dw[8 * qd], dw[8 * qd + 2], dw[8 * qd + 4], dw[8 * qd + 6]};
-        const uint32_t h4[4] = {dw[8 * qd + 1], dw[8 * qd + 3], dw[8 * qd + 5], dw[8 * qd + 7]};
-        oz_slices4_biased(l4, h4, s6);
-#pragma unroll
-        for (int sl = 0; sl < OZ_ND; ++sl) w[sl][qd] = s6[sl];
-    }
-#pragma unroll
-    for (int sl = 0; sl < OZ_ND; ++sl)
-        tmem_st4(acol + sl * (OZ_KC / 4) + hf * 4, w[sl][0], w[sl][1], w[sl][2], w[sl][3]);
-}
-
 // ---------------------------------------------------------------------------
 // A operand: thread per product row of every angle tile of every case (flat
 // index space `start`, OZ_M rows per tile): the pi/tau recurrence over the
 // case's orders; each chunk's row values scaled by 2^(OZ_FRAC - e_k - g_r),
 // g_r the row's exponent over all the case's orders (the largest entry of its
 // table), their digits and the row's six digit slices, OZ_AROW bytes per
-// chunk, to aop[C.a_off + ((tile nkx + chunk) OZ_M + row) OZ_AROW].  Rows past
-// the case's angles get the digits of zero.
+// chunk as OZ_AROW / 16 pieces of 16 bytes, piece i (slice i / 2, orders
+// 16 (i % 2) .. + 15) of the row at aop[C.a_off + (tile nkx + chunk)
+// OZ_ACHUNK + (i OZ_M + row) 16]: the rows of a piece are consecutive, so the
+// product kernel's warps read 512 contiguous bytes per load.  Rows past the
+// case's angles get the digits of zero.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(128) k_oz_aop(DevBatch B, long long total, const long long *__restrict__ start,
                                                 unsigned char *__restrict__ aop) {
@@ -394,7 +379,7 @@ __global__ void __launch_bounds__(128) k_oz_aop(DevBatch B, long long total, con
     const double sg = mirror ? -1. : 1.;
     const int gr = gact ? (int) B.oz_rowexp[C.rx_off + ((size_t) h * C.nkx + C.nkx - 1) * 2 + mirror] : 0;
     const double gsc = gact ? oz_pow2(OZ_FRAC - gr) : 0.;
-    uint4 *dst = (uint4 *) (aop + C.a_off + ((size_t) t * C.nkx * OZ_M + row) * OZ_AROW);
+    uint4 *dst = (uint4 *) (aop + C.a_off + (size_t) t * C.nkx * OZ_ACHUNK) + row;
     double p0 = 0., p1 = 1., kmu = mu, k1 = 2.;        // pi_{k-1}, pi_k, k mu, k + 1
     for (int kc = 0; kc < C.nkx; ++kc) {
         // the chunk's scale 2^(OZ_FRAC - e_k - g_r); the mirror row carries s_k
@@ -423,8 +408,8 @@ __global__ void __launch_bounds__(128) k_oz_aop(DevBatch B, long long total, con
         uint4 *dc = dst + (size_t) kc * (OZ_ACHUNK / 16);
 #pragma unroll
         for (int sl = 0; sl < OZ_ND; ++sl) {
-            dc[2 * sl] = make_uint4(w[sl][0], w[sl][1], w[sl][2], w[sl][3]);
-            dc[2 * sl + 1] = make_uint4(w[sl][4], w[sl][5], w[sl][6], w[sl][7]);
+            dc[(2 * sl) * OZ_M] = make_uint4(w[sl][0], w[sl][1], w[sl][2], w[sl][3]);
+            dc[(2 * sl + 1) * OZ_M] = make_uint4(w[sl][4], w[sl][5], w[sl][6], w[sl][7]);
         }
     }
 }
@@ -507,8 +492,9 @@ __global__ void __launch_bounds__(OZ_T, 1) k_angular_oz(DevBatch B, const AngIte
         // ---------------- warps 0-3: the A digit slices, one row (lane) per thread ----------------
         const int row = tid;
         const uint32_t tlane = tmem + ((uint32_t) (warp * 32) << 16);
-        // this row's A digit slices: chunk kc of the item's angle tile at arow + kc OZ_ACHUNK
-        const uint4 *arow = (const uint4 *) (B.oz_aop + C.a_off + ((size_t) it.xt * C.nkx * OZ_M + row) * OZ_AROW);
+        // this row's A digit slices: piece i of chunk kc of the item's angle
+        // tile at arow[kc OZ_ACHUNK / 16 + i OZ_M]
+        const uint4 *arow = (const uint4 *) (B.oz_aop + C.a_off + (size_t) it.xt * C.nkx * OZ_ACHUNK) + row;
         // The digit warps take the D' columns of a group's finished sums out of
         // tensor memory (warps 4-7 take the S columns): once the quadratic
         // forms are done with the buffer's previous group, after the group's
@@ -548,7 +534,7 @@ __global__ void __launch_bounds__(OZ_T, 1) k_angular_oz(DevBatch B, const AngIte
                 const uint4 *ac = arow + (size_t) kc * (OZ_ACHUNK / 16);
                 uint4 a[2 * OZ_ND];
 #pragma unroll
-                for (int i = 0; i < 2 * OZ_ND; ++i) a[i] = ac[i];
+                for (int i = 0; i < 2 * OZ_ND; ++i) a[i] = ac[i * OZ_M];
                 const bool ok = q < OZ_ASTAGES || mbar_wait(adone0 + 8 * s, ((q / OZ_ASTAGES) - 1) & 1, err);
                 if (__any_sync(0xffffffffu, !ok)) {
                     bad = 1;
@@ -570,7 +556,7 @@ __global__ void __launch_bounds__(OZ_T, 1) k_angular_oz(DevBatch B, const AngIte
         }
         while (!bad && hold_next < it.rend - it.rbeg) bad = take(hold_next++);
     } else if (warp >= OZ_QUAD_WARP) {
-        // ---------------- warps 14-17: quadratic forms, one row per thread ----------------
+        // ---------------- warps 10-13: quadratic forms, one row per thread ----------------
         // A warp whose wait fails keeps taking the barriers of the four warps,
         // which stop together.
         const int t1 = tid - OZ_QUAD_WARP * 32;              // product row

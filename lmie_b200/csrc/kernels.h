@@ -37,7 +37,7 @@ struct DevCase {
     int G;                      // angular radius groups
     int nkx;                    // int8 K3: chunks of OZ_KC orders its row exponents cover
     long long rx_off;           // int8 K3: its row exponents ([nh][nkx][2] bytes)
-    long long a_off;            // int8 K3: its A operand digits ([tile][nkx][OZ_M rows][OZ_AROW bytes])
+    long long a_off;            // int8 K3: its A operand digits ([tile][nkx][OZ_AROW / 16 pieces][OZ_M rows][16 bytes])
     double trunc_band;          // > 0: K4 records where |beta_l| comes within trunc_band (2l + 1)
                                 // of `accuracy` (band[2c], band[2c + 1]; see launch_expand)
 };

@@ -36,10 +36,11 @@
 //
 // The A operand of a chunk of an angle tile is the same for every radius
 // group of its case (the row exponent g_r is taken over all the case's
-// orders): it is formed once per (case, tile, chunk) into memory, product
-// row by product row, OZ_AROW bytes each -- slice s at 32 s, order 4 j + u
-// in byte u of its 32-bit word j -- and the product kernel stores it into
-// tensor memory as it is.
+// orders): it is formed once per (case, tile, chunk) into memory, OZ_AROW
+// bytes per product row -- slice s at 32 s, order 4 j + u in byte u of its
+// 32-bit word j -- kept as 16-byte pieces with the rows of a piece
+// consecutive (piece i of row r at 16 (i OZ_M + r)), and the product kernel
+// stores it into tensor memory as it is.
 //
 // Layout of one chunk (OZ_KC orders) of the B operand in memory: OZ_ND
 // slices, slice s holding digit s of every row, each slice in the tensor
