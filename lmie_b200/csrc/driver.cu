@@ -291,7 +291,6 @@ struct Plan {
     unsigned char *bop8 = nullptr;   // its B operand digits
     signed char *rowexp = nullptr;   // its row exponents
     int *colexp = nullptr;      // its column exponents
-    long long *bcorr = nullptr; // its bias terms of the digit combination
     long long *rx_start = nullptr;   // (case, half-angle) index space of the row exponents
     long long n_rx = 0;
     unsigned char *aop = nullptr;    // its A operand digits, every (case, angle tile, chunk)
@@ -477,7 +476,7 @@ int run_accumulate(Plan &L, cudaStream_t s) {
             return -1;
         if (L.oz && L.n_ang > 0) {
             if (launch_oz_operands(s, B, L.n_rx, L.rx_start, L.rowexp, L.n_arow, L.a_start, L.aop, L.n_groups,
-                                   L.coef, L.bop8, L.colexp, L.bcorr))
+                                   L.coef, L.bop8, L.colexp))
                 return -1;
             if (g_ctx.timing) LMIEB_CUDA_TRY(cudaEventRecord(g_ctx.k3[0], s));
             if (launch_angular_oz(s, B, L.n_ang, L.ang, L.bop8, L.part, L.o_trunc + 2 * L.ncase)) return -1;
@@ -1354,7 +1353,6 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
                 add((size_t) bop8_bytes);
                 add((size_t) rx_bytes);
                 add((size_t) L.n_groups * OZ_NP * 4);
-                add((size_t) L.n_groups * OZ_NP * 16);
                 add((size_t) (1 + nd1) * R * 16);
                 add((size_t) aop_bytes);
             }
@@ -1437,8 +1435,6 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
             L.rowexp = A.take<signed char>((size_t) rx_bytes);
             L.colexp = A.take<int>((size_t) L.n_groups * OZ_NP);
             B.oz_radexp = A.take<int>((size_t) (1 + nd1) * R * 4);
-            L.bcorr = A.take<long long>((size_t) L.n_groups * OZ_NP * 2);
-            B.oz_bcorr = L.bcorr;
             L.rx_start = (long long *) dptr(h_rxs);
             L.aop = A.take<unsigned char>((size_t) aop_bytes);
             L.a_start = (long long *) dptr(h_axs);
@@ -1473,7 +1469,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         if (L.acc_mode == LMIEB_ACC_PARTIAL) L.o_acc = (double *) take(L.acc_n * 8);
     }
     if (!L.sums || !L.pfn || !L.exq || (solve && !L.part) || (L.tc && !L.bop) ||
-        (L.oz && solve && (!L.bop8 || !L.rowexp || !L.colexp || !L.bcorr || (aop_bytes && !L.aop)))) {
+        (L.oz && solve && (!L.bop8 || !L.rowexp || !L.colexp || (aop_bytes && !L.aop)))) {
         fprintf(stderr, "ERROR: lmie_b200: device arena too small\n");
         return -1;
     }

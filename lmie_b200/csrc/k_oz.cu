@@ -66,18 +66,17 @@ constexpr int OZ_MAX_NS = 1 + OZ_MAX_NC1 + OZ_MAX_ND2;
 constexpr uint32_t OZ_ACOLS = OZ_ND * OZ_KC / 4;                 // tensor-memory columns of an A stage
 constexpr uint32_t OZ_ACOL = OZ_ND * OZ_NP;                      // first A stage column
 // barriers: afull[OZ_ASTAGES], adone[OZ_ASTAGES], bfull[OZ_BSLOTS], bdone[OZ_BSLOTS], accfull, accfree,
-// qdone, hready[2], hfree[2], fin
-constexpr int OZ_NBAR = 2 * OZ_ASTAGES + 2 * OZ_BSLOTS + 8;
+// hready[2], hfree[2], fin
+constexpr int OZ_NBAR = 2 * OZ_ASTAGES + 2 * OZ_BSLOTS + 7;
 constexpr uint32_t OZ_RING = OZ_BSLOTS * OZ_BSTAGE;
 constexpr int OZ_HB = OZ_NP * OZ_M;                         // doubles of one sums buffer
 constexpr uint32_t OZ_HBUF = 2 * OZ_HB * 8;                 // two groups' sums, unscaled, [column][row]
 constexpr uint32_t OZ_WBUF = OZ_MAX_GN * OZ_MAX_NS * 8;     // a group's radius weights
 constexpr uint32_t OZ_CBUF = OZ_NP * 8;                     // a group's column scales
-constexpr uint32_t OZ_KBUF = OZ_NP * 16;                    // a group's bias terms of the combination
 // shared-memory offsets
 constexpr uint32_t OZ_O_HBUF = OZ_RING, OZ_O_WBUF = OZ_O_HBUF + OZ_HBUF;
-constexpr uint32_t OZ_O_CBUF = OZ_O_WBUF + OZ_WBUF, OZ_O_KBUF = OZ_O_CBUF + OZ_CBUF;
-constexpr uint32_t OZ_O_BARS = OZ_O_KBUF + OZ_KBUF;
+constexpr uint32_t OZ_O_CBUF = OZ_O_WBUF + OZ_WBUF;
+constexpr uint32_t OZ_O_BARS = OZ_O_CBUF + OZ_CBUF;
 constexpr uint32_t OZ_SMEM = OZ_O_BARS + OZ_NBAR * 8 + 16;
 constexpr uint32_t OZ_TMEM_COLS = 512;
 
@@ -91,9 +90,9 @@ static_assert(OZ_SMEM <= 227 * 1024, "shared memory per block");
 static_assert(OZ_FRAC - 1 <= 8 * OZ_ND - 2, "digit weights: the top digit holds |V| / 2^40 <= 64");
 static_assert(OZ_ND == 6, "oz_combine splits the six diagonals into two int64 halves");
 
-// instruction descriptor of kind::i8: D int32, A unsigned 8-bit, B signed 8-bit, both K-major
+// instruction descriptor of kind::i8: D int32, A and B signed 8-bit, both K-major
 __host__ __device__ constexpr uint32_t idesc_i8(int m, int n) {
-    return (2u << 4) | (0u << 7) | (1u << 10) | ((uint32_t) (n >> 3) << 17) | ((uint32_t) (m >> 4) << 24);
+    return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t) (n >> 3) << 17) | ((uint32_t) (m >> 4) << 24);
 }
 
 // true in one lane of a converged warp (the lowest)
@@ -142,13 +141,12 @@ __device__ __forceinline__ void issue_chunk_i8(uint32_t a0, uint32_t b0, uint32_
 }
 
 // sum_d 2^(-8 d) ACC_d of six int32 accumulators, exactly: U = ACC_0 2^16 +
-// ACC_1 2^8 + ACC_2 - cU and L = ACC_3 2^16 + ACC_4 2^8 + ACC_5 - cL (cU, cL:
-// the same forms of the A-digit bias sums of the column, k_oz_bop) are below
-// 2^48 in magnitude, become doubles exactly (x + 1.5 2^52 read as an integer),
-// and the result is 2^-16 (U + 2^-24 L) with one rounding; times `scale`.
-__device__ __forceinline__ longlong2 oz_halves(const uint32_t (&a)[OZ_ND], long long cU, long long cL) {
-    const long long U = (long long) (int) a[0] * 65536 + (long long) (int) a[1] * 256 + (long long) (int) a[2] - cU;
-    const long long L = (long long) (int) a[3] * 65536 + (long long) (int) a[4] * 256 + (long long) (int) a[5] - cL;
+// ACC_1 2^8 + ACC_2 and L = ACC_3 2^16 + ACC_4 2^8 + ACC_5 are below 2^48 in
+// magnitude, become doubles exactly (x + 1.5 2^52 read as an integer), and
+// the result is 2^-16 (U + 2^-24 L) with one rounding; times `scale`.
+__device__ __forceinline__ longlong2 oz_halves(const uint32_t (&a)[OZ_ND]) {
+    const long long U = (long long) (int) a[0] * 65536 + (long long) (int) a[1] * 256 + (long long) (int) a[2];
+    const long long L = (long long) (int) a[3] * 65536 + (long long) (int) a[4] * 256 + (long long) (int) a[5];
     return make_longlong2(U, L);
 }
 
@@ -161,37 +159,30 @@ __device__ __forceinline__ double oz_unscaled(longlong2 h) {
 
 __device__ __forceinline__ double oz_value(longlong2 h, double scale) { return oz_unscaled(h) * scale; }
 
-__device__ __forceinline__ double oz_combine(const uint32_t (&a)[OZ_ND], long long cU, long long cL, double scale) {
-    return oz_value(oz_halves(a, cU, cL), scale);
+__device__ __forceinline__ double oz_combine(const uint32_t (&a)[OZ_ND], double scale) {
+    return oz_value(oz_halves(a), scale);
 }
 
-// The exact sums of `ncol` columns from c0 on (multiples of 4) of this
-// thread's lane: six accumulators per column from tensor memory (taddr: the
-// lane's column c0 of diagonal 0), bias terms ks[2 c], ks[2 c + 1], unscaled
-// values to hb[c OZ_M] (warp-wide; the bias terms are loaded ahead of the
-// stores, which the compiler could not move them past).
-__device__ __forceinline__ void oz_read_sums(uint32_t taddr, int c0, int ncol, const long long *ks, double *hb) {
+// The exact sums of `ncol` columns (a multiple of 8) of this thread's lane:
+// six accumulators per column from tensor memory (taddr: the lane's first
+// column of diagonal 0), eight columns per wait, unscaled values to
+// hb[c OZ_M] (warp-wide).
+__device__ __forceinline__ void oz_read_sums(uint32_t taddr, int ncol, double *hb) {
 #pragma unroll 1
-    for (int c = c0; c < c0 + ncol; c += 4) {
-        long long kU[4], kL[4];
+    for (int c = 0; c < ncol; c += 8) {
+        uint32_t a[OZ_ND][8];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            kU[i] = ks[2 * (c + i)];
-            kL[i] = ks[2 * (c + i) + 1];
-        }
-        uint32_t a[OZ_ND][4];
-#pragma unroll
-        for (int d = 0; d < OZ_ND; ++d) tmem_ld4(taddr + d * OZ_NP + (c - c0), a[d]);
+        for (int d = 0; d < OZ_ND; ++d) tmem_ld8(taddr + d * OZ_NP + c, a[d]);
         tmem_wait_ld();
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
+        for (int i = 0; i < 8; ++i) {
             uint32_t col[OZ_ND];
 #pragma unroll
             for (int d = 0; d < OZ_ND; ++d) {
                 reg_after_wait(a[d][i]);
                 col[d] = a[d][i];
             }
-            hb[(c + i) * OZ_M] = oz_unscaled(oz_halves(col, kU[i], kL[i]));
+            hb[(c + i) * OZ_M] = oz_unscaled(oz_halves(col));
         }
     }
 }
@@ -231,16 +222,14 @@ __global__ void k_oz_rowexp(DevBatch B, long long total, const long long *__rest
 // n = tid % 64 (S re, S im, ..., then D' re, D' im, ...) and every fourth
 // block of 16 orders.  The column exponent f_n (largest ilogb(|v| 2^e_k) + 2
 // over the column) comes from the exponents K1 tracked while it wrote the
-// coefficients; the kernel writes the digit slices of every chunk and sums
-// the row's digits per slice; rows and orders without a value get zero.
+// coefficients; the kernel writes the digit slices of every chunk; rows and
+// orders without a value get zero.
 // ---------------------------------------------------------------------------
 constexpr int OZ_BOP_T = 256;
 constexpr int OZ_BOP_J = OZ_BOP_T / OZ_NP;            // threads per row
 
 __global__ void __launch_bounds__(OZ_BOP_T) k_oz_bop(DevBatch B, const double *__restrict__ coef,
-                                                      unsigned char *__restrict__ bop, int *__restrict__ colexp,
-                                                      long long *__restrict__ bcorr) {
-    __shared__ int sb[OZ_ND][OZ_NP];                  // sums of each digit slice over the group's orders
+                                                      unsigned char *__restrict__ bop, int *__restrict__ colexp) {
     const int g = blockIdx.x, tid = threadIdx.x;
     const int r0 = B.tg_r0[g], gn = B.tg_n[g], nk = B.tg_nk[g];
     const int C1 = 1 + B.nd1, P = gn * C1;
@@ -250,7 +239,6 @@ __global__ void __launch_bounds__(OZ_BOP_T) k_oz_bop(DevBatch B, const double *_
     const bool real = rp < P, dpart = n >= OZ_NHALF;
     const double *cf = coef + comp;                   // component `comp` of the double4 entries
     const size_t tot = (size_t) B.tot;
-    for (int i = tid; i < OZ_ND * OZ_NP; i += OZ_BOP_T) sb[i / OZ_NP][i % OZ_NP] = 0;
     int n1 = 0, f = 0;
     size_t base = 0;
     if (real) {
@@ -262,9 +250,7 @@ __global__ void __launch_bounds__(OZ_BOP_T) k_oz_bop(DevBatch B, const double *_
         f = m ? max(m - 1021, -900) : 0;
     }
     if (j0 == 0) colexp[(size_t) g * OZ_NP + n] = f;
-    __syncthreads();
     // digits, 16 orders at a time
-    int ds[OZ_ND] = {0, 0, 0, 0, 0, 0};
     unsigned char *rb = bop + B.tg_off[g] + (n >> 3) * 128 + (n & 7) * 16;
     for (int blk = j0; blk < 2 * nk; blk += OZ_BOP_J) {
         uint32_t w[OZ_ND][4];
@@ -281,32 +267,12 @@ __global__ void __launch_bounds__(OZ_BOP_T) k_oz_bop(DevBatch B, const double *_
             uint32_t s6[OZ_ND];
             oz_slices4(lo, hi, s6);
 #pragma unroll
-            for (int s = 0; s < OZ_ND; ++s) {
-                w[s][qd] = s6[s];
-                const uint32_t x = s6[s];
-                ds[s] += (int) (signed char) (x & 0xff) + (int) (signed char) ((x >> 8) & 0xff) +
-                         (int) (signed char) ((x >> 16) & 0xff) + (int) (signed char) (x >> 24);
-            }
+            for (int s = 0; s < OZ_ND; ++s) w[s][qd] = s6[s];
         }
         unsigned char *cb = rb + (size_t) (blk >> 1) * OZ_BSTAGE + (blk & 1) * OZ_LBO_B;
 #pragma unroll
         for (int s = 0; s < OZ_ND; ++s)
             *(uint4 *) (cb + s * OZ_BSLICE) = make_uint4(w[s][0], w[s][1], w[s][2], w[s][3]);
-    }
-#pragma unroll
-    for (int s = 0; s < OZ_ND; ++s)
-        if (ds[s]) atomicAdd(&sb[s][n], ds[s]);
-    __syncthreads();
-    // corrections of the combination: 128 times the sums of the B digits
-    // j <= d, in the two int64 forms of oz_combine
-    if (tid < OZ_NP) {
-        long long cc[OZ_ND], run = 0;
-        for (int d = 0; d < OZ_ND; ++d) {
-            run += sb[d][tid];
-            cc[d] = 128 * run;
-        }
-        bcorr[((size_t) g * OZ_NP + tid) * 2] = cc[0] * 65536 + cc[1] * 256 + cc[2];
-        bcorr[((size_t) g * OZ_NP + tid) * 2 + 1] = cc[3] * 65536 + cc[4] * 256 + cc[5];
     }
 }
 
@@ -400,7 +366,7 @@ __global__ void __launch_bounds__(128) k_oz_aop(DevBatch B, long long total, con
                 uint32_t s6[OZ_ND];
                 const uint32_t l4[4] = {dw[8 * qd], dw[8 * qd + 2], dw[8 * qd + 4], dw[8 * qd + 6]};
                 const uint32_t h4[4] = {dw[8 * qd + 1], dw[8 * qd + 3], dw[8 * qd + 5], dw[8 * qd + 7]};
-                oz_slices4_biased(l4, h4, s6);
+                oz_slices4(l4, h4, s6);
 #pragma unroll
                 for (int sl = 0; sl < OZ_ND; ++sl) w[sl][hf * 4 + qd] = s6[sl];
             }
@@ -440,14 +406,13 @@ __global__ void __launch_bounds__(OZ_T, 1) k_angular_oz(DevBatch B, const AngIte
     double *hbuf = (double *) (smem + OZ_O_HBUF);            // [2][OZ_NP][OZ_M] sums of a group, unscaled
     double *wsh = (double *) (smem + OZ_O_WBUF);             // [OZ_MAX_GN][OZ_MAX_NS] weights
     double *csh = (double *) (smem + OZ_O_CBUF);             // [OZ_NP] column scales
-    long long *ksh = (long long *) (smem + OZ_O_KBUF);       // [OZ_NP][2] bias terms
     uint64_t *bars = (uint64_t *) (smem + OZ_O_BARS);
     uint32_t *tmem_hold = (uint32_t *) (bars + OZ_NBAR);
     const uint32_t bring = smem_u32(smem);
     const uint32_t afull0 = smem_u32(bars), adone0 = afull0 + 8 * OZ_ASTAGES;
     const uint32_t bfull0 = adone0 + 8 * OZ_ASTAGES, bdone0 = bfull0 + 8 * OZ_BSLOTS;
-    const uint32_t accfull = bdone0 + 8 * OZ_BSLOTS, accfree = accfull + 8, qdone = accfree + 8;
-    const uint32_t hready0 = qdone + 8, hfree0 = hready0 + 16, fin = hfree0 + 16;
+    const uint32_t accfull = bdone0 + 8 * OZ_BSLOTS, accfree = accfull + 8;
+    const uint32_t hready0 = accfree + 8, hfree0 = hready0 + 16, fin = hfree0 + 16;
 
     const int tid = threadIdx.x, warp = tid >> 5;
     const AngItem it = items[blockIdx.x];
@@ -471,7 +436,6 @@ __global__ void __launch_bounds__(OZ_T, 1) k_angular_oz(DevBatch B, const AngIte
         }
         mbar_init(accfull, 1);
         mbar_init(accfree, 256);
-        mbar_init(qdone, 128);
         for (int i = 0; i < 2; ++i) {
             mbar_init(hready0 + 8 * i, 256);
             mbar_init(hfree0 + 8 * i, 128);
@@ -480,8 +444,6 @@ __global__ void __launch_bounds__(OZ_T, 1) k_angular_oz(DevBatch B, const AngIte
         fence_mbar_init();
     }
     if (warp == 0) tmem_alloc(smem_u32(tmem_hold), OZ_TMEM_COLS);
-    // the first group's bias terms
-    if (tid < 2 * OZ_NP) ksh[tid] = B.oz_bcorr[(size_t) it.rbeg * 2 * OZ_NP + tid];
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
@@ -501,16 +463,14 @@ __global__ void __launch_bounds__(OZ_T, 1) k_angular_oz(DevBatch B, const AngIte
         // last products.  Returns nonzero when a wait gave up.
         auto take = [&](int gh) -> int {
             const int g = it.rbeg + gh, ncol = B.tg_n[g] * CPR;
-            // the bias terms of the group are staged, the buffer's previous
-            // group (gh - 2) has been through the quadratic forms
+            // the buffer's previous group (gh - 2) has been through the quadratic forms
             const int b = gh & 1;
-            bool ok = gh == 0 || mbar_wait(qdone, (gh - 1) & 1, err);
-            ok = ok && (gh < 2 || mbar_wait(hfree0 + 8 * b, ((gh >> 1) - 1) & 1, err));
+            bool ok = gh < 2 || mbar_wait(hfree0 + 8 * b, ((gh >> 1) - 1) & 1, err);
             ok = ok && mbar_wait(accfull, gh & 1, err);
             double *hb = hbuf + b * OZ_HB;
             if (__any_sync(0xffffffffu, !ok)) return 1;
             tc_fence_after();
-            oz_read_sums(tlane + OZ_NHALF, OZ_NHALF, (ncol + 3) & ~3, ksh, hb + row);
+            oz_read_sums(tlane + OZ_NHALF, (ncol + 7) & ~7, hb + OZ_NHALF * OZ_M + row);
             tc_fence_before();
             mbar_arrive(accfree);
             mbar_arrive(hready0 + 8 * b);
@@ -573,24 +533,38 @@ __global__ void __launch_bounds__(OZ_T, 1) k_angular_oz(DevBatch B, const AngIte
         for (int s = 0; s < 1 + NC1 + OZ_MAX_ND2; ++s)
 #pragma unroll
             for (int e = 0; e < 4; ++e) racc[s][e] = 0.;
+        // the scales of this row and of its pair row (which holds this row's sm)
+        const double rsc = oz_pow2(eact ? (int) gtab[2 * (C.nkx - 1)] : 0);
+        const double rsp = __shfl_xor_sync(0xffffffffu, rsc, 1);
+        // A group's radius weights (gn NS <= OZ_MAX_GN OZ_MAX_NS = 128 values:
+        // at most one per thread) and column scales (with the row-independent
+        // factor of the combination), fetched into registers one group ahead
+        // so that their loads overlap the previous group's forms.
+        double wnext = 0., cnext = 0.;
+        auto fetch = [&](int g) {
+            const int gn = B.tg_n[g];
+            if (t1 < gn * NS && gn <= OZ_MAX_GN) {
+                const int p = t1 / NS, s = t1 - p * NS;
+                const int slot = s == 0 ? 0 : (s <= NC1 ? slot1[s - 1] : 1 + B.idx2[s - 1 - NC1]);
+                wnext = B.w[(size_t) slot * R + B.tg_r0[g] + p];
+            }
+            if (t1 < OZ_NP) cnext = oz_pow2(B.oz_colexp[(size_t) g * OZ_NP + t1] + OZ_CSHIFT);
+        };
+        if (it.rbeg < it.rend) fetch(it.rbeg);
         int gi = 0;
         for (int g = it.rbeg; g < it.rend; ++g, ++gi) {
-            const int gr0 = B.tg_r0[g], gn = B.tg_n[g];
+            const int gn = B.tg_n[g];
             // the previous group's weights and scales have been read by all four warps
             if (oz_epi_sync_or(bad || gn > OZ_MAX_GN)) {
                 bad = 1;
                 break;
             }
-            for (int i = t1; i < gn * NS; i += 128) {
-                const int p = i / NS, s = i - p * NS;
-                const int slot = s == 0 ? 0 : (s <= NC1 ? slot1[s - 1] : 1 + B.idx2[s - 1 - NC1]);
-                wsh[p * OZ_MAX_NS + s] = B.w[(size_t) slot * R + gr0 + p];
+            if (t1 < gn * NS) {
+                const int p = t1 / NS;
+                wsh[p * OZ_MAX_NS + (t1 - p * NS)] = wnext;
             }
-            // column scales with the row-independent factor of the combination
-            if (t1 < OZ_NP) csh[t1] = oz_pow2(B.oz_colexp[(size_t) g * OZ_NP + t1] + OZ_CSHIFT);
-            // the scales of this row and of its pair row (which holds this row's sm)
-            const double rsc = oz_pow2(eact ? (int) gtab[2 * (C.nkx - 1)] : 0);
-            const double rsp = __shfl_xor_sync(0xffffffffu, rsc, 1);
+            if (t1 < OZ_NP) csh[t1] = cnext;
+            if (g + 1 < it.rend) fetch(g + 1);
             oz_epi_sync_or(0);
             // both halves of the group's sums are in its buffer
             const double *hb = hbuf + (gi & 1) * OZ_HB;
@@ -722,13 +696,11 @@ __global__ void __launch_bounds__(OZ_T, 1) k_angular_oz(DevBatch B, const AngIte
         int gi = 0;
         for (int g = it.rbeg; g < it.rend && !bad; ++g, ++gi) {
             const int ncol = B.tg_n[g] * CPR;                 // used columns of each half
-            // every reader has staged its bias terms of this group, the
-            // buffer's previous group has been through the quadratic forms,
-            // and this group's products are done (warp-uniform: the
+            // the buffer's previous group has been through the quadratic
+            // forms and this group's products are done (warp-uniform: the
             // tensor-memory accesses below are warp-wide)
             const int b = gi & 1;
-            bool ok = gi == 0 || mbar_wait(qdone, (gi - 1) & 1, err);
-            ok = ok && (gi < 2 || mbar_wait(hfree0 + 8 * b, ((gi >> 1) - 1) & 1, err));
+            bool ok = gi < 2 || mbar_wait(hfree0 + 8 * b, ((gi >> 1) - 1) & 1, err);
             ok = ok && mbar_wait(accfull, gi & 1, err);
             double *hb = hbuf + b * OZ_HB;
             if (__any_sync(0xffffffffu, !ok)) {
@@ -739,18 +711,10 @@ __global__ void __launch_bounds__(OZ_T, 1) k_angular_oz(DevBatch B, const AngIte
             // the exact sums of the group's used S columns into the buffer
             // (the digit warps take the D' columns); the accumulators go back
             // right after
-            oz_read_sums(trow, 0, (ncol + 3) & ~3, ksh, hb + t1);
+            oz_read_sums(trow, (ncol + 7) & ~7, hb + t1);
             tc_fence_before();
             mbar_arrive(accfree);
             mbar_arrive(hready0 + 8 * b);
-            // once both halves are out (the digit warps no longer read the bias
-            // terms), the next group's bias terms
-            if (__any_sync(0xffffffffu, !mbar_wait(accfree, gi & 1, err))) {
-                bad = 1;
-                break;
-            }
-            if (g + 1 < it.rend) ksh[t1] = B.oz_bcorr[(size_t) (g + 1) * 2 * OZ_NP + t1];
-            mbar_arrive(qdone);
         }
     }
     if (bad) atomicExch(err, 1);
@@ -781,8 +745,6 @@ __global__ void __launch_bounds__(128, 1) k_oz_selftest(int K, const double *__r
     uint64_t *bars = (uint64_t *) (smem + OZ_BSTAGE);
     uint32_t *tmem_hold = (uint32_t *) (bars + 2);
     __shared__ int fB[OZ_NP];
-    __shared__ long long kB[OZ_NP][2];          // bias terms of the combination per column
-    long long sbs[OZ_ND] = {0, 0, 0, 0, 0, 0}; // this thread's B row: sums of its digits
     const uint32_t b0 = smem_u32(smem), done = smem_u32(bars);
     const int tid = threadIdx.x, warp = tid >> 5;
     if (tid == 0) {
@@ -820,12 +782,11 @@ __global__ void __launch_bounds__(128, 1) k_oz_selftest(int K, const double *__r
                     oz_digits(Bm[(size_t) n * K + k], oz_pow2(OZ_FRAC + ek - fB[n]), lb[u], hb[u]);
                 }
                 uint32_t s6[OZ_ND], t6[OZ_ND];
-                oz_slices4_biased(lo, hi, s6);
+                oz_slices4(lo, hi, s6);
                 oz_slices4(lb, hb, t6);
                 for (int s = 0; s < OZ_ND; ++s) {
                     wa[s][qd] = s6[s];
                     wb[s][qd] = t6[s];
-                    for (int u = 0; u < 4; ++u) sbs[s] += (signed char) ((t6[s] >> (8 * u)) & 0xff);
                 }
             }
             for (int s = 0; s < OZ_ND; ++s)
@@ -850,16 +811,6 @@ __global__ void __launch_bounds__(128, 1) k_oz_selftest(int K, const double *__r
         bad = __syncthreads_or(lbad);
         tc_fence_after();
     }
-    if (tid < OZ_NP) {
-        long long c[OZ_ND], run = 0;
-        for (int d = 0; d < OZ_ND; ++d) {
-            run += sbs[d];
-            c[d] = 128 * run;
-        }
-        kB[tid][0] = c[0] * 65536 + c[1] * 256 + c[2];
-        kB[tid][1] = c[3] * 65536 + c[4] * 256 + c[5];
-    }
-    __syncthreads();
     if (!bad) {
         const uint32_t trow = tmem + ((uint32_t) (warp * 32) << 16);
         for (int c = 0; c < OZ_NP; c += 16) {
@@ -873,7 +824,7 @@ __global__ void __launch_bounds__(128, 1) k_oz_selftest(int K, const double *__r
                     col[d] = a[d][i];
                 }
                 D[(size_t) tid * OZ_NP + c + i] =
-                    oz_combine(col, kB[c + i][0], kB[c + i][1], oz_pow2(gA + fB[c + i] + OZ_CSHIFT));
+                    oz_combine(col, oz_pow2(gA + fB[c + i] + OZ_CSHIFT));
             }
         }
     } else if (tid == 0) {
@@ -905,7 +856,7 @@ int launch_oz(cudaStream_t s, const DevBatch &B, int nitems, const AngItem *item
 
 int launch_oz_operands(cudaStream_t s, const DevBatch &B, long long nrow, const long long *row_start,
                        signed char *rowexp, long long narow, const long long *arow_start, unsigned char *aop,
-                       int ngroups, const double *coef, unsigned char *bop, int *colexp, long long *bcorr) {
+                       int ngroups, const double *coef, unsigned char *bop, int *colexp) {
     if (nrow > 0) {
         k_oz_rowexp<<<ceil_div(nrow, 128), 128, 0, s>>>(B, nrow, row_start, rowexp);
         LMIEB_CUDA_TRY(cudaGetLastError());
@@ -915,7 +866,7 @@ int launch_oz_operands(cudaStream_t s, const DevBatch &B, long long nrow, const 
         LMIEB_CUDA_TRY(cudaGetLastError());
     }
     if (ngroups > 0) {
-        k_oz_bop<<<ngroups, OZ_BOP_T, 0, s>>>(B, coef, bop, colexp, bcorr);
+        k_oz_bop<<<ngroups, OZ_BOP_T, 0, s>>>(B, coef, bop, colexp);
         LMIEB_CUDA_TRY(cudaGetLastError());
     }
     return 0;

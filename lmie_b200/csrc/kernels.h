@@ -79,7 +79,6 @@ struct DevBatch {
     int *oz_radexp;             // [1 + nd1][R][4]: per radius, coefficient column and component, the
                                 //     largest (biased exponent + e_k) over the orders, 0 if no normal
                                 //     value (written by K1)
-    const long long *oz_bcorr;  // [group][OZ_NP][2] bias terms of the digit combination
 };
 
 // Coefficient columns: column 0 = value, column 1+k = index1 slot k.  Entry
@@ -119,13 +118,13 @@ int launch_angular_tc(cudaStream_t s, const DevBatch &B, int nitems, const AngIt
 int launch_tc_selftest(cudaStream_t s, int K, const double *A, const double *Bm, double *D, int *err);
 // K3 as an exact fixed-point contraction on the int8 tensor cores (k_oz.cu):
 // the row exponents (thread per (case, half-angle) of the flat index space
-// row_start) and the B operand digits and column exponents (block per radius
-// group) from K1's FP64 coefficient columns, then the products; items as for
-// launch_angular_tc.  bcorr: [group][OZ_NP][2] terms of the combination.
+// row_start), the A operand digits (thread per product row of every angle
+// tile, arow_start) and the B operand digits and column exponents (block per
+// radius group) from K1's FP64 coefficient columns, then the products; items
+// as for launch_angular_tc.
 int launch_oz_operands(cudaStream_t s, const DevBatch &B, long long nrow, const long long *row_start,
                        signed char *rowexp, long long narow, const long long *arow_start, unsigned char *aop,
-                       int ngroups, const double *coef, unsigned char *bop, int *colexp,
-                       long long *bcorr);
+                       int ngroups, const double *coef, unsigned char *bop, int *colexp);
 int launch_angular_oz(cudaStream_t s, const DevBatch &B, int nitems, const AngItem *items, const unsigned char *bop,
                       double *part, int *err);
 // D[128 x OZ_NP] = A[128 x K] B[OZ_NP x K]^T through the same fixed-point path

@@ -22,12 +22,8 @@
 //     the 21 products with i + j < 6 are summed by tcgen05.mma kind::i8 into
 //     six int32 accumulators, one per diagonal i + j; the dropped products
 //     (i + j >= 6) are below 2^-46 of the largest term each;
-//   - B digits are signed bytes; A digits are stored as the unsigned bytes
-//     d + 128 (no conversion after the extraction below), so diagonal d also
-//     sums 128 times the B digits j <= d over the group's orders, which the
-//     combination removes with the column's digit sums (exact: every int32
-//     sum stays below 6 * 255 * 128 * 5120 < 2^31 for groups of up to 5120
-//     orders);
+//   - A and B digits are signed bytes; every int32 sum is exact (below
+//     6 * 128 * 128 * 5120 < 2^31 for groups of up to 5120 orders);
 //   - C = 2^(g_r + f_n - 14) sum_d 2^(-8 d) ACC_d, formed exactly in int64
 //     halves and FP64.
 // Each product then carries ~2^-46 of the largest term of its row and column
@@ -141,15 +137,6 @@ __device__ __forceinline__ void oz_t4(uint32_t w0, uint32_t w1, uint32_t w2, uin
     b1 = __byte_perm(t0, t1, 0x7632);
     b2 = __byte_perm(t2, t3, 0x5410);
     b3 = __byte_perm(t2, t3, 0x7632);
-}
-
-// Digit slices of four consecutive orders of one row: w[s] holds digit s of
-// the four orders (byte u = order u) as the unsigned byte d + 128.
-__device__ __forceinline__ void oz_slices4_biased(const uint32_t (&lo)[4], const uint32_t (&hi)[4],
-                                                  uint32_t (&w)[OZ_ND]) {
-    uint32_t x2, x3;
-    oz_t4(lo[0], lo[1], lo[2], lo[3], w[5], w[4], w[3], w[2]);
-    oz_t4(hi[0], hi[1], hi[2], hi[3], w[1], w[0], x2, x3);
 }
 
 // Digit slices of four consecutive orders of one row: w[s] holds digit s of
