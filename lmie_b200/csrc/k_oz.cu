@@ -564,22 +564,27 @@ __global__ void __launch_bounds__(OZ_T, 1) k_angular_oz(DevBatch B, const AngIte
                 wsh[p * OZ_MAX_NS + (t1 - p * NS)] = wnext;
             }
             if (t1 < OZ_NP) csh[t1] = cnext;
-            if (g + 1 < it.rend) fetch(g + 1);
             oz_epi_sync_or(0);
+            // the next group's loads, in flight during this group's forms (a
+            // barrier waits for the loads issued before it)
+            if (g + 1 < it.rend) fetch(g + 1);
             // both halves of the group's sums are in its buffer
             const double *hb = hbuf + (gi & 1) * OZ_HB;
             if (__any_sync(0xffffffffu, !mbar_wait(hready0 + 8 * (gi & 1), (gi >> 1) & 1, err))) {
                 bad = 1;
                 continue;
             }
+            // The row scales are left out here: every term of racc[s][0] carries
+            // rsc^2, of racc[s][1] rsp^2 and of racc[s][2..3] rsc rsp (powers of
+            // two, applied once at the end).
             for (int p = 0; p < gn; ++p) {
                 // columns of S (i < CPR, this row) and D' (i >= CPR, the pair row: sm)
                 double v[2 * CPR];
 #pragma unroll
                 for (int i = 0; i < CPR; ++i) {
                     const int cs = p * CPR + i, cd = OZ_NHALF + p * CPR + i;
-                    v[i] = hb[cs * OZ_M + t1] * (rsc * csh[cs]);
-                    v[CPR + i] = hb[cd * OZ_M + (t1 ^ 1)] * (rsp * csh[cd]);
+                    v[i] = hb[cs * OZ_M + t1] * csh[cs];
+                    v[CPR + i] = hb[cd * OZ_M + (t1 ^ 1)] * csh[cd];
                 }
                 const double *wp = wsh + p * OZ_MAX_NS;
                 const double f = wp[0];
@@ -620,19 +625,22 @@ __global__ void __launch_bounds__(OZ_T, 1) k_angular_oz(DevBatch B, const AngIte
         }
         if (oz_epi_sync_or(bad)) bad = 1;
         if (!bad && eact) {
-            // phase-matrix elements: ((A + B) / 4, (A - B) / 4, -C / 2, D / 2)
+            // phase-matrix elements: ((A + B) / 4, (A - B) / 4, -C / 2, D / 2),
+            // with the row scales
             const int jj = emir ? n_qang - 1 - ej : ej;
             const int Q = 4 * (1 + B.nd);
             double *pc = part + C.part_off + (size_t) it.g * Q * n_qang;
+            const double ss = rsc * rsc, mm = rsp * rsp, sm = rsc * rsp;
 #pragma unroll
             for (int s = 0; s < 1 + NC1 + OZ_MAX_ND2; ++s) {
                 if (s >= NS) break;
                 const int slot = s == 0 ? 0 : (s <= NC1 ? slot1[s - 1] : 1 + B.idx2[s - 1 - NC1]);
                 double *o = pc + (size_t) slot * 4 * n_qang + jj;
-                o[0] = .25 * (racc[s][0] + racc[s][1]);
-                o[(size_t) n_qang] = .25 * (racc[s][0] - racc[s][1]);
-                o[(size_t) 2 * n_qang] = -.5 * racc[s][2];
-                o[(size_t) 3 * n_qang] = .5 * racc[s][3];
+                const double a = racc[s][0] * ss, b = racc[s][1] * mm;
+                o[0] = .25 * (a + b);
+                o[(size_t) n_qang] = .25 * (a - b);
+                o[(size_t) 2 * n_qang] = -.5 * (racc[s][2] * sm);
+                o[(size_t) 3 * n_qang] = .5 * (racc[s][3] * sm);
             }
         }
     } else if (warp == OZ_COPY_WARP) {
