@@ -299,6 +299,8 @@ struct Plan {
     int n_groups = 0;
     ExpItem *ex = nullptr;
     int n_ex = 0;
+    ExpItem *gx = nullptr;      // (case, 0, angle tile) of the GSF expansion runs, longest first
+    int n_gx = 0;
     long long *pf_start = nullptr, *ck_gc = nullptr, *ck_lc = nullptr, *fin_start = nullptr, *pu_start = nullptr;
     long long pf_total = 0, nck_gc = 0, nck_lc = 0, nfin = 0, pu_total = 0;
     double *save1_in = nullptr, *save2_in = nullptr, *w2 = nullptr;
@@ -509,12 +511,12 @@ int run_finish(Plan &L, cudaStream_t s) {
     LMIEB_CUDA_TRY(cudaMemsetAsync(L.o_trunc, 0, sizeof(int) * 2 * L.ncase, s));
     LMIEB_CUDA_TRY(cudaMemsetAsync(L.o_trunc + 2 * L.ncase + 1, 0, sizeof(int) * 4 * L.ncase, s));
     stage(5);
-    if (L.want_gc && launch_expand(s, B, 0, L.nck_gc, L.ck_gc, L.n_ex, L.ex, L.nfin, L.fin_start, L.pfn,
-                                   L.ckpt, L.exq, L.o_gc, L.o_trunc, L.o_trunc + 2 * L.ncase + 1))
+    if (L.want_gc && launch_expand(s, B, 0, L.nck_gc, L.ck_gc, L.n_ex, L.ex, L.n_gx, L.gx, L.nfin, L.fin_start,
+                                   L.pfn, L.ckpt, L.exq, L.o_gc, L.o_trunc, L.o_trunc + 2 * L.ncase + 1))
         return -1;
     stage(6);
-    if (L.want_lc && launch_expand(s, B, 1, L.nck_lc, L.ck_lc, L.n_ex, L.ex, L.nfin, L.fin_start, L.pfn,
-                                   L.ckpt, L.exq, L.o_lc, L.o_trunc + L.ncase, L.o_trunc + 4 * L.ncase + 1))
+    if (L.want_lc && launch_expand(s, B, 1, L.nck_lc, L.ck_lc, L.n_ex, L.ex, 0, nullptr, L.nfin, L.fin_start,
+                                   L.pfn, L.ckpt, L.exq, L.o_lc, L.o_trunc + L.ncase, L.o_trunc + 4 * L.ncase + 1))
         return -1;
     stage(7);
     if (L.pf_from) {
@@ -1145,10 +1147,25 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         for (int lt = 0; lt < nlt; ++lt)
             for (int at = 0; at < nat; ++at) *e++ = ExpItem{k, lt, at};
     });
+    // the GSF expansion runs one block per (case, angle tile) over all the
+    // case's orders: cases with the most orders first
+    static std::vector<ExpItem> gx;
+    gx.clear();
+    if (L.want_gc) {
+        std::vector<int> byn(ncase);
+        for (int k = 0; k < ncase; ++k) byn[k] = k;
+        std::stable_sort(byn.begin(), byn.end(), [&](int a, int b) { return cs[a].n_coef > cs[b].n_coef; });
+        for (int k : byn) {
+            int nlt, nat;
+            if (!ex_tiles(cs[k], nlt, nat) || nlt == 0) continue;
+            for (int at = 0; at < nat; ++at) gx.push_back(ExpItem{k, 0, at});
+        }
+    }
     L.nck_gc = ck_gc[ncase];
     L.nck_lc = ck_lc[ncase];
     L.nfin = fin_start[ncase];
     L.n_ex = (int) ex.size();
+    L.n_gx = (int) gx.size();
 
     // ---- user angles and output offsets ----
     // the user angles depend only on their number: one copy per distinct count
@@ -1198,7 +1215,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         }
         if (finish) {
             nl += 1 + (L.pf_total > 0);                                          // normalisation
-            if (L.want_gc && L.n_ex > 0) nl += 3;
+            if (L.want_gc && L.n_ex > 0) nl += 1 + expand_gsf_launches(ncol);
             if (L.want_lc && L.n_ex > 0) nl += 3;
             if (L.pf_from && L.pu_total > 0) nl += 1;
         }
@@ -1253,6 +1270,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         add(fv.size() * 8); add(rc.size() * 8); add(ml.size() * 16); add(laml.size() * 8);
         add((size_t) nd1 * 4); add((size_t) nd2 * 4); add(mu_user.size() * 8);
         add(ang.size() * sizeof(AngItem)); add(ang64.size() * sizeof(AngItem)); add(ex.size() * sizeof(ExpItem));
+        add(gx.size() * sizeof(ExpItem));
         add(tc_pos.size() * 4); add(tc_roff.size() * 8); add(tg_r0.size() * 4); add(tg_n.size() * 4);
         add(tg_nk.size() * 4); add(tg_off.size() * 8); add(oz_f2.size() * 8); add(rx_start.size() * 8);
         add(a_start.size() * 8);
@@ -1297,6 +1315,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     AngItem *h_ang = put(hp, ho, ang.data(), ang.size());
     AngItem *h_ang64 = put(hp, ho, ang64.data(), ang64.size());
     ExpItem *h_ex = put(hp, ho, ex.data(), ex.size());
+    ExpItem *h_gx = put(hp, ho, gx.data(), gx.size());
     int *h_tcpos = put(hp, ho, tc_pos.data(), tc_pos.size());
     long long *h_tcroff = put(hp, ho, tc_roff.data(), tc_roff.size());
     int *h_tgr0 = put(hp, ho, tg_r0.data(), tg_r0.size());
@@ -1413,6 +1432,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     L.ang = (AngItem *) dptr(h_ang);
     L.ang64 = (AngItem *) dptr(h_ang64);
     L.ex = (ExpItem *) dptr(h_ex);
+    L.gx = (ExpItem *) dptr(h_gx);
     L.pf_start = (long long *) dptr(h_pfs);
     L.ck_gc = (long long *) dptr(h_ckg);
     L.ck_lc = (long long *) dptr(h_ckl);

@@ -966,17 +966,19 @@ __device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b)
 }
 
 // ---------------------------------------------------------------------------
-// K4b of the GSF expansion on the FP64 tensor cores: one block of 4 warps per
-// (case, order tile, angle tile).  For each order parity the 16 orders of
-// that parity form an M = 16 product over K = the tile's EX_AT node pairs:
-// the basis functions against the folded moments of that parity.  Each
-// function feeds two outputs per column (N = 2 ncol): p00 -> (e0: m0, e3: m5),
-// p0+2 -> (e4: m6, e5: m7), p2+2 -> (e1: m2, e2: m3) and p2-2 -> (e1: m1,
-// e2: m4), the last two into the same accumulators (the sums of the FP64
-// kernel, k_exp_tile<0>, in another order).  Basis and moments are staged in
-// the m8n8k4 fragment order, so every operand load of a warp reads 32
-// consecutive doubles.  Warp w takes parity w & 1 and the orders
-// 8 (w >> 1) .. + 7 of it.
+// K4 of the GSF expansion on the FP64 tensor cores (k_exp_gsf): one block of
+// 4 warps per (case, angle tile) runs over all the case's orders, a tile of
+// EX_LT orders at a time.  Thread (function f, node pair ia) continues its
+// basis recurrence from tile to tile in registers (no checkpoints), writing
+// the tile's values into shared memory; the weighted phase-matrix moments of
+// the block's node pairs are staged once; the recurrence coefficients of the
+// next tile are loaded while the current one's are used.  For each order
+// parity the 16 orders of that parity form an M = 16 product over K = the
+// EX_AT node pairs (mma.sync m8n8k4 f64), the basis functions against the
+// folded moments of that parity, whose raw sums go to exq per angle tile
+// (the sums of the FP64 kernel, k_exp_tile<0>, in another order).  Basis and
+// moments are staged in the m8n8k4 fragment order, so every operand load of
+// a warp reads 32 consecutive doubles.
 // ---------------------------------------------------------------------------
 constexpr int EX_NB = 4;                 // n-blocks of 8 outputs: up to 16 columns
 constexpr int EX_KS = EX_AT / 4;         // k-steps of 4 node pairs
@@ -986,15 +988,13 @@ constexpr int EX_KS = EX_AT / 4;         // k-steps of 4 node pairs
 constexpr int EX_SEG = 36;
 constexpr int EX_AF = 4 * 2 * 2 * EX_KS * EX_SEG;   // basis fragments: [f][parity][m-block][k-step]
 
-// doubles of the moment fragments: [parity][4 function slots][n-block][k-step]
-__host__ __device__ inline int ex_bf_size(int ncol) { return 2 * 4 * ((2 * ncol + 7) / 8) * EX_KS * EX_SEG; }
-
 // GSF function F of one node pair over the orders of a tile (u < lt, zeros
 // after), into its fragment positions (order u = par + 2 m: block par,
-// m >> 3, row m & 7); the recurrence coefficients' loads of the fully
-// unrolled steps do not depend on the chain and go ahead of it.
+// m >> 3, row m & 7), continuing the chain (prev, cur) from the previous
+// tile; the recurrence coefficients' loads of the fully unrolled steps do not
+// depend on the chain and go ahead of it.
 template <int F>
-__device__ __forceinline__ void gsf_tile_chain(double *af, const double *rcs, double x, double prev, double cur,
+__device__ __forceinline__ void gsf_tile_chain(double *af, const double *rcs, double x, double &prev, double &cur,
                                                int l0, int lt) {
     if (lt == EX_LT && l0 >= 3) {
 #pragma unroll
@@ -1018,47 +1018,32 @@ __device__ __forceinline__ void gsf_tile_chain(double *af, const double *rcs, do
     }
 }
 
-__global__ void __launch_bounds__(128) k_exp_tile_gsf(DevBatch B, const ExpItem *__restrict__ items,
-                                                     const double *__restrict__ pfn,
-                                                     const double *__restrict__ ckpt, double *__restrict__ exq) {
+// doubles between the k-steps of the moment fragments (staged once per
+// block: no padding)
+constexpr int EX_BSEG = 32;
+
+__host__ __device__ inline int ex_bf_run_size(int ncol) { return 2 * 4 * ((2 * ncol + 7) / 8) * EX_KS * EX_BSEG; }
+
+__global__ void __launch_bounds__(128) k_exp_gsf(DevBatch B, const ExpItem *__restrict__ items,
+                                                const double *__restrict__ pfn, double *__restrict__ exq) {
     extern __shared__ double sm[];
     const ExpItem it = items[blockIdx.x];
     const DevCase &C = B.cs[it.c];
     const int nh = C.nh, nq = C.n_qang, ncf = C.n_coef;
     const int ncol = 1 + B.nd, nbn = (2 * ncol + 7) >> 3;
-    const int l0 = it.lt * EX_LT, lt = min(EX_LT, ncf - l0);
     const int i0 = it.at * EX_AT;
     const double *mup = B.mu_pool + C.mu_off, *wqp = mup + nq;
-    double *Af = sm;                                       // basis fragments
-    double *Bf = Af + EX_AF;                               // moment fragments
-    double *rcs = Bf + ex_bf_size(ncol);                   // [8 EX_LT] recurrence coefficients
-    for (int t = threadIdx.x; t < 8 * lt; t += blockDim.x) rcs[t] = B.rc[8 * (size_t) l0 + t];
-    __syncthreads();
-    // basis functions of the tile, thread per (function, node pair): order
-    // u = par + 2 (8 mb + m) is row m of block (par, mb); node pair ia is
-    // column ia & 3 of k-step ia >> 2
-    {
-        const int f = threadIdx.x >> 5, ia = threadIdx.x & 31, i = i0 + ia;
-        double *af = Af + (size_t) f * (2 * 2 * EX_KS * EX_SEG) + (ia >> 2) * EX_SEG + (ia & 3);
-        double prev = 0., cur = 0., x = 0.;
-        if (i < nh) {
-            x = mup[nh + i];
-            const size_t o = (((size_t) it.lt * 4 + f) * nh + i) * 2;
-            prev = ckpt[C.ck_off + o];
-            cur = ckpt[C.ck_off + o + 1];
-        }
-        // warp-uniform function: one specialised chain each
-        if (f == 0) gsf_tile_chain<0>(af, rcs, x, prev, cur, l0, i < nh ? lt : 0);
-        else if (f == 1) gsf_tile_chain<1>(af, rcs, x, prev, cur, l0, i < nh ? lt : 0);
-        else if (f == 2) gsf_tile_chain<2>(af, rcs, x, prev, cur, l0, i < nh ? lt : 0);
-        else gsf_tile_chain<3>(af, rcs, x, prev, cur, l0, i < nh ? lt : 0);
-    }
+    double *Af = sm;                                       // basis fragments of the current tile
+    double *Bf = Af + EX_AF;                               // moment fragments of the block's node pairs
+    double *rcs = Bf + ex_bf_run_size(ncol);               // [2][8 EX_LT] recurrence coefficients of a tile
     // weighted moments of the node pairs, folded for either order parity
     // (s = (-1)^l multiplies the mirror node's terms), into the fragment of
     // each (function slot, output): slot 0 p00 (m0, m5), 1 p2+2 (m2, m3),
-    // 2 p2-2 (m1, m4), 3 p0+2 (m6, m7); column n = 2 col + output
-    // (columns past ncol are left as they are: they only reach outputs that
-    // are not kept; node pairs past the case's angles get zeros)
+    // 2 p2-2 (m1, m4), 3 p0+2 (m6, m7); column n = 2 col + output (columns
+    // past ncol only reach outputs that are not kept: zeros; node pairs past
+    // the case's angles get zeros)
+    for (int t = threadIdx.x; t < 8 * nbn * EX_KS * EX_BSEG; t += blockDim.x) Bf[t] = 0.;
+    __syncthreads();
     for (int t = threadIdx.x; t < ncol * EX_AT; t += blockDim.x) {
         const int col = t / EX_AT, ia = t % EX_AT, i = i0 + ia;
         double u0 = 0., u1 = 0., u2 = 0., u3 = 0., v0 = 0., v1 = 0., v2 = 0., v3 = 0.;
@@ -1082,62 +1067,96 @@ __global__ void __launch_bounds__(128) k_exp_tile_gsf(DevBatch B, const ExpItem 
 #pragma unroll
                 for (int j = 0; j < 2; ++j) {
                     const int n = 2 * col + j, nb = n >> 3, nl = n & 7;
-                    Bf[(((par * 4 + slot) * nbn + nb) * EX_KS + ks) * EX_SEG + (nl << 2) + k] = m[mom[slot][j]];
+                    Bf[(((par * 4 + slot) * nbn + nb) * EX_KS + ks) * EX_BSEG + (nl << 2) + k] = m[mom[slot][j]];
                 }
         }
     }
+    // the chain of this thread: function f at node pair ia, from order 0
+    const int f = threadIdx.x >> 5, ia = threadIdx.x & 31, i = i0 + ia;
+    double *af = Af + (size_t) f * (2 * 2 * EX_KS * EX_SEG) + (ia >> 2) * EX_SEG + (ia & 3);
+    const double x = i < nh ? mup[nh + i] : 0.;
+    double prev = 0., cur = 0.;
+    // the first tile's recurrence coefficients
+    const int nlt = (ncf + EX_LT - 1) / EX_LT;
+    for (int t = threadIdx.x; t < 8 * min(EX_LT, ncf); t += blockDim.x) rcs[t] = B.rc[t];
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int par = warp & 1, mb = warp >> 1;
-    double acc[3][EX_NB][2];
-#pragma unroll
-    for (int g = 0; g < 3; ++g)
-#pragma unroll
-        for (int nb = 0; nb < EX_NB; ++nb) acc[g][nb][0] = acc[g][nb][1] = 0.;
     const double *a0 = Af + ((0 * 2 + par) * 2 + mb) * EX_KS * EX_SEG + lane;   // function 0 (p00)
     constexpr int AF = 2 * 2 * EX_KS * EX_SEG;                                   // stride of a function
-    const double *b0 = Bf + (size_t) par * 4 * nbn * EX_KS * EX_SEG + lane;
-    const int BS = nbn * EX_KS * EX_SEG;                                          // stride of a slot
-#pragma unroll 2
-    for (int ks = 0; ks < EX_KS; ++ks) {
-        const double a00 = a0[ks * EX_SEG], a02 = a0[AF + ks * EX_SEG];
-        const double a22 = a0[2 * AF + ks * EX_SEG], a2m = a0[3 * AF + ks * EX_SEG];
-#pragma unroll
-        for (int nb = 0; nb < EX_NB; ++nb) {
-            if (nb >= nbn) break;
-            const double *bb = b0 + (nb * EX_KS + ks) * EX_SEG;
-            dmma(acc[0][nb][0], acc[0][nb][1], a00, bb[0]);
-            dmma(acc[1][nb][0], acc[1][nb][1], a22, bb[BS]);
-            dmma(acc[1][nb][0], acc[1][nb][1], a2m, bb[2 * BS]);
-            dmma(acc[2][nb][0], acc[2][nb][1], a02, bb[3 * BS]);
+    const double *b0 = Bf + (size_t) par * 4 * nbn * EX_KS * EX_BSEG + lane;
+    const int BS = nbn * EX_KS * EX_BSEG;                                         // stride of a slot
+    double *out = exq + C.ex_off + (size_t) it.at * ncol * 6 * ncf;
+    for (int lt = 0; lt < nlt; ++lt) {
+        const int l0 = lt * EX_LT, lc = min(EX_LT, ncf - l0);
+        const double *rc = rcs + (lt & 1) * 8 * EX_LT;
+        // the next tile's coefficients, loaded now and stored after the chain
+        const int l1 = l0 + EX_LT, lc1 = min(EX_LT, ncf - l1);
+        const int t0 = threadIdx.x, t1 = threadIdx.x + 128;
+        double r0 = 0., r1 = 0.;
+        if (lc1 > 0) {
+            if (t0 < 8 * lc1) r0 = B.rc[8 * (size_t) l1 + t0];
+            if (t1 < 8 * lc1) r1 = B.rc[8 * (size_t) l1 + t1];
         }
-    }
-    __syncthreads();
-    // accumulators: row m = lane >> 2 (order), columns 2 (lane & 3) + {0, 1}:
-    // one column, its two outputs; staged as [col][6][EX_LT] in Af's space
-    double *S = Af;
-    {
-        const int u = par + 2 * (8 * mb + (lane >> 2));
+        // basis functions of the tile (warp-uniform function: one specialised chain each)
+        const int lct = i < nh ? lc : 0;
+        if (f == 0) gsf_tile_chain<0>(af, rc, x, prev, cur, l0, lct);
+        else if (f == 1) gsf_tile_chain<1>(af, rc, x, prev, cur, l0, lct);
+        else if (f == 2) gsf_tile_chain<2>(af, rc, x, prev, cur, l0, lct);
+        else gsf_tile_chain<3>(af, rc, x, prev, cur, l0, lct);
+        if (lc1 > 0) {
+            double *rn = rcs + ((lt + 1) & 1) * 8 * EX_LT;
+            if (t0 < 8 * lc1) rn[t0] = r0;
+            if (t1 < 8 * lc1) rn[t1] = r1;
+        }
+        __syncthreads();
+        // For each order parity the 16 orders of that parity form an M = 16
+        // product over K = the tile's EX_AT node pairs: the basis functions
+        // against the folded moments of that parity.  Each function feeds
+        // two outputs per column (N = 2 ncol): p00 -> (e0: m0, e3: m5), p0+2
+        // -> (e4: m6, e5: m7), p2+2 -> (e1: m2, e2: m3) and p2-2 -> (e1: m1,
+        // e2: m4), the last two into the same accumulators.  Warp w takes
+        // parity w & 1 and the orders 8 (w >> 1) .. + 7 of it.
+        double acc[3][EX_NB][2];
 #pragma unroll
-        for (int nb = 0; nb < EX_NB; ++nb) {
-            if (nb >= nbn) break;
-            const int col = 4 * nb + (lane & 3);
-            if (col < ncol) {
-                double *sc = S + (size_t) col * 6 * EX_LT + u;
-                sc[0 * EX_LT] = acc[0][nb][0];
-                sc[3 * EX_LT] = acc[0][nb][1];
-                sc[1 * EX_LT] = acc[1][nb][0];
-                sc[2 * EX_LT] = acc[1][nb][1];
-                sc[4 * EX_LT] = acc[2][nb][0];
-                sc[5 * EX_LT] = acc[2][nb][1];
+        for (int g = 0; g < 3; ++g)
+#pragma unroll
+            for (int nb = 0; nb < EX_NB; ++nb) acc[g][nb][0] = acc[g][nb][1] = 0.;
+#pragma unroll 2
+        for (int ks = 0; ks < EX_KS; ++ks) {
+            const double a00 = a0[ks * EX_SEG], a02 = a0[AF + ks * EX_SEG];
+            const double a22 = a0[2 * AF + ks * EX_SEG], a2m = a0[3 * AF + ks * EX_SEG];
+#pragma unroll
+            for (int nb = 0; nb < EX_NB; ++nb) {
+                if (nb >= nbn) break;
+                const double *bb = b0 + (nb * EX_KS + ks) * EX_BSEG;
+                dmma(acc[0][nb][0], acc[0][nb][1], a00, bb[0]);
+                dmma(acc[1][nb][0], acc[1][nb][1], a22, bb[BS]);
+                dmma(acc[1][nb][0], acc[1][nb][1], a2m, bb[2 * BS]);
+                dmma(acc[2][nb][0], acc[2][nb][1], a02, bb[3 * BS]);
             }
         }
-    }
-    __syncthreads();
-    double *out = exq + C.ex_off + (size_t) it.at * ncol * 6 * ncf;
-    for (int t = threadIdx.x; t < ncol * 6 * lt; t += blockDim.x) {
-        const int ce = t / lt, u = t - ce * lt;
-        out[(size_t) ce * ncf + l0 + u] = S[(size_t) ce * EX_LT + u];
+        // accumulators: row m = lane >> 2 (order), columns 2 (lane & 3) + {0, 1}:
+        // one column, its two outputs; raw sums of the angle tile to exq
+        const int u = par + 2 * (8 * mb + (lane >> 2));
+        if (u < lc) {
+#pragma unroll
+            for (int nb = 0; nb < EX_NB; ++nb) {
+                if (nb >= nbn) break;
+                const int col = 4 * nb + (lane & 3);
+                if (col < ncol) {
+                    double *oc = out + (size_t) col * 6 * ncf + l0 + u;
+                    oc[0 * (size_t) ncf] = acc[0][nb][0];
+                    oc[3 * (size_t) ncf] = acc[0][nb][1];
+                    oc[1 * (size_t) ncf] = acc[1][nb][0];
+                    oc[2 * (size_t) ncf] = acc[1][nb][1];
+                    oc[4 * (size_t) ncf] = acc[2][nb][0];
+                    oc[5 * (size_t) ncf] = acc[2][nb][1];
+                }
+            }
+        }
+        // the tile's basis has been read before the next tile's chains overwrite it
+        __syncthreads();
     }
 }
 
@@ -1455,8 +1474,9 @@ int run_angular_nc2(cudaStream_t s, const DevBatch &B, int nc2, int c1base, int 
 
 template <int KIND>
 int run_expand(cudaStream_t s, const DevBatch &B, long long nck, const long long *ck_start,
-               int nitems, const ExpItem *items, long long nfin, const long long *fin_start, const double *pfn,
-               double *ckpt, double *exq, double *coefs, int *trunc, int *band) {
+               int nitems, const ExpItem *items, int nruns, const ExpItem *runs, long long nfin,
+               const long long *fin_start, const double *pfn, double *ckpt, double *exq, double *coefs,
+               int *trunc, int *band) {
     constexpr int NF = KIND == 0 ? 4 : 1;
     constexpr int SMAX = 200 * 1024;
     constexpr int NM = KIND == 0 ? 8 : 6;
@@ -1471,19 +1491,19 @@ int run_expand(cudaStream_t s, const DevBatch &B, long long nck, const long long
         LMIEB_CUDA_TRY(cudaFuncSetAttribute(k_exp_tile<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMAX));
         attr = true;
     }
-    k_exp_ckpt<KIND><<<ceil_div(nck, 128), 128, 0, s>>>(B, nck, ck_start, ckpt);
-    LMIEB_CUDA_TRY(cudaGetLastError());
     const int ncol = 1 + B.nd;
-    if (KIND == 0 && 2 * ncol <= 8 * EX_NB) {
-        // the GSF contraction on the FP64 tensor cores
-        const size_t smm = sizeof(double) * ((size_t) EX_AF + ex_bf_size(ncol) + (size_t) 8 * EX_LT);
+    if (KIND == 0 && expand_gsf_launches(ncol) == 1) {
+        // the GSF contraction on the FP64 tensor cores, one block per (case, angle tile)
+        const size_t smm = sizeof(double) * ((size_t) EX_AF + ex_bf_run_size(ncol) + (size_t) 2 * 8 * EX_LT);
         static bool attr_mma = false;
         if (!attr_mma) {
-            LMIEB_CUDA_TRY(cudaFuncSetAttribute(k_exp_tile_gsf, cudaFuncAttributeMaxDynamicSharedMemorySize, SMAX));
+            LMIEB_CUDA_TRY(cudaFuncSetAttribute(k_exp_gsf, cudaFuncAttributeMaxDynamicSharedMemorySize, SMAX));
             attr_mma = true;
         }
-        if (nitems > 0) k_exp_tile_gsf<<<nitems, 128, smm, s>>>(B, items, pfn, ckpt, exq);
+        if (nruns > 0) k_exp_gsf<<<nruns, 128, smm, s>>>(B, runs, pfn, exq);
     } else {
+        k_exp_ckpt<KIND><<<ceil_div(nck, 128), 128, 0, s>>>(B, nck, ck_start, ckpt);
+        LMIEB_CUDA_TRY(cudaGetLastError());
         const int nt = std::min(EX_TMAX, std::max(128, (ncol * EX_LT + 31) / 32 * 32));
         k_exp_tile<KIND><<<nitems, nt, sm, s>>>(B, items, pfn, ckpt, exq);
     }
@@ -1595,15 +1615,18 @@ int launch_normalize(cudaStream_t s, const DevBatch &B, long long total, const l
     return 0;
 }
 
+int expand_gsf_launches(int ncol) { return 2 * ncol <= 8 * EX_NB ? 1 : 2; }
+
 int launch_expand(cudaStream_t s, const DevBatch &B, int kind, long long nck,
-                  const long long *ck_start, int nitems, const ExpItem *items, long long nfin,
-                  const long long *fin_start, const double *pfn, double *ckpt, double *exq,
+                  const long long *ck_start, int nitems, const ExpItem *items, int nruns, const ExpItem *runs,
+                  long long nfin, const long long *fin_start, const double *pfn, double *ckpt, double *exq,
                   double *coefs, int *trunc, int *band) {
     if (nitems <= 0) return 0;
     if (kind == 0)
-        return run_expand<0>(s, B, nck, ck_start, nitems, items, nfin, fin_start, pfn, ckpt, exq, coefs, trunc,
-                             band);
-    return run_expand<1>(s, B, nck, ck_start, nitems, items, nfin, fin_start, pfn, ckpt, exq, coefs, trunc, band);
+        return run_expand<0>(s, B, nck, ck_start, nitems, items, nruns, runs, nfin, fin_start, pfn, ckpt, exq,
+                             coefs, trunc, band);
+    return run_expand<1>(s, B, nck, ck_start, nitems, items, 0, nullptr, nfin, fin_start, pfn, ckpt, exq, coefs,
+                         trunc, band);
 }
 
 int launch_phase_user(cudaStream_t s, const DevBatch &B, int kind, long long total, const long long *start,

@@ -155,10 +155,15 @@ struct ExpItem {
 };
 // ck_start: flat (case, half-angle, function) checkpoint-thread index space;
 // fin_start: flat (case, column, order) index space of the finalisation.
+// runs: (case, 0, angle tile) items of the GSF expansion on the FP64 tensor
+// cores, one block each over all the case's orders (used with kind 0 when the
+// columns fit it, see expand_gsf_launches; else the items and checkpoints).
 int launch_expand(cudaStream_t s, const DevBatch &B, int kind, long long nck,
-                  const long long *ck_start, int nitems, const ExpItem *items, long long nfin,
-                  const long long *fin_start, const double *pfn, double *ckpt, double *exq,
+                  const long long *ck_start, int nitems, const ExpItem *items, int nruns, const ExpItem *runs,
+                  long long nfin, const long long *fin_start, const double *pfn, double *ckpt, double *exq,
                   double *coefs, int *trunc, int *band);
+// kernels the GSF expansion launches before its finalisation for ncol columns
+int expand_gsf_launches(int ncol);
 
 // K5: flat (case, column, user angle) index space.
 int launch_phase_user(cudaStream_t s, const DevBatch &B, int kind, long long total, const long long *start,
