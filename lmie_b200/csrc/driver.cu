@@ -97,6 +97,18 @@ struct Ctx {
     int submits = 0;                // sub-batches submitted since the counters were reset
     int call_slot[2] = {-1, -1};    // slots of the first two sub-batches since then
     long long redo = 0;             // INT8 cases solved again in FP64 since then
+    // The FP64 re-solve of INT8 cases takes their coefficient columns and
+    // per-radius sums from the INT8 sub-batch's arena (K1 computed them there
+    // with the same operations) instead of running K1 again.
+    struct Gather {
+        bool on = false;
+        const double *coef = nullptr, *rs = nullptr;   // the source sub-batch's K1 outputs
+        long long tot = 0;                             // its orders per coefficient column
+        int R = 0;                                     // its radii
+        std::vector<DevCase> cs;                       // its cases, in the order of the re-solve
+    } gather;
+    cudaEvent_t redo_read = nullptr;   // after a re-solve that reads another slot's arena
+    int redo_src = -1;                 // that slot: its next upload waits for the event
     std::vector<std::pair<long long, int>> finished;   // (ticket, rc) of recently collected sub-batches
     char *flush = nullptr;
     cudaEvent_t ev[NSTAGE + 1] = {};
@@ -301,6 +313,8 @@ struct Plan {
     int n_ex = 0;
     ExpItem *gx = nullptr;      // (case, 0, angle tile) of the GSF expansion runs, longest first
     int n_gx = 0;
+    GatherSeg *gsegs = nullptr; // K1's outputs copied from an earlier sub-batch instead of computed
+    int n_gseg = 0;
     long long *pf_start = nullptr, *ck_gc = nullptr, *ck_lc = nullptr, *fin_start = nullptr, *pu_start = nullptr;
     long long pf_total = 0, nck_gc = 0, nck_lc = 0, nfin = 0, pu_total = 0;
     double *save1_in = nullptr, *save2_in = nullptr, *w2 = nullptr;
@@ -355,6 +369,7 @@ int ensure_ready() {
     LMIEB_CUDA_TRY(cudaEventCreate(&c.k3[1]));
     LMIEB_CUDA_TRY(cudaEventCreateWithFlags(&c.save.ready, cudaEventDisableTiming));
     LMIEB_CUDA_TRY(cudaEventCreateWithFlags(&c.gl_ready, cudaEventDisableTiming));
+    LMIEB_CUDA_TRY(cudaEventCreateWithFlags(&c.redo_read, cudaEventDisableTiming));
     c.ready = true;
     return 0;
 }
@@ -462,10 +477,14 @@ int run_accumulate(Plan &L, cudaStream_t s) {
         return 0;
     }
     if (L.save_control != 2) {
-        for (int ch = 0; ch < (L.nd1c > 0 ? L.nd1c : 1); ++ch) {
-            const int c0 = ch * 4;
-            const int nc = std::max(0, std::min(4, B.nd1 - c0));
-            if (launch_coef(s, B, nc, c0, ch == 0, L.ck, L.coef, L.bop, L.rs)) return -1;
+        if (L.n_gseg > 0) {
+            if (launch_gather(s, L.n_gseg, L.gsegs, L.coef, L.rs)) return -1;
+        } else {
+            for (int ch = 0; ch < (L.nd1c > 0 ? L.nd1c : 1); ++ch) {
+                const int c0 = ch * 4;
+                const int nc = std::max(0, std::min(4, B.nd1 - c0));
+                if (launch_coef(s, B, nc, c0, ch == 0, L.ck, L.coef, L.bop, L.rs)) return -1;
+            }
         }
         stage(2);
         if (launch_reduce_scalars(s, B, L.rs, L.sums, L.save_control == 1 ? L.o_save1 : nullptr)) return -1;
@@ -764,6 +783,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         C.accuracy = p.accuracy;
         C.r0 = cr0[k];
         C.nr = p.n;
+        C.o0 = cs1[k];
         C.n1 = p.n1;
         C.n_qang = p.n_qang;
         C.nh = p.n_qang / 2;
@@ -790,6 +810,30 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         }
     });
     const long long tot = off[R], ckn = ckoff[R];
+    // an FP64 re-solve whose cases' K1 outputs are in an earlier sub-batch's
+    // arena: their copy, in pieces of at most GATHER_PIECE doubles (one
+    // block each), replaces K1
+    std::vector<GatherSeg> gsegs;
+    if (c.gather.on && (int) c.gather.cs.size() == ncase && p0.precision == LMIEB_PRECISION_FP64 &&
+        L.save_control == 0 && L.acc_mode == LMIEB_ACC_WHOLE) {
+        constexpr long long GATHER_PIECE = 1 << 15;
+        auto add_seg = [&](const double *src, int which, long long dst_off, long long n) {
+            for (long long a = 0; a < n; a += GATHER_PIECE)
+                gsegs.push_back(GatherSeg{src + a, dst_off + a, std::min(GATHER_PIECE, n - a), which});
+        };
+        const int C1 = 1 + nd1;
+        for (int k = 0; k < ncase; ++k) {
+            const DevCase &F = c.gather.cs[k], &T = cs[k];
+            const long long no = cs1[k + 1] - cs1[k];   // the case's orders (the same radii in both)
+            for (int col = 0; col < C1; ++col) {
+                add_seg(c.gather.coef + ((size_t) col * c.gather.tot + F.o0) * 4, 0, ((long long) col * tot + T.o0) * 4,
+                        no * 4);
+                for (int q = 0; q < 5; ++q)
+                    add_seg(c.gather.rs + (size_t) (col * 5 + q) * c.gather.R + F.r0, 1,
+                            (long long) (col * 5 + q) * R + T.r0, T.nr);
+            }
+        }
+    }
     // K1 launch order: cases by their largest n1, largest first, each from its
     // largest radius down, so that the longest recurrences start first
     std::vector<int> k1ord(ncase);
@@ -1205,7 +1249,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         if (!solve) {
             // integrals uploaded (or zero on an empty share)
         } else if (L.save_control != 2) {
-            nl += (long long) std::max(L.nd1c, 1) + 1;                          // K1 per chunk, K2
+            nl += (gsegs.empty() ? (long long) std::max(L.nd1c, 1) : 1) + 1;   // K1 per chunk (or its copy), K2
             if (L.tc) nl += (L.n_ang > 0) + (L.n_ang64 > 0 ? L.n_ang_launch : 0);   // K3
             else if (L.oz) nl += (L.n_ang > 0 ? 3 : 0) + (L.n_ang64 > 0 ? L.n_ang_launch : 0);   // operands, K3
             else nl += L.n_ang > 0 ? L.n_ang_launch : 0;
@@ -1271,6 +1315,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         add((size_t) nd1 * 4); add((size_t) nd2 * 4); add(mu_user.size() * 8);
         add(ang.size() * sizeof(AngItem)); add(ang64.size() * sizeof(AngItem)); add(ex.size() * sizeof(ExpItem));
         add(gx.size() * sizeof(ExpItem));
+        add(gsegs.size() * sizeof(GatherSeg));
         add(tc_pos.size() * 4); add(tc_roff.size() * 8); add(tg_r0.size() * 4); add(tg_n.size() * 4);
         add(tg_nk.size() * 4); add(tg_off.size() * 8); add(oz_f2.size() * 8); add(rx_start.size() * 8);
         add(a_start.size() * 8);
@@ -1316,6 +1361,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     AngItem *h_ang64 = put(hp, ho, ang64.data(), ang64.size());
     ExpItem *h_ex = put(hp, ho, ex.data(), ex.size());
     ExpItem *h_gx = put(hp, ho, gx.data(), gx.size());
+    GatherSeg *h_gs = put(hp, ho, gsegs.data(), gsegs.size());
     int *h_tcpos = put(hp, ho, tc_pos.data(), tc_pos.size());
     long long *h_tcroff = put(hp, ho, tc_roff.data(), tc_roff.size());
     int *h_tgr0 = put(hp, ho, tg_r0.data(), tg_r0.size());
@@ -1433,6 +1479,8 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     L.ang64 = (AngItem *) dptr(h_ang64);
     L.ex = (ExpItem *) dptr(h_ex);
     L.gx = (ExpItem *) dptr(h_gx);
+    L.gsegs = (GatherSeg *) dptr(h_gs);
+    L.n_gseg = (int) gsegs.size();
     L.pf_start = (long long *) dptr(h_pfs);
     L.ck_gc = (long long *) dptr(h_ckg);
     L.ck_lc = (long long *) dptr(h_ckl);
@@ -1503,6 +1551,10 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     // those of the previous one; with per-stage timing both use the context's
     // stream (the stage events are shared) and run one after the other.
     cudaStream_t s = c.timing ? c.stream : S.stream;
+    if (c.redo_src == (int) (&S - c.slot)) {
+        LMIEB_CUDA_TRY(cudaStreamWaitEvent(s, c.redo_read, 0));
+        c.redo_src = -1;
+    }
     stage(0);
     LMIEB_CUDA_TRY(cudaEventRecord(S.t_begin, s));
     if (c.submits == 1) LMIEB_CUDA_TRY(cudaEventRecord(c.t_first, s));
@@ -1722,10 +1774,25 @@ int collect_slot(Slot &S) {
             redo_early = fit_sub((int) rq.size(), rq.data());
             if (c.submits < 2) c.call_slot[c.submits] = 2;
             ++c.submits;
-            if (submit_sub(R3, c.redo_ticket++, redo_early, rq.data(), rr.data())) {
+            // their coefficient columns and per-radius sums from this
+            // sub-batch's arena, which this slot's next upload waits for
+            const Plan &SL = *S.plan;
+            // (offsets: without the split form, coefficient offsets are the n1 prefix sums)
+            c.gather.on = SL.coef && SL.rs && !SL.tc && P.save_control == 0 && P.acc_mode == LMIEB_ACC_WHOLE;
+            c.gather.coef = SL.coef;
+            c.gather.rs = SL.rs;
+            c.gather.tot = SL.B.tot;
+            c.gather.R = SL.B.R;
+            c.gather.cs.clear();
+            for (int i = 0; i < redo_early; ++i) c.gather.cs.push_back(P.cs[redo[i]]);
+            const int rc3 = submit_sub(R3, c.redo_ticket++, redo_early, rq.data(), rr.data());
+            c.gather.on = false;
+            if (rc3) {
                 R3.pend.active = false;
                 return -1;
             }
+            LMIEB_CUDA_TRY(cudaEventRecord(c.redo_read, R3.stream));
+            c.redo_src = (int) (&S - c.slot);
         }
     }
     for (size_t p = 0; p + 1 < P.piece.size(); ++p) {

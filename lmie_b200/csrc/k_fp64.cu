@@ -1562,6 +1562,22 @@ int launch_coef(cudaStream_t s, const DevBatch &B, int nc, int c0, int write_val
     return 0;
 }
 
+namespace {
+__global__ void __launch_bounds__(256) k_gather(const GatherSeg *__restrict__ segs, double *__restrict__ coef,
+                                               double *__restrict__ rs) {
+    const GatherSeg g = segs[blockIdx.x];
+    double *dst = (g.which ? rs : coef) + g.dst_off;
+    for (long long i = threadIdx.x; i < g.n; i += blockDim.x) dst[i] = g.src[i];
+}
+}  // namespace
+
+int launch_gather(cudaStream_t s, int nseg, const GatherSeg *segs, double *coef, double *rs) {
+    if (nseg <= 0) return 0;
+    k_gather<<<nseg, 256, 0, s>>>(segs, coef, rs);
+    LMIEB_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
 int launch_reduce_scalars(cudaStream_t s, const DevBatch &B, const double *rs, double *sums, double *save1) {
     dim3 grid(B.ncase, 1 + B.nd);
     k_reduce_scalars<<<grid, 256, 0, s>>>(B, rs, sums, save1);

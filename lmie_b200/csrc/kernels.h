@@ -12,6 +12,14 @@
 // limit of every bounded wait of the tensor-core kernels (~1 s at 1.96 GHz), in SM clock cycles
 constexpr long long LMIEB_WAIT_CYCLES = 1LL << 31;
 
+// One contiguous copy of a sub-batch whose coefficients were computed by an
+// earlier sub-batch: n doubles from src (that sub-batch's arena) to the
+// coefficient columns (which = 0) or per-radius sums (which = 1) at dst_off.
+struct GatherSeg {
+    const double *src;
+    long long dst_off, n;
+    int which;
+};
 // K1 keeps its downward recurrences at the top of every block of K1_B orders.
 constexpr int K1_B = 16;
 // doubles per checkpoint block of a chunk of nc tangent-linear columns
@@ -23,6 +31,7 @@ struct DevCase {
     cplx m, minv;
     double accuracy;            // expansion truncation threshold
     int r0, nr;                 // radius range [r0, r0 + nr) in the batch lists
+    long long o0;               // its first order in the coefficient columns (sum of n1 of the radii before)
     int n1, n_qang, nh, n_coef, n_angles;
     int ml_off;                 // m_l / lambda_l of this case at [ml_off, ml_off + nd)
     long long mu_off;           // Gauss nodes/weights in the node pool
@@ -158,6 +167,9 @@ struct ExpItem {
 // runs: (case, 0, angle tile) items of the GSF expansion on the FP64 tensor
 // cores, one block each over all the case's orders (used with kind 0 when the
 // columns fit it, see expand_gsf_launches; else the items and checkpoints).
+// K1's outputs (coefficient columns, per-radius sums) copied in instead of
+// computed: one block per segment
+int launch_gather(cudaStream_t s, int nseg, const GatherSeg *segs, double *coef, double *rs);
 int launch_expand(cudaStream_t s, const DevBatch &B, int kind, long long nck,
                   const long long *ck_start, int nitems, const ExpItem *items, int nruns, const ExpItem *runs,
                   long long nfin, const long long *fin_start, const double *pfn, double *ckpt, double *exq,
