@@ -16,6 +16,7 @@
 #include <condition_variable>
 #include <functional>
 #include <mutex>
+#include <set>
 #include <thread>
 #include <unordered_map>
 #include <vector>
@@ -190,10 +191,39 @@ struct RadiusGroup {
 } g_group;
 Nccl g_nccl;
 
-// fn(i) for every i in [0, n) on the host's cores (dynamic chunks of `grain`)
+// Physical cores of the host (distinct core ids of the online CPUs; the
+// hardware threads if the topology cannot be read): memory-bound copies
+// run faster on one thread per core than on both threads of each core.
+int host_cores() {
+    static const int n = [] {
+        const int hw = (int) std::max(1u, std::thread::hardware_concurrency());
+        std::set<std::pair<int, int>> ids;
+        for (int cpu = 0; cpu < hw; ++cpu) {
+            char path[128];
+            int pkg = -1, core = -1;
+            snprintf(path, sizeof path, "/sys/devices/system/cpu/cpu%d/topology/physical_package_id", cpu);
+            if (FILE *f = fopen(path, "r")) {
+                if (fscanf(f, "%d", &pkg) != 1) pkg = -1;
+                fclose(f);
+            }
+            snprintf(path, sizeof path, "/sys/devices/system/cpu/cpu%d/topology/core_id", cpu);
+            if (FILE *f = fopen(path, "r")) {
+                if (fscanf(f, "%d", &core) != 1) core = -1;
+                fclose(f);
+            }
+            if (pkg < 0 || core < 0) return hw;
+            ids.insert({pkg, core});
+        }
+        return ids.empty() ? hw : (int) ids.size();
+    }();
+    return n;
+}
+
+// fn(i) for every i in [0, n) on the host's cores (dynamic chunks of
+// `grain`), on at most max_threads threads (0: one per hardware thread)
 template <class F>
-void parallel_for(int n, int grain, F &&fn) {
-    const int hw = (int) std::max(1u, std::thread::hardware_concurrency());
+void parallel_for(int n, int grain, F &&fn, int max_threads = 0) {
+    const int hw = max_threads > 0 ? max_threads : (int) std::max(1u, std::thread::hardware_concurrency());
     const int nt = std::min(std::min(hw, 32), (n + grain - 1) / grain);
     if (nt <= 1) {
         for (int i = 0; i < n; ++i) fn(i);
@@ -229,14 +259,14 @@ extern "C" void lmieb_host_parallel(int n, int n_threads, void (*fn)(void *, int
     host_pool().run(nt, body);
 }
 
-// memcpy of a large block on several host threads
+// memcpy of a large block on one host thread per core
 void par_memcpy(void *dst, const void *src, size_t bytes) {
     const size_t chunk = std::max((size_t) 256 << 10, (bytes / 16 + 4095) & ~(size_t) 4095);
     const int n = (int) ((bytes + chunk - 1) / chunk);
     parallel_for(n, 1, [&](int i) {
         const size_t a = (size_t) i * chunk, b = std::min(bytes, a + chunk);
         memcpy((char *) dst + a, (const char *) src + a, b - a);
-    });
+    }, host_cores());
 }
 
 double now_ms() {
@@ -1807,9 +1837,16 @@ int collect_slot(Slot &S) {
             const DevCase &C = P.cs[k];
             lmieb_result &r = P.rs[k];
             memcpy(r.scal, hs + C.scal_off, (size_t) ncol * 4 * 8);
+            // rows laid out one after the other (the blocks of lmie_out_alloc)
+            // take one copy per run
             auto put = [&](double **rows, double *flat, const double *src, size_t len) {
                 if (rows) {
-                    for (int i = 0; i < ncol * 6; ++i) memcpy(rows[i], src + (size_t) i * len, len * 8);
+                    for (int j = 0; j < ncol * 6;) {
+                        int e = j + 1;
+                        while (e < ncol * 6 && rows[e] == rows[j] + (size_t) (e - j) * len) ++e;
+                        memcpy(rows[j], src + (size_t) j * len, (size_t) (e - j) * len * 8);
+                        j = e;
+                    }
                 } else if (flat) {
                     memcpy(flat, src, (size_t) ncol * 6 * len * 8);
                 }
@@ -1819,7 +1856,7 @@ int collect_slot(Slot &S) {
             if (P.pf_from) put(r.pf_rows, r.pf, hpf + C.pf_out_off, (size_t) C.n_angles);
             const int t = P.want_lc ? htr[ncase + k] : (P.want_gc ? htr[k] : 0);
             r.n_coef_out = (P.want_gc || P.want_lc) ? (t > 0 ? C.n_coef - t + 1 : C.n_coef) : 0;
-        });
+        }, host_cores());
     }
     LMIEB_CUDA_TRY(cudaEventSynchronize(S.done));
     c.host_ms[2] += t_unpack - P.t_submit + waited;
