@@ -174,6 +174,41 @@ def test_truncation_at_the_threshold_is_solved_in_fp64():
         assert np.array_equal(getattr(got, name), getattr(ref, name)), name
 
 
+def test_re_solves_in_every_part_are_the_fp64_form():
+    """Cases on the truncation threshold in each of four pipelined parts: their
+    FP64 re-solves copy the coefficients from the int8 part's device memory
+    while later parts reuse the same buffers; every re-solved case is the FP64
+    form's bit for bit and the others stay within the bounds."""
+    import math
+    lib = _lib()
+    cases, at = [], []
+    for i, c in enumerate(workloads.batched_uneven(48)):
+        # (cases under 16 orders keep the FP64 angular stage: no re-solve)
+        if i % 3 == 0 and n1(2 * math.pi * c.r2 / c.lam) >= 16:
+            (full,) = abi.solve_batch(lib, [dataclasses.replace(c, accuracy=0.)], precision=abi.PRECISION_FP64)
+            beta = np.abs(full.gc[0])
+            l0 = int(np.argmax(beta <= 1e-7))
+            if l0 > 0 and beta[l0] > 0:
+                c = dataclasses.replace(c, accuracy=float(beta[l0]))
+                at.append(i)
+        cases.append(c)
+    assert len(at) >= 4, at
+    lib.lmieb_set_pipeline.argtypes = [C.c_int]
+    lib.lmieb_set_pipeline(4)
+    try:
+        ref, got, redo = _both(cases)
+    finally:
+        lib.lmieb_set_pipeline(0)
+    assert redo >= len(at), (redo, at)
+    for i, (g, r) in enumerate(zip(got, ref)):
+        if i in at:
+            assert g.n_coef == r.n_coef, i
+            for name in ("gc", "pf", "gc_l", "pf_l"):
+                assert np.array_equal(getattr(g, name), getattr(r, name)), (i, name)
+        else:
+            _check(g, r, f"case {i}")
+
+
 def test_precision_stress_large_particles():
     """Size parameter 5000 (n1 = 5077, 10154 Gauss angles, 8000 radii, four
     derivatives): 159 chunks per radius group, near the exact-sum limit."""
