@@ -386,9 +386,15 @@ int ensure_ready() {
     c.sms = prop.multiProcessorCount;
     LMIEB_CUDA_TRY(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
     for (int i = 0; i <= NSTAGE; ++i) LMIEB_CUDA_TRY(cudaEventCreate(&c.ev[i]));
+    // the third slot runs the FP64 re-solves of a few int8 cases next to the
+    // following sub-batch: at the highest priority, its blocks are scheduled
+    // as soon as SMs free up instead of waiting behind that sub-batch's
+    int prio_lo = 0, prio_hi = 0;
+    LMIEB_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
     for (Slot &S : c.slot) {
         S.plan = new Plan();
-        LMIEB_CUDA_TRY(cudaStreamCreateWithFlags(&S.stream, cudaStreamNonBlocking));
+        LMIEB_CUDA_TRY(cudaStreamCreateWithPriority(&S.stream, cudaStreamNonBlocking,
+                                                    &S == &c.slot[2] ? prio_hi : prio_lo));
         LMIEB_CUDA_TRY(cudaEventCreateWithFlags(&S.done, cudaEventDisableTiming));
         for (cudaEvent_t &e : S.piece) LMIEB_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         LMIEB_CUDA_TRY(cudaEventCreate(&S.t_begin));
@@ -786,18 +792,13 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         fprintf(stderr, "ERROR: lmie_b200: a case without radii\n");
         return -1;
     }
-    // per-radius arrays: every element is written below; kept between calls
-    // (calls are serialised) so that their pages are not faulted in and
-    // zeroed again for every sub-batch
-    static std::vector<double> x, xl, w;
-    static std::vector<int> n1r, n2r, rcase;
+    // per-radius arrays the packing reads: every element is written below;
+    // kept between calls (calls are serialised) so that their pages are not
+    // faulted in and zeroed again for every sub-batch (the other per-radius
+    // inputs go straight into the staging buffer, below)
+    static std::vector<int> n1r;
     static std::vector<long long> off, ckoff;
-    x.resize(R);
-    xl.resize((size_t) std::max(nd1, 1) * R);
-    w.resize((size_t) ncol * R);
     n1r.resize(R);
-    n2r.resize(R);
-    rcase.resize(R);
     off.resize(R + 1);
     ckoff.resize(R + 1);
     std::vector<cplx> ml((size_t) std::max(1, ncase * nd));
@@ -827,12 +828,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         long long o = cs1[k];
         long long t = ct0[k];
         for (int i = 0, r = cr0[k]; i < p.n; ++i, ++r) {
-            x[r] = p.x[i];
-            for (int q = 0; q < nd1; ++q) xl[(size_t) q * R + r] = p.xl[(size_t) q * p.n + i];
-            for (int q = 0; q < ncol; ++q) w[(size_t) q * R + r] = p.w[(size_t) q * p.n + i];
             n1r[r] = p.n1r[i];
-            n2r[r] = p.n2r[i];
-            rcase[r] = k;
             o += n1r[r];
             off[r + 1] = o;
             t += (n1r[r] + K1_B - 1) / K1_B;
@@ -1338,7 +1334,8 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     size_t in_bytes = 0;
     {
         auto add = [&](size_t b) { in_bytes += pad(b); };
-        add(cs.size() * sizeof(DevCase)); add((size_t) R * 8); add(xl.size() * 8); add(w.size() * 8);
+        add(cs.size() * sizeof(DevCase)); add((size_t) R * 8); add((size_t) std::max(nd1, 1) * R * 8);
+        add((size_t) ncol * R * 8);
         add((size_t) R * 4); add((size_t) R * 4); add((size_t) R * 4);
         add((size_t) (R + 1) * 8); add((size_t) (R + 1) * 8);
         add(fv.size() * 8); add(rc.size() * 8); add(ml.size() * 16); add(laml.size() * 8);
@@ -1370,12 +1367,23 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     char *hp = S.hbuf;
     size_t ho = 0;
     DevCase *h_cs = put(hp, ho, cs.data(), cs.size());
-    double *h_x = put(hp, ho, x.data(), (size_t) R);
-    double *h_xl = put(hp, ho, xl.data(), xl.size());
-    double *h_w = put(hp, ho, w.data(), w.size());
+    // the per-radius inputs go straight from the cases into the staging
+    // buffer (one pass over them, on one thread per core)
+    double *h_x = put(hp, ho, (const double *) nullptr, (size_t) R);
+    double *h_xl = put(hp, ho, (const double *) nullptr, (size_t) std::max(nd1, 1) * R);
+    double *h_w = put(hp, ho, (const double *) nullptr, (size_t) ncol * R);
     int *h_n1r = put(hp, ho, n1r.data(), (size_t) R);
-    int *h_n2r = put(hp, ho, n2r.data(), (size_t) R);
-    int *h_rcase = put(hp, ho, rcase.data(), (size_t) R);
+    int *h_n2r = put(hp, ho, (const int *) nullptr, (size_t) R);
+    int *h_rcase = put(hp, ho, (const int *) nullptr, (size_t) R);
+    parallel_for(ncase, 16, [&](int k) {
+        const lmieb_problem &p = ps[k];
+        const int r0 = cr0[k];
+        memcpy(h_x + r0, p.x, (size_t) p.n * 8);
+        for (int q = 0; q < nd1; ++q) memcpy(h_xl + (size_t) q * R + r0, p.xl + (size_t) q * p.n, (size_t) p.n * 8);
+        for (int q = 0; q < ncol; ++q) memcpy(h_w + (size_t) q * R + r0, p.w + (size_t) q * p.n, (size_t) p.n * 8);
+        memcpy(h_n2r + r0, p.n2r, (size_t) p.n * 4);
+        for (int i = 0; i < p.n; ++i) h_rcase[r0 + i] = k;
+    }, host_cores());
     int *h_k1ord = put(hp, ho, k1ord.data(), (size_t) ncase);
     long long *h_k1pre = put(hp, ho, k1pre.data(), (size_t) ncase + 1);
     long long *h_off = put(hp, ho, coff.data(), (size_t) R + 1);
