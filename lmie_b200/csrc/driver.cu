@@ -347,6 +347,8 @@ struct Plan {
     int n_gseg = 0;
     long long *pf_start = nullptr, *ck_gc = nullptr, *ck_lc = nullptr, *fin_start = nullptr, *pu_start = nullptr;
     long long pf_total = 0, nck_gc = 0, nck_lc = 0, nfin = 0, pu_total = 0;
+    double *pu_scr = nullptr;   // K5 partial sums of cases of several parts
+    long long pu_nred = 0, *pu_red = nullptr;   // their (case, column, element, angle) index space
     double *save1_in = nullptr, *save2_in = nullptr, *w2 = nullptr;
     double *o_scal = nullptr, *o_gc = nullptr, *o_lc = nullptr, *o_pf = nullptr;
     int *o_trunc = nullptr;     // [2][ncase]: gc, lc
@@ -577,7 +579,9 @@ int run_finish(Plan &L, cudaStream_t s) {
     if (L.pf_from) {
         const int *tr = L.want_lc ? L.o_trunc + L.ncase : L.o_trunc;
         const double *cf = L.pf_from == 1 ? L.o_gc : L.o_lc;
-        if (launch_phase_user(s, B, L.pf_from == 1 ? 0 : 1, L.pu_total, L.pu_start, cf, tr, L.o_pf)) return -1;
+        if (launch_phase_user(s, B, L.pf_from == 1 ? 0 : 1, L.pu_total, L.pu_start, cf, tr, L.o_pf, L.pu_scr,
+                              L.pu_nred, L.pu_red))
+            return -1;
     }
     stage(8);
     return 0;
@@ -1239,7 +1243,8 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
 
     // ---- user angles and output offsets ----
     // the user angles depend only on their number: one copy per distinct count
-    std::vector<long long> pu_start(ncase + 1, 0);
+    std::vector<long long> pu_start(ncase + 1, 0), pu_red(ncase + 1, 0);
+    long long pu_scr_total = 0;
     std::vector<double> mu_user;
     std::unordered_map<int, long long> mu_at;
     size_t o_scal = 0, o_gc = 0, o_lc = 0, o_pf = 0;
@@ -1255,7 +1260,12 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
                 mu_user.insert(mu_user.end(), ps[k].mu_user, ps[k].mu_user + C.n_angles);
             }
         }
-        pu_start[k + 1] = pu_start[k] + (C.n_angles + PU_T - 1) / PU_T;   // K5 blocks (all columns)
+        // K5: parts of PU_LP orders; the partial sums of a case of several
+        C.pu_parts = (L.pf_from && C.n_angles > 0) ? std::max(1, (C.n_coef + PU_LP - 1) / PU_LP) : 0;
+        C.pu_scr_off = pu_scr_total;
+        const long long pu_n = (long long) ncol * 6 * C.n_angles;
+        if (C.pu_parts > 1) pu_scr_total += C.pu_parts * pu_n;
+        pu_red[k + 1] = pu_red[k] + (C.pu_parts > 1 ? pu_n : 0);
         C.scal_off = (int) o_scal;
         o_scal += (size_t) ncol * 4;
         C.gc_off = (long long) o_gc;
@@ -1265,7 +1275,14 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         C.pf_out_off = (long long) o_pf;
         o_pf += (size_t) ncol * 6 * C.n_angles;
     }
+    // K5 blocks (all columns per block), cases in K1's launch order: the most
+    // orders first
+    for (int kr = 0; kr < ncase; ++kr) {
+        const DevCase &C = cs[k1ord[kr]];
+        pu_start[kr + 1] = pu_start[kr] + (long long) ((C.n_angles + PU_T - 1) / PU_T) * C.pu_parts;
+    }
     L.pu_total = pu_start[ncase];
+    L.pu_nred = pu_red[ncase];
 
     // ---- launches per device run and algorithmic work ----
     {
@@ -1287,7 +1304,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
             nl += 1 + (L.pf_total > 0);                                          // normalisation
             if (L.want_gc && L.n_ex > 0) nl += 1 + expand_gsf_launches(ncol);
             if (L.want_lc && L.n_ex > 0) nl += 3;
-            if (L.pf_from && L.pu_total > 0) nl += 1;
+            if (L.pf_from && L.pu_total > 0) nl += 1 + (L.pu_nred > 0);
         }
         L.launches = nl;
         double fang = 0., frec = 0., fgsf = 0., fexp = 0.;
@@ -1346,7 +1363,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         add(tc_pos.size() * 4); add(tc_roff.size() * 8); add(tg_r0.size() * 4); add(tg_n.size() * 4);
         add(tg_nk.size() * 4); add(tg_off.size() * 8); add(oz_f2.size() * 8); add(rx_start.size() * 8);
         add(a_start.size() * 8);
-        for (int q = 0; q < 5; ++q) add((size_t) (ncase + 1) * 8);
+        for (int q = 0; q < 6; ++q) add((size_t) (ncase + 1) * 8);   // prefix arrays over the cases
         add((size_t) ncase * 4); add((size_t) (ncase + 1) * 8);             // K1 launch order
         add(gl_ns.size() * 4); add(gl_mo.size() * 8); add(gl_go.size() * 8); add(gl_pt.size() * 4);
         add(gl_pi.size() * 4); add(gl_guess.size() * 8); add(gl_jr.size() * 8);
@@ -1414,6 +1431,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     long long *h_ckl = put(hp, ho, ck_lc.data(), ck_lc.size());
     long long *h_fin = put(hp, ho, fin_start.data(), fin_start.size());
     long long *h_pus = put(hp, ho, pu_start.data(), pu_start.size());
+    long long *h_pur = put(hp, ho, pu_red.data(), pu_red.size());
     int *h_gns = put(hp, ho, gl_ns.data(), gl_ns.size());
     long long *h_gmo = put(hp, ho, gl_mo.data(), gl_mo.size());
     long long *h_ggo = put(hp, ho, gl_go.data(), gl_go.size());
@@ -1467,6 +1485,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         add((size_t) L.pf_total * 8);
         add((size_t) ck_total * 8);
         add((size_t) ex_total * 8);
+        add((size_t) pu_scr_total * 8);
     }
     if (ensure_device(S, dev_bytes)) return -1;
     Arena A{S.dbuf, 0, S.dcap};
@@ -1524,6 +1543,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     L.ck_lc = (long long *) dptr(h_ckl);
     L.fin_start = (long long *) dptr(h_fin);
     L.pu_start = (long long *) dptr(h_pus);
+    L.pu_red = (long long *) dptr(h_pur);
     if (L.save_control == 2) {
         L.save1_in = save_hit ? c.save.d : (double *) dptr(h_s1);
         L.save2_in = save_hit ? c.save.d + (size_t) 4 * R : (double *) dptr(h_s2);
@@ -1559,6 +1579,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     L.pfn = A.take<double>((size_t) L.pf_total);
     L.ckpt = A.take<double>((size_t) ck_total);
     L.exq = A.take<double>((size_t) ex_total);
+    L.pu_scr = A.take<double>((size_t) pu_scr_total);
     {
         char *o = d_out;
         auto take = [&](size_t bytes) { char *r = o; o += pad(bytes); return r; };

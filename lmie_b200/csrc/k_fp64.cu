@@ -1329,24 +1329,36 @@ __global__ void k_exp_final(DevBatch B, long long total, const long long *__rest
 
 // ---------------------------------------------------------------------------
 // K5: phase matrix at the user's angles from the truncated expansion; one
-// block per (case, tile of PU_T user angles), one thread per angle.  The
-// basis functions of an order are generated once per angle and used by up to
-// CG columns at a time; the expansion coefficients of those columns (GSF:
-// with the a2 +- a3 pair combined) and the recurrence coefficients of PU_T
-// orders at a time are staged in shared memory, which all threads read.
+// block per (case, tile of PU_T user angles, part of PU_LP orders), one
+// thread per angle, cases with the most orders first.  A block runs the basis
+// recurrences from order 0 and sums the terms of its part's orders, so that a
+// case with many orders is spread over several blocks instead of one long
+// chain; a case of several parts writes their sums to scr, added up in order
+// by k_phase_user_sum.  The basis functions of an order are generated once
+// per angle and used by up to CG columns at a time; the expansion
+// coefficients of those columns (GSF: with the a2 +- a3 pair combined) and the
+// recurrence coefficients of PU_T orders at a time are staged in shared
+// memory, which all threads read.
 // ---------------------------------------------------------------------------
 template <int KIND, int CG>
 __global__ void __launch_bounds__(PU_T) k_phase_user(DevBatch B, const long long *__restrict__ start,
                                                      const double *__restrict__ coefs,
-                                                     const int *__restrict__ trunc, double *__restrict__ out) {
+                                                     const int *__restrict__ trunc, double *__restrict__ out,
+                                                     double *__restrict__ scr) {
     __shared__ double cfs[CG][6][PU_T], rcs[8 * PU_T];
-    const int c = find_case(start, B.ncase, blockIdx.x);
+    const int kr = find_case(start, B.ncase, blockIdx.x);
+    const int c = B.k1ord[kr];
     const DevCase &C = B.cs[c];
     const int na = C.n_angles, ncf = C.n_coef, ncol = 1 + B.nd;
-    const int local = (int) (blockIdx.x - start[c]);
-    const int a = local * PU_T + threadIdx.x;
+    const int ntile = (na + PU_T - 1) / PU_T;
+    const int local = (int) (blockIdx.x - start[kr]);
+    const int part = local / ntile, tile = local - part * ntile;
+    const int a = tile * PU_T + threadIdx.x;
     const bool act = a < na;
     const int nt = trunc[c] > 0 ? ncf - trunc[c] + 1 : ncf;
+    // this block's orders [lbeg, lend); the tiles of PU_T orders before lbeg
+    // only advance the recurrences (PU_LP is a multiple of PU_T)
+    const int lbeg = part * PU_LP, lend = min(nt, lbeg + PU_LP);
     const double x = act ? B.mu_user[C.mu_user_off + a] : 0.;
     const double *cf0 = coefs + (KIND == 0 ? C.gc_off : C.lc_off);
     for (int g0 = 0; g0 < ncol; g0 += CG) {
@@ -1357,10 +1369,11 @@ __global__ void __launch_bounds__(PU_T) k_phase_user(DevBatch B, const long long
 #pragma unroll
             for (int e = 0; e < 6; ++e) s[g][e] = 0.;
         double q[4] = {0., 0., 0., 0.}, p[4] = {0., 0., 0., 0.};
-        for (int l0 = 0; l0 < nt; l0 += PU_T) {
-            const int lt = min(PU_T, nt - l0);
+        for (int l0 = 0; l0 < lend; l0 += PU_T) {
+            const int lt = min(PU_T, lend - l0);
+            const bool sum = l0 >= lbeg;
             __syncthreads();
-            for (int t = threadIdx.x; t < ng * PU_T; t += PU_T) {
+            for (int t = threadIdx.x; sum && t < ng * PU_T; t += PU_T) {
                 const int g = t / PU_T, u = t % PU_T;
                 const double *cf = cf0 + (size_t) (g0 + g) * 6 * ncf + l0 + u;
                 double v[6] = {0., 0., 0., 0., 0., 0.};
@@ -1387,6 +1400,7 @@ __global__ void __launch_bounds__(PU_T) k_phase_user(DevBatch B, const long long
                         q[f] = p[f];
                         p[f] = v;
                     }
+                    if (!sum) continue;
 #pragma unroll
                     for (int g = 0; g < CG; ++g) {
                         s[g][0] += cfs[g][0][u] * p[0];
@@ -1402,6 +1416,7 @@ __global__ void __launch_bounds__(PU_T) k_phase_user(DevBatch B, const long long
                     const double v = l < 2 ? basis_first<1>(0, l, x) : basis_step<1>(0, rl, x, p[0], q[0]);
                     q[0] = p[0];
                     p[0] = v;
+                    if (!sum) continue;
 #pragma unroll
                     for (int g = 0; g < CG; ++g)
 #pragma unroll
@@ -1413,7 +1428,8 @@ __global__ void __launch_bounds__(PU_T) k_phase_user(DevBatch B, const long long
 #pragma unroll
             for (int g = 0; g < CG; ++g) {
                 if (g >= ng) break;
-                double *o = out + C.pf_out_off + (size_t) (g0 + g) * 6 * na;
+                double *o = (C.pu_parts > 1 ? scr + C.pu_scr_off + (size_t) part * ncol * 6 * na
+                                            : out + C.pf_out_off) + (size_t) (g0 + g) * 6 * na;
                 if (KIND == 0) {
                     o[a] = s[g][0];
                     o[(size_t) 3 * na + a] = s[g][3];
@@ -1432,6 +1448,21 @@ __global__ void __launch_bounds__(PU_T) k_phase_user(DevBatch B, const long long
             }
         }
     }
+}
+
+// The phase matrix of cases of several K5 parts: thread per (case, column,
+// element, angle) of the flat space `start`, the parts' sums added in order.
+__global__ void k_phase_user_sum(DevBatch B, long long total, const long long *__restrict__ start,
+                                 const double *__restrict__ scr, double *__restrict__ out) {
+    const long long e = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= total) return;
+    const int c = find_case(start, B.ncase, e);
+    const DevCase &C = B.cs[c];
+    const long long local = e - start[c], n = (long long) (1 + B.nd) * 6 * C.n_angles;
+    const double *sp = scr + C.pu_scr_off + local;
+    double v = sp[0];
+    for (int p = 1; p < C.pu_parts; ++p) v += sp[(size_t) p * n];
+    out[C.pf_out_off + local] = v;
 }
 
 template <int NC1, int NC2>
@@ -1646,19 +1677,24 @@ int launch_expand(cudaStream_t s, const DevBatch &B, int kind, long long nck,
 }
 
 int launch_phase_user(cudaStream_t s, const DevBatch &B, int kind, long long total, const long long *start,
-                      const double *coefs, const int *trunc, double *pf_out) {
+                      const double *coefs, const int *trunc, double *pf_out, double *scr, long long nred,
+                      const long long *red_start) {
     if (total <= 0) return 0;
     const int ncol = 1 + B.nd;
     const unsigned nb = (unsigned) total;
     if (kind == 0) {
-        if (ncol == 1) k_phase_user<0, 1><<<nb, PU_T, 0, s>>>(B, start, coefs, trunc, pf_out);
-        else if (ncol <= 3) k_phase_user<0, 3><<<nb, PU_T, 0, s>>>(B, start, coefs, trunc, pf_out);
-        else k_phase_user<0, 5><<<nb, PU_T, 0, s>>>(B, start, coefs, trunc, pf_out);
+        if (ncol == 1) k_phase_user<0, 1><<<nb, PU_T, 0, s>>>(B, start, coefs, trunc, pf_out, scr);
+        else if (ncol <= 3) k_phase_user<0, 3><<<nb, PU_T, 0, s>>>(B, start, coefs, trunc, pf_out, scr);
+        else k_phase_user<0, 5><<<nb, PU_T, 0, s>>>(B, start, coefs, trunc, pf_out, scr);
     } else {
-        if (ncol == 1) k_phase_user<1, 1><<<nb, PU_T, 0, s>>>(B, start, coefs, trunc, pf_out);
-        else if (ncol <= 3) k_phase_user<1, 3><<<nb, PU_T, 0, s>>>(B, start, coefs, trunc, pf_out);
-        else k_phase_user<1, 5><<<nb, PU_T, 0, s>>>(B, start, coefs, trunc, pf_out);
+        if (ncol == 1) k_phase_user<1, 1><<<nb, PU_T, 0, s>>>(B, start, coefs, trunc, pf_out, scr);
+        else if (ncol <= 3) k_phase_user<1, 3><<<nb, PU_T, 0, s>>>(B, start, coefs, trunc, pf_out, scr);
+        else k_phase_user<1, 5><<<nb, PU_T, 0, s>>>(B, start, coefs, trunc, pf_out, scr);
     }
     LMIEB_CUDA_TRY(cudaGetLastError());
+    if (nred > 0) {
+        k_phase_user_sum<<<ceil_div(nred, 256), 256, 0, s>>>(B, nred, red_start, scr, pf_out);
+        LMIEB_CUDA_TRY(cudaGetLastError());
+    }
     return 0;
 }
