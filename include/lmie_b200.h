@@ -80,15 +80,25 @@ double lmieb_get_work_granularity(int precision);
 int lmieb_set_split_segment(int chunks);
 int lmieb_get_split_segment(void);
 
+/* Orders per block of the phase matrix at the user angles (its tiles: 64 user
+ * angles by this many orders; a case with more orders is spread over several
+ * blocks whose sums are added in order): a multiple of 64 from 64 to 4096,
+ * default 256; results differ only in the order of partial sums.  Returns 0
+ * or -1. */
+int lmieb_set_user_angle_part(int orders);
+int lmieb_get_user_angle_part(void);
+
 /* Autotuner: solves the batch in[0..n_cases) (outputs in out, allocated by
  * the caller or a previous call) repeatedly.  It first picks the angular work
  * granularity (32, 64, 128, 256 items per SM for FP64; 1, 2, 4 for the
  * tensor-core stage) by the device time of the kernels (per-stage CUDA events,
  * one sub-batch) plus the host time of packing the work items, then the
- * pipeline depth (1, 2, 3, 4, 6 parts) by the wall time
- * of the public batch call, and keeps both for later calls
- * (lmieb_set_work_granularity, lmieb_set_pipeline).  Reports the choice and
- * the best wall time (ms) through the non-NULL pointers.  Returns 0 or -1. */
+ * orders per block of the user-angle phase matrix (128, 256, 512) by that
+ * stage's device time, then the pipeline depth (1, 2, 3, 4, 6 parts) by the
+ * wall time of the public batch call, and keeps all three for later calls
+ * (lmieb_set_work_granularity, lmieb_set_user_angle_part,
+ * lmieb_set_pipeline).  Reports the granularity, the pipeline depth and the
+ * best wall time (ms) through the non-NULL pointers.  Returns 0 or -1. */
 int lmie_solution_autotune(int n_cases, lmie_in_data *in, lmie_out_data *out, int n_threads, int precision,
                            int *best_chunks, double *best_items, double *best_ms);
 

@@ -45,6 +45,8 @@ def library() -> C.CDLL:
         lib.lmieb_set_split_segment.argtypes = [C.c_int]
         lib.lmieb_save_cache_stats.argtypes = [C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
         lib.lmieb_get_split_segment.argtypes = []
+        lib.lmieb_set_user_angle_part.argtypes = [C.c_int]
+        lib.lmieb_get_user_angle_part.argtypes = []
         abi.bind_group(lib)
         _lib = lib
     return _lib

@@ -168,6 +168,7 @@ int prec_slot(int precision) {
 // Orders (in chunks of TC_KC) per FP32 segment of the tensor-core stage's
 // hi*hi products; set by lmieb_set_split_segment.
 int g_tc_seg = 2;
+int g_pu_lp = PU_LP;     // orders per K5 block (lmieb_set_user_angle_part)
 
 // Radius sharing: the group lmie_solution(..., use_mpi != 0) shares its radii
 // with, and how the integrals are summed over it -- the caller's function, or
@@ -1261,7 +1262,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
             }
         }
         // K5: parts of PU_LP orders; the partial sums of a case of several
-        C.pu_parts = (L.pf_from && C.n_angles > 0) ? std::max(1, (C.n_coef + PU_LP - 1) / PU_LP) : 0;
+        C.pu_parts = (L.pf_from && C.n_angles > 0) ? std::max(1, (C.n_coef + g_pu_lp - 1) / g_pu_lp) : 0;
         C.pu_scr_off = pu_scr_total;
         const long long pu_n = (long long) ncol * 6 * C.n_angles;
         if (C.pu_parts > 1) pu_scr_total += C.pu_parts * pu_n;
@@ -1503,6 +1504,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     B.R = R;
     B.nd = nd; B.nd1 = nd1; B.nd2 = nd2;
     B.n1max = n1max; B.ncmax = ncmax;
+    B.pu_lp = g_pu_lp;
     B.cs = (const DevCase *) dptr(h_cs);
     B.idx1 = (const int *) dptr(h_i1);
     B.idx2 = (const int *) dptr(h_i2);
@@ -2515,6 +2517,22 @@ extern "C" int lmieb_set_split_segment(int chunks) {
     }
     g_tc_seg = chunks;
     return 0;
+}
+
+extern "C" int lmieb_set_user_angle_part(int orders) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    if (orders < PU_T || orders > 4096 || orders % PU_T) {
+        fprintf(stderr, "ERROR: lmieb_set_user_angle_part: %d orders (a multiple of %d, %d..4096)\n", orders, PU_T,
+                PU_T);
+        return -1;
+    }
+    g_pu_lp = orders;
+    return 0;
+}
+
+extern "C" int lmieb_get_user_angle_part(void) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    return g_pu_lp;
 }
 
 extern "C" int lmieb_get_split_segment(void) {

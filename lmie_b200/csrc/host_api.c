@@ -1094,10 +1094,36 @@ int lmie_solution_autotune(int n_cases, lmie_in_data *in, lmie_out_data *out, in
           }
      }
      lmieb_set_timing(keep_timing);
-     /* 2. pipeline depth: the overlap of host work with the device, by the
+     lmieb_set_work_granularity(precision, bi);
+     /* 2. orders per block of the phase matrix at the user angles (its tile
+      *    along the orders), by that stage's device time */
+     {
+          static const int part_c[] = {128, 256, 512};
+          int bp = lmieb_get_user_angle_part();
+          double bu = -1.;
+          g_pipeline = 1;
+          lmieb_set_timing(1);
+          for (b = 0; b < 3 && rc == 0; ++b) {
+               double d = -1.;
+               lmieb_set_user_angle_part(part_c[b]);
+               for (r = 0; r < 3 && rc == 0; ++r) {
+                    double st[LMIEB_N_STAGES];
+                    rc = lmie_solution_batch2(n_cases, in, out, 0, 0, n_threads, precision);
+                    lmieb_last_timing(st, LMIEB_N_STAGES);
+                    if (r > 0 && (d < 0. || st[7] < d))       /* stage 7: user angles */
+                         d = st[7];
+               }
+               if (rc == 0 && (bu < 0. || d < bu)) {
+                    bu = d;
+                    bp = part_c[b];
+               }
+          }
+          lmieb_set_timing(keep_timing);
+          lmieb_set_user_angle_part(bp);
+     }
+     /* 3. pipeline depth: the overlap of host work with the device, by the
       *    wall time of the public batch call (one call to settle the buffers,
       *    then the faster of two) */
-     lmieb_set_work_granularity(precision, bi);
      for (a = 0; a < 5 && rc == 0; ++a) {
           double t = -1.;
           if (chunk_c[a] > 1 && n_cases < 2 * chunk_c[a])

@@ -1329,7 +1329,7 @@ __global__ void k_exp_final(DevBatch B, long long total, const long long *__rest
 
 // ---------------------------------------------------------------------------
 // K5: phase matrix at the user's angles from the truncated expansion; one
-// block per (case, tile of PU_T user angles, part of PU_LP orders), one
+// block per (case, tile of PU_T user angles, part of B.pu_lp orders), one
 // thread per angle, cases with the most orders first.  A block runs the basis
 // recurrences from order 0 and sums the terms of its part's orders, so that a
 // case with many orders is spread over several blocks instead of one long
@@ -1357,8 +1357,8 @@ __global__ void __launch_bounds__(PU_T) k_phase_user(DevBatch B, const long long
     const bool act = a < na;
     const int nt = trunc[c] > 0 ? ncf - trunc[c] + 1 : ncf;
     // this block's orders [lbeg, lend); the tiles of PU_T orders before lbeg
-    // only advance the recurrences (PU_LP is a multiple of PU_T)
-    const int lbeg = part * PU_LP, lend = min(nt, lbeg + PU_LP);
+    // only advance the recurrences (pu_lp is a multiple of PU_T)
+    const int lbeg = part * B.pu_lp, lend = min(nt, lbeg + B.pu_lp);
     const double x = act ? B.mu_user[C.mu_user_off + a] : 0.;
     const double *cf0 = coefs + (KIND == 0 ? C.gc_off : C.lc_off);
     for (int g0 = 0; g0 < ncol; g0 += CG) {

@@ -42,7 +42,7 @@ struct DevCase {
     long long gc_off, lc_off;   // [ncol][6][n_coef] outputs
     long long pf_out_off;       // [ncol][6][n_angles] output (user angles)
     long long mu_user_off;      // user-angle cosines
-    int pu_parts;               // K5: parts of PU_LP orders (each angle tile's blocks)
+    int pu_parts;               // K5: parts of pu_lp orders (each angle tile's blocks)
     long long pu_scr_off;       // K5 with more than one part: its [part][ncol][6][n_angles] partial sums
     int scal_off;               // [ncol][4] normalised cross sections and g
     int G;                      // angular radius groups
@@ -58,6 +58,7 @@ struct DevBatch {
     int R;                      // radii over all cases
     int nd, nd1, nd2;           // derivative layout (uniform over the batch)
     int n1max, ncmax;           // largest n1 and n_coef (table lengths)
+    int pu_lp;                  // K5: orders per block (a multiple of PU_T)
     const DevCase *cs;          // [ncase]
     const int *idx1, *idx2;     // [nd1], [nd2]
     const cplx *m_l;            // [ncase * nd]
@@ -158,7 +159,7 @@ int launch_normalize(cudaStream_t s, const DevBatch &B, long long total, const l
 // with a truncation band d_l = C.trunc_band (2l + 1), band[2c] and band[2c+1]
 // get n_coef - l for the first l with |beta_l| <= accuracy + d_l and
 // <= accuracy - d_l.
-constexpr int PU_LP = 256;     // orders per K5 part (a multiple of PU_T)
+constexpr int PU_LP = 256;     // default orders per K5 block (a multiple of PU_T)
 constexpr int PU_T = 64;       // user angles per K5 block (and orders staged per step)
 constexpr int EX_LT = 32;       // orders per tile
 constexpr int EX_AT = 32;       // half-angles per tile
@@ -180,7 +181,7 @@ int launch_expand(cudaStream_t s, const DevBatch &B, int kind, long long nck,
 // kernels the GSF expansion launches before its finalisation for ncol columns
 int expand_gsf_launches(int ncol);
 
-// K5: block per (case, tile of PU_T user angles, part of PU_LP orders),
+// K5: block per (case, tile of PU_T user angles, part of B.pu_lp orders),
 // cases in K1's launch order (start: the blocks before each case in that
 // order); cases of several parts add them up from scr (red_start: flat
 // (case, column, element, angle) index space of those cases).

@@ -129,3 +129,19 @@ def test_slave_entry_reports_no_mpi():
     lib = libs.product()
     lib.lmie_solution_slave.restype = C.c_int
     assert lib.lmie_solution_slave() == -1
+
+
+def test_user_angle_part_argument_checks():
+    """Orders per block of the user-angle phase matrix: multiples of 64 from
+    64 to 4096 (no GPU needed to set it)."""
+    import ctypes as C
+    lib = libs.product()
+    lib.lmieb_set_user_angle_part.argtypes = [C.c_int]
+    keep = lib.lmieb_get_user_angle_part()
+    try:
+        for bad in (0, 32, 100, 4160, -64):
+            assert lib.lmieb_set_user_angle_part(bad) == -1, bad
+        assert lib.lmieb_get_user_angle_part() == keep
+        assert lib.lmieb_set_user_angle_part(128) == 0 and lib.lmieb_get_user_angle_part() == 128
+    finally:
+        lib.lmieb_set_user_angle_part(keep)

@@ -5,6 +5,7 @@ what the reference gives: the batch changes only how work is grouped on the
 device (radius groups, summation order), so results agree to the parity
 tolerance."""
 import dataclasses
+import math
 
 import numpy as np
 import pytest
@@ -141,6 +142,7 @@ def test_autotune_picks_a_candidate_and_keeps_results():
         assert got["pipeline_parts"] in (1, 2, 3, 4, 6)
         assert got["angular_items_per_sm"] in (32.0, 64.0, 128.0, 256.0)
         assert got["ms_per_call"] > 0
+        assert lib.lmieb_get_user_angle_part() in (128, 256, 512)
         after = abi.solve_batch(lib, cases, n_threads=4)
         for i, (a, r) in enumerate(zip(after, ref)):
             err = libs.compare(a, r)
@@ -149,6 +151,29 @@ def test_autotune_picks_a_candidate_and_keeps_results():
         lib.lmieb_set_pipeline(0)
         lib.lmieb_set_work_granularity(abi.PRECISION_FP64, keep)
         lib.lmieb_set_work_granularity(0, C.c_double(4.0))
+        lib.lmieb_set_user_angle_part(256)
+
+
+def test_user_angle_parts_only_reorder_sums():
+    """The phase matrix at the user angles with 64 orders per block (large
+    cases spread over many blocks whose sums are added in order) and with
+    4096 (every case in one block): the same values to round-off."""
+    import ctypes as C
+    lib = libs.product()
+    lib.lmieb_set_user_angle_part.argtypes = [C.c_int]
+    cases = [c for c in workloads.batched_uneven(96) if 2 * math.pi * c.r2 / c.lam > 100][:6]
+    assert len(cases) >= 3
+    try:
+        assert lib.lmieb_set_user_angle_part(64) == 0
+        many = abi.solve_batch(lib, cases, n_threads=4)
+        assert lib.lmieb_set_user_angle_part(4096) == 0
+        one = abi.solve_batch(lib, cases, n_threads=4)
+    finally:
+        lib.lmieb_set_user_angle_part(256)
+    for i, (a, b) in enumerate(zip(many, one)):
+        assert a.rc == 0 and b.rc == 0 and a.n_coef == b.n_coef, i
+        for name in ("pf", "pf_l"):
+            assert libs.relmax(getattr(a, name), getattr(b, name)) <= 1e-13, (i, name)
 
 
 def test_repeated_plan_is_replayed_as_a_graph():
