@@ -991,14 +991,18 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         for (size_t i = 0; i < tmp.size(); ++i) out[at[cls[i]]++] = tmp[i].second;
     };
     // coefficient offsets of the radii whose coefficients K1 writes in FP64
-    // (all radii, or with split precision those of the FP64 cases)
-    static std::vector<long long> coff;
-    coff.resize(R + 1);
-    coff[0] = 0;
-    for (int k = 0; k < ncase; ++k) {
-        const DevCase &C = cs[k];
-        for (int r = C.r0; r < C.r0 + C.nr; ++r) coff[r + 1] = coff[r] + (case_tc[k] ? 0 : n1r[r]);
+    // (all radii: the order offsets `off`; with split precision those of the
+    // FP64 cases)
+    static std::vector<long long> coff_tc;
+    if (L.tc) {
+        coff_tc.resize(R + 1);
+        coff_tc[0] = 0;
+        for (int k = 0; k < ncase; ++k) {
+            const DevCase &C = cs[k];
+            for (int r = C.r0; r < C.r0 + C.nr; ++r) coff_tc[r + 1] = coff_tc[r] + (case_tc[k] ? 0 : n1r[r]);
+        }
     }
+    const std::vector<long long> &coff = L.tc ? coff_tc : off;
     // split precision: radius groups of tc_rg(nd1) radii, each with its B operand block
     static std::vector<int> tc_pos;
     static std::vector<long long> tc_roff;
@@ -1076,11 +1080,52 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     if (L.oz) {
         const int RG = oz_rg(nd1);
         std::vector<int> cg0(ncase + 1, 0);
+        std::vector<long long> cb0(ncase + 1, 0);     // B operand chunks before each case
         std::vector<double> wc(ncase, 0.);
+        // per case, in parallel: its groups of RG radii and their chunks
+        parallel_for(ncase, 64, [&](int k) {
+            const DevCase &C = cs[k];
+            if (!case_oz[k]) return;
+            long long ch = 0;
+            for (int r = C.r0; r < C.r0 + C.nr; r += RG) {
+                const int n = std::min(RG, C.r0 + C.nr - r);
+                int mx = 1;
+                for (int i = 0; i < n; ++i) mx = std::max(mx, n1r[r + i]);
+                ch += (mx + OZ_KC - 1) / OZ_KC;
+            }
+            cg0[k + 1] = (C.nr + RG - 1) / RG;
+            cb0[k + 1] = ch;
+            wc[k] = (double) (ch + cg0[k + 1]);       // chunks, plus one per group for its epilogue
+        });
+        for (int k = 0; k < ncase; ++k) {
+            cg0[k + 1] += cg0[k];
+            cb0[k + 1] += cb0[k];
+        }
+        tg_r0.resize(cg0[ncase]);
+        tg_n.resize(cg0[ncase]);
+        tg_nk.resize(cg0[ncase]);
+        tg_off.resize(cg0[ncase]);
+        parallel_for(ncase, 64, [&](int k) {
+            const DevCase &C = cs[k];
+            if (!case_oz[k]) return;
+            int g = cg0[k];
+            long long o = cb0[k] * OZ_BSTAGE;
+            for (int r = C.r0; r < C.r0 + C.nr; r += RG, ++g) {
+                const int n = std::min(RG, C.r0 + C.nr - r);
+                int mx = 1;
+                for (int i = 0; i < n; ++i) mx = std::max(mx, n1r[r + i]);
+                const int nk = (mx + OZ_KC - 1) / OZ_KC;
+                tg_r0[g] = r;
+                tg_n[g] = n;
+                tg_nk[g] = nk;
+                tg_off[g] = o;
+                o += (long long) nk * OZ_BSTAGE;
+            }
+        });
+        bop8_bytes = cb0[ncase] * OZ_BSTAGE;
         double W = 0.;
         for (int k = 0; k < ncase; ++k) {
             DevCase &C = cs[k];
-            cg0[k] = (int) tg_r0.size();
             rx_start[k + 1] = rx_start[k];
             a_start[k + 1] = a_start[k];
             if (!case_oz[k]) continue;
@@ -1095,21 +1140,8 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
             aop_bytes += (long long) ntile * C.nkx * OZ_ACHUNK;
             a_start[k + 1] += (long long) ntile * OZ_M;
             nkx_all = std::max(nkx_all, C.nkx);
-            for (int r = C.r0; r < C.r0 + C.nr; r += RG) {
-                const int n = std::min(RG, C.r0 + C.nr - r);
-                int mx = 1;
-                for (int i = 0; i < n; ++i) mx = std::max(mx, n1r[r + i]);
-                const int nk = (mx + OZ_KC - 1) / OZ_KC;
-                tg_r0.push_back(r);
-                tg_n.push_back(n);
-                tg_nk.push_back(nk);
-                tg_off.push_back(bop8_bytes);
-                bop8_bytes += (long long) nk * OZ_BSTAGE;
-                wc[k] += nk + 1;                       // chunks, plus one for the group's epilogue
-            }
             W += wc[k] * ((C.nh + OZ_HALF - 1) / OZ_HALF);
         }
-        cg0[ncase] = (int) tg_r0.size();
         L.n_groups = (int) tg_r0.size();
         L.n_rx = rx_start[ncase];
         L.n_arow = a_start[ncase];
