@@ -76,6 +76,12 @@ struct Slot {
     size_t hcap = 0;
     Plan *plan = nullptr;
     cudaStream_t stream = nullptr;     // the sub-batches of this slot (consecutive ones overlap)
+    // The copies of the results run on a stream of their own: a stream whose
+    // last operation was a device-to-host copy queues its next commands (the
+    // next upload included) behind every download in flight, those of the
+    // other slots too.
+    cudaStream_t down = nullptr;
+    cudaEvent_t kdone = nullptr;       // after the sub-batch's kernels (the downloads wait for it)
     cudaEvent_t done = nullptr;
     cudaEvent_t piece[MAX_PIECES] = {};  // after the copy of each piece of the results
     cudaEvent_t t_begin = nullptr, t_end = nullptr;   // device span of the sub-batch
@@ -398,6 +404,8 @@ int ensure_ready() {
         S.plan = new Plan();
         LMIEB_CUDA_TRY(cudaStreamCreateWithPriority(&S.stream, cudaStreamNonBlocking,
                                                     &S == &c.slot[2] ? prio_hi : prio_lo));
+        LMIEB_CUDA_TRY(cudaStreamCreateWithFlags(&S.down, cudaStreamNonBlocking));
+        LMIEB_CUDA_TRY(cudaEventCreateWithFlags(&S.kdone, cudaEventDisableTiming));
         LMIEB_CUDA_TRY(cudaEventCreateWithFlags(&S.done, cudaEventDisableTiming));
         for (cudaEvent_t &e : S.piece) LMIEB_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         LMIEB_CUDA_TRY(cudaEventCreate(&S.t_begin));
@@ -1653,6 +1661,8 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     if (c.submits == 1) LMIEB_CUDA_TRY(cudaEventRecord(c.t_first, s));
     LMIEB_CUDA_TRY(fault_injected("h2d") ? cudaErrorInvalidValue
                                          : cudaMemcpyAsync(d_in, hp, h_in_end, cudaMemcpyHostToDevice, s));
+    // the slot's previous results must have left the output block
+    if (!c.timing) LMIEB_CUDA_TRY(cudaStreamWaitEvent(s, S.done, 0));
     LMIEB_CUDA_TRY(cudaMemsetAsync(d_out, 0, out_bytes, s));
     // Gauss-angle pool entries another sub-batch is still computing
     if (c.gl_pending) LMIEB_CUDA_TRY(cudaStreamWaitEvent(s, c.gl_ready, 0));
@@ -1722,10 +1732,16 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     // save_control kernels, integrals), then per piece its slices of the
     // cross sections, expansions and phase matrices.
     std::vector<int> piece(1, 0);
+    cudaStream_t ds = s;
+    if (!c.timing) {
+        ds = S.down;
+        LMIEB_CUDA_TRY(cudaEventRecord(S.kdone, s));
+        LMIEB_CUDA_TRY(cudaStreamWaitEvent(ds, S.kdone, 0));
+    }
     {
         const char *misc = (const char *) L.o_trunc;
         const size_t moff = (size_t) (misc - d_out);
-        LMIEB_CUDA_TRY(cudaMemcpyAsync(h_out + moff, misc, out_bytes - moff, cudaMemcpyDeviceToHost, s));
+        LMIEB_CUDA_TRY(cudaMemcpyAsync(h_out + moff, misc, out_bytes - moff, cudaMemcpyDeviceToHost, ds));
         const int np = (int) std::max<size_t>(1, std::min<size_t>(MAX_PIECES, out_bytes / PIECE_BYTES));
         const double per = (double) (o_scal + o_gc + o_lc + o_pf) / np;
         double run = 0.;
@@ -1744,7 +1760,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         auto down = [&](double *base, size_t a, size_t b) -> cudaError_t {
             if (b <= a) return cudaSuccess;
             const size_t off = (size_t) ((char *) (base + a) - d_out);
-            return cudaMemcpyAsync(h_out + off, base + a, (b - a) * 8, cudaMemcpyDeviceToHost, s);
+            return cudaMemcpyAsync(h_out + off, base + a, (b - a) * 8, cudaMemcpyDeviceToHost, ds);
         };
         for (size_t p = 0; p + 1 < piece.size(); ++p) {
             size_t s0, g0, l0, f0, s1, g1, l1, f1;
@@ -1754,12 +1770,12 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
             LMIEB_CUDA_TRY(down(L.o_gc, g0, g1));
             LMIEB_CUDA_TRY(down(L.o_lc, l0, l1));
             LMIEB_CUDA_TRY(down(L.o_pf, f0, f1));
-            LMIEB_CUDA_TRY(cudaEventRecord(S.piece[p], s));
+            LMIEB_CUDA_TRY(cudaEventRecord(S.piece[p], ds));
         }
     }
     stage(NSTAGE);
-    LMIEB_CUDA_TRY(cudaEventRecord(S.t_end, s));
-    LMIEB_CUDA_TRY(cudaEventRecord(S.done, s));
+    LMIEB_CUDA_TRY(cudaEventRecord(S.t_end, ds));
+    LMIEB_CUDA_TRY(cudaEventRecord(S.done, ds));
     S.have_plan = true;
     c.last_slot = (int) (&S - c.slot);
 

@@ -324,8 +324,13 @@ typedef struct {
      int rc;
      int n, nd, n_coef_all;
      double *qx, *qw, *nr, *qx_l, *qw_l, *nr_l;
-     double *x, *xl, *w, *w2, *mu_user, *sv1, *sv2, *dev_out;
+     double *x, *xl, *w, *w2, *mu_user, *dev_out;
      double **rows;             /* the caller's output rows, in device column order */
+     /* every array above comes out of one zeroed block (a second one holds
+        this process's share of the radii): a case's scratch is released
+        with one or two free() calls, not one per array */
+     char *blk, *blk2, *blk_at;
+     size_t blk_size, blk_left;
      int *n1r, *n2r, *idx1, *idx2;
      /* radius sharing (lmieb.h): the mode and this process's share */
      int acc_mode, share_rank, share_world;
@@ -335,15 +340,104 @@ typedef struct {
      lmieb_result R;
 } case_job;
 
+/* Released case blocks, kept by size class (powers of two from 4 KB) for the
+ * cases of later calls: returning them to the C heap gave the pages back to
+ * the system, and the next call's allocations faulted them in again (about
+ * a microsecond per case on each side).  At most BLK_POOL_MAX bytes stay.
+ * Each class is a stack of pointers, so that a release does not touch the
+ * block itself; a batch releases its cases under one lock. */
+#define BLK_CLASSES 20
+#define BLK_POOL_MAX ((size_t) 1 << 30)
+typedef struct {
+     char **p;
+     int n, cap;
+} blk_stack;
+static pthread_mutex_t blk_mu = PTHREAD_MUTEX_INITIALIZER;
+static blk_stack blk_pool[BLK_CLASSES];
+static size_t blk_pooled;
+
+static int blk_class(size_t bytes) {
+     int c = 0;
+     while (c < BLK_CLASSES && ((size_t) 4096 << c) < bytes)
+          ++c;
+     return c;
+}
+
+/* A zeroed block of at least `bytes` (a pooled one when there is one). */
+static char *blk_get(size_t bytes) {
+     const int c = blk_class(bytes);
+     char *p = NULL;
+     if (c == BLK_CLASSES)
+          return (char *) calloc(1, bytes);
+     pthread_mutex_lock(&blk_mu);
+     if (blk_pool[c].n > 0) {
+          p = blk_pool[c].p[--blk_pool[c].n];
+          blk_pooled -= (size_t) 4096 << c;
+     }
+     pthread_mutex_unlock(&blk_mu);
+     if (!p)
+          return (char *) calloc(1, (size_t) 4096 << c);
+     memset(p, 0, bytes);
+     return p;
+}
+
+/* Keeps the block in the pool; 0 when it must go back to the heap instead
+   (its class too large, the pool full).  Called with blk_mu held. */
+static int blk_keep(char *p, size_t bytes) {
+     const int c = blk_class(bytes);
+     blk_stack *st;
+     if (c == BLK_CLASSES || blk_pooled + ((size_t) 4096 << c) > BLK_POOL_MAX)
+          return 0;
+     st = &blk_pool[c];
+     if (st->n == st->cap) {
+          const int cap = st->cap ? 2 * st->cap : 256;
+          char **q = (char **) realloc(st->p, (size_t) cap * sizeof(char *));
+          if (!q)
+               return 0;
+          st->p = q;
+          st->cap = cap;
+     }
+     st->p[st->n++] = p;
+     blk_pooled += (size_t) 4096 << c;
+     return 1;
+}
+
+/* Releases the scratch of one case (idempotent). */
 static void job_free(case_job *j) {
-     free(j->qx); free(j->qw); free(j->nr); free(j->qx_l); free(j->qw_l); free(j->nr_l);
-     free(j->x); free(j->xl); free(j->w); free(j->w2); free(j->mu_user);
-     free(j->n1r); free(j->n2r); free(j->idx1); free(j->idx2); free(j->dev_out);
-     free(j->sv1); free(j->sv2); free(j->rows);
+     if (j->blk) {
+          int kept;
+          pthread_mutex_lock(&blk_mu);
+          kept = blk_keep(j->blk, j->blk_size);
+          pthread_mutex_unlock(&blk_mu);
+          if (!kept)
+               free(j->blk);
+     }
+     free(j->blk2);
+     j->blk = j->blk2 = j->blk_at = NULL;
+     j->blk_size = j->blk_left = 0;
      j->rows = NULL;
      j->qx = j->qw = j->nr = j->qx_l = j->qw_l = j->nr_l = NULL;
-     j->x = j->xl = j->w = j->w2 = j->mu_user = j->dev_out = j->sv1 = j->sv2 = NULL;
+     j->x = j->xl = j->w = j->w2 = j->mu_user = j->dev_out = NULL;
      j->n1r = j->n2r = j->idx1 = j->idx2 = NULL;
+}
+
+/* bytes one array of the block takes (16-byte aligned; at least 16, as an
+   empty array is still a valid pointer) */
+static size_t blk_round(size_t bytes) {
+     return bytes ? (bytes + 15) & ~(size_t) 15 : 16;
+}
+
+/* The next `bytes` of the case's block (zeroed), or NULL when the block the
+   case was sized for is used up. */
+static void *job_take(case_job *j, size_t bytes) {
+     void *p;
+     bytes = blk_round(bytes);
+     if (!j->blk_at || bytes > j->blk_left)
+          return NULL;
+     p = j->blk_at;
+     j->blk_at += bytes;
+     j->blk_left -= bytes;
+     return p;
 }
 
 /* Keeps radius i of a prepared case when i % share_world == share_rank (the
@@ -354,9 +448,14 @@ static int share_radii(case_job *j, int n, int nd, int nd1) {
      const int w = j->share_world, r0 = j->share_rank;
      const int m = j->acc_mode == LMIEB_ACC_FINISH ? 0 : (n > r0 ? (n - r0 + w - 1) / w : 0);
      const size_t mm = m > 0 ? (size_t) m : 1;
-     double *x = lmieb_arr1(mm), *xl = lmieb_arr1(mm * (nd1 > 0 ? nd1 : 1)), *wt = lmieb_arr1(mm * (1 + nd));
-     int *n1r = (int *) calloc(mm, sizeof(int)), *n2r = (int *) calloc(mm, sizeof(int));
+     const size_t bx = blk_round(mm * 8), bxl = blk_round(mm * (nd1 > 0 ? nd1 : 1) * 8);
+     const size_t bw = blk_round(mm * (1 + nd) * 8), bn = blk_round(mm * 4);
+     char *b = (char *) calloc(1, bx + bxl + bw + 2 * bn);
+     double *x = (double *) b, *xl = (double *) (b + bx), *wt = (double *) (b + bx + bxl);
+     int *n1r = (int *) (b + bx + bxl + bw), *n2r = (int *) (b + bx + bxl + bw + bn);
      int t, k;
+     if (!b)
+          return -1;
      for (t = 0; t < m; ++t) {
           const int i = r0 + t * w;
           x[t] = j->x[i];
@@ -367,7 +466,8 @@ static int share_radii(case_job *j, int n, int nd, int nd1) {
           for (k = 0; k <= nd; ++k)
                wt[(size_t) k * m + t] = j->w[(size_t) k * n + i];
      }
-     free(j->x); free(j->xl); free(j->w); free(j->n1r); free(j->n2r);
+     free(j->blk2);
+     j->blk2 = b;
      j->x = x; j->xl = xl; j->w = wt; j->n1r = n1r; j->n2r = n2r;
      return m;
 }
@@ -438,14 +538,31 @@ static int job_prepare(case_job *j) {
           return -1;
      }
      j->n = n;
+     {
+          /* the block: every array below at its largest (the Mie split nd1 <= nd) */
+          const size_t un = (size_t) n, und = (size_t) (nd > 0 ? nd : 1), ncol1 = (size_t) (1 + nd);
+          const size_t bytes = 3 * blk_round(un * 8) + 3 * blk_round(un * nd * 8) + 2 * blk_round(und * 4) +
+                               blk_round(un * 8) + blk_round(un * und * 8) + blk_round(un * ncol1 * 8) +
+                               2 * blk_round(un * 4) +
+                               (j->save_control == 2 ? blk_round(un * und * 8) : 0) +
+                               (j->calc_pf && j->n_angles > 0 ? blk_round((size_t) j->n_angles * 8) : 0) +
+                               blk_round(ncol1 * 4 * 8) + blk_round(3 * ncol1 * 6 * sizeof(double *));
+          j->blk = blk_get(bytes);
+          if (!j->blk) {
+               fprintf(stderr, "ERROR: lmie_b200: out of host memory for a case's scratch\n");
+               return -1;
+          }
+          j->blk_at = j->blk;
+          j->blk_size = j->blk_left = bytes;
+     }
 
      /* size distribution quadrature and moments */
-     j->qx = lmieb_arr1(n);
-     j->qw = lmieb_arr1(n);
-     j->nr = lmieb_arr1(n);
-     j->qx_l = lmieb_arr1((size_t) n * nd);
-     j->qw_l = lmieb_arr1((size_t) n * nd);
-     j->nr_l = lmieb_arr1((size_t) n * nd);
+     j->qx = (double *) job_take(j, (size_t) n * 8);
+     j->qw = (double *) job_take(j, (size_t) n * 8);
+     j->nr = (double *) job_take(j, (size_t) n * 8);
+     j->qx_l = (double *) job_take(j, (size_t) n * nd * 8);
+     j->qw_l = (double *) job_take(j, (size_t) n * nd * 8);
+     j->nr_l = (double *) job_take(j, (size_t) n * nd * 8);
      memset(&din, 0, sizeof(din));
      din.dist_type = j->dist_type; din.n_int1 = j->n_int1; din.n_int2 = j->n_int2;
      din.n_quad = j->n_quad; din.nd = nd;
@@ -470,8 +587,8 @@ static int job_prepare(case_job *j) {
      *j->vavg = mom.vavg; *j->ravg = mom.ravg; *j->rvw = mom.rvw;
 
      /* derivative split (reference src/lmie_interface.c:304-353) */
-     j->idx1 = (int *) calloc(nd > 0 ? nd : 1, sizeof(int));
-     j->idx2 = (int *) calloc(nd > 0 ? nd : 1, sizeof(int));
+     j->idx1 = (int *) job_take(j, (size_t) (nd > 0 ? nd : 1) * 4);
+     j->idx2 = (int *) job_take(j, (size_t) (nd > 0 ? nd : 1) * 4);
      for (i = 0; i < nd; ++i) {
           if (j->lambda_l[i] != 0. || j->mr_l[i] != 0. || j->mi_l[i] != 0. ||
               j->r21_l[i] != 0. || j->r22_l[i] != 0.)
@@ -489,11 +606,11 @@ static int job_prepare(case_job *j) {
 
      /* per-radius size parameters, truncation and weights
       * (reference src/lmie_core.c:263-292) */
-     j->x = lmieb_arr1(n);
-     j->xl = lmieb_arr1((size_t) n * (nd1 > 0 ? nd1 : 1));
-     j->w = lmieb_arr1((size_t) n * (1 + nd));
-     j->n1r = (int *) calloc(n, sizeof(int));
-     j->n2r = (int *) calloc(n, sizeof(int));
+     j->x = (double *) job_take(j, (size_t) n * 8);
+     j->xl = (double *) job_take(j, (size_t) n * (nd > 0 ? nd : 1) * 8);
+     j->w = (double *) job_take(j, (size_t) n * (1 + nd) * 8);
+     j->n1r = (int *) job_take(j, (size_t) n * 4);
+     j->n2r = (int *) job_take(j, (size_t) n * 4);
      for (i = 0; i < n; ++i) {
           double x = 2. * M_PI * j->qx[i] / j->lambda;
           double complex z = m * x;
@@ -530,6 +647,10 @@ static int job_prepare(case_job *j) {
                return -1;
           }
           n = share_radii(j, n, nd, nd1);
+          if (n < 0) {
+               fprintf(stderr, "ERROR: lmie_b200: out of host memory for a case's scratch\n");
+               return -1;
+          }
      }
 
      /* save_control: allocate / gather the per-radius kernels */
@@ -543,7 +664,7 @@ static int job_prepare(case_job *j) {
                        "save_control = 1 call\n");
                return -1;
           }
-          j->w2 = lmieb_arr1((size_t) n * (nd > 0 ? nd : 1));
+          j->w2 = (double *) job_take(j, (size_t) n * (nd > 0 ? nd : 1) * 8);
           for (i = 0; i < n; ++i)
                for (k = 0; k < nd2; ++k) {
                     int kk = j->idx2[k];
@@ -562,7 +683,7 @@ static int job_prepare(case_job *j) {
                j->theta[i] = i * d;
           mu_user = user_cosines(j->n_angles);
           if (!mu_user) {
-               j->mu_user = lmieb_arr1(j->n_angles);
+               j->mu_user = (double *) job_take(j, (size_t) j->n_angles * 8);
                user_cosines_fill(j->n_angles, j->mu_user);
                mu_user = j->mu_user;
           }
@@ -592,10 +713,10 @@ static int job_prepare(case_job *j) {
      /* results: the scalars in a small staging array, the expansions and the
         phase matrix straight into the caller's rows */
      ncol = 1 + nd;
-     j->dev_out = lmieb_arr1((size_t) ncol * 4);
+     j->dev_out = (double *) job_take(j, (size_t) ncol * 4 * 8);
      memset(&j->R, 0, sizeof(j->R));
      j->R.scal = j->dev_out;
-     j->rows = (double **) calloc((size_t) 3 * ncol * 6, sizeof(double *));
+     j->rows = (double **) job_take(j, (size_t) 3 * ncol * 6 * sizeof(double *));
      for (k = 0; k < ncol * 6; ++k) {
           const int col = k / 6, e = k % 6;
           if (j->P.want_gc)
@@ -748,15 +869,13 @@ static void job_stage(void *arg, int i) {
      if (p->stage == 0) {
           job_from_struct(&p->jobs[i], &p->in[i], &p->out[i], p->verbose);
           p->jobs[i].rc = job_prepare(&p->jobs[i]);
-     } else if (p->stage == 2) {
-          job_free(&p->jobs[i]);
      } else if (p->jobs[i].rc == 0) {
           job_finish(&p->jobs[i]);
      }
 }
 
-/* Runs stage 0 (set up from in/out and prepare), 1 (finish) or 2 (release
- * the host scratch) of every job on up to n_threads host threads. */
+/* Runs stage 0 (set up from in/out and prepare) or 1 (finish) of every job
+ * on up to n_threads host threads. */
 static void run_jobs_io(case_job *jobs, lmie_in_data *in, lmie_out_data *out, int verbose, int n, int stage,
                         int n_threads) {
      job_pool p;
@@ -766,6 +885,19 @@ static void run_jobs_io(case_job *jobs, lmie_in_data *in, lmie_out_data *out, in
 
 static void run_jobs(case_job *jobs, int n, int stage, int n_threads) {
      run_jobs_io(jobs, NULL, NULL, 0, n, stage, n_threads);
+}
+
+/* Releases the host scratch of jobs[0..n) on the calling thread: the blocks
+ * go to the pool under one lock (job_free is idempotent). */
+static void jobs_release(case_job *jobs, int n) {
+     int i;
+     pthread_mutex_lock(&blk_mu);
+     for (i = 0; i < n; ++i)
+          if (jobs[i].blk && blk_keep(jobs[i].blk, jobs[i].blk_size))
+               jobs[i].blk = NULL;
+     pthread_mutex_unlock(&blk_mu);
+     for (i = 0; i < n; ++i)
+          job_free(&jobs[i]);
 }
 
 /* Two prepared cases can share a device batch when their derivative layout
@@ -899,7 +1031,7 @@ static int finish_chunk(chunk_tickets *ct, case_job *jobs, int j0, int j1, const
      }
      /* the chunk's host scratch is no longer referenced: released here, while
         the device still works on the next chunk */
-     run_jobs(jobs + j0, j1 - j0, 2, n_threads);
+     jobs_release(jobs + j0, j1 - j0);
      ct->n = 0;
      return rc;
 }
@@ -1038,7 +1170,7 @@ int lmie_solution_batch2(int n_cases, lmie_in_data *in, lmie_out_data *out, int 
      lmieb_host_phase(0, t_prep);
      lmieb_host_phase(4, t_fin);
      if (rc != 0)      /* chunks given up before their finish (job_free is idempotent) */
-          run_jobs(jobs, prepared, 2, n_threads);
+          jobs_release(jobs, prepared);
      free(bnd);
      for (c = 0; c < 2; ++c) {
           free(tk[c]); free(tb[c]); free(te[c]);
