@@ -205,18 +205,32 @@ __global__ void __launch_bounds__(64) k_mie(DevBatch B, int c0, int write_value,
     }
 
     // ---- downward sweeps: checkpoints only ----
+    // Two independent chains: D_n from n2 and the psi ratio from n1 (n2 > n1).
+    // Below n1 they advance in the same loop, so that the dependent steps of
+    // one fill the latency of the other; each chain's arithmetic and order
+    // are those of a sweep of its own.
     {
         cplx D = mk(0., 0.), Dl[NC > 0 ? NC : 1];
+        double rn = 0., rl[NC > 0 ? NC : 1];
 #pragma unroll
-        for (int k = 0; k < NC; ++k) Dl[k] = mk(0., 0.);
-        for (int c = 0; c < nb; ++c)
+        for (int k = 0; k < NC; ++k) {
+            Dl[k] = mk(0., 0.);
+            rl[k] = 0.;
+        }
+        for (int c = 0; c < nb; ++c) {
+            double *q = ckr + (size_t) c * CW;
             if (c * K1_B + K1_B >= n2) {
-                double *q = ckr + (size_t) c * CW;
                 q[0] = q[1] = 0.;
 #pragma unroll
                 for (int k = 0; k < NC; ++k) q[2 + 2 * k] = q[3 + 2 * k] = 0.;
             }
-        for (int j = n2 - 1; j >= 1; --j) {
+            if (c * K1_B + K1_B >= n1) {
+                q[2 + 2 * NC] = 0.;
+#pragma unroll
+                for (int k = 0; k < NC; ++k) q[3 + 2 * NC + k] = 0.;
+            }
+        }
+        auto d_step = [&](int j) {
             const cplx c1 = (j + 1.) * zinv;
             const cplx ic2 = cinv(D + c1);
             D = c1 - ic2;
@@ -239,20 +253,8 @@ __global__ void __launch_bounds__(64) k_mie(DevBatch B, int c0, int write_value,
                     q[3 + 2 * k] = Dl[k].im;
                 }
             }
-        }
-    }
-    {
-        double rn = 0., rl[NC > 0 ? NC : 1];
-#pragma unroll
-        for (int k = 0; k < NC; ++k) rl[k] = 0.;
-        for (int c = 0; c < nb; ++c)
-            if (c * K1_B + K1_B >= n1) {
-                double *q = ckr + (size_t) c * CW + 2 + 2 * NC;
-                q[0] = 0.;
-#pragma unroll
-                for (int k = 0; k < NC; ++k) q[1 + k] = 0.;
-            }
-        for (int j = n1 - 1; j >= 1; --j) {
+        };
+        auto r_step = [&](int j) {
             const double a1 = (2. * j + 1.) * xinv;
             const double rnew = 1. / (a1 - rn);
             if (NC > 0) {
@@ -267,6 +269,11 @@ __global__ void __launch_bounds__(64) k_mie(DevBatch B, int c0, int write_value,
 #pragma unroll
                 for (int k = 0; k < NC; ++k) q[1 + k] = rl[k];
             }
+        };
+        for (int j = n2 - 1; j >= n1; --j) d_step(j);
+        for (int j = n1 - 1; j >= 1; --j) {
+            d_step(j);
+            r_step(j);
         }
     }
 
@@ -308,7 +315,9 @@ __global__ void __launch_bounds__(64) k_mie(DevBatch B, int c0, int write_value,
     for (int c = 0; c < nb; ++c) {
         const int lo = c * K1_B + 1, hi = min(c * K1_B + K1_B, n1);
         const double *q = ckr + (size_t) c * CW;
-        // replay D, D_l from the block's top (t <= n2) down to lo
+        // replay D, D_l from the block's top (t <= n2) and the psi ratio and
+        // its tangents from hi (t >= hi) down to lo: one loop below hi, as in
+        // the downward sweeps
         {
             const int t = min(c * K1_B + K1_B, n2);
             cplx D = mk(q[0], q[1]), Dl[NC > 0 ? NC : 1];
@@ -319,7 +328,14 @@ __global__ void __launch_bounds__(64) k_mie(DevBatch B, int c0, int write_value,
 #pragma unroll
                 for (int k = 0; k < NC; ++k) Dlloc[k][t - lo] = Dl[k];
             }
-            for (int j = t - 1; j >= lo; --j) {
+            const double *qr = q + 2 + 2 * NC;
+            double rn = qr[0], rl[NC > 0 ? NC : 1];
+#pragma unroll
+            for (int k = 0; k < NC; ++k) rl[k] = qr[1 + k];
+            rloc[hi - lo] = rn;
+#pragma unroll
+            for (int k = 0; k < NC; ++k) rlloc[k][hi - lo] = rl[k];
+            auto d_step = [&](int j) {
                 const cplx c1 = (j + 1.) * zinv;
                 const cplx ic2 = cinv(D + c1);
                 D = c1 - ic2;
@@ -337,18 +353,8 @@ __global__ void __launch_bounds__(64) k_mie(DevBatch B, int c0, int write_value,
 #pragma unroll
                     for (int k = 0; k < NC; ++k) Dlloc[k][j - lo] = Dl[k];
                 }
-            }
-        }
-        // replay the psi ratio and its tangents from the block's top (t = hi) down to lo
-        {
-            const double *qr = q + 2 + 2 * NC;
-            double rn = qr[0], rl[NC > 0 ? NC : 1];
-#pragma unroll
-            for (int k = 0; k < NC; ++k) rl[k] = qr[1 + k];
-            rloc[hi - lo] = rn;
-#pragma unroll
-            for (int k = 0; k < NC; ++k) rlloc[k][hi - lo] = rl[k];
-            for (int j = hi - 1; j >= lo; --j) {
+            };
+            auto r_step = [&](int j) {
                 const double a1 = (2. * j + 1.) * xinv;
                 const double rnew = 1. / (a1 - rn);
                 if (NC > 0) {
@@ -360,6 +366,11 @@ __global__ void __launch_bounds__(64) k_mie(DevBatch B, int c0, int write_value,
                 rloc[j - lo] = rn;
 #pragma unroll
                 for (int k = 0; k < NC; ++k) rlloc[k][j - lo] = rl[k];
+            };
+            for (int j = t - 1; j >= hi; --j) d_step(j);
+            for (int j = hi - 1; j >= lo; --j) {
+                d_step(j);
+                r_step(j);
             }
         }
         for (int j = lo; j <= hi; ++j) {
