@@ -20,8 +20,11 @@ struct GatherSeg {
     long long dst_off, n;
     int which;
 };
-// K1 keeps its downward recurrences at the top of every block of K1_B orders.
-constexpr int K1_B = 16;
+// K1 keeps its downward recurrences at the top of every block of K1_B orders
+// and replays a block into per-thread arrays of K1_B entries: with 8 they stay
+// in L1 at four blocks of 64 threads per SM (16: 3.9 ms of K1 on the
+// 4096-case batch, 8: 3.7 ms, 4: 3.7 ms).
+constexpr int K1_B = 8;
 // doubles per checkpoint block of a chunk of nc tangent-linear columns
 __host__ __device__ constexpr int k1_ck_width(int nc) { return 3 + 3 * nc; }
 
