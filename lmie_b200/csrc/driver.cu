@@ -1199,14 +1199,17 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
             wc[k] = (double) (cs1[k + 1] - cs1[k]) * cs[k].nh;
             W += wc[k];
         }
-        const double wt = std::max(W / (g_items_per_sm[0] * c.sms), 64. * 2 * 64 * 16);   // work per block
+        // work per block; in a tensor-core batch these are the cases under 16
+        // orders (a few half-angles, up to ~2000 radii each), whose blocks
+        // would otherwise walk all their radii one after the other
+        const double wt = std::max(W / (g_items_per_sm[0] * c.sms), (L.tc || L.oz) ? 4096. : 64. * 2 * 64 * 16);
         std::vector<std::pair<double, AngItem>> tmp;
         for (int k = 0; k < ncase; ++k) {
             DevCase &C = cs[k];
             if (C.n_qang <= 0 || case_tc[k] || case_oz[k]) continue;
             const int xt = (C.nh + per - 1) / per;
             int G = (int) std::lround(wc[k] / (xt * wt));
-            G = std::max(1, std::min(G, C.nr));
+            G = std::max(1, std::min(G, (L.tc || L.oz) ? std::min(C.nr, 64) : C.nr));
             std::vector<int> gs(G + 1, C.r0 + C.nr);
             gs[0] = C.r0;
             const long long o0 = off[C.r0], ot = off[C.r0 + C.nr] - o0;
