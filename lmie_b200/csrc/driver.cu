@@ -82,6 +82,10 @@ struct Slot {
     // other slots too.
     cudaStream_t down = nullptr;
     cudaEvent_t kdone = nullptr;       // after the sub-batch's kernels (the downloads wait for it)
+    // int8 K3's A operand and row exponents depend on the angles only: they
+    // run on this stream beside K1 (fork and join events)
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
     cudaEvent_t done = nullptr;
     cudaEvent_t piece[MAX_PIECES] = {};  // after the copy of each piece of the results
     cudaEvent_t t_begin = nullptr, t_end = nullptr;   // device span of the sub-batch
@@ -333,6 +337,8 @@ struct Plan {
     AngItem *ang64 = nullptr;   // with tc: FP64 K3 items of the cases kept off the tensor cores
     int n_ang64 = 0;
     int tc = 0;                 // K3 in split precision on the tensor cores
+    cudaStream_t side = nullptr;       // the slot's side stream and its fork / join events
+    cudaEvent_t fork = nullptr, join = nullptr;
     int tc_seg = 2;             // its segment length (chunks)
     float *bop = nullptr;       // its B operand (tc_layout.cuh)
     size_t bop_bytes = 0;
@@ -405,6 +411,10 @@ int ensure_ready() {
         LMIEB_CUDA_TRY(cudaStreamCreateWithPriority(&S.stream, cudaStreamNonBlocking,
                                                     &S == &c.slot[2] ? prio_hi : prio_lo));
         LMIEB_CUDA_TRY(cudaStreamCreateWithFlags(&S.down, cudaStreamNonBlocking));
+        LMIEB_CUDA_TRY(cudaStreamCreateWithPriority(&S.side, cudaStreamNonBlocking,
+                                                    &S == &c.slot[2] ? prio_hi : prio_lo));
+        LMIEB_CUDA_TRY(cudaEventCreateWithFlags(&S.fork, cudaEventDisableTiming));
+        LMIEB_CUDA_TRY(cudaEventCreateWithFlags(&S.join, cudaEventDisableTiming));
         LMIEB_CUDA_TRY(cudaEventCreateWithFlags(&S.kdone, cudaEventDisableTiming));
         LMIEB_CUDA_TRY(cudaEventCreateWithFlags(&S.done, cudaEventDisableTiming));
         for (cudaEvent_t &e : S.piece) LMIEB_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -524,6 +534,18 @@ int run_accumulate(Plan &L, cudaStream_t s) {
         return 0;
     }
     if (L.save_control != 2) {
+        // int8 K3's row exponents and A operand (the angles only) on the slot's
+        // side stream while K1 runs: K1 keeps 8 warps per SM, so their blocks
+        // find room beside it (with per-stage timing: in line, below)
+        const bool fork = L.oz && L.n_ang > 0 && L.side && !g_ctx.timing;
+        if (fork) {
+            LMIEB_CUDA_TRY(cudaEventRecord(L.fork, s));
+            LMIEB_CUDA_TRY(cudaStreamWaitEvent(L.side, L.fork, 0));
+            if (launch_oz_operands(L.side, B, L.n_rx, L.rx_start, L.rowexp, L.n_arow, L.a_start, L.aop, 0,
+                                   nullptr, nullptr, nullptr))
+                return -1;
+            LMIEB_CUDA_TRY(cudaEventRecord(L.join, L.side));
+        }
         if (L.n_gseg > 0) {
             if (launch_gather(s, L.n_gseg, L.gsegs, L.coef, L.rs)) return -1;
         } else {
@@ -543,8 +565,9 @@ int run_accumulate(Plan &L, cudaStream_t s) {
             launch_angular_tc(s, B, L.n_ang, L.ang, L.bop, L.part, L.tc_seg, L.o_trunc + 2 * L.ncase))
             return -1;
         if (L.oz && L.n_ang > 0) {
-            if (launch_oz_operands(s, B, L.n_rx, L.rx_start, L.rowexp, L.n_arow, L.a_start, L.aop, L.n_groups,
-                                   L.coef, L.bop8, L.colexp))
+            if (fork) LMIEB_CUDA_TRY(cudaStreamWaitEvent(s, L.join, 0));
+            if (launch_oz_operands(s, B, fork ? 0 : L.n_rx, L.rx_start, L.rowexp, fork ? 0 : L.n_arow, L.a_start,
+                                   L.aop, L.n_groups, L.coef, L.bop8, L.colexp))
                 return -1;
             if (g_ctx.timing) LMIEB_CUDA_TRY(cudaEventRecord(g_ctx.k3[0], s));
             if (launch_angular_oz(s, B, L.n_ang, L.ang, L.bop8, L.part, L.o_trunc + 2 * L.ncase)) return -1;
@@ -753,6 +776,9 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
     S.have_plan = false;        // the slot's graph is kept while the plan repeats (below)
     Plan &L = *S.plan;
     L = Plan();
+    L.side = S.side;
+    L.fork = S.fork;
+    L.join = S.join;
     const lmieb_problem &p0 = ps[0];
     const int nd = p0.nd, nd1 = p0.nd1, nd2 = p0.nd2, ncol = 1 + nd;
     const size_t Q = (size_t) 4 * ncol;
