@@ -37,6 +37,7 @@ constexpr int NSTAGE = LMIEB_N_STAGES;
 constexpr size_t FLUSH_BYTES = (size_t) 256 << 20;     // > 126 MB L2
 constexpr size_t BATCH_BYTES = (size_t) 24 << 30;      // device working set of one sub-batch
 constexpr int MAX_PIECES = 16;                         // results come back in up to 16 pieces of cases
+constexpr int SLOT_GRAPHS = 4;                         // captured kernel sequences kept per slot
 constexpr size_t PIECE_BYTES = (size_t) 8 << 20;       // of about 8 MB or more
 
 // Every staged array starts on a 256-byte boundary and takes at least one
@@ -90,9 +91,18 @@ struct Slot {
     cudaEvent_t piece[MAX_PIECES] = {};  // after the copy of each piece of the results
     cudaEvent_t t_begin = nullptr, t_end = nullptr;   // device span of the sub-batch
     bool have_plan = false;
-    cudaGraphExec_t graph = nullptr;   // the plan's kernel sequence, captured for re-runs
-    unsigned long long graph_sig = 0;  // the plan the graph was captured from
-    unsigned long long last_sig = 0;   // the plan of the slot's previous sub-batch
+    // Kernel sequences of the slot's recent plans, captured for re-runs.  A
+    // pipelined call gives each slot several parts in turn, so one graph per
+    // slot would be replaced by every part; the cache keeps SLOT_GRAPHS of
+    // them (least recently used goes first), each replayed only for the plan
+    // whose signature it was captured from.
+    struct Graph {
+        cudaGraphExec_t exec = nullptr;
+        unsigned long long sig = 0, used = 0;
+    } graphs[SLOT_GRAPHS];
+    unsigned long long seen[2 * SLOT_GRAPHS] = {};   // signatures of the slot's recent plans (a ring)
+    int seen_at = 0;
+    unsigned long long clock = 0;
     Pending pend;
 };
 
@@ -463,9 +473,35 @@ bool fault_injected(const char *site) {
     return false;
 }
 
+// Forgets every captured sequence of the slot (its arena or a pool they
+// point at was replaced).
 void drop_graph(Slot &S) {
-    if (S.graph) cudaGraphExecDestroy(S.graph);
-    S.graph = nullptr;
+    for (Slot::Graph &g : S.graphs) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        g = Slot::Graph();
+    }
+    for (unsigned long long &v : S.seen) v = 0;
+}
+
+// The slot's captured sequence of plan `sig`, or null.
+cudaGraphExec_t find_graph(Slot &S, unsigned long long sig) {
+    for (Slot::Graph &g : S.graphs)
+        if (g.exec && g.sig == sig) {
+            g.used = ++S.clock;
+            return g.exec;
+        }
+    return nullptr;
+}
+
+// Whether plan `sig` came to the slot recently; records it.
+bool seen_plan(Slot &S, unsigned long long sig) {
+    bool hit = false;
+    for (unsigned long long v : S.seen) hit = hit || v == sig;
+    if (!hit) {
+        S.seen[S.seen_at] = sig;
+        S.seen_at = (S.seen_at + 1) % (2 * SLOT_GRAPHS);
+    }
+    return hit;
 }
 
 int ensure_device(Slot &S, size_t bytes) {
@@ -649,14 +685,22 @@ int capture_plan(Slot &S, cudaStream_t s) {
         fprintf(stderr, "ERROR: lmie_b200: graph capture failed (%s)\n", cudaGetErrorString(ec));
         return -1;
     }
-    const cudaError_t ei = fault_injected("graph") ? cudaErrorInvalidValue : cudaGraphInstantiate(&S.graph, g, 0);
+    // into a free entry, else in place of the least recently used
+    Slot::Graph *slot_g = &S.graphs[0];
+    for (Slot::Graph &e : S.graphs)
+        if (!e.exec || (slot_g->exec && e.used < slot_g->used)) slot_g = &e;
+    if (slot_g->exec) cudaGraphExecDestroy(slot_g->exec);
+    *slot_g = Slot::Graph();
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t ei = fault_injected("graph") ? cudaErrorInvalidValue : cudaGraphInstantiate(&exec, g, 0);
     cudaGraphDestroy(g);
     if (ei != cudaSuccess) {
-        S.graph = nullptr;
         fprintf(stderr, "ERROR: lmie_b200: graph instantiation failed (%s)\n", cudaGetErrorString(ei));
         return -1;
     }
-    S.graph_sig = plan_sig(*S.plan);
+    slot_g->exec = exec;
+    slot_g->sig = plan_sig(*S.plan);
+    slot_g->used = ++S.clock;
     ++c.graph_captures;
     return 0;
 }
@@ -1719,17 +1763,21 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         LMIEB_CUDA_TRY(cudaEventRecord(c.gl_ready, s));
         c.gl_pending = true;
     }
-    // A sub-batch whose kernel sequence is the slot's previous one again (the
-    // same structure of radii, orders and angles in the same arena: retrieval
-    // loops that change the refractive index or the weights) replays it as a
-    // CUDA graph, captured the second time it comes.
+    // A sub-batch whose kernel sequence the slot ran recently (the same
+    // structure of radii, orders and angles in the same arena: retrieval loops
+    // that change the refractive index or the weights, the parts of repeated
+    // pipelined calls) replays it as a CUDA graph, captured the second time it
+    // comes.
     const unsigned long long sig = plan_sig(L);
-    if (S.graph && S.graph_sig != sig) drop_graph(S);
     const bool replayable = !c.timing && L.acc_mode == LMIEB_ACC_WHOLE && L.save_control == 0;
-    if (replayable && !S.graph && S.last_sig == sig && capture_plan(S, s)) return -1;
-    S.last_sig = sig;
-    if (replayable && S.graph) {
-        LMIEB_CUDA_TRY(cudaGraphLaunch(S.graph, s));
+    cudaGraphExec_t graph = replayable ? find_graph(S, sig) : nullptr;
+    const bool again = seen_plan(S, sig);
+    if (replayable && !graph && again) {
+        if (capture_plan(S, s)) return -1;
+        graph = find_graph(S, sig);
+    }
+    if (graph) {
+        LMIEB_CUDA_TRY(cudaGraphLaunch(graph, s));
         ++c.graph_replays;
     } else if (run_accumulate(L, s)) {
         return -1;
@@ -2317,18 +2365,19 @@ extern "C" int lmieb_rerun_device(int reps, int flush_l2, double *ms_total, doub
     if (flush_l2 && !c.flush) LMIEB_CUDA_TRY(cudaMalloc((void **) &c.flush, FLUSH_BYTES));
     const bool was = c.timing;
     // each plan's kernel sequence as one CUDA graph (captured once per plan)
+    cudaGraphExec_t gx[2] = {nullptr, nullptr};
     for (int i = 0; i < ns; ++i) {
         Slot &S = c.slot[c.call_slot[i]];
-        if (S.graph && S.graph_sig == plan_sig(*S.plan)) continue;
-        drop_graph(S);
-        if (capture_plan(S, c.stream)) return -1;
+        const unsigned long long sig = plan_sig(*S.plan);
+        if (!find_graph(S, sig) && capture_plan(S, c.stream)) return -1;
+        gx[i] = find_graph(S, sig);
     }
     double total = 0., st[NSTAGE] = {}, k3 = 0.;
     cudaEvent_t e0 = c.ev[0], e1 = c.ev[NSTAGE];
     for (int i = 0; i < reps; ++i) {
         if (flush_l2) LMIEB_CUDA_TRY(cudaMemsetAsync(c.flush, i & 0xff, FLUSH_BYTES, c.stream));
         LMIEB_CUDA_TRY(cudaEventRecord(e0, c.stream));
-        for (int j = 0; j < ns; ++j) LMIEB_CUDA_TRY(cudaGraphLaunch(c.slot[c.call_slot[j]].graph, c.stream));
+        for (int j = 0; j < ns; ++j) LMIEB_CUDA_TRY(cudaGraphLaunch(gx[j], c.stream));
         LMIEB_CUDA_TRY(cudaEventRecord(e1, c.stream));
         LMIEB_CUDA_TRY(cudaEventSynchronize(e1));
         float ms = 0.f;
