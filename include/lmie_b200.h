@@ -117,12 +117,12 @@ int lmieb_oz_selftest(int K, double *max_rel_err);
  * the product kernel's bounded waits, taken without a fault. */
 int lmieb_oz_selftest_wait(int K, long long wait_cycles, int withhold, double *max_rel_err);
 
-/* Graph replay of the product path: a sub-batch whose kernel sequence is the
- * same as the previous one on its slot -- the same structure of cases,
- * radii, orders and angles in the same device arena, as in retrieval loops
- * that change the refractive index or the size-distribution weights between
- * calls -- runs as one CUDA graph, captured the second time the sequence
- * comes.  Counts of the sequences captured and replayed since the library was
+/* Graph replay of the product path: a sub-batch whose kernel sequence is one
+ * its slot ran recently (each slot keeps four) -- the same structure of
+ * cases, radii, orders and angles in the same device arena, as in retrieval
+ * loops that change the refractive index or the size-distribution weights
+ * between calls, or the parts of a repeated pipelined call -- runs as one
+ * CUDA graph, captured the second time the sequence comes.  Counts of the sequences captured and replayed since the library was
  * loaded (timing mode, radius groups and save_control launch kernel by
  * kernel).  Returns 0. */
 int lmieb_graph_stats(long long *captures, long long *replays);
