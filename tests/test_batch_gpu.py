@@ -176,6 +176,35 @@ def test_user_angle_parts_only_reorder_sums():
             assert libs.relmax(getattr(a, name), getattr(b, name)) <= 1e-13, (i, name)
 
 
+def test_pipelined_calls_replay_their_parts_as_graphs():
+    """A call cut into four parts hands each of the two slots two parts in
+    turn; each slot keeps the graphs of its recent plans, so repeating the
+    call replays every part (captured on the second call): the results are
+    those of the first, kernel-by-kernel call bit for bit."""
+    import ctypes as C
+    lib = libs.product()
+    lib.lmieb_graph_stats.argtypes = [C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
+    def stats():
+        a, b = C.c_longlong(), C.c_longlong()
+        lib.lmieb_graph_stats(C.byref(a), C.byref(b))
+        return a.value, b.value
+    cases = workloads.batched_uneven(96)
+    try:
+        lib.lmieb_set_pipeline(4)
+        first = abi.solve_batch(lib, cases, n_threads=4)
+        c0, r0 = stats()
+        for _ in range(3):
+            again = abi.solve_batch(lib, cases, n_threads=4)
+        c1, r1 = stats()
+    finally:
+        lib.lmieb_set_pipeline(0)
+    assert c1 - c0 <= 4 and r1 - r0 >= 8, (c0, r0, c1, r1)
+    for i, (a, b) in enumerate(zip(first, again)):
+        assert a.rc == 0 and b.rc == 0 and a.n_coef == b.n_coef and a.scalars == b.scalars, i
+        for name in ("gc", "pf", "gc_l", "pf_l"):
+            assert np.array_equal(getattr(a, name), getattr(b, name)), (i, name)
+
+
 def test_repeated_plan_is_replayed_as_a_graph():
     """A solve whose structure repeats (here the refractive index changes
     between calls, the radii, orders and angles do not) is captured the
