@@ -326,12 +326,12 @@ typedef struct {
      double *qx, *qw, *nr, *qx_l, *qw_l, *nr_l;
      double *x, *xl, *w, *w2, *mu_user, *dev_out;
      double **rows;             /* the caller's output rows, in device column order */
-     /* every array above comes out of one zeroed block (a second one holds
-        this process's share of the radii): a case's scratch is released
-        with one or two free() calls, not one per array */
+     int *n1r, *n2r, *idx1, *idx2;
+     /* the arrays above (qx .. idx2) come out of one zeroed block (a second
+        one holds this process's share of the radii): a case's scratch is
+        released with one or two calls, not one per array */
      char *blk, *blk2, *blk_at;
      size_t blk_size, blk_left;
-     int *n1r, *n2r, *idx1, *idx2;
      /* radius sharing (lmieb.h): the mode and this process's share */
      int acc_mode, share_rank, share_world;
      const double *acc_in;
@@ -443,7 +443,7 @@ static void *job_take(case_job *j, size_t bytes) {
 /* Keeps radius i of a prepared case when i % share_world == share_rank (the
  * reference's MPI master deals its radii out to the workers the same way,
  * src/lmie_schedule.c:574-597), none when finishing from summed integrals.
- * Returns the number kept. */
+ * Returns the number kept, or -1 when the host is out of memory. */
 static int share_radii(case_job *j, int n, int nd, int nd1) {
      const int w = j->share_world, r0 = j->share_rank;
      const int m = j->acc_mode == LMIEB_ACC_FINISH ? 0 : (n > r0 ? (n - r0 + w - 1) / w : 0);
