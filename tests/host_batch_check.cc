@@ -3,8 +3,9 @@
 // hands to the device (a hash of every per-radius array) and writes
 // recognisable results, so that the preparation, the chunking into parts,
 // the per-case scratch blocks (carved from one pooled block, re-zeroed when
-// reused), the scatter into the callers' arrays, the failure path and the
-// radius sharing can be checked without a GPU.  Prints "ok" or the failed
+// reused), the quadrature of every size distribution, the scatter into the
+// callers' arrays, the failure path and the radius sharing can be checked
+// without a GPU.  Prints "ok" or the failed
 // check; exit status 0 only with "ok".
 #include <algorithm>
 #include <atomic>
@@ -191,6 +192,67 @@ lmie_in_data make_case(int i) {
     return in;
 }
 
+// case i of the other distributions (the parameters of the named test cases)
+lmie_in_data make_other(int i) {
+    lmie_in_data in = make_case(0);
+    in.lambda = 0.6 + 0.01 * i;
+    in.mr = 1.6 + 1e-3 * i;             // the key of the case (apart from make_case's)
+    in.n_int1 = 0;
+    in.n_int2 = 3;
+    in.n_quad = 40;
+    in.a3 = in.a4 = in.a5 = 0.;
+    in.r1 = 0.01;
+    in.r2 = 4.;
+    switch (i % 7) {
+    case 0:
+        in.dist_type = SIZE_DIST_MODIFIED_GAMMA;
+        in.a1 = 2.;
+        in.a2 = 0.5;
+        in.a3 = 1.;
+        in.r2 = 3.;
+        in.n_int2 = 2;
+        in.n_quad = 50;
+        break;
+    case 1:
+        in.dist_type = SIZE_DIST_POWER_LAW;      // its range follows from a1, a2
+        in.a1 = 0.5;
+        in.a2 = 0.2;
+        break;
+    case 2:
+        in.dist_type = SIZE_DIST_MODIFIED_POWER_LAW;
+        in.a1 = -3.;
+        in.r1 = 0.1;
+        in.r2 = 2.;
+        in.n_int1 = 2;
+        in.n_quad = 30;
+        break;
+    case 3:
+        in.dist_type = SIZE_DIST_MODIFIED_BIMODAL_LOG_NORMAL;
+        in.a1 = 0.2;
+        in.a2 = 0.2;
+        in.a3 = 1.;
+        in.a4 = 0.3;
+        in.a5 = 0.1;
+        break;
+    case 4:
+        in.dist_type = SIZE_DIST_EXPONENTIAL;
+        in.a1 = 2.;
+        in.r2 = 2.;
+        break;
+    case 5:
+        in.dist_type = SIZE_DIST_MONO;
+        in.a1 = in.r1 = in.r2 = 1.3;
+        break;
+    default:
+        in.dist_type = SIZE_DIST_GAMMA;          // an odd number of Gauss points
+        in.a1 = 0.5;
+        in.a2 = 0.2;
+        in.n_quad = 41;
+        break;
+    }
+    return in;
+}
+
 // the scatter of case i's stubbed results into out
 void check_out(const lmie_in_data &in, const lmie_out_data &o, const Seen &s, int i) {
     const double mr = in.mr;
@@ -280,6 +342,28 @@ int main() {
             CHECK(g_batch[in[i].mr].hash == first[in[i].mr], "case %d after a failure", i);
             check_out(in[i], o2[i], g_batch[in[i].mr], i);
             lmie_out_free(&o2[i], 1);
+        }
+    }
+
+    // the other size distributions (their quadratures and weights) the same way
+    {
+        std::vector<lmie_in_data> oth;
+        for (int i = 0; i < 14; ++i) oth.push_back(make_other(i));
+        std::map<double, unsigned long long> h1;
+        for (int q = 0; q < 3; ++q) {
+            lmieb_set_pipeline(q == 1 ? 4 : 1);
+            std::vector<lmie_out_data> o(oth.size());
+            g_batch.clear();
+            const int rc = lmie_solution_batch2((int) oth.size(), oth.data(), o.data(), 1, 0, 4, 0);
+            CHECK(rc == 0, "other distributions: rc %d (call %d)", rc, q);
+            for (size_t i = 0; i < oth.size(); ++i) {
+                const Seen &s = g_batch[oth[i].mr];
+                CHECK(s.n > 0 && s.n_coef > 8, "other case %d: %d radii, %d coefficients", (int) i, s.n, s.n_coef);
+                if (q == 0) h1[oth[i].mr] = s.hash;
+                else CHECK(s.hash == h1[oth[i].mr], "other case %d differs (call %d)", (int) i, q);
+                if (s.n_coef > 8) check_out(oth[i], o[i], s, 100 + (int) i);
+                lmie_out_free(&o[i], 1);
+            }
         }
     }
 
