@@ -29,7 +29,8 @@ namespace {
 
 struct Seen {
     unsigned long long hash = 0;
-    int n_coef = 0, n = 0;
+    int n_coef = 0, n = 0, n_qang = 0, save_control = 0;
+    bool has_w2 = false, has_saved = false;
     std::vector<double> x;
 };
 std::mutex g_mu;
@@ -59,10 +60,15 @@ Seen record(const lmieb_problem &p) {
     h = fnv(h, p.n1r, sizeof(int) * p.n);
     h = fnv(h, p.n2r, sizeof(int) * p.n);
     if (p.n_angles > 0) h = fnv(h, p.mu_user, sizeof(double) * p.n_angles);
+    if (p.save_control == 2 && p.w2) h = fnv(h, p.w2, sizeof(double) * (p.nd > 0 ? p.nd : 1) * p.n);
     Seen s;
     s.hash = h;
     s.n_coef = p.n_coef;
     s.n = p.n;
+    s.n_qang = p.n_qang;
+    s.save_control = p.save_control;
+    s.has_w2 = p.w2 != nullptr;
+    s.has_saved = p.save1_rows != nullptr && (p.n_qang == 0 || p.save2_rows != nullptr);
     s.x.assign(p.x, p.x + p.n);
     return s;
 }
@@ -82,6 +88,10 @@ void fill(const lmieb_problem &p, lmieb_result &r) {
             for (int j = 0; j < p.n_angles; ++j) r.pf_rows[k][j] = row_of(p.mr, k, j) + 0.5;
     }
     r.n_coef_out = p.n_coef - 1;
+    if (r.save1)
+        for (int i = 0; i < 4 * p.n; ++i) r.save1[i] = p.mr + i * 1e-6;
+    if (r.save2)
+        for (size_t i = 0; i < (size_t) 4 * p.n * p.n_qang; ++i) r.save2[i] = p.mr - i * 1e-9;
 }
 
 }  // namespace
@@ -324,6 +334,38 @@ int main() {
         CHECK(share.n == (full.n - 1 + 2) / 3, "share of %d radii: %d", full.n, share.n);
         for (int t = 0; t < share.n && t < (int) share.x.size(); ++t)
             CHECK(share.x[t] == full.x[1 + 3 * t], "share radius %d", t);
+        lmie_out_free(&o, 1);
+    }
+
+    // save_control 1 (the kernels come back through save1 / save2, which
+    // belong to the caller), then 2 (a re-weighting call that reads them and
+    // hands over the shape-derivative weights w2)
+    {
+        lmie_in_data sc = in[2];
+        sc.save_control = 1;
+        lmie_out_data o;
+        memset(&o, 0, sizeof o);
+        CHECK(lmie_solution(&sc, &o, 1, 0, 4, 0) == 0, "save_control 1");
+        const Seen s1 = g_single[sc.mr];
+        CHECK(s1.save_control == 1 && o.save1 && o.save2, "save_control 1 kept no kernels");
+        if (o.save1 && o.save2) {
+            CHECK(o.save1[3][s1.n - 1] == sc.mr + (3 * s1.n + s1.n - 1) * 1e-6, "save1");
+            CHECK(o.save2[0][1][2] == sc.mr - (1.0 * s1.n_qang + 2) * 1e-9, "save2");
+        }
+        check_out(sc, o, s1, 2);
+        sc.save_control = 2;
+        sc.a2 *= 1.1;                        // new shape weights, the same radii
+        CHECK(lmie_solution(&sc, &o, 0, 0, 4, 0) == 0, "save_control 2");
+        const Seen s2 = g_single[sc.mr];
+        CHECK(s2.save_control == 2 && s2.has_w2 && s2.has_saved && s2.n == s1.n, "save_control 2 inputs");
+        check_out(sc, o, s2, 2);
+        sc.save_control = 2;                 // without kept kernels: rejected
+        lmie_out_data none;
+        memset(&none, 0, sizeof none);
+        CHECK(lmie_solution(&sc, &none, 1, 0, 4, 0) == -1, "save_control 2 without kernels accepted");
+        lmie_out_free(&none, 1);
+        free(o.save1);
+        free(o.save2);
         lmie_out_free(&o, 1);
     }
 

@@ -3,7 +3,8 @@ the device layer replaced by a recording stub (tests/host_batch_check.cc):
 every case hands the device the same per-radius arrays whether the call is
 cut into 1, 3 or 4 parts and when its scratch blocks are reused from the
 pool, for every size distribution; the stub's results land in the right
-callers' arrays; a single solve prepares what the batch prepares; a process
+callers' arrays; a single solve prepares what the batch prepares; save_control
+1 returns the kernels and 2 reads them with its w2 weights; a process
 of a radius group gets radii rank, rank + world, ...; a case the host
 rejects fails the call and the next call is whole again."""
 import shutil
