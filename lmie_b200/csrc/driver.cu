@@ -1408,7 +1408,7 @@ int submit_sub(Slot &S, long long ticket, int ncase, const lmieb_problem *ps, lm
         } else if (L.save_control != 2) {
             nl += (gsegs.empty() ? (long long) std::max(L.nd1c, 1) : 1) + 1;   // K1 per chunk (or its copy), K2
             if (L.tc) nl += (L.n_ang > 0) + (L.n_ang64 > 0 ? L.n_ang_launch : 0);   // K3
-            else if (L.oz) nl += (L.n_ang > 0 ? 3 : 0) + (L.n_ang64 > 0 ? L.n_ang_launch : 0);   // operands, K3
+            else if (L.oz) nl += (L.n_ang > 0 ? 4 : 0) + (L.n_ang64 > 0 ? L.n_ang_launch : 0);   // row exponents, A, B, K3
             else nl += L.n_ang > 0 ? L.n_ang_launch : 0;
             if (L.n_ang > 0 || L.n_ang64 > 0) nl += 1;                          // group reduction
         } else {
