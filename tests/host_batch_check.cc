@@ -4,8 +4,8 @@
 // recognisable results, so that the preparation, the chunking into parts,
 // the per-case scratch blocks (carved from one pooled block, re-zeroed when
 // reused), the quadrature of every size distribution, the scatter into the
-// callers' arrays, the failure path and the radius sharing can be checked
-// without a GPU.  Prints "ok" or the failed
+// callers' arrays (the Fortran entry's column-major ones too), save_control,
+// the failure path and the radius sharing can be checked without a GPU.  Prints "ok" or the failed
 // check; exit status 0 only with "ok".
 #include <algorithm>
 #include <atomic>
@@ -319,6 +319,45 @@ int main() {
         CHECK(g_single.count(in[5].mr) && g_single[in[5].mr].hash == first[in[5].mr], "single case differs");
         check_out(in[5], o, g_single[in[5].mr], 5);
         lmie_out_free(&o, 1);
+    }
+
+    // the Fortran entry (lmie_solution2_l_, all arguments by reference) on
+    // flat column-major arrays: gc(max_coef,6), gc_l(max_coef,6,nd),
+    // pf(n_angles,6), pf_l(n_angles,6,nd) -- the batch's problem, and the
+    // results at their column-major places
+    {
+        lmie_in_data c = in[3];
+        int mc = lmie_calc_max_coef(c.lambda, c.dist_type, c.a1, c.a2, c.a3, c.r1, c.r2);
+        int na = c.n_angles, nd = ND, n_coef = 0, one = 1, zero = 0, nt = 4;
+        int n_int1 = c.n_int1, n_int2 = c.n_int2, n_quad = c.n_quad;
+        enum size_dist_type dt = c.dist_type;
+        double lam = c.lambda, mr = c.mr, mi = c.mi, a1 = c.a1, a2 = c.a2, a3 = c.a3, a4 = c.a4, a5 = c.a5;
+        double r1 = c.r1, r2 = c.r2, acc = c.accuracy;
+        std::vector<double> gc(6 * mc), gcl(6 * mc * nd), pf(6 * na), pfl(6 * na * nd), theta(na);
+        double sc[13] = {}, scl[13][ND] = {};
+        double **sv1 = nullptr, ***sv2 = nullptr;
+        const int rc = lmie_solution2_l_(
+            &one, &zero, &one, &dt, &n_int1, &n_int2, &n_quad, &na, &nd, &zero, &lam, &mr, &mi, &a1, &a2, &a3,
+            &a4, &a5, &r1, &r2, c.lambda_l, c.mr_l, c.mi_l, c.a1_l, c.a2_l, c.a3_l, c.a4_l, c.a5_l, c.r1_l,
+            c.r2_l, &acc, &n_coef, &sc[0], &sc[1], &sc[2], &sc[3], &sc[4], &sc[5], &sc[6], &sc[7], &sc[8],
+            &sc[9], &sc[10], &sc[11], &sc[12], gc.data(), nullptr, theta.data(), pf.data(), scl[0], scl[1],
+            scl[2], scl[3], scl[4], scl[5], scl[6], scl[7], scl[8], scl[9], scl[10], scl[11], scl[12],
+            gcl.data(), nullptr, pfl.data(), &sv1, &sv2, &mc, &zero, &nt, &zero);
+        CHECK(rc == 0, "Fortran entry rc %d", rc);
+        const Seen &s = g_single[c.mr];
+        CHECK(s.hash == first[c.mr], "Fortran entry: the problem differs from the batch's");
+        CHECK(n_coef == s.n_coef - 1, "Fortran entry n_coef %d", n_coef);
+        CHECK(sc[9] == scal_of(mr, 0, 0) && sc[12] == scal_of(mr, 0, 3), "Fortran entry cext, g");
+        CHECK(scl[10][2] == scal_of(mr, 3, 1), "Fortran entry csca_l");
+        for (int e = 0; e < 6 && s.n_coef > 5; ++e) {
+            CHECK(gc[(size_t) e * mc + 5] == row_of(mr, e, 5), "Fortran gc(6,%d)", e + 1);
+            CHECK(pf[(size_t) e * na + 17] == row_of(mr, e, 17) + 0.5, "Fortran pf(18,%d)", e + 1);
+            for (int k = 0; k < nd; ++k) {
+                CHECK(gcl[((size_t) k * 6 + e) * mc + 5] == row_of(mr, (1 + k) * 6 + e, 5), "Fortran gc_l");
+                CHECK(pfl[((size_t) k * 6 + e) * na + 17] == row_of(mr, (1 + k) * 6 + e, 17) + 0.5,
+                      "Fortran pf_l");
+            }
+        }
     }
 
     // radius sharing: process 1 of 3 gets radii 1, 4, 7, ... of the case

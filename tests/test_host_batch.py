@@ -3,8 +3,10 @@ the device layer replaced by a recording stub (tests/host_batch_check.cc):
 every case hands the device the same per-radius arrays whether the call is
 cut into 1, 3 or 4 parts and when its scratch blocks are reused from the
 pool, for every size distribution; the stub's results land in the right
-callers' arrays; a single solve prepares what the batch prepares; save_control
-1 returns the kernels and 2 reads them with its w2 weights; a process
+callers' arrays; a single solve prepares what the batch prepares, and so
+does the Fortran entry on column-major arrays, whose results land at their
+column-major places; save_control 1 returns the kernels and 2 reads them
+with its w2 weights; a process
 of a radius group gets radii rank, rank + world, ...; a case the host
 rejects fails the call and the next call is whole again."""
 import shutil
@@ -21,7 +23,7 @@ def _build_and_run(tmp_path, flags):
     cc, cxx = shutil.which("gcc"), shutil.which("g++")
     inc = ["-I", str(ROOT / "include"), "-I", str(CSRC)]
     objs = []
-    for src in ("host_api.c", "host_dist.c"):
+    for src in ("host_api.c", "host_dist.c", "host_fortran.c"):
         obj = tmp_path / (src + ".o")
         subprocess.run([cc, *flags, "-std=gnu99", "-fPIC", *inc, "-c", str(CSRC / src), "-o", str(obj)],
                        check=True)
